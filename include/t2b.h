@@ -1,0 +1,193 @@
+/*
+ * t2b.h - C ABI of the Blackwell (sm_100a) E-step library libt2b.so.
+ *
+ * The E-step hot path of RELION's MlOptimiser (as accelerated by T2-RELION):
+ * Fourier-slice projection of the references, diff2 over every
+ * (particle, orientation, translation), conversion to posterior weights with
+ * the significance threshold, the adaptive-oversampling fine pass, the
+ * weighted sums, backprojection into the padded reconstruction grid and the
+ * skip-gridding division of backprojected data by backprojected weights.
+ *
+ * Conventions
+ *  - every function returns T2B_OK (0) or a T2B_ERR_* code; t2b_last_error()
+ *    gives the message of the calling thread's last failure.  No C++
+ *    exception crosses this boundary.
+ *  - the caller owns host buffers; the context owns device buffers.  Device
+ *    pointers passed in (the *_device entry points) stay owned by the caller.
+ *  - complex arrays are interleaved (re, im) float32.  2D Fourier images are
+ *    the windowed FFTW half transform of a current_size x current_size image:
+ *    current_size rows x (current_size/2 + 1) columns, pixel n = i*xh + j,
+ *    ky = i for i < xh else i - current_size, kx = j.
+ *  - 3D model grids use the centred half-complex layout of RELION's Projector:
+ *    element (x, y, z) at ((z - initz) * ydim + (y - inity)) * xdim + x.
+ *  - one context per device; calls on one context are serialised internally.
+ */
+#ifndef T2B_H
+#define T2B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define T2B_OK 0
+#define T2B_ERR_ARG 1        /* invalid argument / size                                  */
+#define T2B_ERR_CUDA 2       /* CUDA runtime or driver failure                           */
+#define T2B_ERR_NOSIGNIF 3   /* zero sum of weights / no significant sample (ERRNOSIGNIFS,
+                                ERRSUMWEIGHTZERO of src/error.h:259-280)                   */
+#define T2B_ERR_STATE 4      /* call order (e.g. E-step before t2b_configure)            */
+#define T2B_ERR_NOMEM 5      /* device memory or workspace capacity exceeded             */
+#define T2B_ERR_TIMEOUT 6    /* a bounded device-side wait ran out                       */
+#define T2B_ERR_UNSUPPORTED 7
+
+#define T2B_DIFF2_PLAIN_FP32 0   /* SIMT FP32 cross-term contraction                       */
+#define T2B_DIFF2_SPLIT_BF16 1   /* tcgen05 BF16 hi/lo three-product contraction, FP32 acc */
+
+typedef struct t2b_ctx t2b_ctx;
+
+/* Context on CUDA device `device`.  Replaces MlDeviceBundle construction
+ * (src/acc/cuda/cuda_ml_optimiser.h:17-72). */
+int t2b_create(int device, t2b_ctx** ctx);
+void t2b_destroy(t2b_ctx* ctx);
+const char* t2b_last_error(void);
+/* Library version string. */
+const char* t2b_version(void);
+
+/* Reference model of class `iclass` (AccProjector::setMdlDim + initMdl,
+ * src/acc/acc_projector.h:69-78).  ref_dim 3: xdim = pad/2+1, ydim = zdim =
+ * pad (the padded size of RELION's Projector, src/projector.cpp:55-80);
+ * ref_dim 2: zdim = 1.  `mdl` is host memory, complex interleaved. */
+int t2b_projector_set(t2b_ctx* ctx, int iclass, int ref_dim, int xdim, int ydim, int zdim,
+                      int inity, int initz, int r_max, int padding_factor, const float* mdl);
+
+/* Backprojection grid of class `iclass`, zeroed (AccBackprojector::setMdlDim
+ * + initMdl, src/acc/acc_backprojector.h:51-79). */
+int t2b_backprojector_init(t2b_ctx* ctx, int iclass, int ref_dim, int xdim, int ydim, int zdim,
+                           int inity, int initz, int r_max, int padding_factor);
+/* Zero the grid again (AccBackprojector::initMdl). */
+int t2b_backprojector_clear(t2b_ctx* ctx, int iclass);
+/* Copy grid to host (AccBackprojector::getMdlData, src/acc/acc_backprojector_impl.h:84-100).
+ * real/imag/weight each hold xdim*ydim*zdim floats. */
+int t2b_backprojector_get(t2b_ctx* ctx, int iclass, float* real, float* imag, float* weight);
+/* Device pointers of the grid (AccBackprojector::getMdlDataPtrs): complex
+ * interleaved data and weight; for an in-place NCCL reduction. */
+int t2b_backprojector_device_ptrs(t2b_ctx* ctx, int iclass, float** data, float** weight);
+
+/* Per-iteration sampling and E-step configuration.  Mirrors what
+ * MlOptimiserCuda reads from MlOptimiser / HealpixSampling
+ * (src/acc/acc_ml_optimiser_impl.h:2359-2560, src/healpix_sampling.cpp). */
+typedef struct t2b_config {
+    int ori_size;              /* full box size                                       */
+    int current_size;          /* windowed size of both passes (even)                 */
+    int ref_dim;               /* 3 (3D refs, 2D particles) or 2 (2D classification)  */
+    int nr_classes;
+    int n_dir, n_psi;          /* coarse orientations per class = n_dir * n_psi       */
+    int n_trans;               /* coarse translations                                 */
+    int adaptive_oversampling; /* 0: single pass; 1: coarse + fine pass               */
+    int nover_rot, nover_trans;/* oversampling factors of the fine pass (1 if none)   */
+    int maximum_significants;  /* <= 0: off (only 0/-1 supported)                     */
+    int diff2_mode;            /* T2B_DIFF2_*                                         */
+    int max_batch;             /* particles per t2b_estep_* call                      */
+    int _pad;
+    const double* eul_coarse;  /* n_dir*n_psi x 9, Euler matrices (Euler_angles2matrix) */
+    const double* eul_fine;    /* n_dir*n_psi*nover_rot x 9, or NULL                    */
+    const double* trans_px;    /* n_trans x 2: coarse shifts in pixels                  */
+    const double* trans_px_fine;/* n_trans*nover_trans x 2, or NULL                     */
+    const double* trans_prior; /* n_trans x 2: HealpixSampling::translations_{x,y}      */
+    const double* pdf_direction;/* nr_classes x n_dir                                   */
+    const double* pdf_class;   /* nr_classes                                            */
+    const int* mresol;         /* current_size*(current_size/2+1): ring index or -1     */
+    double sigma2_offset;
+    double pixel_size;
+    double adaptive_fraction;
+    size_t fine_capacity;      /* fine hypotheses per batch (0: default)                */
+} t2b_config;
+
+/* Validate the configuration, build the projection tables of all coarse and
+ * fine orientations and the phase tables, and size the workspace.  The
+ * projectors of all classes must be set first. */
+int t2b_configure(t2b_ctx* ctx, const t2b_config* cfg);
+
+/* One batch of particles.  Host variant: pointers are host memory.  Device
+ * variant: pointers are device memory (already resident). */
+typedef struct t2b_batch {
+    int n;                      /* particles in this batch (<= max_batch)               */
+    int _pad;
+    const float* fimg;          /* n x 2P, masked image (FFTW window), complex           */
+    const float* fimg_nomask;   /* n x 2P or NULL (then fimg is used)                    */
+    const float* ctf;           /* n x P                                                 */
+    const float* minvsigma2;    /* n x P, 1/(fudge*sigma2_noise[ires]), 0 outside mask   */
+    const double* scalars;      /* n x 8: minvsigma2_dc, highres_Xi2, old_offset x, y,
+                                   prior x, y, scale_correction, unused                  */
+} t2b_batch;
+
+typedef struct t2b_result {
+    double* min_diff2;          /* n: final pass (exp_min_diff2)                        */
+    double* sum_weight;         /* n: final pass (exp_sum_weight)                       */
+    double* sig_weight;         /* n: final pass (exp_significant_weight)               */
+    double* coarse_sum_weight;  /* n                                                    */
+    double* coarse_sig_weight;  /* n                                                    */
+    long long* nr_sign;         /* n: METADATA_NR_SIGN                                  */
+    long long* n_coarse_sig;    /* n: size of Mcoarse_significant                       */
+    double* pmax;               /* n: METADATA_PMAX                                     */
+    int* pose;                  /* n x 5: iclass, iorient, iover_rot, itrans, iover_trans */
+    double* wsum_norm;          /* n: exp_wsum_norm_correction                          */
+    double* sumw;               /* n: thr_sumw_group                                    */
+    double* wsum_sigma2_offset; /* n                                                    */
+    double* wsum_sigma2;        /* n x (ori_size/2+1)                                   */
+    double* wsum_pdf_class;     /* n x nr_classes                                       */
+    double* wsum_pdf_dir;       /* n x nr_classes*n_dir                                 */
+    int* status;                /* n: T2B_OK or T2B_ERR_NOSIGNIF per particle           */
+} t2b_result;
+
+/* E-step of one batch (MlOptimiserCuda::doThreadExpectationSomeParticles,
+ * src/acc/cuda/cuda_ml_optimiser.cu:1345-1405, minus image preparation):
+ * coarse pass, weights, fine pass, weights, weighted sums, backprojection into
+ * the grids of t2b_backprojector_init.  The host variant copies the batch in,
+ * runs, and copies the results out before returning.  The device variant only
+ * enqueues on `stream` (cudaStream_t, NULL = the context's stream); result
+ * pointers are device memory and valid after the stream completes. */
+int t2b_estep_batch_host(t2b_ctx* ctx, const t2b_batch* batch, const t2b_result* out);
+int t2b_estep_batch_device(t2b_ctx* ctx, const t2b_batch* batch, const t2b_result* out, void* stream);
+
+/* Skip-gridding reconstruction division in FP64 on the device
+ * (BackProjector::reconstruct, src/backprojector.cpp:1463-1531).  Output is
+ * the FFTW-ordered transform of a pad^3 volume, [pad][pad][pad/2+1] complex
+ * double, host memory. */
+int t2b_reconstruct_divide(t2b_ctx* ctx, int iclass, double* fconv);
+
+/* Projections of `n` orientations (host Euler matrices, n x 9) of class
+ * `iclass` on the current_size window (AccProjectorKernel::project3Dmodel,
+ * src/acc/acc_projectorkernel_impl.h:179-250); out: host, n x 2P. */
+int t2b_project(t2b_ctx* ctx, int iclass, const double* eulers, int n, int current_size, float* out);
+
+/* Inspection of the last batch (test support): coarse diff2 of particle b
+ * (nr_classes*n_dir*n_psi*n_trans floats, orientation-major), and the fine
+ * pass (pairs: coarse hidden index per significant pair; diff2: pairs x
+ * nover_rot*nover_trans).  *count receives the number of pairs. */
+int t2b_debug_coarse_diff2(t2b_ctx* ctx, int b, float* out);
+int t2b_debug_fine(t2b_ctx* ctx, int b, long long* pairs, float* diff2, long long cap, long long* count);
+
+/* Device time of the stages of the last batch, in ms (CUDA events):
+ * [0] prep+norms, [1] coarse diff2, [2] coarse weights, [3] fine pass,
+ * [4] fine weights, [5] weighted sums + backprojection.  n <= 6. */
+int t2b_last_stage_ms(t2b_ctx* ctx, float* ms, int n);
+
+/* Host sampling (HealpixSampling, src/healpix_sampling.cpp:534-640,
+ * 1787-2040), C1 symmetry, no perturbation.  Fills Euler matrices of the
+ * coarse orientations (idir*n_psi + ipsi), of the fine orientations
+ * ((idir*n_psi + ipsi)*nover_rot + iover_rot), the coarse/fine translations
+ * (pixels) and the prior translations (Angstrom).  Query sizes with NULL
+ * outputs.  ref_dim 2 gives in-plane (psi-only) sampling. */
+int t2b_sampling(int ref_dim, int healpix_order, double psi_step, int adaptive_oversampling,
+                 double offset_range_px, double offset_step_px, double pixel_size,
+                 int* n_dir, int* n_psi, int* n_trans, int* nover_rot, int* nover_trans,
+                 double* eul_coarse, double* eul_fine, double* trans_px, double* trans_px_fine,
+                 double* trans_prior, double* angles_coarse /* n_dir*n_psi x 3: rot tilt psi */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* T2B_H */

@@ -1,0 +1,364 @@
+"""Host-side mirror of the RELION E-step accelerator interface over libt2b.so.
+
+The reference drives its GPU E-step through C++ classes: AccProjector
+(src/acc/acc_projector.h:69-78), AccBackprojector (src/acc/acc_backprojector.h:
+51-79), MlDeviceBundle and MlOptimiserCuda (src/acc/cuda/cuda_ml_optimiser.h:
+17-186).  This module exposes the same surface in Python on top of the C ABI in
+include/t2b.h; include/t2b_adapter.hpp does the same for C++ callers.
+
+Every call goes to the CUDA library.  There is no CPU fallback: importing this
+package fails loudly when libt2b.so is missing, and every non-zero status of
+the C ABI raises T2BError with the library's message.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libt2b.so")
+
+T2B_OK = 0
+T2B_ERR_ARG = 1
+T2B_ERR_CUDA = 2
+T2B_ERR_NOSIGNIF = 3
+T2B_ERR_STATE = 4
+T2B_ERR_NOMEM = 5
+T2B_ERR_TIMEOUT = 6
+T2B_ERR_UNSUPPORTED = 7
+DIFF2_PLAIN_FP32 = 0
+DIFF2_SPLIT_BF16 = 1
+
+# every symbol include/t2b.h declares
+ABI_SYMBOLS = (
+    "t2b_create", "t2b_destroy", "t2b_last_error", "t2b_version",
+    "t2b_projector_set", "t2b_backprojector_init", "t2b_backprojector_clear",
+    "t2b_backprojector_get", "t2b_backprojector_device_ptrs", "t2b_configure",
+    "t2b_estep_batch_host", "t2b_estep_batch_device", "t2b_reconstruct_divide",
+    "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_last_stage_ms",
+    "t2b_sampling",
+)
+
+
+class T2BError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"t2b error {code}: {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with t2-relion_b200/build.py "
+                          "(__graft_entry__.build()); there is no CPU fallback")
+    return ctypes.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+_p = ctypes.c_void_p
+_d = ctypes.POINTER(ctypes.c_double)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("ori_size", ctypes.c_int), ("current_size", ctypes.c_int), ("ref_dim", ctypes.c_int),
+        ("nr_classes", ctypes.c_int), ("n_dir", ctypes.c_int), ("n_psi", ctypes.c_int),
+        ("n_trans", ctypes.c_int), ("adaptive_oversampling", ctypes.c_int),
+        ("nover_rot", ctypes.c_int), ("nover_trans", ctypes.c_int),
+        ("maximum_significants", ctypes.c_int), ("diff2_mode", ctypes.c_int),
+        ("max_batch", ctypes.c_int), ("_pad", ctypes.c_int),
+        ("eul_coarse", _p), ("eul_fine", _p), ("trans_px", _p), ("trans_px_fine", _p),
+        ("trans_prior", _p), ("pdf_direction", _p), ("pdf_class", _p), ("mresol", _p),
+        ("sigma2_offset", ctypes.c_double), ("pixel_size", ctypes.c_double),
+        ("adaptive_fraction", ctypes.c_double), ("fine_capacity", ctypes.c_size_t),
+    ]
+
+
+class Batch(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("_pad", ctypes.c_int), ("fimg", _p), ("fimg_nomask", _p),
+                ("ctf", _p), ("minvsigma2", _p), ("scalars", _p)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [(name, _p) for name in (
+        "min_diff2", "sum_weight", "sig_weight", "coarse_sum_weight", "coarse_sig_weight",
+        "nr_sign", "n_coarse_sig", "pmax", "pose", "wsum_norm", "sumw", "wsum_sigma2_offset",
+        "wsum_sigma2", "wsum_pdf_class", "wsum_pdf_dir", "status")]
+
+
+def _setup_prototypes():
+    i, v, c = ctypes.c_int, ctypes.c_void_p, ctypes.c_char_p
+    lib.t2b_create.argtypes = [i, ctypes.POINTER(v)]
+    lib.t2b_destroy.argtypes = [v]
+    lib.t2b_destroy.restype = None
+    lib.t2b_last_error.restype = c
+    lib.t2b_version.restype = c
+    lib.t2b_projector_set.argtypes = [v, i, i, i, i, i, i, i, i, i, v]
+    lib.t2b_backprojector_init.argtypes = [v, i, i, i, i, i, i, i, i, i]
+    lib.t2b_backprojector_clear.argtypes = [v, i]
+    lib.t2b_backprojector_get.argtypes = [v, i, v, v, v]
+    lib.t2b_backprojector_device_ptrs.argtypes = [v, i, ctypes.POINTER(v), ctypes.POINTER(v)]
+    lib.t2b_configure.argtypes = [v, ctypes.POINTER(Config)]
+    lib.t2b_estep_batch_host.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(Result)]
+    lib.t2b_estep_batch_device.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(Result), v]
+    lib.t2b_reconstruct_divide.argtypes = [v, i, v]
+    lib.t2b_project.argtypes = [v, i, v, i, i, v]
+    lib.t2b_debug_coarse_diff2.argtypes = [v, i, v]
+    lib.t2b_debug_fine.argtypes = [v, i, v, v, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+    lib.t2b_last_stage_ms.argtypes = [v, v, i]
+    lib.t2b_sampling.argtypes = [i, i, ctypes.c_double, i, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double] + [ctypes.POINTER(i)] * 5 + [v] * 6
+
+
+_setup_prototypes()
+
+
+def _check(code):
+    if code != T2B_OK:
+        raise T2BError(code, lib.t2b_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def version():
+    return lib.t2b_version().decode()
+
+
+def sampling(ref_dim, healpix_order, psi_step, adaptive_oversampling, offset_range_px,
+             offset_step_px, pixel_size):
+    """HealpixSampling-equivalent orientation / translation lists (C1, no perturbation).
+
+    Returns a dict with eul_coarse (O x 9), eul_fine (O*R x 9), trans_px (T x 2),
+    trans_px_fine (T*V x 2), trans_prior (T x 2, Angstrom), angles (O x 3) and
+    the counts n_dir, n_psi, n_trans, nover_rot, nover_trans.
+    """
+    n = [ctypes.c_int() for _ in range(5)]
+    args = (ref_dim, healpix_order, psi_step, adaptive_oversampling, offset_range_px,
+            offset_step_px, pixel_size)
+    _check(lib.t2b_sampling(*args, *[ctypes.byref(x) for x in n], *([None] * 6)))
+    nd, npsi, nt, nr, nv = (x.value for x in n)
+    o = nd * npsi
+    out = dict(n_dir=nd, n_psi=npsi, n_trans=nt, nover_rot=nr, nover_trans=nv,
+               eul_coarse=np.zeros((o, 9)), eul_fine=np.zeros((o * nr, 9)),
+               trans_px=np.zeros((nt, 2)), trans_px_fine=np.zeros((nt * nv, 2)),
+               trans_prior=np.zeros((nt, 2)), angles=np.zeros((o, 3)))
+    _check(lib.t2b_sampling(*args, *[ctypes.byref(x) for x in n],
+                            _ptr(out["eul_coarse"]), _ptr(out["eul_fine"]), _ptr(out["trans_px"]),
+                            _ptr(out["trans_px_fine"]), _ptr(out["trans_prior"]), _ptr(out["angles"])))
+    return out
+
+
+def mresol_map(s):
+    """Mresol of the window (src/ml_optimiser.cpp:5628-5660): ring index or -1."""
+    xh = s // 2 + 1
+    i = np.arange(s)[:, None]
+    ip = np.where(i < xh, i, i - s)
+    jp = np.arange(xh)[None, :]
+    ires = np.rint(np.sqrt(ip * ip + jp * jp)).astype(np.int32)
+    m = np.where((ires < xh) & ~((jp == 0) & (ip < 0)), ires, -1)
+    return np.ascontiguousarray(m.reshape(-1), dtype=np.int32)
+
+
+class EStep:
+    """One E-step context on one GPU (MlDeviceBundle + MlOptimiserCuda)."""
+
+    def __init__(self, device=0):
+        self._h = ctypes.c_void_p()
+        _check(lib.t2b_create(device, ctypes.byref(self._h)))
+        self._keep = []
+        self.cfg = None
+
+    def close(self):
+        if self._h:
+            lib.t2b_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # AccProjector::setMdlDim + initMdl
+    def set_projector(self, iclass, model, ref_dim, r_max, padding_factor):
+        m = np.ascontiguousarray(model, dtype=np.complex64)
+        if ref_dim == 3:
+            zdim, ydim, xdim = m.shape
+        else:
+            ydim, xdim = m.shape
+            zdim = 1
+        _check(lib.t2b_projector_set(self._h, iclass, ref_dim, xdim, ydim, zdim, -(ydim // 2),
+                                     -(zdim // 2) if ref_dim == 3 else 0, r_max, padding_factor,
+                                     _ptr(m)))
+
+    # AccBackprojector::setMdlDim + initMdl
+    def init_backprojector(self, iclass, ref_dim, pad_size, r_max, padding_factor):
+        xdim, ydim = pad_size // 2 + 1, pad_size
+        zdim = pad_size if ref_dim == 3 else 1
+        self._grid_shape = (zdim, ydim, xdim) if ref_dim == 3 else (ydim, xdim)
+        _check(lib.t2b_backprojector_init(self._h, iclass, ref_dim, xdim, ydim, zdim, -(ydim // 2),
+                                          -(zdim // 2) if ref_dim == 3 else 0, r_max, padding_factor))
+
+    def clear_backprojector(self, iclass):
+        _check(lib.t2b_backprojector_clear(self._h, iclass))
+
+    # AccBackprojector::getMdlData
+    def get_backprojector(self, iclass):
+        shape = self._grid_shape
+        re = np.zeros(shape, np.float32)
+        im = np.zeros(shape, np.float32)
+        w = np.zeros(shape, np.float32)
+        _check(lib.t2b_backprojector_get(self._h, iclass, _ptr(re), _ptr(im), _ptr(w)))
+        return re + 1j * im.astype(np.complex64), w
+
+    def backprojector_device_ptrs(self, iclass):
+        d, w = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib.t2b_backprojector_device_ptrs(self._h, iclass, ctypes.byref(d), ctypes.byref(w)))
+        return d.value, w.value
+
+    def configure(self, *, ori_size, current_size, ref_dim, nr_classes, samp, pdf_direction,
+                  pdf_class, sigma2_offset, pixel_size, adaptive_fraction=0.999,
+                  adaptive_oversampling=0, diff2_mode=DIFF2_PLAIN_FP32, max_batch=64,
+                  fine_capacity=0, maximum_significants=-1):
+        arrays = dict(
+            eul_coarse=np.ascontiguousarray(samp["eul_coarse"], np.float64),
+            eul_fine=np.ascontiguousarray(samp["eul_fine"], np.float64),
+            trans_px=np.ascontiguousarray(samp["trans_px"], np.float64),
+            trans_px_fine=np.ascontiguousarray(samp["trans_px_fine"], np.float64),
+            trans_prior=np.ascontiguousarray(samp["trans_prior"], np.float64),
+            pdf_direction=np.ascontiguousarray(pdf_direction, np.float64),
+            pdf_class=np.ascontiguousarray(pdf_class, np.float64),
+            mresol=mresol_map(current_size))
+        c = Config()
+        c.ori_size, c.current_size, c.ref_dim = ori_size, current_size, ref_dim
+        c.nr_classes, c.n_dir, c.n_psi, c.n_trans = nr_classes, samp["n_dir"], samp["n_psi"], samp["n_trans"]
+        c.adaptive_oversampling = adaptive_oversampling
+        c.nover_rot = samp["nover_rot"] if adaptive_oversampling else 1
+        c.nover_trans = samp["nover_trans"] if adaptive_oversampling else 1
+        c.maximum_significants = maximum_significants
+        c.diff2_mode, c.max_batch = diff2_mode, max_batch
+        for k, a in arrays.items():
+            setattr(c, k, _ptr(a))
+        c.sigma2_offset, c.pixel_size, c.adaptive_fraction = sigma2_offset, pixel_size, adaptive_fraction
+        c.fine_capacity = fine_capacity
+        _check(lib.t2b_configure(self._h, ctypes.byref(c)))
+        self.cfg = dict(ori_size=ori_size, current_size=current_size, nr_classes=nr_classes,
+                        n_dir=samp["n_dir"], n_psi=samp["n_psi"], n_trans=samp["n_trans"],
+                        R=c.nover_rot, V=c.nover_trans, ovs=adaptive_oversampling,
+                        max_batch=max_batch)
+        return self.cfg
+
+    def _result_arrays(self, n):
+        cfg = self.cfg
+        half = cfg["ori_size"] // 2 + 1
+        K, nd = cfg["nr_classes"], cfg["n_dir"]
+        return dict(
+            min_diff2=np.zeros(n), sum_weight=np.zeros(n), sig_weight=np.zeros(n),
+            coarse_sum_weight=np.zeros(n), coarse_sig_weight=np.zeros(n),
+            nr_sign=np.zeros(n, np.int64), n_coarse_sig=np.zeros(n, np.int64), pmax=np.zeros(n),
+            pose=np.zeros((n, 5), np.int32), wsum_norm=np.zeros(n), sumw=np.zeros(n),
+            wsum_sigma2_offset=np.zeros(n), wsum_sigma2=np.zeros((n, half)),
+            wsum_pdf_class=np.zeros((n, K)), wsum_pdf_dir=np.zeros((n, K * nd)),
+            status=np.zeros(n, np.int32))
+
+    # MlOptimiserCuda::doThreadExpectationSomeParticles for one batch (host buffers)
+    def expectation(self, fimg, ctf, minvsigma2, scalars, fimg_nomask=None):
+        fimg = np.ascontiguousarray(fimg, np.complex64)
+        n = fimg.shape[0]
+        arrs = [fimg, np.ascontiguousarray(ctf, np.float32), np.ascontiguousarray(minvsigma2, np.float32),
+                np.ascontiguousarray(scalars, np.float64)]
+        fnm = None if fimg_nomask is None else np.ascontiguousarray(fimg_nomask, np.complex64)
+        b = Batch(n, 0, _ptr(arrs[0]), _ptr(fnm), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(arrs[3]))
+        res = self._result_arrays(n)
+        r = Result(*[_ptr(res[name]) for name, _ in Result._fields_])
+        _check(lib.t2b_estep_batch_host(self._h, ctypes.byref(b), ctypes.byref(r)))
+        return res
+
+    # device-resident variant: arguments are objects with .data_ptr() (e.g. torch tensors)
+    def expectation_device(self, n, fimg_ptr, ctf_ptr, minv_ptr, scal_ptr, result_ptrs, stream=0,
+                           fimg_nomask_ptr=None):
+        b = Batch(n, 0, fimg_ptr, fimg_nomask_ptr, ctf_ptr, minv_ptr, scal_ptr)
+        r = Result(*[result_ptrs[name] for name, _ in Result._fields_])
+        _check(lib.t2b_estep_batch_device(self._h, ctypes.byref(b), ctypes.byref(r),
+                                          ctypes.c_void_p(stream)))
+
+    def stage_ms(self):
+        ms = np.zeros(6, np.float32)
+        _check(lib.t2b_last_stage_ms(self._h, _ptr(ms), 6))
+        return ms
+
+    def coarse_diff2(self, b):
+        cfg = self.cfg
+        out = np.zeros(cfg["nr_classes"] * cfg["n_dir"] * cfg["n_psi"] * cfg["n_trans"], np.float32)
+        _check(lib.t2b_debug_coarse_diff2(self._h, b, _ptr(out)))
+        return out
+
+    def fine(self, b, cap=1 << 20):
+        cfg = self.cfg
+        cnt = ctypes.c_longlong()
+        _check(lib.t2b_debug_fine(self._h, b, None, None, 0, ctypes.byref(cnt)))
+        m = min(cnt.value, cap)
+        pairs = np.zeros(max(m, 1), np.int64)
+        d2 = np.zeros((max(m, 1), cfg["R"] * cfg["V"]), np.float32)
+        _check(lib.t2b_debug_fine(self._h, b, _ptr(pairs), _ptr(d2), m, ctypes.byref(cnt)))
+        return pairs[:m], d2[:m]
+
+    def reconstruct_divide(self, iclass):
+        zdim, ydim, xdim = self._grid_shape
+        ps = ydim
+        out = np.zeros((ps, ps, ps // 2 + 1), np.complex128)
+        _check(lib.t2b_reconstruct_divide(self._h, iclass, _ptr(out)))
+        return out
+
+    def project(self, iclass, eulers, current_size):
+        e = np.ascontiguousarray(eulers, np.float64).reshape(-1, 9)
+        P = current_size * (current_size // 2 + 1)
+        out = np.zeros((e.shape[0], P), np.complex64)
+        _check(lib.t2b_project(self._h, iclass, _ptr(e), e.shape[0], current_size, _ptr(out)))
+        return out
+
+
+# Reference-named wrappers (the names RELION's host code uses) ---------------
+class AccProjector:
+    """AccProjector (src/acc/acc_projector.h): setMdlDim + initMdl on a context."""
+
+    def __init__(self, estep, iclass=0):
+        self.estep, self.iclass = estep, iclass
+        self._dims = None
+
+    def setMdlDim(self, xdim, ydim, zdim, inity, initz, maxr, paddingFactor):
+        self._dims = (xdim, ydim, zdim, inity, initz, maxr, paddingFactor)
+        return True
+
+    def initMdl(self, data):
+        xdim, ydim, zdim, inity, initz, maxr, pad = self._dims
+        ref_dim = 3 if zdim > 1 else 2
+        shape = (zdim, ydim, xdim) if ref_dim == 3 else (ydim, xdim)
+        self.estep.set_projector(self.iclass, np.asarray(data).reshape(shape), ref_dim, maxr, pad)
+
+
+class AccBackprojector:
+    """AccBackprojector (src/acc/acc_backprojector.h): grid on the device."""
+
+    def __init__(self, estep, iclass=0):
+        self.estep, self.iclass = estep, iclass
+
+    def setMdlDim(self, xdim, ydim, zdim, inity, initz, max_r, paddingFactor):
+        self._dims = (xdim, ydim, zdim, max_r, paddingFactor)
+        return xdim * ydim * zdim * 12
+
+    def initMdl(self):
+        xdim, ydim, zdim, max_r, pad = self._dims
+        self.estep.init_backprojector(self.iclass, 3 if zdim > 1 else 2, ydim, max_r, pad)
+
+    def getMdlData(self):
+        data, w = self.estep.get_backprojector(self.iclass)
+        return data.real.astype(np.float32), data.imag.astype(np.float32), w

@@ -1,0 +1,628 @@
+// C ABI of libt2b: context, model / grid management, configuration, the
+// batched E-step and its host <-> device plumbing.
+//
+// Replaces the reference's per-particle task graph
+// (src/acc/cuda/cuda_ml_optimiser.cu:101-1130), its arena allocators
+// (custom_allocator.cuh) and the host packer (acc_boo.h) by one preallocated
+// workspace per context and a fixed sequence of batched kernels with no host
+// synchronisation between the coarse pass and the backprojection.
+#include "t2b_internal.cuh"
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+namespace t2b {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+
+template <typename F>
+static int guarded(F&& f)
+{
+    try {
+        f();
+        return T2B_OK;
+    } catch (const Error& e) {
+        set_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return T2B_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return T2B_ERR_ARG;
+    }
+}
+
+template <typename T>
+static T* dalloc(t2b_ctx* c, size_t n)
+{
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{T2B_ERR_NOMEM, "cudaMalloc of " + std::to_string(n * sizeof(T)) + " bytes failed"};
+    }
+    c->allocs.push_back(p);
+    return static_cast<T*>(p);
+}
+
+static void free_allocs(t2b_ctx* c)
+{
+    for (void* p : c->allocs) cudaFree(p);
+    c->allocs.clear();
+    c->configured = false;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        T2B_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+static void check_volume(int ref_dim, int xdim, int ydim, int zdim, int inity, int initz, int r_max, int pad)
+{
+    T2B_REQUIRE(ref_dim == 2 || ref_dim == 3, T2B_ERR_ARG, "ref_dim must be 2 or 3");
+    T2B_REQUIRE(xdim > 1 && ydim > 1 && zdim >= 1 && r_max > 0 && pad >= 1, T2B_ERR_ARG, "bad volume dimensions");
+    T2B_REQUIRE(xdim == ydim / 2 + 1, T2B_ERR_ARG, "xdim must be ydim/2+1 (half-complex)");
+    T2B_REQUIRE(ref_dim == 2 ? zdim == 1 : zdim == ydim, T2B_ERR_ARG, "zdim must equal ydim (3D) or 1 (2D)");
+    T2B_REQUIRE(inity == -(ydim / 2) && (ref_dim == 2 || initz == -(zdim / 2)), T2B_ERR_ARG,
+                "origin must be at the centre (inity = -ydim/2)");
+    T2B_REQUIRE(r_max * pad + 1 < xdim, T2B_ERR_ARG, "r_max*padding_factor must fit the grid");
+}
+
+}  // namespace t2b
+
+using namespace t2b;
+
+extern "C" {
+
+const char* t2b_last_error(void) { return g_err.c_str(); }
+const char* t2b_version(void) { return "t2b 0.1 sm_100a"; }
+
+int t2b_create(int device, t2b_ctx** out)
+{
+    return guarded([&] {
+        T2B_REQUIRE(out != nullptr, T2B_ERR_ARG, "null output pointer");
+        int n = 0;
+        T2B_CUDA(cudaGetDeviceCount(&n));
+        T2B_REQUIRE(device >= 0 && device < n, T2B_ERR_ARG, "no such CUDA device");
+        DeviceGuard g(device);
+        cudaDeviceProp prop;
+        T2B_CUDA(cudaGetDeviceProperties(&prop, device));
+        T2B_REQUIRE(prop.major >= 10, T2B_ERR_UNSUPPORTED, "libt2b is built for sm_100a (Blackwell)");
+        auto* c = new t2b_ctx();
+        c->device = device;
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete c; T2B_CUDA(e); }
+        for (auto& ev : c->ev) cudaEventCreate(&ev);
+        *out = c;
+    });
+}
+
+void t2b_destroy(t2b_ctx* c)
+{
+    if (!c) return;
+    {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+        free_allocs(c);
+        for (auto p : c->mdl) cudaFree(p);
+        for (auto p : c->gdata) cudaFree(p);
+        for (auto p : c->gweight) cudaFree(p);
+        for (auto& ev : c->ev) cudaEventDestroy(ev);
+        cudaStreamDestroy(c->stream);
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    delete c;
+}
+
+int t2b_projector_set(t2b_ctx* c, int iclass, int ref_dim, int xdim, int ydim, int zdim, int inity, int initz,
+                      int r_max, int pad, const float* mdl)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && mdl && iclass >= 0 && iclass < 4096, T2B_ERR_ARG, "bad projector arguments");
+        check_volume(ref_dim, xdim, ydim, zdim, inity, initz, r_max, pad);
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        if ((int)c->mvol.size() <= iclass) { c->mvol.resize(iclass + 1); c->mdl.resize(iclass + 1, nullptr); }
+        Volume v;
+        v.ref_dim = ref_dim; v.xdim = xdim; v.ydim = ydim; v.zdim = zdim;
+        v.inity = inity; v.initz = initz; v.r_max = r_max; v.pad = pad;
+        if (c->mdl[iclass] && c->mvol[iclass].nvox() != v.nvox()) { cudaFree(c->mdl[iclass]); c->mdl[iclass] = nullptr; }
+        if (!c->mdl[iclass]) {
+            void* p = nullptr;
+            if (cudaMalloc(&p, v.nvox() * sizeof(float2)) != cudaSuccess) {
+                cudaGetLastError();
+                throw Error{T2B_ERR_NOMEM, "model allocation failed"};
+            }
+            c->mdl[iclass] = (float2*)p;
+        }
+        c->mvol[iclass] = v;
+        T2B_CUDA(cudaMemcpyAsync(c->mdl[iclass], mdl, v.nvox() * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        c->configured = false;  // projection tables are stale
+    });
+}
+
+int t2b_backprojector_init(t2b_ctx* c, int iclass, int ref_dim, int xdim, int ydim, int zdim, int inity, int initz,
+                           int r_max, int pad)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && iclass >= 0 && iclass < 4096, T2B_ERR_ARG, "bad backprojector arguments");
+        check_volume(ref_dim, xdim, ydim, zdim, inity, initz, r_max, pad);
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        if ((int)c->gvol.size() <= iclass) {
+            c->gvol.resize(iclass + 1);
+            c->gdata.resize(iclass + 1, nullptr);
+            c->gweight.resize(iclass + 1, nullptr);
+        }
+        Volume v;
+        v.ref_dim = ref_dim; v.xdim = xdim; v.ydim = ydim; v.zdim = zdim;
+        v.inity = inity; v.initz = initz; v.r_max = r_max; v.pad = pad;
+        if (c->gdata[iclass] && c->gvol[iclass].nvox() != v.nvox()) {
+            cudaFree(c->gdata[iclass]); cudaFree(c->gweight[iclass]);
+            c->gdata[iclass] = nullptr; c->gweight[iclass] = nullptr;
+        }
+        if (!c->gdata[iclass]) {
+            void *p = nullptr, *q = nullptr;
+            if (cudaMalloc(&p, v.nvox() * sizeof(float2)) != cudaSuccess || cudaMalloc(&q, v.nvox() * sizeof(float)) != cudaSuccess) {
+                cudaGetLastError();
+                if (p) cudaFree(p);
+                throw Error{T2B_ERR_NOMEM, "grid allocation failed"};
+            }
+            c->gdata[iclass] = (float2*)p;
+            c->gweight[iclass] = (float*)q;
+        }
+        c->gvol[iclass] = v;
+        T2B_CUDA(cudaMemsetAsync(c->gdata[iclass], 0, v.nvox() * sizeof(float2), c->stream));
+        T2B_CUDA(cudaMemsetAsync(c->gweight[iclass], 0, v.nvox() * sizeof(float), c->stream));
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        c->configured = false;  // grid pointer table is stale
+    });
+}
+
+int t2b_backprojector_clear(t2b_ctx* c, int iclass)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && iclass >= 0 && iclass < (int)c->gvol.size() && c->gdata[iclass], T2B_ERR_ARG, "no such grid");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        const Volume& v = c->gvol[iclass];
+        T2B_CUDA(cudaMemsetAsync(c->gdata[iclass], 0, v.nvox() * sizeof(float2), c->stream));
+        T2B_CUDA(cudaMemsetAsync(c->gweight[iclass], 0, v.nvox() * sizeof(float), c->stream));
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int t2b_backprojector_get(t2b_ctx* c, int iclass, float* real, float* imag, float* weight)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && iclass >= 0 && iclass < (int)c->gvol.size() && c->gdata[iclass], T2B_ERR_ARG, "no such grid");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        const Volume& v = c->gvol[iclass];
+        std::vector<float2> tmp(v.nvox());
+        T2B_CUDA(cudaMemcpyAsync(tmp.data(), c->gdata[iclass], v.nvox() * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
+        if (weight)
+            T2B_CUDA(cudaMemcpyAsync(weight, c->gweight[iclass], v.nvox() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        for (size_t i = 0; i < v.nvox(); i++) {
+            if (real) real[i] = tmp[i].x;
+            if (imag) imag[i] = tmp[i].y;
+        }
+    });
+}
+
+int t2b_backprojector_device_ptrs(t2b_ctx* c, int iclass, float** data, float** weight)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && iclass >= 0 && iclass < (int)c->gvol.size() && c->gdata[iclass], T2B_ERR_ARG, "no such grid");
+        if (data) *data = reinterpret_cast<float*>(c->gdata[iclass]);
+        if (weight) *weight = c->gweight[iclass];
+    });
+}
+
+int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && cfg, T2B_ERR_ARG, "null argument");
+        const t2b_config& f = *cfg;
+        T2B_REQUIRE(f.ori_size > 0 && f.current_size > 0 && f.current_size % 2 == 0 && f.current_size <= f.ori_size,
+                    T2B_ERR_ARG, "current_size must be even and <= ori_size");
+        T2B_REQUIRE(f.ref_dim == 2 || f.ref_dim == 3, T2B_ERR_ARG, "ref_dim must be 2 or 3");
+        T2B_REQUIRE(f.nr_classes >= 1 && f.n_dir >= 1 && f.n_psi >= 1 && f.n_trans >= 1, T2B_ERR_ARG, "empty sampling");
+        T2B_REQUIRE(f.adaptive_oversampling == 0 || f.adaptive_oversampling == 1, T2B_ERR_ARG,
+                    "adaptive_oversampling must be 0 or 1");
+        const int R = f.adaptive_oversampling ? f.nover_rot : 1, V = f.adaptive_oversampling ? f.nover_trans : 1;
+        T2B_REQUIRE(R >= 1 && R <= 8 && V >= 1 && V <= 4, T2B_ERR_ARG, "oversampling factors must be <= 8 (rot), <= 4 (trans)");
+        T2B_REQUIRE(f.maximum_significants <= 0, T2B_ERR_UNSUPPORTED, "maximum_significants > 0 is not supported");
+        T2B_REQUIRE(f.diff2_mode == T2B_DIFF2_PLAIN_FP32 || f.diff2_mode == T2B_DIFF2_SPLIT_BF16, T2B_ERR_ARG, "bad diff2_mode");
+        T2B_REQUIRE(f.diff2_mode != T2B_DIFF2_SPLIT_BF16 || tc_supported(), T2B_ERR_UNSUPPORTED,
+                    "split-BF16 tcgen05 contraction unavailable in this build");
+        T2B_REQUIRE(f.max_batch >= 1 && f.max_batch <= 4096, T2B_ERR_ARG, "max_batch must be in [1, 4096]");
+        T2B_REQUIRE(f.eul_coarse && f.trans_px && f.trans_prior && f.pdf_direction && f.pdf_class && f.mresol,
+                    T2B_ERR_ARG, "missing sampling arrays");
+        T2B_REQUIRE(!f.adaptive_oversampling || (f.eul_fine && f.trans_px_fine), T2B_ERR_ARG, "missing fine sampling arrays");
+        T2B_REQUIRE(f.adaptive_fraction > 0. && f.adaptive_fraction <= 1., T2B_ERR_ARG, "adaptive_fraction must be in (0,1]");
+        T2B_REQUIRE(f.pixel_size > 0., T2B_ERR_ARG, "pixel_size must be positive");
+        T2B_REQUIRE((int)c->mvol.size() >= f.nr_classes && (int)c->gvol.size() >= f.nr_classes, T2B_ERR_STATE,
+                    "set projectors and backprojectors of every class before t2b_configure");
+        for (int k = 0; k < f.nr_classes; k++) {
+            T2B_REQUIRE(c->mdl[k] && c->gdata[k], T2B_ERR_STATE, "projector/backprojector of a class is missing");
+            T2B_REQUIRE(c->mvol[k].ref_dim == f.ref_dim && c->gvol[k].ref_dim == f.ref_dim, T2B_ERR_ARG, "ref_dim mismatch");
+            T2B_REQUIRE(c->gvol[k].nvox() == c->gvol[0].nvox() && c->gvol[k].r_max == c->gvol[0].r_max, T2B_ERR_ARG,
+                        "all backprojection grids must share one geometry");
+        }
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        free_allocs(c);
+        c->cfg = f;
+        const int s = f.current_size, xh = s / 2 + 1, P = s * xh;
+        const int K = f.nr_classes, O = f.n_dir * f.n_psi, T = f.n_trans, B = f.max_batch;
+        const long long KO = (long long)K * O;
+        Tables& tb = c->tb;
+        tb = Tables{};
+        tb.s = s; tb.xh = xh; tb.P = P; tb.ori_size = f.ori_size;
+        tb.K = K; tb.n_dir = f.n_dir; tb.n_psi = f.n_psi; tb.O = O; tb.T = T;
+        tb.R = R; tb.V = V; tb.ovs = f.adaptive_oversampling; tb.ref_dim = f.ref_dim;
+        tb.sigma2_offset = f.sigma2_offset; tb.pixel_size = f.pixel_size; tb.adaptive_fraction = f.adaptive_fraction;
+        cudaStream_t st = c->stream;
+        // host-side tables: normalised pdf_orientation and the skip mask
+        std::vector<double> pdf_o((size_t)K * f.n_dir);
+        double om = 0.;
+        for (int k = 0; k < K; k++)
+            for (int d = 0; d < f.n_dir; d++) om += f.pdf_direction[k * f.n_dir + d] * f.n_psi;
+        om /= (double)(K * f.n_dir * f.n_psi);
+        std::vector<unsigned char> skip(KO);
+        for (int k = 0; k < K; k++)
+            for (int d = 0; d < f.n_dir; d++) {
+                double v = f.pdf_direction[k * f.n_dir + d];
+                const bool sk = !(f.pdf_class[k] > 0.) || !(v > 0.);
+                if (om != 0.) v /= om;
+                pdf_o[(size_t)k * f.n_dir + d] = v;
+                for (int p = 0; p < f.n_psi; p++) skip[(size_t)k * O + d * f.n_psi + p] = sk;
+            }
+        auto up = [&](const void* h, size_t bytes) {
+            void* d = dalloc<unsigned char>(c, bytes);
+            T2B_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+            return d;
+        };
+        tb.pdf_o = (const double*)up(pdf_o.data(), pdf_o.size() * sizeof(double));
+        tb.skip = (const unsigned char*)up(skip.data(), skip.size());
+        tb.mresol = (const int*)up(f.mresol, (size_t)P * sizeof(int));
+        tb.eul_c = (const double*)up(f.eul_coarse, (size_t)O * 9 * sizeof(double));
+        tb.trans_c = (const double*)up(f.trans_px, (size_t)T * 2 * sizeof(double));
+        tb.trans_prior = (const double*)up(f.trans_prior, (size_t)T * 2 * sizeof(double));
+        if (tb.ovs) {
+            tb.eul_f = (const double*)up(f.eul_fine, (size_t)O * R * 9 * sizeof(double));
+            tb.trans_f = (const double*)up(f.trans_px_fine, (size_t)T * V * 2 * sizeof(double));
+        } else {
+            tb.eul_f = tb.eul_c;
+            tb.trans_f = tb.trans_c;
+        }
+        // projection tables (per class, resident)
+        float2* pc = dalloc<float2>(c, (size_t)KO * P);
+        for (int k = 0; k < K; k++) {
+            const Volume& v = c->mvol[k];
+            T2B_REQUIRE(v.r_max * v.pad + 1 < v.xdim, T2B_ERR_ARG, "projector too small");
+            launch_project_table(v, c->mdl[k], tb.eul_c, O, s, pc + (size_t)k * O * P, st);
+        }
+        tb.proj_c = pc;
+        if (tb.ovs) {
+            float2* pf = dalloc<float2>(c, (size_t)KO * R * P);
+            for (int k = 0; k < K; k++)
+                launch_project_table(c->mvol[k], c->mdl[k], tb.eul_f, O * R, s, pf + (size_t)k * O * R * P, st);
+            tb.proj_f = pf;
+        } else {
+            tb.proj_f = pc;
+        }
+        float2* abc = dalloc<float2>(c, (size_t)T * P);
+        launch_phase_table(tb.trans_c, T, s, f.ori_size, abc, st);
+        tb.ab_c = abc;
+        if (tb.ovs) {
+            float2* abf = dalloc<float2>(c, (size_t)T * V * P);
+            launch_phase_table(tb.trans_f, T * V, s, f.ori_size, abf, st);
+            tb.ab_f = abf;
+        } else {
+            tb.ab_f = abc;
+        }
+        // workspace
+        Work& w = c->wk;
+        w = Work{};
+        const long long KOT = KO * T;
+        w.cvec = dalloc<float2>(c, (size_t)B * P);
+        w.w2 = dalloc<float>(c, (size_t)B * P);
+        w.c0 = dalloc<float>(c, B);
+        w.norms = dalloc<float>(c, (size_t)B * KO);
+        w.d2c = dalloc<float>(c, (size_t)B * KOT);
+        w.wc = dalloc<double>(c, (size_t)B * KOT);
+        w.minkey_c = dalloc<unsigned>(c, B);
+        w.minkey_f = dalloc<unsigned>(c, B);
+        w.pdf_t = dalloc<double>(c, (size_t)B * T);
+        w.sum_c = dalloc<double>(c, B);
+        w.sum_f = dalloc<double>(c, B);
+        w.sel_c = dalloc<SelState>(c, B);
+        w.sel_f = dalloc<SelState>(c, B);
+        w.hist_cnt = dalloc<unsigned>(c, (size_t)B * HIST_BINS);
+        w.hist_sum = dalloc<double>(c, (size_t)B * HIST_BINS);
+        w.cand = dalloc<double>(c, (size_t)B * CAND_CAP);
+        const size_t fine_cap = f.fine_capacity ? f.fine_capacity : (size_t)32 << 20;
+        w.pair_cap = std::max<long long>((long long)(fine_cap / (size_t)(R * V)), (long long)B * 64);
+        w.pairs = dalloc<long long>(c, w.pair_cap);
+        w.pair_b = dalloc<int>(c, w.pair_cap);
+        w.pair_off = dalloc<long long>(c, B + 1);
+        w.max_chunks = (int)((KOT + 4095) / 4096);
+        w.chunk_cnt = dalloc<int>(c, (size_t)B * w.max_chunks);
+        w.d2f = dalloc<float>(c, (size_t)w.pair_cap * R * V);
+        w.wf = dalloc<double>(c, (size_t)w.pair_cap * R * V);
+        w.groups = dalloc<long long>(c, w.pair_cap);
+        w.group_b = dalloc<int>(c, w.pair_cap);
+        w.group_off = dalloc<long long>(c, B + 1);
+        w.counters = dalloc<unsigned long long>(c, 16);
+        w.status = dalloc<int>(c, B);
+        // staging of host inputs and internal results
+        w.fimg = dalloc<float2>(c, (size_t)B * P);
+        w.fimg_nm = dalloc<float2>(c, (size_t)B * P);
+        w.ctf = dalloc<float>(c, (size_t)B * P);
+        w.minv = dalloc<float>(c, (size_t)B * P);
+        w.scal = dalloc<double>(c, (size_t)B * 8);
+        w.r_min = dalloc<double>(c, B); w.r_sum = dalloc<double>(c, B); w.r_sig = dalloc<double>(c, B);
+        w.r_csum = dalloc<double>(c, B); w.r_csig = dalloc<double>(c, B); w.r_pmax = dalloc<double>(c, B);
+        w.r_nsign = dalloc<long long>(c, B); w.r_ncsig = dalloc<long long>(c, B);
+        w.r_pose = dalloc<int>(c, (size_t)B * 5);
+        w.r_norm = dalloc<double>(c, B); w.r_sumw = dalloc<double>(c, B); w.r_sig_off = dalloc<double>(c, B);
+        w.r_sigma2 = dalloc<double>(c, (size_t)B * (f.ori_size / 2 + 1));
+        w.r_pdf_class = dalloc<double>(c, (size_t)B * K);
+        w.r_pdf_dir = dalloc<double>(c, (size_t)B * K * f.n_dir);
+        // grid pointer tables
+        float2** gd = dalloc<float2*>(c, K);
+        float** gw = dalloc<float*>(c, K);
+        T2B_CUDA(cudaMemcpyAsync(gd, c->gdata.data(), K * sizeof(float2*), cudaMemcpyHostToDevice, st));
+        T2B_CUDA(cudaMemcpyAsync(gw, c->gweight.data(), K * sizeof(float*), cudaMemcpyHostToDevice, st));
+        c->gd_table = gd;
+        c->gw_table = gw;
+        c->tc = TcOperands{};
+        if (f.diff2_mode == T2B_DIFF2_SPLIT_BF16) tc_prepare_projections(tb, c->tc, st);
+        T2B_CUDA(cudaStreamSynchronize(st));
+        c->configured = true;
+    });
+}
+
+}  // extern "C"
+
+namespace t2b {
+
+// Enqueue the whole E-step of the batch in `w` on `st`.
+static void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st)
+{
+    const Tables& tb = c->tb;
+    T2B_CUDA(cudaMemsetAsync(w.counters, 0, 16 * sizeof(unsigned long long), st));
+    cudaEventRecord(c->ev[0], st);
+    launch_prep(tb, w, st);
+    launch_norms(tb, w, st);
+    cudaEventRecord(c->ev[1], st);
+    if (c->cfg.diff2_mode == T2B_DIFF2_SPLIT_BF16) tc_launch_diff2(tb, w, c->tc, st);
+    else launch_diff2_simt(tb, w, st);
+    cudaEventRecord(c->ev[2], st);
+    launch_weights_coarse(tb, w, c->cfg.maximum_significants, st);
+    cudaEventRecord(c->ev[3], st);
+    if (tb.ovs) launch_fine(tb, w, st);
+    cudaEventRecord(c->ev[4], st);
+    if (tb.ovs) launch_weights_fine(tb, w, st);
+    cudaEventRecord(c->ev[5], st);
+    launch_wsum_bp(tb, w, c->gvol[0], c->gd_table, c->gw_table, st);
+    cudaEventRecord(c->ev[6], st);
+}
+
+static void check_batch(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
+{
+    T2B_REQUIRE(c && b && r, T2B_ERR_ARG, "null argument");
+    T2B_REQUIRE(c->configured, T2B_ERR_STATE, "t2b_configure must be called before the E-step");
+    T2B_REQUIRE(b->n >= 1 && b->n <= c->cfg.max_batch, T2B_ERR_ARG, "batch size out of range");
+    T2B_REQUIRE(b->fimg && b->ctf && b->minvsigma2 && b->scalars, T2B_ERR_ARG, "missing batch inputs");
+}
+
+static void collect_stage_ms(t2b_ctx* c)
+{
+    for (int i = 0; i < 6; i++) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+}
+
+}  // namespace t2b
+
+extern "C" {
+
+int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
+{
+    return guarded([&] {
+        check_batch(c, b, r);
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        cudaStream_t st = c->stream;
+        Work w = c->wk;
+        const int n = b->n, P = c->tb.P;
+        w.n = n;
+        T2B_CUDA(cudaMemcpyAsync((void*)w.fimg, b->fimg, (size_t)n * P * sizeof(float2), cudaMemcpyHostToDevice, st));
+        T2B_CUDA(cudaMemcpyAsync((void*)w.fimg_nm, b->fimg_nomask ? b->fimg_nomask : b->fimg, (size_t)n * P * sizeof(float2),
+                                 cudaMemcpyHostToDevice, st));
+        T2B_CUDA(cudaMemcpyAsync((void*)w.ctf, b->ctf, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
+        T2B_CUDA(cudaMemcpyAsync((void*)w.minv, b->minvsigma2, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
+        T2B_CUDA(cudaMemcpyAsync((void*)w.scal, b->scalars, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, st));
+        enqueue_estep(c, w, st);
+        const int K = c->tb.K, half = c->cfg.ori_size / 2 + 1;
+        auto d2h = [&](void* dst, const void* src, size_t bytes) {
+            if (dst) T2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        };
+        d2h(r->min_diff2, w.r_min, n * sizeof(double));
+        d2h(r->sum_weight, w.r_sum, n * sizeof(double));
+        d2h(r->sig_weight, w.r_sig, n * sizeof(double));
+        d2h(r->coarse_sum_weight, w.r_csum, n * sizeof(double));
+        d2h(r->coarse_sig_weight, w.r_csig, n * sizeof(double));
+        d2h(r->nr_sign, w.r_nsign, n * sizeof(long long));
+        d2h(r->n_coarse_sig, w.r_ncsig, n * sizeof(long long));
+        d2h(r->pmax, w.r_pmax, n * sizeof(double));
+        d2h(r->pose, w.r_pose, n * 5 * sizeof(int));
+        d2h(r->wsum_norm, w.r_norm, n * sizeof(double));
+        d2h(r->sumw, w.r_sumw, n * sizeof(double));
+        d2h(r->wsum_sigma2_offset, w.r_sig_off, n * sizeof(double));
+        d2h(r->wsum_sigma2, w.r_sigma2, (size_t)n * half * sizeof(double));
+        d2h(r->wsum_pdf_class, w.r_pdf_class, (size_t)n * K * sizeof(double));
+        d2h(r->wsum_pdf_dir, w.r_pdf_dir, (size_t)n * K * c->tb.n_dir * sizeof(double));
+        d2h(r->status, w.status, n * sizeof(int));
+        T2B_CUDA(cudaStreamSynchronize(st));
+        collect_stage_ms(c);
+        c->last_n = n;
+    });
+}
+
+int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, void* stream)
+{
+    return guarded([&] {
+        check_batch(c, b, r);
+        T2B_REQUIRE(r->min_diff2 && r->sum_weight && r->sig_weight && r->coarse_sum_weight && r->coarse_sig_weight &&
+                        r->nr_sign && r->n_coarse_sig && r->pmax && r->pose && r->wsum_norm && r->sumw &&
+                        r->wsum_sigma2_offset && r->wsum_sigma2 && r->wsum_pdf_class && r->wsum_pdf_dir && r->status,
+                    T2B_ERR_ARG, "the device variant needs every result array");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+        Work w = c->wk;
+        w.n = b->n;
+        w.fimg = (const float2*)b->fimg;
+        w.fimg_nm = (const float2*)(b->fimg_nomask ? b->fimg_nomask : b->fimg);
+        w.ctf = b->ctf;
+        w.minv = b->minvsigma2;
+        w.scal = b->scalars;
+        w.r_min = r->min_diff2; w.r_sum = r->sum_weight; w.r_sig = r->sig_weight;
+        w.r_csum = r->coarse_sum_weight; w.r_csig = r->coarse_sig_weight; w.r_pmax = r->pmax;
+        w.r_nsign = r->nr_sign; w.r_ncsig = r->n_coarse_sig; w.r_pose = r->pose;
+        w.r_norm = r->wsum_norm; w.r_sumw = r->sumw; w.r_sig_off = r->wsum_sigma2_offset;
+        w.r_sigma2 = r->wsum_sigma2; w.r_pdf_class = r->wsum_pdf_class; w.r_pdf_dir = r->wsum_pdf_dir;
+        w.status = r->status;
+        enqueue_estep(c, w, st);
+        c->last_n = b->n;
+    });
+}
+
+int t2b_last_stage_ms(t2b_ctx* c, float* ms, int n)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && ms && n >= 0 && n <= 6, T2B_ERR_ARG, "bad arguments");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        collect_stage_ms(c);
+        for (int i = 0; i < n; i++) ms[i] = c->stage_ms[i];
+    });
+}
+
+int t2b_debug_coarse_diff2(t2b_ctx* c, int b, float* out)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && out && c->configured && b >= 0 && b < c->last_n, T2B_ERR_ARG, "bad particle index");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        const size_t n = (size_t)c->tb.K * c->tb.O * c->tb.T;
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        T2B_CUDA(cudaMemcpy(out, c->wk.d2c + (size_t)b * n, n * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+int t2b_debug_fine(t2b_ctx* c, int b, long long* pairs, float* diff2, long long cap, long long* count)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && count && c->configured && b >= 0 && b < c->last_n, T2B_ERR_ARG, "bad particle index");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        long long off[2];
+        T2B_CUDA(cudaMemcpy(off, c->wk.pair_off + b, 2 * sizeof(long long), cudaMemcpyDeviceToHost));
+        const long long np = off[1] - off[0];
+        *count = np;
+        const long long m = std::min(np, cap);
+        const int rv = c->tb.ovs ? c->tb.R * c->tb.V : 1;
+        if (pairs && m > 0)
+            T2B_CUDA(cudaMemcpy(pairs, c->wk.pairs + off[0], m * sizeof(long long), cudaMemcpyDeviceToHost));
+        if (diff2 && m > 0 && c->tb.ovs)
+            T2B_CUDA(cudaMemcpy(diff2, c->wk.d2f + off[0] * rv, (size_t)m * rv * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+int t2b_reconstruct_divide(t2b_ctx* c, int iclass, double* fconv)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && fconv && iclass >= 0 && iclass < (int)c->gvol.size() && c->gdata[iclass], T2B_ERR_ARG,
+                    "no such grid");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        const Volume& v = c->gvol[iclass];
+        T2B_REQUIRE(v.ref_dim == 3, T2B_ERR_UNSUPPORTED, "reconstruction division is implemented for 3D grids");
+        const int ps = v.ydim, fx = ps / 2 + 1;
+        const size_t total = (size_t)ps * ps * fx;
+        double2* fc = nullptr;
+        double *fw = nullptr, *rad = nullptr;
+        cudaStream_t st = c->stream;
+        auto cleanup = [&] { cudaFree(fc); cudaFree(fw); cudaFree(rad); };
+        if (cudaMalloc(&fc, total * sizeof(double2)) != cudaSuccess || cudaMalloc(&fw, total * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&rad, 2 * (size_t)v.r_max * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            cleanup();
+            throw Error{T2B_ERR_NOMEM, "reconstruction buffers"};
+        }
+        try {
+            launch_reconstruct(v, c->gdata[iclass], c->gweight[iclass], fc, fw, rad, rad + v.r_max, st);
+            T2B_CUDA(cudaMemcpyAsync(fconv, fc, total * sizeof(double2), cudaMemcpyDeviceToHost, st));
+            T2B_CUDA(cudaStreamSynchronize(st));
+        } catch (...) {
+            cleanup();
+            throw;
+        }
+        cleanup();
+    });
+}
+
+int t2b_project(t2b_ctx* c, int iclass, const double* eulers, int n, int current_size, float* out)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && eulers && out && n > 0 && current_size > 0 && current_size % 2 == 0, T2B_ERR_ARG, "bad arguments");
+        T2B_REQUIRE(iclass >= 0 && iclass < (int)c->mvol.size() && c->mdl[iclass], T2B_ERR_ARG, "no such projector");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        const int P = current_size * (current_size / 2 + 1);
+        double* de = nullptr;
+        float2* dout = nullptr;
+        cudaStream_t st = c->stream;
+        if (cudaMalloc(&de, (size_t)n * 9 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&dout, (size_t)n * P * sizeof(float2)) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(de);
+            throw Error{T2B_ERR_NOMEM, "projection buffers"};
+        }
+        try {
+            T2B_CUDA(cudaMemcpyAsync(de, eulers, (size_t)n * 9 * sizeof(double), cudaMemcpyHostToDevice, st));
+            launch_project_table(c->mvol[iclass], c->mdl[iclass], de, n, current_size, dout, st);
+            T2B_CUDA(cudaMemcpyAsync(out, dout, (size_t)n * P * sizeof(float2), cudaMemcpyDeviceToHost, st));
+            T2B_CUDA(cudaStreamSynchronize(st));
+        } catch (...) {
+            cudaFree(de);
+            cudaFree(dout);
+            throw;
+        }
+        cudaFree(de);
+        cudaFree(dout);
+    });
+}
+
+}  // extern "C"

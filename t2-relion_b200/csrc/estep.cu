@@ -1,0 +1,1191 @@
+// E-step stages of libt2b for sm_100a.
+//
+// Data flow of one batch of particles (all on the device, no host sync):
+//   prep      cvec = Minvsigma2 * scale * CTF * X, w2 = 0.5 * Minvsigma2 * (scale CTF)^2,
+//             c0 = highres_Xi2/2 + sum 0.5 Minvsigma2 |X|^2
+//   norms     N[b][oc] = sum_p w2[b][p] |P_oc[p]|^2
+//   diff2     D[b][oc*T+t] = c0[b] + N[b][oc] - 2 sum_p Re(P_oc[p] conj(cvec_b[p] ab_t[p]))
+//             which equals highres_Xi2/2 + sum_p 0.5 M |scale CTF P - shift_t X|^2
+//             (src/ml_optimiser.cpp:7251-7272; the reference GPU kernel splits the
+//             same three terms, coarse_splitImg_BCF_PMO.cuh:139-693)
+//   weights   w = pdf_o pdf_t exp(-(D - min)) in FP64, sum, significance threshold by
+//             an exact MSB-first radix search on the FP64 bit patterns
+//             (src/ml_optimiser.cpp:7770-7990, sort + cumulative sum)
+//   compact   ordered list of significant coarse pairs per particle
+//   fine      32 fine hypotheses per significant pair (8 rotations x 4 shifts)
+//   weights   same on the fine set
+//   wsum+BP   per (particle, significant orientation): weighted sums, sigma2 rings,
+//             prior sums, then trilinear backprojection with float2 atomics
+//             (src/ml_optimiser.cpp:8153-8700, src/backprojector.cpp:55-230)
+#include "t2b_internal.cuh"
+#include <algorithm>
+#include <cfloat>
+
+namespace t2b {
+namespace {
+
+__device__ __forceinline__ unsigned f2key(float f)
+{
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key2f(unsigned k)
+{
+    const unsigned u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+template <typename T>
+__device__ T block_sum(T v, T* sh /* >= 32 */)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? sh[threadIdx.x] : T(0);
+    if (wid == 0)
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (threadIdx.x == 0) sh[0] = v;
+    __syncthreads();
+    const T r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// ------------------------------------------------------------------ prep
+__global__ void k_prep(Tables tb, Work w)
+{
+    __shared__ double sh[32];
+    const int b = blockIdx.x, P = tb.P;
+    const double* sc = w.scal + 8 * (size_t)b;
+    const float scale = (float)sc[6];
+    double acc = 0.;
+    for (int n = threadIdx.x; n < P; n += blockDim.x) {
+        const float2 X = w.fimg[(size_t)b * P + n];
+        const float M = w.minv[(size_t)b * P + n];
+        const float c = w.ctf[(size_t)b * P + n] * scale;
+        const float mc = M * c;
+        w.cvec[(size_t)b * P + n] = make_float2(mc * X.x, mc * X.y);
+        w.w2[(size_t)b * P + n] = 0.5f * M * c * c;
+        acc += 0.5 * (double)M * ((double)X.x * X.x + (double)X.y * X.y);
+    }
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) {
+        w.c0[b] = (float)(sc[1] / 2. + acc);
+        w.minkey_c[b] = 0xffffffffu;
+        w.minkey_f[b] = 0xffffffffu;
+        w.sum_c[b] = 0.;
+        w.sum_f[b] = 0.;
+        w.status[b] = T2B_OK;
+        SelState z{};
+        z.argmax = 0x7fffffffffffffffLL;
+        w.sel_c[b] = z;
+        w.sel_f[b] = z;
+        w.r_norm[b] = 0.; w.r_sumw[b] = 0.; w.r_sig_off[b] = 0.;
+    }
+    const int half = tb.ori_size / 2 + 1;
+    for (int i = threadIdx.x; i < half; i += blockDim.x) w.r_sigma2[(size_t)b * half + i] = 0.;
+    for (int i = threadIdx.x; i < tb.K; i += blockDim.x) w.r_pdf_class[(size_t)b * tb.K + i] = 0.;
+    for (int i = threadIdx.x; i < tb.K * tb.n_dir; i += blockDim.x) w.r_pdf_dir[(size_t)b * tb.K * tb.n_dir + i] = 0.;
+    for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) {
+        w.hist_cnt[(size_t)b * HIST_BINS + i] = 0;
+        w.hist_sum[(size_t)b * HIST_BINS + i] = 0.;
+    }
+}
+
+// ----------------------------------------------------------------- norms
+// N[b][oc] = sum_p w2[b][p] |P_oc[p]|^2 ; tile 64 orientations x 16 particles.
+__global__ void __launch_bounds__(256) k_norms(Tables tb, Work w, const float2* __restrict__ proj, int nrows,
+                                               float* __restrict__ out)
+{
+    __shared__ float Ps[32][65];
+    __shared__ float Ws[32][17];
+    const int o0 = blockIdx.x * 64, b0 = blockIdx.y * 16, P = tb.P;
+    const int to = threadIdx.x & 63, tbq = threadIdx.x >> 6;  // 4 particles per thread
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int p0 = 0; p0 < P; p0 += 32) {
+        for (int idx = threadIdx.x; idx < 64 * 32; idx += 256) {
+            const int oo = idx >> 5, pp = idx & 31;
+            float v = 0.f;
+            if (o0 + oo < nrows && p0 + pp < P) {
+                const float2 z = proj[(size_t)(o0 + oo) * P + p0 + pp];
+                v = z.x * z.x + z.y * z.y;
+            }
+            Ps[pp][oo] = v;
+        }
+        for (int idx = threadIdx.x; idx < 16 * 32; idx += 256) {
+            const int bb = idx >> 5, pp = idx & 31;
+            Ws[pp][bb] = (b0 + bb < w.n && p0 + pp < P) ? w.w2[(size_t)(b0 + bb) * P + p0 + pp] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int pp = 0; pp < 32; pp++) {
+            const float pv = Ps[pp][to];
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[j] += pv * Ws[pp][tbq * 4 + j];
+        }
+        __syncthreads();
+    }
+    for (int j = 0; j < 4; j++) {
+        const int b = b0 + tbq * 4 + j, o = o0 + to;
+        if (b < w.n && o < nrows) out[(size_t)b * nrows + o] = acc[j];
+    }
+}
+
+// --------------------------------------------------- plain FP32 diff2 GEMM
+// C[oc][col] = sum_k Bm[oc][k] A[col][k], k over interleaved (re, im) of the P
+// pixels, col = b*T + t.  A is built on the fly from cvec and the phase table.
+// 128 x 128 tile, 256 threads, 8x8 register micro-tile, double-buffered smem.
+constexpr int SB_M = 128, SB_N = 128, SB_KP = 8, SB_K = 16, SB_LD = 132;
+
+__global__ void __launch_bounds__(256, 2) k_diff2_simt(Tables tb, Work w)
+{
+    __shared__ __align__(16) float Bs[2][SB_K][SB_LD];
+    __shared__ __align__(16) float As[2][SB_K][SB_LD];
+    __shared__ unsigned smin[SB_N + 2];
+    const int P = tb.P, T = tb.T, KO = tb.K * tb.O;
+    const int m0 = blockIdx.x * SB_M, n0 = blockIdx.y * SB_N;
+    const int ncols = w.n * T;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int bfirst = n0 / T;
+
+    // loader coordinates: thread loads rows/cols (tid>>3) + 32*j, pixel (tid & 7)
+    const int lrow = tid >> 3, lp = tid & 7;
+    int la_b[4], la_t[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int col = n0 + lrow + 32 * j;
+        la_b[j] = col < ncols ? col / T : -1;
+        la_t[j] = col < ncols ? col - (col / T) * T : 0;
+    }
+    float2 rb[4], ra[4];
+    auto gload = [&](int p0) {
+        const int p = p0 + lp;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int row = m0 + lrow + 32 * j;
+            rb[j] = (row < KO && p < P) ? tb.proj_c[(size_t)row * P + p] : make_float2(0.f, 0.f);
+            if (la_b[j] >= 0 && p < P) {
+                const float2 c = w.cvec[(size_t)la_b[j] * P + p];
+                const float2 ab = tb.ab_c[(size_t)la_t[j] * P + p];
+                ra[j] = make_float2(c.x * ab.x - c.y * ab.y, c.x * ab.y + c.y * ab.x);
+            } else {
+                ra[j] = make_float2(0.f, 0.f);
+            }
+        }
+    };
+    auto sstore = [&](int buf) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            Bs[buf][2 * lp][lrow + 32 * j] = rb[j].x;
+            Bs[buf][2 * lp + 1][lrow + 32 * j] = rb[j].y;
+            As[buf][2 * lp][lrow + 32 * j] = ra[j].x;
+            As[buf][2 * lp + 1][lrow + 32 * j] = ra[j].y;
+        }
+    };
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+    for (int i = tid; i < SB_N + 2; i += 256) smin[i] = 0xffffffffu;
+
+    gload(0);
+    sstore(0);
+    __syncthreads();
+    int buf = 0;
+    for (int p0 = 0; p0 < P; p0 += SB_KP) {
+        const bool more = p0 + SB_KP < P;
+        if (more) gload(p0 + SB_KP);
+#pragma unroll
+        for (int k = 0; k < SB_K; k++) {
+            const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][k][ty * 4]);
+            const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][k][64 + ty * 4]);
+            const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][k][tx * 4]);
+            const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][k][64 + tx * 4]);
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fmaf(bv[i], av[j], acc[i][j]);
+        }
+        if (more) {
+            sstore(buf ^ 1);
+            __syncthreads();
+            buf ^= 1;
+        }
+    }
+    // epilogue
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int oc = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+        if (oc >= KO) continue;
+        const bool skip = tb.skip[oc] != 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int col = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+            if (col >= ncols) continue;
+            const int b = col / T, t = col - b * T;
+            float d;
+            if (skip) {
+                d = -999.f;
+            } else {
+                d = w.c0[b] + w.norms[(size_t)b * KO + oc] - 2.f * acc[i][j];
+                atomicMin(&smin[b - bfirst], f2key(d));
+            }
+            w.d2c[((size_t)b * KO + oc) * T + t] = d;
+        }
+    }
+    __syncthreads();
+    const int nb = min(SB_N / T + 2, SB_N + 2);
+    for (int i = tid; i < nb; i += 256) {
+        const int b = bfirst + i;
+        if (b < w.n && smin[i] != 0xffffffffu) atomicMin(&w.minkey_c[b], smin[i]);
+    }
+}
+
+// ---------------------------------------------------------------- priors
+// pdf_offset of every coarse translation, normalised by its mean
+// (src/ml_optimiser.cpp:7629-7716).  One CTA per particle.
+__global__ void k_pdf_t(Tables tb, Work w)
+{
+    __shared__ double sh[32];
+    const int b = blockIdx.x, T = tb.T;
+    const double* sc = w.scal + 8 * (size_t)b;
+    double local = 0.;
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+        const double ox = sc[2] + tb.trans_prior[2 * t], oy = sc[3] + tb.trans_prior[2 * t + 1];
+        double td = (ox - sc[4]) * (ox - sc[4]) + (oy - sc[5]) * (oy - sc[5]);
+        td *= tb.pixel_size * tb.pixel_size;
+        double v;
+        if (tb.sigma2_offset < 0.0001) v = td > 0. ? 0. : 1.;
+        else v = exp(td / (-2. * tb.sigma2_offset)) / (2. * 3.14159265358979323846 * tb.sigma2_offset);
+        w.pdf_t[(size_t)b * T + t] = v;
+        local += v;
+    }
+    const double mean = block_sum(local, sh) / T;
+    for (int t = threadIdx.x; t < T; t += blockDim.x)
+        if (mean > 0.) w.pdf_t[(size_t)b * T + t] /= mean;
+}
+
+// ------------------------------------------------------- weights (FP64)
+// Segment of particle b: coarse = [0, K*O*T) of d2c/wc; fine = the pair range
+// of b times R*V in d2f/wf.  Element -> (oc, t) for the priors.
+struct Seg {
+    const float* d;
+    double* wout;
+    long long beg, end;   // element range (global index into d / wout)
+};
+
+__device__ __forceinline__ Seg seg_of(const Tables& tb, const Work& w, bool fine, int b)
+{
+    Seg s;
+    if (!fine) {
+        const long long n = (long long)tb.K * tb.O * tb.T;
+        s.d = w.d2c; s.wout = w.wc; s.beg = (long long)b * n; s.end = s.beg + n;
+    } else {
+        const long long rv = (long long)tb.R * tb.V;
+        s.d = w.d2f; s.wout = w.wf; s.beg = w.pair_off[b] * rv; s.end = w.pair_off[b + 1] * rv;
+    }
+    return s;
+}
+
+__device__ __forceinline__ void elem_oct(const Tables& tb, const Work& w, bool fine, int b, long long i,
+                                         int& oc, int& t)
+{
+    long long ih;
+    if (!fine) ih = i - (long long)b * tb.K * tb.O * tb.T;
+    else ih = w.pairs[i / ((long long)tb.R * tb.V)];
+    oc = (int)(ih / tb.T);
+    t = (int)(ih - (long long)oc * tb.T);
+}
+
+// digit layout of the radix search over the 64-bit pattern of positive doubles
+__device__ __forceinline__ int digit_width(int shift) { return shift == 0 ? 4 : 12; }
+
+// pass 1: weights, sum, max, level-0 histogram (top 12 bits)
+__global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned* hc = reinterpret_cast<unsigned*>(smem_raw);
+    double* hs = reinterpret_cast<double*>(smem_raw + HIST_BINS * sizeof(unsigned));
+    __shared__ double sh[32];
+    const int b = blockIdx.y;
+    if (fine && w.status[b] != T2B_OK) return;
+    for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
+    __syncthreads();
+    const Seg sg = seg_of(tb, w, fine, b);
+    const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
+    double lsum = 0.;
+    unsigned long long lmax = 0;
+    for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float d = sg.d[i];
+        double wt = 0.;
+        if (d >= 0.f) {
+            int oc, t;
+            elem_oct(tb, w, fine, b, i, oc, t);
+            const int k = oc / tb.O, o = oc - k * tb.O, idir = o / tb.n_psi;
+            const double dd = (double)d - mn;
+            if (dd <= 700.) wt = tb.pdf_o[k * tb.n_dir + idir] * w.pdf_t[(size_t)b * tb.T + t] * exp(-dd);
+        }
+        sg.wout[i] = wt;
+        if (wt > 0.) {
+            const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
+            const int dg = (int)(bits >> 52);
+            atomicAdd(&hc[dg], 1u);
+            atomicAdd(&hs[dg], wt);
+            lsum += wt;
+            lmax = max(lmax, bits);
+        }
+    }
+    lsum = block_sum(lsum, sh);
+    for (int o = 16; o > 0; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    if ((threadIdx.x & 31) == 0 && lmax) atomicMax(&sel->maxbits, lmax);
+    if (threadIdx.x == 0) atomicAdd(fine ? &w.sum_f[b] : &w.sum_c[b], lsum);
+    __syncthreads();
+    for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x)
+        if (hc[i]) {
+            atomicAdd(&w.hist_cnt[(size_t)b * HIST_BINS + i], hc[i]);
+            atomicAdd(&w.hist_sum[(size_t)b * HIST_BINS + i], hs[i]);
+        }
+}
+
+__global__ void k_sel_init(Work w, int fine, double frac)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= w.n) return;
+    SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    const double S = fine ? w.sum_f[b] : w.sum_c[b];
+    if (w.status[b] != T2B_OK) { sel->phase = 3; return; }
+    if (!(S > 0.) || S != S) {
+        sel->phase = 3;
+        w.status[b] = T2B_ERR_NOSIGNIF;
+        return;
+    }
+    sel->target = frac * S;
+    sel->cum_above = 0.;
+    sel->count_above = 0;
+    sel->prefix = 0;
+    sel->shift = 52;
+    sel->phase = 0;
+    sel->ncand = 0;
+}
+
+// Choose the digit bin that contains the crossing of the descending
+// cumulative sum; narrow the prefix or move on to the gather.  One CTA per
+// particle; bins are visited from the largest digit down.
+__global__ void __launch_bounds__(1024) k_select(Work w, int fine)
+{
+    __shared__ double ssum[1024];
+    __shared__ unsigned long long scnt[1024];
+    __shared__ int chosen, lastne;
+    const int b = blockIdx.x;
+    SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    if (sel->phase != 0) return;
+    const int width = digit_width(sel->shift);
+    const int nb = 1 << width;
+    unsigned* hc = w.hist_cnt + (size_t)b * HIST_BINS;
+    double* hs = w.hist_sum + (size_t)b * HIST_BINS;
+    // thread i owns descending positions [i*per, (i+1)*per); position p is digit nb-1-p
+    const int per = (nb + 1023) / 1024;
+    double ls = 0.;
+    unsigned long long lc = 0;
+    for (int j = 0; j < per; j++) {
+        const int pos = threadIdx.x * per + j;
+        if (pos < nb) { ls += hs[nb - 1 - pos]; lc += hc[nb - 1 - pos]; }
+    }
+    ssum[threadIdx.x] = ls;
+    scnt[threadIdx.x] = lc;
+    if (threadIdx.x == 0) { chosen = 0x7fffffff; lastne = -1; }
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {  // inclusive scan
+        double vs = 0.;
+        unsigned long long vc = 0;
+        if (threadIdx.x >= off) { vs = ssum[threadIdx.x - off]; vc = scnt[threadIdx.x - off]; }
+        __syncthreads();
+        ssum[threadIdx.x] += vs;
+        scnt[threadIdx.x] += vc;
+        __syncthreads();
+    }
+    const double base = sel->cum_above, target = sel->target;
+    double before = threadIdx.x ? ssum[threadIdx.x - 1] : 0.;
+    for (int j = 0; j < per; j++) {
+        const int pos = threadIdx.x * per + j;
+        if (pos >= nb) break;
+        const double s = hs[nb - 1 - pos];
+        if (hc[nb - 1 - pos] > 0) {
+            atomicMax(&lastne, pos);
+            if (base + before + s > target) { atomicMin(&chosen, pos); break; }
+        }
+        before += s;
+    }
+    __syncthreads();
+    // no crossing (adaptive_fraction ~ 1 under rounding): the lowest non-empty bin
+    const int pos = chosen != 0x7fffffff ? chosen : lastne;
+    if (pos >= 0 && pos >= threadIdx.x * per && pos < (threadIdx.x + 1) * per) {
+        double bsum = threadIdx.x ? ssum[threadIdx.x - 1] : 0.;
+        unsigned long long bc = threadIdx.x ? scnt[threadIdx.x - 1] : 0;
+        for (int p = threadIdx.x * per; p < pos; p++) { bsum += hs[nb - 1 - p]; bc += hc[nb - 1 - p]; }
+        const int digit = nb - 1 - pos;
+        const unsigned long long cnt = hc[digit];
+        sel->cum_above += bsum;
+        sel->count_above += bc;
+        sel->prefix = (sel->prefix << width) | (unsigned long long)digit;
+        if (cnt <= (unsigned long long)CAND_CAP || sel->shift == 0) {
+            sel->phase = 1;
+            sel->ncand = 0;
+        } else {
+            sel->shift = sel->shift == 4 ? 0 : sel->shift - 12;
+        }
+    }
+    if (pos < 0 && threadIdx.x == 0) { sel->phase = 3; w.status[b] = T2B_ERR_NOSIGNIF; }
+    __syncthreads();
+    for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
+}
+
+// level >= 1 histogram of the next digit among the elements under the prefix
+__global__ void __launch_bounds__(256) k_hist_level(Tables tb, Work w, int fine)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned* hc = reinterpret_cast<unsigned*>(smem_raw);
+    double* hs = reinterpret_cast<double*>(smem_raw + HIST_BINS * sizeof(unsigned));
+    const int b = blockIdx.y;
+    const SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    if (sel->phase != 0) return;
+    const int shift = sel->shift, width = digit_width(shift);
+    const unsigned long long prefix = sel->prefix;
+    const int nb = 1 << width;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
+    __syncthreads();
+    const Seg sg = seg_of(tb, w, fine, b);
+    for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double wt = sg.wout[i];
+        if (!(wt > 0.)) continue;
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
+        if ((bits >> (shift + width)) != prefix) continue;
+        const int dg = (int)((bits >> shift) & (unsigned long long)(nb - 1));
+        atomicAdd(&hc[dg], 1u);
+        atomicAdd(&hs[dg], wt);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        if (hc[i]) {
+            atomicAdd(&w.hist_cnt[(size_t)b * HIST_BINS + i], hc[i]);
+            atomicAdd(&w.hist_sum[(size_t)b * HIST_BINS + i], hs[i]);
+        }
+}
+
+__global__ void __launch_bounds__(256) k_gather(Tables tb, Work w, int fine)
+{
+    const int b = blockIdx.y;
+    SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    if (sel->phase != 1) return;
+    const int shift = sel->shift;
+    const unsigned long long prefix = sel->prefix;
+    const Seg sg = seg_of(tb, w, fine, b);
+    for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double wt = sg.wout[i];
+        if (!(wt > 0.)) continue;
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
+        if ((bits >> shift) != prefix) continue;
+        const long long pos = atomicAdd((unsigned long long*)&sel->ncand, 1ull);
+        if (pos < CAND_CAP) w.cand[(size_t)b * CAND_CAP + pos] = wt;
+    }
+}
+
+// Sort the candidates (descending) and walk the cumulative sum
+// (src/ml_optimiser.cpp:7905-7935).
+__global__ void __launch_bounds__(1024) k_final(Work w, int fine, int ipass)
+{
+    __shared__ double c[CAND_CAP];
+    const int b = blockIdx.x;
+    SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    if (sel->phase != 1) return;
+    const long long nc = sel->ncand;
+    if (nc <= 0) {  // nothing under the chosen prefix: inconsistent histogram
+        if (threadIdx.x == 0) { sel->phase = 3; w.status[b] = T2B_ERR_NOSIGNIF; }
+        return;
+    }
+    if (nc > CAND_CAP) {
+        // only reachable with every remaining bit fixed: all candidates are equal
+        if (threadIdx.x == 0) {
+            const double v = w.cand[(size_t)b * CAND_CAP];
+            long long need = (long long)floor((sel->target - sel->cum_above) / v) + 1;
+            need = max(1LL, min(need, nc));
+            sel->thr = v;
+            sel->nr_sign = (long long)sel->count_above + need;
+            sel->phase = 2;
+        }
+        return;
+    }
+    int m = 1;
+    while (m < nc) m <<= 1;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) c[i] = i < nc ? w.cand[(size_t)b * CAND_CAP + i] : -1.;
+    __syncthreads();
+    // bitonic sort, descending
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool desc = (i & k) == 0;
+                    const double a = c[i], bb = c[l];
+                    if (desc ? (a < bb) : (a > bb)) { c[i] = bb; c[l] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    if (threadIdx.x == 0) {
+        double cum = sel->cum_above;
+        long long k = -1;
+        for (long long i = 0; i < nc; i++) {
+            cum += c[i];
+            if (cum > sel->target) { k = i; break; }
+        }
+        if (k < 0) k = nc - 1;
+        sel->thr = c[k];
+        sel->nr_sign = ipass == 0 ? (long long)sel->count_above + k + 1 : 0;
+        sel->phase = 2;
+    }
+}
+
+// ------------------------------------------------- ordered compaction
+constexpr int CHUNK = 4096;
+
+__global__ void __launch_bounds__(256) k_count_sig(Tables tb, Work w)
+{
+    const int b = blockIdx.y;
+    const SelState* sel = &w.sel_c[b];
+    const long long n = (long long)tb.K * tb.O * tb.T;
+    const int nch = (int)((n + CHUNK - 1) / CHUNK);
+    __shared__ int cnt;
+    for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+        if (threadIdx.x == 0) cnt = 0;
+        __syncthreads();
+        int local = 0;
+        if (sel->phase == 2) {
+            const double thr = sel->thr;
+            const unsigned long long maxbits = sel->maxbits;
+            for (long long i = (long long)c * CHUNK + threadIdx.x; i < min(n, (long long)(c + 1) * CHUNK); i += blockDim.x) {
+                const double wt = w.wc[(size_t)b * n + i];
+                if (wt >= thr) local++;
+                if ((unsigned long long)__double_as_longlong(wt) == maxbits)
+                    atomicMin((long long*)&w.sel_c[b].argmax, i);
+            }
+        }
+        local = __reduce_add_sync(0xffffffffu, local);
+        if ((threadIdx.x & 31) == 0 && local) atomicAdd(&cnt, local);
+        __syncthreads();
+        if (threadIdx.x == 0) w.chunk_cnt[(size_t)b * w.max_chunks + c] = cnt;
+        __syncthreads();
+    }
+}
+
+// exclusive scan of the chunk counts and of the per-particle totals (1 CTA)
+__global__ void __launch_bounds__(1024) k_scan_pairs(Tables tb, Work w)
+{
+    __shared__ long long sh[1024];
+    __shared__ long long base;
+    const long long n = (long long)tb.K * tb.O * tb.T;
+    const int nch = (int)((n + CHUNK - 1) / CHUNK);
+    if (threadIdx.x == 0) { base = 0; w.pair_off[0] = 0; }
+    __syncthreads();
+    for (int b = 0; b < w.n; b++) {
+        long long run = 0;
+        for (int c0 = 0; c0 < nch; c0 += 1024) {
+            const int c = c0 + threadIdx.x;
+            const long long v = c < nch ? w.chunk_cnt[(size_t)b * w.max_chunks + c] : 0;
+            sh[threadIdx.x] = v;
+            __syncthreads();
+            for (int off = 1; off < 1024; off <<= 1) {
+                const long long u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+                __syncthreads();
+                sh[threadIdx.x] += u;
+                __syncthreads();
+            }
+            if (c < nch) w.chunk_cnt[(size_t)b * w.max_chunks + c] = (int)(run + sh[threadIdx.x] - v);
+            const long long tot = sh[1023];
+            __syncthreads();
+            run += tot;
+        }
+        if (threadIdx.x == 0) {
+            long long cnt = run;
+            if (base + cnt > w.pair_cap) {  // capacity exceeded: drop the particle
+                cnt = 0;
+                w.status[b] = T2B_ERR_NOMEM;
+            }
+            w.r_ncsig[b] = cnt;
+            base += cnt;
+            w.pair_off[b + 1] = base;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_compact(Tables tb, Work w, int gather_final)
+{
+    __shared__ int sh[256];
+    const int b = blockIdx.y;
+    const SelState* sel = &w.sel_c[b];
+    if (sel->phase != 2 || w.status[b] != T2B_OK) return;
+    const long long n = (long long)tb.K * tb.O * tb.T;
+    const int nch = (int)((n + CHUNK - 1) / CHUNK);
+    const double thr = sel->thr;
+    const long long pbase = w.pair_off[b];
+    for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+        const long long beg = (long long)c * CHUNK + threadIdx.x * (CHUNK / 256);
+        int local = 0;
+        for (int j = 0; j < CHUNK / 256; j++) {
+            const long long i = beg + j;
+            if (i < n && w.wc[(size_t)b * n + i] >= thr) local++;
+        }
+        sh[threadIdx.x] = local;
+        __syncthreads();
+        for (int off = 1; off < 256; off <<= 1) {
+            const int u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += u;
+            __syncthreads();
+        }
+        long long pos = pbase + w.chunk_cnt[(size_t)b * w.max_chunks + c] + sh[threadIdx.x] - local;
+        for (int j = 0; j < CHUNK / 256; j++) {
+            const long long i = beg + j;
+            if (i < n) {
+                const double wt = w.wc[(size_t)b * n + i];
+                if (wt >= thr) {
+                    w.pairs[pos] = i;
+                    w.pair_b[pos] = b;
+                    if (gather_final) w.wf[pos] = wt;
+                    pos++;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------- fine pass
+// One work item per significant coarse pair, pulled from a device queue by a
+// persistent grid: R fine orientations x V fine shifts against the pair
+// (src/ml_optimiser.cpp:7090-7272 with exp_ipass == 1).
+constexpr int MAXR = 8, MAXV = 4;
+
+__global__ void __launch_bounds__(256) k_fine(Tables tb, Work w)
+{
+    __shared__ long long item;
+    __shared__ float red[8][MAXR * MAXV + MAXR];
+    const int P = tb.P, R = tb.R, V = tb.V, T = tb.T;
+    const long long total = w.pair_off[w.n];
+    for (;;) {
+        if (threadIdx.x == 0) item = (long long)atomicAdd(&w.counters[0], 1ull);
+        __syncthreads();
+        const long long q = item;
+        __syncthreads();
+        if (q >= total) break;
+        const int b = w.pair_b[q];
+        const long long ih = w.pairs[q];
+        const int oc = (int)(ih / T), t = (int)(ih - (long long)oc * T);
+        float cr[MAXR][MAXV], nr[MAXR];
+#pragma unroll
+        for (int r = 0; r < MAXR; r++) {
+            nr[r] = 0.f;
+#pragma unroll
+            for (int v = 0; v < MAXV; v++) cr[r][v] = 0.f;
+        }
+        for (int p = threadIdx.x; p < P; p += blockDim.x) {
+            const float2 c = w.cvec[(size_t)b * P + p];
+            const float wv = w.w2[(size_t)b * P + p];
+            float2 a[MAXV];
+#pragma unroll
+            for (int v = 0; v < MAXV; v++) {
+                if (v < V) {
+                    const float2 ab = tb.ab_f[(size_t)(t * V + v) * P + p];
+                    a[v] = make_float2(c.x * ab.x - c.y * ab.y, c.x * ab.y + c.y * ab.x);
+                } else {
+                    a[v] = make_float2(0.f, 0.f);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < MAXR; r++) {
+                if (r < R) {
+                    const float2 pv = tb.proj_f[((size_t)oc * R + r) * P + p];
+                    nr[r] += wv * (pv.x * pv.x + pv.y * pv.y);
+#pragma unroll
+                    for (int v = 0; v < MAXV; v++) cr[r][v] += pv.x * a[v].x + pv.y * a[v].y;
+                }
+            }
+        }
+        // block reduction of the R*V cross terms and R norms
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+        for (int r = 0; r < MAXR; r++) {
+#pragma unroll
+            for (int v = 0; v < MAXV; v++) {
+                float x = cr[r][v];
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                if (lane == 0) red[wid][r * MAXV + v] = x;
+            }
+            float x = nr[r];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) red[wid][MAXR * MAXV + r] = x;
+        }
+        __syncthreads();
+        if (threadIdx.x < R * V) {
+            const int r = threadIdx.x / V, v = threadIdx.x - r * V;
+            float cs = 0.f, ns = 0.f;
+            for (int j = 0; j < 8; j++) { cs += red[j][r * MAXV + v]; ns += red[j][MAXR * MAXV + r]; }
+            const float d = w.c0[b] + ns - 2.f * cs;
+            w.d2f[q * R * V + r * V + v] = d;
+            atomicMin(&w.minkey_f[b], f2key(d));
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_argmax_fine(Tables tb, Work w)
+{
+    const int b = blockIdx.y;
+    const SelState* sel = &w.sel_f[b];
+    if (sel->phase != 2) return;
+    const long long rv = (long long)tb.R * tb.V;
+    const long long beg = w.pair_off[b] * rv, end = w.pair_off[b + 1] * rv;
+    for (long long i = beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
+         i += (long long)gridDim.x * blockDim.x)
+        if ((unsigned long long)__double_as_longlong(w.wf[i]) == sel->maxbits)
+            atomicMin((long long*)&w.sel_f[b].argmax, i);
+}
+
+// --------------------------------------------------- orientation groups
+// Consecutive pairs of a particle with the same orientation form one group;
+// a work item of the weighted sums is (group, fine rotation).  1 CTA.
+__global__ void __launch_bounds__(1024) k_groups(Tables tb, Work w, int R)
+{
+    __shared__ long long sh[1024];
+    __shared__ long long base;
+    if (threadIdx.x == 0) { base = 0; w.group_off[0] = 0; }
+    __syncthreads();
+    const int T = tb.T;
+    for (int b = 0; b < w.n; b++) {
+        const long long beg = w.pair_off[b], end = w.pair_off[b + 1];
+        for (long long q0 = beg; q0 < end; q0 += 1024) {
+            const long long q = q0 + threadIdx.x;
+            const int f = (q < end && (q == beg || w.pairs[q] / T != w.pairs[q - 1] / T)) ? 1 : 0;
+            sh[threadIdx.x] = f;
+            __syncthreads();
+            for (int off = 1; off < 1024; off <<= 1) {
+                const long long u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+                __syncthreads();
+                sh[threadIdx.x] += u;
+                __syncthreads();
+            }
+            if (f) {
+                const long long g = base + sh[threadIdx.x] - 1;
+                w.groups[g] = q;
+                w.group_b[g] = b;
+            }
+            const long long tot = sh[1023];
+            __syncthreads();
+            if (threadIdx.x == 0) base += tot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) w.group_off[b + 1] = base;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) w.counters[3] = (unsigned long long)base * R;  // wsum work items
+}
+
+// ---------------------------------------------- weighted sums + backprojection
+constexpr int ENT_CAP = 512;
+
+struct GridPtrs {
+    float2* const* data;
+    float* const* weight;
+};
+
+__global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, GridPtrs gp)
+{
+    __shared__ long long item;
+    __shared__ int nent;
+    __shared__ float ent_w[ENT_CAP];
+    __shared__ int ent_tv[ENT_CAP];
+    __shared__ double ssig[1024];
+    __shared__ double shr[32];
+    const int P = tb.P, T = tb.T, xh = tb.xh, s = tb.s;
+    const int R = tb.ovs ? tb.R : 1, V = tb.ovs ? tb.V : 1;
+    const long long G = w.group_off[w.n];
+    const unsigned long long nitems = (unsigned long long)G * R;
+    const float2* proj = tb.ovs ? tb.proj_f : tb.proj_c;
+    const float2* abt = tb.ovs ? tb.ab_f : tb.ab_c;
+    const int nring = s / 2 + 1;
+    for (;;) {
+        if (threadIdx.x == 0) item = (long long)atomicAdd(&w.counters[2], 1ull);
+        __syncthreads();
+        const long long it = item;
+        if ((unsigned long long)it >= nitems) break;
+        const long long gi = it / R;
+        const int r = (int)(it - gi * R);
+        const int b = w.group_b[gi];
+        const long long qa = w.groups[gi];
+        const long long qb = (gi + 1 < G && w.group_b[gi + 1] == b) ? w.groups[gi + 1] : w.pair_off[b + 1];
+        const int oc = (int)(w.pairs[qa] / T);
+        const int k = oc / tb.O, o = oc - k * tb.O, idir = o / tb.n_psi;
+        const long long tab = tb.ovs ? (long long)oc * R + r : oc;
+        const double* A = tb.ovs ? tb.eul_f + 9 * ((size_t)o * R + r) : tb.eul_c + 9 * (size_t)o;
+        const SelState* sel = tb.ovs ? &w.sel_f[b] : &w.sel_c[b];
+        const double thr = sel->thr;
+        const double S = tb.ovs ? w.sum_f[b] : w.sum_c[b];
+        const double* sc = w.scal + 8 * (size_t)b;
+        if (threadIdx.x == 0) nent = 0;
+        for (int i = threadIdx.x; i < nring; i += blockDim.x) ssig[i] = 0.;
+        __syncthreads();
+        if (w.status[b] == T2B_OK) {
+            const long long nh = (qb - qa) * V;
+            for (long long e0 = 0; e0 < nh; e0 += ENT_CAP) {
+                // collect the significant hypotheses of this orientation
+                for (long long e = e0 + threadIdx.x; e < min(nh, e0 + ENT_CAP); e += blockDim.x) {
+                    const long long q = qa + e / V;
+                    const int v = (int)(e % V);
+                    const double wt = tb.ovs ? w.wf[q * R * V + r * V + v] : w.wf[q];
+                    if (wt >= thr) {
+                        const int t = (int)(w.pairs[q] - (long long)oc * T);
+                        const double wn = wt / S;
+                        const int pos = atomicAdd(&nent, 1);
+                        ent_w[pos] = (float)wn;
+                        ent_tv[pos] = t * V + v;
+                        // scalar sums of src/ml_optimiser.cpp:8480-8540
+                        atomicAdd(&w.r_sumw[b], wn);
+                        atomicAdd(&w.r_pdf_class[(size_t)b * tb.K + k], wn);
+                        atomicAdd(&w.r_pdf_dir[(size_t)b * tb.K * tb.n_dir + k * tb.n_dir + idir], wn);
+                        const double* sh = tb.ovs ? tb.trans_f + 2 * (t * V + v) : tb.trans_c + 2 * t;
+                        const double dx = sc[4] - sc[2] - sh[0], dy = sc[5] - sc[3] - sh[1];
+                        atomicAdd(&w.r_sig_off[b], wn * tb.pixel_size * tb.pixel_size * (dx * dx + dy * dy));
+                    }
+                }
+                __syncthreads();
+                const int ne = nent;
+                if (ne > 0) {
+                    double nacc = 0.;
+                    const float scale = (float)sc[6];
+                    for (int n = threadIdx.x; n < P; n += blockDim.x) {
+                        const float2 pv = proj[(size_t)tab * P + n];
+                        const float c = w.ctf[(size_t)b * P + n] * scale;
+                        const float frr = pv.x * c, fri = pv.y * c;
+                        const float2 X = w.fimg[(size_t)b * P + n];
+                        const float2 Xn = w.fimg_nm[(size_t)b * P + n];
+                        const float minv = n == 0 ? (float)sc[0] : w.minv[(size_t)b * P + n];
+                        const int ires = tb.mresol[n];
+                        float fir = 0.f, fii = 0.f, fw = 0.f, wd = 0.f;
+                        for (int e = 0; e < ne; e++) {
+                            const float wn = ent_w[e];
+                            const float2 ab = abt[(size_t)ent_tv[e] * P + n];
+                            const float sr = ab.x * X.x - ab.y * X.y, si = ab.x * X.y + ab.y * X.x;
+                            const float dr = frr - sr, di = fri - si;
+                            wd += wn * (dr * dr + di * di);
+                            const float wx = wn * c * minv;
+                            const float nr_ = ab.x * Xn.x - ab.y * Xn.y, ni = ab.x * Xn.y + ab.y * Xn.x;
+                            fir += nr_ * wx;
+                            fii += ni * wx;
+                            fw += wx * c;
+                        }
+                        if (ires > -1) {
+                            atomicAdd(&ssig[ires], (double)wd);
+                            nacc += wd;
+                        }
+                        // backprojection of this pixel (src/backprojector.cpp:140-228)
+                        if (fw > 0.f) {
+                            const int i = n / xh, x = n - i * xh;
+                            const int y = (i < xh) ? i : i - s;
+                            if (i >= xh && x == 0) continue;
+                            if (x * x + y * y > g.r_max * g.r_max) continue;
+                            double xp = (A[0] * x + A[3] * y) * g.pad;
+                            double yp = (A[1] * x + A[4] * y) * g.pad;
+                            double zp = (A[2] * x + A[5] * y) * g.pad;
+                            float vr = fir, vi = fii;
+                            if (xp < 0) { xp = -xp; yp = -yp; zp = -zp; vi = -vi; }
+                            const int x0 = (int)floor(xp);
+                            const float fx = (float)(xp - x0);
+                            int y0 = (int)floor(yp);
+                            const float fy = (float)(yp - y0);
+                            y0 -= g.inity;
+                            float2* gd = gp.data[k];
+                            float* gw = gp.weight[k];
+                            if (g.ref_dim == 3) {
+                                int z0 = (int)floor(zp);
+                                const float fz = (float)(zp - z0);
+                                z0 -= g.initz;
+                                if (x0 < 0 || x0 + 1 >= g.xdim || y0 < 0 || y0 + 1 >= g.ydim || z0 < 0 || z0 + 1 >= g.zdim) continue;
+                                const float mfx = 1.f - fx, mfy = 1.f - fy, mfz = 1.f - fz;
+                                const float dd[8] = {mfz * mfy * mfx, mfz * mfy * fx, mfz * fy * mfx, mfz * fy * fx,
+                                                     fz * mfy * mfx,  fz * mfy * fx,  fz * fy * mfx,  fz * fy * fx};
+#pragma unroll
+                                for (int cc = 0; cc < 8; cc++) {
+                                    const size_t idx = ((size_t)(z0 + (cc >> 2)) * g.ydim + y0 + ((cc >> 1) & 1)) * g.xdim + x0 + (cc & 1);
+                                    atomicAdd(&gd[idx], make_float2(dd[cc] * vr, dd[cc] * vi));
+                                    atomicAdd(&gw[idx], dd[cc] * fw);
+                                }
+                            } else {
+                                if (x0 < 0 || x0 + 1 >= g.xdim || y0 < 0 || y0 + 1 >= g.ydim) continue;
+                                const float mfx = 1.f - fx, mfy = 1.f - fy;
+                                const float dd[4] = {mfy * mfx, mfy * fx, fy * mfx, fy * fx};
+#pragma unroll
+                                for (int cc = 0; cc < 4; cc++) {
+                                    const size_t idx = (size_t)(y0 + (cc >> 1)) * g.xdim + x0 + (cc & 1);
+                                    atomicAdd(&gd[idx], make_float2(dd[cc] * vr, dd[cc] * vi));
+                                    atomicAdd(&gw[idx], dd[cc] * fw);
+                                }
+                            }
+                        }
+                    }
+                    nacc = block_sum(nacc, shr);
+                    if (threadIdx.x == 0) atomicAdd(&w.r_norm[b], nacc);
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) nent = 0;
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+        const int half = tb.ori_size / 2 + 1;
+        for (int i = threadIdx.x; i < nring && i < half; i += blockDim.x)
+            if (ssig[i] != 0.) atomicAdd(&w.r_sigma2[(size_t)b * half + i], ssig[i]);
+        __syncthreads();
+    }
+}
+
+// ----------------------------------------------------------- results
+__global__ void k_results(Tables tb, Work w)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= w.n) return;
+    const SelState& sc = w.sel_c[b];
+    const SelState& sf = tb.ovs ? w.sel_f[b] : w.sel_c[b];
+    w.r_csum[b] = w.sum_c[b];
+    w.r_csig[b] = sc.thr;
+    w.r_nsign[b] = sc.nr_sign;
+    const double S = tb.ovs ? w.sum_f[b] : w.sum_c[b];
+    w.r_sum[b] = S;
+    w.r_sig[b] = sf.thr;
+    w.r_min[b] = (double)key2f(tb.ovs ? w.minkey_f[b] : w.minkey_c[b]);
+    int* pose = w.r_pose + 5 * (size_t)b;
+    if (w.status[b] != T2B_OK || sf.phase != 2) {
+        if (w.status[b] == T2B_OK) w.status[b] = T2B_ERR_NOSIGNIF;
+        w.r_pmax[b] = -1.;
+        for (int j = 0; j < 5; j++) pose[j] = -1;
+        return;
+    }
+    const long long am = sf.argmax;
+    const long long nfinal = tb.ovs ? (w.pair_off[w.n] * tb.R * tb.V) : (long long)tb.K * tb.O * tb.T;
+    if (am < 0 || am >= nfinal) {  // the maximum was not located: report, do not index
+        w.status[b] = T2B_ERR_NOSIGNIF;
+        w.r_pmax[b] = -1.;
+        for (int j = 0; j < 5; j++) pose[j] = -1;
+        return;
+    }
+    w.r_pmax[b] = __longlong_as_double((long long)sf.maxbits) / S;
+    long long ih;
+    int r = 0, v = 0;
+    if (tb.ovs) {
+        const long long rv = (long long)tb.R * tb.V;
+        const long long q = am / rv;
+        r = (int)((am % rv) / tb.V);
+        v = (int)(am % tb.V);
+        ih = w.pairs[q];
+    } else {
+        ih = am;
+    }
+    const int oc = (int)(ih / tb.T);
+    pose[0] = oc / tb.O;
+    pose[1] = oc % tb.O;
+    pose[2] = r;
+    pose[3] = (int)(ih % tb.T);
+    pose[4] = v;
+}
+
+// --------------------------------------------------- reconstruction (FP64)
+__global__ void k_decenter(Volume g, const float2* __restrict__ data, const float* __restrict__ weight,
+                           double2* __restrict__ fconv, double* __restrict__ fw, double* rad, double* cnt)
+{
+    const int ps = g.ydim, fx = ps / 2 + 1;
+    const long long total = (long long)ps * ps * fx;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= total) return;
+    const int j = (int)(n % fx);
+    const int i = (int)((n / fx) % ps);
+    const int k = (int)(n / ((long long)fx * ps));
+    const int kp = k < fx ? k : k - ps, ip = i < fx ? i : i - ps, jp = j;
+    const int rp = g.r_max * g.pad;
+    const int r2 = kp * kp + ip * ip + jp * jp;
+    double2 v = make_double2(0., 0.);
+    double wv = 0.;
+    if (r2 <= rp * rp) {
+        const size_t src = ((size_t)(kp - g.initz) * g.ydim + (ip - g.inity)) * g.xdim + jp;
+        const float2 d = data[src];
+        v = make_double2(d.x, d.y);
+        wv = weight[src];
+    }
+    fconv[n] = v;
+    fw[n] = wv;
+    if (r2 < rp * rp) {
+        const int ires = (int)floor(sqrt((double)r2) / g.pad);
+        atomicAdd(&rad[ires], wv);
+        atomicAdd(&cnt[ires], 1.);
+    }
+}
+
+__global__ void k_radnorm(int r_max, double* rad, const double* cnt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < r_max && (cnt[i] > 0. || rad[i] > 0.)) rad[i] /= 1000. * cnt[i];
+}
+
+__global__ void k_divide(Volume g, double2* __restrict__ fconv, const double* __restrict__ fw, const double* rad)
+{
+    const int ps = g.ydim, fx = ps / 2 + 1;
+    const long long total = (long long)ps * ps * fx;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= total) return;
+    const int j = (int)(n % fx);
+    const int i = (int)((n / fx) % ps);
+    const int k = (int)(n / ((long long)fx * ps));
+    const int kp = k < fx ? k : k - ps, ip = i < fx ? i : i - ps;
+    const int r2 = kp * kp + ip * ip + j * j;
+    const int ires = (int)floor(sqrt((double)r2) / g.pad);
+    const double wv = fmax(fw[n], rad[ires < g.r_max ? ires : g.r_max - 1]);
+    if (wv != 0.) {
+        double2 v = fconv[n];
+        v.x /= wv;
+        v.y /= wv;
+        fconv[n] = v;
+    }
+}
+
+int sm_count()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+int grid_x_for(int nb)
+{
+    const int target = 4 * sm_count();
+    return std::max(1, (target + nb - 1) / std::max(1, nb));
+}
+
+const size_t HIST_SMEM = HIST_BINS * (sizeof(unsigned) + sizeof(double));
+
+void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStream_t st)
+{
+    const int gx = grid_x_for(w.n);
+    dim3 grid(gx, w.n);
+    k_sel_init<<<(w.n + 127) / 128, 128, 0, st>>>(w, fine, tb.adaptive_fraction);
+    k_select<<<w.n, 1024, 0, st>>>(w, fine);
+    for (int level = 1; level < 6; level++) {
+        k_hist_level<<<grid, 256, HIST_SMEM, st>>>(tb, w, fine);
+        k_select<<<w.n, 1024, 0, st>>>(w, fine);
+    }
+    k_gather<<<grid, 256, 0, st>>>(tb, w, fine);
+    k_final<<<w.n, 1024, 0, st>>>(w, fine, ipass);
+}
+
+}  // namespace
+
+void launch_prep(const Tables& tb, const Work& w, cudaStream_t st)
+{
+    k_prep<<<w.n, 256, 0, st>>>(tb, w);
+    k_pdf_t<<<w.n, 128, 0, st>>>(tb, w);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void launch_norms(const Tables& tb, const Work& w, cudaStream_t st)
+{
+    const int KO = tb.K * tb.O;
+    dim3 grid((KO + 63) / 64, (w.n + 15) / 16);
+    k_norms<<<grid, 256, 0, st>>>(tb, w, tb.proj_c, KO, w.norms);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void launch_diff2_simt(const Tables& tb, const Work& w, cudaStream_t st)
+{
+    const int KO = tb.K * tb.O;
+    dim3 grid((KO + SB_M - 1) / SB_M, (w.n * tb.T + SB_N - 1) / SB_N);
+    k_diff2_simt<<<grid, 256, 0, st>>>(tb, w);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStream_t st)
+{
+    (void)maxsig;
+    static bool attr = false;
+    if (!attr) {
+        T2B_CUDA(cudaFuncSetAttribute(k_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HIST_SMEM));
+        T2B_CUDA(cudaFuncSetAttribute(k_hist_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HIST_SMEM));
+        attr = true;
+    }
+    const int gx = grid_x_for(w.n);
+    dim3 grid(gx, w.n);
+    k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 0);
+    run_selection(tb, w, 0, 0, st);
+    const long long n = (long long)tb.K * tb.O * tb.T;
+    const int nch = (int)((n + CHUNK - 1) / CHUNK);
+    dim3 gc(std::min(nch, gx), w.n);
+    k_count_sig<<<gc, 256, 0, st>>>(tb, w);
+    k_scan_pairs<<<1, 1024, 0, st>>>(tb, w);
+    k_compact<<<gc, 256, 0, st>>>(tb, w, tb.ovs ? 0 : 1);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void launch_fine(const Tables& tb, const Work& w, cudaStream_t st)
+{
+    k_fine<<<2 * sm_count(), 256, 0, st>>>(tb, w);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void launch_weights_fine(const Tables& tb, const Work& w, cudaStream_t st)
+{
+    const int gx = grid_x_for(w.n);
+    dim3 grid(gx, w.n);
+    k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 1);
+    run_selection(tb, w, 1, 1, st);
+    k_argmax_fine<<<grid, 256, 0, st>>>(tb, w);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* const* grid_data,
+                    float* const* grid_weight, cudaStream_t st)
+{
+    k_groups<<<1, 1024, 0, st>>>(tb, w, tb.ovs ? tb.R : 1);
+    GridPtrs gp{grid_data, grid_weight};
+    k_wsum_bp<<<2 * sm_count(), 256, 0, st>>>(tb, w, g, gp);
+    k_results<<<(w.n + 127) / 128, 128, 0, st>>>(tb, w);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void launch_reconstruct(const Volume& g, const float2* data, const float* weight, double2* fconv,
+                        double* fw, double* rad, double* cnt, cudaStream_t st)
+{
+    const int ps = g.ydim, fx = ps / 2 + 1;
+    const long long total = (long long)ps * ps * fx;
+    T2B_CUDA(cudaMemsetAsync(rad, 0, sizeof(double) * g.r_max, st));
+    T2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(double) * g.r_max, st));
+    const int nb = (int)((total + 255) / 256);
+    k_decenter<<<nb, 256, 0, st>>>(g, data, weight, fconv, fw, rad, cnt);
+    k_radnorm<<<(g.r_max + 255) / 256, 256, 0, st>>>(g.r_max, rad, cnt);
+    k_divide<<<nb, 256, 0, st>>>(g, fconv, fw, rad);
+    T2B_CUDA(cudaGetLastError());
+}
+
+}  // namespace t2b

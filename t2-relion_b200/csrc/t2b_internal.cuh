@@ -1,0 +1,172 @@
+// Internal declarations of libt2b (sm_100a E-step).  Not part of the ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "../../include/t2b.h"
+
+namespace t2b {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define T2B_CUDA(call)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            throw ::t2b::Error{T2B_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+#define T2B_REQUIRE(cond, code, msg)                                                         \
+    do {                                                                                     \
+        if (!(cond)) throw ::t2b::Error{(code), (msg)};                                      \
+    } while (0)
+
+// ------------------------------------------------------------- geometry
+struct Volume {           // projector model or backprojection grid
+    int ref_dim = 0, xdim = 0, ydim = 0, zdim = 0, inity = 0, initz = 0, r_max = 0, pad = 0;
+    size_t nvox() const { return (size_t)xdim * ydim * zdim; }
+};
+
+// Per-particle state of the radix significance search (FP64 weights).
+struct SelState {
+    double target;            // adaptive_fraction * sum of weights
+    double cum_above;         // sum of the weights above the current prefix bin
+    unsigned long long count_above;
+    unsigned long long prefix;
+    int shift;                // bits below the current prefix
+    int phase;                // 0 searching, 1 gather, 2 done, 3 failed
+    long long ncand;
+    double thr;
+    long long nr_sign;
+    unsigned long long maxbits;
+    long long argmax;
+};
+
+constexpr int HIST_BINS = 4096;  // 12-bit digits
+constexpr int CAND_CAP = 4096;   // candidates sorted in shared memory
+
+// Device views of the per-iteration tables.
+struct Tables {
+    int s, xh, P, ori_size;
+    int K, n_dir, n_psi, O, T, R, V, ovs, ref_dim;
+    const float2* proj_c;     // K*O x P
+    const float2* proj_f;     // K*O*R x P (ovs) else == proj_c
+    const float2* ab_c;       // T x P phase factors
+    const float2* ab_f;       // T*V x P
+    const double* eul_c;      // O x 9 (A)
+    const double* eul_f;      // O*R x 9
+    const double* trans_c;    // T x 2 pixel shifts
+    const double* trans_f;    // T*V x 2
+    const double* trans_prior;// T x 2
+    const double* pdf_o;      // K*n_dir, normalised
+    const unsigned char* skip;// K*O: orientation not evaluated (pdf <= 0)
+    const int* mresol;        // P
+    double sigma2_offset, pixel_size, adaptive_fraction;
+};
+
+// Device views of the batch workspace.
+struct Work {
+    int n;                    // particles in the batch
+    const float2* fimg;       // n x P
+    const float2* fimg_nm;    // n x P
+    const float* ctf;         // n x P
+    const float* minv;        // n x P
+    const double* scal;       // n x 8
+    float2* cvec;             // n x P  (M * s * ctf * X)
+    float* w2;                // n x P  (0.5 * M * s^2 * ctf^2)
+    float* c0;                // n      (Xi2/2 + sum 0.5 M |X|^2)
+    float* norms;             // n x K*O
+    float* d2c;               // n x K*O*T
+    double* wc;               // n x K*O*T
+    unsigned* minkey_c;       // n
+    unsigned* minkey_f;       // n
+    double* pdf_t;            // n x T
+    double* sum_c;            // n
+    double* sum_f;            // n
+    SelState* sel_c;          // n
+    SelState* sel_f;          // n
+    unsigned* hist_cnt;       // n x HIST_BINS
+    double* hist_sum;         // n x HIST_BINS
+    double* cand;             // n x CAND_CAP
+    long long* pairs;         // pair_cap: coarse hidden index of significant pairs
+    int* pair_b;              // pair_cap
+    long long* pair_off;      // n+1
+    long long pair_cap;
+    int* chunk_cnt;           // n x max_chunks
+    int max_chunks;
+    float* d2f;               // pair_cap * R*V
+    double* wf;               // pair_cap * R*V (final weights when ovs; coarse gathered otherwise)
+    long long* groups;        // pair_cap: first pair of each orientation group
+    int* group_b;             // pair_cap
+    long long* group_off;     // n+1
+    unsigned long long* counters; // queue heads etc. (16)
+    int* status;              // n
+    // results (device)
+    double *r_min, *r_sum, *r_sig, *r_csum, *r_csig, *r_pmax;
+    long long *r_nsign, *r_ncsig;
+    int* r_pose;
+    double *r_norm, *r_sumw, *r_sig_off, *r_sigma2, *r_pdf_class, *r_pdf_dir;
+};
+
+// ------------------------------------------------------------- kernels
+// projection tables (project.cu)
+void launch_project_table(const Volume& v, const float2* mdl, const double* eul9, int n, int s,
+                          float2* out, cudaStream_t st);
+void launch_phase_table(const double* shifts, int n, int s, int ori_size, float2* out, cudaStream_t st);
+
+// E-step stages (estep.cu)
+void launch_prep(const Tables& tb, const Work& w, cudaStream_t st);
+void launch_norms(const Tables& tb, const Work& w, cudaStream_t st);
+void launch_diff2_simt(const Tables& tb, const Work& w, cudaStream_t st);
+void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStream_t st);
+void launch_fine(const Tables& tb, const Work& w, cudaStream_t st);
+void launch_weights_fine(const Tables& tb, const Work& w, cudaStream_t st);
+void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* const* grid_data,
+                    float* const* grid_weight, cudaStream_t st);
+void launch_reconstruct(const Volume& g, const float2* data, const float* weight, double2* fconv,
+                        double* fw, double* rad, double* cnt, cudaStream_t st);
+
+// tcgen05 split-BF16 coarse diff2 (diff2_tc.cu)
+struct TcOperands {
+    void* bh;                 // K*O_pad x Kdim bf16 (projections, hi)
+    void* bl;                 // lo
+    void* ah;                 // N_pad x Kdim bf16 (shifted images, hi)
+    void* al;
+    int m_pad, n_pad, kdim;   // padded sizes
+};
+void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
+void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
+bool tc_supported();
+
+}  // namespace t2b
+
+struct t2b_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::vector<t2b::Volume> mvol;            // per class projector geometry
+    std::vector<float2*> mdl;                 // per class device model
+    std::vector<t2b::Volume> gvol;            // per class BP grid geometry
+    std::vector<float2*> gdata;               // per class grid data
+    std::vector<float*> gweight;              // per class grid weight
+    bool configured = false;
+    t2b_config cfg{};
+    t2b::Tables tb{};
+    t2b::Work wk{};
+    t2b::TcOperands tc{};
+    std::vector<void*> allocs;                // owned device allocations (tables + workspace)
+    float2** gd_table = nullptr;              // device table of per-class grid data pointers
+    float** gw_table = nullptr;               // device table of per-class grid weight pointers
+    int last_n = 0;                           // particles of the last batch
+    cudaEvent_t ev[8]{};
+    float stage_ms[6]{};
+};

@@ -1,0 +1,78 @@
+"""Small seeded E-step problems shared by the parity tests."""
+import numpy as np
+
+from conftest import load_package
+
+
+def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=None, ref_dim=3):
+    t2b = load_package()
+    import t2relion_b200.synthetic as sy
+    import oracle as orc
+    presets = {
+        # box 64, order 2 (9216 orientations), 29 shifts, r 16: the CPU-runnable refine
+        "refine_o2": dict(N=64, angpix=2.0, order=2, psi=7.5, rng=3, r=16, snr=0.05, ovs=0),
+        # box 64, order 1 + adaptive oversampling (fine pass), 29 shifts
+        "refine_o1_ovs": dict(N=64, angpix=2.0, order=1, psi=15.0, rng=3, r=16, snr=0.05, ovs=1),
+        # 2D classification: 2D references, psi 6 deg, oversampling 1
+        "class2d": dict(N=48, angpix=2.0, order=0, psi=6.0, rng=3, r=12, snr=0.2, ovs=1),
+    }
+    p = presets[name]
+    N, r, s = p["N"], p["r"], 2 * p["r"]
+    ref_dim = 2 if name == "class2d" else 3
+    maps = []
+    for k in range(nr_classes):
+        vol = sy.blob_volume(N, 40 if ref_dim == 3 else 12, seed=seed + 101 * k, ndim=ref_dim)
+        maps.append(sy.fourier_map(vol, r))
+    samp = t2b.sampling(ref_dim, p["order"], p["psi"], p["ovs"], p["rng"], 1, p["angpix"])
+    cls = np.arange(n_particles) % nr_classes
+    parts = sy.make_particles(maps[0], n_particles, ori_size=N, s=s, r_max=r, angpix=p["angpix"],
+                              snr=p["snr"], seed=seed, max_shift=p["rng"], ref_dim=ref_dim,
+                              classes=cls, class_maps=maps)
+    sigma2_offset = (p["rng"] * p["angpix"]) ** 2
+    pdf_dir = np.ones((nr_classes, samp["n_dir"])) / (samp["n_dir"] * nr_classes)
+    pdf_cls = np.ones(nr_classes) / nr_classes
+    ps = sy.pad_size(r)
+    prob = orc.Problem(ori_size=N, s=s, ref_dim=ref_dim, maps=maps, r_max=r, pad=2, samp=samp,
+                       pdf_direction=pdf_dir, pdf_class=pdf_cls, sigma2_offset=sigma2_offset,
+                       pixel_size=p["angpix"], adaptive_fraction=0.999, ovs=p["ovs"], bp_pad_size=ps,
+                       bp_r_max=r)
+    mres = sy.mresol(s)
+    oparts = prob.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], mres)
+
+    def product():
+        es = t2b.EStep(0)
+        for k in range(nr_classes):
+            es.set_projector(k, maps[k], ref_dim, r, 2)
+            es.init_backprojector(k, ref_dim, ps, r, 2)
+        es.configure(ori_size=N, current_size=s, ref_dim=ref_dim, nr_classes=nr_classes, samp=samp,
+                     pdf_direction=pdf_dir, pdf_class=pdf_cls, sigma2_offset=sigma2_offset,
+                     pixel_size=p["angpix"], adaptive_oversampling=p["ovs"], diff2_mode=diff2_mode,
+                     max_batch=max_batch or n_particles)
+        return es
+
+    return dict(t2b=t2b, sy=sy, maps=maps, samp=samp, parts=parts, prob=prob, oparts=oparts,
+                product=product, N=N, s=s, r=r, pad_size=ps, ovs=p["ovs"], K=nr_classes, ref_dim=ref_dim)
+
+
+def fsc(a, b, shells, nshell):
+    """Fourier shell correlation of two centred half-complex grids."""
+    num = np.bincount(shells, (a * np.conj(b)).real, nshell)
+    da = np.bincount(shells, np.abs(a) ** 2, nshell)
+    db = np.bincount(shells, np.abs(b) ** 2, nshell)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return num / np.sqrt(da * db)
+
+
+def shells_of(shape):
+    if len(shape) == 3:
+        z, y, x = shape
+        kz = np.arange(z)[:, None, None] - z // 2
+        ky = np.arange(y)[None, :, None] - y // 2
+        kx = np.arange(x)[None, None, :]
+        r = np.sqrt(kz * kz + ky * ky + kx * kx)
+    else:
+        y, x = shape
+        ky = np.arange(y)[:, None] - y // 2
+        kx = np.arange(x)[None, :]
+        r = np.sqrt(ky * ky + kx * kx)
+    return np.rint(r).astype(int).reshape(-1)

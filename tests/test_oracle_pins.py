@@ -1,0 +1,83 @@
+"""Pins of the FP64 oracle against the reference's own known answers (CPU)."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def test_ctf_golden_value(oracle):
+    # tests/ctf.cpp:5-9 of the reference: setValues(10000,12000,90,300,2.7,0.1,0,1,0), getCTF(10,10)
+    v = oracle.ctf_value([10000.0, 12000.0, 90.0, 300.0, 2.7, 0.1, 0.0, 1.0, 0.0], 10.0, 10.0)
+    assert v == pytest.approx(0.59154, abs=5e-6)
+
+
+def test_ctf_image_matches_generator(oracle, synth):
+    p = [15000.0, 14500.0, 33.0, 300.0, 2.7, 0.1, 0.0, 1.0, 0.0]
+    a = oracle.ctf_image(p, 128, 1.3, 80)
+    b = synth.ctf_image(p, 128, 1.3, 80)
+    assert np.max(np.abs(a - b)) < 1e-6
+
+
+def _ref_hp():
+    path = os.path.join(ROOT, "oracle", "_ref", "libhp_ref.so")
+    if not os.path.exists(path):
+        pytest.skip("reference HEALPix not built (needs the reference tree)")
+    lib = ctypes.CDLL(path)
+    lib.ref_hp_pix2zphi.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double)]
+    return lib
+
+
+@pytest.mark.parametrize("order", [0, 1, 2, 3, 4])
+def test_healpix_matches_reference(oracle, order):
+    ref = _ref_hp()
+    z, f = ctypes.c_double(), ctypes.c_double()
+    for pix in range(12 * 4 ** order):
+        ref.ref_hp_pix2zphi(order, pix, ctypes.byref(z), ctypes.byref(f))
+        oz, of = oracle.healpix_pix2zphi(order, pix)
+        assert (oz, of) == (z.value, f.value)
+
+
+def test_shift_convention(oracle, synth):
+    """diff2 of a particle made from the reference at the true pose is minimal there."""
+    N, r, s = 32, 8, 16
+    vol = synth.blob_volume(N, 10, seed=3)
+    fmap = synth.fourier_map(vol, r)
+    samp = dict(n_dir=1, n_psi=1, n_trans=3, nover_rot=1, nover_trans=1,
+                eul_coarse=synth.euler_matrix(10., 40., 70.).reshape(1, 9), eul_fine=np.zeros((1, 9)),
+                trans_px=np.array([[0., 0.], [1.5, -1.], [-2., 0.5]]), trans_px_fine=np.zeros((3, 2)),
+                trans_prior=np.zeros((3, 2)))
+    pr = oracle.Problem(ori_size=N, s=s, ref_dim=3, maps=[fmap], r_max=r, pad=2, samp=samp,
+                        pdf_direction=np.ones((1, 1)), pdf_class=np.ones(1), sigma2_offset=100.,
+                        pixel_size=1., adaptive_fraction=0.999, ovs=0, bp_pad_size=synth.pad_size(r), bp_r_max=r)
+    parts = synth.make_particles(fmap, 1, ori_size=N, s=s, r_max=r, angpix=1., snr=1e6, seed=1, max_shift=0)
+    # rebuild the particle at the sampled pose with shift (1.5, -1)
+    A = samp["eul_coarse"].reshape(3, 3)
+    proj = synth.project(fmap, A[None], s, r)[0]
+    ky, kx = synth.window_coords(s)
+    X = parts["ctf"][0] * proj * np.exp(2j * np.pi * (kx * 1.5 + ky * -1.0) / N)
+    mres = synth.mresol(s)
+    P = pr.particles(X[None], parts["ctf"], parts["minv"], parts["scalars"], mres)
+    d2, mn = pr.coarse_diff2(P, 0)
+    assert np.argmin(d2) == 1
+    assert d2[1] == pytest.approx(parts["scalars"][0, 1] / 2, abs=1e-6 * abs(d2).max())
+
+
+def test_oracle_projection_matches_numpy(oracle, synth):
+    N, r, s = 32, 8, 16
+    fmap = synth.fourier_map(synth.blob_volume(N, 10, seed=4), r)
+    samp = dict(n_dir=1, n_psi=1, n_trans=1, nover_rot=1, nover_trans=1, eul_coarse=np.eye(3).reshape(1, 9),
+                eul_fine=np.zeros((1, 9)), trans_px=np.zeros((1, 2)), trans_px_fine=np.zeros((1, 2)),
+                trans_prior=np.zeros((1, 2)))
+    pr = oracle.Problem(ori_size=N, s=s, ref_dim=3, maps=[fmap], r_max=r, pad=2, samp=samp,
+                        pdf_direction=np.ones((1, 1)), pdf_class=np.ones(1), sigma2_offset=1., pixel_size=1.,
+                        adaptive_fraction=0.999, ovs=0, bp_pad_size=synth.pad_size(r), bp_r_max=r)
+    rng = np.random.default_rng(0)
+    for _ in range(5):
+        A = synth.euler_matrix(*rng.uniform(-180, 180, 3))
+        a = pr.project(0, A)
+        b = synth.project(fmap, A[None], s, r)[0]
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
