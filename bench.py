@@ -1,0 +1,371 @@
+"""E-step throughput benchmark (particles/s) on the box-128 refinement workload.
+
+Workload (the headline configuration): 128^3 map of 40 seeded Gaussian blobs at
+1.3 A/px; particles 128x128 with CTF (300 kV, Cs 2.7, Q0 0.1, defocus U(1,3) um,
+astigmatism <= 0.1 um) and white noise at SNR 0.03; HEALPix order 3 x 48 psi =
+36,864 coarse orientations, adaptive oversampling 1 (fine pass at order 4, 8
+rotations x 4 shifts per significant coarse pair); translations range 5 step 1
+(81); Fourier radius 40 px (80 x 41 = 3,280 pixels); backprojection into the
+2x padded 259 x 259 x 130 grid.  A step is one E-step over one batch of
+`--batch` particles: coarse diff2, FP64 weights and significance, fine pass,
+FP64 weights, weighted sums and backprojection.
+
+value: particles/s with inputs resident in HBM (device entry point, CUDA events
+on the launching stream, max over ranks).  e2e: the same metric through the
+host entry point with pinned host buffers (H2D of the batch and D2H of the
+results inside the timed region).  `--impl reference` times the reference's CPU
+E-step (the FP64 port in oracle/) on the host cores instead.
+"""
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_package():
+    name = "t2relion_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = os.path.join(ROOT, "t2-relion_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+WORKLOAD = dict(name="refine3d_box128_order3_ovs1", ori_size=128, angpix=1.3, n_blobs=40, order=3,
+                psi_step=7.5, offset_range=5, offset_step=1, r_max=40, bp_r_max=64, snr=0.03, seed=11)
+METRIC = "E-step particles/s box128: learned+split-BF16 vs plain FP32 GPU; roofline %"
+
+
+def build_problem(t2b, sy, n_particles, seed):
+    w = WORKLOAD
+    N, r = w["ori_size"], w["r_max"]
+    s = 2 * r
+    vol = sy.blob_volume(N, w["n_blobs"], seed=w["seed"])
+    fmap = sy.fourier_map(vol, r)
+    samp = t2b.sampling(3, w["order"], w["psi_step"], 1, w["offset_range"], w["offset_step"], w["angpix"])
+    parts = sy.make_particles(fmap, n_particles, ori_size=N, s=s, r_max=r, angpix=w["angpix"], snr=w["snr"],
+                              seed=seed, max_shift=w["offset_range"])
+    return fmap, samp, parts
+
+
+def setup_context(t2b, sy, fmap, samp, mode, batch, device=0):
+    w = WORKLOAD
+    es = t2b.EStep(device)
+    es.set_projector(0, fmap, 3, w["r_max"], 2)
+    es.init_backprojector(0, 3, sy.pad_size(w["bp_r_max"]), w["bp_r_max"], 2)
+    es.configure(ori_size=w["ori_size"], current_size=2 * w["r_max"], ref_dim=3, nr_classes=1, samp=samp,
+                 pdf_direction=np.full((1, samp["n_dir"]), 1.0 / samp["n_dir"]), pdf_class=np.ones(1),
+                 sigma2_offset=(w["offset_range"] * w["angpix"]) ** 2, pixel_size=w["angpix"],
+                 adaptive_oversampling=1, diff2_mode=mode, max_batch=batch)
+    return es
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d, "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def cpu_baseline(sy, fmap, samp, parts, seconds=20.0):
+    """FP64 oracle (reference CPU E-step port) on the host cores, bounded sample.
+
+    Sample: one particle per host thread through the coarse pass (the part of the
+    reference's E-step that is > 95 % of its time at this workload) over a slice
+    of the 36,864 orientations sized to take about `seconds`; particles/s is
+    extrapolated to the full orientation set.
+    """
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    w = WORKLOAD
+    s = 2 * w["r_max"]
+    cores = os.cpu_count() or 1
+    O = samp["n_dir"] * samp["n_psi"]
+    # calibrate the slice on one particle, one thread
+    def run_slice(nd, npart, nthreads):
+        sub = dict(samp)
+        sub["n_dir"] = nd
+        sub["eul_coarse"] = samp["eul_coarse"][: nd * samp["n_psi"]]
+        prob = orc.Problem(ori_size=w["ori_size"], s=s, ref_dim=3, maps=[fmap], r_max=w["r_max"], pad=2,
+                           samp=sub, pdf_direction=np.ones((1, nd)), pdf_class=np.ones(1),
+                           sigma2_offset=1.0, pixel_size=w["angpix"], adaptive_fraction=0.999, ovs=0,
+                           bp_pad_size=sy.pad_size(w["r_max"]), bp_r_max=w["r_max"])
+        op = prob.particles(parts["fimg"][:npart], parts["ctf"][:npart], parts["minv"][:npart],
+                            parts["scalars"][:npart], sy.mresol(s))
+        t0 = time.perf_counter()
+        ths = [threading.Thread(target=prob.coarse_diff2, args=(op, i)) for i in range(npart)]
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        return time.perf_counter() - t0
+    t1 = run_slice(1, 1, 1)                      # one direction = 48 orientations
+    nd = int(max(1, min(samp["n_dir"], seconds / max(t1, 1e-6))))
+    npart = min(cores, parts["fimg"].shape[0])
+    t = run_slice(nd, npart, npart)
+    frac = nd * samp["n_psi"] / O
+    value = npart * frac / t
+    return {"value": value, "unit": "particles/s", "cores": npart, "kind": "port",
+            "sample": f"{npart} particles x {nd * samp['n_psi']} of {O} orientations (coarse pass, FP64 oracle), "
+                      f"{t:.1f} s, extrapolated to the full orientation set"}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    t2b = load_package()
+    import t2relion_b200.synthetic as sy
+    fmap, samp, parts = build_problem(t2b, sy, max(8, os.cpu_count() or 1), WORKLOAD["seed"] + 1)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(sy, fmap, samp, parts, seconds=args.ref_seconds)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v if v else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD["name"], "particles_per_step": cb["cores"]},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="splitbf16", choices=["splitbf16", "plain"])
+    ap.add_argument("--batch", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+    t2b = load_package()
+    import t2relion_b200.synthetic as sy
+    torch.cuda.set_device(local)
+    B = args.batch
+    fmap, samp, parts = build_problem(t2b, sy, B, WORKLOAD["seed"] + 1000 * rank)
+    mode = t2b.DIFF2_SPLIT_BF16 if args.mode == "splitbf16" else t2b.DIFF2_PLAIN_FP32
+    es = setup_context(t2b, sy, fmap, samp, mode, B, device=local)
+    dev = torch.device("cuda", local)
+    P = parts["fimg"].shape[1]
+    fimg = torch.from_numpy(parts["fimg"].view(np.float32)).to(dev)
+    ctf = torch.from_numpy(parts["ctf"]).to(dev)
+    minv = torch.from_numpy(parts["minv"]).to(dev)
+    scal = torch.from_numpy(parts["scalars"]).to(dev)
+    half = WORKLOAD["ori_size"] // 2 + 1
+    K, nd = 1, samp["n_dir"]
+    res = {k: torch.zeros(shape, dtype=dt, device=dev) for k, shape, dt in [
+        ("min_diff2", B, torch.float64), ("sum_weight", B, torch.float64), ("sig_weight", B, torch.float64),
+        ("coarse_sum_weight", B, torch.float64), ("coarse_sig_weight", B, torch.float64),
+        ("nr_sign", B, torch.int64), ("n_coarse_sig", B, torch.int64), ("pmax", B, torch.float64),
+        ("pose", (B, 5), torch.int32), ("wsum_norm", B, torch.float64), ("sumw", B, torch.float64),
+        ("wsum_sigma2_offset", B, torch.float64), ("wsum_sigma2", (B, half), torch.float64),
+        ("wsum_pdf_class", (B, K), torch.float64), ("wsum_pdf_dir", (B, K * nd), torch.float64),
+        ("status", B, torch.int32)]}
+    rptr = {k: ctypes.c_void_p(v.data_ptr()) for k, v in res.items()}
+    # an explicit stream: the library runs a NULL stream argument on its own stream
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+
+    def step():
+        es.expectation_device(B, ctypes.c_void_p(fimg.data_ptr()), ctypes.c_void_p(ctf.data_ptr()),
+                              ctypes.c_void_p(minv.data_ptr()), ctypes.c_void_p(scal.data_ptr()), rptr,
+                              stream=stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    assert stream.cuda_stream != 0
+    if int(res["status"].ne(0).sum()) != 0:
+        raise RuntimeError(f"E-step status errors: {res['status'].cpu().numpy()}")
+    gemm_ms = []
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+            # the library's own CUDA events bracket each stage on this stream
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    stage = es.stage_ms()  # last step's stages
+    total_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        torch.distributed.barrier()
+    total_ms = max_over_ranks(total_ms, world)
+    # per-stage times averaged over separately synchronised steps (not part of `value`)
+    stages = []
+    for _ in range(min(3, args.steps)):
+        step()
+        stages.append(es.stage_ms())
+    stages = np.mean(np.array(stages), axis=0)
+    ms_per_step = total_ms / args.steps
+    value = B * args.steps * world / (total_ms / 1000.0)
+
+    # end to end through the host entry point (pinned host buffers)
+    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
+           [("fimg", parts["fimg"].view(np.float32)), ("ctf", parts["ctf"]), ("minv", parts["minv"]),
+            ("scal", parts["scalars"])]}
+    hres = {k: torch.zeros(v.shape, dtype=v.dtype).pin_memory() for k, v in res.items()}
+    lib = t2b.lib
+    batch = t2b.Batch(B, 0, ctypes.c_void_p(pin["fimg"].data_ptr()), None, ctypes.c_void_p(pin["ctf"].data_ptr()),
+                      ctypes.c_void_p(pin["minv"].data_ptr()), ctypes.c_void_p(pin["scal"].data_ptr()))
+    result = t2b.Result(*[ctypes.c_void_p(hres[n].data_ptr()) for n, _ in t2b.Result._fields_])
+
+    def e2e_step():
+        t2b._check(lib.t2b_estep_batch_host(es._h, ctypes.byref(batch), ctypes.byref(result)))
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    h2d = sum(v.numel() * v.element_size() for v in pin.values())
+    d2h = sum(v.numel() * v.element_size() for v in hres.values())
+    e2e = {"value": B * args.steps * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h}
+
+    # roofline of the dominant kernel (coarse diff2 contraction)
+    O, T = samp["n_dir"] * samp["n_psi"], samp["n_trans"]
+    flops = 8.0 * K * O * T * P * B
+    gemm = float(stages[2])
+    peaks, src = measured_peaks()
+    if mode == t2b.DIFF2_SPLIT_BF16:
+        peak = peaks.get("bf16_tflops_sustained", 1400.0)
+        bound = "tensor"
+    else:
+        peak = 148 * 128 * 2 * 1.965e-3  # FP32 SIMT nominal TFLOP/s (no measured figure)
+        bound = "fp32_simt"
+        src = "nominal"
+    achieved = flops / (gemm / 1000.0) / 1e12
+    roof = {"bound": bound, "kernel": "k_diff2_tc" if mode else "k_diff2_simt", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src,
+            "traffic": None, "flops_per_launch": flops}
+    line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+bf16x3/f64" if mode else "f32/f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"], "particles_per_step": B, "diff2": args.mode,
+                       "orientations": O, "translations": T, "pixels": P,
+                       "l2": "working set > L2 (bf16 hi/lo projection operands 0.97 GB per step)"},
+            "e2e": e2e, "gpu_launches": None, "clocks": clk.summary(), "roofline": roof,
+            "stage_ms": {n: float(v) for n, v in zip(
+                ["prep_norms", "operand_split", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
+                 "wsum_bp"], stages)},
+            "nr_sign_mean": float(res["nr_sign"].double().mean())}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sy, fmap, samp, parts)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    es.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -170,9 +170,10 @@ int t2b_project(t2b_ctx* ctx, int iclass, const double* eulers, int n, int curre
 int t2b_debug_coarse_diff2(t2b_ctx* ctx, int b, float* out);
 int t2b_debug_fine(t2b_ctx* ctx, int b, long long* pairs, float* diff2, long long cap, long long* count);
 
-/* Device time of the stages of the last batch, in ms (CUDA events):
- * [0] prep+norms, [1] coarse diff2, [2] coarse weights, [3] fine pass,
- * [4] fine weights, [5] weighted sums + backprojection.  n <= 6. */
+/* Device time of the stages of the last batch, in ms (CUDA events on the
+ * stream the stages ran on): [0] prep + norms, [1] tensor-core operand split,
+ * [2] coarse diff2 contraction, [3] coarse weights + significance + compaction,
+ * [4] fine pass, [5] fine weights, [6] weighted sums + backprojection.  n <= 7. */
 int t2b_last_stage_ms(t2b_ctx* ctx, float* ms, int n);
 
 /* Host sampling (HealpixSampling, src/healpix_sampling.cpp:534-640,

@@ -291,8 +291,8 @@ class EStep:
                                           ctypes.c_void_p(stream)))
 
     def stage_ms(self):
-        ms = np.zeros(6, np.float32)
-        _check(lib.t2b_last_stage_ms(self._h, _ptr(ms), 6))
+        ms = np.zeros(7, np.float32)
+        _check(lib.t2b_last_stage_ms(self._h, _ptr(ms), 7))
         return ms
 
     def coarse_diff2(self, b):

@@ -372,6 +372,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         w.group_b = dalloc<int>(c, w.pair_cap);
         w.group_off = dalloc<long long>(c, B + 1);
         w.counters = dalloc<unsigned long long>(c, 16);
+        w.err = dalloc<int>(c, 1);
         w.status = dalloc<int>(c, B);
         // staging of host inputs and internal results
         w.fimg = dalloc<float2>(c, (size_t)B * P);
@@ -395,7 +396,17 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         c->gd_table = gd;
         c->gw_table = gw;
         c->tc = TcOperands{};
-        if (f.diff2_mode == T2B_DIFF2_SPLIT_BF16) tc_prepare_projections(tb, c->tc, st);
+        if (f.diff2_mode == T2B_DIFF2_SPLIT_BF16) {
+            TcOperands& op = c->tc;
+            op.kdim = (int)tc_kdim(P);
+            op.m_pad = (int)((KO + 127) / 128 * 128);
+            op.n_pad = (B * T + 255) / 256 * 256;
+            op.bh = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kdim);
+            op.bl = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kdim);
+            op.ah = dalloc<uint16_t>(c, (size_t)op.n_pad * op.kdim);
+            op.al = dalloc<uint16_t>(c, (size_t)op.n_pad * op.kdim);
+            tc_prepare_projections(tb, op, st);
+        }
         T2B_CUDA(cudaStreamSynchronize(st));
         c->configured = true;
     });
@@ -410,21 +421,25 @@ static void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st)
 {
     const Tables& tb = c->tb;
     T2B_CUDA(cudaMemsetAsync(w.counters, 0, 16 * sizeof(unsigned long long), st));
+    T2B_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     cudaEventRecord(c->ev[0], st);
     launch_prep(tb, w, st);
     launch_norms(tb, w, st);
     cudaEventRecord(c->ev[1], st);
-    if (c->cfg.diff2_mode == T2B_DIFF2_SPLIT_BF16) tc_launch_diff2(tb, w, c->tc, st);
-    else launch_diff2_simt(tb, w, st);
+    const bool tc = c->cfg.diff2_mode == T2B_DIFF2_SPLIT_BF16;
+    if (tc) tc_split_images(tb, w, c->tc, st);
     cudaEventRecord(c->ev[2], st);
-    launch_weights_coarse(tb, w, c->cfg.maximum_significants, st);
+    if (tc) tc_launch_diff2(tb, w, c->tc, st);
+    else launch_diff2_simt(tb, w, st);
     cudaEventRecord(c->ev[3], st);
-    if (tb.ovs) launch_fine(tb, w, st);
+    launch_weights_coarse(tb, w, c->cfg.maximum_significants, st);
     cudaEventRecord(c->ev[4], st);
-    if (tb.ovs) launch_weights_fine(tb, w, st);
+    if (tb.ovs) launch_fine(tb, w, st);
     cudaEventRecord(c->ev[5], st);
-    launch_wsum_bp(tb, w, c->gvol[0], c->gd_table, c->gw_table, st);
+    if (tb.ovs) launch_weights_fine(tb, w, st);
     cudaEventRecord(c->ev[6], st);
+    launch_wsum_bp(tb, w, c->gvol[0], c->gd_table, c->gw_table, st);
+    cudaEventRecord(c->ev[7], st);
 }
 
 static void check_batch(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
@@ -437,7 +452,7 @@ static void check_batch(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
 
 static void collect_stage_ms(t2b_ctx* c)
 {
-    for (int i = 0; i < 6; i++) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+    for (int i = 0; i < 7; i++) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
 }
 
 }  // namespace t2b
@@ -519,7 +534,7 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
 int t2b_last_stage_ms(t2b_ctx* c, float* ms, int n)
 {
     return guarded([&] {
-        T2B_REQUIRE(c && ms && n >= 0 && n <= 6, T2B_ERR_ARG, "bad arguments");
+        T2B_REQUIRE(c && ms && n >= 0 && n <= 7, T2B_ERR_ARG, "bad arguments");
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard g(c->device);
         T2B_CUDA(cudaStreamSynchronize(c->stream));

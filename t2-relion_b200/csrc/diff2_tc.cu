@@ -1,18 +1,458 @@
-// tcgen05 split-BF16 coarse diff2 (placeholder until the tensor-core kernel lands).
+// Coarse diff2 on the 5th-generation tensor cores (tcgen05, sm_100a) with a
+// three-product split-BF16 contraction and FP32 accumulation in TMEM.
+//
+// The cross term of diff2 (src/ml_optimiser.cpp:7251-7272; the reference's
+// coarse_splitImg_BCF_PMO.cuh:139-693 runs it as 3xTF32 mma.sync) is a real
+// GEMM over K = 2P interleaved (re, im) values:
+//     C[oc][b*T+t] = sum_k Proj[oc][k] * Img[b*T+t][k]
+// Every FP32 operand x is split as hi = bf16(x), lo = bf16(x - hi), and
+//     C ~= Ph.Ih + Ph.Il + Pl.Ih      (the lo.lo term is below FP32 resolution)
+// The three products accumulate into one FP32 TMEM accumulator.
+//
+// Kernel: persistent, one CTA per SM, 192 threads.
+//   warp 0      TMA producer: per 64-wide K block loads Ph, Pl (128 x 64) and
+//               Ih, Il (256 x 64) with 128-byte swizzle into a 2-stage ring
+//   warp 1      MMA issuer: 12 x tcgen05.mma (M128 N256 K16) per K block into a
+//               double-buffered 2 x 256-column TMEM accumulator
+//   warps 2-5   epilogue: tcgen05.ld 32x32b, transpose through shared memory,
+//               diff2 = c0 + norm - C written coalesced along t, per-particle
+//               minimum by shared + global atomics
+// Every mbarrier wait is bounded (2 s); on expiry the CTA records
+// T2B_ERR_TIMEOUT in a device flag, waits (bounded) for its own copies and
+// MMAs, frees TMEM and returns.
 #include "t2b_internal.cuh"
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <algorithm>
 
 namespace t2b {
+namespace {
 
-bool tc_supported() { return false; }
+constexpr int TM = 128, TN = 256, TK = 64;
+constexpr int STAGES = 2;
+constexpr uint32_t A_BYTES = TM * TK * 2;              // 16 KB
+constexpr uint32_t B_BYTES = TN * TK * 2;              // 32 KB
+constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
+constexpr int NTHREADS = 192;
+constexpr uint32_t TMEM_COLS = 512;
+constexpr int EPI_LD = 33;
+constexpr size_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 4 * 32 * EPI_LD * 4 + 4 * (TN + 2) * 4;
+constexpr unsigned long long WAIT_NS = 2000000000ull;
 
-void tc_prepare_projections(const Tables&, TcOperands&, cudaStream_t)
+// instruction descriptor: D f32, A/B bf16, both K-major, N = 256, M = 128
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtimer()
 {
-    throw Error{T2B_ERR_UNSUPPORTED, "split-BF16 contraction not built"};
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
-void tc_launch_diff2(const Tables&, const Work&, TcOperands&, cudaStream_t)
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t n)
 {
-    throw Error{T2B_ERR_UNSUPPORTED, "split-BF16 contraction not built"};
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(n));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase of parity `parity`; false on timeout / abort.
+__device__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag)
+{
+    const unsigned long long t0 = gtimer();
+    for (uint32_t i = 1;; i++) {
+        if (mbar_try(b, parity)) return true;
+        if ((i & 255u) == 0) {
+            if (*abort_flag) return false;
+            if (gtimer() - t0 > WAIT_NS) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            su32(dst)),
+        "l"(map), "r"(su32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset
+    d |= (uint64_t)1 << 46;             // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void umma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t accum)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            dtmem),
+        "l"(a), "l"(b), "r"(IDESC), "r"(accum));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned f2key(float f)
+{
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+struct TcParams {
+    int m_tiles, n_tiles, kblocks;
+    int KO, T, ncols;
+    const float* c0;
+    const float* norms;
+    const unsigned char* skip;
+    float* d2c;
+    unsigned* minkey;
+    int* err;
+};
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+k_diff2_tc(const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUtensorMap mPl,
+           const __grid_constant__ CUtensorMap mIh, const __grid_constant__ CUtensorMap mIl, TcParams p)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], tfull_bar[2], tempty_bar[2], drain_bar;
+    __shared__ uint32_t tmem_base_slot;
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t base = (su32(smem_raw) + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - su32(smem_raw));
+    float* epi = reinterpret_cast<float*>(gbase + STAGES * STAGE_BYTES);          // 4 x 32 x 33
+    unsigned* smin = reinterpret_cast<unsigned*>(epi + 4 * 32 * EPI_LD);          // 4 x (TN+2)
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) { mbar_init(&full_bar[s], 1); mbar_init(&empty_bar[s], 1); }
+        for (int s = 0; s < 2; s++) { mbar_init(&tfull_bar[s], 1); mbar_init(&tempty_bar[s], 4); }
+        mbar_init(&drain_bar, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_slot;
+    const int ntiles = p.m_tiles * p.n_tiles;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer
+        int it = 0;
+        int issued[STAGES] = {0, 0};
+        uint32_t last_par[STAGES] = {0, 0};
+        for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
+            const int mt = tile / p.n_tiles, nt = tile - mt * p.n_tiles;
+            for (int kb = 0; kb < p.kblocks; kb++, it++) {
+                const int s = it % STAGES;
+                const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+                if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
+                uint8_t* st = gbase + s * STAGE_BYTES;
+                mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+                tma_load(st, &mPh, &full_bar[s], kb * TK, mt * TM);
+                tma_load(st + A_BYTES, &mPl, &full_bar[s], kb * TK, mt * TM);
+                tma_load(st + 2 * A_BYTES, &mIh, &full_bar[s], kb * TK, nt * TN);
+                tma_load(st + 2 * A_BYTES + B_BYTES, &mIl, &full_bar[s], kb * TK, nt * TN);
+                issued[s] = 1;
+                last_par[s] = ph;
+            }
+        }
+        if (abort_flag) {
+            // let the copies already in flight land before the CTA exits
+            volatile int never = 0;
+            for (int s = 0; s < STAGES; s++)
+                if (issued[s]) mbar_wait(&full_bar[s], last_par[s], &never);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer
+        int it = 0, tl = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x, tl++) {
+            const int abuf = tl & 1;
+            const uint32_t aph = (uint32_t)(tl >> 1) & 1u;
+            if (!mbar_wait(&tempty_bar[abuf], aph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
+            tc_fence_after();
+            const uint32_t dt = tmem + (uint32_t)(abuf * TN);
+            bool ok = true;
+            for (int kb = 0; kb < p.kblocks; kb++, it++) {
+                const int s = it % STAGES;
+                const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+                if (!mbar_wait(&full_bar[s], ph, &abort_flag)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t sa = base + s * STAGE_BYTES;
+                const uint64_t dPh = sdesc(sa), dPl = sdesc(sa + A_BYTES);
+                const uint64_t dIh = sdesc(sa + 2 * A_BYTES), dIl = sdesc(sa + 2 * A_BYTES + B_BYTES);
+#pragma unroll
+                for (int k = 0; k < TK / 16; k++) {
+                    const uint64_t ko = (uint64_t)(k * 32) >> 4;  // 32 bytes per K=16 step
+                    umma(dt, dPh + ko, dIh + ko, (kb | k) != 0);
+                    umma(dt, dPh + ko, dIl + ko, 1);
+                    umma(dt, dPl + ko, dIh + ko, 1);
+                }
+                umma_commit(&empty_bar[s]);  // stage free once these MMAs retire
+            }
+            if (!ok) { abort_flag = 1; break; }
+            umma_commit(&tfull_bar[abuf]);   // accumulator ready
+        }
+        // drain: every MMA issued by this thread has retired before TMEM is freed
+        umma_commit(&drain_bar);
+        volatile int never = 0;
+        mbar_wait(&drain_bar, 0, &never);
+    } else if (warp >= 2) {
+        // ---------------- epilogue (warps 2..5 -> TMEM lane quarters 2,3,0,1)
+        const int q = warp & 3;
+        const int ew = warp - 2;
+        float* sbuf = epi + ew * 32 * EPI_LD;
+        unsigned* wmin = smin + ew * (TN + 2);
+        int tl = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x, tl++) {
+            const int mt = tile / p.n_tiles, nt = tile - mt * p.n_tiles;
+            const int abuf = tl & 1;
+            const uint32_t aph = (uint32_t)(tl >> 1) & 1u;
+            if (!mbar_wait(&tfull_bar[abuf], aph, &abort_flag)) { abort_flag = 1; break; }
+            tc_fence_after();
+            const int n0 = nt * TN;
+            const int bfirst = n0 / p.T;
+            for (int i = lane; i < TN + 2; i += 32) wmin[i] = 0xffffffffu;
+            __syncwarp();
+            for (int c = 0; c < TN / 32; c++) {
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
+#pragma unroll
+                for (int j = 0; j < 32; j++) sbuf[lane * EPI_LD + j] = __uint_as_float(v[j]);
+                __syncwarp();
+                // lane = column within the chunk; rows walk the warp's 32 TMEM lanes
+                const int col = n0 + c * 32 + lane;
+                const bool cok = col < p.ncols;
+                const int b = cok ? col / p.T : 0;
+                const int t = cok ? col - b * p.T : 0;
+                const float c0 = cok ? p.c0[b] : 0.f;
+                unsigned lmin = 0xffffffffu;
+                for (int r = 0; r < 32; r++) {
+                    const int oc = mt * TM + q * 32 + r;
+                    if (!cok || oc >= p.KO) continue;
+                    float d;
+                    if (p.skip[oc]) {
+                        d = -999.f;
+                    } else {
+                        d = c0 + p.norms[(size_t)b * p.KO + oc] - sbuf[r * EPI_LD + lane];
+                        lmin = min(lmin, f2key(d));
+                    }
+                    p.d2c[((size_t)b * p.KO + oc) * p.T + t] = d;
+                }
+                if (cok && lmin != 0xffffffffu) atomicMin(&wmin[b - bfirst], lmin);
+                __syncwarp();
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty_bar[abuf]);
+            for (int i = lane; i < TN + 2; i += 32) {
+                const int b = bfirst + i;
+                if (wmin[i] != 0xffffffffu && b * p.T < p.ncols) atomicMin(&p.minkey[b], wmin[i]);
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (abort_flag && threadIdx.x == 0) atomicExch(p.err, T2B_ERR_TIMEOUT);
+    tc_fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+// ------------------------------------------------------------------ operands
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo)
+{
+    hi = __float2bfloat16_rn(x);
+    lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// projections (K*O x P complex) -> Ph/Pl (m_pad x kdim bf16), zero padded
+__global__ void k_split_proj(const float2* __restrict__ proj, int rows, int P, int kdim,
+                             __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / (kdim / 2);
+        const int pp = (int)(i - r * (kdim / 2));
+        float2 v = make_float2(0.f, 0.f);
+        if (r < rows && pp < P) v = proj[r * P + pp];
+        __nv_bfloat16 h0, l0, h1, l1;
+        split_bf16(v.x, h0, l0);
+        split_bf16(v.y, h1, l1);
+        reinterpret_cast<__nv_bfloat162*>(hi)[i] = __halves2bfloat162(h0, h1);
+        reinterpret_cast<__nv_bfloat162*>(lo)[i] = __halves2bfloat162(l0, l1);
+    }
+}
+
+// shifted, CTF- and sigma-weighted images: column b*T+t, value cvec_b[p] * ab_t[p]
+__global__ void k_split_img(const float2* __restrict__ cvec, const float2* __restrict__ ab, int ncols, int T, int P,
+                            int kdim, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long col = i / (kdim / 2);
+        const int pp = (int)(i - col * (kdim / 2));
+        float2 v = make_float2(0.f, 0.f);
+        if (col < ncols && pp < P) {
+            const int b = (int)(col / T), t = (int)(col - (long long)b * T);
+            const float2 c = cvec[(size_t)b * P + pp];
+            const float2 a = ab[(size_t)t * P + pp];
+            v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+        }
+        __nv_bfloat16 h0, l0, h1, l1;
+        split_bf16(v.x, h0, l0);
+        split_bf16(v.y, h1, l1);
+        reinterpret_cast<__nv_bfloat162*>(hi)[i] = __halves2bfloat162(h0, h1);
+        reinterpret_cast<__nv_bfloat162*>(lo)[i] = __halves2bfloat162(l0, l1);
+    }
+}
+
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encoder()
+{
+    static EncodeFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p)
+            throw Error{T2B_ERR_CUDA, "cuTensorMapEncodeTiled unavailable"};
+        fn = reinterpret_cast<EncodeFn>(p);
+    }
+    return fn;
+}
+
+CUtensorMap make_map(void* ptr, int rows, int kdim, int box_rows)
+{
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kdim * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims, strides, box, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error{T2B_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    return m;
+}
+
+int sms()
+{
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+}  // namespace
+
+bool tc_supported() { return true; }
+
+size_t tc_kdim(int P) { return (size_t)((2 * P + TK - 1) / TK) * TK; }
+
+void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
+{
+    const int rows = tb.K * tb.O;
+    op.m_pad = (rows + TM - 1) / TM * TM;
+    op.kdim = (int)tc_kdim(tb.P);
+    const size_t n = (size_t)op.m_pad * op.kdim;
+    T2B_REQUIRE(op.bh && op.bl, T2B_ERR_STATE, "tensor-core operands not allocated");
+    const long long total = (long long)n / 2;
+    k_split_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, op.kdim, (__nv_bfloat16*)op.bh,
+                                            (__nv_bfloat16*)op.bl, total);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st)
+{
+    const int ncols = w.n * tb.T;
+    const int n_pad = (ncols + TN - 1) / TN * TN;
+    T2B_REQUIRE(n_pad <= op.n_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
+    const long long total = (long long)n_pad * op.kdim / 2;
+    k_split_img<<<4 * sms(), 256, 0, st>>>(w.cvec, tb.ab_c, ncols, tb.T, tb.P, op.kdim, (__nv_bfloat16*)op.ah,
+                                           (__nv_bfloat16*)op.al, total);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st)
+{
+    const int ncols = w.n * tb.T;
+    const int n_pad = (ncols + TN - 1) / TN * TN;
+    T2B_REQUIRE(n_pad <= op.n_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
+    const CUtensorMap mPh = make_map(op.bh, op.m_pad, op.kdim, TM);
+    const CUtensorMap mPl = make_map(op.bl, op.m_pad, op.kdim, TM);
+    const CUtensorMap mIh = make_map(op.ah, n_pad, op.kdim, TN);
+    const CUtensorMap mIl = make_map(op.al, n_pad, op.kdim, TN);
+    TcParams p;
+    p.m_tiles = op.m_pad / TM;
+    p.n_tiles = n_pad / TN;
+    p.kblocks = op.kdim / TK;
+    p.KO = tb.K * tb.O;
+    p.T = tb.T;
+    p.ncols = ncols;
+    p.c0 = w.c0;
+    p.norms = w.norms;
+    p.skip = tb.skip;
+    p.d2c = w.d2c;
+    p.minkey = w.minkey_c;
+    p.err = w.err;
+    static bool attr = false;
+    if (!attr) {
+        T2B_CUDA(cudaFuncSetAttribute(k_diff2_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+        attr = true;
+    }
+    const int grid = std::min(sms(), p.m_tiles * p.n_tiles);
+    k_diff2_tc<<<grid, NTHREADS, SMEM_BYTES, st>>>(mPh, mPl, mIh, mIl, p);
+    T2B_CUDA(cudaGetLastError());
 }
 
 }  // namespace t2b

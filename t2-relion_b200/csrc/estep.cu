@@ -4,7 +4,7 @@
 //   prep      cvec = Minvsigma2 * scale * CTF * X, w2 = 0.5 * Minvsigma2 * (scale CTF)^2,
 //             c0 = highres_Xi2/2 + sum 0.5 Minvsigma2 |X|^2
 //   norms     N[b][oc] = sum_p w2[b][p] |P_oc[p]|^2
-//   diff2     D[b][oc*T+t] = c0[b] + N[b][oc] - 2 sum_p Re(P_oc[p] conj(cvec_b[p] ab_t[p]))
+//   diff2     D[b][oc*T+t] = c0[b] + N[b][oc] - sum_p Re(P_oc[p] conj(cvec_b[p] ab_t[p]))
 //             which equals highres_Xi2/2 + sum_p 0.5 M |scale CTF P - shift_t X|^2
 //             (src/ml_optimiser.cpp:7251-7272; the reference GPU kernel splits the
 //             same three terms, coarse_splitImg_BCF_PMO.cuh:139-693)
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(256, 2) k_diff2_simt(Tables tb, Work w)
             if (skip) {
                 d = -999.f;
             } else {
-                d = w.c0[b] + w.norms[(size_t)b * KO + oc] - 2.f * acc[i][j];
+                d = w.c0[b] + w.norms[(size_t)b * KO + oc] - acc[i][j];
                 atomicMin(&smin[b - bfirst], f2key(d));
             }
             w.d2c[((size_t)b * KO + oc) * T + t] = d;
@@ -742,7 +742,7 @@ __global__ void __launch_bounds__(256) k_fine(Tables tb, Work w)
             const int r = threadIdx.x / V, v = threadIdx.x - r * V;
             float cs = 0.f, ns = 0.f;
             for (int j = 0; j < 8; j++) { cs += red[j][r * MAXV + v]; ns += red[j][MAXR * MAXV + r]; }
-            const float d = w.c0[b] + ns - 2.f * cs;
+            const float d = w.c0[b] + ns - cs;
             w.d2f[q * R * V + r * V + v] = d;
             atomicMin(&w.minkey_f[b], f2key(d));
         }
@@ -975,6 +975,7 @@ __global__ void k_results(Tables tb, Work w)
     w.r_sig[b] = sf.thr;
     w.r_min[b] = (double)key2f(tb.ovs ? w.minkey_f[b] : w.minkey_c[b]);
     int* pose = w.r_pose + 5 * (size_t)b;
+    if (*w.err != 0 && w.status[b] == T2B_OK) w.status[b] = *w.err;
     if (w.status[b] != T2B_OK || sf.phase != 2) {
         if (w.status[b] == T2B_OK) w.status[b] = T2B_ERR_NOSIGNIF;
         w.r_pmax[b] = -1.;

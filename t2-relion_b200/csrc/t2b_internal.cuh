@@ -109,6 +109,7 @@ struct Work {
     int* group_b;             // pair_cap
     long long* group_off;     // n+1
     unsigned long long* counters; // queue heads etc. (16)
+    int* err;                 // device error flag of bounded waits (T2B_ERR_TIMEOUT)
     int* status;              // n
     // results (device)
     double *r_min, *r_sum, *r_sig, *r_csum, *r_csig, *r_pmax;
@@ -143,7 +144,9 @@ struct TcOperands {
     void* al;
     int m_pad, n_pad, kdim;   // padded sizes
 };
+size_t tc_kdim(int P);
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
+void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
 void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
 bool tc_supported();
 
@@ -168,5 +171,5 @@ struct t2b_ctx {
     float** gw_table = nullptr;               // device table of per-class grid weight pointers
     int last_n = 0;                           // particles of the last batch
     cudaEvent_t ev[8]{};
-    float stage_ms[6]{};
+    float stage_ms[7]{};
 };

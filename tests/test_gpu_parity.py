@@ -15,14 +15,24 @@ pytestmark = pytest.mark.gpu
 DIFF2_RTOL = 1e-5
 
 
-@pytest.fixture(scope="module", params=["refine_o2", "refine_o1_ovs"])
+_ORACLE = {}
+
+
+@pytest.fixture(scope="module", params=[("refine_o2", 0), ("refine_o1_ovs", 0),
+                                        ("refine_o2", 1), ("refine_o1_ovs", 1)],
+                ids=["o2-plain", "o1ovs-plain", "o2-splitbf16", "o1ovs-splitbf16"])
 def run(request):
-    pb = problems.build(request.param)
+    name, mode = request.param
+    pb = problems.build(name, diff2_mode=mode)
     es = pb["product"]()
     P = pb["parts"]
     res = es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
     pb["es"], pb["res"] = es, res
-    pb["ores"] = pb["prob"].estep(pb["oparts"])
+    if name not in _ORACLE:
+        _ORACLE[name] = pb["prob"].estep(pb["oparts"])
+        _ORACLE[name + "_grids"] = pb["prob"].grids()
+    pb["ores"] = _ORACLE[name]
+    pb["ogrids"] = _ORACLE[name + "_grids"]
     yield pb
     es.close()
 
@@ -101,7 +111,7 @@ def test_final_weights_close(run):
 def test_backprojection_fsc(run):
     es = run["es"]
     data, w = es.get_backprojector(0)
-    od, ow = run["prob"].grids()
+    od, ow = run["ogrids"]
     od, ow = od[0], ow[0]
     sh = problems.shells_of(data.shape)
     nsh = run["r"] * 2 + 1
