@@ -158,6 +158,27 @@ int t2b_estep_batch_device(t2b_ctx* ctx, const t2b_batch* batch, const t2b_resul
  * double, host memory. */
 int t2b_reconstruct_divide(t2b_ctx* ctx, int iclass, double* fconv);
 
+/* Maximum r_max of t2b_reconstruct_divide_noalloc. */
+#define T2B_NOALLOC_MAX_RMAX 2048
+
+/* No counterpart in the reference.  The skip-gridding division of
+ * t2b_reconstruct_divide for callers that cannot allocate device memory: in a
+ * RELION process the GPU arena allocator has already reserved most free device
+ * memory, and cudaMalloc/cudaFree would synchronise the whole device under
+ * work running on other streams.  Everything is caller-owned device memory:
+ * `data` (complex interleaved) and `weight` are a centred 3D grid as returned
+ * by t2b_backprojector_device_ptrs; `fconv` receives [pad][pad][pad/2+1]
+ * complex doubles.  Enqueued on `stream` (cudaStream_t, NULL = legacy default
+ * stream); no cudaMalloc, cudaFree or allocating library call.  Scratch (the
+ * radial weight averages) is a fixed device array of 2 * T2B_NOALLOC_MAX_RMAX
+ * doubles per device, shared by all calls and cleared by each: calls on one
+ * device must not overlap on the GPU.  r_max > T2B_NOALLOC_MAX_RMAX returns
+ * T2B_ERR_ARG.  The first call on a device resolves the scratch address; make
+ * it before any stream capture. */
+int t2b_reconstruct_divide_noalloc(const float* data, const float* weight, int xdim, int ydim, int zdim,
+                                   int inity, int initz, int r_max, int padding_factor, double* fconv,
+                                   void* stream);
+
 /* Projections of `n` orientations (host Euler matrices, n x 9) of class
  * `iclass` on the current_size window (AccProjectorKernel::project3Dmodel,
  * src/acc/acc_projectorkernel_impl.h:179-250); out: host, n x 2P. */

@@ -36,7 +36,7 @@ ABI_SYMBOLS = (
     "t2b_backprojector_get", "t2b_backprojector_device_ptrs", "t2b_configure",
     "t2b_estep_batch_host", "t2b_estep_batch_device", "t2b_reconstruct_divide",
     "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_last_stage_ms",
-    "t2b_sampling",
+    "t2b_sampling", "t2b_reconstruct_divide_noalloc",
 )
 
 
@@ -102,6 +102,7 @@ def _setup_prototypes():
     lib.t2b_estep_batch_host.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(Result)]
     lib.t2b_estep_batch_device.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(Result), v]
     lib.t2b_reconstruct_divide.argtypes = [v, i, v]
+    lib.t2b_reconstruct_divide_noalloc.argtypes = [v, v, i, i, i, i, i, i, i, v, v]
     lib.t2b_project.argtypes = [v, i, v, i, i, v]
     lib.t2b_debug_coarse_diff2.argtypes = [v, i, v]
     lib.t2b_debug_fine.argtypes = [v, i, v, v, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
