@@ -47,6 +47,8 @@ def load_package():
 
 WORKLOAD = dict(name="refine3d_box128_order3_ovs1", ori_size=128, angpix=1.3, n_blobs=40, order=3,
                 psi_step=7.5, offset_range=5, offset_step=1, r_max=40, bp_r_max=64, snr=0.03, seed=11)
+# reduced case for ncu captures (device memory of a few GB): HEALPix order 2, otherwise identical
+PROFILE_WORKLOAD = dict(WORKLOAD, name="refine3d_box128_order2_ovs1_profile", order=2)
 METRIC = "E-step particles/s box128: learned+split-BF16 vs plain FP32 GPU; roofline %"
 
 
@@ -230,7 +232,11 @@ def main():
     ap.add_argument("--batch", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
+    ap.add_argument("--profile-case", action="store_true",
+                    help="HEALPix order 2 instead of 3 (for ncu captures; not a bench number)")
     args = ap.parse_args()
+    if args.profile_case:
+        WORKLOAD.update(PROFILE_WORKLOAD)
     world, rank, local = dist_init()
     if args.impl == "reference":
         run_reference(args, world, rank)

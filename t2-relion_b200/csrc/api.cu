@@ -8,6 +8,7 @@
 // synchronisation between the coarse pass and the backprojection.
 #include "t2b_internal.cuh"
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -287,12 +288,14 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             for (int d = 0; d < f.n_dir; d++) om += f.pdf_direction[k * f.n_dir + d] * f.n_psi;
         om /= (double)(K * f.n_dir * f.n_psi);
         std::vector<unsigned char> skip(KO);
+        double lpo_min = INFINITY, lpo_max = -INFINITY;
         for (int k = 0; k < K; k++)
             for (int d = 0; d < f.n_dir; d++) {
                 double v = f.pdf_direction[k * f.n_dir + d];
                 const bool sk = !(f.pdf_class[k] > 0.) || !(v > 0.);
                 if (om != 0.) v /= om;
                 pdf_o[(size_t)k * f.n_dir + d] = v;
+                if (!sk) { lpo_min = std::min(lpo_min, std::log(v)); lpo_max = std::max(lpo_max, std::log(v)); }
                 for (int p = 0; p < f.n_psi; p++) skip[(size_t)k * O + d * f.n_psi + p] = sk;
             }
         auto up = [&](const void* h, size_t bytes) {
@@ -300,6 +303,9 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             T2B_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
             return d;
         };
+        T2B_REQUIRE(lpo_max > -INFINITY, T2B_ERR_ARG, "every orientation has a zero prior");
+        tb.lpo_min = lpo_min;
+        tb.lpo_max = lpo_max;
         tb.pdf_o = (const double*)up(pdf_o.data(), pdf_o.size() * sizeof(double));
         tb.skip = (const unsigned char*)up(skip.data(), skip.size());
         tb.mresol = (const int*)up(f.mresol, (size_t)P * sizeof(int));
@@ -348,7 +354,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         w.c0 = dalloc<float>(c, B);
         w.norms = dalloc<float>(c, (size_t)B * KO);
         w.d2c = dalloc<float>(c, (size_t)B * KOT);
-        w.wc = dalloc<double>(c, (size_t)B * KOT);
+        w.lbound = dalloc<double>(c, (size_t)B * 2);
         w.minkey_c = dalloc<unsigned>(c, B);
         w.minkey_f = dalloc<unsigned>(c, B);
         w.pdf_t = dalloc<double>(c, (size_t)B * T);
@@ -405,6 +411,12 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             op.bl = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kdim);
             op.ah = dalloc<uint16_t>(c, (size_t)op.n_pad * op.kdim);
             op.al = dalloc<uint16_t>(c, (size_t)op.n_pad * op.kdim);
+            op.kn = (int)tc_kn(P);
+            op.b_pad = (B + 255) / 256 * 256;
+            op.nh = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kn);
+            op.nl = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kn);
+            op.wh = dalloc<uint16_t>(c, (size_t)op.b_pad * op.kn);
+            op.wl = dalloc<uint16_t>(c, (size_t)op.b_pad * op.kn);
             tc_prepare_projections(tb, op, st);
         }
         T2B_CUDA(cudaStreamSynchronize(st));
@@ -423,10 +435,11 @@ static void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st)
     T2B_CUDA(cudaMemsetAsync(w.counters, 0, 16 * sizeof(unsigned long long), st));
     T2B_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     cudaEventRecord(c->ev[0], st);
-    launch_prep(tb, w, st);
-    launch_norms(tb, w, st);
-    cudaEventRecord(c->ev[1], st);
     const bool tc = c->cfg.diff2_mode == T2B_DIFF2_SPLIT_BF16;
+    launch_prep(tb, w, st);
+    if (tc) tc_launch_norms(tb, w, c->tc, st);
+    else launch_norms(tb, w, st);
+    cudaEventRecord(c->ev[1], st);
     if (tc) tc_split_images(tb, w, c->tc, st);
     cudaEventRecord(c->ev[2], st);
     if (tc) tc_launch_diff2(tb, w, c->tc, st);

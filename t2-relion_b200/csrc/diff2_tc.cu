@@ -143,6 +143,7 @@ __device__ __forceinline__ unsigned f2key(float f)
 
 struct TcParams {
     int m_tiles, n_tiles, kblocks;
+    int raw;                  // 1: store the contraction itself (norm GEMM), 0: diff2 epilogue
     int KO, T, ncols;
     const float* c0;
     const float* norms;
@@ -274,13 +275,15 @@ k_diff2_tc(const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUte
                 const bool cok = col < p.ncols;
                 const int b = cok ? col / p.T : 0;
                 const int t = cok ? col - b * p.T : 0;
-                const float c0 = cok ? p.c0[b] : 0.f;
+                const float c0 = (cok && !p.raw) ? p.c0[b] : 0.f;  // raw mode has no c0 array
                 unsigned lmin = 0xffffffffu;
                 for (int r = 0; r < 32; r++) {
                     const int oc = mt * TM + q * 32 + r;
                     if (!cok || oc >= p.KO) continue;
                     float d;
-                    if (p.skip[oc]) {
+                    if (p.raw) {
+                        d = sbuf[r * EPI_LD + lane];
+                    } else if (p.skip[oc]) {
                         d = -999.f;
                     } else {
                         d = c0 + p.norms[(size_t)b * p.KO + oc] - sbuf[r * EPI_LD + lane];
@@ -353,6 +356,34 @@ __global__ void k_split_img(const float2* __restrict__ cvec, const float2* __res
     }
 }
 
+// |projection|^2 (K*O x P) -> hi/lo (m_pad x kn), zero padded
+__global__ void k_split_norm_proj(const float2* __restrict__ proj, int rows, int P, int kn,
+                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / kn;
+        const int pp = (int)(i - r * kn);
+        float v = 0.f;
+        if (r < rows && pp < P) {
+            const float2 z = proj[r * P + pp];
+            v = z.x * z.x + z.y * z.y;
+        }
+        split_bf16(v, hi[i], lo[i]);
+    }
+}
+
+// 0.5 M (scale CTF)^2 (n x P) -> hi/lo (b_pad x kn)
+__global__ void k_split_w2(const float* __restrict__ w2, int n, int P, int kn, __nv_bfloat16* __restrict__ hi,
+                           __nv_bfloat16* __restrict__ lo, long long total)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / kn;
+        const int pp = (int)(i - r * kn);
+        const float v = (r < n && pp < P) ? w2[r * P + pp] : 0.f;
+        split_bf16(v, hi[i], lo[i]);
+    }
+}
+
 using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -398,6 +429,7 @@ int sms()
 bool tc_supported() { return true; }
 
 size_t tc_kdim(int P) { return (size_t)((2 * P + TK - 1) / TK) * TK; }
+size_t tc_kn(int P) { return (size_t)((P + TK - 1) / TK) * TK; }
 
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
 {
@@ -409,7 +441,50 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
     const long long total = (long long)n / 2;
     k_split_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, op.kdim, (__nv_bfloat16*)op.bh,
                                             (__nv_bfloat16*)op.bl, total);
+    T2B_REQUIRE(op.nh && op.nl && op.kn == (int)tc_kn(tb.P), T2B_ERR_STATE, "norm operands not allocated");
+    k_split_norm_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, op.kn, (__nv_bfloat16*)op.nh,
+                                                 (__nv_bfloat16*)op.nl, (long long)op.m_pad * op.kn);
     T2B_CUDA(cudaGetLastError());
+}
+
+static void launch_gemm(const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtensorMap& b_hi,
+                        const CUtensorMap& b_lo, TcParams& p, cudaStream_t st)
+{
+    static bool attr = false;
+    if (!attr) {
+        T2B_CUDA(cudaFuncSetAttribute(k_diff2_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+        attr = true;
+    }
+    const int grid = std::min(sms(), p.m_tiles * p.n_tiles);
+    k_diff2_tc<<<grid, NTHREADS, SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, p);
+    T2B_CUDA(cudaGetLastError());
+}
+
+// N[b][oc] = sum_p w2[b][p] |P_oc[p]|^2 with the same split-BF16 tensor-core kernel
+void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st)
+{
+    const int b_pad = (w.n + TN - 1) / TN * TN;
+    T2B_REQUIRE(b_pad <= op.b_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
+    k_split_w2<<<4 * sms(), 256, 0, st>>>(w.w2, w.n, tb.P, op.kn, (__nv_bfloat16*)op.wh, (__nv_bfloat16*)op.wl,
+                                          (long long)b_pad * op.kn);
+    T2B_CUDA(cudaGetLastError());
+    const CUtensorMap mNh = make_map(op.nh, op.m_pad, op.kn, TM);
+    const CUtensorMap mNl = make_map(op.nl, op.m_pad, op.kn, TM);
+    const CUtensorMap mWh = make_map(op.wh, b_pad, op.kn, TN);
+    const CUtensorMap mWl = make_map(op.wl, b_pad, op.kn, TN);
+    TcParams p{};
+    p.m_tiles = op.m_pad / TM;
+    p.n_tiles = b_pad / TN;
+    p.kblocks = op.kn / TK;
+    p.raw = 1;
+    p.KO = tb.K * tb.O;
+    p.T = 1;
+    p.ncols = w.n;
+    p.skip = tb.skip;
+    p.d2c = w.norms;
+    p.minkey = w.minkey_c;
+    p.err = w.err;
+    launch_gemm(mNh, mNl, mWh, mWl, p, st);
 }
 
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st)
@@ -432,7 +507,8 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     const CUtensorMap mPl = make_map(op.bl, op.m_pad, op.kdim, TM);
     const CUtensorMap mIh = make_map(op.ah, n_pad, op.kdim, TN);
     const CUtensorMap mIl = make_map(op.al, n_pad, op.kdim, TN);
-    TcParams p;
+    TcParams p{};
+    p.raw = 0;
     p.m_tiles = op.m_pad / TM;
     p.n_tiles = n_pad / TN;
     p.kblocks = op.kdim / TK;
@@ -445,14 +521,7 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     p.d2c = w.d2c;
     p.minkey = w.minkey_c;
     p.err = w.err;
-    static bool attr = false;
-    if (!attr) {
-        T2B_CUDA(cudaFuncSetAttribute(k_diff2_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
-        attr = true;
-    }
-    const int grid = std::min(sms(), p.m_tiles * p.n_tiles);
-    k_diff2_tc<<<grid, NTHREADS, SMEM_BYTES, st>>>(mPh, mPl, mIh, mIl, p);
-    T2B_CUDA(cudaGetLastError());
+    launch_gemm(mPh, mPl, mIh, mIl, p, st);
 }
 
 }  // namespace t2b

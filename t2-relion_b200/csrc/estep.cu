@@ -97,18 +97,23 @@ __global__ void k_prep(Tables tb, Work w)
 }
 
 // ----------------------------------------------------------------- norms
-// N[b][oc] = sum_p w2[b][p] |P_oc[p]|^2 ; tile 64 orientations x 16 particles.
+// N[b][oc] = sum_p w2[b][p] |P_oc[p]|^2 ; tile 128 orientations x 64 particles,
+// 4 x 8 outputs per thread, 16 pixels per shared-memory stage.
 __global__ void __launch_bounds__(256) k_norms(Tables tb, Work w, const float2* __restrict__ proj, int nrows,
                                                float* __restrict__ out)
 {
-    __shared__ float Ps[32][65];
-    __shared__ float Ws[32][17];
-    const int o0 = blockIdx.x * 64, b0 = blockIdx.y * 16, P = tb.P;
-    const int to = threadIdx.x & 63, tbq = threadIdx.x >> 6;  // 4 particles per thread
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int p0 = 0; p0 < P; p0 += 32) {
-        for (int idx = threadIdx.x; idx < 64 * 32; idx += 256) {
-            const int oo = idx >> 5, pp = idx & 31;
+    __shared__ __align__(16) float Ps[16][132];
+    __shared__ __align__(16) float Ws[16][68];
+    const int o0 = blockIdx.x * 128, b0 = blockIdx.y * 64, P = tb.P;
+    const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;  // 8 particle groups x 32 orientation groups
+    float acc[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+    for (int p0 = 0; p0 < P; p0 += 16) {
+        for (int idx = threadIdx.x; idx < 128 * 16; idx += 256) {
+            const int oo = idx >> 4, pp = idx & 15;
             float v = 0.f;
             if (o0 + oo < nrows && p0 + pp < P) {
                 const float2 z = proj[(size_t)(o0 + oo) * P + p0 + pp];
@@ -116,22 +121,34 @@ __global__ void __launch_bounds__(256) k_norms(Tables tb, Work w, const float2* 
             }
             Ps[pp][oo] = v;
         }
-        for (int idx = threadIdx.x; idx < 16 * 32; idx += 256) {
-            const int bb = idx >> 5, pp = idx & 31;
+        for (int idx = threadIdx.x; idx < 64 * 16; idx += 256) {
+            const int bb = idx >> 4, pp = idx & 15;
             Ws[pp][bb] = (b0 + bb < w.n && p0 + pp < P) ? w.w2[(size_t)(b0 + bb) * P + p0 + pp] : 0.f;
         }
         __syncthreads();
-#pragma unroll 8
-        for (int pp = 0; pp < 32; pp++) {
-            const float pv = Ps[pp][to];
 #pragma unroll
-            for (int j = 0; j < 4; j++) acc[j] += pv * Ws[pp][tbq * 4 + j];
+        for (int pp = 0; pp < 16; pp++) {
+            const float4 pv = *reinterpret_cast<const float4*>(&Ps[pp][ty * 4]);
+            const float4 w0 = *reinterpret_cast<const float4*>(&Ws[pp][tx * 8]);
+            const float4 w1 = *reinterpret_cast<const float4*>(&Ws[pp][tx * 8 + 4]);
+            const float a[4] = {pv.x, pv.y, pv.z, pv.w};
+            const float c[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a[i], c[j], acc[i][j]);
         }
         __syncthreads();
     }
-    for (int j = 0; j < 4; j++) {
-        const int b = b0 + tbq * 4 + j, o = o0 + to;
-        if (b < w.n && o < nrows) out[(size_t)b * nrows + o] = acc[j];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const int bb = b0 + tx * 8 + j;
+        if (bb >= w.n) continue;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int o = o0 + ty * 4 + i;
+            if (o < nrows) out[(size_t)bb * nrows + o] = acc[i][j];
+        }
     }
 }
 
@@ -250,10 +267,13 @@ __global__ void __launch_bounds__(256, 2) k_diff2_simt(Tables tb, Work w)
 
 // ---------------------------------------------------------------- priors
 // pdf_offset of every coarse translation, normalised by its mean
-// (src/ml_optimiser.cpp:7629-7716).  One CTA per particle.
+// (src/ml_optimiser.cpp:7629-7716), and the per-particle bounds of
+// log(pdf_orientation * pdf_offset) used to skip exp() outside a diff2 window.
+// One CTA per particle.
 __global__ void k_pdf_t(Tables tb, Work w)
 {
     __shared__ double sh[32];
+    __shared__ double smin[32], smax[32];
     const int b = blockIdx.x, T = tb.T;
     const double* sc = w.scal + 8 * (size_t)b;
     double local = 0.;
@@ -268,46 +288,92 @@ __global__ void k_pdf_t(Tables tb, Work w)
         local += v;
     }
     const double mean = block_sum(local, sh) / T;
-    for (int t = threadIdx.x; t < T; t += blockDim.x)
-        if (mean > 0.) w.pdf_t[(size_t)b * T + t] /= mean;
+    double lmin = INFINITY, lmax = -INFINITY;
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+        double v = w.pdf_t[(size_t)b * T + t];
+        if (mean > 0.) v /= mean;
+        w.pdf_t[(size_t)b * T + t] = v;
+        const double lv = v > 0. ? log(v) : -INFINITY;
+        lmin = fmin(lmin, lv);
+        lmax = fmax(lmax, lv);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lmin = fmin(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+        lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) { smin[threadIdx.x >> 5] = lmin; smax[threadIdx.x >> 5] = lmax; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < (int)((blockDim.x + 31) >> 5); i++) { lmin = fmin(lmin, smin[i]); lmax = fmax(lmax, smax[i]); }
+        lmin = fmin(lmin, smin[0]);
+        lmax = fmax(lmax, smax[0]);
+        w.lbound[2 * b] = tb.lpo_min + lmin;
+        w.lbound[2 * b + 1] = tb.lpo_max + lmax;
+    }
 }
 
 // ------------------------------------------------------- weights (FP64)
-// Segment of particle b: coarse = [0, K*O*T) of d2c/wc; fine = the pair range
-// of b times R*V in d2f/wf.  Element -> (oc, t) for the priors.
+// Coarse weights are never stored: every pass recomputes
+//     w = pdf_o pdf_t exp(-(diff2 - min))      (0 if diff2 - min > 700)
+// from the FP32 diff2 array, and skips the exp() outside the diff2 window in
+// which w can fall into the range the pass looks for (bounds from the
+// per-particle extremes of log(pdf_o pdf_t)).  Fine weights are stored (the
+// weighted sums read them).
+__device__ __forceinline__ double coarse_weight(const Tables& tb, const Work& w, int b, long long il, float d, double mn)
+{
+    if (d < 0.f) return 0.;
+    const double dd = (double)d - mn;
+    if (dd > 700.) return 0.;
+    const long long oc = il / tb.T;
+    const int t = (int)(il - oc * tb.T);
+    const int k = (int)(oc / tb.O), o = (int)(oc - (long long)k * tb.O), idir = o / tb.n_psi;
+    return tb.pdf_o[k * tb.n_dir + idir] * w.pdf_t[(size_t)b * tb.T + t] * exp(-dd);
+}
+
+__device__ __forceinline__ double fine_prior(const Tables& tb, const Work& w, int b, long long i)
+{
+    const long long ih = w.pairs[i / ((long long)tb.R * tb.V)];
+    const long long oc = ih / tb.T;
+    const int t = (int)(ih - oc * tb.T);
+    const int k = (int)(oc / tb.O), o = (int)(oc - (long long)k * tb.O), idir = o / tb.n_psi;
+    return tb.pdf_o[k * tb.n_dir + idir] * w.pdf_t[(size_t)b * tb.T + t];
+}
+
+// diff2 window (lo, hi] outside which w cannot lie in [wlo, whi)
+constexpr double WIN_EPS = 1e-6;
+__device__ __forceinline__ void dwindow(double wlo, double whi, double mn, double Lmin, double Lmax, double& lo, double& hi)
+{
+    lo = (whi > 0. && whi < INFINITY && Lmin > -INFINITY) ? mn + Lmin - log(whi) - WIN_EPS : -INFINITY;
+    hi = (wlo > 0.) ? mn + Lmax - log(wlo) + WIN_EPS : INFINITY;
+}
+
+__device__ __forceinline__ double bits2d(unsigned long long u)
+{
+    return u >= 0x7ff0000000000000ull ? INFINITY : __longlong_as_double((long long)u);
+}
+
+// digit layout of the radix search over the 64-bit pattern of positive doubles
+__device__ __forceinline__ int digit_width(int shift) { return shift == 0 ? 4 : 12; }
+
 struct Seg {
-    const float* d;
-    double* wout;
-    long long beg, end;   // element range (global index into d / wout)
+    long long beg, end;   // element range (coarse: local index; fine: global index into d2f / wf)
 };
 
 __device__ __forceinline__ Seg seg_of(const Tables& tb, const Work& w, bool fine, int b)
 {
     Seg s;
     if (!fine) {
-        const long long n = (long long)tb.K * tb.O * tb.T;
-        s.d = w.d2c; s.wout = w.wc; s.beg = (long long)b * n; s.end = s.beg + n;
+        s.beg = 0;
+        s.end = (long long)tb.K * tb.O * tb.T;
     } else {
         const long long rv = (long long)tb.R * tb.V;
-        s.d = w.d2f; s.wout = w.wf; s.beg = w.pair_off[b] * rv; s.end = w.pair_off[b + 1] * rv;
+        s.beg = w.pair_off[b] * rv;
+        s.end = w.pair_off[b + 1] * rv;
     }
     return s;
 }
 
-__device__ __forceinline__ void elem_oct(const Tables& tb, const Work& w, bool fine, int b, long long i,
-                                         int& oc, int& t)
-{
-    long long ih;
-    if (!fine) ih = i - (long long)b * tb.K * tb.O * tb.T;
-    else ih = w.pairs[i / ((long long)tb.R * tb.V)];
-    oc = (int)(ih / tb.T);
-    t = (int)(ih - (long long)oc * tb.T);
-}
-
-// digit layout of the radix search over the 64-bit pattern of positive doubles
-__device__ __forceinline__ int digit_width(int shift) { return shift == 0 ? 4 : 12; }
-
-// pass 1: weights, sum, max, level-0 histogram (top 12 bits)
+// pass 1: weights (stored for the fine set only), sum, max, level-0 histogram
 __global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
 {
     extern __shared__ unsigned char smem_raw[];
@@ -320,20 +386,23 @@ __global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
     __syncthreads();
     const Seg sg = seg_of(tb, w, fine, b);
     const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
+    const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
     double lsum = 0.;
     unsigned long long lmax = 0;
     for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
          i += (long long)gridDim.x * blockDim.x) {
-        const float d = sg.d[i];
-        double wt = 0.;
-        if (d >= 0.f) {
-            int oc, t;
-            elem_oct(tb, w, fine, b, i, oc, t);
-            const int k = oc / tb.O, o = oc - k * tb.O, idir = o / tb.n_psi;
-            const double dd = (double)d - mn;
-            if (dd <= 700.) wt = tb.pdf_o[k * tb.n_dir + idir] * w.pdf_t[(size_t)b * tb.T + t] * exp(-dd);
+        const float d = dsrc[i];
+        double wt;
+        if (fine) {
+            wt = 0.;
+            if (d >= 0.f) {
+                const double dd = (double)d - mn;
+                if (dd <= 700.) wt = fine_prior(tb, w, b, i) * exp(-dd);
+            }
+            w.wf[i] = wt;
+        } else {
+            wt = coarse_weight(tb, w, b, i, d, mn);
         }
-        sg.wout[i] = wt;
         if (wt > 0.) {
             const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
             const int dg = (int)(bits >> 52);
@@ -449,6 +518,17 @@ __global__ void __launch_bounds__(1024) k_select(Work w, int fine)
     for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
 }
 
+// Weight of element i of particle b if it may lie in [wlo, whi), else 0.
+__device__ __forceinline__ double weight_in(const Tables& tb, const Work& w, bool fine, int b, long long i,
+                                            const float* dsrc, double mn, double lo, double hi)
+{
+    if (fine) return w.wf[i];
+    const float d = dsrc[i];
+    const double dd = (double)d;
+    if (d < 0.f || dd <= lo || dd > hi) return 0.;
+    return coarse_weight(tb, w, b, i, d, mn);
+}
+
 // level >= 1 histogram of the next digit among the elements under the prefix
 __global__ void __launch_bounds__(256) k_hist_level(Tables tb, Work w, int fine)
 {
@@ -464,12 +544,17 @@ __global__ void __launch_bounds__(256) k_hist_level(Tables tb, Work w, int fine)
     for (int i = threadIdx.x; i < nb; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
     __syncthreads();
     const Seg sg = seg_of(tb, w, fine, b);
+    const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
+    const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
+    const int sw = shift + width;
+    double lo, hi;
+    dwindow(bits2d(prefix << sw), bits2d((prefix + 1) << sw), mn, w.lbound[2 * b], w.lbound[2 * b + 1], lo, hi);
     for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
          i += (long long)gridDim.x * blockDim.x) {
-        const double wt = sg.wout[i];
+        const double wt = weight_in(tb, w, fine, b, i, dsrc, mn, lo, hi);
         if (!(wt > 0.)) continue;
         const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
-        if ((bits >> (shift + width)) != prefix) continue;
+        if ((bits >> sw) != prefix) continue;
         const int dg = (int)((bits >> shift) & (unsigned long long)(nb - 1));
         atomicAdd(&hc[dg], 1u);
         atomicAdd(&hs[dg], wt);
@@ -490,9 +575,13 @@ __global__ void __launch_bounds__(256) k_gather(Tables tb, Work w, int fine)
     const int shift = sel->shift;
     const unsigned long long prefix = sel->prefix;
     const Seg sg = seg_of(tb, w, fine, b);
+    const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
+    const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
+    double lo, hi;
+    dwindow(bits2d(prefix << shift), bits2d((prefix + 1) << shift), mn, w.lbound[2 * b], w.lbound[2 * b + 1], lo, hi);
     for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
          i += (long long)gridDim.x * blockDim.x) {
-        const double wt = sg.wout[i];
+        const double wt = weight_in(tb, w, fine, b, i, dsrc, mn, lo, hi);
         if (!(wt > 0.)) continue;
         const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
         if ((bits >> shift) != prefix) continue;
@@ -560,25 +649,67 @@ __global__ void __launch_bounds__(1024) k_final(Work w, int fine, int ipass)
 // ------------------------------------------------- ordered compaction
 constexpr int CHUNK = 4096;
 
+// significance predicate w >= thr of a coarse element, with the exp() only
+// inside the ambiguous diff2 window
+struct SigPred {
+    double mn, thr, acc, rej;
+    __device__ bool operator()(const Tables& tb, const Work& w, int b, long long i, float d, double* wout) const
+    {
+        if (d < 0.f) return false;
+        const double dd = (double)d;
+        if (dd - mn > 700.) return false;
+        if (dd > rej) return false;
+        if (dd <= acc && !wout) return true;
+        const double wt = coarse_weight(tb, w, b, i, d, mn);
+        if (wout) *wout = wt;
+        return wt >= thr;
+    }
+};
+
+__device__ __forceinline__ SigPred sig_pred(const Work& w, int b)
+{
+    SigPred p;
+    p.mn = (double)key2f(w.minkey_c[b]);
+    p.thr = w.sel_c[b].thr;
+    const double lt = log(p.thr);
+    p.acc = w.lbound[2 * b] > -INFINITY ? p.mn + w.lbound[2 * b] - lt - WIN_EPS : -INFINITY;
+    p.rej = p.mn + w.lbound[2 * b + 1] - lt + WIN_EPS;
+    return p;
+}
+
 __global__ void __launch_bounds__(256) k_count_sig(Tables tb, Work w)
 {
     const int b = blockIdx.y;
     const SelState* sel = &w.sel_c[b];
     const long long n = (long long)tb.K * tb.O * tb.T;
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
+    const float* dsrc = w.d2c + (size_t)b * (size_t)n;
     __shared__ int cnt;
+    const bool active = sel->phase == 2;
+    SigPred pred{};
+    double alo = 0., ahi = 0.;
+    unsigned long long maxbits = 0;
+    if (active) {
+        pred = sig_pred(w, b);
+        maxbits = sel->maxbits;
+        const double wmax = __longlong_as_double((long long)maxbits);
+        dwindow(wmax, wmax * (1. + 1e-12), pred.mn, w.lbound[2 * b], w.lbound[2 * b + 1], alo, ahi);
+    }
     for (int c = blockIdx.x; c < nch; c += gridDim.x) {
         if (threadIdx.x == 0) cnt = 0;
         __syncthreads();
         int local = 0;
-        if (sel->phase == 2) {
-            const double thr = sel->thr;
-            const unsigned long long maxbits = sel->maxbits;
-            for (long long i = (long long)c * CHUNK + threadIdx.x; i < min(n, (long long)(c + 1) * CHUNK); i += blockDim.x) {
-                const double wt = w.wc[(size_t)b * n + i];
-                if (wt >= thr) local++;
-                if ((unsigned long long)__double_as_longlong(wt) == maxbits)
-                    atomicMin((long long*)&w.sel_c[b].argmax, i);
+        if (active) {
+            const long long end = min(n, (long long)(c + 1) * CHUNK);
+            for (long long i = (long long)c * CHUNK + threadIdx.x; i < end; i += blockDim.x) {
+                const float d = dsrc[i];
+                if (pred(tb, w, b, i, d, nullptr)) local++;
+                const double dd = (double)d;
+                if (d >= 0.f && dd > alo && dd <= ahi) {
+                    const double wt = coarse_weight(tb, w, b, i, d, pred.mn);
+                    if ((unsigned long long)__double_as_longlong(wt) == maxbits)
+                        atomicMin((long long*)&w.sel_c[b].argmax, i);
+                }
             }
         }
         local = __reduce_add_sync(0xffffffffu, local);
@@ -630,45 +761,43 @@ __global__ void __launch_bounds__(1024) k_scan_pairs(Tables tb, Work w)
     }
 }
 
+// Ordered compaction of the significant coarse pairs: rounds of 256
+// consecutive elements, warp ballots and a block prefix keep index order.
 __global__ void __launch_bounds__(256) k_compact(Tables tb, Work w, int gather_final)
 {
-    __shared__ int sh[256];
+    __shared__ int wsum[8];
     const int b = blockIdx.y;
     const SelState* sel = &w.sel_c[b];
     if (sel->phase != 2 || w.status[b] != T2B_OK) return;
     const long long n = (long long)tb.K * tb.O * tb.T;
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
-    const double thr = sel->thr;
+    const float* dsrc = w.d2c + (size_t)b * (size_t)n;
+    const SigPred pred = sig_pred(w, b);
     const long long pbase = w.pair_off[b];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int c = blockIdx.x; c < nch; c += gridDim.x) {
-        const long long beg = (long long)c * CHUNK + threadIdx.x * (CHUNK / 256);
-        int local = 0;
-        for (int j = 0; j < CHUNK / 256; j++) {
-            const long long i = beg + j;
-            if (i < n && w.wc[(size_t)b * n + i] >= thr) local++;
-        }
-        sh[threadIdx.x] = local;
-        __syncthreads();
-        for (int off = 1; off < 256; off <<= 1) {
-            const int u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+        long long pos0 = pbase + w.chunk_cnt[(size_t)b * w.max_chunks + c];
+        for (int r = 0; r < CHUNK / 256; r++) {
+            const long long i = (long long)c * CHUNK + r * 256 + threadIdx.x;
+            double wt = 0.;
+            const bool f = i < n && pred(tb, w, b, i, dsrc[i], gather_final ? &wt : nullptr);
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            if (lane == 0) wsum[wid] = __popc(m);
             __syncthreads();
-            sh[threadIdx.x] += u;
-            __syncthreads();
-        }
-        long long pos = pbase + w.chunk_cnt[(size_t)b * w.max_chunks + c] + sh[threadIdx.x] - local;
-        for (int j = 0; j < CHUNK / 256; j++) {
-            const long long i = beg + j;
-            if (i < n) {
-                const double wt = w.wc[(size_t)b * n + i];
-                if (wt >= thr) {
-                    w.pairs[pos] = i;
-                    w.pair_b[pos] = b;
-                    if (gather_final) w.wf[pos] = wt;
-                    pos++;
-                }
+            int before = 0, tot = 0;
+            for (int j = 0; j < 8; j++) {
+                if (j < wid) before += wsum[j];
+                tot += wsum[j];
             }
+            const long long pos = pos0 + before + __popc(m & ((1u << lane) - 1u));
+            if (f && pos < w.pair_off[b + 1]) {
+                w.pairs[pos] = i;
+                w.pair_b[pos] = b;
+                if (gather_final) w.wf[pos] = wt;
+            }
+            pos0 += tot;
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
@@ -1114,7 +1243,7 @@ void launch_prep(const Tables& tb, const Work& w, cudaStream_t st)
 void launch_norms(const Tables& tb, const Work& w, cudaStream_t st)
 {
     const int KO = tb.K * tb.O;
-    dim3 grid((KO + 63) / 64, (w.n + 15) / 16);
+    dim3 grid((KO + 127) / 128, (w.n + 63) / 64);
     k_norms<<<grid, 256, 0, st>>>(tb, w, tb.proj_c, KO, w.norms);
     T2B_CUDA(cudaGetLastError());
 }

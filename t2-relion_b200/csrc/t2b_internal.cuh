@@ -71,6 +71,7 @@ struct Tables {
     const unsigned char* skip;// K*O: orientation not evaluated (pdf <= 0)
     const int* mresol;        // P
     double sigma2_offset, pixel_size, adaptive_fraction;
+    double lpo_min, lpo_max;  // extremes of log(pdf_o) over evaluated orientations
 };
 
 // Device views of the batch workspace.
@@ -86,7 +87,7 @@ struct Work {
     float* c0;                // n      (Xi2/2 + sum 0.5 M |X|^2)
     float* norms;             // n x K*O
     float* d2c;               // n x K*O*T
-    double* wc;               // n x K*O*T
+    double* lbound;           // n x 2: min / max of log(pdf_o pdf_t)
     unsigned* minkey_c;       // n
     unsigned* minkey_f;       // n
     double* pdf_t;            // n x T
@@ -142,11 +143,18 @@ struct TcOperands {
     void* bl;                 // lo
     void* ah;                 // N_pad x Kdim bf16 (shifted images, hi)
     void* al;
-    int m_pad, n_pad, kdim;   // padded sizes
+    void* nh;                 // K*O_pad x Kn bf16 (|projection|^2, hi)
+    void* nl;
+    void* wh;                 // B_pad x Kn bf16 (0.5 M (scale CTF)^2, hi)
+    void* wl;
+    int m_pad, n_pad, kdim;   // padded sizes of the cross-term operands
+    int kn, b_pad;            // padded sizes of the norm operands
 };
 size_t tc_kdim(int P);
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
+void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
+size_t tc_kn(int P);
 void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
 bool tc_supported();
 

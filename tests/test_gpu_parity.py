@@ -126,3 +126,21 @@ def test_reconstruct_division_matches_oracle(run, oracle):
     got = es.reconstruct_divide(0)
     ref = oracle.reconstruct_divide(data.astype(np.complex128), w.astype(np.float64), run["r"], 2)
     assert np.max(np.abs(got - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref)))
+
+
+def test_splitbf16_matches_plain_with_many_tiles_per_cta():
+    """96 particles: 72 x 11 contraction tiles, several per persistent CTA."""
+    pb = problems.build("refine_o2", n_particles=96, seed=21)
+    P = pb["parts"]
+    out = {}
+    for mode in (0, 1):
+        pb_mode = dict(pb)
+        es = problems.build("refine_o2", n_particles=96, seed=21, diff2_mode=mode)["product"]()
+        res = es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+        d2 = np.stack([es.coarse_diff2(b) for b in range(0, 96, 7)])
+        out[mode] = (res, d2)
+        es.close()
+    (r0, d0), (r1, d1) = out[0], out[1]
+    assert np.all(r0["status"] == 0) and np.all(r1["status"] == 0)
+    assert np.max(np.abs(d1.astype(np.float64) - d0) / np.abs(d0)) <= 2 * DIFF2_RTOL
+    assert np.mean(np.all(r0["pose"] == r1["pose"], axis=1)) >= 0.98
