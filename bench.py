@@ -254,6 +254,7 @@ def main():
     es = setup_context(t2b, sy, fmap, samp, mode, B, device=local)
     dev = torch.device("cuda", local)
     P = parts["fimg"].shape[1]
+    s = 2 * WORKLOAD["r_max"]
     fimg = torch.from_numpy(parts["fimg"].view(np.float32)).to(dev)
     ctf = torch.from_numpy(parts["ctf"]).to(dev)
     minv = torch.from_numpy(parts["minv"]).to(dev)
@@ -296,17 +297,12 @@ def main():
             # the library's own CUDA events bracket each stage on this stream
         ev1.record(stream)
         torch.cuda.synchronize()
-    stage = es.stage_ms()  # last step's stages
+    # kernel nodes of the captured step graph, times the timed steps
+    gpu_launches = es.launch_count() * args.steps if es.launch_count() > 0 else None
     total_ms = ev0.elapsed_time(ev1)
     if world > 1:
         torch.distributed.barrier()
     total_ms = max_over_ranks(total_ms, world)
-    # per-stage times averaged over separately synchronised steps (not part of `value`)
-    stages = []
-    for _ in range(min(3, args.steps)):
-        step()
-        stages.append(es.stage_ms())
-    stages = np.mean(np.array(stages), axis=0)
     ms_per_step = total_ms / args.steps
     value = B * args.steps * world / (total_ms / 1000.0)
 
@@ -332,6 +328,13 @@ def main():
     for _ in range(args.steps):
         e2e_step()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    # per-stage device times (CUDA events around each stage) of separately synchronised
+    # host-path steps; not part of `value`
+    stages = []
+    for _ in range(min(3, args.steps)):
+        e2e_step()
+        stages.append(es.stage_ms())
+    stages = np.mean(np.array(stages), axis=0)
     h2d = sum(v.numel() * v.element_size() for v in pin.values())
     d2h = sum(v.numel() * v.element_size() for v in hres.values())
     e2e = {"value": B * args.steps * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
@@ -350,7 +353,12 @@ def main():
         bound = "fp32_simt"
         src = "nominal"
     achieved = flops / (gemm / 1000.0) / 1e12
+    # the contraction runs over the nk window pixels inside the projection radius only
+    # (projections are zero outside); executed = what the units did
+    nk = int(sum(1 for n in range(P) if (lambda i, x: x * x + (i if i < s // 2 + 1 else i - s) ** 2)(n // (s // 2 + 1), n % (s // 2 + 1)) <= (s // 2) ** 2))
+    executed = (12.0 if mode == t2b.DIFF2_SPLIT_BF16 else 4.0) * K * O * T * nk * B / (gemm / 1000.0) / 1e12
     roof = {"bound": bound, "kernel": "k_diff2_tc" if mode else "k_diff2_simt", "achieved": achieved,
+            "executed_tflops": executed, "contraction_pixels": nk,
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src,
             "traffic": None, "flops_per_launch": flops}
     line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
@@ -359,7 +367,7 @@ def main():
             "config": {"workload": WORKLOAD["name"], "particles_per_step": B, "diff2": args.mode,
                        "orientations": O, "translations": T, "pixels": P,
                        "l2": "working set > L2 (bf16 hi/lo projection operands 0.97 GB per step)"},
-            "e2e": e2e, "gpu_launches": None, "clocks": clk.summary(), "roofline": roof,
+            "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk.summary(), "roofline": roof,
             "stage_ms": {n: float(v) for n, v in zip(
                 ["prep_norms", "operand_split", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
                  "wsum_bp"], stages)},

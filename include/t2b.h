@@ -90,7 +90,8 @@ typedef struct t2b_config {
     int maximum_significants;  /* <= 0: off (only 0/-1 supported)                     */
     int diff2_mode;            /* T2B_DIFF2_*                                         */
     int max_batch;             /* particles per t2b_estep_* call                      */
-    int _pad;
+    int use_graph;             /* 1: t2b_estep_batch_device captures the batch into a CUDA
+                                  graph on first use and replays it                     */
     const double* eul_coarse;  /* n_dir*n_psi x 9, Euler matrices (Euler_angles2matrix) */
     const double* eul_fine;    /* n_dir*n_psi*nover_rot x 9, or NULL                    */
     const double* trans_px;    /* n_trans x 2: coarse shifts in pixels                  */
@@ -191,10 +192,15 @@ int t2b_project(t2b_ctx* ctx, int iclass, const double* eulers, int n, int curre
 int t2b_debug_coarse_diff2(t2b_ctx* ctx, int b, float* out);
 int t2b_debug_fine(t2b_ctx* ctx, int b, long long* pairs, float* diff2, long long cap, long long* count);
 
+/* Kernel launches of the last device batch (the kernel nodes of its CUDA
+ * graph); -1 when the last batch did not run as a graph. */
+int t2b_last_launch_count(t2b_ctx* ctx, int* kernels);
+
 /* Device time of the stages of the last batch, in ms (CUDA events on the
  * stream the stages ran on): [0] prep + norms, [1] tensor-core operand split,
  * [2] coarse diff2 contraction, [3] coarse weights + significance + compaction,
- * [4] fine pass, [5] fine weights, [6] weighted sums + backprojection.  n <= 7. */
+ * [4] fine pass, [5] fine weights, [6] weighted sums + backprojection.  n <= 7.
+ * A batch that ran as a CUDA graph reports -1 for every stage. */
 int t2b_last_stage_ms(t2b_ctx* ctx, float* ms, int n);
 
 /* Host sampling (HealpixSampling, src/healpix_sampling.cpp:534-640,

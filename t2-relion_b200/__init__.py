@@ -36,7 +36,7 @@ ABI_SYMBOLS = (
     "t2b_backprojector_get", "t2b_backprojector_device_ptrs", "t2b_configure",
     "t2b_estep_batch_host", "t2b_estep_batch_device", "t2b_reconstruct_divide",
     "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_last_stage_ms",
-    "t2b_sampling", "t2b_reconstruct_divide_noalloc",
+    "t2b_sampling", "t2b_reconstruct_divide_noalloc", "t2b_last_launch_count",
 )
 
 
@@ -66,7 +66,7 @@ class Config(ctypes.Structure):
         ("n_trans", ctypes.c_int), ("adaptive_oversampling", ctypes.c_int),
         ("nover_rot", ctypes.c_int), ("nover_trans", ctypes.c_int),
         ("maximum_significants", ctypes.c_int), ("diff2_mode", ctypes.c_int),
-        ("max_batch", ctypes.c_int), ("_pad", ctypes.c_int),
+        ("max_batch", ctypes.c_int), ("use_graph", ctypes.c_int),
         ("eul_coarse", _p), ("eul_fine", _p), ("trans_px", _p), ("trans_px_fine", _p),
         ("trans_prior", _p), ("pdf_direction", _p), ("pdf_class", _p), ("mresol", _p),
         ("sigma2_offset", ctypes.c_double), ("pixel_size", ctypes.c_double),
@@ -107,6 +107,7 @@ def _setup_prototypes():
     lib.t2b_debug_coarse_diff2.argtypes = [v, i, v]
     lib.t2b_debug_fine.argtypes = [v, i, v, v, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.t2b_last_stage_ms.argtypes = [v, v, i]
+    lib.t2b_last_launch_count.argtypes = [v, ctypes.POINTER(i)]
     lib.t2b_sampling.argtypes = [i, i, ctypes.c_double, i, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double] + [ctypes.POINTER(i)] * 5 + [v] * 6
 
@@ -228,7 +229,7 @@ class EStep:
     def configure(self, *, ori_size, current_size, ref_dim, nr_classes, samp, pdf_direction,
                   pdf_class, sigma2_offset, pixel_size, adaptive_fraction=0.999,
                   adaptive_oversampling=0, diff2_mode=DIFF2_PLAIN_FP32, max_batch=64,
-                  fine_capacity=0, maximum_significants=-1):
+                  fine_capacity=0, maximum_significants=-1, use_graph=1):
         arrays = dict(
             eul_coarse=np.ascontiguousarray(samp["eul_coarse"], np.float64),
             eul_fine=np.ascontiguousarray(samp["eul_fine"], np.float64),
@@ -245,7 +246,7 @@ class EStep:
         c.nover_rot = samp["nover_rot"] if adaptive_oversampling else 1
         c.nover_trans = samp["nover_trans"] if adaptive_oversampling else 1
         c.maximum_significants = maximum_significants
-        c.diff2_mode, c.max_batch = diff2_mode, max_batch
+        c.diff2_mode, c.max_batch, c.use_graph = diff2_mode, max_batch, use_graph
         for k, a in arrays.items():
             setattr(c, k, _ptr(a))
         c.sigma2_offset, c.pixel_size, c.adaptive_fraction = sigma2_offset, pixel_size, adaptive_fraction
@@ -290,6 +291,11 @@ class EStep:
         r = Result(*[result_ptrs[name] for name, _ in Result._fields_])
         _check(lib.t2b_estep_batch_device(self._h, ctypes.byref(b), ctypes.byref(r),
                                           ctypes.c_void_p(stream)))
+
+    def launch_count(self):
+        k = ctypes.c_int()
+        _check(lib.t2b_last_launch_count(self._h, ctypes.byref(k)))
+        return k.value
 
     def stage_ms(self):
         ms = np.zeros(7, np.float32)

@@ -8,6 +8,7 @@
 // synchronisation between the coarse pass and the backprojection.
 #include "t2b_internal.cuh"
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -51,6 +52,11 @@ static T* dalloc(t2b_ctx* c, size_t n)
 
 static void free_allocs(t2b_ctx* c)
 {
+    if (c->gexec) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+        c->gkey.clear();
+    }
     for (void* p : c->allocs) cudaFree(p);
     c->allocs.clear();
     c->configured = false;
@@ -270,6 +276,8 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         DeviceGuard g(c->device);
         T2B_CUDA(cudaStreamSynchronize(c->stream));
         free_allocs(c);
+        estep_init_attributes();
+        if (f.diff2_mode == T2B_DIFF2_SPLIT_BF16) tc_init_attributes();
         c->cfg = f;
         const int s = f.current_size, xh = s / 2 + 1, P = s * xh;
         const int K = f.nr_classes, O = f.n_dir * f.n_psi, T = f.n_trans, B = f.max_batch;
@@ -307,8 +315,26 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         tb.lpo_min = lpo_min;
         tb.lpo_max = lpo_max;
         tb.pdf_o = (const double*)up(pdf_o.data(), pdf_o.size() * sizeof(double));
+        {
+            std::vector<double> poc((size_t)K * O);
+            for (int k = 0; k < K; k++)
+                for (int o = 0; o < O; o++) poc[(size_t)k * O + o] = pdf_o[(size_t)k * f.n_dir + o / f.n_psi];
+            tb.pdf_oc = (const double*)up(poc.data(), poc.size() * sizeof(double));
+        }
         tb.skip = (const unsigned char*)up(skip.data(), skip.size());
         tb.mresol = (const int*)up(f.mresol, (size_t)P * sizeof(int));
+        {
+            // pixels inside the largest projection radius of all classes
+            int rr = 0;
+            for (int k = 0; k < K; k++) rr = std::max(rr, std::min(s / 2, c->mvol[k].r_max));
+            std::vector<int> kp;
+            for (int n = 0; n < P; n++) {
+                const int i = n / xh, x = n - i * xh, y = (i < xh) ? i : i - s;
+                if (x * x + y * y <= rr * rr) kp.push_back(n);
+            }
+            tb.nk = (int)kp.size();
+            tb.kpix = (const int*)up(kp.data(), kp.size() * sizeof(int));
+        }
         tb.eul_c = (const double*)up(f.eul_coarse, (size_t)O * 9 * sizeof(double));
         tb.trans_c = (const double*)up(f.trans_px, (size_t)T * 2 * sizeof(double));
         tb.trans_prior = (const double*)up(f.trans_prior, (size_t)T * 2 * sizeof(double));
@@ -365,6 +391,10 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         w.hist_cnt = dalloc<unsigned>(c, (size_t)B * HIST_BINS);
         w.hist_sum = dalloc<double>(c, (size_t)B * HIST_BINS);
         w.cand = dalloc<double>(c, (size_t)B * CAND_CAP);
+        w.fcand_w = dalloc<double>(c, (size_t)B * FAST_CAP);
+        w.fcand_i = dalloc<long long>(c, (size_t)B * FAST_CAP);
+        w.flist_w = dalloc<double>(c, (size_t)B * FAST_CAP);
+        w.flist_i = dalloc<long long>(c, (size_t)B * FAST_CAP);
         const size_t fine_cap = f.fine_capacity ? f.fine_capacity : (size_t)32 << 20;
         w.pair_cap = std::max<long long>((long long)(fine_cap / (size_t)(R * V)), (long long)B * 64);
         w.pairs = dalloc<long long>(c, w.pair_cap);
@@ -404,19 +434,20 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         c->tc = TcOperands{};
         if (f.diff2_mode == T2B_DIFF2_SPLIT_BF16) {
             TcOperands& op = c->tc;
-            op.kdim = (int)tc_kdim(P);
+            op.kdim = (int)tc_kdim(tb.nk);
             op.m_pad = (int)((KO + 127) / 128 * 128);
             op.n_pad = (B * T + 255) / 256 * 256;
             op.bh = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kdim);
             op.bl = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kdim);
             op.ah = dalloc<uint16_t>(c, (size_t)op.n_pad * op.kdim);
             op.al = dalloc<uint16_t>(c, (size_t)op.n_pad * op.kdim);
-            op.kn = (int)tc_kn(P);
+            op.kn = (int)tc_kn(tb.nk);
             op.b_pad = (B + 255) / 256 * 256;
             op.nh = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kn);
             op.nl = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kn);
             op.wh = dalloc<uint16_t>(c, (size_t)op.b_pad * op.kn);
             op.wl = dalloc<uint16_t>(c, (size_t)op.b_pad * op.kn);
+            op.maps = dalloc<uint8_t>(c, 8 * 128);
             tc_prepare_projections(tb, op, st);
         }
         T2B_CUDA(cudaStreamSynchronize(st));
@@ -428,31 +459,32 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
 
 namespace t2b {
 
-// Enqueue the whole E-step of the batch in `w` on `st`.
-static void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st)
+// Enqueue the whole E-step of the batch in `w` on `st`.  Stage events are
+// recorded only outside stream capture (a captured batch is timed as a whole).
+static void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events = true)
 {
     const Tables& tb = c->tb;
     T2B_CUDA(cudaMemsetAsync(w.counters, 0, 16 * sizeof(unsigned long long), st));
     T2B_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
-    cudaEventRecord(c->ev[0], st);
+    if (stage_events) cudaEventRecord(c->ev[0], st);
     const bool tc = c->cfg.diff2_mode == T2B_DIFF2_SPLIT_BF16;
     launch_prep(tb, w, st);
     if (tc) tc_launch_norms(tb, w, c->tc, st);
     else launch_norms(tb, w, st);
-    cudaEventRecord(c->ev[1], st);
+    if (stage_events) cudaEventRecord(c->ev[1], st);
     if (tc) tc_split_images(tb, w, c->tc, st);
-    cudaEventRecord(c->ev[2], st);
+    if (stage_events) cudaEventRecord(c->ev[2], st);
     if (tc) tc_launch_diff2(tb, w, c->tc, st);
     else launch_diff2_simt(tb, w, st);
-    cudaEventRecord(c->ev[3], st);
+    if (stage_events) cudaEventRecord(c->ev[3], st);
     launch_weights_coarse(tb, w, c->cfg.maximum_significants, st);
-    cudaEventRecord(c->ev[4], st);
+    if (stage_events) cudaEventRecord(c->ev[4], st);
     if (tb.ovs) launch_fine(tb, w, st);
-    cudaEventRecord(c->ev[5], st);
+    if (stage_events) cudaEventRecord(c->ev[5], st);
     if (tb.ovs) launch_weights_fine(tb, w, st);
-    cudaEventRecord(c->ev[6], st);
+    if (stage_events) cudaEventRecord(c->ev[6], st);
     launch_wsum_bp(tb, w, c->gvol[0], c->gd_table, c->gw_table, st);
-    cudaEventRecord(c->ev[7], st);
+    if (stage_events) cudaEventRecord(c->ev[7], st);
 }
 
 static void check_batch(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
@@ -465,7 +497,12 @@ static void check_batch(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
 
 static void collect_stage_ms(t2b_ctx* c)
 {
-    for (int i = 0; i < 7; i++) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+    for (int i = 0; i < 7; i++) {
+        if (c->last_kernels >= 0 || cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]) != cudaSuccess) {
+            cudaGetLastError();  // do not leave the failure as the runtime's last error
+            c->stage_ms[i] = -1.f;
+        }
+    }
 }
 
 }  // namespace t2b
@@ -510,6 +547,7 @@ int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
         d2h(r->wsum_pdf_dir, w.r_pdf_dir, (size_t)n * K * c->tb.n_dir * sizeof(double));
         d2h(r->status, w.status, n * sizeof(int));
         T2B_CUDA(cudaStreamSynchronize(st));
+        c->last_kernels = -1;
         collect_stage_ms(c);
         c->last_n = n;
     });
@@ -539,8 +577,56 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
         w.r_norm = r->wsum_norm; w.r_sumw = r->sumw; w.r_sig_off = r->wsum_sigma2_offset;
         w.r_sigma2 = r->wsum_sigma2; w.r_pdf_class = r->wsum_pdf_class; w.r_pdf_dir = r->wsum_pdf_dir;
         w.status = r->status;
-        enqueue_estep(c, w, st);
+        if (c->cfg.use_graph) {
+            const std::vector<const void*> key = {(const void*)(intptr_t)b->n, b->fimg, b->fimg_nomask, b->ctf,
+                                                  b->minvsigma2, b->scalars, r->min_diff2, r->sum_weight, r->sig_weight,
+                                                  r->coarse_sum_weight, r->coarse_sig_weight, r->nr_sign,
+                                                  r->n_coarse_sig, r->pmax, r->pose, r->wsum_norm, r->sumw,
+                                                  r->wsum_sigma2_offset, r->wsum_sigma2, r->wsum_pdf_class,
+                                                  r->wsum_pdf_dir, r->status, (const void*)st};
+            if (!c->gexec || key != c->gkey) {
+                if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+                cudaGraph_t graph = nullptr;
+                T2B_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                try {
+                    enqueue_estep(c, w, st, false);
+                } catch (...) {
+                    cudaStreamEndCapture(st, &graph);
+                    if (graph) cudaGraphDestroy(graph);
+                    throw;
+                }
+                T2B_CUDA(cudaStreamEndCapture(st, &graph));
+                size_t nn = 0;
+                T2B_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
+                std::vector<cudaGraphNode_t> nodes(nn);
+                T2B_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
+                int kn = 0;
+                for (auto nd : nodes) {
+                    cudaGraphNodeType ty;
+                    T2B_CUDA(cudaGraphNodeGetType(nd, &ty));
+                    if (ty == cudaGraphNodeTypeKernel) kn++;
+                }
+                const cudaError_t ie = cudaGraphInstantiate(&c->gexec, graph, 0);
+                cudaGraphDestroy(graph);
+                T2B_CUDA(ie);
+                c->gkey = key;
+                c->graph_kernels = kn;
+            }
+            T2B_CUDA(cudaGraphLaunch(c->gexec, st));
+            c->last_kernels = c->graph_kernels;
+        } else {
+            enqueue_estep(c, w, st);
+            c->last_kernels = -1;
+        }
         c->last_n = b->n;
+    });
+}
+
+int t2b_last_launch_count(t2b_ctx* c, int* kernels)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && kernels, T2B_ERR_ARG, "bad arguments");
+        *kernels = c->last_kernels;
     });
 }
 

@@ -153,10 +153,16 @@ struct TcParams {
     int* err;
 };
 
+// maps: device array of tensor-map descriptors (encoded once per configuration);
+// the A (orientation) operand uses maps[ia], maps[ia+1] (hi, lo), the B operand
+// maps[ib], maps[ib+1].
 __global__ void __launch_bounds__(NTHREADS, 1)
-k_diff2_tc(const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUtensorMap mPl,
-           const __grid_constant__ CUtensorMap mIh, const __grid_constant__ CUtensorMap mIl, TcParams p)
+k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
 {
+    const CUtensorMap* mPh = maps + ia;
+    const CUtensorMap* mPl = maps + ia + 1;
+    const CUtensorMap* mIh = maps + ib;
+    const CUtensorMap* mIl = maps + ib + 1;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], tfull_bar[2], tempty_bar[2], drain_bar;
     __shared__ uint32_t tmem_base_slot;
@@ -188,6 +194,11 @@ k_diff2_tc(const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUte
 
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer
+        const CUtensorMap* ms[4] = {mPh, mPl, mIh, mIl};
+        for (int j = 0; j < 4; j++) {
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(ms[j]) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(ms[j]) : "memory");
+        }
         int it = 0;
         int issued[STAGES] = {0, 0};
         uint32_t last_par[STAGES] = {0, 0};
@@ -199,10 +210,10 @@ k_diff2_tc(const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUte
                 if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
                 uint8_t* st = gbase + s * STAGE_BYTES;
                 mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-                tma_load(st, &mPh, &full_bar[s], kb * TK, mt * TM);
-                tma_load(st + A_BYTES, &mPl, &full_bar[s], kb * TK, mt * TM);
-                tma_load(st + 2 * A_BYTES, &mIh, &full_bar[s], kb * TK, nt * TN);
-                tma_load(st + 2 * A_BYTES + B_BYTES, &mIl, &full_bar[s], kb * TK, nt * TN);
+                tma_load(st, mPh, &full_bar[s], kb * TK, mt * TM);
+                tma_load(st + A_BYTES, mPl, &full_bar[s], kb * TK, mt * TM);
+                tma_load(st + 2 * A_BYTES, mIh, &full_bar[s], kb * TK, nt * TN);
+                tma_load(st + 2 * A_BYTES + B_BYTES, mIl, &full_bar[s], kb * TK, nt * TN);
                 issued[s] = 1;
                 last_par[s] = ph;
             }
@@ -318,14 +329,14 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
 }
 
 // projections (K*O x P complex) -> Ph/Pl (m_pad x kdim bf16), zero padded
-__global__ void k_split_proj(const float2* __restrict__ proj, int rows, int P, int kdim,
-                             __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
+__global__ void k_split_proj(const float2* __restrict__ proj, int rows, int P, const int* __restrict__ kpix, int nk,
+                             int kdim, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
         const long long r = i / (kdim / 2);
-        const int pp = (int)(i - r * (kdim / 2));
+        const int kk = (int)(i - r * (kdim / 2));
         float2 v = make_float2(0.f, 0.f);
-        if (r < rows && pp < P) v = proj[r * P + pp];
+        if (r < rows && kk < nk) v = proj[r * P + kpix[kk]];
         __nv_bfloat16 h0, l0, h1, l1;
         split_bf16(v.x, h0, l0);
         split_bf16(v.y, h1, l1);
@@ -336,13 +347,15 @@ __global__ void k_split_proj(const float2* __restrict__ proj, int rows, int P, i
 
 // shifted, CTF- and sigma-weighted images: column b*T+t, value cvec_b[p] * ab_t[p]
 __global__ void k_split_img(const float2* __restrict__ cvec, const float2* __restrict__ ab, int ncols, int T, int P,
-                            int kdim, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
+                            const int* __restrict__ kpix, int nk, int kdim, __nv_bfloat16* __restrict__ hi,
+                            __nv_bfloat16* __restrict__ lo, long long total)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
         const long long col = i / (kdim / 2);
-        const int pp = (int)(i - col * (kdim / 2));
+        const int kk = (int)(i - col * (kdim / 2));
         float2 v = make_float2(0.f, 0.f);
-        if (col < ncols && pp < P) {
+        if (col < ncols && kk < nk) {
+            const int pp = kpix[kk];
             const int b = (int)(col / T), t = (int)(col - (long long)b * T);
             const float2 c = cvec[(size_t)b * P + pp];
             const float2 a = ab[(size_t)t * P + pp];
@@ -357,15 +370,16 @@ __global__ void k_split_img(const float2* __restrict__ cvec, const float2* __res
 }
 
 // |projection|^2 (K*O x P) -> hi/lo (m_pad x kn), zero padded
-__global__ void k_split_norm_proj(const float2* __restrict__ proj, int rows, int P, int kn,
-                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
+__global__ void k_split_norm_proj(const float2* __restrict__ proj, int rows, int P, const int* __restrict__ kpix,
+                                  int nk, int kn, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
+                                  long long total)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
         const long long r = i / kn;
-        const int pp = (int)(i - r * kn);
+        const int kk = (int)(i - r * kn);
         float v = 0.f;
-        if (r < rows && pp < P) {
-            const float2 z = proj[r * P + pp];
+        if (r < rows && kk < nk) {
+            const float2 z = proj[r * P + kpix[kk]];
             v = z.x * z.x + z.y * z.y;
         }
         split_bf16(v, hi[i], lo[i]);
@@ -373,13 +387,13 @@ __global__ void k_split_norm_proj(const float2* __restrict__ proj, int rows, int
 }
 
 // 0.5 M (scale CTF)^2 (n x P) -> hi/lo (b_pad x kn)
-__global__ void k_split_w2(const float* __restrict__ w2, int n, int P, int kn, __nv_bfloat16* __restrict__ hi,
-                           __nv_bfloat16* __restrict__ lo, long long total)
+__global__ void k_split_w2(const float* __restrict__ w2, int n, int P, const int* __restrict__ kpix, int nk, int kn,
+                           __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
         const long long r = i / kn;
-        const int pp = (int)(i - r * kn);
-        const float v = (r < n && pp < P) ? w2[r * P + pp] : 0.f;
+        const int kk = (int)(i - r * kn);
+        const float v = (r < n && kk < nk) ? w2[r * P + kpix[kk]] : 0.f;
         split_bf16(v, hi[i], lo[i]);
     }
 }
@@ -428,35 +442,52 @@ int sms()
 
 bool tc_supported() { return true; }
 
-size_t tc_kdim(int P) { return (size_t)((2 * P + TK - 1) / TK) * TK; }
-size_t tc_kn(int P) { return (size_t)((P + TK - 1) / TK) * TK; }
+size_t tc_kdim(int nk) { return (size_t)((2 * nk + TK - 1) / TK) * TK; }
+size_t tc_kn(int nk) { return (size_t)((nk + TK - 1) / TK) * TK; }
+
+// descriptor slots in op.maps
+enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL, MAP_COUNT };
 
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
 {
+    T2B_REQUIRE(op.maps, T2B_ERR_STATE, "tensor-map buffer not allocated");
+    CUtensorMap h[MAP_COUNT];
+    h[MAP_PH] = make_map(op.bh, op.m_pad, op.kdim, TM);
+    h[MAP_PL] = make_map(op.bl, op.m_pad, op.kdim, TM);
+    h[MAP_IH] = make_map(op.ah, op.n_pad, op.kdim, TN);
+    h[MAP_IL] = make_map(op.al, op.n_pad, op.kdim, TN);
+    h[MAP_NH] = make_map(op.nh, op.m_pad, op.kn, TM);
+    h[MAP_NL] = make_map(op.nl, op.m_pad, op.kn, TM);
+    h[MAP_WH] = make_map(op.wh, op.b_pad, op.kn, TN);
+    h[MAP_WL] = make_map(op.wl, op.b_pad, op.kn, TN);
+    T2B_CUDA(cudaStreamSynchronize(st));
+    T2B_CUDA(cudaMemcpy(op.maps, h, sizeof(h), cudaMemcpyHostToDevice));
     const int rows = tb.K * tb.O;
-    op.m_pad = (rows + TM - 1) / TM * TM;
-    op.kdim = (int)tc_kdim(tb.P);
+    // sizes were fixed when the operand buffers were allocated
+    T2B_REQUIRE(op.m_pad == (rows + TM - 1) / TM * TM && op.kdim == (int)tc_kdim(tb.nk), T2B_ERR_STATE,
+                "tensor-core operand sizes do not match their allocation");
     const size_t n = (size_t)op.m_pad * op.kdim;
     T2B_REQUIRE(op.bh && op.bl, T2B_ERR_STATE, "tensor-core operands not allocated");
     const long long total = (long long)n / 2;
-    k_split_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, op.kdim, (__nv_bfloat16*)op.bh,
+    k_split_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, tb.kpix, tb.nk, op.kdim, (__nv_bfloat16*)op.bh,
                                             (__nv_bfloat16*)op.bl, total);
-    T2B_REQUIRE(op.nh && op.nl && op.kn == (int)tc_kn(tb.P), T2B_ERR_STATE, "norm operands not allocated");
-    k_split_norm_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, op.kn, (__nv_bfloat16*)op.nh,
+    T2B_REQUIRE(op.nh && op.nl && op.kn == (int)tc_kn(tb.nk), T2B_ERR_STATE, "norm operands not allocated");
+    k_split_norm_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, tb.kpix, tb.nk, op.kn, (__nv_bfloat16*)op.nh,
                                                  (__nv_bfloat16*)op.nl, (long long)op.m_pad * op.kn);
     T2B_CUDA(cudaGetLastError());
 }
 
-static void launch_gemm(const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtensorMap& b_hi,
-                        const CUtensorMap& b_lo, TcParams& p, cudaStream_t st)
+void tc_init_attributes()
 {
-    static bool attr = false;
-    if (!attr) {
-        T2B_CUDA(cudaFuncSetAttribute(k_diff2_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
-        attr = true;
-    }
+    T2B_CUDA(cudaFuncSetAttribute(k_diff2_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+    (void)encoder();
+    (void)sms();
+}
+
+static void launch_gemm(const TcOperands& op, int ia, int ib, TcParams& p, cudaStream_t st)
+{
     const int grid = std::min(sms(), p.m_tiles * p.n_tiles);
-    k_diff2_tc<<<grid, NTHREADS, SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, p);
+    k_diff2_tc<<<grid, NTHREADS, SMEM_BYTES, st>>>(static_cast<const CUtensorMap*>(op.maps), ia, ib, p);
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -465,13 +496,9 @@ void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream
 {
     const int b_pad = (w.n + TN - 1) / TN * TN;
     T2B_REQUIRE(b_pad <= op.b_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
-    k_split_w2<<<4 * sms(), 256, 0, st>>>(w.w2, w.n, tb.P, op.kn, (__nv_bfloat16*)op.wh, (__nv_bfloat16*)op.wl,
+    k_split_w2<<<4 * sms(), 256, 0, st>>>(w.w2, w.n, tb.P, tb.kpix, tb.nk, op.kn, (__nv_bfloat16*)op.wh, (__nv_bfloat16*)op.wl,
                                           (long long)b_pad * op.kn);
     T2B_CUDA(cudaGetLastError());
-    const CUtensorMap mNh = make_map(op.nh, op.m_pad, op.kn, TM);
-    const CUtensorMap mNl = make_map(op.nl, op.m_pad, op.kn, TM);
-    const CUtensorMap mWh = make_map(op.wh, b_pad, op.kn, TN);
-    const CUtensorMap mWl = make_map(op.wl, b_pad, op.kn, TN);
     TcParams p{};
     p.m_tiles = op.m_pad / TM;
     p.n_tiles = b_pad / TN;
@@ -484,7 +511,7 @@ void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     p.d2c = w.norms;
     p.minkey = w.minkey_c;
     p.err = w.err;
-    launch_gemm(mNh, mNl, mWh, mWl, p, st);
+    launch_gemm(op, MAP_NH, MAP_WH, p, st);
 }
 
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st)
@@ -493,7 +520,7 @@ void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     const int n_pad = (ncols + TN - 1) / TN * TN;
     T2B_REQUIRE(n_pad <= op.n_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
     const long long total = (long long)n_pad * op.kdim / 2;
-    k_split_img<<<4 * sms(), 256, 0, st>>>(w.cvec, tb.ab_c, ncols, tb.T, tb.P, op.kdim, (__nv_bfloat16*)op.ah,
+    k_split_img<<<4 * sms(), 256, 0, st>>>(w.cvec, tb.ab_c, ncols, tb.T, tb.P, tb.kpix, tb.nk, op.kdim, (__nv_bfloat16*)op.ah,
                                            (__nv_bfloat16*)op.al, total);
     T2B_CUDA(cudaGetLastError());
 }
@@ -503,10 +530,6 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     const int ncols = w.n * tb.T;
     const int n_pad = (ncols + TN - 1) / TN * TN;
     T2B_REQUIRE(n_pad <= op.n_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
-    const CUtensorMap mPh = make_map(op.bh, op.m_pad, op.kdim, TM);
-    const CUtensorMap mPl = make_map(op.bl, op.m_pad, op.kdim, TM);
-    const CUtensorMap mIh = make_map(op.ah, n_pad, op.kdim, TN);
-    const CUtensorMap mIl = make_map(op.al, n_pad, op.kdim, TN);
     TcParams p{};
     p.raw = 0;
     p.m_tiles = op.m_pad / TM;
@@ -521,7 +544,7 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     p.d2c = w.d2c;
     p.minkey = w.minkey_c;
     p.err = w.err;
-    launch_gemm(mPh, mPl, mIh, mIl, p, st);
+    launch_gemm(op, MAP_PH, MAP_IH, p, st);
 }
 
 }  // namespace t2b

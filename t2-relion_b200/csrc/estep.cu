@@ -111,19 +111,20 @@ __global__ void __launch_bounds__(256) k_norms(Tables tb, Work w, const float2* 
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
-    for (int p0 = 0; p0 < P; p0 += 16) {
+    const int nk = tb.nk;
+    for (int p0 = 0; p0 < nk; p0 += 16) {
         for (int idx = threadIdx.x; idx < 128 * 16; idx += 256) {
             const int oo = idx >> 4, pp = idx & 15;
             float v = 0.f;
-            if (o0 + oo < nrows && p0 + pp < P) {
-                const float2 z = proj[(size_t)(o0 + oo) * P + p0 + pp];
+            if (o0 + oo < nrows && p0 + pp < nk) {
+                const float2 z = proj[(size_t)(o0 + oo) * P + tb.kpix[p0 + pp]];
                 v = z.x * z.x + z.y * z.y;
             }
             Ps[pp][oo] = v;
         }
         for (int idx = threadIdx.x; idx < 64 * 16; idx += 256) {
             const int bb = idx >> 4, pp = idx & 15;
-            Ws[pp][bb] = (b0 + bb < w.n && p0 + pp < P) ? w.w2[(size_t)(b0 + bb) * P + p0 + pp] : 0.f;
+            Ws[pp][bb] = (b0 + bb < w.n && p0 + pp < nk) ? w.w2[(size_t)(b0 + bb) * P + tb.kpix[p0 + pp]] : 0.f;
         }
         __syncthreads();
 #pragma unroll
@@ -179,13 +180,15 @@ __global__ void __launch_bounds__(256, 2) k_diff2_simt(Tables tb, Work w)
         la_t[j] = col < ncols ? col - (col / T) * T : 0;
     }
     float2 rb[4], ra[4];
+    const int nk = tb.nk;
     auto gload = [&](int p0) {
-        const int p = p0 + lp;
+        const bool in = p0 + lp < nk;
+        const int p = in ? tb.kpix[p0 + lp] : 0;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int row = m0 + lrow + 32 * j;
-            rb[j] = (row < KO && p < P) ? tb.proj_c[(size_t)row * P + p] : make_float2(0.f, 0.f);
-            if (la_b[j] >= 0 && p < P) {
+            rb[j] = (row < KO && in) ? tb.proj_c[(size_t)row * P + p] : make_float2(0.f, 0.f);
+            if (la_b[j] >= 0 && in) {
                 const float2 c = w.cvec[(size_t)la_b[j] * P + p];
                 const float2 ab = tb.ab_c[(size_t)la_t[j] * P + p];
                 ra[j] = make_float2(c.x * ab.x - c.y * ab.y, c.x * ab.y + c.y * ab.x);
@@ -214,8 +217,8 @@ __global__ void __launch_bounds__(256, 2) k_diff2_simt(Tables tb, Work w)
     sstore(0);
     __syncthreads();
     int buf = 0;
-    for (int p0 = 0; p0 < P; p0 += SB_KP) {
-        const bool more = p0 + SB_KP < P;
+    for (int p0 = 0; p0 < nk; p0 += SB_KP) {
+        const bool more = p0 + SB_KP < nk;
         if (more) gload(p0 + SB_KP);
 #pragma unroll
         for (int k = 0; k < SB_K; k++) {
@@ -319,16 +322,31 @@ __global__ void k_pdf_t(Tables tb, Work w)
 // which w can fall into the range the pass looks for (bounds from the
 // per-particle extremes of log(pdf_o pdf_t)).  Fine weights are stored (the
 // weighted sums read them).
-__device__ __forceinline__ double coarse_weight(const Tables& tb, const Work& w, int b, long long il, float d, double mn)
+__device__ __forceinline__ double coarse_weight_ot(const Tables& tb, const Work& w, int b, long long oc, int t, float d,
+                                                   double mn)
 {
     if (d < 0.f) return 0.;
     const double dd = (double)d - mn;
     if (dd > 700.) return 0.;
-    const long long oc = il / tb.T;
-    const int t = (int)(il - oc * tb.T);
-    const int k = (int)(oc / tb.O), o = (int)(oc - (long long)k * tb.O), idir = o / tb.n_psi;
-    return tb.pdf_o[k * tb.n_dir + idir] * w.pdf_t[(size_t)b * tb.T + t] * exp(-dd);
+    return tb.pdf_oc[oc] * w.pdf_t[(size_t)b * tb.T + t] * exp(-dd);
 }
+
+__device__ __forceinline__ double coarse_weight(const Tables& tb, const Work& w, int b, long long il, float d, double mn)
+{
+    const long long oc = il / tb.T;
+    return coarse_weight_ot(tb, w, b, oc, (int)(il - oc * tb.T), d, mn);
+}
+
+// (orientation, translation) of consecutive coarse elements without divisions
+struct OcT {
+    long long oc;
+    int t;
+    __device__ __forceinline__ OcT(long long i, int T) : oc(i / T), t((int)(i - (i / T) * T)) {}
+    __device__ __forceinline__ void next(int T)
+    {
+        if (++t == T) { t = 0; ++oc; }
+    }
+};
 
 __device__ __forceinline__ double fine_prior(const Tables& tb, const Work& w, int b, long long i)
 {
@@ -373,6 +391,35 @@ __device__ __forceinline__ Seg seg_of(const Tables& tb, const Work& w, bool fine
     return s;
 }
 
+// 16 consecutive diff2 values starting at element i0 (float4 loads when
+// aligned); elements at or past `end` read as -1 (no hypothesis).
+__device__ __forceinline__ void load16(const float* __restrict__ base, long long i0, long long end, float v[16])
+{
+    const float* p = base + i0;
+    if (i0 + 16 <= end && (reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
+        const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float4 f = __ldg(q + j);
+            v[4 * j] = f.x; v[4 * j + 1] = f.y; v[4 * j + 2] = f.z; v[4 * j + 3] = f.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] = (i0 + j < end) ? p[j] : -1.f;
+    }
+}
+
+// Floor under which a weight can never reach the significance crossing:
+// elements below tau hold less than n*tau <= (1-f) max <= (1-f) S of the mass,
+// because the weight of the minimum-diff2 element is >= exp(Lmin).  They enter
+// the sum but need no histogram entry.
+__device__ __forceinline__ double hist_floor(const Tables& tb, const Work& w, int b, long long nseg)
+{
+    const double Lmin = w.lbound[2 * b];
+    if (!(tb.adaptive_fraction < 1.) || !(Lmin > -INFINITY) || nseg <= 0) return 0.;
+    return (1. - tb.adaptive_fraction) * exp(Lmin) / (double)nseg;
+}
+
 // pass 1: weights (stored for the fine set only), sum, max, level-0 histogram
 __global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
 {
@@ -387,29 +434,46 @@ __global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
     const Seg sg = seg_of(tb, w, fine, b);
     const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
     const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
+    const double tau = hist_floor(tb, w, b, sg.end - sg.beg);
+    // weights below exp(Lmin) e^-46 / n add < 1e-20 of the sum in total: no exp() for them
+    const double Lmin = w.lbound[2 * b], Lmax = w.lbound[2 * b + 1];
+    // and are below the histogram floor tau (so every pass agrees on the candidates)
+    double cut = 700.;
+    if (Lmin > -INFINITY && sg.end > sg.beg && tau > 0.)
+        cut = fmin(700., fmax((Lmax - Lmin) + log((double)(sg.end - sg.beg)) + 46., Lmax - log(tau)));
     double lsum = 0.;
     unsigned long long lmax = 0;
-    for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
-         i += (long long)gridDim.x * blockDim.x) {
-        const float d = dsrc[i];
-        double wt;
-        if (fine) {
-            wt = 0.;
-            if (d >= 0.f) {
-                const double dd = (double)d - mn;
-                if (dd <= 700.) wt = fine_prior(tb, w, b, i) * exp(-dd);
+    const long long stride = (long long)gridDim.x * blockDim.x * 16;
+    for (long long i0 = sg.beg + ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 16; i0 < sg.end; i0 += stride) {
+        float v[16];
+        load16(dsrc, i0, sg.end, v);
+        OcT ot(fine ? 0 : i0, tb.T);
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const long long i = i0 + j;
+            const float d = v[j];
+            double wt = 0.;
+            if (fine) {
+                if (i >= sg.end) continue;
+                if (d >= 0.f) {
+                    const double dd = (double)d - mn;
+                    if (dd <= 700.) wt = fine_prior(tb, w, b, i) * exp(-dd);
+                }
+                w.wf[i] = wt;
+            } else {
+                if (d >= 0.f && (double)d - mn <= cut) wt = coarse_weight_ot(tb, w, b, ot.oc, ot.t, d, mn);
+                ot.next(tb.T);
             }
-            w.wf[i] = wt;
-        } else {
-            wt = coarse_weight(tb, w, b, i, d, mn);
-        }
-        if (wt > 0.) {
-            const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
-            const int dg = (int)(bits >> 52);
-            atomicAdd(&hc[dg], 1u);
-            atomicAdd(&hs[dg], wt);
-            lsum += wt;
-            lmax = max(lmax, bits);
+            if (wt > 0.) {
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
+                lsum += wt;
+                lmax = max(lmax, bits);
+                if (wt >= tau) {
+                    const int dg = (int)(bits >> 52);
+                    atomicAdd(&hc[dg], 1u);
+                    atomicAdd(&hs[dg], wt);
+                }
+            }
         }
     }
     lsum = block_sum(lsum, sh);
@@ -506,7 +570,10 @@ __global__ void __launch_bounds__(1024) k_select(Work w, int fine)
         sel->cum_above += bsum;
         sel->count_above += bc;
         sel->prefix = (sel->prefix << width) | (unsigned long long)digit;
-        if (cnt <= (unsigned long long)CAND_CAP || sel->shift == 0) {
+        if (sel->shift == 52 && sel->count_above + cnt <= (unsigned long long)FAST_CAP) {
+            sel->phase = 4;  // few candidates: gather the crossing bin and everything above it
+            sel->ncand = 0;
+        } else if (cnt <= (unsigned long long)CAND_CAP || sel->shift == 0) {
             sel->phase = 1;
             sel->ncand = 0;
         } else {
@@ -516,17 +583,6 @@ __global__ void __launch_bounds__(1024) k_select(Work w, int fine)
     if (pos < 0 && threadIdx.x == 0) { sel->phase = 3; w.status[b] = T2B_ERR_NOSIGNIF; }
     __syncthreads();
     for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
-}
-
-// Weight of element i of particle b if it may lie in [wlo, whi), else 0.
-__device__ __forceinline__ double weight_in(const Tables& tb, const Work& w, bool fine, int b, long long i,
-                                            const float* dsrc, double mn, double lo, double hi)
-{
-    if (fine) return w.wf[i];
-    const float d = dsrc[i];
-    const double dd = (double)d;
-    if (d < 0.f || dd <= lo || dd > hi) return 0.;
-    return coarse_weight(tb, w, b, i, d, mn);
 }
 
 // level >= 1 histogram of the next digit among the elements under the prefix
@@ -549,15 +605,33 @@ __global__ void __launch_bounds__(256) k_hist_level(Tables tb, Work w, int fine)
     const int sw = shift + width;
     double lo, hi;
     dwindow(bits2d(prefix << sw), bits2d((prefix + 1) << sw), mn, w.lbound[2 * b], w.lbound[2 * b + 1], lo, hi);
-    for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
-         i += (long long)gridDim.x * blockDim.x) {
-        const double wt = weight_in(tb, w, fine, b, i, dsrc, mn, lo, hi);
-        if (!(wt > 0.)) continue;
-        const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
-        if ((bits >> sw) != prefix) continue;
-        const int dg = (int)((bits >> shift) & (unsigned long long)(nb - 1));
-        atomicAdd(&hc[dg], 1u);
-        atomicAdd(&hs[dg], wt);
+    const long long stride = (long long)gridDim.x * blockDim.x * 16;
+    for (long long i0 = sg.beg + ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 16; i0 < sg.end; i0 += stride) {
+        float v[16];
+        if (!fine) load16(dsrc, i0, sg.end, v);
+        OcT ot(fine ? 0 : i0, tb.T);
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const long long i = i0 + j;
+            const long long oc = ot.oc;
+            const int t = ot.t;
+            if (!fine) ot.next(tb.T);
+            if (i >= sg.end) continue;
+            double wt;
+            if (fine) {
+                wt = w.wf[i];
+            } else {
+                const double dd = (double)v[j];
+                if (v[j] < 0.f || dd <= lo || dd > hi) continue;
+                wt = coarse_weight_ot(tb, w, b, oc, t, v[j], mn);
+            }
+            if (!(wt > 0.)) continue;
+            const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
+            if ((bits >> sw) != prefix) continue;
+            const int dg = (int)((bits >> shift) & (unsigned long long)(nb - 1));
+            atomicAdd(&hc[dg], 1u);
+            atomicAdd(&hs[dg], wt);
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += blockDim.x)
@@ -579,14 +653,32 @@ __global__ void __launch_bounds__(256) k_gather(Tables tb, Work w, int fine)
     const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
     double lo, hi;
     dwindow(bits2d(prefix << shift), bits2d((prefix + 1) << shift), mn, w.lbound[2 * b], w.lbound[2 * b + 1], lo, hi);
-    for (long long i = sg.beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < sg.end;
-         i += (long long)gridDim.x * blockDim.x) {
-        const double wt = weight_in(tb, w, fine, b, i, dsrc, mn, lo, hi);
-        if (!(wt > 0.)) continue;
-        const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
-        if ((bits >> shift) != prefix) continue;
-        const long long pos = atomicAdd((unsigned long long*)&sel->ncand, 1ull);
-        if (pos < CAND_CAP) w.cand[(size_t)b * CAND_CAP + pos] = wt;
+    const long long stride = (long long)gridDim.x * blockDim.x * 16;
+    for (long long i0 = sg.beg + ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 16; i0 < sg.end; i0 += stride) {
+        float v[16];
+        if (!fine) load16(dsrc, i0, sg.end, v);
+        OcT ot(fine ? 0 : i0, tb.T);
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const long long i = i0 + j;
+            const long long oc = ot.oc;
+            const int t = ot.t;
+            if (!fine) ot.next(tb.T);
+            if (i >= sg.end) continue;
+            double wt;
+            if (fine) {
+                wt = w.wf[i];
+            } else {
+                const double dd = (double)v[j];
+                if (v[j] < 0.f || dd <= lo || dd > hi) continue;
+                wt = coarse_weight_ot(tb, w, b, oc, t, v[j], mn);
+            }
+            if (!(wt > 0.)) continue;
+            const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
+            if ((bits >> shift) != prefix) continue;
+            const long long pos = atomicAdd((unsigned long long*)&sel->ncand, 1ull);
+            if (pos < CAND_CAP) w.cand[(size_t)b * CAND_CAP + pos] = wt;
+        }
     }
 }
 
@@ -646,6 +738,150 @@ __global__ void __launch_bounds__(1024) k_final(Work w, int fine, int ipass)
     }
 }
 
+// ------------------------------------------------- fast selection path
+// When the crossing bin of the level-0 histogram and every bin above it hold
+// at most FAST_CAP weights (the usual, concentrated posterior), one pass
+// gathers all of them with their indices and one CTA per particle sorts them
+// by weight, walks the cumulative sum exactly as src/ml_optimiser.cpp:
+// 7905-7935 does, and emits the index-ordered significant list.
+__global__ void __launch_bounds__(256) k_gather_fast(Tables tb, Work w, int fine)
+{
+    const int b = blockIdx.y;
+    SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    if (sel->phase != 4) return;
+    const Seg sg = seg_of(tb, w, fine, b);
+    const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
+    const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
+    const double wlo = fmax(bits2d(sel->prefix << 52), hist_floor(tb, w, b, sg.end - sg.beg));
+    double lo, hi;
+    dwindow(wlo, INFINITY, mn, w.lbound[2 * b], w.lbound[2 * b + 1], lo, hi);
+    double* cw = w.fcand_w + (size_t)b * FAST_CAP;
+    long long* ci = w.fcand_i + (size_t)b * FAST_CAP;
+    const long long stride = (long long)gridDim.x * blockDim.x * 16;
+    for (long long i0 = sg.beg + ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 16; i0 < sg.end; i0 += stride) {
+        float v[16];
+        if (!fine) load16(dsrc, i0, sg.end, v);
+        OcT ot(fine ? 0 : i0, tb.T);
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const long long i = i0 + j;
+            const long long oc = ot.oc;
+            const int t = ot.t;
+            if (!fine) ot.next(tb.T);
+            if (i >= sg.end) continue;
+            double wt;
+            if (fine) {
+                wt = w.wf[i];
+            } else {
+                if (v[j] < 0.f || (double)v[j] > hi) continue;
+                wt = coarse_weight_ot(tb, w, b, oc, t, v[j], mn);
+            }
+            if (!(wt >= wlo) || !(wt > 0.)) continue;
+            const long long pos = atomicAdd((unsigned long long*)&sel->ncand, 1ull);
+            if (pos < FAST_CAP) { cw[pos] = wt; ci[pos] = i; }
+        }
+    }
+}
+
+// bitonic sort of n2 (power of two) (key, index) pairs in shared memory;
+// by_weight: weight descending then index ascending; else index ascending
+__device__ void bitonic_pairs(double* kw, long long* ki, int n2, bool by_weight)
+{
+    for (int k = 2; k <= n2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    bool swap;
+                    if (by_weight) {
+                        const bool before = kw[l] > kw[i] || (kw[l] == kw[i] && ki[l] < ki[i]);  // l should precede i
+                        swap = up ? before : !before;
+                    } else {
+                        swap = up ? (ki[l] < ki[i]) : (ki[l] > ki[i]);
+                    }
+                    if (swap) {
+                        const double tw = kw[i]; kw[i] = kw[l]; kw[l] = tw;
+                        const long long tx = ki[i]; ki[i] = ki[l]; ki[l] = tx;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass)
+{
+    extern __shared__ unsigned char smem_raw[];
+    double* sw = reinterpret_cast<double*>(smem_raw);
+    long long* si = reinterpret_cast<long long*>(smem_raw + FAST_CAP * sizeof(double));
+    __shared__ int msig;
+    const int b = blockIdx.x;
+    SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    if (sel->phase != 4) return;
+    const long long nc = sel->ncand;
+    if (nc <= 0 || nc > FAST_CAP) {  // excluded by the histogram counts
+        if (threadIdx.x == 0) { sel->phase = 3; w.status[b] = T2B_ERR_NOSIGNIF; }
+        return;
+    }
+    int n2 = 1;
+    while (n2 < nc) n2 <<= 1;
+    for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+        sw[i] = i < nc ? w.fcand_w[(size_t)b * FAST_CAP + i] : -1.;
+        si[i] = i < nc ? w.fcand_i[(size_t)b * FAST_CAP + i] : 0x7fffffffffffffffLL;
+    }
+    __syncthreads();
+    bitonic_pairs(sw, si, n2, true);
+    if (threadIdx.x == 0) {
+        double cum = 0.;
+        long long k = -1;
+        for (long long i = 0; i < nc; i++) {
+            cum += sw[i];
+            if (cum > sel->target) { k = i; break; }
+        }
+        if (k < 0) k = nc - 1;
+        const double thr = sw[k];
+        long long m = k + 1;
+        while (m < nc && sw[m] >= thr) m++;
+        sel->thr = thr;
+        sel->nr_sign = ipass == 0 ? k + 1 : 0;
+        sel->argmax = si[0];
+        msig = (int)m;
+    }
+    __syncthreads();
+    if (!fine) {
+        const int m = msig;
+        int m2 = 1;
+        while (m2 < m) m2 <<= 1;
+        for (int i = m + threadIdx.x; i < m2; i += blockDim.x) { sw[i] = 0.; si[i] = 0x7fffffffffffffffLL; }
+        __syncthreads();
+        bitonic_pairs(sw, si, m2, false);
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            w.flist_w[(size_t)b * FAST_CAP + i] = sw[i];
+            w.flist_i[(size_t)b * FAST_CAP + i] = si[i];
+        }
+        if (threadIdx.x == 0) w.r_ncsig[b] = m;
+    }
+    if (threadIdx.x == 0) {
+        sel->fast = 1;
+        sel->phase = 2;
+    }
+}
+
+// copy the fast-path significant lists to their place in the batch pair list
+__global__ void __launch_bounds__(256) k_write_fast(Work w, int gather_final)
+{
+    const int b = blockIdx.x;
+    const SelState* sel = &w.sel_c[b];
+    if (!sel->fast || sel->phase != 2 || w.status[b] != T2B_OK) return;
+    const long long beg = w.pair_off[b], m = w.pair_off[b + 1] - beg;
+    for (long long i = threadIdx.x; i < m; i += blockDim.x) {
+        w.pairs[beg + i] = w.flist_i[(size_t)b * FAST_CAP + i];
+        w.pair_b[beg + i] = b;
+        if (gather_final) w.wf[beg + i] = w.flist_w[(size_t)b * FAST_CAP + i];
+    }
+}
+
 // ------------------------------------------------- ordered compaction
 constexpr int CHUNK = 4096;
 
@@ -677,127 +913,168 @@ __device__ __forceinline__ SigPred sig_pred(const Work& w, int b)
     return p;
 }
 
+// Per chunk of 4096 coarse elements: number of significant ones (thread t
+// covers 16 consecutive elements), and the index of the maximum weight.
 __global__ void __launch_bounds__(256) k_count_sig(Tables tb, Work w)
 {
+    __shared__ int wsum[8];
     const int b = blockIdx.y;
     const SelState* sel = &w.sel_c[b];
+    if (sel->phase != 2 || w.status[b] != T2B_OK || sel->fast) return;
     const long long n = (long long)tb.K * tb.O * tb.T;
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
     const float* dsrc = w.d2c + (size_t)b * (size_t)n;
-    __shared__ int cnt;
-    const bool active = sel->phase == 2;
-    SigPred pred{};
-    double alo = 0., ahi = 0.;
-    unsigned long long maxbits = 0;
-    if (active) {
-        pred = sig_pred(w, b);
-        maxbits = sel->maxbits;
-        const double wmax = __longlong_as_double((long long)maxbits);
-        dwindow(wmax, wmax * (1. + 1e-12), pred.mn, w.lbound[2 * b], w.lbound[2 * b + 1], alo, ahi);
-    }
+    const SigPred pred = sig_pred(w, b);
+    const unsigned long long maxbits = sel->maxbits;
+    const double wmax = __longlong_as_double((long long)maxbits);
+    double alo, ahi;
+    dwindow(wmax, wmax * (1. + 1e-12), pred.mn, w.lbound[2 * b], w.lbound[2 * b + 1], alo, ahi);
     for (int c = blockIdx.x; c < nch; c += gridDim.x) {
-        if (threadIdx.x == 0) cnt = 0;
-        __syncthreads();
+        const long long i0 = (long long)c * CHUNK + threadIdx.x * 16;
+        float v[16];
+        load16(dsrc, i0, n, v);
         int local = 0;
-        if (active) {
-            const long long end = min(n, (long long)(c + 1) * CHUNK);
-            for (long long i = (long long)c * CHUNK + threadIdx.x; i < end; i += blockDim.x) {
-                const float d = dsrc[i];
-                if (pred(tb, w, b, i, d, nullptr)) local++;
-                const double dd = (double)d;
-                if (d >= 0.f && dd > alo && dd <= ahi) {
-                    const double wt = coarse_weight(tb, w, b, i, d, pred.mn);
-                    if ((unsigned long long)__double_as_longlong(wt) == maxbits)
-                        atomicMin((long long*)&w.sel_c[b].argmax, i);
-                }
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const long long i = i0 + j;
+            const float d = v[j];
+            if (d < 0.f) continue;
+            if (pred(tb, w, b, i, d, nullptr)) local++;
+            const double dd = (double)d;
+            if (dd > alo && dd <= ahi) {
+                const double wt = coarse_weight(tb, w, b, i, d, pred.mn);
+                if ((unsigned long long)__double_as_longlong(wt) == maxbits) atomicMin((long long*)&w.sel_c[b].argmax, i);
             }
         }
         local = __reduce_add_sync(0xffffffffu, local);
-        if ((threadIdx.x & 31) == 0 && local) atomicAdd(&cnt, local);
+        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = local;
         __syncthreads();
-        if (threadIdx.x == 0) w.chunk_cnt[(size_t)b * w.max_chunks + c] = cnt;
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int j = 0; j < 8; j++) t += wsum[j];
+            w.chunk_cnt[(size_t)b * w.max_chunks + c] = t;
+        }
         __syncthreads();
     }
 }
 
-// exclusive scan of the chunk counts and of the per-particle totals (1 CTA)
-__global__ void __launch_bounds__(1024) k_scan_pairs(Tables tb, Work w)
+// exclusive scan of the chunk counts of one particle (one CTA per particle)
+__global__ void __launch_bounds__(1024) k_scan_chunks(Tables tb, Work w)
 {
     __shared__ long long sh[1024];
-    __shared__ long long base;
+    const int b = blockIdx.x;
     const long long n = (long long)tb.K * tb.O * tb.T;
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
-    if (threadIdx.x == 0) { base = 0; w.pair_off[0] = 0; }
+    if (w.sel_c[b].fast) return;  // list and count come from the fast path
+    const bool active = w.sel_c[b].phase == 2 && w.status[b] == T2B_OK;
+    long long run = 0;
+    for (int c0 = 0; c0 < nch; c0 += 1024) {
+        const int c = c0 + threadIdx.x;
+        const long long v = (active && c < nch) ? w.chunk_cnt[(size_t)b * w.max_chunks + c] : 0;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            const long long u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += u;
+            __syncthreads();
+        }
+        if (c < nch) w.chunk_cnt[(size_t)b * w.max_chunks + c] = (int)(run + sh[threadIdx.x] - v);
+        const long long tot = sh[1023];
+        __syncthreads();
+        run += tot;
+    }
+    if (threadIdx.x == 0) w.r_ncsig[b] = run;
+}
+
+// pair offsets of the batch (1 CTA); particles past the pair capacity are dropped
+__global__ void __launch_bounds__(1024) k_pair_offsets(Work w)
+{
+    __shared__ long long sh[1024];
+    __shared__ long long carry;
+    if (threadIdx.x == 0) { carry = 0; w.pair_off[0] = 0; }
     __syncthreads();
-    for (int b = 0; b < w.n; b++) {
-        long long run = 0;
-        for (int c0 = 0; c0 < nch; c0 += 1024) {
-            const int c = c0 + threadIdx.x;
-            const long long v = c < nch ? w.chunk_cnt[(size_t)b * w.max_chunks + c] : 0;
-            sh[threadIdx.x] = v;
+    for (int b0 = 0; b0 < w.n; b0 += 1024) {
+        const int b = b0 + threadIdx.x;
+        long long v = b < w.n ? w.r_ncsig[b] : 0;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            const long long u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
             __syncthreads();
-            for (int off = 1; off < 1024; off <<= 1) {
-                const long long u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
-                __syncthreads();
-                sh[threadIdx.x] += u;
-                __syncthreads();
-            }
-            if (c < nch) w.chunk_cnt[(size_t)b * w.max_chunks + c] = (int)(run + sh[threadIdx.x] - v);
-            const long long tot = sh[1023];
+            sh[threadIdx.x] += u;
             __syncthreads();
-            run += tot;
         }
-        if (threadIdx.x == 0) {
-            long long cnt = run;
-            if (base + cnt > w.pair_cap) {  // capacity exceeded: drop the particle
-                cnt = 0;
-                w.status[b] = T2B_ERR_NOMEM;
-            }
-            w.r_ncsig[b] = cnt;
-            base += cnt;
-            w.pair_off[b + 1] = base;
+        long long end = carry + sh[threadIdx.x];
+        if (b < w.n && end > w.pair_cap) {  // capacity exceeded: drop this particle
+            w.status[b] = T2B_ERR_NOMEM;
+            w.r_ncsig[b] = 0;
         }
+        __syncthreads();
+        // recompute with the dropped particles removed
+        v = b < w.n ? w.r_ncsig[b] : 0;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            const long long u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += u;
+            __syncthreads();
+        }
+        end = carry + sh[threadIdx.x];
+        if (b < w.n) w.pair_off[b + 1] = end;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = end;
         __syncthreads();
     }
 }
 
-// Ordered compaction of the significant coarse pairs: rounds of 256
-// consecutive elements, warp ballots and a block prefix keep index order.
+// Ordered compaction of the significant coarse pairs: thread t of a chunk
+// owns 16 consecutive elements; a block scan of the per-thread counts keeps
+// index order.
 __global__ void __launch_bounds__(256) k_compact(Tables tb, Work w, int gather_final)
 {
     __shared__ int wsum[8];
     const int b = blockIdx.y;
     const SelState* sel = &w.sel_c[b];
-    if (sel->phase != 2 || w.status[b] != T2B_OK) return;
+    if (sel->phase != 2 || w.status[b] != T2B_OK || sel->fast) return;
     const long long n = (long long)tb.K * tb.O * tb.T;
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
     const float* dsrc = w.d2c + (size_t)b * (size_t)n;
     const SigPred pred = sig_pred(w, b);
-    const long long pbase = w.pair_off[b];
+    const long long pbase = w.pair_off[b], pend = w.pair_off[b + 1];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int c = blockIdx.x; c < nch; c += gridDim.x) {
-        long long pos0 = pbase + w.chunk_cnt[(size_t)b * w.max_chunks + c];
-        for (int r = 0; r < CHUNK / 256; r++) {
-            const long long i = (long long)c * CHUNK + r * 256 + threadIdx.x;
-            double wt = 0.;
-            const bool f = i < n && pred(tb, w, b, i, dsrc[i], gather_final ? &wt : nullptr);
-            const unsigned m = __ballot_sync(0xffffffffu, f);
-            if (lane == 0) wsum[wid] = __popc(m);
-            __syncthreads();
-            int before = 0, tot = 0;
-            for (int j = 0; j < 8; j++) {
-                if (j < wid) before += wsum[j];
-                tot += wsum[j];
-            }
-            const long long pos = pos0 + before + __popc(m & ((1u << lane) - 1u));
-            if (f && pos < w.pair_off[b + 1]) {
-                w.pairs[pos] = i;
-                w.pair_b[pos] = b;
-                if (gather_final) w.wf[pos] = wt;
-            }
-            pos0 += tot;
-            __syncthreads();
+        const long long i0 = (long long)c * CHUNK + threadIdx.x * 16;
+        float v[16];
+        load16(dsrc, i0, n, v);
+        unsigned flags = 0;
+        int local = 0;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            if (v[j] >= 0.f && pred(tb, w, b, i0 + j, v[j], nullptr)) { flags |= 1u << j; local++; }
         }
+        int incl = local;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) wsum[wid] = incl;
+        __syncthreads();
+        int before = 0;
+        for (int j = 0; j < wid; j++) before += wsum[j];
+        long long pos = pbase + w.chunk_cnt[(size_t)b * w.max_chunks + c] + before + incl - local;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            if (!(flags & (1u << j))) continue;
+            if (pos < pend) {
+                w.pairs[pos] = i0 + j;
+                w.pair_b[pos] = b;
+                if (gather_final) w.wf[pos] = coarse_weight(tb, w, b, i0 + j, v[j], pred.mn);
+            }
+            pos++;
+        }
+        __syncthreads();
     }
 }
 
@@ -883,52 +1160,13 @@ __global__ void __launch_bounds__(256) k_argmax_fine(Tables tb, Work w)
 {
     const int b = blockIdx.y;
     const SelState* sel = &w.sel_f[b];
-    if (sel->phase != 2) return;
+    if (sel->phase != 2 || sel->fast) return;
     const long long rv = (long long)tb.R * tb.V;
     const long long beg = w.pair_off[b] * rv, end = w.pair_off[b + 1] * rv;
     for (long long i = beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
          i += (long long)gridDim.x * blockDim.x)
         if ((unsigned long long)__double_as_longlong(w.wf[i]) == sel->maxbits)
             atomicMin((long long*)&w.sel_f[b].argmax, i);
-}
-
-// --------------------------------------------------- orientation groups
-// Consecutive pairs of a particle with the same orientation form one group;
-// a work item of the weighted sums is (group, fine rotation).  1 CTA.
-__global__ void __launch_bounds__(1024) k_groups(Tables tb, Work w, int R)
-{
-    __shared__ long long sh[1024];
-    __shared__ long long base;
-    if (threadIdx.x == 0) { base = 0; w.group_off[0] = 0; }
-    __syncthreads();
-    const int T = tb.T;
-    for (int b = 0; b < w.n; b++) {
-        const long long beg = w.pair_off[b], end = w.pair_off[b + 1];
-        for (long long q0 = beg; q0 < end; q0 += 1024) {
-            const long long q = q0 + threadIdx.x;
-            const int f = (q < end && (q == beg || w.pairs[q] / T != w.pairs[q - 1] / T)) ? 1 : 0;
-            sh[threadIdx.x] = f;
-            __syncthreads();
-            for (int off = 1; off < 1024; off <<= 1) {
-                const long long u = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
-                __syncthreads();
-                sh[threadIdx.x] += u;
-                __syncthreads();
-            }
-            if (f) {
-                const long long g = base + sh[threadIdx.x] - 1;
-                w.groups[g] = q;
-                w.group_b[g] = b;
-            }
-            const long long tot = sh[1023];
-            __syncthreads();
-            if (threadIdx.x == 0) base += tot;
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) w.group_off[b + 1] = base;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) w.counters[3] = (unsigned long long)base * R;  // wsum work items
 }
 
 // ---------------------------------------------- weighted sums + backprojection
@@ -949,21 +1187,41 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
     __shared__ double shr[32];
     const int P = tb.P, T = tb.T, xh = tb.xh, s = tb.s;
     const int R = tb.ovs ? tb.R : 1, V = tb.ovs ? tb.V : 1;
-    const long long G = w.group_off[w.n];
-    const unsigned long long nitems = (unsigned long long)G * R;
+    (void)xh;
+    const long long npairs = w.pair_off[w.n];
+    const unsigned long long nitems = (unsigned long long)npairs * R;
     const float2* proj = tb.ovs ? tb.proj_f : tb.proj_c;
     const float2* abt = tb.ovs ? tb.ab_f : tb.ab_c;
     const int nring = s / 2 + 1;
+    __shared__ long long grp_end;
     for (;;) {
-        if (threadIdx.x == 0) item = (long long)atomicAdd(&w.counters[2], 1ull);
+        if (threadIdx.x == 0) {
+            item = (long long)atomicAdd(&w.counters[2], 1ull);
+            // a work item is (first pair of an orientation group, fine rotation)
+            grp_end = -1;
+            if ((unsigned long long)item < nitems) {
+                const long long q = item / R;
+                const int bq = w.pair_b[q];
+                const long long oc = w.pairs[q] / T;
+                if (q == w.pair_off[bq] || w.pairs[q - 1] / T != oc) {
+                    long long e = q + 1;
+                    const long long pend = w.pair_off[bq + 1];
+                    while (e < pend && w.pairs[e] / T == oc) e++;
+                    grp_end = e;
+                }
+            }
+        }
         __syncthreads();
         const long long it = item;
         if ((unsigned long long)it >= nitems) break;
-        const long long gi = it / R;
-        const int r = (int)(it - gi * R);
-        const int b = w.group_b[gi];
-        const long long qa = w.groups[gi];
-        const long long qb = (gi + 1 < G && w.group_b[gi + 1] == b) ? w.groups[gi + 1] : w.pair_off[b + 1];
+        const long long qa = it / R;
+        const long long qb = grp_end;
+        const int r = (int)(it - qa * R);
+        if (qb < 0) {  // not the start of a group
+            __syncthreads();
+            continue;
+        }
+        const int b = w.pair_b[qa];
         const int oc = (int)(w.pairs[qa] / T);
         const int k = oc / tb.O, o = oc - k * tb.O, idir = o / tb.n_psi;
         const long long tab = tb.ovs ? (long long)oc * R + r : oc;
@@ -1216,6 +1474,7 @@ int grid_x_for(int nb)
 }
 
 const size_t HIST_SMEM = HIST_BINS * (sizeof(unsigned) + sizeof(double));
+const size_t FAST_SMEM = FAST_CAP * (sizeof(double) + sizeof(long long));
 
 void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStream_t st)
 {
@@ -1229,6 +1488,8 @@ void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStr
     }
     k_gather<<<grid, 256, 0, st>>>(tb, w, fine);
     k_final<<<w.n, 1024, 0, st>>>(w, fine, ipass);
+    k_gather_fast<<<grid, 256, 0, st>>>(tb, w, fine);
+    k_final_fast<<<w.n, 1024, FAST_SMEM, st>>>(w, fine, ipass);
 }
 
 }  // namespace
@@ -1256,15 +1517,17 @@ void launch_diff2_simt(const Tables& tb, const Work& w, cudaStream_t st)
     T2B_CUDA(cudaGetLastError());
 }
 
+void estep_init_attributes()
+{
+    T2B_CUDA(cudaFuncSetAttribute(k_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HIST_SMEM));
+    T2B_CUDA(cudaFuncSetAttribute(k_hist_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HIST_SMEM));
+    T2B_CUDA(cudaFuncSetAttribute(k_final_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FAST_SMEM));
+    (void)sm_count();
+}
+
 void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStream_t st)
 {
     (void)maxsig;
-    static bool attr = false;
-    if (!attr) {
-        T2B_CUDA(cudaFuncSetAttribute(k_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HIST_SMEM));
-        T2B_CUDA(cudaFuncSetAttribute(k_hist_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HIST_SMEM));
-        attr = true;
-    }
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
     k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 0);
@@ -1273,8 +1536,10 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
     dim3 gc(std::min(nch, gx), w.n);
     k_count_sig<<<gc, 256, 0, st>>>(tb, w);
-    k_scan_pairs<<<1, 1024, 0, st>>>(tb, w);
+    k_scan_chunks<<<w.n, 1024, 0, st>>>(tb, w);
+    k_pair_offsets<<<1, 1024, 0, st>>>(w);
     k_compact<<<gc, 256, 0, st>>>(tb, w, tb.ovs ? 0 : 1);
+    k_write_fast<<<w.n, 256, 0, st>>>(w, tb.ovs ? 0 : 1);
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -1297,7 +1562,6 @@ void launch_weights_fine(const Tables& tb, const Work& w, cudaStream_t st)
 void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* const* grid_data,
                     float* const* grid_weight, cudaStream_t st)
 {
-    k_groups<<<1, 1024, 0, st>>>(tb, w, tb.ovs ? tb.R : 1);
     GridPtrs gp{grid_data, grid_weight};
     k_wsum_bp<<<2 * sm_count(), 256, 0, st>>>(tb, w, g, gp);
     k_results<<<(w.n + 127) / 128, 128, 0, st>>>(tb, w);

@@ -49,10 +49,12 @@ struct SelState {
     long long nr_sign;
     unsigned long long maxbits;
     long long argmax;
+    int fast;                 // selected by the fast path
 };
 
 constexpr int HIST_BINS = 4096;  // 12-bit digits
 constexpr int CAND_CAP = 4096;   // candidates sorted in shared memory
+constexpr int FAST_CAP = 4096;   // weights gathered by the fast selection path
 
 // Device views of the per-iteration tables.
 struct Tables {
@@ -69,7 +71,10 @@ struct Tables {
     const double* trans_prior;// T x 2
     const double* pdf_o;      // K*n_dir, normalised
     const unsigned char* skip;// K*O: orientation not evaluated (pdf <= 0)
+    const double* pdf_oc;     // K*O: normalised pdf_orientation of each orientation
     const int* mresol;        // P
+    const int* kpix;          // nk: window pixels inside the projection radius (the only
+    int nk;                   //     pixels whose projection, hence contraction term, can be non-zero)
     double sigma2_offset, pixel_size, adaptive_fraction;
     double lpo_min, lpo_max;  // extremes of log(pdf_o) over evaluated orientations
 };
@@ -98,6 +103,10 @@ struct Work {
     unsigned* hist_cnt;       // n x HIST_BINS
     double* hist_sum;         // n x HIST_BINS
     double* cand;             // n x CAND_CAP
+    double* fcand_w;          // n x FAST_CAP: fast-path candidates (weight, index)
+    long long* fcand_i;
+    double* flist_w;          // n x FAST_CAP: fast-path significant list, index order
+    long long* flist_i;
     long long* pairs;         // pair_cap: coarse hidden index of significant pairs
     int* pair_b;              // pair_cap
     long long* pair_off;      // n+1
@@ -126,6 +135,8 @@ void launch_project_table(const Volume& v, const float2* mdl, const double* eul9
 void launch_phase_table(const double* shifts, int n, int s, int ori_size, float2* out, cudaStream_t st);
 
 // E-step stages (estep.cu)
+void estep_init_attributes();
+void tc_init_attributes();
 void launch_prep(const Tables& tb, const Work& w, cudaStream_t st);
 void launch_norms(const Tables& tb, const Work& w, cudaStream_t st);
 void launch_diff2_simt(const Tables& tb, const Work& w, cudaStream_t st);
@@ -149,12 +160,13 @@ struct TcOperands {
     void* wl;
     int m_pad, n_pad, kdim;   // padded sizes of the cross-term operands
     int kn, b_pad;            // padded sizes of the norm operands
+    void* maps;               // 8 CUtensorMap descriptors (128 B each) in device memory
 };
-size_t tc_kdim(int P);
+size_t tc_kdim(int nk);
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
 void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
-size_t tc_kn(int P);
+size_t tc_kn(int nk);
 void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
 bool tc_supported();
 
@@ -178,6 +190,10 @@ struct t2b_ctx {
     float2** gd_table = nullptr;              // device table of per-class grid data pointers
     float** gw_table = nullptr;               // device table of per-class grid weight pointers
     int last_n = 0;                           // particles of the last batch
+    cudaGraphExec_t gexec = nullptr;          // captured device batch
+    std::vector<const void*> gkey;            // shape / buffers / stream it was captured for
+    int graph_kernels = -1;                   // kernel nodes of the captured batch
+    int last_kernels = -1;
     cudaEvent_t ev[8]{};
     float stage_ms[7]{};
 };
