@@ -141,6 +141,20 @@ __device__ __forceinline__ unsigned f2key(float f)
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
+// Tile order: groups of GROUP_M orientation tiles, the batch columns inside a
+// group, so the 148 tiles that run together share few operand strips.
+constexpr int GROUP_M = 16;
+__device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, int& mt, int& nt)
+{
+    const int per_group = GROUP_M * n_tiles;
+    const int g = tile / per_group;
+    const int first = g * GROUP_M;
+    const int gm = min(GROUP_M, m_tiles - first);
+    const int r = tile - g * per_group;
+    mt = first + r % gm;
+    nt = r / gm;
+}
+
 struct TcParams {
     int m_tiles, n_tiles, kblocks;
     int raw;                  // 1: store the contraction itself (norm GEMM), 0: diff2 epilogue
@@ -203,7 +217,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         int issued[STAGES] = {0, 0};
         uint32_t last_par[STAGES] = {0, 0};
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
-            const int mt = tile / p.n_tiles, nt = tile - mt * p.n_tiles;
+            int mt, nt;
+            tile_coords(tile, p.m_tiles, p.n_tiles, mt, nt);
             for (int kb = 0; kb < p.kblocks; kb++, it++) {
                 const int s = it % STAGES;
                 const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
@@ -266,7 +281,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         unsigned* wmin = smin + ew * (TN + 2);
         int tl = 0;
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x, tl++) {
-            const int mt = tile / p.n_tiles, nt = tile - mt * p.n_tiles;
+            int mt, nt;
+            tile_coords(tile, p.m_tiles, p.n_tiles, mt, nt);
             const int abuf = tl & 1;
             const uint32_t aph = (uint32_t)(tl >> 1) & 1u;
             if (!mbar_wait(&tfull_bar[abuf], aph, &abort_flag)) { abort_flag = 1; break; }

@@ -1,0 +1,115 @@
+"""Data-parallel E-step over several GPUs: one process per GPU.
+
+Particles of an iteration are independent (the reference farms them out to MPI
+followers, src/ml_optimiser_mpi.cpp:1155-1444), so every rank runs the E-step on
+its own shard with no communication on the data path.  The one exchange is at
+the end of the iteration: summing the backprojection grids and the weighted
+sums over the ranks of one gold-standard half, which the reference does by a
+device-to-host copy, a host double sum and MPI Send/Recv
+(src/ml_optimiser_mpi.cpp:1465-1480, 1732-1830).  Here it is an in-place
+all-reduce on the device grids through torch.distributed (NCCL over
+NVLink/NVSwitch on GPUs, gloo on CPU).
+"""
+import ctypes
+
+import numpy as np
+
+
+def shard_range(n, rank, world):
+    """Contiguous, balanced [begin, end) of `n` particles for `rank` of `world`."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad rank / world")
+    base, extra = divmod(n, world)
+    begin = rank * base + min(rank, extra)
+    return begin, begin + base + (1 if rank < extra else 0)
+
+
+# --- zero-copy torch view of library device memory (DLPack) -----------------
+class _DLDevice(ctypes.Structure):
+    _fields_ = [("device_type", ctypes.c_int32), ("device_id", ctypes.c_int32)]
+
+
+class _DLDataType(ctypes.Structure):
+    _fields_ = [("code", ctypes.c_uint8), ("bits", ctypes.c_uint8), ("lanes", ctypes.c_uint16)]
+
+
+class _DLTensor(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("device", _DLDevice), ("ndim", ctypes.c_int32),
+                ("dtype", _DLDataType), ("shape", ctypes.POINTER(ctypes.c_int64)),
+                ("strides", ctypes.POINTER(ctypes.c_int64)), ("byte_offset", ctypes.c_uint64)]
+
+
+class _DLManagedTensor(ctypes.Structure):
+    pass
+
+
+_DELETER = ctypes.CFUNCTYPE(None, ctypes.POINTER(_DLManagedTensor))
+_DLManagedTensor._fields_ = [("dl_tensor", _DLTensor), ("manager_ctx", ctypes.c_void_p),
+                             ("deleter", _DELETER)]
+_KEEP = {}
+
+
+@_DELETER
+def _release(ptr):
+    _KEEP.pop(ctypes.addressof(ptr.contents), None)
+
+
+def device_view(ptr, n_floats, device):
+    """A float32 torch tensor aliasing `n_floats` floats of CUDA memory at `ptr`.
+
+    The memory stays owned by the library; the view must not outlive it.
+    """
+    import torch
+    shape = (ctypes.c_int64 * 1)(n_floats)
+    mt = _DLManagedTensor()
+    mt.dl_tensor.data = ptr
+    mt.dl_tensor.device = _DLDevice(2, device)  # kDLCUDA
+    mt.dl_tensor.ndim = 1
+    mt.dl_tensor.dtype = _DLDataType(2, 32, 1)  # kDLFloat, 32 bits
+    mt.dl_tensor.shape = shape
+    mt.dl_tensor.strides = None
+    mt.dl_tensor.byte_offset = 0
+    mt.manager_ctx = None
+    mt.deleter = _release
+    _KEEP[ctypes.addressof(mt)] = (mt, shape)
+    pycapsule_new = ctypes.pythonapi.PyCapsule_New
+    pycapsule_new.restype = ctypes.py_object
+    pycapsule_new.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+    cap = pycapsule_new(ctypes.addressof(mt), b"dltensor", None)
+    return torch.utils.dlpack.from_dlpack(cap)
+
+
+def allreduce_grids_(estep, nr_classes, group=None):
+    """Sum the device BP grids of every class over the ranks of `group`, in place."""
+    import torch
+    import torch.distributed as dist
+    dev = torch.cuda.current_device()
+    for k in range(nr_classes):
+        data_ptr, w_ptr = estep.backprojector_device_ptrs(k)
+        nvox = int(np.prod(estep._grid_shape))
+        for ptr, n in ((data_ptr, 2 * nvox), (w_ptr, nvox)):
+            dist.all_reduce(device_view(ptr, n, dev), op=dist.ReduceOp.SUM, group=group)
+
+
+# per-particle fields of a result dict that are summed into the model
+SUMMED = ("wsum_sigma2", "wsum_pdf_class", "wsum_pdf_dir", "wsum_norm", "sumw", "wsum_sigma2_offset")
+
+
+def reduce_wsums(results, group=None):
+    """Sum the weighted sums of this rank's particles, then over the ranks (FP64).
+
+    `results`: list of result dicts of t2relion_b200.EStep.expectation.  Returns a
+    dict of summed arrays, identical on every rank of `group`.
+    """
+    import torch
+    import torch.distributed as dist
+    out = {}
+    for key in SUMMED:
+        local = sum(np.asarray(r[key], np.float64).sum(axis=0) for r in results)
+        t = torch.as_tensor(np.atleast_1d(local), dtype=torch.float64)
+        if dist.is_initialized() and dist.get_world_size(group) > 1:
+            if dist.get_backend(group) == "nccl":
+                t = t.cuda()
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        out[key] = t.cpu().numpy()
+    return out
