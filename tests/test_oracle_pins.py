@@ -81,3 +81,56 @@ def test_oracle_projection_matches_numpy(oracle, synth):
         a = pr.project(0, A)
         b = synth.project(fmap, A[None], s, r)[0]
         assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
+
+
+def _ref_acc():
+    path = os.path.join(ROOT, "oracle", "_ref", "libacc_ref.so")
+    if not os.path.exists(path):
+        pytest.skip("reference CPU kernels not built (needs the reference tree)")
+    lib = ctypes.CDLL(path)
+    f, i, p = ctypes.c_float, ctypes.c_int, ctypes.c_void_p
+    lib.ref_coarse_diff2.argtypes = [p, i, i, i, i, i, i, i, p, i, p, p, p, i, i, p, p, i, f, p]
+    lib.ref_coarse_diff2.restype = i
+    return lib
+
+
+def test_coarse_diff2_matches_reference_cpu_kernel(oracle, synth):
+    """FP64 oracle vs the reference's CpuKernels::diff2_coarse (FP32) on the same inputs.
+
+    The reference kernel takes the CTF-divided image and corr = Minvsigma2 CTF^2
+    (acc_coarse.h:309-346), which is the same diff2 as the oracle's
+    sum 0.5 M |CTF P - shift X|^2; agreement to FP32 accumulation accuracy pins the
+    oracle's projection, phase-shift and difference conventions to reference code.
+    """
+    import problems
+    lib = _ref_acc()
+    pb = problems.build("refine_o2", n_particles=2, seed=29)
+    samp, prob, P = pb["samp"], pb["prob"], pb["parts"]
+    fmap = pb["maps"][0]
+    mz, my, mx = fmap.shape
+    mdl = np.ascontiguousarray(fmap.view(np.float32))
+    O, T = prob.O, prob.T
+    sel = np.arange(0, O, 1)[:1024]
+    eul = samp["eul_coarse"].reshape(-1, 3, 3)[sel]
+    einv = np.ascontiguousarray(np.transpose(eul, (0, 2, 1)).reshape(-1, 9), np.float32)
+    s, N = pb["s"], pb["N"]
+    tx = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 0] / N, np.float32)
+    ty = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 1] / N, np.float32)
+    for b in range(2):
+        ref_o, _ = prob.coarse_diff2(pb["oparts"], b)
+        ref_o = ref_o.reshape(O, T)[sel]
+        ctf = P["ctf"][b].astype(np.float64)
+        X = P["fimg"][b].astype(np.complex128) / ctf
+        re = np.ascontiguousarray(X.real, np.float32)
+        im = np.ascontiguousarray(X.imag, np.float32)
+        corr = np.ascontiguousarray(P["minv"][b] * ctf * ctf, np.float32)
+        out = np.zeros((len(sel), T), np.float32)
+        rc = lib.ref_coarse_diff2(mdl.ctypes.data, mx, my, mz, -(my // 2), -(mz // 2), pb["r"], 2,
+                                  einv.ctypes.data, len(sel), re.ctypes.data, im.ctypes.data, corr.ctypes.data,
+                                  s // 2 + 1, s, tx.ctypes.data, ty.ctypes.data, T,
+                                  float(P["scalars"][b, 1] / 2), out.ctypes.data)
+        assert rc == 0
+        rel = np.abs(out.astype(np.float64) - ref_o) / np.abs(ref_o)
+        assert np.max(rel) < 2e-4, np.max(rel)
+        assert np.median(rel) < 1e-5
+        assert np.array_equal(np.argmin(out, axis=1), np.argmin(ref_o, axis=1))
