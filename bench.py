@@ -14,7 +14,8 @@ value: particles/s with inputs resident in HBM (device entry point, CUDA events
 on the launching stream, max over ranks).  e2e: the same metric through the
 host entry point with pinned host buffers (H2D of the batch and D2H of the
 results inside the timed region).  `--impl reference` times the reference's CPU
-E-step (the FP64 port in oracle/) on the host cores instead.
+E-step on the host cores instead: the reference's own CPU diff2 kernel compiled
+from its sources (oracle/_ref) when built, else the FP64 port in oracle/.
 """
 import argparse
 import ctypes
@@ -77,16 +78,56 @@ def setup_context(t2b, sy, fmap, samp, mode, batch, device=0):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock / throttle-reason sampling during the timed region.
+
+    NVML (pynvml) polled every 10 ms from a thread, on the device whose UUID
+    torch reports for `gpu`; nvidia-smi at 200 ms when pynvml is missing.
+    """
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, gpu):
         self.gpu = gpu
         self.proc = None
+        self.thread = None
+        self.samples = []   # (sm_mhz, reason bits)
+        self.max_mhz = None
+        self.lines = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+        try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid if not uuid.startswith("GPU-") else uuid)
+        except pynvml.NVMLError:
+            if pynvml.nvmlDeviceGetCount() == 1:
+                return pynvml, pynvml.nvmlDeviceGetHandleByIndex(0)
+            raise
+
+    def _poll(self, nv, h):
+        while not self.stop.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except nv.NVMLError:
+                pass
+            self.stop.wait(0.01)
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -96,7 +137,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -107,9 +150,13 @@ class ClockSampler:
             self.lines = [l for l in out.splitlines() if l.strip()]
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
+        sm, mx, reasons = [], self.max_mhz, set()
+        for mhz, bits in self.samples:
+            sm.append(float(mhz))
+            for n, b in self.REASONS:
+                if bits & b:
+                    reasons.add(n)
+        for l in self.lines:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
                 continue
@@ -118,11 +165,12 @@ class ClockSampler:
                 mx = float(f[2])
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
+            for (n, _), v in zip(self.REASONS, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.samples else ("nvidia-smi" if self.lines else None)}
 
 
 def measured_peaks():
@@ -134,22 +182,61 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def cpu_baseline(sy, fmap, samp, parts, seconds=20.0):
-    """FP64 oracle (reference CPU E-step port) on the host cores, bounded sample.
+def _coarse_slice_timer(sy, fmap, samp, parts):
+    """A function (n_dir, n_particles) -> seconds that runs the coarse pass of one
+    particle per host thread over the first n_dir directions x all psi.
 
-    Sample: one particle per host thread through the coarse pass (the part of the
-    reference's E-step that is > 95 % of its time at this workload) over a slice
-    of the 36,864 orientations sized to take about `seconds`; particles/s is
-    extrapolated to the full orientation set.
+    The reference's own CPU kernel (CpuKernels::diff2_coarse, compiled from the
+    reference sources into oracle/_ref/libacc_ref.so) when that library is
+    present, else the FP64 port in oracle/.  Returns (timer, kind).
     """
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
     w = WORKLOAD
     s = 2 * w["r_max"]
-    cores = os.cpu_count() or 1
-    O = samp["n_dir"] * samp["n_psi"]
-    # calibrate the slice on one particle, one thread
-    def run_slice(nd, npart, nthreads):
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libacc_ref.so")
+    if os.path.exists(lib_path):
+        lib = ctypes.CDLL(lib_path)
+        lib.ref_coarse_diff2.restype = ctypes.c_int
+        fm = np.ascontiguousarray(fmap.view(np.float32))
+        mz, my, mx = fmap.shape
+        eul = samp["eul_coarse"].reshape(-1, 3, 3)
+        einv = np.ascontiguousarray(np.transpose(eul, (0, 2, 1)).reshape(-1, 9), np.float32)
+        N = w["ori_size"]
+        tx = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 0] / N, np.float32)
+        ty = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 1] / N, np.float32)
+        T = len(tx)
+        ops = []
+        for b in range(parts["fimg"].shape[0]):
+            ctf = parts["ctf"][b].astype(np.float64)
+            X = parts["fimg"][b].astype(np.complex128) / ctf
+            ops.append((np.ascontiguousarray(X.real, np.float32), np.ascontiguousarray(X.imag, np.float32),
+                        np.ascontiguousarray(parts["minv"][b] * ctf * ctf, np.float32),
+                        float(parts["scalars"][b, 1] / 2)))
+
+        def run(nd, npart):
+            no = nd * samp["n_psi"]
+            outs = [np.empty((no, T), np.float32) for _ in range(npart)]
+
+            def one(b):
+                re, im, corr, xi2 = ops[b]
+                lib.ref_coarse_diff2(ctypes.c_void_p(fm.ctypes.data), mx, my, mz, -(my // 2), -(mz // 2),
+                                     w["r_max"], 2, ctypes.c_void_p(einv.ctypes.data), no,
+                                     ctypes.c_void_p(re.ctypes.data), ctypes.c_void_p(im.ctypes.data),
+                                     ctypes.c_void_p(corr.ctypes.data), s // 2 + 1, s,
+                                     ctypes.c_void_p(tx.ctypes.data), ctypes.c_void_p(ty.ctypes.data), T,
+                                     ctypes.c_float(xi2), ctypes.c_void_p(outs[b].ctypes.data))
+            t0 = time.perf_counter()
+            ths = [threading.Thread(target=one, args=(b,)) for b in range(npart)]
+            for th in ths:
+                th.start()
+            for th in ths:
+                th.join()
+            return time.perf_counter() - t0
+        return run, "reference"
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    def run(nd, npart):
         sub = dict(samp)
         sub["n_dir"] = nd
         sub["eul_coarse"] = samp["eul_coarse"][: nd * samp["n_psi"]]
@@ -166,14 +253,30 @@ def cpu_baseline(sy, fmap, samp, parts, seconds=20.0):
         for th in ths:
             th.join()
         return time.perf_counter() - t0
-    t1 = run_slice(1, 1, 1)                      # one direction = 48 orientations
+    return run, "port"
+
+
+def cpu_baseline(sy, fmap, samp, parts, seconds=20.0, timer=None):
+    """The reference's CPU E-step on the host cores, bounded sample.
+
+    Sample: one particle per host thread through the coarse pass (the part of the
+    reference's E-step that is > 95 % of its time at this workload) over a slice
+    of the 36,864 orientations sized to take about `seconds`; particles/s is
+    extrapolated to the full orientation set.
+    """
+    run, kind = timer or _coarse_slice_timer(sy, fmap, samp, parts)
+    cores = os.cpu_count() or 1
+    O = samp["n_dir"] * samp["n_psi"]
+    t1 = run(1, 1)                      # one direction = 48 orientations, one thread
     nd = int(max(1, min(samp["n_dir"], seconds / max(t1, 1e-6))))
     npart = min(cores, parts["fimg"].shape[0])
-    t = run_slice(nd, npart, npart)
+    t = run(nd, npart)
     frac = nd * samp["n_psi"] / O
     value = npart * frac / t
-    return {"value": value, "unit": "particles/s", "cores": npart, "kind": "port",
-            "sample": f"{npart} particles x {nd * samp['n_psi']} of {O} orientations (coarse pass, FP64 oracle), "
+    src = ("CpuKernels::diff2_coarse of the reference, compiled from its sources" if kind == "reference"
+           else "FP64 oracle port")
+    return {"value": value, "unit": "particles/s", "cores": npart, "kind": kind,
+            "sample": f"{npart} particles x {nd * samp['n_psi']} of {O} orientations (coarse pass, {src}), "
                       f"{t:.1f} s, extrapolated to the full orientation set"}
 
 
@@ -206,16 +309,20 @@ def run_reference(args, world, rank):
     t2b = load_package()
     import t2relion_b200.synthetic as sy
     fmap, samp, parts = build_problem(t2b, sy, max(8, os.cpu_count() or 1), WORKLOAD["seed"] + 1)
+    timer = _coarse_slice_timer(sy, fmap, samp, parts)
+    # each step a bounded sample: the whole --warmup W --steps K run stays within a few minutes
+    per_step = min(args.ref_seconds, 150.0 / max(1, args.warmup + args.steps))
     vals = []
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(sy, fmap, samp, parts, seconds=args.ref_seconds)
+        cb = cpu_baseline(sy, fmap, samp, parts, seconds=per_step, timer=timer)
         if i >= args.warmup:
             vals.append(cb["value"])
     v = statistics.median(vals)
     cb["value"] = v
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v if v else None,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if cb["kind"] == "reference" else "f64",
             "data": "synthetic", "config": {"workload": WORKLOAD["name"], "particles_per_step": cb["cores"]},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
