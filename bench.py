@@ -464,10 +464,16 @@ def main():
     # (projections are zero outside); executed = what the units did
     nk = int(sum(1 for n in range(P) if (lambda i, x: x * x + (i if i < s // 2 + 1 else i - s) ** 2)(n // (s // 2 + 1), n % (s // 2 + 1)) <= (s // 2) ** 2))
     executed = (12.0 if mode == t2b.DIFF2_SPLIT_BF16 else 4.0) * K * O * T * nk * B / (gemm / 1000.0) / 1e12
+    # DRAM bytes (read + write) of one diff2 launch of this exact workload from one ncu capture
+    # (dram__bytes_read.sum 8.16 GB + dram__bytes_write.sum 1.56 GB at 128 particles;
+    # profiles/k_diff2_tc_box128_order3_b128_dram.md), scaled by the batch size
+    traffic = None
+    if mode == t2b.DIFF2_SPLIT_BF16 and not args.profile_case:
+        traffic = (8.16e9 + 1.56e9) * B / 128.0
     roof = {"bound": bound, "kernel": "k_diff2_tc" if mode else "k_diff2_simt", "achieved": achieved,
             "executed_tflops": executed, "contraction_pixels": nk,
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src,
-            "traffic": None, "flops_per_launch": flops}
+            "traffic": traffic, "flops_per_launch": flops}
     line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+bf16x3/f64" if mode else "f32/f64", "data": "synthetic",
