@@ -141,6 +141,10 @@ typedef struct t2b_result {
     double* wsum_pdf_class;     /* n x nr_classes                                       */
     double* wsum_pdf_dir;       /* n x nr_classes*n_dir                                 */
     int* status;                /* n: T2B_OK or T2B_ERR_NOSIGNIF per particle           */
+    /* learned proposals (optional, may be NULL; see t2b_proposal_enable) */
+    double* audit_mass;         /* n: posterior mass of the full coarse pass held by the
+                                   particle's proposals (audited particles), else -1     */
+    int* learned;               /* n: 1 if the coarse pass ran on the proposals          */
 } t2b_result;
 
 /* E-step of one batch (MlOptimiserCuda::doThreadExpectationSomeParticles,
@@ -197,11 +201,81 @@ int t2b_debug_fine(t2b_ctx* ctx, int b, long long* pairs, float* diff2, long lon
 int t2b_last_launch_count(t2b_ctx* ctx, int* kernels);
 
 /* Device time of the stages of the last batch, in ms (CUDA events on the
- * stream the stages ran on): [0] prep + norms, [1] tensor-core operand split,
- * [2] coarse diff2 contraction, [3] coarse weights + significance + compaction,
+ * stream the stages ran on): [0] prep (+ proposal network), [1] tensor-core
+ * operand split (+ proposal audit) + norms, [2] coarse diff2 contraction (on the
+ * proposals when they are in use), [3] coarse weights + significance + compaction,
  * [4] fine pass, [5] fine weights, [6] weighted sums + backprojection.  n <= 7.
  * A batch that ran as a CUDA graph reports -1 for every stage. */
 int t2b_last_stage_ms(t2b_ctx* ctx, float* ms, int n);
+
+/* ---------------------------------------------------------------------------
+ * Learned orientation proposals (no counterpart in the reference).
+ *
+ * A network (8 lowest Fourier rings -> 16x16 image -> 2 conv + 3 dense layers,
+ * BF16 weights, FP32 accumulation) ranks the nr_classes*n_dir*n_psi coarse
+ * orientations of each particle; with proposals enabled the coarse pass runs
+ * on the top-k of each particle only and every later stage is unchanged.
+ * Every `audit_every`-th particle also gets the full coarse pass; if the
+ * proposals of an audited particle hold less than `audit_mass` of its coarse
+ * posterior, the whole batch runs the full coarse pass instead (decided on the
+ * device, inside the same launch sequence / CUDA graph).  Requires
+ * diff2_mode T2B_DIFF2_SPLIT_BF16 and nr_classes*n_dir*n_psi <= 49152.
+ * The network survives t2b_configure while nr_classes*n_dir*n_psi is
+ * unchanged; enabling must be repeated after every t2b_configure.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    int n_train;                /* synthetic training particles (e.g. 200000)              */
+    int n_posterior;            /* of those, labelled with the plain E-step posterior too  */
+    int n_val;                  /* held-out particles for the report                       */
+    int epochs, batch;          /* Adam epochs, minibatch (8..1024)                        */
+    float lr;                   /* Adam learning rate                                      */
+    int topk;                   /* proposals per particle for the report                   */
+    unsigned long long seed;
+    double defocus_min, defocus_max, astig_max;   /* Angstrom                              */
+    double voltage, cs, q0;     /* kV, mm, amplitude contrast                              */
+    double max_shift;           /* pixels, uniform in [-max_shift, max_shift]^2            */
+    double sigma_deg;           /* width of the geometric target around the true pose (8)  */
+    float alpha;                /* logit scale of the matched-filter initialisation (3)    */
+    const float* minvsigma2;    /* host, window (current_size x current_size/2+1): noise
+                                   model of the synthetic particles (1/sigma^2 per complex
+                                   component; 0 = no noise)                                */
+} t2b_proposal_train_config;
+
+typedef struct {
+    double loss[64];            /* mean training loss per epoch (first 64 epochs)          */
+    double val_mass_init;       /* mean posterior mass in the top-k of the initial network
+                                   (the matched filter of the references) before training */
+    double val_mass_trained;    /* ... after training                                      */
+    double val_mass_min;        /* smallest after training                                 */
+    double val_frac_999;        /* held-out particles with >= 0.999 of the mass in top-k   */
+    double val_true_hit;        /* held-out particles whose true orientation is in top-k   */
+    double gen_ms, label_ms, train_ms;
+    long long params;           /* network parameters                                      */
+} t2b_proposal_report;
+
+/* Generate the training set from the current references (projection, CTF,
+ * shift, noise), label it (true orientation; plain E-step posterior for
+ * n_posterior particles, which does not touch the backprojection grids),
+ * train with Adam on the device, and report the held-out posterior mass the
+ * top-k proposals hold before and after training.  Needs t2b_configure. */
+int t2b_proposal_train(t2b_ctx* ctx, const t2b_proposal_train_config* cfg, t2b_proposal_report* report);
+/* Enable (topk >= 1) or disable (topk = 0) proposals for the following batches. */
+int t2b_proposal_enable(t2b_ctx* ctx, int topk, int audit_every, double audit_mass);
+/* Network parameters as one flat FP32 vector (count: its length, layout in
+ * t2-relion_b200/proposal.py); get and/or set (NULL to skip); `set` also marks
+ * the network as trained. */
+int t2b_proposal_params(t2b_ctx* ctx, float* get, const float* set, long long* count);
+/* Feature images (n x 256) of a host batch. */
+int t2b_proposal_features(t2b_ctx* ctx, const t2b_batch* batch, float* imgs);
+/* Logits (n x nr_classes*n_dir*n_psi, bias included) of host feature images
+ * through the inference path (tensor-core dense layers). */
+int t2b_proposal_logits(t2b_ctx* ctx, const float* imgs, int n, float* logits);
+/* Loss (mean over the n samples) and its gradient with respect to every
+ * parameter (count floats) through the training kernels; targets: n x 9
+ * (orientation, weight) pairs, weights of a sample summing to 1, orientation
+ * -1 = unused.  Parameters are not updated. */
+int t2b_proposal_grad(t2b_ctx* ctx, const float* imgs, const int* tgt_oc, const float* tgt_w, int n, double* loss,
+                      float* grad);
 
 /* Host sampling (HealpixSampling, src/healpix_sampling.cpp:534-640,
  * 1787-2040), C1 symmetry, no perturbation.  Fills Euler matrices of the

@@ -37,6 +37,8 @@ ABI_SYMBOLS = (
     "t2b_estep_batch_host", "t2b_estep_batch_device", "t2b_reconstruct_divide",
     "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_last_stage_ms",
     "t2b_sampling", "t2b_reconstruct_divide_noalloc", "t2b_last_launch_count",
+    "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
+    "t2b_proposal_logits", "t2b_proposal_grad",
 )
 
 
@@ -83,7 +85,25 @@ class Result(ctypes.Structure):
     _fields_ = [(name, _p) for name in (
         "min_diff2", "sum_weight", "sig_weight", "coarse_sum_weight", "coarse_sig_weight",
         "nr_sign", "n_coarse_sig", "pmax", "pose", "wsum_norm", "sumw", "wsum_sigma2_offset",
-        "wsum_sigma2", "wsum_pdf_class", "wsum_pdf_dir", "status")]
+        "wsum_sigma2", "wsum_pdf_class", "wsum_pdf_dir", "status", "audit_mass", "learned")]
+
+
+class ProposalTrainConfig(ctypes.Structure):
+    _fields_ = [("n_train", ctypes.c_int), ("n_posterior", ctypes.c_int), ("n_val", ctypes.c_int),
+                ("epochs", ctypes.c_int), ("batch", ctypes.c_int), ("lr", ctypes.c_float),
+                ("topk", ctypes.c_int), ("seed", ctypes.c_ulonglong),
+                ("defocus_min", ctypes.c_double), ("defocus_max", ctypes.c_double),
+                ("astig_max", ctypes.c_double), ("voltage", ctypes.c_double), ("cs", ctypes.c_double),
+                ("q0", ctypes.c_double), ("max_shift", ctypes.c_double), ("sigma_deg", ctypes.c_double),
+                ("alpha", ctypes.c_float), ("minvsigma2", _p)]
+
+
+class ProposalReport(ctypes.Structure):
+    _fields_ = [("loss", ctypes.c_double * 64), ("val_mass_init", ctypes.c_double),
+                ("val_mass_trained", ctypes.c_double), ("val_mass_min", ctypes.c_double),
+                ("val_frac_999", ctypes.c_double), ("val_true_hit", ctypes.c_double),
+                ("gen_ms", ctypes.c_double), ("label_ms", ctypes.c_double), ("train_ms", ctypes.c_double),
+                ("params", ctypes.c_longlong)]
 
 
 def _setup_prototypes():
@@ -110,6 +130,12 @@ def _setup_prototypes():
     lib.t2b_last_launch_count.argtypes = [v, ctypes.POINTER(i)]
     lib.t2b_sampling.argtypes = [i, i, ctypes.c_double, i, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double] + [ctypes.POINTER(i)] * 5 + [v] * 6
+    lib.t2b_proposal_train.argtypes = [v, ctypes.POINTER(ProposalTrainConfig), ctypes.POINTER(ProposalReport)]
+    lib.t2b_proposal_enable.argtypes = [v, i, i, ctypes.c_double]
+    lib.t2b_proposal_params.argtypes = [v, v, v, ctypes.POINTER(ctypes.c_longlong)]
+    lib.t2b_proposal_features.argtypes = [v, ctypes.POINTER(Batch), v]
+    lib.t2b_proposal_logits.argtypes = [v, v, i, v]
+    lib.t2b_proposal_grad.argtypes = [v, v, v, v, i, ctypes.POINTER(ctypes.c_double), v]
 
 
 _setup_prototypes()
@@ -269,7 +295,7 @@ class EStep:
             pose=np.zeros((n, 5), np.int32), wsum_norm=np.zeros(n), sumw=np.zeros(n),
             wsum_sigma2_offset=np.zeros(n), wsum_sigma2=np.zeros((n, half)),
             wsum_pdf_class=np.zeros((n, K)), wsum_pdf_dir=np.zeros((n, K * nd)),
-            status=np.zeros(n, np.int32))
+            status=np.zeros(n, np.int32), audit_mass=np.zeros(n), learned=np.zeros(n, np.int32))
 
     # MlOptimiserCuda::doThreadExpectationSomeParticles for one batch (host buffers)
     def expectation(self, fimg, ctf, minvsigma2, scalars, fimg_nomask=None):
@@ -288,9 +314,71 @@ class EStep:
     def expectation_device(self, n, fimg_ptr, ctf_ptr, minv_ptr, scal_ptr, result_ptrs, stream=0,
                            fimg_nomask_ptr=None):
         b = Batch(n, 0, fimg_ptr, fimg_nomask_ptr, ctf_ptr, minv_ptr, scal_ptr)
-        r = Result(*[result_ptrs[name] for name, _ in Result._fields_])
+        r = Result(*[result_ptrs.get(name) for name, _ in Result._fields_])
         _check(lib.t2b_estep_batch_device(self._h, ctypes.byref(b), ctypes.byref(r),
                                           ctypes.c_void_p(stream)))
+
+    # ---------------------------------------------- learned orientation proposals
+    def train_proposals(self, minvsigma2, n_train=200000, n_posterior=20000, n_val=1024, epochs=4, batch=256,
+                        lr=3e-4, topk=64, seed=1, defocus=(10000., 30000.), astig=1000., voltage=300., cs=2.7,
+                        q0=0.1, max_shift=5.0, sigma_deg=8.0, alpha=3.0):
+        """Train the proposal network on particles generated from the current
+        references (t2b_proposal_train); returns the report as a dict."""
+        mv = np.ascontiguousarray(minvsigma2, np.float32)
+        c = ProposalTrainConfig(n_train, n_posterior, n_val, epochs, batch, lr, topk, seed, defocus[0], defocus[1],
+                                astig, voltage, cs, q0, max_shift, sigma_deg, alpha, _ptr(mv))
+        rep = ProposalReport()
+        _check(lib.t2b_proposal_train(self._h, ctypes.byref(c), ctypes.byref(rep)))
+        out = {k: getattr(rep, k) for k, _ in ProposalReport._fields_ if k != "loss"}
+        out["loss"] = list(rep.loss)[:min(epochs, 64)]
+        return out
+
+    def enable_proposals(self, topk=64, audit_every=50, audit_mass=0.999):
+        _check(lib.t2b_proposal_enable(self._h, topk, audit_every, audit_mass))
+
+    def disable_proposals(self):
+        _check(lib.t2b_proposal_enable(self._h, 0, 1, 1.0))
+
+    def proposal_params(self, set_to=None):
+        n = ctypes.c_longlong()
+        _check(lib.t2b_proposal_params(self._h, None, None, ctypes.byref(n)))
+        if set_to is not None:
+            v = np.ascontiguousarray(set_to, np.float32)
+            assert v.size == n.value
+            _check(lib.t2b_proposal_params(self._h, None, _ptr(v), ctypes.byref(n)))
+            return v
+        out = np.zeros(n.value, np.float32)
+        _check(lib.t2b_proposal_params(self._h, _ptr(out), None, ctypes.byref(n)))
+        return out
+
+    def proposal_features(self, fimg, ctf, minvsigma2):
+        fimg = np.ascontiguousarray(fimg, np.complex64)
+        ctf = np.ascontiguousarray(ctf, np.float32)
+        mv = np.ascontiguousarray(minvsigma2, np.float32)
+        n = fimg.shape[0]
+        b = Batch(n, 0, _ptr(fimg), None, _ptr(ctf), _ptr(mv), None)
+        out = np.zeros((n, 256), np.float32)
+        _check(lib.t2b_proposal_features(self._h, ctypes.byref(b), _ptr(out)))
+        return out
+
+    def proposal_logits(self, imgs):
+        imgs = np.ascontiguousarray(imgs, np.float32)
+        cfg = self.cfg
+        out = np.zeros((imgs.shape[0], cfg["nr_classes"] * cfg["n_dir"] * cfg["n_psi"]), np.float32)
+        _check(lib.t2b_proposal_logits(self._h, _ptr(imgs), imgs.shape[0], _ptr(out)))
+        return out
+
+    def proposal_grad(self, imgs, tgt_oc, tgt_w):
+        imgs = np.ascontiguousarray(imgs, np.float32)
+        to = np.ascontiguousarray(tgt_oc, np.int32)
+        tw = np.ascontiguousarray(tgt_w, np.float32)
+        n = ctypes.c_longlong()
+        _check(lib.t2b_proposal_params(self._h, None, None, ctypes.byref(n)))
+        g = np.zeros(n.value, np.float32)
+        loss = ctypes.c_double()
+        _check(lib.t2b_proposal_grad(self._h, _ptr(imgs), _ptr(to), _ptr(tw), imgs.shape[0], ctypes.byref(loss),
+                                     _ptr(g)))
+        return loss.value, g
 
     def launch_count(self):
         k = ctypes.c_int()

@@ -7,6 +7,7 @@
 // workspace per context and a fixed sequence of batched kernels with no host
 // synchronisation between the coarse pass and the backprojection.
 #include "t2b_internal.cuh"
+#include "proposal.cuh"
 #include <algorithm>
 #include <cstdint>
 #include <cmath>
@@ -17,24 +18,6 @@ namespace t2b {
 
 static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
-
-template <typename F>
-static int guarded(F&& f)
-{
-    try {
-        f();
-        return T2B_OK;
-    } catch (const Error& e) {
-        set_error(e.msg);
-        return e.code;
-    } catch (const std::bad_alloc&) {
-        set_error("host allocation failed");
-        return T2B_ERR_NOMEM;
-    } catch (const std::exception& e) {
-        set_error(e.what());
-        return T2B_ERR_ARG;
-    }
-}
 
 template <typename T>
 static T* dalloc(t2b_ctx* c, size_t n)
@@ -61,19 +44,6 @@ static void free_allocs(t2b_ctx* c)
     c->allocs.clear();
     c->configured = false;
 }
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev)
-    {
-        cudaGetDevice(&prev);
-        T2B_CUDA(cudaSetDevice(dev));
-    }
-    ~DeviceGuard()
-    {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
 
 static void check_volume(int ref_dim, int xdim, int ydim, int zdim, int inity, int initz, int r_max, int pad)
 {
@@ -124,6 +94,7 @@ void t2b_destroy(t2b_ctx* c)
         cudaSetDevice(c->device);
         cudaStreamSynchronize(c->stream);
         free_allocs(c);
+        proposal_release(c);
         for (auto p : c->mdl) cudaFree(p);
         for (auto p : c->gdata) cudaFree(p);
         for (auto p : c->gweight) cudaFree(p);
@@ -276,6 +247,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         DeviceGuard g(c->device);
         T2B_CUDA(cudaStreamSynchronize(c->stream));
         free_allocs(c);
+        proposal_invalidate(c);
         estep_init_attributes();
         if (f.diff2_mode == T2B_DIFF2_SPLIT_BF16) tc_init_attributes();
         c->cfg = f;
@@ -410,6 +382,8 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         w.counters = dalloc<unsigned long long>(c, 16);
         w.err = dalloc<int>(c, 1);
         w.status = dalloc<int>(c, B);
+        w.r_learned = dalloc<int>(c, B);
+        w.r_audit = dalloc<double>(c, B);
         // staging of host inputs and internal results
         w.fimg = dalloc<float2>(c, (size_t)B * P);
         w.fimg_nm = dalloc<float2>(c, (size_t)B * P);
@@ -447,7 +421,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             op.nl = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kn);
             op.wh = dalloc<uint16_t>(c, (size_t)op.b_pad * op.kn);
             op.wl = dalloc<uint16_t>(c, (size_t)op.b_pad * op.kn);
-            op.maps = dalloc<uint8_t>(c, 8 * 128);
+            op.maps = dalloc<uint8_t>(c, TC_MAP_SLOTS * 128);
             tc_prepare_projections(tb, op, st);
         }
         T2B_CUDA(cudaStreamSynchronize(st));
@@ -461,20 +435,36 @@ namespace t2b {
 
 // Enqueue the whole E-step of the batch in `w` on `st`.  Stage events are
 // recorded only outside stream capture (a captured batch is timed as a whole).
-static void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events = true)
+// With learned proposals enabled the network ranks the orientations, the
+// audit sets the device gate, and both coarse paths are enqueued: each of
+// their kernels runs or returns on the gate.
+void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool allow_prop)
 {
     const Tables& tb = c->tb;
+    const bool tc = c->cfg.diff2_mode == T2B_DIFF2_SPLIT_BF16;
+    const bool pm = allow_prop && tc && c->net && c->net->enabled && c->net->ready;
+    if (pm) {
+        w.gate = &c->net->ps->gate;
+        w.prop = c->net->prop;
+        w.kprop = c->net->kprop;
+    } else {
+        w.gate = nullptr;
+        w.prop = nullptr;
+        w.kprop = 0;
+    }
     T2B_CUDA(cudaMemsetAsync(w.counters, 0, 16 * sizeof(unsigned long long), st));
     T2B_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     if (stage_events) cudaEventRecord(c->ev[0], st);
-    const bool tc = c->cfg.diff2_mode == T2B_DIFF2_SPLIT_BF16;
     launch_prep(tb, w, st);
-    if (tc) tc_launch_norms(tb, w, c->tc, st);
-    else launch_norms(tb, w, st);
+    if (pm) proposal_infer(c, w, st);
     if (stage_events) cudaEventRecord(c->ev[1], st);
     if (tc) tc_split_images(tb, w, c->tc, st);
+    if (pm) proposal_audit(c, w, st);
+    if (tc) tc_launch_norms(tb, w, c->tc, st, w.gate, 0);
+    else launch_norms(tb, w, st);
     if (stage_events) cudaEventRecord(c->ev[2], st);
-    if (tc) tc_launch_diff2(tb, w, c->tc, st);
+    if (pm) proposal_coarse(c, w, st);
+    if (tc) tc_launch_diff2(tb, w, c->tc, st, w.gate, 0);
     else launch_diff2_simt(tb, w, st);
     if (stage_events) cudaEventRecord(c->ev[3], st);
     launch_weights_coarse(tb, w, c->cfg.maximum_significants, st);
@@ -525,7 +515,7 @@ int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
         T2B_CUDA(cudaMemcpyAsync((void*)w.ctf, b->ctf, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
         T2B_CUDA(cudaMemcpyAsync((void*)w.minv, b->minvsigma2, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
         T2B_CUDA(cudaMemcpyAsync((void*)w.scal, b->scalars, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, st));
-        enqueue_estep(c, w, st);
+        enqueue_estep(c, w, st, true, true);
         const int K = c->tb.K, half = c->cfg.ori_size / 2 + 1;
         auto d2h = [&](void* dst, const void* src, size_t bytes) {
             if (dst) T2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
@@ -546,6 +536,8 @@ int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
         d2h(r->wsum_pdf_class, w.r_pdf_class, (size_t)n * K * sizeof(double));
         d2h(r->wsum_pdf_dir, w.r_pdf_dir, (size_t)n * K * c->tb.n_dir * sizeof(double));
         d2h(r->status, w.status, n * sizeof(int));
+        d2h(r->learned, w.r_learned, n * sizeof(int));
+        d2h(r->audit_mass, w.r_audit, n * sizeof(double));
         T2B_CUDA(cudaStreamSynchronize(st));
         c->last_kernels = -1;
         collect_stage_ms(c);
@@ -577,19 +569,23 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
         w.r_norm = r->wsum_norm; w.r_sumw = r->sumw; w.r_sig_off = r->wsum_sigma2_offset;
         w.r_sigma2 = r->wsum_sigma2; w.r_pdf_class = r->wsum_pdf_class; w.r_pdf_dir = r->wsum_pdf_dir;
         w.status = r->status;
+        w.r_learned = r->learned;
+        w.r_audit = r->audit_mass;
         if (c->cfg.use_graph) {
             const std::vector<const void*> key = {(const void*)(intptr_t)b->n, b->fimg, b->fimg_nomask, b->ctf,
                                                   b->minvsigma2, b->scalars, r->min_diff2, r->sum_weight, r->sig_weight,
                                                   r->coarse_sum_weight, r->coarse_sig_weight, r->nr_sign,
                                                   r->n_coarse_sig, r->pmax, r->pose, r->wsum_norm, r->sumw,
                                                   r->wsum_sigma2_offset, r->wsum_sigma2, r->wsum_pdf_class,
-                                                  r->wsum_pdf_dir, r->status, (const void*)st};
+                                                  r->wsum_pdf_dir, r->status, r->learned, r->audit_mass,
+                                                  (const void*)st,
+                                                  (const void*)(intptr_t)(c->net && c->net->enabled ? c->net->kprop : 0)};
             if (!c->gexec || key != c->gkey) {
                 if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
                 cudaGraph_t graph = nullptr;
                 T2B_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                 try {
-                    enqueue_estep(c, w, st, false);
+                    enqueue_estep(c, w, st, false, true);
                 } catch (...) {
                     cudaStreamEndCapture(st, &graph);
                     if (graph) cudaGraphDestroy(graph);
@@ -615,7 +611,7 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
             T2B_CUDA(cudaGraphLaunch(c->gexec, st));
             c->last_kernels = c->graph_kernels;
         } else {
-            enqueue_estep(c, w, st);
+            enqueue_estep(c, w, st, true, true);
             c->last_kernels = -1;
         }
         c->last_n = b->n;

@@ -12,7 +12,8 @@
 // Kernel: persistent, one CTA per SM, 192 threads.
 //   warp 0      TMA producer: per 64-wide K block loads Ph, Pl (128 x 64) and
 //               Ih, Il (256 x 64) with 128-byte swizzle into a 2-stage ring
-//   warp 1      MMA issuer: 12 x tcgen05.mma (M128 N256 K16) per K block into a
+//   warp 1      MMA issuer: 12 x tcgen05.mma (M128 N256 K16) per K block (4 per
+//               product; the network GEMMs use one product, BF16 x BF16) into a
 //               double-buffered 2 x 256-column TMEM accumulator
 //   warps 2-5   epilogue: tcgen05.ld 32x32b, transpose through shared memory,
 //               diff2 = c0 + norm - C written coalesced along t, per-particle
@@ -24,6 +25,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <algorithm>
+#include <cstring>
 
 namespace t2b {
 namespace {
@@ -157,7 +159,7 @@ __device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, 
 
 struct TcParams {
     int m_tiles, n_tiles, kblocks;
-    int raw;                  // 1: store the contraction itself (norm GEMM), 0: diff2 epilogue
+    int raw;                  // 1: store the contraction itself (norm and network GEMMs), 0: diff2 epilogue
     int KO, T, ncols;
     const float* c0;
     const float* norms;
@@ -165,6 +167,15 @@ struct TcParams {
     float* d2c;
     unsigned* minkey;
     int* err;
+    int products;             // 1: hi.hi, 2: + hi(A).lo(B), 3: + lo(A).hi(B) (split-BF16)
+    // proposal tiles (mode 1): tile i holds particles [i*ppt, i*ppt + ppt); A rows
+    // [i*128, i*128+128) are their gathered proposals (kslot rows each, the first
+    // KO of them used), B rows from i*ppt*T are their shifted images; norms and
+    // d2c are per (particle, proposal); ncols = particles of the batch
+    int mode, ppt, kslot;
+    const int* prop;          // mode 1: global orientation of every (particle, proposal)
+    const int* gate;          // run only when (*gate != 0) == gate_run (null: always)
+    int gate_run;
 };
 
 // maps: device array of tensor-map descriptors (encoded once per configuration);
@@ -173,6 +184,7 @@ struct TcParams {
 __global__ void __launch_bounds__(NTHREADS, 1)
 k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
 {
+    if (p.gate && ((*p.gate != 0) != (p.gate_run != 0))) return;  // uniform: the whole CTA leaves
     const CUtensorMap* mPh = maps + ia;
     const CUtensorMap* mPl = maps + ia + 1;
     const CUtensorMap* mIh = maps + ib;
@@ -208,27 +220,38 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
 
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer
-        const CUtensorMap* ms[4] = {mPh, mPl, mIh, mIl};
-        for (int j = 0; j < 4; j++) {
+        // only the descriptors this launch reads (the lo slots may not exist)
+        const CUtensorMap* ms[4] = {mPh, mIh, mIl, mPl};
+        const int nmaps = 2 + (p.products >= 2 ? 1 : 0) + (p.products == 3 ? 1 : 0);
+        for (int j = 0; j < nmaps; j++) {
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(ms[j]) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(ms[j]) : "memory");
         }
         int it = 0;
         int issued[STAGES] = {0, 0};
         uint32_t last_par[STAGES] = {0, 0};
+        const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + B_BYTES * (p.products >= 2 ? 2u : 1u);
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
-            int mt, nt;
-            tile_coords(tile, p.m_tiles, p.n_tiles, mt, nt);
+            int ya, yb;
+            if (p.mode == 0) {
+                int mt, nt;
+                tile_coords(tile, p.m_tiles, p.n_tiles, mt, nt);
+                ya = mt * TM;
+                yb = nt * TN;
+            } else {
+                ya = tile * TM;
+                yb = tile * p.ppt * p.T;
+            }
             for (int kb = 0; kb < p.kblocks; kb++, it++) {
                 const int s = it % STAGES;
                 const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
                 if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
                 uint8_t* st = gbase + s * STAGE_BYTES;
-                mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-                tma_load(st, mPh, &full_bar[s], kb * TK, mt * TM);
-                tma_load(st + A_BYTES, mPl, &full_bar[s], kb * TK, mt * TM);
-                tma_load(st + 2 * A_BYTES, mIh, &full_bar[s], kb * TK, nt * TN);
-                tma_load(st + 2 * A_BYTES + B_BYTES, mIl, &full_bar[s], kb * TK, nt * TN);
+                mbar_expect_tx(&full_bar[s], tx_bytes);
+                tma_load(st, mPh, &full_bar[s], kb * TK, ya);
+                if (p.products == 3) tma_load(st + A_BYTES, mPl, &full_bar[s], kb * TK, ya);
+                tma_load(st + 2 * A_BYTES, mIh, &full_bar[s], kb * TK, yb);
+                if (p.products >= 2) tma_load(st + 2 * A_BYTES + B_BYTES, mIl, &full_bar[s], kb * TK, yb);
                 issued[s] = 1;
                 last_par[s] = ph;
             }
@@ -261,8 +284,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 for (int k = 0; k < TK / 16; k++) {
                     const uint64_t ko = (uint64_t)(k * 32) >> 4;  // 32 bytes per K=16 step
                     umma(dt, dPh + ko, dIh + ko, (kb | k) != 0);
-                    umma(dt, dPh + ko, dIl + ko, 1);
-                    umma(dt, dPl + ko, dIh + ko, 1);
+                    if (p.products >= 2) umma(dt, dPh + ko, dIl + ko, 1);
+                    if (p.products == 3) umma(dt, dPl + ko, dIh + ko, 1);
                 }
                 umma_commit(&empty_bar[s]);  // stage free once these MMAs retire
             }
@@ -281,14 +304,14 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         unsigned* wmin = smin + ew * (TN + 2);
         int tl = 0;
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x, tl++) {
-            int mt, nt;
-            tile_coords(tile, p.m_tiles, p.n_tiles, mt, nt);
+            int mt = 0, nt = 0;
+            if (p.mode == 0) tile_coords(tile, p.m_tiles, p.n_tiles, mt, nt);
             const int abuf = tl & 1;
             const uint32_t aph = (uint32_t)(tl >> 1) & 1u;
             if (!mbar_wait(&tfull_bar[abuf], aph, &abort_flag)) { abort_flag = 1; break; }
             tc_fence_after();
             const int n0 = nt * TN;
-            const int bfirst = n0 / p.T;
+            const int bfirst = p.mode == 0 ? n0 / p.T : tile * p.ppt;
             for (int i = lane; i < TN + 2; i += 32) wmin[i] = 0xffffffffu;
             __syncwarp();
             for (int c = 0; c < TN / 32; c++) {
@@ -297,28 +320,53 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
 #pragma unroll
                 for (int j = 0; j < 32; j++) sbuf[lane * EPI_LD + j] = __uint_as_float(v[j]);
                 __syncwarp();
-                // lane = column within the chunk; rows walk the warp's 32 TMEM lanes
-                const int col = n0 + c * 32 + lane;
-                const bool cok = col < p.ncols;
-                const int b = cok ? col / p.T : 0;
-                const int t = cok ? col - b * p.T : 0;
-                const float c0 = (cok && !p.raw) ? p.c0[b] : 0.f;  // raw mode has no c0 array
                 unsigned lmin = 0xffffffffu;
-                for (int r = 0; r < 32; r++) {
-                    const int oc = mt * TM + q * 32 + r;
-                    if (!cok || oc >= p.KO) continue;
-                    float d;
-                    if (p.raw) {
-                        d = sbuf[r * EPI_LD + lane];
-                    } else if (p.skip[oc]) {
-                        d = -999.f;
-                    } else {
-                        d = c0 + p.norms[(size_t)b * p.KO + oc] - sbuf[r * EPI_LD + lane];
-                        lmin = min(lmin, f2key(d));
+                int b;
+                if (p.mode == 0) {
+                    // lane = column within the chunk; rows walk the warp's 32 TMEM lanes
+                    const int col = n0 + c * 32 + lane;
+                    const bool cok = col < p.ncols;
+                    b = cok ? col / p.T : 0;
+                    const int t = cok ? col - b * p.T : 0;
+                    const float c0 = (cok && !p.raw) ? p.c0[b] : 0.f;  // raw mode has no c0 array
+                    for (int r = 0; r < 32; r++) {
+                        const int oc = mt * TM + q * 32 + r;
+                        if (!cok || oc >= p.KO) continue;
+                        float d;
+                        if (p.raw) {
+                            d = sbuf[r * EPI_LD + lane];
+                        } else if (p.skip[oc]) {
+                            d = -999.f;
+                        } else {
+                            d = c0 + p.norms[(size_t)b * p.KO + oc] - sbuf[r * EPI_LD + lane];
+                            lmin = min(lmin, f2key(d));
+                        }
+                        p.d2c[((size_t)b * p.KO + oc) * p.T + t] = d;
                     }
-                    p.d2c[((size_t)b * p.KO + oc) * p.T + t] = d;
+                } else {
+                    // proposal tile: column -> (particle slot, translation), row -> (slot, proposal)
+                    const int col = c * 32 + lane;
+                    const int bc = col / p.T;
+                    const int t = col - bc * p.T;
+                    b = bfirst + bc;
+                    const bool cok = bc < p.ppt && b < p.ncols;
+                    const float c0 = cok ? p.c0[b] : 0.f;
+                    for (int r = 0; r < 32; r++) {
+                        const int row = q * 32 + r;
+                        const int bp = row / p.kslot, j = row - bp * p.kslot;
+                        if (!cok || bp != bc || j >= p.KO) continue;
+                        const size_t pj = (size_t)b * p.KO + j;
+                        float d;
+                        if (p.skip[p.prop[pj]]) {
+                            d = -999.f;
+                        } else {
+                            d = c0 + p.norms[pj] - sbuf[r * EPI_LD + lane];
+                            lmin = min(lmin, f2key(d));
+                        }
+                        p.d2c[pj * p.T + t] = d;
+                    }
                 }
-                if (cok && lmin != 0xffffffffu) atomicMin(&wmin[b - bfirst], lmin);
+                if (lmin != 0xffffffffu) atomicMin(&wmin[b - bfirst], lmin);
                 __syncwarp();
             }
             tc_fence_before();
@@ -326,7 +374,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             if (lane == 0) mbar_arrive(&tempty_bar[abuf]);
             for (int i = lane; i < TN + 2; i += 32) {
                 const int b = bfirst + i;
-                if (wmin[i] != 0xffffffffu && b * p.T < p.ncols) atomicMin(&p.minkey[b], wmin[i]);
+                if (wmin[i] != 0xffffffffu && (p.mode == 0 ? b * p.T < p.ncols : b < p.ncols))
+                    atomicMin(&p.minkey[b], wmin[i]);
             }
             __syncwarp();
         }
@@ -461,13 +510,22 @@ bool tc_supported() { return true; }
 size_t tc_kdim(int nk) { return (size_t)((2 * nk + TK - 1) / TK) * TK; }
 size_t tc_kn(int nk) { return (size_t)((nk + TK - 1) / TK) * TK; }
 
-// descriptor slots in op.maps
-enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL, MAP_COUNT };
+// descriptor slots in op.maps (TC_MAP_SLOTS of 128 bytes)
+enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL,
+       MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_COUNT };
+static_assert(MAP_COUNT <= TC_MAP_SLOTS, "tensor-map slots");
+static_assert(sizeof(CUtensorMap) == 128, "tensor-map size");
+
+void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128)
+{
+    const CUtensorMap m = make_map(ptr, rows, kdim, a_side ? TM : TN);
+    std::memcpy(out128, &m, sizeof(m));
+}
 
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
 {
     T2B_REQUIRE(op.maps, T2B_ERR_STATE, "tensor-map buffer not allocated");
-    CUtensorMap h[MAP_COUNT];
+    CUtensorMap h[MAP_WL + 1];
     h[MAP_PH] = make_map(op.bh, op.m_pad, op.kdim, TM);
     h[MAP_PL] = make_map(op.bl, op.m_pad, op.kdim, TM);
     h[MAP_IH] = make_map(op.ah, op.n_pad, op.kdim, TN);
@@ -477,7 +535,7 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
     h[MAP_WH] = make_map(op.wh, op.b_pad, op.kn, TN);
     h[MAP_WL] = make_map(op.wl, op.b_pad, op.kn, TN);
     T2B_CUDA(cudaStreamSynchronize(st));
-    T2B_CUDA(cudaMemcpy(op.maps, h, sizeof(h), cudaMemcpyHostToDevice));
+    T2B_CUDA(cudaMemcpy(op.maps, h, sizeof(h), cudaMemcpyHostToDevice));  // slots MAP_PH..MAP_WL
     const int rows = tb.K * tb.O;
     // sizes were fixed when the operand buffers were allocated
     T2B_REQUIRE(op.m_pad == (rows + TM - 1) / TM * TM && op.kdim == (int)tc_kdim(tb.nk), T2B_ERR_STATE,
@@ -508,7 +566,7 @@ static void launch_gemm(const TcOperands& op, int ia, int ib, TcParams& p, cudaS
 }
 
 // N[b][oc] = sum_p w2[b][p] |P_oc[p]|^2 with the same split-BF16 tensor-core kernel
-void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st)
+void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate, int gate_run)
 {
     const int b_pad = (w.n + TN - 1) / TN * TN;
     T2B_REQUIRE(b_pad <= op.b_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
@@ -527,6 +585,9 @@ void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     p.d2c = w.norms;
     p.minkey = w.minkey_c;
     p.err = w.err;
+    p.products = 3;
+    p.gate = gate;
+    p.gate_run = gate_run;
     launch_gemm(op, MAP_NH, MAP_WH, p, st);
 }
 
@@ -541,7 +602,7 @@ void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     T2B_CUDA(cudaGetLastError());
 }
 
-void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st)
+void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate, int gate_run)
 {
     const int ncols = w.n * tb.T;
     const int n_pad = (ncols + TN - 1) / TN * TN;
@@ -560,7 +621,98 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     p.d2c = w.d2c;
     p.minkey = w.minkey_c;
     p.err = w.err;
+    p.products = 3;
+    p.gate = gate;
+    p.gate_run = gate_run;
     launch_gemm(op, MAP_PH, MAP_IH, p, st);
+}
+
+void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_side)
+{
+    T2B_REQUIRE(slot >= MAP_PGH && slot < MAP_COUNT && op.maps, T2B_ERR_STATE, "bad tensor-map slot");
+    unsigned char blob[128];
+    tc_encode(ptr, rows, kdim, a_side, blob);
+    T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * slot, blob, 128, cudaMemcpyHostToDevice));
+}
+
+int tc_slot_proposals() { return MAP_PGH; }
+int tc_slot_audit() { return MAP_IAH; }
+
+// Restricted coarse pass: every particle against its own proposals only.
+// Tiles of ppt particles: A = gathered proposal projections (slots MAP_PGH/PGL,
+// 128 rows per tile), B = the particles' shifted images (MAP_IH/IL, rows from
+// tile*ppt*T).  Runs while *w.gate != 0.
+void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, const float* nprop,
+                    cudaStream_t st)
+{
+    T2B_REQUIRE(ppt >= 1 && ppt * kslot == TM && ppt * tb.T <= TN && w.kprop <= kslot, T2B_ERR_STATE,
+                "proposal tile shape");
+    TcParams p{};
+    p.mode = 1;
+    p.ppt = ppt;
+    p.kslot = kslot;
+    p.m_tiles = (w.n + ppt - 1) / ppt;
+    p.n_tiles = 1;
+    p.kblocks = op.kdim / TK;
+    p.KO = w.kprop;
+    p.T = tb.T;
+    p.ncols = w.n;
+    p.c0 = w.c0;
+    p.norms = nprop;
+    p.skip = tb.skip;
+    p.prop = w.prop;
+    p.d2c = w.d2c;
+    p.minkey = w.minkey_c;
+    p.err = w.err;
+    p.products = 3;
+    p.gate = w.gate;
+    p.gate_run = 1;
+    launch_gemm(op, MAP_PGH, MAP_IH, p, st);
+}
+
+// Full coarse pass of the audited particles: dense tiles over every
+// orientation against the audit image operand (MAP_IAH/IAL, na_max*T rows).
+void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
+                     unsigned* minkeya, int* err, cudaStream_t st)
+{
+    TcParams p{};
+    p.m_tiles = op.m_pad / TM;
+    p.n_tiles = (na_max * tb.T + TN - 1) / TN;
+    p.kblocks = op.kdim / TK;
+    p.KO = tb.K * tb.O;
+    p.T = tb.T;
+    p.ncols = na_max * tb.T;
+    p.c0 = c0a;
+    p.norms = norma;
+    p.skip = tb.skip;
+    p.d2c = d2a;
+    p.minkey = minkeya;
+    p.err = err;
+    p.products = 3;
+    launch_gemm(op, MAP_PH, MAP_IAH, p, st);
+}
+
+// out[n][m] = sum_k A[m][k] B[n][k]: both operands K-major BF16 behind the
+// tensor maps maps[ia] (A, 128-row box) and maps[ib] (B, 256-row box); K a
+// multiple of 64; products = 1 is one BF16 product (the lo halves are not read).
+void tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* out, int products, int* err,
+                 cudaStream_t st)
+{
+    T2B_REQUIRE(K % TK == 0 && M > 0 && N > 0 && products >= 1 && products <= 3, T2B_ERR_ARG, "tensor-core GEMM shape");
+    TcParams p{};
+    p.m_tiles = (M + TM - 1) / TM;
+    p.n_tiles = (N + TN - 1) / TN;
+    p.kblocks = K / TK;
+    p.raw = 1;
+    p.KO = M;
+    p.T = 1;
+    p.ncols = N;
+    p.d2c = out;
+    p.err = err;
+    p.products = products;
+    const int grid = std::min(sms(), p.m_tiles * p.n_tiles);
+    k_diff2_tc<<<grid, NTHREADS, SMEM_BYTES, st>>>(static_cast<const CUtensorMap*>(maps), ia, ib, p);
+    T2B_CUDA(cudaGetLastError());
 }
 
 }  // namespace t2b

@@ -331,10 +331,30 @@ __device__ __forceinline__ double coarse_weight_ot(const Tables& tb, const Work&
     return tb.pdf_oc[oc] * w.pdf_t[(size_t)b * tb.T + t] * exp(-dd);
 }
 
-__device__ __forceinline__ double coarse_weight(const Tables& tb, const Work& w, int b, long long il, float d, double mn)
+// Learned proposals: while *w.gate != 0 the coarse arrays of particle b hold
+// kprop x T elements, proposal j being the global orientation w.prop[b*kprop+j];
+// otherwise K*O x T elements in global orientation order.
+__device__ __forceinline__ bool prop_mode(const Work& w) { return w.gate && *w.gate != 0; }
+__device__ __forceinline__ long long coarse_n(const Tables& tb, const Work& w, bool pm)
+{
+    return pm ? (long long)w.kprop * tb.T : (long long)tb.K * tb.O * tb.T;
+}
+__device__ __forceinline__ long long glob_oc(const Work& w, int b, long long oc, bool pm)
+{
+    return pm ? (long long)w.prop[(size_t)b * w.kprop + oc] : oc;
+}
+__device__ __forceinline__ long long glob_il(const Tables& tb, const Work& w, int b, long long il, bool pm)
+{
+    if (!pm) return il;
+    const long long j = il / tb.T;
+    return glob_oc(w, b, j, true) * tb.T + (il - j * tb.T);
+}
+
+__device__ __forceinline__ double coarse_weight(const Tables& tb, const Work& w, int b, long long il, float d, double mn,
+                                                bool pm)
 {
     const long long oc = il / tb.T;
-    return coarse_weight_ot(tb, w, b, oc, (int)(il - oc * tb.T), d, mn);
+    return coarse_weight_ot(tb, w, b, glob_oc(w, b, oc, pm), (int)(il - oc * tb.T), d, mn);
 }
 
 // (orientation, translation) of consecutive coarse elements without divisions
@@ -382,7 +402,7 @@ __device__ __forceinline__ Seg seg_of(const Tables& tb, const Work& w, bool fine
     Seg s;
     if (!fine) {
         s.beg = 0;
-        s.end = (long long)tb.K * tb.O * tb.T;
+        s.end = coarse_n(tb, w, prop_mode(w));
     } else {
         const long long rv = (long long)tb.R * tb.V;
         s.beg = w.pair_off[b] * rv;
@@ -432,6 +452,7 @@ __global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
     for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
     __syncthreads();
     const Seg sg = seg_of(tb, w, fine, b);
+    const bool pm = !fine && prop_mode(w);
     const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
     const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
     const double tau = hist_floor(tb, w, b, sg.end - sg.beg);
@@ -461,7 +482,7 @@ __global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
                 }
                 w.wf[i] = wt;
             } else {
-                if (d >= 0.f && (double)d - mn <= cut) wt = coarse_weight_ot(tb, w, b, ot.oc, ot.t, d, mn);
+                if (d >= 0.f && (double)d - mn <= cut) wt = coarse_weight_ot(tb, w, b, glob_oc(w, b, ot.oc, pm), ot.t, d, mn);
                 ot.next(tb.T);
             }
             if (wt > 0.) {
@@ -600,6 +621,7 @@ __global__ void __launch_bounds__(256) k_hist_level(Tables tb, Work w, int fine)
     for (int i = threadIdx.x; i < nb; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
     __syncthreads();
     const Seg sg = seg_of(tb, w, fine, b);
+    const bool pm = !fine && prop_mode(w);
     const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
     const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
     const int sw = shift + width;
@@ -623,7 +645,7 @@ __global__ void __launch_bounds__(256) k_hist_level(Tables tb, Work w, int fine)
             } else {
                 const double dd = (double)v[j];
                 if (v[j] < 0.f || dd <= lo || dd > hi) continue;
-                wt = coarse_weight_ot(tb, w, b, oc, t, v[j], mn);
+                wt = coarse_weight_ot(tb, w, b, glob_oc(w, b, oc, pm), t, v[j], mn);
             }
             if (!(wt > 0.)) continue;
             const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
@@ -649,6 +671,7 @@ __global__ void __launch_bounds__(256) k_gather(Tables tb, Work w, int fine)
     const int shift = sel->shift;
     const unsigned long long prefix = sel->prefix;
     const Seg sg = seg_of(tb, w, fine, b);
+    const bool pm = !fine && prop_mode(w);
     const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
     const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
     double lo, hi;
@@ -671,7 +694,7 @@ __global__ void __launch_bounds__(256) k_gather(Tables tb, Work w, int fine)
             } else {
                 const double dd = (double)v[j];
                 if (v[j] < 0.f || dd <= lo || dd > hi) continue;
-                wt = coarse_weight_ot(tb, w, b, oc, t, v[j], mn);
+                wt = coarse_weight_ot(tb, w, b, glob_oc(w, b, oc, pm), t, v[j], mn);
             }
             if (!(wt > 0.)) continue;
             const unsigned long long bits = (unsigned long long)__double_as_longlong(wt);
@@ -750,6 +773,7 @@ __global__ void __launch_bounds__(256) k_gather_fast(Tables tb, Work w, int fine
     SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
     if (sel->phase != 4) return;
     const Seg sg = seg_of(tb, w, fine, b);
+    const bool pm = !fine && prop_mode(w);
     const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
     const float* dsrc = fine ? w.d2f : w.d2c + (size_t)b * (size_t)(sg.end - sg.beg);
     const double wlo = fmax(bits2d(sel->prefix << 52), hist_floor(tb, w, b, sg.end - sg.beg));
@@ -774,7 +798,7 @@ __global__ void __launch_bounds__(256) k_gather_fast(Tables tb, Work w, int fine
                 wt = w.wf[i];
             } else {
                 if (v[j] < 0.f || (double)v[j] > hi) continue;
-                wt = coarse_weight_ot(tb, w, b, oc, t, v[j], mn);
+                wt = coarse_weight_ot(tb, w, b, glob_oc(w, b, oc, pm), t, v[j], mn);
             }
             if (!(wt >= wlo) || !(wt > 0.)) continue;
             const long long pos = atomicAdd((unsigned long long*)&sel->ncand, 1ull);
@@ -869,14 +893,15 @@ __global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass
 }
 
 // copy the fast-path significant lists to their place in the batch pair list
-__global__ void __launch_bounds__(256) k_write_fast(Work w, int gather_final)
+__global__ void __launch_bounds__(256) k_write_fast(Tables tb, Work w, int gather_final)
 {
     const int b = blockIdx.x;
     const SelState* sel = &w.sel_c[b];
     if (!sel->fast || sel->phase != 2 || w.status[b] != T2B_OK) return;
+    const bool pm = prop_mode(w);
     const long long beg = w.pair_off[b], m = w.pair_off[b + 1] - beg;
     for (long long i = threadIdx.x; i < m; i += blockDim.x) {
-        w.pairs[beg + i] = w.flist_i[(size_t)b * FAST_CAP + i];
+        w.pairs[beg + i] = glob_il(tb, w, b, w.flist_i[(size_t)b * FAST_CAP + i], pm);
         w.pair_b[beg + i] = b;
         if (gather_final) w.wf[beg + i] = w.flist_w[(size_t)b * FAST_CAP + i];
     }
@@ -889,6 +914,7 @@ constexpr int CHUNK = 4096;
 // inside the ambiguous diff2 window
 struct SigPred {
     double mn, thr, acc, rej;
+    bool pm;
     __device__ bool operator()(const Tables& tb, const Work& w, int b, long long i, float d, double* wout) const
     {
         if (d < 0.f) return false;
@@ -896,7 +922,7 @@ struct SigPred {
         if (dd - mn > 700.) return false;
         if (dd > rej) return false;
         if (dd <= acc && !wout) return true;
-        const double wt = coarse_weight(tb, w, b, i, d, mn);
+        const double wt = coarse_weight(tb, w, b, i, d, mn, pm);
         if (wout) *wout = wt;
         return wt >= thr;
     }
@@ -910,6 +936,7 @@ __device__ __forceinline__ SigPred sig_pred(const Work& w, int b)
     const double lt = log(p.thr);
     p.acc = w.lbound[2 * b] > -INFINITY ? p.mn + w.lbound[2 * b] - lt - WIN_EPS : -INFINITY;
     p.rej = p.mn + w.lbound[2 * b + 1] - lt + WIN_EPS;
+    p.pm = prop_mode(w);
     return p;
 }
 
@@ -921,10 +948,10 @@ __global__ void __launch_bounds__(256) k_count_sig(Tables tb, Work w)
     const int b = blockIdx.y;
     const SelState* sel = &w.sel_c[b];
     if (sel->phase != 2 || w.status[b] != T2B_OK || sel->fast) return;
-    const long long n = (long long)tb.K * tb.O * tb.T;
+    const SigPred pred = sig_pred(w, b);
+    const long long n = coarse_n(tb, w, pred.pm);
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
     const float* dsrc = w.d2c + (size_t)b * (size_t)n;
-    const SigPred pred = sig_pred(w, b);
     const unsigned long long maxbits = sel->maxbits;
     const double wmax = __longlong_as_double((long long)maxbits);
     double alo, ahi;
@@ -942,7 +969,7 @@ __global__ void __launch_bounds__(256) k_count_sig(Tables tb, Work w)
             if (pred(tb, w, b, i, d, nullptr)) local++;
             const double dd = (double)d;
             if (dd > alo && dd <= ahi) {
-                const double wt = coarse_weight(tb, w, b, i, d, pred.mn);
+                const double wt = coarse_weight(tb, w, b, i, d, pred.mn, pred.pm);
                 if ((unsigned long long)__double_as_longlong(wt) == maxbits) atomicMin((long long*)&w.sel_c[b].argmax, i);
             }
         }
@@ -963,7 +990,7 @@ __global__ void __launch_bounds__(1024) k_scan_chunks(Tables tb, Work w)
 {
     __shared__ long long sh[1024];
     const int b = blockIdx.x;
-    const long long n = (long long)tb.K * tb.O * tb.T;
+    const long long n = coarse_n(tb, w, prop_mode(w));
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
     if (w.sel_c[b].fast) return;  // list and count come from the fast path
     const bool active = w.sel_c[b].phase == 2 && w.status[b] == T2B_OK;
@@ -1038,10 +1065,10 @@ __global__ void __launch_bounds__(256) k_compact(Tables tb, Work w, int gather_f
     const int b = blockIdx.y;
     const SelState* sel = &w.sel_c[b];
     if (sel->phase != 2 || w.status[b] != T2B_OK || sel->fast) return;
-    const long long n = (long long)tb.K * tb.O * tb.T;
+    const SigPred pred = sig_pred(w, b);
+    const long long n = coarse_n(tb, w, pred.pm);
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
     const float* dsrc = w.d2c + (size_t)b * (size_t)n;
-    const SigPred pred = sig_pred(w, b);
     const long long pbase = w.pair_off[b], pend = w.pair_off[b + 1];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int c = blockIdx.x; c < nch; c += gridDim.x) {
@@ -1068,9 +1095,9 @@ __global__ void __launch_bounds__(256) k_compact(Tables tb, Work w, int gather_f
         for (int j = 0; j < 16; j++) {
             if (!(flags & (1u << j))) continue;
             if (pos < pend) {
-                w.pairs[pos] = i0 + j;
+                w.pairs[pos] = glob_il(tb, w, b, i0 + j, pred.pm);
                 w.pair_b[pos] = b;
-                if (gather_final) w.wf[pos] = coarse_weight(tb, w, b, i0 + j, v[j], pred.mn);
+                if (gather_final) w.wf[pos] = coarse_weight(tb, w, b, i0 + j, v[j], pred.mn, pred.pm);
             }
             pos++;
         }
@@ -1287,7 +1314,7 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                             nacc += wd;
                         }
                         // backprojection of this pixel (src/backprojector.cpp:140-228)
-                        if (fw > 0.f) {
+                        if (fw > 0.f && !w.no_bp) {
                             const int i = n / xh, x = n - i * xh;
                             const int y = (i < xh) ? i : i - s;
                             if (i >= xh && x == 0) continue;
@@ -1354,6 +1381,7 @@ __global__ void k_results(Tables tb, Work w)
     if (b >= w.n) return;
     const SelState& sc = w.sel_c[b];
     const SelState& sf = tb.ovs ? w.sel_f[b] : w.sel_c[b];
+    if (w.r_learned) w.r_learned[b] = prop_mode(w) ? 1 : 0;
     w.r_csum[b] = w.sum_c[b];
     w.r_csig[b] = sc.thr;
     w.r_nsign[b] = sc.nr_sign;
@@ -1370,7 +1398,8 @@ __global__ void k_results(Tables tb, Work w)
         return;
     }
     const long long am = sf.argmax;
-    const long long nfinal = tb.ovs ? (w.pair_off[w.n] * tb.R * tb.V) : (long long)tb.K * tb.O * tb.T;
+    const bool pm = prop_mode(w);
+    const long long nfinal = tb.ovs ? (w.pair_off[w.n] * tb.R * tb.V) : coarse_n(tb, w, pm);
     if (am < 0 || am >= nfinal) {  // the maximum was not located: report, do not index
         w.status[b] = T2B_ERR_NOSIGNIF;
         w.r_pmax[b] = -1.;
@@ -1387,7 +1416,7 @@ __global__ void k_results(Tables tb, Work w)
         v = (int)(am % tb.V);
         ih = w.pairs[q];
     } else {
-        ih = am;
+        ih = glob_il(tb, w, b, am, pm);
     }
     const int oc = (int)(ih / tb.T);
     pose[0] = oc / tb.O;
@@ -1539,7 +1568,7 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
     k_scan_chunks<<<w.n, 1024, 0, st>>>(tb, w);
     k_pair_offsets<<<1, 1024, 0, st>>>(w);
     k_compact<<<gc, 256, 0, st>>>(tb, w, tb.ovs ? 0 : 1);
-    k_write_fast<<<w.n, 256, 0, st>>>(w, tb.ovs ? 0 : 1);
+    k_write_fast<<<w.n, 256, 0, st>>>(tb, w, tb.ovs ? 0 : 1);
     T2B_CUDA(cudaGetLastError());
 }
 

@@ -1,0 +1,74 @@
+// Learned orientation proposals: shared constants and state (internal).
+#pragma once
+#include "t2b_internal.cuh"
+
+namespace t2b {
+
+constexpr int NET_NPIX = 256;      // 16 x 16 feature image
+constexpr int NET_C1 = 16, NET_C2 = 32;
+constexpr int NET_H0 = 2048, NET_H1 = 1024, NET_H2 = 1024;
+constexpr int NET_RING = 8;        // Fourier rings read by the network
+constexpr int NET_MAX_RING = 512;  // ring pixels of the window (|k| <= 8: 145)
+constexpr int NET_NPOST = 8;       // posterior labels kept per training particle
+constexpr int NET_NTGT = 1 + NET_NPOST;
+constexpr int NET_TOPK_CAND = 2048;
+constexpr int NET_MAX_KO = 49152;  // logits of one particle held in shared memory by the top-k
+
+// offsets (elements) of the parameters in the flat FP32 / BF16 vectors;
+// w3 last, with zero rows up to a multiple of 128 for the tensor-core operand
+struct NetLayout {
+    size_t wc1, bc1, wc2, bc2, b1, b2, b3, w1, w2, w3, total, alloc;
+    int KO, KOpad;
+};
+NetLayout net_layout(int KO);
+
+struct PropState {        // device
+    int gate;             // 1: the batch's coarse pass runs on the proposals
+    int na;               // audited particles of the batch
+    long long seen;       // particles of the stream so far
+};
+
+struct GenParams {
+    unsigned long long seed;
+    double dmin, dmax, astig, kv, cs, q0, angpix, max_shift;
+    const float* minv;    // device, P: noise model (1/sigma^2 per pixel, 0 = no noise)
+};
+
+struct ProposalNet {
+    NetLayout L{};
+    int KO = 0;
+    bool trained = false;
+    long long adam_t = 0;
+    std::vector<void*> owned;          // parameters and optimiser state
+    std::vector<void*> ws;             // per-configuration workspace below
+    float *th = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    void* thb = nullptr;               // BF16 copy of th (every forward pass reads it)
+    bool ready = false;                // workspace matches the configuration
+    bool enabled = false;
+    int kprop = 64, every = 50, na_max = 0, ppt = 1, kslot = 128, b_pad = 0;
+    double thr = 0.999;
+    int nring = 0;
+    int *ring = nullptr, *ring_k = nullptr;
+    float* img = nullptr;
+    void *x0b = nullptr, *h1b = nullptr, *h2b = nullptr;
+    float *y1 = nullptr, *y2 = nullptr, *logits = nullptr;
+    int* prop = nullptr;
+    void* maps = nullptr;              // 6 tensor maps: W1, X0b, W2, H1b, W3, H2b
+    void *pg_h = nullptr, *pg_l = nullptr;
+    float* nprop = nullptr;
+    PropState* ps = nullptr;
+    int* audit_b = nullptr;
+    void *ia_h = nullptr, *ia_l = nullptr;
+    float *w2a = nullptr, *c0a = nullptr, *norma = nullptr, *d2a = nullptr;
+    unsigned* minkeya = nullptr;
+    double* asum = nullptr;
+};
+
+// inference, audit and restricted coarse pass of one batch (proposal.cu)
+void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st);
+void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st);
+void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st);
+void proposal_release(t2b_ctx* c);    // context destruction
+void proposal_invalidate(t2b_ctx* c); // configuration changed
+
+}  // namespace t2b

@@ -4,11 +4,15 @@
 #include <cstdint>
 #include <cstddef>
 #include <mutex>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 #include "../../include/t2b.h"
 
 namespace t2b {
+
+struct ProposalNet;
 
 // ---------------------------------------------------------------- errors
 void set_error(const std::string& msg);
@@ -29,6 +33,38 @@ struct Error {
     do {                                                                                     \
         if (!(cond)) throw ::t2b::Error{(code), (msg)};                                      \
     } while (0)
+
+// Run f, turning exceptions into status codes and the thread's error message.
+template <typename F>
+inline int guarded(F&& f)
+{
+    try {
+        f();
+        return T2B_OK;
+    } catch (const Error& e) {
+        set_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return T2B_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return T2B_ERR_ARG;
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        T2B_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
 
 // ------------------------------------------------------------- geometry
 struct Volume {           // projector model or backprojection grid
@@ -121,6 +157,13 @@ struct Work {
     unsigned long long* counters; // queue heads etc. (16)
     int* err;                 // device error flag of bounded waits (T2B_ERR_TIMEOUT)
     int* status;              // n
+    // learned orientation proposals (gate == nullptr: every orientation is evaluated)
+    const int* gate;          // device flag: != 0 while the coarse pass runs on the proposals only
+    const int* prop;          // n x kprop: global orientation of each proposal (ranked)
+    int kprop;
+    int no_bp;                // 1: weighted sums only, the grids are not touched
+    int* r_learned;           // n (optional): 1 if the particle's coarse pass used the proposals
+    double* r_audit;          // n (optional): posterior mass in the proposals (audited), else -1
     // results (device)
     double *r_min, *r_sum, *r_sig, *r_csum, *r_csig, *r_pmax;
     long long *r_nsign, *r_ncsig;
@@ -160,17 +203,36 @@ struct TcOperands {
     void* wl;
     int m_pad, n_pad, kdim;   // padded sizes of the cross-term operands
     int kn, b_pad;            // padded sizes of the norm operands
-    void* maps;               // 8 CUtensorMap descriptors (128 B each) in device memory
+    void* maps;               // TC_MAP_SLOTS CUtensorMap descriptors (128 B each) in device memory
 };
+constexpr int TC_MAP_SLOTS = 16;
 size_t tc_kdim(int nk);
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
-void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
+void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate = nullptr,
+                     int gate_run = 0);
 size_t tc_kn(int nk);
-void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
+void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate = nullptr,
+                     int gate_run = 0);
 bool tc_supported();
+void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128);
+void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_side);
+int tc_slot_proposals();
+int tc_slot_audit();
+void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, const float* nprop,
+                    cudaStream_t st);
+void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
+                     unsigned* minkeya, int* err, cudaStream_t st);
+void tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* out, int products, int* err,
+                 cudaStream_t st);
 
 }  // namespace t2b
+
+namespace t2b {
+// Enqueue one E-step of the batch in `w` (api.cu); allow_prop = false forces the
+// full coarse pass even while proposals are enabled.
+void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool allow_prop);
+}
 
 struct t2b_ctx {
     int device = 0;
@@ -196,4 +258,5 @@ struct t2b_ctx {
     int last_kernels = -1;
     cudaEvent_t ev[8]{};
     float stage_ms[7]{};
+    t2b::ProposalNet* net = nullptr;          // learned orientation proposals (proposal.cu)
 };
