@@ -417,8 +417,7 @@ __global__ void __launch_bounds__(256) k_audit_mass(Tables tb, Work w, const Pro
 
 __global__ void k_audit_final(PropState* ps, const int* audit_b, const double* asum, double thr, double* r_audit)
 {
-    const int a = threadIdx.x;
-    if (a < ps->na) {
+    for (int a = threadIdx.x; a < ps->na; a += blockDim.x) {
         const double m = asum[2 * a] > 0. ? asum[2 * a + 1] / asum[2 * a] : 0.;
         if (r_audit) r_audit[audit_b[a]] = m;
         if (!(m >= thr)) atomicExch(&ps->gate, 0);
