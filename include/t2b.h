@@ -213,8 +213,10 @@ int t2b_last_stage_ms(t2b_ctx* ctx, float* ms, int n);
  *
  * A network (8 lowest Fourier rings -> 16x16 image -> 2 conv + 3 dense layers,
  * BF16 weights, FP32 accumulation) ranks the nr_classes*n_dir*n_psi coarse
- * orientations of each particle; with proposals enabled the coarse pass runs
- * on the top-k of each particle only and every later stage is unchanged.
+ * orientations of each particle (optionally followed by an exact
+ * low-resolution rescoring of its best candidates); with proposals enabled the
+ * coarse pass runs on the top-k of each particle only and every later stage is
+ * unchanged.
  * Every `audit_every`-th particle also gets the full coarse pass; if the
  * proposals of an audited particle hold less than `audit_mass` of its coarse
  * posterior, the whole batch runs the full coarse pass instead (decided on the
@@ -230,6 +232,8 @@ typedef struct {
     int epochs, batch;          /* Adam epochs, minibatch (8..1024)                        */
     float lr;                   /* Adam learning rate                                      */
     int topk;                   /* proposals per particle for the report                   */
+    int rescore;                /* network candidates rescored at low resolution for the
+                                   report's *_rescored figures (0: not measured)           */
     unsigned long long seed;
     double defocus_min, defocus_max, astig_max;   /* Angstrom                              */
     double voltage, cs, q0;     /* kV, mm, amplitude contrast                              */
@@ -249,6 +253,9 @@ typedef struct {
     double val_mass_min;        /* smallest after training                                 */
     double val_frac_999;        /* held-out particles with >= 0.999 of the mass in top-k   */
     double val_true_hit;        /* held-out particles whose true orientation is in top-k   */
+    double val_mass_rescored;   /* mean mass in the top-k after low-resolution rescoring   */
+    double val_mass_min_rescored;
+    double val_frac_999_rescored;
     double gen_ms, label_ms, train_ms;
     long long params;           /* network parameters                                      */
 } t2b_proposal_report;
@@ -259,8 +266,12 @@ typedef struct {
  * train with Adam on the device, and report the held-out posterior mass the
  * top-k proposals hold before and after training.  Needs t2b_configure. */
 int t2b_proposal_train(t2b_ctx* ctx, const t2b_proposal_train_config* cfg, t2b_proposal_report* report);
-/* Enable (topk >= 1) or disable (topk = 0) proposals for the following batches. */
-int t2b_proposal_enable(t2b_ctx* ctx, int topk, int audit_every, double audit_mass);
+/* Enable (topk >= 1) or disable (topk = 0) proposals for the following batches.
+ * rescore > 0: the network's top `rescore` orientations are rescored by the
+ * exact low-resolution posterior (the coarse diff2 over the network's ring
+ * pixels, with the particle's CTF, noise model and every translation) and the
+ * best `topk` of them are the proposals; rescore = 0: the network's top-k. */
+int t2b_proposal_enable(t2b_ctx* ctx, int topk, int rescore, int audit_every, double audit_mass);
 /* Network parameters as one flat FP32 vector (count: its length, layout in
  * t2-relion_b200/proposal.py); get and/or set (NULL to skip); `set` also marks
  * the network as trained. */

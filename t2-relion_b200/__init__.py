@@ -91,7 +91,7 @@ class Result(ctypes.Structure):
 class ProposalTrainConfig(ctypes.Structure):
     _fields_ = [("n_train", ctypes.c_int), ("n_posterior", ctypes.c_int), ("n_val", ctypes.c_int),
                 ("epochs", ctypes.c_int), ("batch", ctypes.c_int), ("lr", ctypes.c_float),
-                ("topk", ctypes.c_int), ("seed", ctypes.c_ulonglong),
+                ("topk", ctypes.c_int), ("rescore", ctypes.c_int), ("seed", ctypes.c_ulonglong),
                 ("defocus_min", ctypes.c_double), ("defocus_max", ctypes.c_double),
                 ("astig_max", ctypes.c_double), ("voltage", ctypes.c_double), ("cs", ctypes.c_double),
                 ("q0", ctypes.c_double), ("max_shift", ctypes.c_double), ("sigma_deg", ctypes.c_double),
@@ -102,6 +102,8 @@ class ProposalReport(ctypes.Structure):
     _fields_ = [("loss", ctypes.c_double * 64), ("val_mass_init", ctypes.c_double),
                 ("val_mass_trained", ctypes.c_double), ("val_mass_min", ctypes.c_double),
                 ("val_frac_999", ctypes.c_double), ("val_true_hit", ctypes.c_double),
+                ("val_mass_rescored", ctypes.c_double), ("val_mass_min_rescored", ctypes.c_double),
+                ("val_frac_999_rescored", ctypes.c_double),
                 ("gen_ms", ctypes.c_double), ("label_ms", ctypes.c_double), ("train_ms", ctypes.c_double),
                 ("params", ctypes.c_longlong)]
 
@@ -131,7 +133,7 @@ def _setup_prototypes():
     lib.t2b_sampling.argtypes = [i, i, ctypes.c_double, i, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double] + [ctypes.POINTER(i)] * 5 + [v] * 6
     lib.t2b_proposal_train.argtypes = [v, ctypes.POINTER(ProposalTrainConfig), ctypes.POINTER(ProposalReport)]
-    lib.t2b_proposal_enable.argtypes = [v, i, i, ctypes.c_double]
+    lib.t2b_proposal_enable.argtypes = [v, i, i, i, ctypes.c_double]
     lib.t2b_proposal_params.argtypes = [v, v, v, ctypes.POINTER(ctypes.c_longlong)]
     lib.t2b_proposal_features.argtypes = [v, ctypes.POINTER(Batch), v]
     lib.t2b_proposal_logits.argtypes = [v, v, i, v]
@@ -320,12 +322,13 @@ class EStep:
 
     # ---------------------------------------------- learned orientation proposals
     def train_proposals(self, minvsigma2, n_train=200000, n_posterior=20000, n_val=1024, epochs=4, batch=256,
-                        lr=3e-4, topk=64, seed=1, defocus=(10000., 30000.), astig=1000., voltage=300., cs=2.7,
-                        q0=0.1, max_shift=5.0, sigma_deg=8.0, alpha=3.0):
+                        lr=3e-4, topk=64, rescore=0, seed=1, defocus=(10000., 30000.), astig=1000., voltage=300.,
+                        cs=2.7, q0=0.1, max_shift=5.0, sigma_deg=8.0, alpha=3.0):
         """Train the proposal network on particles generated from the current
         references (t2b_proposal_train); returns the report as a dict."""
         mv = np.ascontiguousarray(minvsigma2, np.float32)
-        c = ProposalTrainConfig(n_train, n_posterior, n_val, epochs, batch, lr, topk, seed, defocus[0], defocus[1],
+        c = ProposalTrainConfig(n_train, n_posterior, n_val, epochs, batch, lr, topk, rescore, seed, defocus[0],
+                                defocus[1],
                                 astig, voltage, cs, q0, max_shift, sigma_deg, alpha, _ptr(mv))
         rep = ProposalReport()
         _check(lib.t2b_proposal_train(self._h, ctypes.byref(c), ctypes.byref(rep)))
@@ -333,11 +336,11 @@ class EStep:
         out["loss"] = list(rep.loss)[:min(epochs, 64)]
         return out
 
-    def enable_proposals(self, topk=64, audit_every=50, audit_mass=0.999):
-        _check(lib.t2b_proposal_enable(self._h, topk, audit_every, audit_mass))
+    def enable_proposals(self, topk=64, rescore=0, audit_every=50, audit_mass=0.999):
+        _check(lib.t2b_proposal_enable(self._h, topk, rescore, audit_every, audit_mass))
 
     def disable_proposals(self):
-        _check(lib.t2b_proposal_enable(self._h, 0, 1, 1.0))
+        _check(lib.t2b_proposal_enable(self._h, 0, 0, 1, 1.0))
 
     def proposal_params(self, set_to=None):
         n = ctypes.c_longlong()

@@ -275,6 +275,96 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
         prop[(size_t)b * k + j] = j < nc ? (int)(0xffffffffu - (unsigned)(cand[j] & 0xffffffffull)) : 0;
 }
 
+// ------------------------------------------------ low-resolution rescoring
+// Exact low-resolution score of each of the network's K1 candidates: over the
+// ring pixels only, d(j, t) = sum_p w2_p |P_j,p|^2 - Re(P_j,p conj(cvec_p ab_t,p))
+// (the coarse diff2 restricted to the ring, up to a per-particle constant) and
+// score_j = log sum_t pdf_t(t) exp(dmin - d(j, t)), the log of the particle's
+// low-resolution posterior of orientation j up to a constant.  CTA = 32
+// candidates x 8 translation lanes of one particle; the shifted ring image of
+// the particle sits in shared memory.
+constexpr int RS_CAND = 32;
+constexpr int RS_SMEM_MAX = 200 * 1024;
+__global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const int* __restrict__ ring, int nring,
+                                                      const int* __restrict__ cand, int k1, float* __restrict__ score)
+{
+    extern __shared__ float2 S[];          // T x nring shifted ring image, then 32 x nring projections
+    __shared__ float w2s[NET_MAX_RING];
+    const int b = blockIdx.y, j0 = blockIdx.x * RS_CAND;
+    const int T = tb.T, P = tb.P;
+    float2* Pj = S + (size_t)T * nring;
+    for (int i = threadIdx.x; i < T * nring; i += blockDim.x) {
+        const int t = i / nring, q = i - t * nring, n = ring[q];
+        const float2 c = w.cvec[(size_t)b * P + n];
+        const float2 a = tb.ab_c[(size_t)t * P + n];
+        S[i] = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+    }
+    for (int q = threadIdx.x; q < nring; q += blockDim.x) w2s[q] = w.w2[(size_t)b * P + ring[q]];
+    for (int i = threadIdx.x; i < RS_CAND * nring; i += blockDim.x) {
+        const int jj = i / nring, q = i - jj * nring;
+        const int j = j0 + jj;
+        Pj[i] = j < k1 ? tb.proj_c[(size_t)cand[(size_t)b * k1 + j] * P + ring[q]] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int jj = threadIdx.x >> 3, lane8 = threadIdx.x & 7;
+    const float2* pj = Pj + (size_t)jj * nring;
+    float nrm = 0.f;
+    for (int q = lane8; q < nring; q += 8) nrm += w2s[q] * (pj[q].x * pj[q].x + pj[q].y * pj[q].y);
+    for (int o = 4; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+    float dmin = INFINITY;
+    float dv[(256 + 7) / 8];
+    int nt = 0;
+    for (int t = lane8; t < T; t += 8, nt++) {
+        const float2* st = S + (size_t)t * nring;
+        float cacc = 0.f;
+        for (int q = 0; q < nring; q++) cacc += pj[q].x * st[q].x + pj[q].y * st[q].y;
+        const float d = nrm - cacc;
+        dv[nt] = d;
+        dmin = fminf(dmin, d);
+    }
+    for (int o = 4; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+    double se = 0.;
+    nt = 0;
+    for (int t = lane8; t < T; t += 8, nt++) se += w.pdf_t[(size_t)b * T + t] * exp((double)(dmin - dv[nt]));
+    for (int o = 4; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
+    const int j = j0 + jj;
+    if (lane8 == 0 && j < k1) {
+        const int oc = cand[(size_t)b * k1 + j];
+        score[(size_t)b * k1 + j] = (tb.skip[oc] || !(se > 0.)) ? -INFINITY
+                                                                : (float)(log(se) - (double)dmin + log(tb.pdf_oc[oc]));
+    }
+}
+
+// the k best-scored candidates of each particle, ranked (ties by rank in the network's list)
+__global__ void __launch_bounds__(1024) k_rescore_select(const int* __restrict__ cand, const float* __restrict__ score,
+                                                         int k1, int k, int* __restrict__ prop)
+{
+    __shared__ unsigned long long key[NET_TOPK_CAND];
+    const int b = blockIdx.x;
+    int n2 = 1;
+    while (n2 < k1) n2 <<= 1;
+    for (int i = threadIdx.x; i < n2; i += blockDim.x)
+        key[i] = i < k1 ? ((unsigned long long)f2key(score[(size_t)b * k1 + i]) << 32) | (unsigned)(0xffffffffu - (unsigned)i)
+                        : 0ull;
+    __syncthreads();
+    for (int kk = 2; kk <= n2; kk <<= 1)
+        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+            for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+                const int l = i ^ jj;
+                if (l > i) {
+                    const bool desc = (i & kk) == 0;
+                    const unsigned long long a = key[i], c = key[l];
+                    if (desc ? (a < c) : (a > c)) { key[i] = c; key[l] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+        const int r = (int)(0xffffffffu - (unsigned)(key[j] & 0xffffffffull));
+        prop[(size_t)b * k + j] = cand[(size_t)b * k1 + r];
+    }
+}
+
 // ---------------------------------------------- proposal coarse operands
 // Gathered split-BF16 projections of every (particle, proposal) and its norm
 // N = sum_p w2 |P|^2 (FP32 from the FP32 table).  Row of (b, j) in the A
@@ -1139,6 +1229,8 @@ void net_setup(t2b_ctx* c, int na_max)
     N.logits = (float*)net_dalloc(W, (size_t)B * KO * sizeof(float));
     N.prop = (int*)net_dalloc(W, (size_t)B * 128 * sizeof(int));
     T2B_CUDA(cudaMemset(N.prop, 0, (size_t)B * 128 * sizeof(int)));
+    N.cand1 = (int*)net_dalloc(W, (size_t)B * NET_TOPK_CAND * sizeof(int));
+    N.score1 = (float*)net_dalloc(W, (size_t)B * NET_TOPK_CAND * sizeof(float));
     // tensor maps of the dense layers: W1, X0b, W2, H1b, W3, H2b
     unsigned char blobs[6][128];
     const bf16* thb = (const bf16*)N.thb;
@@ -1181,6 +1273,7 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.c0a, 0, (size_t)N.na_max * sizeof(float)));
     T2B_CUDA(cudaMemset(N.norma, 0, (size_t)N.na_max * KO * sizeof(float)));
     T2B_CUDA(cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, KO * (int)sizeof(unsigned)));
+    T2B_CUDA(cudaFuncSetAttribute(k_prop_rescore, cudaFuncAttributeMaxDynamicSharedMemorySize, RS_SMEM_MAX));
     T2B_CUDA(cudaDeviceSynchronize());
     N.ready = true;
 }
@@ -1308,8 +1401,18 @@ void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st)
     k_features<<<w.n, NET_NPIX, 0, st>>>(w.fimg, w.ctf, w.minv, tb.P, N.ring, N.ring_k, N.nring, N.img, nullptr, nullptr);
     k_conv_fwd<<<w.n, 256, 0, st>>>(N.img, (const bf16*)N.thb, N.L, w.n, nullptr, nullptr, (bf16*)N.x0b);
     infer_dense(N, w.n, w.err, st);
-    k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO, N.kprop,
-                                                       N.prop);
+    if (N.k1 > 0) {
+        // network top-k1, exact low-resolution rescoring, top-kprop of those
+        k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO, N.k1,
+                                                           N.cand1);
+        const size_t smem = (size_t)(tb.T + RS_CAND) * N.nring * sizeof(float2);
+        k_prop_rescore<<<dim3((N.k1 + RS_CAND - 1) / RS_CAND, w.n), 256, smem, st>>>(tb, w, N.ring, N.nring, N.cand1,
+                                                                                     N.k1, N.score1);
+        k_rescore_select<<<w.n, 1024, 0, st>>>(N.cand1, N.score1, N.k1, N.kprop, N.prop);
+    } else {
+        k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO,
+                                                           N.kprop, N.prop);
+    }
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -1428,8 +1531,12 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
         N.enabled = false;
         N.trained = false;
         N.kprop = f.topk;
+        N.k1 = 0;
         set_tile_shape(N, tb.T);
         net_setup(c, std::max(1, N.na_max));
+        T2B_REQUIRE(f.rescore == 0 || (f.rescore >= f.topk && f.rescore <= NET_TOPK_CAND && f.rescore <= KO &&
+                                       (size_t)(tb.T + RS_CAND) * N.nring * sizeof(float2) <= (size_t)RS_SMEM_MAX),
+                    T2B_ERR_ARG, "bad rescore candidate count");
         *rep = t2b_proposal_report{};
         rep->params = real_params(KO);
 
@@ -1579,6 +1686,11 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
             rep->train_ms = elapsed();
             N.trained = true;
             validate(&rep->val_mass_trained, &rep->val_mass_min, &rep->val_frac_999, &rep->val_true_hit);
+            if (f.rescore > 0) {
+                N.k1 = f.rescore;
+                validate(&rep->val_mass_rescored, &rep->val_mass_min_rescored, &rep->val_frac_999_rescored, nullptr);
+                N.k1 = 0;
+            }
         } catch (...) {
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
@@ -1590,7 +1702,7 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
     });
 }
 
-int t2b_proposal_enable(t2b_ctx* c, int topk, int audit_every, double audit_mass)
+int t2b_proposal_enable(t2b_ctx* c, int topk, int rescore, int audit_every, double audit_mass)
 {
     return guarded([&] {
         T2B_REQUIRE(c, T2B_ERR_ARG, "null context");
@@ -1607,13 +1719,18 @@ int t2b_proposal_enable(t2b_ctx* c, int topk, int audit_every, double audit_mass
                     "no trained proposal network for this orientation sampling");
         T2B_REQUIRE(topk >= 1 && topk <= 128 && topk <= KO && audit_every >= 1 && audit_mass > 0. && audit_mass <= 1.,
                     T2B_ERR_ARG, "bad proposal settings");
+        T2B_REQUIRE(rescore == 0 || (rescore >= topk && rescore <= NET_TOPK_CAND && rescore <= KO), T2B_ERR_ARG,
+                    "rescore must be 0 or in [topk, min(2048, nr_classes*n_dir*n_psi)]");
         ProposalNet& N = *c->net;
+        const int B = c->cfg.max_batch;
+        net_setup(c, std::min(B, (B + audit_every - 1) / audit_every + 1));
+        T2B_REQUIRE(rescore == 0 || (size_t)(c->tb.T + RS_CAND) * N.nring * sizeof(float2) <= (size_t)RS_SMEM_MAX,
+                    T2B_ERR_UNSUPPORTED, "too many translations for the low-resolution rescoring");
+        N.k1 = rescore;
         N.kprop = topk;
         N.every = audit_every;
         N.thr = audit_mass;
         set_tile_shape(N, c->tb.T);
-        const int B = c->cfg.max_batch;
-        net_setup(c, std::min(B, (B + audit_every - 1) / audit_every + 1));
         T2B_CUDA(cudaMemset(N.ps, 0, sizeof(PropState)));
         N.enabled = true;
     });

@@ -46,6 +46,9 @@ struct ProposalNet {
     bool ready = false;                // workspace matches the configuration
     bool enabled = false;
     int kprop = 64, every = 50, na_max = 0, ppt = 1, kslot = 128, b_pad = 0;
+    int k1 = 0;                        // network candidates rescored at low resolution (0: none)
+    int* cand1 = nullptr;              // B x k1 network candidates
+    float* score1 = nullptr;           // B x k1 low-resolution scores
     double thr = 0.999;
     int nring = 0;
     int *ring = nullptr, *ring_k = nullptr;

@@ -95,32 +95,36 @@ def test_tensor_core_logits_match_oracle(o2):
 @pytest.fixture(scope="module")
 def trained(o2):
     es = o2["es"]
-    rep = es.train_proposals(o2["parts"]["minv"][0], n_train=24000, n_posterior=2048, n_val=512, epochs=3,
-                             batch=256, lr=3e-4, topk=64, seed=3, max_shift=3.0)
+    rep = es.train_proposals(o2["parts"]["minv"][0], n_train=40000, n_posterior=4096, n_val=512, epochs=4,
+                             batch=256, lr=3e-4, topk=64, rescore=512, seed=3, max_shift=3.0)
     o2["report"] = rep
     return o2
 
 
 def test_training_gains_over_initial_network(trained):
+    """Held-out posterior mass in the top-64: the trained network against the
+    matched filter it starts from, and with the low-resolution rescoring."""
     rep = trained["report"]
+    print("proposal training report:", rep)
     assert rep["params"] > 10_000_000
     assert rep["loss"][-1] < rep["loss"][0]
-    assert rep["val_mass_trained"] >= rep["val_mass_init"] - 1e-3
-    assert rep["val_mass_trained"] >= 0.95
+    assert rep["val_mass_trained"] > rep["val_mass_init"] + 0.02, rep
+    assert rep["val_mass_rescored"] >= rep["val_mass_trained"], rep
+    assert rep["val_frac_999_rescored"] >= 0.98, rep
 
 
 def test_learned_estep_matches_full_estep(trained):
     es, P = trained["es"], trained["parts"]
     es.disable_proposals()
     full = es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
-    es.enable_proposals(topk=64, audit_every=4, audit_mass=0.999)
+    es.enable_proposals(topk=64, rescore=512, audit_every=4, audit_mass=0.999)
     got = es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
     es.disable_proposals()
     assert np.all(got["status"] == 0)
     audited = got["audit_mass"] >= 0
     assert audited.sum() == len(audited) // 4
-    if got["learned"][0]:
-        assert np.all(got["audit_mass"][audited] >= 0.999)
+    assert np.all(got["learned"] == 1), got["audit_mass"][audited]
+    assert np.all(got["audit_mass"][audited] >= 0.999)
     same = np.all(got["pose"] == full["pose"], axis=1)
     assert same.mean() >= 0.995, same.mean()
 
@@ -149,9 +153,9 @@ def test_graph_batch_with_proposals_matches_host(trained):
     import torch
     es, P = trained["es"], trained["parts"]
     n = 32
-    es.enable_proposals(topk=64, audit_every=16, audit_mass=0.999)
+    es.enable_proposals(topk=64, rescore=512, audit_every=16, audit_mass=0.999)
     ref = es.expectation(P["fimg"][:n], P["ctf"][:n], P["minv"][:n], P["scalars"][:n])
-    es.enable_proposals(topk=64, audit_every=16, audit_mass=0.999)  # restart the audit stream
+    es.enable_proposals(topk=64, rescore=512, audit_every=16, audit_mass=0.999)  # restart the audit stream
     dev = torch.device("cuda")
     fimg = torch.from_numpy(np.ascontiguousarray(P["fimg"][:n]).view(np.float32)).to(dev)
     ctf = torch.from_numpy(np.ascontiguousarray(P["ctf"][:n])).to(dev)
