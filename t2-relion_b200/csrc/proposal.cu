@@ -280,58 +280,111 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
 // ring pixels only, d(j, t) = sum_p w2_p |P_j,p|^2 - Re(P_j,p conj(cvec_p ab_t,p))
 // (the coarse diff2 restricted to the ring, up to a per-particle constant) and
 // score_j = log sum_t pdf_t(t) exp(dmin - d(j, t)), the log of the particle's
-// low-resolution posterior of orientation j up to a constant.  CTA = 32
-// candidates x 8 translation lanes of one particle; the shifted ring image of
-// the particle sits in shared memory.
+// low-resolution posterior of orientation j up to a constant.
 constexpr int RS_CAND = 32;
 constexpr int RS_SMEM_MAX = 200 * 1024;
-__global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const int* __restrict__ ring, int nring,
-                                                      const int* __restrict__ cand, int k1, float* __restrict__ score)
+constexpr int RS_TMAX = 96;            // translations per CTA tile (3 per lane)
+
+// Ring operands of the rescoring.  projR[oc][q]: the projection of every
+// coarse orientation at the ring pixels (once per configuration); per batch
+// Sg[b][q][t] = cvec_b ab_t at ring pixel q (t < RS_TMAX, zero beyond T) and
+// w2r[b][q].
+__global__ void k_ring_table(const float2* __restrict__ proj, int P, const int* __restrict__ ring, int nring, int KO,
+                             float2* __restrict__ projR)
 {
-    extern __shared__ float2 S[];          // T x nring shifted ring image, then 32 x nring projections
+    const size_t total = (size_t)KO * nring;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t oc = i / nring;
+        projR[i] = proj[oc * P + ring[i - oc * nring]];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_ring_images(Tables tb, Work w, const int* __restrict__ ring, int nring,
+                                                     float2* __restrict__ Sg, float* __restrict__ w2r)
+{
+    const int b = blockIdx.x, P = tb.P;
+    for (int i = threadIdx.x; i < nring * RS_TMAX; i += blockDim.x) {
+        const int t = i / nring, q = i - t * nring, n = ring[q];   // q fastest: coalesced reads
+        float2 v = make_float2(0.f, 0.f);
+        if (t < tb.T) {
+            const float2 c = w.cvec[(size_t)b * P + n];
+            const float2 a = tb.ab_c[(size_t)t * P + n];
+            v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+        }
+        Sg[((size_t)b * nring + q) * RS_TMAX + t] = v;
+    }
+    for (int q = threadIdx.x; q < nring; q += blockDim.x) w2r[(size_t)b * nring + q] = w.w2[(size_t)b * P + ring[q]];
+}
+
+// Exact low-resolution score of each of the network's K1 candidates (see the
+// comment above).  CTA = 32 candidates x up to 96 translations of one particle;
+// warp w owns candidates 4w..4w+3, lane l the translations l, l+32, l+64, so a
+// thread keeps a 4 x 3 register tile per ring pixel.  Shared memory: the
+// particle's shifted ring image [pixel][translation] and the 32 candidates'
+// ring projections [candidate][pixel] (read as broadcasts).
+__global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const float2* __restrict__ Sg,
+                                                      const float* __restrict__ w2r, const float2* __restrict__ projR,
+                                                      int nring, const int* __restrict__ cand, int k1,
+                                                      float* __restrict__ score)
+{
+    extern __shared__ float2 S[];          // nring x RS_TMAX, then RS_CAND x nring
     __shared__ float w2s[NET_MAX_RING];
     const int b = blockIdx.y, j0 = blockIdx.x * RS_CAND;
-    const int T = tb.T, P = tb.P;
-    float2* Pj = S + (size_t)T * nring;
-    for (int i = threadIdx.x; i < T * nring; i += blockDim.x) {
-        const int t = i / nring, q = i - t * nring, n = ring[q];
-        const float2 c = w.cvec[(size_t)b * P + n];
-        const float2 a = tb.ab_c[(size_t)t * P + n];
-        S[i] = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+    const int T = tb.T;
+    float2* Pj = S + (size_t)nring * RS_TMAX;
+    {
+        const float4* src = reinterpret_cast<const float4*>(Sg + (size_t)b * nring * RS_TMAX);
+        float4* dst = reinterpret_cast<float4*>(S);
+        for (int i = threadIdx.x; i < nring * RS_TMAX / 2; i += blockDim.x) dst[i] = src[i];
     }
-    for (int q = threadIdx.x; q < nring; q += blockDim.x) w2s[q] = w.w2[(size_t)b * P + ring[q]];
+    for (int q = threadIdx.x; q < nring; q += blockDim.x) w2s[q] = w2r[(size_t)b * nring + q];
     for (int i = threadIdx.x; i < RS_CAND * nring; i += blockDim.x) {
         const int jj = i / nring, q = i - jj * nring;
         const int j = j0 + jj;
-        Pj[i] = j < k1 ? tb.proj_c[(size_t)cand[(size_t)b * k1 + j] * P + ring[q]] : make_float2(0.f, 0.f);
+        Pj[i] = j < k1 ? projR[(size_t)cand[(size_t)b * k1 + j] * nring + q] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    const int jj = threadIdx.x >> 3, lane8 = threadIdx.x & 7;
-    const float2* pj = Pj + (size_t)jj * nring;
-    float nrm = 0.f;
-    for (int q = lane8; q < nring; q += 8) nrm += w2s[q] * (pj[q].x * pj[q].x + pj[q].y * pj[q].y);
-    for (int o = 4; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
-    float dmin = INFINITY;
-    float dv[(256 + 7) / 8];
-    int nt = 0;
-    for (int t = lane8; t < T; t += 8, nt++) {
-        const float2* st = S + (size_t)t * nring;
-        float cacc = 0.f;
-        for (int q = 0; q < nring; q++) cacc += pj[q].x * st[q].x + pj[q].y * st[q].y;
-        const float d = nrm - cacc;
-        dv[nt] = d;
-        dmin = fminf(dmin, d);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float acc[4][3] = {};
+    float nrm[4] = {};
+    const float2* pw = Pj + (size_t)(warp * 4) * nring;
+    for (int q = 0; q < nring; q++) {
+        const float2* sq = S + (size_t)q * RS_TMAX + lane;
+        const float2 s0 = sq[0], s1 = sq[32], s2 = sq[64];
+        const float wq = w2s[q];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float2 pv = pw[c * nring + q];
+            acc[c][0] += pv.x * s0.x + pv.y * s0.y;
+            acc[c][1] += pv.x * s1.x + pv.y * s1.y;
+            acc[c][2] += pv.x * s2.x + pv.y * s2.y;
+            nrm[c] += wq * (pv.x * pv.x + pv.y * pv.y);
+        }
     }
-    for (int o = 4; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
-    double se = 0.;
-    nt = 0;
-    for (int t = lane8; t < T; t += 8, nt++) se += w.pdf_t[(size_t)b * T + t] * exp((double)(dmin - dv[nt]));
-    for (int o = 4; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
-    const int j = j0 + jj;
-    if (lane8 == 0 && j < k1) {
-        const int oc = cand[(size_t)b * k1 + j];
-        score[(size_t)b * k1 + j] = (tb.skip[oc] || !(se > 0.)) ? -INFINITY
-                                                                : (float)(log(se) - (double)dmin + log(tb.pdf_oc[oc]));
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        float d[3];
+        float dmin = INFINITY;
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            const int t = lane + 32 * m;
+            d[m] = nrm[c] - acc[c][m];
+            if (t < T) dmin = fminf(dmin, d[m]);
+        }
+        for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+        double se = 0.;
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            const int t = lane + 32 * m;
+            if (t < T) se += w.pdf_t[(size_t)b * T + t] * exp((double)(dmin - d[m]));
+        }
+        for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
+        const int j = j0 + warp * 4 + c;
+        if (lane == 0 && j < k1) {
+            const int oc = cand[(size_t)b * k1 + j];
+            score[(size_t)b * k1 + j] = (tb.skip[oc] || !(se > 0.)) ? -INFINITY
+                                                                    : (float)(log(se) - (double)dmin + log(tb.pdf_oc[oc]));
+        }
     }
 }
 
@@ -425,6 +478,7 @@ __global__ void k_audit_begin(PropState* ps, int* audit_b, int n, int every, int
 
 // image operand rows, w2 and c0 of the audited particles into the audit slots
 __global__ void __launch_bounds__(256) k_audit_operands(const PropState* ps, const int* audit_b, Work w, int T, int P,
+                                                        const int* __restrict__ kpix, int nk, int kn,
                                                         int kdim, const bf16* __restrict__ ih, const bf16* __restrict__ il,
                                                         bf16* __restrict__ iah, bf16* __restrict__ ial,
                                                         float* __restrict__ w2a, float* __restrict__ c0a)
@@ -440,28 +494,56 @@ __global__ void __launch_bounds__(256) k_audit_operands(const PropState* ps, con
             reinterpret_cast<uint4*>(ial + dst)[k] = reinterpret_cast<const uint4*>(il + src)[k];
         }
     } else {
-        for (int p = threadIdx.x; p < P; p += blockDim.x) w2a[(size_t)a * P + p] = w.w2[(size_t)b * P + p];
+        for (int k = threadIdx.x; k < kn; k += blockDim.x)
+            w2a[(size_t)a * kn + k] = k < nk ? w.w2[(size_t)b * P + kpix[k]] : 0.f;
         if (threadIdx.x == 0) c0a[a] = w.c0[b];
     }
 }
 
-// audit norms N[a][oc] = sum_p w2a[a][p] |P_oc[p]|^2 (one warp per (a, oc))
-__global__ void __launch_bounds__(256) k_audit_norms(Tables tb, const PropState* ps, const float* __restrict__ w2a,
-                                                     float* __restrict__ norma)
+// audit norms N[a][oc] = sum_k w2a[a][k] |P_oc|^2_k for every audit slot in one
+// pass over the split-BF16 |P|^2 operand (hi + lo, the norm GEMM's A operand;
+// k the in-radius pixel index, rows of kn elements, zero beyond nk); one warp
+// per orientation, 8 elements (16 bytes) per lane and load
+constexpr int AUDIT_NORM_SLOTS = 4;
+__global__ void __launch_bounds__(256) k_audit_norms(int KO, int kn, const PropState* ps, const bf16* __restrict__ nh,
+                                                     const bf16* __restrict__ nl, const float* __restrict__ w2a,
+                                                     int na_max, float* __restrict__ norma)
 {
-    const int KO = tb.K * tb.O;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    const int a = blockIdx.y;
-    if (a >= ps->na || warp >= KO) return;
-    const float2* src = tb.proj_c + (size_t)warp * tb.P;
-    float acc = 0.f;
-    for (int k = lane; k < tb.nk; k += 32) {
-        const int p = tb.kpix[k];
-        const float2 v = src[p];
-        acc += w2a[(size_t)a * tb.P + p] * (v.x * v.x + v.y * v.y);
+    if (warp >= KO) return;
+    const int na = min(ps->na, na_max);
+    const uint4* h = reinterpret_cast<const uint4*>(nh + (size_t)warp * kn);
+    const uint4* l = reinterpret_cast<const uint4*>(nl + (size_t)warp * kn);
+    const int nv = kn / 8;
+    for (int a0 = 0; a0 < na; a0 += AUDIT_NORM_SLOTS) {
+        float acc[AUDIT_NORM_SLOTS] = {};
+        for (int v = lane; v < nv; v += 32) {
+            const uint4 hv = h[v], lv = l[v];
+            const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&hv);
+            const __nv_bfloat162* lp = reinterpret_cast<const __nv_bfloat162*>(&lv);
+            float x[8];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const float2 hf = __bfloat1622float2(hp[e]), lf = __bfloat1622float2(lp[e]);
+                x[2 * e] = hf.x + lf.x;
+                x[2 * e + 1] = hf.y + lf.y;
+            }
+#pragma unroll
+            for (int a = 0; a < AUDIT_NORM_SLOTS; a++) {
+                if (a0 + a >= na) break;
+                const float4* wp = reinterpret_cast<const float4*>(w2a + (size_t)(a0 + a) * kn + 8 * v);
+                const float4 w0 = wp[0], w1 = wp[1];
+                acc[a] += w0.x * x[0] + w0.y * x[1] + w0.z * x[2] + w0.w * x[3] + w1.x * x[4] + w1.y * x[5] +
+                          w1.z * x[6] + w1.w * x[7];
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < AUDIT_NORM_SLOTS; a++) {
+            float v = acc[a];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0 && a0 + a < na) norma[(size_t)(a0 + a) * KO + warp] = v;
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) norma[(size_t)a * KO + warp] = acc;
 }
 
 // posterior mass of the audited particles: total and inside the proposals
@@ -486,12 +568,16 @@ __global__ void __launch_bounds__(256) k_audit_mass(Tables tb, Work w, const Pro
     const double mn = (double)key2f(minkeya[a]);
     const long long n = (long long)KO * T;
     const float* d = d2a + (size_t)a * n;
+    // hypotheses beyond this diff2 distance from the minimum weigh less than
+    // e^-60 of the heaviest one (after the prior ratio); all of them together
+    // are below 1e-18 of the sum
+    const double cut = fmin(700., 60. + (w.lbound[2 * b + 1] - w.lbound[2 * b]));
     double sa = 0., sp = 0.;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const float v = d[i];
         if (v < 0.f) continue;
         const double dd = (double)v - mn;
-        if (dd > 700.) continue;
+        if (dd > cut) continue;
         const int oc = (int)(i / T), t = (int)(i - (long long)oc * T);
         const double wt = tb.pdf_oc[oc] * w.pdf_t[(size_t)b * T + t] * exp(-dd);
         sa += wt;
@@ -1231,6 +1317,10 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.prop, 0, (size_t)B * 128 * sizeof(int)));
     N.cand1 = (int*)net_dalloc(W, (size_t)B * NET_TOPK_CAND * sizeof(int));
     N.score1 = (float*)net_dalloc(W, (size_t)B * NET_TOPK_CAND * sizeof(float));
+    N.projR = (float2*)net_dalloc(W, (size_t)KO * N.nring * sizeof(float2));
+    k_ring_table<<<gridsz((size_t)KO * N.nring), 256>>>(tb.proj_c, P, N.ring, N.nring, KO, N.projR);
+    N.Sg = (float2*)net_dalloc(W, (size_t)B * N.nring * RS_TMAX * sizeof(float2));
+    N.w2r = (float*)net_dalloc(W, (size_t)B * N.nring * sizeof(float));
     // tensor maps of the dense layers: W1, X0b, W2, H1b, W3, H2b
     unsigned char blobs[6][128];
     const bf16* thb = (const bf16*)N.thb;
@@ -1263,13 +1353,13 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.ia_l, 0, (size_t)ia_rows * op.kdim * sizeof(bf16)));
     tc_set_map(c->tc, tc_slot_audit(), N.ia_h, ia_rows, op.kdim, false);
     tc_set_map(c->tc, tc_slot_audit() + 1, N.ia_l, ia_rows, op.kdim, false);
-    N.w2a = (float*)net_dalloc(W, (size_t)N.na_max * P * sizeof(float));
+    N.w2a = (float*)net_dalloc(W, (size_t)N.na_max * std::max(P, op.kn) * sizeof(float));
     N.c0a = (float*)net_dalloc(W, (size_t)N.na_max * sizeof(float));
     N.norma = (float*)net_dalloc(W, (size_t)N.na_max * KO * sizeof(float));
     N.d2a = (float*)net_dalloc(W, (size_t)N.na_max * KO * tb.T * sizeof(float));
     N.minkeya = (unsigned*)net_dalloc(W, (size_t)N.na_max * sizeof(unsigned));
     N.asum = (double*)net_dalloc(W, (size_t)N.na_max * 2 * sizeof(double));
-    T2B_CUDA(cudaMemset(N.w2a, 0, (size_t)N.na_max * P * sizeof(float)));
+    T2B_CUDA(cudaMemset(N.w2a, 0, (size_t)N.na_max * std::max(P, op.kn) * sizeof(float)));
     T2B_CUDA(cudaMemset(N.c0a, 0, (size_t)N.na_max * sizeof(float)));
     T2B_CUDA(cudaMemset(N.norma, 0, (size_t)N.na_max * KO * sizeof(float)));
     T2B_CUDA(cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, KO * (int)sizeof(unsigned)));
@@ -1405,9 +1495,10 @@ void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st)
         // network top-k1, exact low-resolution rescoring, top-kprop of those
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO, N.k1,
                                                            N.cand1);
-        const size_t smem = (size_t)(tb.T + RS_CAND) * N.nring * sizeof(float2);
-        k_prop_rescore<<<dim3((N.k1 + RS_CAND - 1) / RS_CAND, w.n), 256, smem, st>>>(tb, w, N.ring, N.nring, N.cand1,
-                                                                                     N.k1, N.score1);
+        const size_t smem = (size_t)(RS_TMAX + RS_CAND) * N.nring * sizeof(float2);
+        k_ring_images<<<w.n, 256, 0, st>>>(tb, w, N.ring, N.nring, N.Sg, N.w2r);
+        k_prop_rescore<<<dim3((N.k1 + RS_CAND - 1) / RS_CAND, w.n), 256, smem, st>>>(tb, w, N.Sg, N.w2r, N.projR, N.nring,
+                                                                                     N.cand1, N.k1, N.score1);
         k_rescore_select<<<w.n, 1024, 0, st>>>(N.cand1, N.score1, N.k1, N.kprop, N.prop);
     } else {
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO,
@@ -1423,13 +1514,15 @@ void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st)
     TcOperands& op = c->tc;
     const int KO = tb.K * tb.O;
     k_audit_begin<<<1, 256, 0, st>>>(N.ps, N.audit_b, w.n, N.every, N.na_max, N.minkeya, N.asum, w.r_audit);
-    k_audit_operands<<<dim3(tb.T + 1, N.na_max), 256, 0, st>>>(N.ps, N.audit_b, w, tb.T, tb.P, op.kdim,
+    k_audit_operands<<<dim3(tb.T + 1, N.na_max), 256, 0, st>>>(N.ps, N.audit_b, w, tb.T, tb.P, tb.kpix, tb.nk, op.kn,
+                                                               op.kdim,
                                                                (const bf16*)op.ah, (const bf16*)op.al, (bf16*)N.ia_h,
                                                                (bf16*)N.ia_l, N.w2a, N.c0a);
-    k_audit_norms<<<dim3((KO * 32 + 255) / 256, N.na_max), 256, 0, st>>>(tb, N.ps, N.w2a, N.norma);
+    k_audit_norms<<<(KO * 32 + 255) / 256, 256, 0, st>>>(KO, op.kn, N.ps, (const bf16*)op.nh, (const bf16*)op.nl,
+                                                        N.w2a, N.na_max, N.norma);
     T2B_CUDA(cudaGetLastError());
     tc_launch_audit(tb, op, N.na_max, N.c0a, N.norma, N.d2a, N.minkeya, w.err, st);
-    k_audit_mass<<<dim3(96, N.na_max), 256, ((KO + 31) / 32) * sizeof(unsigned), st>>>(tb, w, N.ps, N.audit_b, N.d2a,
+    k_audit_mass<<<dim3(2 * 148, N.na_max), 256, ((KO + 31) / 32) * sizeof(unsigned), st>>>(tb, w, N.ps, N.audit_b, N.d2a,
                                                                                      N.minkeya, N.asum);
     k_audit_final<<<1, 1024, 0, st>>>(N.ps, N.audit_b, N.asum, N.thr, w.r_audit);
     T2B_CUDA(cudaGetLastError());
@@ -1535,7 +1628,7 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
         set_tile_shape(N, tb.T);
         net_setup(c, std::max(1, N.na_max));
         T2B_REQUIRE(f.rescore == 0 || (f.rescore >= f.topk && f.rescore <= NET_TOPK_CAND && f.rescore <= KO &&
-                                       (size_t)(tb.T + RS_CAND) * N.nring * sizeof(float2) <= (size_t)RS_SMEM_MAX),
+                                       tb.T <= RS_TMAX && (size_t)(RS_TMAX + RS_CAND) * N.nring * sizeof(float2) <= (size_t)RS_SMEM_MAX),
                     T2B_ERR_ARG, "bad rescore candidate count");
         *rep = t2b_proposal_report{};
         rep->params = real_params(KO);
@@ -1723,9 +1816,10 @@ int t2b_proposal_enable(t2b_ctx* c, int topk, int rescore, int audit_every, doub
                     "rescore must be 0 or in [topk, min(2048, nr_classes*n_dir*n_psi)]");
         ProposalNet& N = *c->net;
         const int B = c->cfg.max_batch;
-        net_setup(c, std::min(B, (B + audit_every - 1) / audit_every + 1));
-        T2B_REQUIRE(rescore == 0 || (size_t)(c->tb.T + RS_CAND) * N.nring * sizeof(float2) <= (size_t)RS_SMEM_MAX,
-                    T2B_ERR_UNSUPPORTED, "too many translations for the low-resolution rescoring");
+        // at most ceil(B / every) multiples of `every` in any B consecutive stream positions
+        net_setup(c, std::min(B, (B + audit_every - 1) / audit_every));
+        T2B_REQUIRE(rescore == 0 || c->tb.T <= RS_TMAX && (size_t)(RS_TMAX + RS_CAND) * N.nring * sizeof(float2) <= (size_t)RS_SMEM_MAX,
+                    T2B_ERR_UNSUPPORTED, "the low-resolution rescoring takes at most 96 translations");
         N.k1 = rescore;
         N.kprop = topk;
         N.every = audit_every;

@@ -47,6 +47,9 @@ struct ProposalNet {
     bool enabled = false;
     int kprop = 64, every = 50, na_max = 0, ppt = 1, kslot = 128, b_pad = 0;
     int k1 = 0;                        // network candidates rescored at low resolution (0: none)
+    float2* projR = nullptr;           // K*O x nring: projections at the ring pixels
+    float2* Sg = nullptr;              // B x nring x 96: shifted ring images of the batch
+    float* w2r = nullptr;              // B x nring
     int* cand1 = nullptr;              // B x k1 network candidates
     float* score1 = nullptr;           // B x k1 low-resolution scores
     double thr = 0.999;

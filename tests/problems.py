@@ -13,6 +13,9 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
         "refine_o2": dict(N=64, angpix=2.0, order=2, psi=7.5, rng=3, r=16, snr=0.05, ovs=0),
         # box 64, order 1 + adaptive oversampling (fine pass), 29 shifts
         "refine_o1_ovs": dict(N=64, angpix=2.0, order=1, psi=15.0, rng=3, r=16, snr=0.05, ovs=1),
+        # box 64, order 2 + adaptive oversampling, high SNR: a sharp posterior, the regime in
+        # which the learned proposals hold the posterior (the box-128 benchmark's regime)
+        "learn_o2": dict(N=64, angpix=2.0, order=2, psi=7.5, rng=3, r=16, snr=0.5, ovs=1),
         # 2D classification: 2D references, psi 6 deg, oversampling 1
         "class2d": dict(N=48, angpix=2.0, order=0, psi=6.0, rng=3, r=12, snr=0.2, ovs=1),
     }

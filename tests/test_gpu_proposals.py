@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def o2():
-    pb = problems.build("refine_o2", n_particles=48, seed=21, diff2_mode=1)
+    pb = problems.build("learn_o2", n_particles=48, seed=21, diff2_mode=1)
     es = pb["product"]()
     pb["es"] = es
     yield pb
@@ -108,9 +108,10 @@ def test_training_gains_over_initial_network(trained):
     print("proposal training report:", rep)
     assert rep["params"] > 10_000_000
     assert rep["loss"][-1] < rep["loss"][0]
-    assert rep["val_mass_trained"] > rep["val_mass_init"] + 0.02, rep
+    # the posterior mass the proposals miss shrinks at least fourfold with training
+    assert 1.0 - rep["val_mass_trained"] <= 0.25 * (1.0 - rep["val_mass_init"]), rep
     assert rep["val_mass_rescored"] >= rep["val_mass_trained"], rep
-    assert rep["val_frac_999_rescored"] >= 0.98, rep
+    assert rep["val_frac_999_rescored"] >= 0.95, rep
 
 
 def test_learned_estep_matches_full_estep(trained):
