@@ -410,27 +410,41 @@ __global__ void k_split_proj(const float2* __restrict__ proj, int rows, int P, c
     }
 }
 
-// shifted, CTF- and sigma-weighted images: column b*T+t, value cvec_b[p] * ab_t[p]
-__global__ void k_split_img(const float2* __restrict__ cvec, const float2* __restrict__ ab, int ncols, int T, int P,
-                            const int* __restrict__ kpix, int nk, int kdim, __nv_bfloat16* __restrict__ hi,
-                            __nv_bfloat16* __restrict__ lo, long long total)
+// shifted, CTF- and sigma-weighted images: column b*T+t, value cvec_b[p] * ab_t[p];
+// one operand row per CTA iteration, 4 complex values (16-byte stores) per thread
+__global__ void __launch_bounds__(128) k_split_img(const float2* __restrict__ cvec, const float2* __restrict__ ab,
+                                                   int ncols, int nrows, int T, int P, const int* __restrict__ kpix,
+                                                   int nk, int kdim, __nv_bfloat16* __restrict__ hi,
+                                                   __nv_bfloat16* __restrict__ lo)
 {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        const long long col = i / (kdim / 2);
-        const int kk = (int)(i - col * (kdim / 2));
-        float2 v = make_float2(0.f, 0.f);
-        if (col < ncols && kk < nk) {
-            const int pp = kpix[kk];
-            const int b = (int)(col / T), t = (int)(col - (long long)b * T);
-            const float2 c = cvec[(size_t)b * P + pp];
-            const float2 a = ab[(size_t)t * P + pp];
-            v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+    const int nv = kdim / 8;  // groups of 4 complex values
+    for (int col = blockIdx.x; col < nrows; col += gridDim.x) {
+        const bool ok = col < ncols;
+        const int b = ok ? col / T : 0, t = ok ? col - b * T : 0;
+        const float2* cb = cvec + (size_t)b * P;
+        const float2* at = ab + (size_t)t * P;
+        uint4* dh = reinterpret_cast<uint4*>(hi + (size_t)col * kdim);
+        uint4* dl = reinterpret_cast<uint4*>(lo + (size_t)col * kdim);
+        for (int g = threadIdx.x; g < nv; g += blockDim.x) {
+            __nv_bfloat162 h[4], l[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int kk = 4 * g + e;
+                float2 v = make_float2(0.f, 0.f);
+                if (ok && kk < nk) {
+                    const int pp = kpix[kk];
+                    const float2 c = cb[pp], a = at[pp];
+                    v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+                }
+                __nv_bfloat16 h0, l0, h1, l1;
+                split_bf16(v.x, h0, l0);
+                split_bf16(v.y, h1, l1);
+                h[e] = __halves2bfloat162(h0, h1);
+                l[e] = __halves2bfloat162(l0, l1);
+            }
+            dh[g] = *reinterpret_cast<const uint4*>(h);
+            dl[g] = *reinterpret_cast<const uint4*>(l);
         }
-        __nv_bfloat16 h0, l0, h1, l1;
-        split_bf16(v.x, h0, l0);
-        split_bf16(v.y, h1, l1);
-        reinterpret_cast<__nv_bfloat162*>(hi)[i] = __halves2bfloat162(h0, h1);
-        reinterpret_cast<__nv_bfloat162*>(lo)[i] = __halves2bfloat162(l0, l1);
     }
 }
 
@@ -596,9 +610,8 @@ void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     const int ncols = w.n * tb.T;
     const int n_pad = (ncols + TN - 1) / TN * TN;
     T2B_REQUIRE(n_pad <= op.n_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
-    const long long total = (long long)n_pad * op.kdim / 2;
-    k_split_img<<<4 * sms(), 256, 0, st>>>(w.cvec, tb.ab_c, ncols, tb.T, tb.P, tb.kpix, tb.nk, op.kdim, (__nv_bfloat16*)op.ah,
-                                           (__nv_bfloat16*)op.al, total);
+    k_split_img<<<std::min(n_pad, 16 * sms()), 128, 0, st>>>(w.cvec, tb.ab_c, ncols, n_pad, tb.T, tb.P, tb.kpix, tb.nk,
+                                                            op.kdim, (__nv_bfloat16*)op.ah, (__nv_bfloat16*)op.al);
     T2B_CUDA(cudaGetLastError());
 }
 

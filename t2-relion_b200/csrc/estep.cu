@@ -1133,7 +1133,10 @@ __global__ void __launch_bounds__(256) k_fine(Tables tb, Work w)
 #pragma unroll
             for (int v = 0; v < MAXV; v++) cr[r][v] = 0.f;
         }
-        for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        // only the pixels inside the projection radius: the projections, hence the
+        // cross and norm terms, are zero outside
+        for (int k = threadIdx.x; k < tb.nk; k += blockDim.x) {
+            const int p = tb.kpix[k];
             const float2 c = w.cvec[(size_t)b * P + p];
             const float wv = w.w2[(size_t)b * P + p];
             float2 a[MAXV];
@@ -1574,7 +1577,7 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
 
 void launch_fine(const Tables& tb, const Work& w, cudaStream_t st)
 {
-    k_fine<<<2 * sm_count(), 256, 0, st>>>(tb, w);
+    k_fine<<<3 * sm_count(), 256, 0, st>>>(tb, w);   // 80 registers: 3 CTAs per SM
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -1592,7 +1595,7 @@ void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* co
                     float* const* grid_weight, cudaStream_t st)
 {
     GridPtrs gp{grid_data, grid_weight};
-    k_wsum_bp<<<2 * sm_count(), 256, 0, st>>>(tb, w, g, gp);
+    k_wsum_bp<<<3 * sm_count(), 256, 0, st>>>(tb, w, g, gp);   // 80 registers: 3 CTAs per SM
     k_results<<<(w.n + 127) / 128, 128, 0, st>>>(tb, w);
     T2B_CUDA(cudaGetLastError());
 }

@@ -282,7 +282,6 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
 // score_j = log sum_t pdf_t(t) exp(dmin - d(j, t)), the log of the particle's
 // low-resolution posterior of orientation j up to a constant.
 constexpr int RS_CAND = 32;
-constexpr int RS_SMEM_MAX = 200 * 1024;
 constexpr int RS_TMAX = 96;            // translations per CTA tile (3 per lane)
 
 // Ring operands of the rescoring.  projR[oc][q]: the projection of every
@@ -319,46 +318,58 @@ __global__ void __launch_bounds__(256) k_ring_images(Tables tb, Work w, const in
 // Exact low-resolution score of each of the network's K1 candidates (see the
 // comment above).  CTA = 32 candidates x up to 96 translations of one particle;
 // warp w owns candidates 4w..4w+3, lane l the translations l, l+32, l+64, so a
-// thread keeps a 4 x 3 register tile per ring pixel.  Shared memory: the
-// particle's shifted ring image [pixel][translation] and the 32 candidates'
-// ring projections [candidate][pixel] (read as broadcasts).
+// thread keeps a 4 x 3 register tile.  The ring pixels stream through shared
+// memory in chunks of RS_Q (the particle's shifted ring image [pixel][t] and
+// the candidates' ring projections [candidate][pixel], read as broadcasts),
+// 33 KB per CTA so that several CTAs share an SM.
+constexpr int RS_Q = 32;
 __global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const float2* __restrict__ Sg,
                                                       const float* __restrict__ w2r, const float2* __restrict__ projR,
                                                       int nring, const int* __restrict__ cand, int k1,
                                                       float* __restrict__ score)
 {
-    extern __shared__ float2 S[];          // nring x RS_TMAX, then RS_CAND x nring
-    __shared__ float w2s[NET_MAX_RING];
+    __shared__ __align__(16) float2 S[RS_Q * RS_TMAX];
+    __shared__ float2 Pj[RS_CAND * (RS_Q + 1)];
+    __shared__ float w2s[RS_Q];
+    __shared__ int oc_s[RS_CAND];
     const int b = blockIdx.y, j0 = blockIdx.x * RS_CAND;
     const int T = tb.T;
-    float2* Pj = S + (size_t)nring * RS_TMAX;
-    {
-        const float4* src = reinterpret_cast<const float4*>(Sg + (size_t)b * nring * RS_TMAX);
-        float4* dst = reinterpret_cast<float4*>(S);
-        for (int i = threadIdx.x; i < nring * RS_TMAX / 2; i += blockDim.x) dst[i] = src[i];
+    if (threadIdx.x < RS_CAND) {
+        const int j = j0 + threadIdx.x;
+        oc_s[threadIdx.x] = j < k1 ? cand[(size_t)b * k1 + j] : -1;
     }
-    for (int q = threadIdx.x; q < nring; q += blockDim.x) w2s[q] = w2r[(size_t)b * nring + q];
-    for (int i = threadIdx.x; i < RS_CAND * nring; i += blockDim.x) {
-        const int jj = i / nring, q = i - jj * nring;
-        const int j = j0 + jj;
-        Pj[i] = j < k1 ? projR[(size_t)cand[(size_t)b * k1 + j] * nring + q] : make_float2(0.f, 0.f);
-    }
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float acc[4][3] = {};
     float nrm[4] = {};
-    const float2* pw = Pj + (size_t)(warp * 4) * nring;
-    for (int q = 0; q < nring; q++) {
-        const float2* sq = S + (size_t)q * RS_TMAX + lane;
-        const float2 s0 = sq[0], s1 = sq[32], s2 = sq[64];
-        const float wq = w2s[q];
+    for (int q0 = 0; q0 < nring; q0 += RS_Q) {
+        const int nq = min(RS_Q, nring - q0);
+        __syncthreads();
+        {
+            const float4* src = reinterpret_cast<const float4*>(Sg + ((size_t)b * nring + q0) * RS_TMAX);
+            float4* dst = reinterpret_cast<float4*>(S);
+            for (int i = threadIdx.x; i < nq * RS_TMAX / 2; i += blockDim.x) dst[i] = src[i];
+        }
+        for (int i = threadIdx.x; i < RS_CAND * RS_Q; i += blockDim.x) {
+            const int jj = i / RS_Q, q = i - jj * RS_Q;
+            const int oc = oc_s[jj];
+            Pj[jj * (RS_Q + 1) + q] = (oc >= 0 && q < nq) ? projR[(size_t)oc * nring + q0 + q] : make_float2(0.f, 0.f);
+        }
+        if (threadIdx.x < RS_Q) w2s[threadIdx.x] = threadIdx.x < nq ? w2r[(size_t)b * nring + q0 + threadIdx.x] : 0.f;
+        __syncthreads();
+        const float2* pw = Pj + (warp * 4) * (RS_Q + 1);
+#pragma unroll 4
+        for (int q = 0; q < nq; q++) {
+            const float2* sq = S + q * RS_TMAX + lane;
+            const float2 s0 = sq[0], s1 = sq[32], s2 = sq[64];
+            const float wq = w2s[q];
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const float2 pv = pw[c * nring + q];
-            acc[c][0] += pv.x * s0.x + pv.y * s0.y;
-            acc[c][1] += pv.x * s1.x + pv.y * s1.y;
-            acc[c][2] += pv.x * s2.x + pv.y * s2.y;
-            nrm[c] += wq * (pv.x * pv.x + pv.y * pv.y);
+            for (int c = 0; c < 4; c++) {
+                const float2 pv = pw[c * (RS_Q + 1) + q];
+                acc[c][0] += pv.x * s0.x + pv.y * s0.y;
+                acc[c][1] += pv.x * s1.x + pv.y * s1.y;
+                acc[c][2] += pv.x * s2.x + pv.y * s2.y;
+                nrm[c] += wq * (pv.x * pv.x + pv.y * pv.y);
+            }
         }
     }
 #pragma unroll
@@ -381,7 +392,7 @@ __global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const f
         for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
         const int j = j0 + warp * 4 + c;
         if (lane == 0 && j < k1) {
-            const int oc = cand[(size_t)b * k1 + j];
+            const int oc = oc_s[warp * 4 + c];
             score[(size_t)b * k1 + j] = (tb.skip[oc] || !(se > 0.)) ? -INFINITY
                                                                     : (float)(log(se) - (double)dmin + log(tb.pdf_oc[oc]));
         }
@@ -1363,7 +1374,6 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.c0a, 0, (size_t)N.na_max * sizeof(float)));
     T2B_CUDA(cudaMemset(N.norma, 0, (size_t)N.na_max * KO * sizeof(float)));
     T2B_CUDA(cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, KO * (int)sizeof(unsigned)));
-    T2B_CUDA(cudaFuncSetAttribute(k_prop_rescore, cudaFuncAttributeMaxDynamicSharedMemorySize, RS_SMEM_MAX));
     T2B_CUDA(cudaDeviceSynchronize());
     N.ready = true;
 }
@@ -1495,10 +1505,9 @@ void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st)
         // network top-k1, exact low-resolution rescoring, top-kprop of those
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO, N.k1,
                                                            N.cand1);
-        const size_t smem = (size_t)(RS_TMAX + RS_CAND) * N.nring * sizeof(float2);
         k_ring_images<<<w.n, 256, 0, st>>>(tb, w, N.ring, N.nring, N.Sg, N.w2r);
-        k_prop_rescore<<<dim3((N.k1 + RS_CAND - 1) / RS_CAND, w.n), 256, smem, st>>>(tb, w, N.Sg, N.w2r, N.projR, N.nring,
-                                                                                     N.cand1, N.k1, N.score1);
+        k_prop_rescore<<<dim3((N.k1 + RS_CAND - 1) / RS_CAND, w.n), 256, 0, st>>>(tb, w, N.Sg, N.w2r, N.projR, N.nring,
+                                                                                  N.cand1, N.k1, N.score1);
         k_rescore_select<<<w.n, 1024, 0, st>>>(N.cand1, N.score1, N.k1, N.kprop, N.prop);
     } else {
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO,
@@ -1628,7 +1637,7 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
         set_tile_shape(N, tb.T);
         net_setup(c, std::max(1, N.na_max));
         T2B_REQUIRE(f.rescore == 0 || (f.rescore >= f.topk && f.rescore <= NET_TOPK_CAND && f.rescore <= KO &&
-                                       tb.T <= RS_TMAX && (size_t)(RS_TMAX + RS_CAND) * N.nring * sizeof(float2) <= (size_t)RS_SMEM_MAX),
+                                       tb.T <= RS_TMAX),
                     T2B_ERR_ARG, "bad rescore candidate count");
         *rep = t2b_proposal_report{};
         rep->params = real_params(KO);
@@ -1818,7 +1827,7 @@ int t2b_proposal_enable(t2b_ctx* c, int topk, int rescore, int audit_every, doub
         const int B = c->cfg.max_batch;
         // at most ceil(B / every) multiples of `every` in any B consecutive stream positions
         net_setup(c, std::min(B, (B + audit_every - 1) / audit_every));
-        T2B_REQUIRE(rescore == 0 || c->tb.T <= RS_TMAX && (size_t)(RS_TMAX + RS_CAND) * N.nring * sizeof(float2) <= (size_t)RS_SMEM_MAX,
+        T2B_REQUIRE(rescore == 0 || c->tb.T <= RS_TMAX,
                     T2B_ERR_UNSUPPORTED, "the low-resolution rescoring takes at most 96 translations");
         N.k1 = rescore;
         N.kprop = topk;
