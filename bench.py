@@ -496,9 +496,11 @@ def main():
     # per-stage device times (CUDA events around each stage) of separately synchronised
     # host-path steps; not part of `value`
     stages = []
+    es.stage_timing(True)
     for _ in range(min(3, args.steps)):
         e2e_step()
         stages.append(es.stage_ms())
+    es.stage_timing(False)
     stages = np.mean(np.array(stages), axis=0)
     h2d = sum(v.numel() * v.element_size() for v in pin.values())
     d2h = sum(v.numel() * v.element_size() for v in hres.values())
@@ -542,7 +544,7 @@ def main():
                        "l2": "working set > L2 (bf16 hi/lo projection operands 0.97 GB per step)"},
             "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk.summary(), "roofline": roof,
             "stage_ms": {n: float(v) for n, v in zip(
-                ["prep_norms", "operand_split", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
+                ["prep_network", "operands_audit_norms", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
                  "wsum_bp"], stages)},
             "nr_sign_mean": float(res["nr_sign"].double().mean())}
     if learned is not None:

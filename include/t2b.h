@@ -196,9 +196,13 @@ int t2b_project(t2b_ctx* ctx, int iclass, const double* eulers, int n, int curre
 int t2b_debug_coarse_diff2(t2b_ctx* ctx, int b, float* out);
 int t2b_debug_fine(t2b_ctx* ctx, int b, long long* pairs, float* diff2, long long cap, long long* count);
 
-/* Kernel launches of the last device batch (the kernel nodes of its CUDA
- * graph); -1 when the last batch did not run as a graph. */
+/* Kernel launches of the last batch (the kernel nodes of its CUDA graph);
+ * -1 when the last batch did not run as a graph.  With use_graph set, both
+ * entry points replay a graph captured once per batch shape. */
 int t2b_last_launch_count(t2b_ctx* ctx, int* kernels);
+/* on != 0: host batches run uncaptured and record the per-stage events of
+ * t2b_last_stage_ms (measurement support); 0 (default): graph replay. */
+int t2b_stage_timing(t2b_ctx* ctx, int on);
 
 /* Device time of the stages of the last batch, in ms (CUDA events on the
  * stream the stages ran on): [0] prep (+ proposal network), [1] tensor-core

@@ -38,7 +38,7 @@ ABI_SYMBOLS = (
     "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_last_stage_ms",
     "t2b_sampling", "t2b_reconstruct_divide_noalloc", "t2b_last_launch_count",
     "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
-    "t2b_proposal_logits", "t2b_proposal_grad",
+    "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
 )
 
 
@@ -130,6 +130,7 @@ def _setup_prototypes():
     lib.t2b_debug_fine.argtypes = [v, i, v, v, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.t2b_last_stage_ms.argtypes = [v, v, i]
     lib.t2b_last_launch_count.argtypes = [v, ctypes.POINTER(i)]
+    lib.t2b_stage_timing.argtypes = [v, i]
     lib.t2b_sampling.argtypes = [i, i, ctypes.c_double, i, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double] + [ctypes.POINTER(i)] * 5 + [v] * 6
     lib.t2b_proposal_train.argtypes = [v, ctypes.POINTER(ProposalTrainConfig), ctypes.POINTER(ProposalReport)]
@@ -387,6 +388,9 @@ class EStep:
         k = ctypes.c_int()
         _check(lib.t2b_last_launch_count(self._h, ctypes.byref(k)))
         return k.value
+
+    def stage_timing(self, on):
+        _check(lib.t2b_stage_timing(self._h, 1 if on else 0))
 
     def stage_ms(self):
         ms = np.zeros(7, np.float32)

@@ -35,11 +35,7 @@ static T* dalloc(t2b_ctx* c, size_t n)
 
 static void free_allocs(t2b_ctx* c)
 {
-    if (c->gexec) {
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
-        c->gkey.clear();
-    }
+    c->drop_graphs();
     for (void* p : c->allocs) cudaFree(p);
     c->allocs.clear();
     c->configured = false;
@@ -497,6 +493,48 @@ static void collect_stage_ms(t2b_ctx* c)
 
 }  // namespace t2b
 
+namespace t2b {
+
+// Enqueue the batch in `w` on `st` as a CUDA graph: captured once per key
+// (batch shape, buffers, stream, proposal settings) into slot `g`, replayed
+// afterwards.  Returns the kernel nodes of the graph.
+static int replay_graph(t2b_ctx* c, Work& w, cudaStream_t st, const std::vector<const void*>& key,
+                        t2b_ctx::GraphSlot& g)
+{
+    if (!g.exec || key != g.key) {
+        if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
+        cudaGraph_t graph = nullptr;
+        T2B_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue_estep(c, w, st, false, true);
+        } catch (...) {
+            cudaStreamEndCapture(st, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        T2B_CUDA(cudaStreamEndCapture(st, &graph));
+        size_t nn = 0;
+        T2B_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
+        std::vector<cudaGraphNode_t> nodes(nn);
+        T2B_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
+        int kn = 0;
+        for (auto nd : nodes) {
+            cudaGraphNodeType ty;
+            T2B_CUDA(cudaGraphNodeGetType(nd, &ty));
+            if (ty == cudaGraphNodeTypeKernel) kn++;
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        T2B_CUDA(ie);
+        g.key = key;
+        g.kernels = kn;
+    }
+    T2B_CUDA(cudaGraphLaunch(g.exec, st));
+    return g.kernels;
+}
+
+}  // namespace t2b
+
 extern "C" {
 
 int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
@@ -515,7 +553,16 @@ int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
         T2B_CUDA(cudaMemcpyAsync((void*)w.ctf, b->ctf, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
         T2B_CUDA(cudaMemcpyAsync((void*)w.minv, b->minvsigma2, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
         T2B_CUDA(cudaMemcpyAsync((void*)w.scal, b->scalars, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, st));
-        enqueue_estep(c, w, st, true, true);
+        // the batch computation itself: a replayed graph unless stage timing is on
+        const bool graph = c->cfg.use_graph && !c->stage_timing;
+        if (graph) {
+            const std::vector<const void*> key = {(const void*)(intptr_t)n, (const void*)st,
+                                                  (const void*)(intptr_t)(c->net && c->net->enabled ? c->net->kprop : 0)};
+            c->last_kernels = replay_graph(c, w, st, key, c->g_host);
+        } else {
+            enqueue_estep(c, w, st, true, true);
+            c->last_kernels = -1;
+        }
         const int K = c->tb.K, half = c->cfg.ori_size / 2 + 1;
         auto d2h = [&](void* dst, const void* src, size_t bytes) {
             if (dst) T2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
@@ -539,7 +586,6 @@ int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
         d2h(r->learned, w.r_learned, n * sizeof(int));
         d2h(r->audit_mass, w.r_audit, n * sizeof(double));
         T2B_CUDA(cudaStreamSynchronize(st));
-        c->last_kernels = -1;
         collect_stage_ms(c);
         c->last_n = n;
     });
@@ -580,41 +626,21 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
                                                   r->wsum_pdf_dir, r->status, r->learned, r->audit_mass,
                                                   (const void*)st,
                                                   (const void*)(intptr_t)(c->net && c->net->enabled ? c->net->kprop : 0)};
-            if (!c->gexec || key != c->gkey) {
-                if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
-                cudaGraph_t graph = nullptr;
-                T2B_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                try {
-                    enqueue_estep(c, w, st, false, true);
-                } catch (...) {
-                    cudaStreamEndCapture(st, &graph);
-                    if (graph) cudaGraphDestroy(graph);
-                    throw;
-                }
-                T2B_CUDA(cudaStreamEndCapture(st, &graph));
-                size_t nn = 0;
-                T2B_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
-                std::vector<cudaGraphNode_t> nodes(nn);
-                T2B_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
-                int kn = 0;
-                for (auto nd : nodes) {
-                    cudaGraphNodeType ty;
-                    T2B_CUDA(cudaGraphNodeGetType(nd, &ty));
-                    if (ty == cudaGraphNodeTypeKernel) kn++;
-                }
-                const cudaError_t ie = cudaGraphInstantiate(&c->gexec, graph, 0);
-                cudaGraphDestroy(graph);
-                T2B_CUDA(ie);
-                c->gkey = key;
-                c->graph_kernels = kn;
-            }
-            T2B_CUDA(cudaGraphLaunch(c->gexec, st));
-            c->last_kernels = c->graph_kernels;
+            c->last_kernels = replay_graph(c, w, st, key, c->g_dev);
         } else {
             enqueue_estep(c, w, st, true, true);
             c->last_kernels = -1;
         }
         c->last_n = b->n;
+    });
+}
+
+int t2b_stage_timing(t2b_ctx* c, int on)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c, T2B_ERR_ARG, "null context");
+        std::lock_guard<std::mutex> lk(c->mu);
+        c->stage_timing = on != 0;
     });
 }
 

@@ -1213,7 +1213,7 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
     __shared__ int nent;
     __shared__ float ent_w[ENT_CAP];
     __shared__ int ent_tv[ENT_CAP];
-    __shared__ double ssig[1024];
+    __shared__ float ssig[1024];   // per-item ring sums (FP32, as the reference GPU path), FP64 across items
     __shared__ double shr[32];
     const int P = tb.P, T = tb.T, xh = tb.xh, s = tb.s;
     const int R = tb.ovs ? tb.R : 1, V = tb.ovs ? tb.V : 1;
@@ -1261,7 +1261,7 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
         const double S = tb.ovs ? w.sum_f[b] : w.sum_c[b];
         const double* sc = w.scal + 8 * (size_t)b;
         if (threadIdx.x == 0) nent = 0;
-        for (int i = threadIdx.x; i < nring; i += blockDim.x) ssig[i] = 0.;
+        for (int i = threadIdx.x; i < nring; i += blockDim.x) ssig[i] = 0.f;
         __syncthreads();
         if (w.status[b] == T2B_OK) {
             const long long nh = (qb - qa) * V;
@@ -1313,7 +1313,7 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                             fw += wx * c;
                         }
                         if (ires > -1) {
-                            atomicAdd(&ssig[ires], (double)wd);
+                            atomicAdd(&ssig[ires], wd);
                             nacc += wd;
                         }
                         // backprojection of this pixel (src/backprojector.cpp:140-228)
@@ -1372,7 +1372,7 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
         __syncthreads();
         const int half = tb.ori_size / 2 + 1;
         for (int i = threadIdx.x; i < nring && i < half; i += blockDim.x)
-            if (ssig[i] != 0.) atomicAdd(&w.r_sigma2[(size_t)b * half + i], ssig[i]);
+            if (ssig[i] != 0.f) atomicAdd(&w.r_sigma2[(size_t)b * half + i], (double)ssig[i]);
         __syncthreads();
     }
 }

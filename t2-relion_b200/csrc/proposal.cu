@@ -281,7 +281,6 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
 // (the coarse diff2 restricted to the ring, up to a per-particle constant) and
 // score_j = log sum_t pdf_t(t) exp(dmin - d(j, t)), the log of the particle's
 // low-resolution posterior of orientation j up to a constant.
-constexpr int RS_CAND = 32;
 constexpr int RS_TMAX = 96;            // translations per CTA tile (3 per lane)
 
 // Ring operands of the rescoring.  projR[oc][q]: the projection of every
@@ -316,31 +315,34 @@ __global__ void __launch_bounds__(256) k_ring_images(Tables tb, Work w, const in
 }
 
 // Exact low-resolution score of each of the network's K1 candidates (see the
-// comment above).  CTA = 32 candidates x up to 96 translations of one particle;
-// warp w owns candidates 4w..4w+3, lane l the translations l, l+32, l+64, so a
-// thread keeps a 4 x 3 register tile.  The ring pixels stream through shared
-// memory in chunks of RS_Q (the particle's shifted ring image [pixel][t] and
-// the candidates' ring projections [candidate][pixel], read as broadcasts),
-// 33 KB per CTA so that several CTAs share an SM.
+// comment above).  CTA = 64 candidates x up to 96 translations of one particle;
+// warp w owns candidates 8w..8w+7, lane l the translations l, l+32, l+64, so a
+// thread keeps an 8 x 3 register tile.  The ring pixels stream through shared
+// memory in chunks of RS_Q: the particle's shifted ring image [pixel][t] and
+// the candidates' ring projections [pixel][candidate] (a warp reads its 8
+// candidates of a pixel as four 16-byte broadcasts).
 constexpr int RS_Q = 32;
+constexpr int RS_CPW = 8;                  // candidates per warp
+constexpr int RS_CTA = 8 * RS_CPW;         // candidates per CTA
+constexpr int RS_PLD = RS_CTA + 2;         // row stride of Pj (16-byte rows, fewer bank conflicts on fill)
 __global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const float2* __restrict__ Sg,
                                                       const float* __restrict__ w2r, const float2* __restrict__ projR,
                                                       int nring, const int* __restrict__ cand, int k1,
                                                       float* __restrict__ score)
 {
     __shared__ __align__(16) float2 S[RS_Q * RS_TMAX];
-    __shared__ float2 Pj[RS_CAND * (RS_Q + 1)];
+    __shared__ __align__(16) float2 Pj[RS_Q * RS_PLD];
     __shared__ float w2s[RS_Q];
-    __shared__ int oc_s[RS_CAND];
-    const int b = blockIdx.y, j0 = blockIdx.x * RS_CAND;
+    __shared__ int oc_s[RS_CTA];
+    const int b = blockIdx.y, j0 = blockIdx.x * RS_CTA;
     const int T = tb.T;
-    if (threadIdx.x < RS_CAND) {
+    if (threadIdx.x < RS_CTA) {
         const int j = j0 + threadIdx.x;
         oc_s[threadIdx.x] = j < k1 ? cand[(size_t)b * k1 + j] : -1;
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float acc[4][3] = {};
-    float nrm[4] = {};
+    float acc[RS_CPW][3] = {};
+    float nrm[RS_CPW] = {};
     for (int q0 = 0; q0 < nring; q0 += RS_Q) {
         const int nq = min(RS_Q, nring - q0);
         __syncthreads();
@@ -349,31 +351,36 @@ __global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const f
             float4* dst = reinterpret_cast<float4*>(S);
             for (int i = threadIdx.x; i < nq * RS_TMAX / 2; i += blockDim.x) dst[i] = src[i];
         }
-        for (int i = threadIdx.x; i < RS_CAND * RS_Q; i += blockDim.x) {
-            const int jj = i / RS_Q, q = i - jj * RS_Q;
+        for (int i = threadIdx.x; i < RS_CTA * RS_Q; i += blockDim.x) {
+            const int jj = i / RS_Q, q = i - jj * RS_Q;     // q fastest: each candidate's row is contiguous
             const int oc = oc_s[jj];
-            Pj[jj * (RS_Q + 1) + q] = (oc >= 0 && q < nq) ? projR[(size_t)oc * nring + q0 + q] : make_float2(0.f, 0.f);
+            Pj[q * RS_PLD + jj] = (oc >= 0 && q < nq) ? projR[(size_t)oc * nring + q0 + q] : make_float2(0.f, 0.f);
         }
         if (threadIdx.x < RS_Q) w2s[threadIdx.x] = threadIdx.x < nq ? w2r[(size_t)b * nring + q0 + threadIdx.x] : 0.f;
         __syncthreads();
-        const float2* pw = Pj + (warp * 4) * (RS_Q + 1);
-#pragma unroll 4
+#pragma unroll 2
         for (int q = 0; q < nq; q++) {
             const float2* sq = S + q * RS_TMAX + lane;
             const float2 s0 = sq[0], s1 = sq[32], s2 = sq[64];
             const float wq = w2s[q];
+            const float4* pq = reinterpret_cast<const float4*>(Pj + q * RS_PLD + warp * RS_CPW);
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const float2 pv = pw[c * (RS_Q + 1) + q];
-                acc[c][0] += pv.x * s0.x + pv.y * s0.y;
-                acc[c][1] += pv.x * s1.x + pv.y * s1.y;
-                acc[c][2] += pv.x * s2.x + pv.y * s2.y;
-                nrm[c] += wq * (pv.x * pv.x + pv.y * pv.y);
+            for (int h = 0; h < RS_CPW / 2; h++) {
+                const float4 pp = pq[h];
+                const float2 pv[2] = {make_float2(pp.x, pp.y), make_float2(pp.z, pp.w)};
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int c = 2 * h + e;
+                    acc[c][0] += pv[e].x * s0.x + pv[e].y * s0.y;
+                    acc[c][1] += pv[e].x * s1.x + pv[e].y * s1.y;
+                    acc[c][2] += pv[e].x * s2.x + pv[e].y * s2.y;
+                    nrm[c] += wq * (pv[e].x * pv[e].x + pv[e].y * pv[e].y);
+                }
             }
         }
     }
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
+    for (int c = 0; c < RS_CPW; c++) {
         float d[3];
         float dmin = INFINITY;
 #pragma unroll
@@ -390,9 +397,9 @@ __global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const f
             if (t < T) se += w.pdf_t[(size_t)b * T + t] * exp((double)(dmin - d[m]));
         }
         for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
-        const int j = j0 + warp * 4 + c;
+        const int j = j0 + warp * RS_CPW + c;
         if (lane == 0 && j < k1) {
-            const int oc = oc_s[warp * 4 + c];
+            const int oc = oc_s[warp * RS_CPW + c];
             score[(size_t)b * k1 + j] = (tb.skip[oc] || !(se > 0.)) ? -INFINITY
                                                                     : (float)(log(se) - (double)dmin + log(tb.pdf_oc[oc]));
         }
@@ -1506,7 +1513,7 @@ void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st)
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO, N.k1,
                                                            N.cand1);
         k_ring_images<<<w.n, 256, 0, st>>>(tb, w, N.ring, N.nring, N.Sg, N.w2r);
-        k_prop_rescore<<<dim3((N.k1 + RS_CAND - 1) / RS_CAND, w.n), 256, 0, st>>>(tb, w, N.Sg, N.w2r, N.projR, N.nring,
+        k_prop_rescore<<<dim3((N.k1 + RS_CTA - 1) / RS_CTA, w.n), 256, 0, st>>>(tb, w, N.Sg, N.w2r, N.projR, N.nring,
                                                                                   N.cand1, N.k1, N.score1);
         k_rescore_select<<<w.n, 1024, 0, st>>>(N.cand1, N.score1, N.k1, N.kprop, N.prop);
     } else {
@@ -1570,14 +1577,7 @@ using namespace t2b;
 
 namespace {
 
-void drop_graph(t2b_ctx* c)
-{
-    if (c->gexec) {
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
-        c->gkey.clear();
-    }
-}
+void drop_graph(t2b_ctx* c) { c->drop_graphs(); }
 
 long long real_params(int KO)
 {

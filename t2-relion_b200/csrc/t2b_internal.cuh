@@ -252,9 +252,21 @@ struct t2b_ctx {
     float2** gd_table = nullptr;              // device table of per-class grid data pointers
     float** gw_table = nullptr;               // device table of per-class grid weight pointers
     int last_n = 0;                           // particles of the last batch
-    cudaGraphExec_t gexec = nullptr;          // captured device batch
-    std::vector<const void*> gkey;            // shape / buffers / stream it was captured for
-    int graph_kernels = -1;                   // kernel nodes of the captured batch
+    struct GraphSlot {                        // a captured batch and what it was captured for
+        cudaGraphExec_t exec = nullptr;
+        std::vector<const void*> key;         // shape / buffers / stream / proposal settings
+        int kernels = -1;                     // its kernel nodes
+    };
+    GraphSlot g_dev, g_host;                  // device and host entry points
+    bool stage_timing = false;                // host batches run uncaptured with stage events
+    void drop_graphs()
+    {
+        for (GraphSlot* g : {&g_dev, &g_host}) {
+            if (g->exec) cudaGraphExecDestroy(g->exec);
+            g->exec = nullptr;
+            g->key.clear();
+        }
+    }
     int last_kernels = -1;
     cudaEvent_t ev[8]{};
     float stage_ms[7]{};
