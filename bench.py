@@ -51,9 +51,12 @@ WORKLOAD = dict(name="refine3d_box128_order3_ovs1", ori_size=128, angpix=1.3, n_
 # reduced case for ncu captures (device memory of a few GB): HEALPix order 2, otherwise identical
 PROFILE_WORKLOAD = dict(WORKLOAD, name="refine3d_box128_order2_ovs1_profile", order=2)
 METRIC = "E-step particles/s box128: learned+split-BF16 vs plain FP32 GPU; roofline %"
-# learned proposals: network top-512 rescored at low resolution, best 64 to the coarse
+# learned proposals: network top-1024 rescored at low resolution, best 64 to the coarse
 # pass; every 50th particle (2 %) audited by the full coarse pass (>= 0.999 of its mass)
-PROP = dict(topk=64, rescore=512, audit_every=50, audit_mass=0.999)
+PROP = dict(topk=64, rescore=1024, audit_every=50, audit_mass=0.999)
+# DRAM bytes (read + write) of the audit + proposal k_diff2_tc launches of one learned step
+# at 128 particles, from one ncu capture (None until captured)
+LEARNED_TRAFFIC = None  # set once the 96-column proposal tiles are captured
 
 
 def build_problem(t2b, sy, n_particles, seed):
@@ -376,6 +379,8 @@ def main():
     ap.add_argument("--mode", default="learned", choices=["learned", "splitbf16", "plain"],
                     help="learned: proposal network + split-BF16 tensor-core contraction (the headline); "
                          "splitbf16: full coarse pass on tcgen05; plain: full coarse pass, FP32 SIMT")
+    ap.add_argument("--topk", type=int, default=PROP["topk"], help="learned: proposals per particle")
+    ap.add_argument("--rescore", type=int, default=PROP["rescore"], help="learned: network candidates rescored")
     ap.add_argument("--train-particles", type=int, default=200000)
     ap.add_argument("--train-epochs", type=int, default=8)
     ap.add_argument("--batch", type=int, default=128)
@@ -386,6 +391,7 @@ def main():
     args = ap.parse_args()
     if args.profile_case:
         WORKLOAD.update(PROFILE_WORKLOAD)
+    PROP.update(topk=args.topk, rescore=args.rescore)
     world, rank, local = dist_init()
     if args.impl == "reference":
         run_reference(args, world, rank)
@@ -408,11 +414,13 @@ def main():
         t0 = time.perf_counter()
         rep = es.train_proposals(parts["minv"][0], n_train=args.train_particles, n_posterior=8192, n_val=1024,
                                  epochs=args.train_epochs, batch=256, lr=3e-4, topk=PROP["topk"],
-                                 rescore=PROP["rescore"], seed=WORKLOAD["seed"], max_shift=WORKLOAD["offset_range"])
+                                 rescore=PROP["rescore"], seed=WORKLOAD["seed"], max_shift=WORKLOAD["offset_range"],
+                                 sigma_deg=5.0)
         learned = {"train_s": time.perf_counter() - t0, "train_particles": args.train_particles,
                    "train_epochs": args.train_epochs, "val_mass_init": rep["val_mass_init"],
                    "val_mass_network": rep["val_mass_trained"], "val_mass_rescored": rep["val_mass_rescored"],
-                   "val_frac_999_rescored": rep["val_frac_999_rescored"], "final_loss": rep["loss"][-1],
+                   "val_frac_999_rescored": rep["val_frac_999_rescored"],
+                   "val_frac_999_candidates": rep["val_frac_999_candidates"], "final_loss": rep["loss"][-1],
                    **PROP}
         es.enable_proposals(topk=PROP["topk"], rescore=PROP["rescore"], audit_every=PROP["audit_every"],
                             audit_mass=PROP["audit_mass"])
@@ -507,35 +515,57 @@ def main():
     e2e = {"value": B * args.steps * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h}
 
-    # roofline of the dominant kernel (coarse diff2 contraction)
+    # roofline of the dominant kernel (the tcgen05 contraction k_diff2_tc)
     O, T = samp["n_dir"] * samp["n_psi"], samp["n_trans"]
-    flops = 8.0 * K * O * T * P * B
-    if learned is not None:   # contraction on the proposals only
-        flops = 8.0 * PROP["topk"] * T * P * B
-    gemm = float(stages[2])
     peaks, src = measured_peaks()
-    if mode == t2b.DIFF2_SPLIT_BF16:
-        peak = peaks.get("bf16_tflops_sustained", 1400.0)
-        bound = "tensor"
-    else:
-        peak = 148 * 128 * 2 * 1.965e-3  # FP32 SIMT nominal TFLOP/s (no measured figure)
-        bound = "fp32_simt"
-        src = "nominal"
-    achieved = flops / (gemm / 1000.0) / 1e12
     # the contraction runs over the nk window pixels inside the projection radius only
-    # (projections are zero outside); executed = what the units did
+    # (projections are zero outside); "executed" counts what the tensor cores did
     nk = int(sum(1 for n in range(P) if (lambda i, x: x * x + (i if i < s // 2 + 1 else i - s) ** 2)(n // (s // 2 + 1), n % (s // 2 + 1)) <= (s // 2) ** 2))
-    executed = (12.0 if mode == t2b.DIFF2_SPLIT_BF16 else 4.0) * K * O * T * nk * B / (gemm / 1000.0) / 1e12
-    # DRAM bytes (read + write) of one diff2 launch of this exact workload from one ncu capture
-    # (dram__bytes_read.sum 8.16 GB + dram__bytes_write.sum 1.56 GB at 128 particles;
-    # profiles/k_diff2_tc_box128_order3_b128_dram.md), scaled by the batch size
-    traffic = None
-    if mode == t2b.DIFF2_SPLIT_BF16 and not args.profile_case:
-        traffic = (8.16e9 + 1.56e9) * B / 128.0
-    roof = {"bound": bound, "kernel": "k_diff2_tc" if mode else "k_diff2_simt", "achieved": achieved,
-            "executed_tflops": executed, "contraction_pixels": nk,
-            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src,
-            "traffic": traffic, "flops_per_launch": flops}
+    kdim = (2 * nk + 63) // 64 * 64
+    if learned is None:
+        flops = 8.0 * K * O * T * P * B
+        gemm = float(stages[2])
+        if mode == t2b.DIFF2_SPLIT_BF16:
+            peak = peaks.get("bf16_tflops_sustained", 1400.0)
+            bound = "tensor"
+        else:
+            peak = 148 * 128 * 2 * 1.965e-3  # FP32 SIMT nominal TFLOP/s (no measured figure)
+            bound = "fp32_simt"
+            src = "nominal"
+        achieved = flops / (gemm / 1000.0) / 1e12
+        executed = (12.0 if mode == t2b.DIFF2_SPLIT_BF16 else 4.0) * K * O * T * nk * B / (gemm / 1000.0) / 1e12
+        # DRAM bytes (read + write) of one diff2 launch of this exact workload from one ncu capture
+        # (dram__bytes_read.sum 8.16 GB + dram__bytes_write.sum 1.56 GB at 128 particles;
+        # profiles/k_diff2_tc_box128_order3_b128_dram.md), scaled by the batch size
+        traffic = None
+        if mode == t2b.DIFF2_SPLIT_BF16 and not args.profile_case:
+            traffic = (8.16e9 + 1.56e9) * B / 128.0
+        roof = {"bound": bound, "kernel": "k_diff2_tc" if mode else "k_diff2_simt", "achieved": achieved,
+                "executed_tflops": executed, "contraction_pixels": nk,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src,
+                "traffic": traffic, "flops_per_launch": flops}
+    else:
+        # learned: the audit's full coarse contraction (audited particles x every orientation)
+        # and the contraction on the proposals (every particle x its top-k), each one launch of
+        # k_diff2_tc per step, timed by the library's CUDA events around exactly those launches
+        na = float((hres["audit_mass"].numpy() >= 0).sum())          # audited particles of the last step
+        t_audit, t_prop = float(stages[7]), float(stages[8])
+        f_audit = 8.0 * K * O * T * P * na
+        f_prop = 8.0 * PROP["topk"] * T * P * B
+        ntile_audit = ((K * O + 127) // 128) * ((int(np.ceil(B / PROP["audit_every"])) * T + 255) // 256)
+        tile_flops = 128 * 256 * kdim * 2 * 3.0
+        if T <= 96:      # one particle per 128 x 96 tile
+            prop_exec = B * 128 * 96 * kdim * 2 * 3.0
+        else:
+            prop_exec = ((B + 1) // 2 if (PROP["topk"] <= 64 and 2 * T <= 256) else B) * tile_flops
+        executed = (ntile_audit * tile_flops + prop_exec) / ((t_audit + t_prop) / 1000.0) / 1e12
+        peak = peaks.get("bf16_tflops_sustained", 1400.0)
+        achieved = (f_audit + f_prop) / ((t_audit + t_prop) / 1000.0) / 1e12
+        roof = {"bound": "tensor", "kernel": "k_diff2_tc (audit + proposal launches)", "achieved": achieved,
+                "executed_tflops": executed, "contraction_pixels": nk, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "peak_source": src, "traffic": LEARNED_TRAFFIC,
+                "flops_per_launch": (f_audit + f_prop) / 2.0, "audit_ms": t_audit, "proposal_ms": t_prop,
+                "audited_particles": na}
     line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+bf16x3/f64" if mode else "f32/f64", "data": "synthetic",
@@ -545,7 +575,7 @@ def main():
             "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk.summary(), "roofline": roof,
             "stage_ms": {n: float(v) for n, v in zip(
                 ["prep_network", "operands_audit_norms", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
-                 "wsum_bp"], stages)},
+                 "wsum_bp", "audit_contraction", "proposal_contraction"], stages)},
             "nr_sign_mean": float(res["nr_sign"].double().mean())}
     if learned is not None:
         learned["learned_fraction"] = float(hres["learned"].double().mean())

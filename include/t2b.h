@@ -208,7 +208,9 @@ int t2b_stage_timing(t2b_ctx* ctx, int on);
  * stream the stages ran on): [0] prep (+ proposal network), [1] tensor-core
  * operand split (+ proposal audit) + norms, [2] coarse diff2 contraction (on the
  * proposals when they are in use), [3] coarse weights + significance + compaction,
- * [4] fine pass, [5] fine weights, [6] weighted sums + backprojection.  n <= 7.
+ * [4] fine pass, [5] fine weights, [6] weighted sums + backprojection; with
+ * learned proposals also [7] the audit's full coarse contraction and [8] the
+ * contraction on the proposals alone (-1 otherwise).  n <= 9.
  * A batch that ran as a CUDA graph reports -1 for every stage. */
 int t2b_last_stage_ms(t2b_ctx* ctx, float* ms, int n);
 
@@ -260,6 +262,7 @@ typedef struct {
     double val_mass_rescored;   /* mean mass in the top-k after low-resolution rescoring   */
     double val_mass_min_rescored;
     double val_frac_999_rescored;
+    double val_frac_999_candidates; /* ... particles whose `rescore` network candidates hold >= 0.999 */
     double gen_ms, label_ms, train_ms;
     long long params;           /* network parameters                                      */
 } t2b_proposal_report;

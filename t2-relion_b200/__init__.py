@@ -103,7 +103,7 @@ class ProposalReport(ctypes.Structure):
                 ("val_mass_trained", ctypes.c_double), ("val_mass_min", ctypes.c_double),
                 ("val_frac_999", ctypes.c_double), ("val_true_hit", ctypes.c_double),
                 ("val_mass_rescored", ctypes.c_double), ("val_mass_min_rescored", ctypes.c_double),
-                ("val_frac_999_rescored", ctypes.c_double),
+                ("val_frac_999_rescored", ctypes.c_double), ("val_frac_999_candidates", ctypes.c_double),
                 ("gen_ms", ctypes.c_double), ("label_ms", ctypes.c_double), ("train_ms", ctypes.c_double),
                 ("params", ctypes.c_longlong)]
 
@@ -324,7 +324,7 @@ class EStep:
     # ---------------------------------------------- learned orientation proposals
     def train_proposals(self, minvsigma2, n_train=200000, n_posterior=20000, n_val=1024, epochs=4, batch=256,
                         lr=3e-4, topk=64, rescore=0, seed=1, defocus=(10000., 30000.), astig=1000., voltage=300.,
-                        cs=2.7, q0=0.1, max_shift=5.0, sigma_deg=8.0, alpha=3.0):
+                        cs=2.7, q0=0.1, max_shift=5.0, sigma_deg=5.0, alpha=3.0):
         """Train the proposal network on particles generated from the current
         references (t2b_proposal_train); returns the report as a dict."""
         mv = np.ascontiguousarray(minvsigma2, np.float32)
@@ -393,8 +393,8 @@ class EStep:
         _check(lib.t2b_stage_timing(self._h, 1 if on else 0))
 
     def stage_ms(self):
-        ms = np.zeros(7, np.float32)
-        _check(lib.t2b_last_stage_ms(self._h, _ptr(ms), 7))
+        ms = np.zeros(9, np.float32)
+        _check(lib.t2b_last_stage_ms(self._h, _ptr(ms), 9))
         return ms
 
     def coarse_diff2(self, b):

@@ -455,11 +455,11 @@ void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool
     if (pm) proposal_infer(c, w, st);
     if (stage_events) cudaEventRecord(c->ev[1], st);
     if (tc) tc_split_images(tb, w, c->tc, st);
-    if (pm) proposal_audit(c, w, st);
+    if (pm) proposal_audit(c, w, st, stage_events ? c->ev + 8 : nullptr);
     if (tc) tc_launch_norms(tb, w, c->tc, st, w.gate, 0);
     else launch_norms(tb, w, st);
     if (stage_events) cudaEventRecord(c->ev[2], st);
-    if (pm) proposal_coarse(c, w, st);
+    if (pm) proposal_coarse(c, w, st, stage_events ? c->ev + 10 : nullptr);
     if (tc) tc_launch_diff2(tb, w, c->tc, st, w.gate, 0);
     else launch_diff2_simt(tb, w, st);
     if (stage_events) cudaEventRecord(c->ev[3], st);
@@ -471,6 +471,7 @@ void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool
     if (stage_events) cudaEventRecord(c->ev[6], st);
     launch_wsum_bp(tb, w, c->gvol[0], c->gd_table, c->gw_table, st);
     if (stage_events) cudaEventRecord(c->ev[7], st);
+    if (stage_events) c->prop_events = pm;
 }
 
 static void check_batch(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
@@ -487,6 +488,13 @@ static void collect_stage_ms(t2b_ctx* c)
         if (c->last_kernels >= 0 || cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]) != cudaSuccess) {
             cudaGetLastError();  // do not leave the failure as the runtime's last error
             c->stage_ms[i] = -1.f;
+        }
+    }
+    for (int i = 0; i < 2; i++) {
+        if (c->last_kernels >= 0 || !c->prop_events ||
+            cudaEventElapsedTime(&c->stage_ms[7 + i], c->ev[8 + 2 * i], c->ev[9 + 2 * i]) != cudaSuccess) {
+            cudaGetLastError();
+            c->stage_ms[7 + i] = -1.f;
         }
     }
 }
@@ -548,15 +556,18 @@ int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
         const int n = b->n, P = c->tb.P;
         w.n = n;
         T2B_CUDA(cudaMemcpyAsync((void*)w.fimg, b->fimg, (size_t)n * P * sizeof(float2), cudaMemcpyHostToDevice, st));
-        T2B_CUDA(cudaMemcpyAsync((void*)w.fimg_nm, b->fimg_nomask ? b->fimg_nomask : b->fimg, (size_t)n * P * sizeof(float2),
-                                 cudaMemcpyHostToDevice, st));
+        if (b->fimg_nomask)
+            T2B_CUDA(cudaMemcpyAsync((void*)w.fimg_nm, b->fimg_nomask, (size_t)n * P * sizeof(float2),
+                                     cudaMemcpyHostToDevice, st));
+        else
+            w.fimg_nm = w.fimg;   // no separate unmasked image: the masked one serves both
         T2B_CUDA(cudaMemcpyAsync((void*)w.ctf, b->ctf, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
         T2B_CUDA(cudaMemcpyAsync((void*)w.minv, b->minvsigma2, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
         T2B_CUDA(cudaMemcpyAsync((void*)w.scal, b->scalars, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, st));
         // the batch computation itself: a replayed graph unless stage timing is on
         const bool graph = c->cfg.use_graph && !c->stage_timing;
         if (graph) {
-            const std::vector<const void*> key = {(const void*)(intptr_t)n, (const void*)st,
+            const std::vector<const void*> key = {(const void*)(intptr_t)n, (const void*)st, (const void*)w.fimg_nm,
                                                   (const void*)(intptr_t)(c->net && c->net->enabled ? c->net->kprop : 0)};
             c->last_kernels = replay_graph(c, w, st, key, c->g_host);
         } else {
@@ -655,7 +666,7 @@ int t2b_last_launch_count(t2b_ctx* c, int* kernels)
 int t2b_last_stage_ms(t2b_ctx* c, float* ms, int n)
 {
     return guarded([&] {
-        T2B_REQUIRE(c && ms && n >= 0 && n <= 7, T2B_ERR_ARG, "bad arguments");
+        T2B_REQUIRE(c && ms && n >= 0 && n <= 9, T2B_ERR_ARG, "bad arguments");
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard g(c->device);
         T2B_CUDA(cudaStreamSynchronize(c->stream));

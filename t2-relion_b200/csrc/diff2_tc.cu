@@ -41,8 +41,10 @@ constexpr int EPI_LD = 33;
 constexpr size_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 4 * 32 * EPI_LD * 4 + 4 * (TN + 2) * 4;
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
-// instruction descriptor: D f32, A/B bf16, both K-major, N = 256, M = 128
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+// instruction descriptor: D f32, A/B bf16, both K-major, M = 128; N (bits 17-22, N/8)
+// is set per launch (256, or 96 for one particle's translations)
+constexpr uint32_t IDESC_BASE = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TM >> 4) << 24);
+__host__ __device__ constexpr uint32_t idesc_for(int n) { return IDESC_BASE | ((uint32_t)(n >> 3) << 17); }
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -109,12 +111,12 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr)
     return d;
 }
 
-__device__ __forceinline__ void umma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t accum)
+__device__ __forceinline__ void umma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum)
 {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
             dtmem),
-        "l"(a), "l"(b), "r"(IDESC), "r"(accum));
+        "l"(a), "l"(b), "r"(idesc), "r"(accum));
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar)
 {
@@ -176,6 +178,9 @@ struct TcParams {
     const int* prop;          // mode 1: global orientation of every (particle, proposal)
     const int* gate;          // run only when (*gate != 0) == gate_run (null: always)
     int gate_run;
+    int tn;                   // N of the tile (multiple of 32, <= 256; 0 = 256); B maps with a tn-row box
+    int mtp;                  // mode 1 with ppt = 1: consecutive tiles per particle (0 = 1); A rows of
+                              // tile i are rows [i*128, i*128+128), proposal j = (i % mtp)*128 + row
 };
 
 // maps: device array of tensor-map descriptors (encoded once per configuration);
@@ -230,7 +235,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         int it = 0;
         int issued[STAGES] = {0, 0};
         uint32_t last_par[STAGES] = {0, 0};
-        const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + B_BYTES * (p.products >= 2 ? 2u : 1u);
+        const uint32_t b_bytes = (uint32_t)(p.tn ? p.tn : TN) * TK * 2;
+        const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + b_bytes * (p.products >= 2 ? 2u : 1u);
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
             int ya, yb;
             if (p.mode == 0) {
@@ -240,7 +246,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 yb = nt * TN;
             } else {
                 ya = tile * TM;
-                yb = tile * p.ppt * p.T;
+                yb = (tile / (p.mtp ? p.mtp : 1)) * p.ppt * p.T;
             }
             for (int kb = 0; kb < p.kblocks; kb++, it++) {
                 const int s = it % STAGES;
@@ -264,6 +270,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         }
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer
+        const uint32_t idesc = idesc_for(p.tn ? p.tn : TN);
         int it = 0, tl = 0;
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x, tl++) {
             const int abuf = tl & 1;
@@ -283,9 +290,9 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
 #pragma unroll
                 for (int k = 0; k < TK / 16; k++) {
                     const uint64_t ko = (uint64_t)(k * 32) >> 4;  // 32 bytes per K=16 step
-                    umma(dt, dPh + ko, dIh + ko, (kb | k) != 0);
-                    if (p.products >= 2) umma(dt, dPh + ko, dIl + ko, 1);
-                    if (p.products == 3) umma(dt, dPl + ko, dIh + ko, 1);
+                    umma(dt, dPh + ko, dIh + ko, idesc, (kb | k) != 0);
+                    if (p.products >= 2) umma(dt, dPh + ko, dIl + ko, idesc, 1);
+                    if (p.products == 3) umma(dt, dPl + ko, dIh + ko, idesc, 1);
                 }
                 umma_commit(&empty_bar[s]);  // stage free once these MMAs retire
             }
@@ -311,10 +318,27 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             if (!mbar_wait(&tfull_bar[abuf], aph, &abort_flag)) { abort_flag = 1; break; }
             tc_fence_after();
             const int n0 = nt * TN;
-            const int bfirst = p.mode == 0 ? n0 / p.T : tile * p.ppt;
+            const int mtp = p.mtp ? p.mtp : 1;
+            const int bfirst = p.mode == 0 ? n0 / p.T : (tile / mtp) * p.ppt;
+            const int jbase = p.mode == 0 ? 0 : (tile % mtp) * TM;
             for (int i = lane; i < TN + 2; i += 32) wmin[i] = 0xffffffffu;
+            // proposal tiles: the per-row data of the warp's 32 rows (orientation skip flag
+            // and norm), one row per lane, broadcast by shuffles in the chunk loop below
+            int my_skip = 1;
+            float my_norm = 0.f;
+            if (p.mode != 0) {
+                const int row = q * 32 + lane;
+                const int bp = row / p.kslot, j = jbase + row - bp * p.kslot;
+                const int bb = bfirst + bp;
+                if (bp < p.ppt && bb < p.ncols && j < p.KO) {
+                    const size_t pj = (size_t)bb * p.KO + j;
+                    my_skip = p.skip[p.prop[pj]] ? 1 : 0;
+                    my_norm = p.norms[pj];
+                }
+            }
             __syncwarp();
-            for (int c = 0; c < TN / 32; c++) {
+            const int nchunk = (p.tn ? p.tn : TN) / 32;
+            for (int c = 0; c < nchunk; c++) {
                 uint32_t v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
 #pragma unroll
@@ -353,14 +377,16 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                     const float c0 = cok ? p.c0[b] : 0.f;
                     for (int r = 0; r < 32; r++) {
                         const int row = q * 32 + r;
-                        const int bp = row / p.kslot, j = row - bp * p.kslot;
+                        const int bp = row / p.kslot, j = jbase + row - bp * p.kslot;
+                        const int skip_r = __shfl_sync(0xffffffffu, my_skip, r);
+                        const float norm_r = __shfl_sync(0xffffffffu, my_norm, r);
                         if (!cok || bp != bc || j >= p.KO) continue;
                         const size_t pj = (size_t)b * p.KO + j;
                         float d;
-                        if (p.skip[p.prop[pj]]) {
+                        if (skip_r) {
                             d = -999.f;
                         } else {
-                            d = c0 + p.norms[pj] - sbuf[r * EPI_LD + lane];
+                            d = c0 + norm_r - sbuf[r * EPI_LD + lane];
                             lmin = min(lmin, f2key(d));
                         }
                         p.d2c[pj * p.T + t] = d;
@@ -526,7 +552,7 @@ size_t tc_kn(int nk) { return (size_t)((nk + TK - 1) / TK) * TK; }
 
 // descriptor slots in op.maps (TC_MAP_SLOTS of 128 bytes)
 enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL,
-       MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_COUNT };
+       MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_IH96, MAP_IL96, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL, MAP_COUNT };
 static_assert(MAP_COUNT <= TC_MAP_SLOTS, "tensor-map slots");
 static_assert(sizeof(CUtensorMap) == 128, "tensor-map size");
 
@@ -550,6 +576,9 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
     h[MAP_WL] = make_map(op.wl, op.b_pad, op.kn, TN);
     T2B_CUDA(cudaStreamSynchronize(st));
     T2B_CUDA(cudaMemcpy(op.maps, h, sizeof(h), cudaMemcpyHostToDevice));  // slots MAP_PH..MAP_WL
+    // the image operand with a 96-row box: one particle's translations per tile (proposal pass)
+    CUtensorMap h96[2] = {make_map(op.ah, op.n_pad, op.kdim, 96), make_map(op.al, op.n_pad, op.kdim, 96)};
+    T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * MAP_IH96, h96, sizeof(h96), cudaMemcpyHostToDevice));
     const int rows = tb.K * tb.O;
     // sizes were fixed when the operand buffers were allocated
     T2B_REQUIRE(op.m_pad == (rows + TM - 1) / TM * TM && op.kdim == (int)tc_kdim(tb.nk), T2B_ERR_STATE,
@@ -650,16 +679,59 @@ void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_
 
 int tc_slot_proposals() { return MAP_PGH; }
 int tc_slot_audit() { return MAP_IAH; }
+int tc_slot_rescore() { return MAP_RAH; }
+
+void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows)
+{
+    T2B_REQUIRE(slot >= MAP_PGH && slot < MAP_COUNT && op.maps, T2B_ERR_STATE, "bad tensor-map slot");
+    const CUtensorMap m = make_map(ptr, rows, kdim, box_rows);
+    T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * slot, &m, 128, cudaMemcpyHostToDevice));
+}
+
+// Low-resolution rescoring contraction: particle b's K1 candidates (gathered ring
+// projections, slots MAP_RAH/RAL, rows b*K1 + j) against its T shifted ring
+// images (MAP_RBH/RBL, 96-row box from row b*T); d = c0 + norm - C into d2
+// (n x K1 x T), per-particle minimum into minkey.  K1 a multiple of 128.
+void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* c0, const float* norms,
+                       const unsigned char* skip, const int* cand, float* d2, unsigned* minkey, int* err,
+                       const int* gate, cudaStream_t st)
+{
+    T2B_REQUIRE(k1 % TM == 0 && T <= 96 && kr % TK == 0, T2B_ERR_STATE, "rescoring tile shape");
+    TcParams p{};
+    p.mode = 1;
+    p.ppt = 1;
+    p.kslot = TM;
+    p.mtp = k1 / TM;
+    p.tn = 96;
+    p.m_tiles = n * p.mtp;
+    p.n_tiles = 1;
+    p.kblocks = kr / TK;
+    p.KO = k1;
+    p.T = T;
+    p.ncols = n;
+    p.c0 = c0;
+    p.norms = norms;
+    p.skip = skip;
+    p.prop = cand;
+    p.d2c = d2;
+    p.minkey = minkey;
+    p.err = err;
+    p.products = 3;
+    p.gate = gate;
+    p.gate_run = 1;
+    launch_gemm(op, MAP_RAH, MAP_RBH, p, st);
+}
 
 // Restricted coarse pass: every particle against its own proposals only.
 // Tiles of ppt particles: A = gathered proposal projections (slots MAP_PGH/PGL,
-// 128 rows per tile), B = the particles' shifted images (MAP_IH/IL, rows from
-// tile*ppt*T).  Runs while *w.gate != 0.
-void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, const float* nprop,
+// 128 rows per tile), B = the particles' shifted images (rows from tile*ppt*T;
+// tn = 96: one particle per tile through the 96-row-box maps MAP_IH96/IL96,
+// tn = 256: MAP_IH/IL).  Runs while *w.gate != 0.
+void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, int tn, const float* nprop,
                     cudaStream_t st)
 {
-    T2B_REQUIRE(ppt >= 1 && ppt * kslot == TM && ppt * tb.T <= TN && w.kprop <= kslot, T2B_ERR_STATE,
-                "proposal tile shape");
+    T2B_REQUIRE(ppt >= 1 && ppt * kslot == TM && ppt * tb.T <= tn && w.kprop <= kslot && (tn == 96 || tn == TN),
+                T2B_ERR_STATE, "proposal tile shape");
     TcParams p{};
     p.mode = 1;
     p.ppt = ppt;
@@ -680,7 +752,8 @@ void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, in
     p.products = 3;
     p.gate = w.gate;
     p.gate_run = 1;
-    launch_gemm(op, MAP_PGH, MAP_IH, p, st);
+    p.tn = tn;
+    launch_gemm(op, MAP_PGH, tn == 96 ? MAP_IH96 : MAP_IH, p, st);
 }
 
 // Full coarse pass of the audited particles: dense tiles over every

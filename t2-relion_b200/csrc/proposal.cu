@@ -214,7 +214,7 @@ __global__ void k_bias_act(const float* __restrict__ y, const bf16* __restrict__
 // selected set.
 __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits, const bf16* __restrict__ bias,
                                                const unsigned char* __restrict__ skip, int KO, int k,
-                                               int* __restrict__ prop)
+                                               int* __restrict__ prop, int ranked)
 {
     extern __shared__ unsigned keys[];
     __shared__ unsigned hist[256];
@@ -246,6 +246,37 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
         __syncthreads();
     }
     const unsigned kth = s_prefix;
+    if (!ranked) {
+        // the set only, in index order: keys above the k-th, then the first ties at it;
+        // thread t owns the contiguous index range [t*per, (t+1)*per)
+        __shared__ unsigned sc_hi[1024], sc_eq[1024];
+        const int per = (KO + blockDim.x - 1) / blockDim.x;
+        const int i0 = threadIdx.x * per, i1 = min(KO, i0 + per);
+        unsigned nhi = 0, neq = 0;
+        for (int i = i0; i < i1; i++) { nhi += keys[i] > kth; neq += keys[i] == kth; }
+        sc_hi[threadIdx.x] = nhi;
+        sc_eq[threadIdx.x] = neq;
+        __syncthreads();
+        for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+            const unsigned a = threadIdx.x >= off ? sc_hi[threadIdx.x - off] : 0u;
+            const unsigned e = threadIdx.x >= off ? sc_eq[threadIdx.x - off] : 0u;
+            __syncthreads();
+            sc_hi[threadIdx.x] += a;
+            sc_eq[threadIdx.x] += e;
+            __syncthreads();
+        }
+        const unsigned total_hi = sc_hi[blockDim.x - 1];
+        unsigned ph = sc_hi[threadIdx.x] - nhi, pe = sc_eq[threadIdx.x] - neq;
+        for (int i = i0; i < i1; i++) {
+            if (keys[i] > kth) {
+                prop[(size_t)b * k + ph++] = i;
+            } else if (keys[i] == kth) {
+                const unsigned pos = total_hi + pe++;
+                if (pos < (unsigned)k) prop[(size_t)b * k + pos] = i;
+            }
+        }
+        return;
+    }
     // every key above the k-th, and the ties at it
     for (int i = threadIdx.x; i < KO; i += blockDim.x)
         if (keys[i] >= kth) {
@@ -277,132 +308,123 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
 
 // ------------------------------------------------ low-resolution rescoring
 // Exact low-resolution score of each of the network's K1 candidates: over the
-// ring pixels only, d(j, t) = sum_p w2_p |P_j,p|^2 - Re(P_j,p conj(cvec_p ab_t,p))
-// (the coarse diff2 restricted to the ring, up to a per-particle constant) and
-// score_j = log sum_t pdf_t(t) exp(dmin - d(j, t)), the log of the particle's
-// low-resolution posterior of orientation j up to a constant.
-constexpr int RS_TMAX = 96;            // translations per CTA tile (3 per lane)
+// ring pixels only, d(j, t) = c0 + sum_q w2_q |P_j,q|^2 - Re(P_j,q conj(cvec_q ab_t,q))
+// (the coarse diff2 restricted to the ring plus the particle's constant) and
+// score_j = log sum_t pdf_t(t) exp(dmin - d(j, t)) + log pdf_o(j), the log of
+// the particle's low-resolution posterior of orientation j up to a constant.
+// The contraction runs on the tensor cores (tc_launch_rescore: split-BF16, one
+// 128 x 96 tile per 128 candidates of a particle); its operands are the ring
+// pixels as K = 2 x ring (re, im interleaved), zero padded to kr.
+constexpr int RS_TMAX = 96;            // translations of one rescoring tile
 
-// Ring operands of the rescoring.  projR[oc][q]: the projection of every
-// coarse orientation at the ring pixels (once per configuration); per batch
-// Sg[b][q][t] = cvec_b ab_t at ring pixel q (t < RS_TMAX, zero beyond T) and
-// w2r[b][q].
+// projections of every coarse orientation at the ring pixels: FP32 (norms) and
+// split-BF16 rows (the contraction's A operand); once per configuration
 __global__ void k_ring_table(const float2* __restrict__ proj, int P, const int* __restrict__ ring, int nring, int KO,
-                             float2* __restrict__ projR)
+                             int kr, float2* __restrict__ projR, bf16* __restrict__ rh, bf16* __restrict__ rl)
 {
-    const size_t total = (size_t)KO * nring;
+    const size_t total = (size_t)KO * (kr / 2);
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        const size_t oc = i / nring;
-        projR[i] = proj[oc * P + ring[i - oc * nring]];
+        const size_t oc = i / (kr / 2);
+        const int q = (int)(i - oc * (kr / 2));
+        float2 v = make_float2(0.f, 0.f);
+        if (q < nring) {
+            v = proj[oc * P + ring[q]];
+            projR[oc * nring + q] = v;
+        }
+        const bf16 hx = __float2bfloat16_rn(v.x), hy = __float2bfloat16_rn(v.y);
+        reinterpret_cast<__nv_bfloat162*>(rh)[i] = __halves2bfloat162(hx, hy);
+        reinterpret_cast<__nv_bfloat162*>(rl)[i] = __halves2bfloat162(__float2bfloat16_rn(v.x - __bfloat162float(hx)),
+                                                                      __float2bfloat16_rn(v.y - __bfloat162float(hy)));
     }
 }
 
-__global__ void __launch_bounds__(256) k_ring_images(Tables tb, Work w, const int* __restrict__ ring, int nring,
-                                                     float2* __restrict__ Sg, float* __restrict__ w2r)
+// per batch: the shifted ring images cvec_b ab_t as split-BF16 rows b*T + t (the
+// contraction's B operand), and w2 at the ring pixels
+__global__ void __launch_bounds__(128) k_ring_images(Tables tb, Work w, const int* __restrict__ ring, int nring, int kr,
+                                                     bf16* __restrict__ sh, bf16* __restrict__ sl, float* __restrict__ w2r)
 {
-    const int b = blockIdx.x, P = tb.P;
-    for (int i = threadIdx.x; i < nring * RS_TMAX; i += blockDim.x) {
-        const int t = i / nring, q = i - t * nring, n = ring[q];   // q fastest: coalesced reads
+    const int row = blockIdx.x, P = tb.P;
+    const int b = row / tb.T, t = row - b * tb.T;
+    if (b >= w.n) return;
+    for (int q = threadIdx.x; q < kr / 2; q += blockDim.x) {
         float2 v = make_float2(0.f, 0.f);
-        if (t < tb.T) {
+        if (q < nring) {
+            const int n = ring[q];
             const float2 c = w.cvec[(size_t)b * P + n];
             const float2 a = tb.ab_c[(size_t)t * P + n];
             v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+            if (t == 0) w2r[(size_t)b * nring + q] = w.w2[(size_t)b * P + n];
         }
-        Sg[((size_t)b * nring + q) * RS_TMAX + t] = v;
+        const bf16 hx = __float2bfloat16_rn(v.x), hy = __float2bfloat16_rn(v.y);
+        reinterpret_cast<__nv_bfloat162*>(sh + (size_t)row * kr)[q] = __halves2bfloat162(hx, hy);
+        reinterpret_cast<__nv_bfloat162*>(sl + (size_t)row * kr)[q] =
+            __halves2bfloat162(__float2bfloat16_rn(v.x - __bfloat162float(hx)), __float2bfloat16_rn(v.y - __bfloat162float(hy)));
     }
-    for (int q = threadIdx.x; q < nring; q += blockDim.x) w2r[(size_t)b * nring + q] = w.w2[(size_t)b * P + ring[q]];
 }
 
-// Exact low-resolution score of each of the network's K1 candidates (see the
-// comment above).  CTA = 64 candidates x up to 96 translations of one particle;
-// warp w owns candidates 8w..8w+7, lane l the translations l, l+32, l+64, so a
-// thread keeps an 8 x 3 register tile.  The ring pixels stream through shared
-// memory in chunks of RS_Q: the particle's shifted ring image [pixel][t] and
-// the candidates' ring projections [pixel][candidate] (a warp reads its 8
-// candidates of a pixel as four 16-byte broadcasts).
-constexpr int RS_Q = 32;
-constexpr int RS_CPW = 8;                  // candidates per warp
-constexpr int RS_CTA = 8 * RS_CPW;         // candidates per CTA
-constexpr int RS_PLD = RS_CTA + 2;         // row stride of Pj (16-byte rows, fewer bank conflicts on fill)
-__global__ void __launch_bounds__(256) k_prop_rescore(Tables tb, Work w, const float2* __restrict__ Sg,
-                                                      const float* __restrict__ w2r, const float2* __restrict__ projR,
-                                                      int nring, const int* __restrict__ cand, int k1,
-                                                      float* __restrict__ score)
+// candidate rows (b*K1 + j) of the A operand, their ring norms, and the reset of
+// the per-particle minimum; one warp per candidate
+__global__ void __launch_bounds__(256) k_rescore_gather(int n, int k1, int nring, int kr, const int* __restrict__ cand,
+                                                        const float2* __restrict__ projR, const bf16* __restrict__ rh,
+                                                        const bf16* __restrict__ rl, const float* __restrict__ w2r,
+                                                        bf16* __restrict__ ah, bf16* __restrict__ al,
+                                                        float* __restrict__ rnorm, unsigned* __restrict__ rmin)
 {
-    __shared__ __align__(16) float2 S[RS_Q * RS_TMAX];
-    __shared__ __align__(16) float2 Pj[RS_Q * RS_PLD];
-    __shared__ float w2s[RS_Q];
-    __shared__ int oc_s[RS_CTA];
-    const int b = blockIdx.y, j0 = blockIdx.x * RS_CTA;
-    const int T = tb.T;
-    if (threadIdx.x < RS_CTA) {
-        const int j = j0 + threadIdx.x;
-        oc_s[threadIdx.x] = j < k1 ? cand[(size_t)b * k1 + j] : -1;
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float acc[RS_CPW][3] = {};
-    float nrm[RS_CPW] = {};
-    for (int q0 = 0; q0 < nring; q0 += RS_Q) {
-        const int nq = min(RS_Q, nring - q0);
-        __syncthreads();
-        {
-            const float4* src = reinterpret_cast<const float4*>(Sg + ((size_t)b * nring + q0) * RS_TMAX);
-            float4* dst = reinterpret_cast<float4*>(S);
-            for (int i = threadIdx.x; i < nq * RS_TMAX / 2; i += blockDim.x) dst[i] = src[i];
-        }
-        for (int i = threadIdx.x; i < RS_CTA * RS_Q; i += blockDim.x) {
-            const int jj = i / RS_Q, q = i - jj * RS_Q;     // q fastest: each candidate's row is contiguous
-            const int oc = oc_s[jj];
-            Pj[q * RS_PLD + jj] = (oc >= 0 && q < nq) ? projR[(size_t)oc * nring + q0 + q] : make_float2(0.f, 0.f);
-        }
-        if (threadIdx.x < RS_Q) w2s[threadIdx.x] = threadIdx.x < nq ? w2r[(size_t)b * nring + q0 + threadIdx.x] : 0.f;
-        __syncthreads();
-#pragma unroll 2
-        for (int q = 0; q < nq; q++) {
-            const float2* sq = S + q * RS_TMAX + lane;
-            const float2 s0 = sq[0], s1 = sq[32], s2 = sq[64];
-            const float wq = w2s[q];
-            const float4* pq = reinterpret_cast<const float4*>(Pj + q * RS_PLD + warp * RS_CPW);
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= (long long)n * k1) return;
+    const int b = (int)(gw / k1);
+    const size_t oc = (size_t)cand[gw];
+    const uint4* sh = reinterpret_cast<const uint4*>(rh + oc * kr);
+    const uint4* sl = reinterpret_cast<const uint4*>(rl + oc * kr);
+    uint4* dh = reinterpret_cast<uint4*>(ah + (size_t)gw * kr);
+    uint4* dl = reinterpret_cast<uint4*>(al + (size_t)gw * kr);
+    float acc = 0.f;
+    for (int v = lane; v < kr / 8; v += 32) {
+        const uint4 hv = sh[v], lv = sl[v];
+        dh[v] = hv;
+        dl[v] = lv;
+        const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&hv);
+        const __nv_bfloat162* lp = reinterpret_cast<const __nv_bfloat162*>(&lv);
 #pragma unroll
-            for (int h = 0; h < RS_CPW / 2; h++) {
-                const float4 pp = pq[h];
-                const float2 pv[2] = {make_float2(pp.x, pp.y), make_float2(pp.z, pp.w)};
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int c = 2 * h + e;
-                    acc[c][0] += pv[e].x * s0.x + pv[e].y * s0.y;
-                    acc[c][1] += pv[e].x * s1.x + pv[e].y * s1.y;
-                    acc[c][2] += pv[e].x * s2.x + pv[e].y * s2.y;
-                    nrm[c] += wq * (pv[e].x * pv[e].x + pv[e].y * pv[e].y);
-                }
+        for (int e = 0; e < 4; e++) {
+            const int q = 4 * v + e;   // ring pixel of this (re, im) pair; zero rows beyond nring
+            if (q < nring) {
+                const float2 hf = __bfloat1622float2(hp[e]), lf = __bfloat1622float2(lp[e]);
+                const float re = hf.x + lf.x, im = hf.y + lf.y;
+                acc += w2r[(size_t)b * nring + q] * (re * re + im * im);
             }
         }
     }
-#pragma unroll
-    for (int c = 0; c < RS_CPW; c++) {
-        float d[3];
-        float dmin = INFINITY;
-#pragma unroll
-        for (int m = 0; m < 3; m++) {
-            const int t = lane + 32 * m;
-            d[m] = nrm[c] - acc[c][m];
-            if (t < T) dmin = fminf(dmin, d[m]);
-        }
-        for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
-        double se = 0.;
-#pragma unroll
-        for (int m = 0; m < 3; m++) {
-            const int t = lane + 32 * m;
-            if (t < T) se += w.pdf_t[(size_t)b * T + t] * exp((double)(dmin - d[m]));
-        }
-        for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
-        const int j = j0 + warp * RS_CPW + c;
-        if (lane == 0 && j < k1) {
-            const int oc = oc_s[warp * RS_CPW + c];
-            score[(size_t)b * k1 + j] = (tb.skip[oc] || !(se > 0.)) ? -INFINITY
-                                                                    : (float)(log(se) - (double)dmin + log(tb.pdf_oc[oc]));
-        }
+    (void)projR;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+        rnorm[gw] = acc;
+        if (gw % k1 == 0) rmin[b] = 0xffffffffu;
+    }
+}
+
+// score of every candidate from its T ring diff2 values; one warp per candidate
+__global__ void __launch_bounds__(256) k_rescore_reduce(Tables tb, Work w, int k1, const int* __restrict__ cand,
+                                                        const float* __restrict__ d2, const unsigned* __restrict__ rmin,
+                                                        float* __restrict__ score)
+{
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= (long long)w.n * k1) return;
+    const int b = (int)(gw / k1), T = tb.T;
+    const float mn = key2f(rmin[b]);
+    const float* d = d2 + (size_t)gw * T;
+    float se = 0.f;   // FP32: a ranking score (terms below e^-80 of the particle's best are dropped)
+    for (int t = lane; t < T; t += 32) {
+        const float v = d[t];
+        if (v < 0.f || v - mn > 80.f) continue;
+        se += (float)w.pdf_t[(size_t)b * T + t] * __expf(mn - v);
+    }
+    for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
+    if (lane == 0) {
+        const int oc = cand[gw];
+        score[gw] = (tb.skip[oc] || !(se > 0.f)) ? -INFINITY : __logf(se) + (float)log(tb.pdf_oc[oc]);
     }
 }
 
@@ -437,33 +459,51 @@ __global__ void __launch_bounds__(1024) k_rescore_select(const int* __restrict__
 }
 
 // ---------------------------------------------- proposal coarse operands
-// Gathered split-BF16 projections of every (particle, proposal) and its norm
-// N = sum_p w2 |P|^2 (FP32 from the FP32 table).  Row of (b, j) in the A
-// operand: (b / ppt) * 128 + (b % ppt) * kslot + j.  Runs while *gate != 0.
-__global__ void __launch_bounds__(256) k_prop_gather(Tables tb, Work w, int ppt, int kslot, int kdim, bf16* __restrict__ ph,
-                                                     bf16* __restrict__ pl, float* __restrict__ nprop)
+// Gathered split-BF16 projection rows of every (particle, proposal), copied
+// from the configuration's coarse operand (16-byte copies), and its norm
+// N = sum_k w2_k |P|^2_k from the same split-BF16 operands the full pass's norm
+// contraction reads (|P|^2 hi + lo per orientation, w2 hi + lo per particle).
+// Row of (b, j) in the A operand: (b / ppt) * 128 + (b % ppt) * kslot + j.
+// Runs while *gate != 0.
+__global__ void __launch_bounds__(256) k_prop_gather(Work w, int ppt, int kslot, int kdim, int kn,
+                                                     const bf16* __restrict__ bh, const bf16* __restrict__ bl,
+                                                     const bf16* __restrict__ nh, const bf16* __restrict__ nl,
+                                                     const bf16* __restrict__ wh, const bf16* __restrict__ wl,
+                                                     bf16* __restrict__ ph, bf16* __restrict__ pl, float* __restrict__ nprop)
 {
     __shared__ float red[32];
     if (!w.gate || *w.gate == 0) return;
     const int b = blockIdx.y, j = blockIdx.x;
     if (b >= w.n || j >= w.kprop) return;
-    const int oc = w.prop[(size_t)b * w.kprop + j];
+    const size_t oc = (size_t)w.prop[(size_t)b * w.kprop + j];
     const size_t row = (size_t)(b / ppt) * 128 + (size_t)(b % ppt) * kslot + j;
-    const float2* src = tb.proj_c + (size_t)oc * tb.P;
-    __nv_bfloat162* dh = reinterpret_cast<__nv_bfloat162*>(ph + row * kdim);
-    __nv_bfloat162* dl = reinterpret_cast<__nv_bfloat162*>(pl + row * kdim);
-    float acc = 0.f;
-    for (int k = threadIdx.x; k < kdim / 2; k += blockDim.x) {
-        float2 v = make_float2(0.f, 0.f);
-        if (k < tb.nk) {
-            const int p = tb.kpix[k];
-            v = src[p];
-            acc += w.w2[(size_t)b * tb.P + p] * (v.x * v.x + v.y * v.y);
+    {
+        const uint4* sh = reinterpret_cast<const uint4*>(bh + oc * kdim);
+        const uint4* sl = reinterpret_cast<const uint4*>(bl + oc * kdim);
+        uint4* dh = reinterpret_cast<uint4*>(ph + row * kdim);
+        uint4* dl = reinterpret_cast<uint4*>(pl + row * kdim);
+        for (int v = threadIdx.x; v < kdim / 8; v += blockDim.x) {
+            dh[v] = sh[v];
+            dl[v] = sl[v];
         }
-        const bf16 hx = __float2bfloat16_rn(v.x), hy = __float2bfloat16_rn(v.y);
-        dh[k] = __halves2bfloat162(hx, hy);
-        dl[k] = __halves2bfloat162(__float2bfloat16_rn(v.x - __bfloat162float(hx)),
-                                   __float2bfloat16_rn(v.y - __bfloat162float(hy)));
+    }
+    const uint4* nhv = reinterpret_cast<const uint4*>(nh + oc * kn);
+    const uint4* nlv = reinterpret_cast<const uint4*>(nl + oc * kn);
+    const uint4* whv = reinterpret_cast<const uint4*>(wh + (size_t)b * kn);
+    const uint4* wlv = reinterpret_cast<const uint4*>(wl + (size_t)b * kn);
+    float acc = 0.f;
+    for (int v = threadIdx.x; v < kn / 8; v += blockDim.x) {
+        const uint4 a0 = nhv[v], a1 = nlv[v], c0 = whv[v], c1 = wlv[v];
+        const __nv_bfloat162* x0 = reinterpret_cast<const __nv_bfloat162*>(&a0);
+        const __nv_bfloat162* x1 = reinterpret_cast<const __nv_bfloat162*>(&a1);
+        const __nv_bfloat162* y0 = reinterpret_cast<const __nv_bfloat162*>(&c0);
+        const __nv_bfloat162* y1 = reinterpret_cast<const __nv_bfloat162*>(&c1);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const float2 p0 = __bfloat1622float2(x0[e]), p1 = __bfloat1622float2(x1[e]);
+            const float2 q0 = __bfloat1622float2(y0[e]), q1 = __bfloat1622float2(y1[e]);
+            acc += (q0.x + q1.x) * (p0.x + p1.x) + (q0.y + q1.y) * (p0.y + p1.y);
+        }
     }
     acc = bsum(acc, red);
     if (threadIdx.x == 0) nprop[(size_t)b * w.kprop + j] = acc;
@@ -1335,10 +1375,29 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.prop, 0, (size_t)B * 128 * sizeof(int)));
     N.cand1 = (int*)net_dalloc(W, (size_t)B * NET_TOPK_CAND * sizeof(int));
     N.score1 = (float*)net_dalloc(W, (size_t)B * NET_TOPK_CAND * sizeof(float));
+    // low-resolution rescoring operands (K = 2 x ring pixels, padded to a multiple of 64)
+    N.kr = (2 * N.nring + 63) / 64 * 64;
     N.projR = (float2*)net_dalloc(W, (size_t)KO * N.nring * sizeof(float2));
-    k_ring_table<<<gridsz((size_t)KO * N.nring), 256>>>(tb.proj_c, P, N.ring, N.nring, KO, N.projR);
-    N.Sg = (float2*)net_dalloc(W, (size_t)B * N.nring * RS_TMAX * sizeof(float2));
+    N.rth = net_dalloc(W, (size_t)KO * N.kr * sizeof(bf16));
+    N.rtl = net_dalloc(W, (size_t)KO * N.kr * sizeof(bf16));
+    k_ring_table<<<gridsz((size_t)KO * N.kr / 2), 256>>>(tb.proj_c, P, N.ring, N.nring, KO, N.kr, N.projR, (bf16*)N.rth,
+                                                         (bf16*)N.rtl);
     N.w2r = (float*)net_dalloc(W, (size_t)B * N.nring * sizeof(float));
+    const size_t ra_rows = (size_t)B * NET_MAX_K1, rb_rows = ((size_t)B * tb.T + RS_TMAX + 255) / 256 * 256;
+    N.rah = net_dalloc(W, ra_rows * N.kr * sizeof(bf16));
+    N.ral = net_dalloc(W, ra_rows * N.kr * sizeof(bf16));
+    N.rbh = net_dalloc(W, rb_rows * N.kr * sizeof(bf16));
+    N.rbl = net_dalloc(W, rb_rows * N.kr * sizeof(bf16));
+    T2B_CUDA(cudaMemset(N.rbh, 0, rb_rows * N.kr * sizeof(bf16)));
+    T2B_CUDA(cudaMemset(N.rbl, 0, rb_rows * N.kr * sizeof(bf16)));
+    N.rnorm = (float*)net_dalloc(W, ra_rows * sizeof(float));
+    N.rd2 = (float*)net_dalloc(W, ra_rows * tb.T * sizeof(float));
+    N.rmin = (unsigned*)net_dalloc(W, (size_t)B * sizeof(unsigned));
+    const int rs = tc_slot_rescore();
+    tc_set_map_box(c->tc, rs, N.rah, (int)ra_rows, N.kr, 128);
+    tc_set_map_box(c->tc, rs + 1, N.ral, (int)ra_rows, N.kr, 128);
+    tc_set_map_box(c->tc, rs + 2, N.rbh, (int)rb_rows, N.kr, RS_TMAX);
+    tc_set_map_box(c->tc, rs + 3, N.rbl, (int)rb_rows, N.kr, RS_TMAX);
     // tensor maps of the dense layers: W1, X0b, W2, H1b, W3, H2b
     unsigned char blobs[6][128];
     const bf16* thb = (const bf16*)N.thb;
@@ -1385,14 +1444,23 @@ void net_setup(t2b_ctx* c, int na_max)
     N.ready = true;
 }
 
+// Proposal tiles: one particle per 128 x 96 tile (up to 128 proposals x its
+// translations) when T <= 96; otherwise 128 x 256 tiles of two particles with
+// up to 64 proposals each, or of one particle.
 void set_tile_shape(ProposalNet& N, int T)
 {
-    if (N.kprop <= 64 && 2 * T <= 256) {
+    if (T <= 96) {
+        N.ppt = 1;
+        N.kslot = 128;
+        N.tn = 96;
+    } else if (N.kprop <= 64 && 2 * T <= 256) {
         N.ppt = 2;
         N.kslot = 64;
+        N.tn = 256;
     } else {
         N.ppt = 1;
         N.kslot = 128;
+        N.tn = 256;
     }
 }
 
@@ -1511,19 +1579,25 @@ void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st)
     if (N.k1 > 0) {
         // network top-k1, exact low-resolution rescoring, top-kprop of those
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO, N.k1,
-                                                           N.cand1);
-        k_ring_images<<<w.n, 256, 0, st>>>(tb, w, N.ring, N.nring, N.Sg, N.w2r);
-        k_prop_rescore<<<dim3((N.k1 + RS_CTA - 1) / RS_CTA, w.n), 256, 0, st>>>(tb, w, N.Sg, N.w2r, N.projR, N.nring,
-                                                                                  N.cand1, N.k1, N.score1);
+                                                           N.cand1, 0);
+        const long long nc = (long long)w.n * N.k1;
+        k_ring_images<<<w.n * tb.T, 128, 0, st>>>(tb, w, N.ring, N.nring, N.kr, (bf16*)N.rbh, (bf16*)N.rbl, N.w2r);
+        k_rescore_gather<<<(int)((nc * 32 + 255) / 256), 256, 0, st>>>(w.n, N.k1, N.nring, N.kr, N.cand1, N.projR,
+                                                                       (const bf16*)N.rth, (const bf16*)N.rtl, N.w2r,
+                                                                       (bf16*)N.rah, (bf16*)N.ral, N.rnorm, N.rmin);
+        T2B_CUDA(cudaGetLastError());
+        tc_launch_rescore(w.n, N.k1, tb.T, N.kr, c->tc, w.c0, N.rnorm, tb.skip, N.cand1, N.rd2, N.rmin, w.err, nullptr,
+                          st);
+        k_rescore_reduce<<<(int)((nc * 32 + 255) / 256), 256, 0, st>>>(tb, w, N.k1, N.cand1, N.rd2, N.rmin, N.score1);
         k_rescore_select<<<w.n, 1024, 0, st>>>(N.cand1, N.score1, N.k1, N.kprop, N.prop);
     } else {
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO,
-                                                           N.kprop, N.prop);
+                                                           N.kprop, N.prop, 1);
     }
     T2B_CUDA(cudaGetLastError());
 }
 
-void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st)
+void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev)
 {
     ProposalNet& N = *c->net;
     const Tables& tb = c->tb;
@@ -1537,21 +1611,29 @@ void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st)
     k_audit_norms<<<(KO * 32 + 255) / 256, 256, 0, st>>>(KO, op.kn, N.ps, (const bf16*)op.nh, (const bf16*)op.nl,
                                                         N.w2a, N.na_max, N.norma);
     T2B_CUDA(cudaGetLastError());
+    if (ev) cudaEventRecord(ev[0], st);
     tc_launch_audit(tb, op, N.na_max, N.c0a, N.norma, N.d2a, N.minkeya, w.err, st);
+    if (ev) cudaEventRecord(ev[1], st);
     k_audit_mass<<<dim3(2 * 148, N.na_max), 256, ((KO + 31) / 32) * sizeof(unsigned), st>>>(tb, w, N.ps, N.audit_b, N.d2a,
                                                                                      N.minkeya, N.asum);
     k_audit_final<<<1, 1024, 0, st>>>(N.ps, N.audit_b, N.asum, N.thr, w.r_audit);
     T2B_CUDA(cudaGetLastError());
 }
 
-void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st)
+void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev)
 {
     ProposalNet& N = *c->net;
     const Tables& tb = c->tb;
-    k_prop_gather<<<dim3(N.kprop, w.n), 256, 0, st>>>(tb, w, N.ppt, N.kslot, c->tc.kdim, (bf16*)N.pg_h, (bf16*)N.pg_l,
-                                                      N.nprop);
+    const TcOperands& op = c->tc;
+    k_prop_gather<<<dim3(N.kprop, w.n), 128, 0, st>>>(w, N.ppt, N.kslot, op.kdim, op.kn, (const bf16*)op.bh,
+                                                      (const bf16*)op.bl, (const bf16*)op.nh, (const bf16*)op.nl,
+                                                      (const bf16*)op.wh, (const bf16*)op.wl, (bf16*)N.pg_h,
+                                                      (bf16*)N.pg_l, N.nprop);
+    (void)tb;
     T2B_CUDA(cudaGetLastError());
-    tc_launch_prop(tb, w, c->tc, N.ppt, N.kslot, N.nprop, st);
+    if (ev) cudaEventRecord(ev[0], st);
+    tc_launch_prop(tb, w, c->tc, N.ppt, N.kslot, N.tn, N.nprop, st);
+    if (ev) cudaEventRecord(ev[1], st);
 }
 
 void proposal_invalidate(t2b_ctx* c)
@@ -1636,7 +1718,7 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
         N.k1 = 0;
         set_tile_shape(N, tb.T);
         net_setup(c, std::max(1, N.na_max));
-        T2B_REQUIRE(f.rescore == 0 || (f.rescore >= f.topk && f.rescore <= NET_TOPK_CAND && f.rescore <= KO &&
+        T2B_REQUIRE(f.rescore == 0 || (f.rescore >= f.topk && f.rescore <= NET_MAX_K1 && f.rescore % 128 == 0 && f.rescore <= KO &&
                                        tb.T <= RS_TMAX),
                     T2B_ERR_ARG, "bad rescore candidate count");
         *rep = t2b_proposal_report{};
@@ -1655,7 +1737,7 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
         T2B_CUDA(cudaMemset(poc.p, 0xff, (size_t)ntr * NET_NPOST * sizeof(int)));
         T2B_CUDA(cudaMemset(pw.p, 0, (size_t)ntr * NET_NPOST * sizeof(float)));
         DevBuf pose((size_t)B * 9 * sizeof(double)), cls((size_t)B * sizeof(int)), marg((size_t)B * KO * sizeof(double));
-        DevBuf cap((size_t)B * sizeof(double)), vlab((size_t)B * sizeof(int));
+        DevBuf cap((size_t)2 * B * sizeof(double)), vlab((size_t)B * sizeof(int));
         GenParams gp{f.seed, f.defocus_min, f.defocus_max, f.astig_max, f.voltage, f.cs, f.q0, tb.pixel_size,
                      f.max_shift, minv_d.as<float>()};
         Work wg = c->wk;
@@ -1723,11 +1805,12 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
             // 3. initial network: the matched filter of the references
             init_from_templates(c, N, f.seed, ctf2.as<float>(), minv_d.as<float>(), f.alpha > 0.f ? f.alpha : 3.f, st);
             // held-out particles: posterior mass of the plain E-step inside the top-k
-            auto validate = [&](double* mean, double* mn, double* frac, double* hit) {
+            auto validate = [&](double* mean, double* mn, double* frac, double* hit, double* frac_cand = nullptr) {
                 const int nv = f.n_val;
                 if (nv <= 0) return;
                 double sum = 0., lo = INFINITY;
-                long long ok = 0, hits = 0;
+                long long ok = 0, hits = 0, ok_cand = 0;
+                std::vector<double> hcc(B);
                 std::vector<double> hc(B);
                 std::vector<int> hp((size_t)B * N.kprop), hl(B);
                 for (int v0 = 0; v0 < nv; v0 += B) {
@@ -1738,6 +1821,11 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
                     wi.n = cnt;
                     proposal_infer(c, wi, st);
                     k_capture<<<cnt, 256, 0, st>>>(marg.as<double>(), KO, N.prop, N.kprop, cap.as<double>());
+                    if (frac_cand && N.k1 > 0) {
+                        k_capture<<<cnt, 256, 0, st>>>(marg.as<double>(), KO, N.cand1, N.k1, cap.as<double>() + B);
+                        T2B_CUDA(cudaMemcpyAsync(hcc.data(), cap.as<double>() + B, cnt * sizeof(double),
+                                                 cudaMemcpyDeviceToHost, st));
+                    }
                     k_nearest<<<cnt, 256, 0, st>>>(tb, pose.as<double>(), cls.as<int>(), cnt, vlab.as<int>());
                     T2B_CUDA(cudaMemcpyAsync(hc.data(), cap.p, cnt * sizeof(double), cudaMemcpyDeviceToHost, st));
                     T2B_CUDA(cudaMemcpyAsync(hp.data(), N.prop, (size_t)cnt * N.kprop * sizeof(int),
@@ -1745,6 +1833,7 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
                     T2B_CUDA(cudaMemcpyAsync(hl.data(), vlab.p, cnt * sizeof(int), cudaMemcpyDeviceToHost, st));
                     T2B_CUDA(cudaStreamSynchronize(st));
                     for (int i = 0; i < cnt; i++) {
+                        if (frac_cand && N.k1 > 0) ok_cand += hcc[i] >= 0.999;
                         sum += hc[i];
                         lo = std::min(lo, hc[i]);
                         ok += hc[i] >= 0.999;
@@ -1756,6 +1845,7 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
                 if (mn) *mn = lo;
                 if (frac) *frac = (double)ok / nv;
                 if (hit) *hit = (double)hits / nv;
+                if (frac_cand) *frac_cand = (double)ok_cand / nv;
             };
             validate(&rep->val_mass_init, nullptr, nullptr, nullptr);
             // 4. Adam epochs over shuffled minibatches
@@ -1790,7 +1880,8 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
             validate(&rep->val_mass_trained, &rep->val_mass_min, &rep->val_frac_999, &rep->val_true_hit);
             if (f.rescore > 0) {
                 N.k1 = f.rescore;
-                validate(&rep->val_mass_rescored, &rep->val_mass_min_rescored, &rep->val_frac_999_rescored, nullptr);
+                validate(&rep->val_mass_rescored, &rep->val_mass_min_rescored, &rep->val_frac_999_rescored, nullptr,
+                         &rep->val_frac_999_candidates);
                 N.k1 = 0;
             }
         } catch (...) {
@@ -1821,8 +1912,8 @@ int t2b_proposal_enable(t2b_ctx* c, int topk, int rescore, int audit_every, doub
                     "no trained proposal network for this orientation sampling");
         T2B_REQUIRE(topk >= 1 && topk <= 128 && topk <= KO && audit_every >= 1 && audit_mass > 0. && audit_mass <= 1.,
                     T2B_ERR_ARG, "bad proposal settings");
-        T2B_REQUIRE(rescore == 0 || (rescore >= topk && rescore <= NET_TOPK_CAND && rescore <= KO), T2B_ERR_ARG,
-                    "rescore must be 0 or in [topk, min(2048, nr_classes*n_dir*n_psi)]");
+        T2B_REQUIRE(rescore == 0 || (rescore >= topk && rescore <= NET_MAX_K1 && rescore % 128 == 0 && rescore <= KO), T2B_ERR_ARG,
+                    "rescore must be 0 or a multiple of 128 in [topk, min(1024, nr_classes*n_dir*n_psi)]");
         ProposalNet& N = *c->net;
         const int B = c->cfg.max_batch;
         // at most ceil(B / every) multiples of `every` in any B consecutive stream positions

@@ -13,6 +13,7 @@ constexpr int NET_NPOST = 8;       // posterior labels kept per training particl
 constexpr int NET_NTGT = 1 + NET_NPOST;
 constexpr int NET_TOPK_CAND = 2048;
 constexpr int NET_MAX_KO = 49152;  // logits of one particle held in shared memory by the top-k
+constexpr int NET_MAX_K1 = 1024;   // network candidates rescored at low resolution
 
 // offsets (elements) of the parameters in the flat FP32 / BF16 vectors;
 // w3 last, with zero rows up to a multiple of 128 for the tensor-core operand
@@ -45,11 +46,16 @@ struct ProposalNet {
     void* thb = nullptr;               // BF16 copy of th (every forward pass reads it)
     bool ready = false;                // workspace matches the configuration
     bool enabled = false;
-    int kprop = 64, every = 50, na_max = 0, ppt = 1, kslot = 128, b_pad = 0;
+    int kprop = 64, every = 50, na_max = 0, ppt = 1, kslot = 128, tn = 256, b_pad = 0;
     int k1 = 0;                        // network candidates rescored at low resolution (0: none)
-    float2* projR = nullptr;           // K*O x nring: projections at the ring pixels
-    float2* Sg = nullptr;              // B x nring x 96: shifted ring images of the batch
+    int kr = 0;                        // K of the rescoring contraction (2 x ring pixels, padded)
+    float2* projR = nullptr;           // K*O x nring: projections at the ring pixels (FP32)
+    void *rth = nullptr, *rtl = nullptr;  // K*O x kr: the same, split-BF16
     float* w2r = nullptr;              // B x nring
+    void *rah = nullptr, *ral = nullptr;  // B*NET_MAX_K1 x kr: gathered candidate rows
+    void *rbh = nullptr, *rbl = nullptr;  // B*T x kr: shifted ring images
+    float *rnorm = nullptr, *rd2 = nullptr;  // B*K1 ring norms, B*K1*T ring diff2
+    unsigned* rmin = nullptr;          // B
     int* cand1 = nullptr;              // B x k1 network candidates
     float* score1 = nullptr;           // B x k1 low-resolution scores
     double thr = 0.999;
@@ -72,8 +78,9 @@ struct ProposalNet {
 
 // inference, audit and restricted coarse pass of one batch (proposal.cu)
 void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st);
-void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st);
-void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st);
+// ev (optional): two events recorded around the audit / proposal contraction
+void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev = nullptr);
+void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev = nullptr);
 void proposal_release(t2b_ctx* c);    // context destruction
 void proposal_invalidate(t2b_ctx* c); // configuration changed
 

@@ -205,7 +205,7 @@ struct TcOperands {
     int kn, b_pad;            // padded sizes of the norm operands
     void* maps;               // TC_MAP_SLOTS CUtensorMap descriptors (128 B each) in device memory
 };
-constexpr int TC_MAP_SLOTS = 16;
+constexpr int TC_MAP_SLOTS = 24;
 size_t tc_kdim(int nk);
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
@@ -219,7 +219,12 @@ void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128);
 void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_side);
 int tc_slot_proposals();
 int tc_slot_audit();
-void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, const float* nprop,
+int tc_slot_rescore();
+void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows);
+void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* c0, const float* norms,
+                       const unsigned char* skip, const int* cand, float* d2, unsigned* minkey, int* err,
+                       const int* gate, cudaStream_t st);
+void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, int tn, const float* nprop,
                     cudaStream_t st);
 void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
                      unsigned* minkeya, int* err, cudaStream_t st);
@@ -268,7 +273,8 @@ struct t2b_ctx {
         }
     }
     int last_kernels = -1;
-    cudaEvent_t ev[8]{};
-    float stage_ms[7]{};
+    cudaEvent_t ev[12]{};                     // 8 stage boundaries + 2 pairs around the proposal-path GEMMs
+    float stage_ms[9]{};
+    bool prop_events = false;                 // the last timed batch recorded ev[8..11]
     t2b::ProposalNet* net = nullptr;          // learned orientation proposals (proposal.cu)
 };
