@@ -55,8 +55,10 @@ METRIC = "E-step particles/s box128: learned+split-BF16 vs plain FP32 GPU; roofl
 # pass; every 50th particle (2 %) audited by the full coarse pass (>= 0.999 of its mass)
 PROP = dict(topk=64, rescore=1024, audit_every=50, audit_mass=0.999)
 # DRAM bytes (read + write) of the audit + proposal k_diff2_tc launches of one learned step
-# at 128 particles, from one ncu capture (None until captured)
-LEARNED_TRAFFIC = None  # set once the 96-column proposal tiles are captured
+# at 128 particles, from one ncu capture
+# (audit 766.02 MB read + 18.59 MB written, proposal pass 548.33 MB + 0.46 MB;
+# profiles/k_diff2_tc_box128_learned_b128_dram.md)
+LEARNED_TRAFFIC = 766.02e6 + 18.59e6 + 548.33e6 + 0.46e6
 
 
 def build_problem(t2b, sy, n_particles, seed):

@@ -104,4 +104,26 @@ private:
     MlDeviceBundle& b_;
 };
 
+// Learned orientation proposals of one bundle (no counterpart in the reference):
+// train once per iteration on particles generated from the uploaded references,
+// then enable for the following batches.
+class ProposalNetwork {
+public:
+    explicit ProposalNetwork(MlDeviceBundle& b) : b_(b) {}
+    t2b_proposal_report train(const t2b_proposal_train_config& cfg)
+    {
+        t2b_proposal_report rep;
+        check(t2b_proposal_train(b_.ctx(), &cfg, &rep));
+        return rep;
+    }
+    void enable(int topk = 64, int rescore = 1024, int audit_every = 50, double audit_mass = 0.999)
+    {
+        check(t2b_proposal_enable(b_.ctx(), topk, rescore, audit_every, audit_mass));
+    }
+    void disable() { check(t2b_proposal_enable(b_.ctx(), 0, 0, 1, 1.0)); }
+
+private:
+    MlDeviceBundle& b_;
+};
+
 }  // namespace t2b

@@ -63,3 +63,31 @@ def test_sampling_2d(t2b):
     assert (s["n_dir"], s["n_psi"], s["nover_rot"], s["n_trans"]) == (1, 60, 2, 81)
     psi = np.degrees(np.arctan2(s["eul_fine"][:, 1], s["eul_fine"][:, 0]))
     assert np.allclose(np.sort(np.mod(psi, 360))[:4], [1.5, 4.5, 7.5, 10.5])
+
+
+def test_cpp_adapter_compiles_and_links(tmp_path):
+    """The C++ classes a maintainer includes (t2b_adapter.hpp) compile against the
+    C ABI and link with libt2b.so (no GPU call is made)."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "use_adapter.cpp"
+    src.write_text(
+        '#include "t2b_adapter.hpp"\n'
+        "int main(int argc, char**) {\n"
+        "  if (argc > 5) {  // never taken: only the symbols are needed\n"
+        "    t2b::MlDeviceBundle b(0);\n"
+        "    t2b::MlOptimiserCuda opt(b);\n"
+        "    t2b::ProposalNetwork net(b);\n"
+        "    net.enable();\n"
+        "    t2b::AccBackprojector bp(b, 0);\n"
+        "  }\n"
+        "  return 0;\n"
+        "}\n")
+    lib_dir = os.path.join(ROOT, "t2-relion_b200")
+    out = tmp_path / "use_adapter"
+    r = subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-L", lib_dir, "-lt2b",
+                        "-Wl,--unresolved-symbols=ignore-in-shared-libs", "-o", str(out)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
