@@ -181,6 +181,11 @@ struct TcParams {
     int tn;                   // N of the tile (multiple of 32, <= 256; 0 = 256); B maps with a tn-row box
     int mtp;                  // mode 1 with ppt = 1: consecutive tiles per particle (0 = 1); A rows of
                               // tile i are rows [i*128, i*128+128), proposal j = (i % mtp)*128 + row
+    // mode 2 (low-resolution rescoring, tiles as mode 1 with ppt = 1): no diff2 is stored;
+    // each epilogue thread reduces its own row (candidate j) over the translations,
+    // d2c[b*KO + j] = log sum_t pdf_t exp(C_t) - norm_j + log pdf_o(j)  (c0 omitted)
+    const double* pdf_t;      // n x T
+    const double* pdf_oc;     // K*O
 };
 
 // maps: device array of tensor-map descriptors (encoded once per configuration);
@@ -338,7 +343,33 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             }
             __syncwarp();
             const int nchunk = (p.tn ? p.tn : TN) / 32;
-            for (int c = 0; c < nchunk; c++) {
+            if (p.mode == 2) {
+                // the thread's row straight from TMEM (32x32b: lane = row, 32 columns per load);
+                // online log-sum-exp over the translations
+                float m = -INFINITY, sacc = 0.f;
+                const double* pt = p.pdf_t + (size_t)bfirst * p.T;
+                for (int c = 0; c < nchunk; c++) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
+#pragma unroll
+                    for (int e = 0; e < 32; e++) {
+                        const int t = c * 32 + e;
+                        if (t < p.T) {
+                            const float x = __uint_as_float(v[e]);
+                            const float w = (float)pt[t];
+                            if (x > m) { sacc = sacc * __expf(m - x) + w; m = x; }
+                            else sacc += w * __expf(x - m);
+                        }
+                    }
+                }
+                const int j = jbase + q * 32 + lane;
+                if (j < p.KO && bfirst < p.ncols) {
+                    const size_t pj = (size_t)bfirst * p.KO + j;
+                    p.d2c[pj] = (my_skip || !(sacc > 0.f)) ? -INFINITY
+                                                           : m - my_norm + __logf(sacc) + (float)log(p.pdf_oc[p.prop[pj]]);
+                }
+            }
+            for (int c = 0; c < (p.mode == 2 ? 0 : nchunk); c++) {
                 uint32_t v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
 #pragma unroll
@@ -690,15 +721,15 @@ void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int
 
 // Low-resolution rescoring contraction: particle b's K1 candidates (gathered ring
 // projections, slots MAP_RAH/RAL, rows b*K1 + j) against its T shifted ring
-// images (MAP_RBH/RBL, 96-row box from row b*T); d = c0 + norm - C into d2
-// (n x K1 x T), per-particle minimum into minkey.  K1 a multiple of 128.
-void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* c0, const float* norms,
-                       const unsigned char* skip, const int* cand, float* d2, unsigned* minkey, int* err,
-                       const int* gate, cudaStream_t st)
+// images (MAP_RBH/RBL, 96-row box from row b*T); the epilogue reduces every
+// candidate's row to its score (mode 2) into score[b*K1 + j].  K1 a multiple of 128.
+void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* norms, const unsigned char* skip,
+                       const int* cand, const double* pdf_t, const double* pdf_oc, float* score, int* err,
+                       cudaStream_t st)
 {
     T2B_REQUIRE(k1 % TM == 0 && T <= 96 && kr % TK == 0, T2B_ERR_STATE, "rescoring tile shape");
     TcParams p{};
-    p.mode = 1;
+    p.mode = 2;
     p.ppt = 1;
     p.kslot = TM;
     p.mtp = k1 / TM;
@@ -709,16 +740,14 @@ void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float
     p.KO = k1;
     p.T = T;
     p.ncols = n;
-    p.c0 = c0;
     p.norms = norms;
     p.skip = skip;
     p.prop = cand;
-    p.d2c = d2;
-    p.minkey = minkey;
+    p.pdf_t = pdf_t;
+    p.pdf_oc = pdf_oc;
+    p.d2c = score;
     p.err = err;
     p.products = 3;
-    p.gate = gate;
-    p.gate_run = 1;
     launch_gemm(op, MAP_RAH, MAP_RBH, p, st);
 }
 

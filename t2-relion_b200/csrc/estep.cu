@@ -1111,7 +1111,7 @@ __global__ void __launch_bounds__(256) k_compact(Tables tb, Work w, int gather_f
 // (src/ml_optimiser.cpp:7090-7272 with exp_ipass == 1).
 constexpr int MAXR = 8, MAXV = 4;
 
-__global__ void __launch_bounds__(256) k_fine(Tables tb, Work w)
+__global__ void __launch_bounds__(256, 4) k_fine(Tables tb, Work w)
 {
     __shared__ long long item;
     __shared__ float red[8][MAXR * MAXV + MAXR];
@@ -1207,6 +1207,20 @@ struct GridPtrs {
     float* const* weight;
 };
 
+// First pair of every orientation group (consecutive pairs of one particle with
+// the same coarse orientation) into w.groups; the count into w.counters[3].
+__global__ void k_group_starts(Tables tb, Work w)
+{
+    const long long npairs = w.pair_off[w.n];
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < npairs; q += (long long)gridDim.x * blockDim.x) {
+        const int b = w.pair_b[q];
+        if (q == w.pair_off[b] || w.pairs[q - 1] / tb.T != w.pairs[q] / tb.T) {
+            const unsigned long long i = atomicAdd(&w.counters[3], 1ull);
+            w.groups[i] = q;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, GridPtrs gp)
 {
     __shared__ long long item;
@@ -1218,39 +1232,33 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
     const int P = tb.P, T = tb.T, xh = tb.xh, s = tb.s;
     const int R = tb.ovs ? tb.R : 1, V = tb.ovs ? tb.V : 1;
     (void)xh;
-    const long long npairs = w.pair_off[w.n];
-    const unsigned long long nitems = (unsigned long long)npairs * R;
+    const unsigned long long nitems = w.counters[3] * (unsigned long long)R;   // (orientation group, rotation)
     const float2* proj = tb.ovs ? tb.proj_f : tb.proj_c;
     const float2* abt = tb.ovs ? tb.ab_f : tb.ab_c;
     const int nring = s / 2 + 1;
-    __shared__ long long grp_end;
+    __shared__ long long grp_end, grp_beg;
     for (;;) {
         if (threadIdx.x == 0) {
             item = (long long)atomicAdd(&w.counters[2], 1ull);
-            // a work item is (first pair of an orientation group, fine rotation)
+            // a work item is (orientation group, fine rotation); find the group's end
             grp_end = -1;
             if ((unsigned long long)item < nitems) {
-                const long long q = item / R;
+                const long long q = w.groups[item / R];
                 const int bq = w.pair_b[q];
                 const long long oc = w.pairs[q] / T;
-                if (q == w.pair_off[bq] || w.pairs[q - 1] / T != oc) {
-                    long long e = q + 1;
-                    const long long pend = w.pair_off[bq + 1];
-                    while (e < pend && w.pairs[e] / T == oc) e++;
-                    grp_end = e;
-                }
+                long long e = q + 1;
+                const long long pend = w.pair_off[bq + 1];
+                while (e < pend && w.pairs[e] / T == oc) e++;
+                grp_end = e;
+                grp_beg = q;
             }
         }
         __syncthreads();
         const long long it = item;
         if ((unsigned long long)it >= nitems) break;
-        const long long qa = it / R;
+        const long long qa = grp_beg;
         const long long qb = grp_end;
-        const int r = (int)(it - qa * R);
-        if (qb < 0) {  // not the start of a group
-            __syncthreads();
-            continue;
-        }
+        const int r = (int)(it % R);
         const int b = w.pair_b[qa];
         const int oc = (int)(w.pairs[qa] / T);
         const int k = oc / tb.O, o = oc - k * tb.O, idir = o / tb.n_psi;
@@ -1577,7 +1585,7 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
 
 void launch_fine(const Tables& tb, const Work& w, cudaStream_t st)
 {
-    k_fine<<<3 * sm_count(), 256, 0, st>>>(tb, w);   // 80 registers: 3 CTAs per SM
+    k_fine<<<4 * sm_count(), 256, 0, st>>>(tb, w);   // <= 64 registers: 4 CTAs per SM
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -1595,7 +1603,8 @@ void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* co
                     float* const* grid_weight, cudaStream_t st)
 {
     GridPtrs gp{grid_data, grid_weight};
-    k_wsum_bp<<<3 * sm_count(), 256, 0, st>>>(tb, w, g, gp);   // 80 registers: 3 CTAs per SM
+    k_group_starts<<<2 * sm_count(), 256, 0, st>>>(tb, w);
+    k_wsum_bp<<<4 * sm_count(), 256, 0, st>>>(tb, w, g, gp);   // 64 registers: 4 CTAs per SM
     k_results<<<(w.n + 127) / 128, 128, 0, st>>>(tb, w);
     T2B_CUDA(cudaGetLastError());
 }

@@ -310,11 +310,12 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
 // Exact low-resolution score of each of the network's K1 candidates: over the
 // ring pixels only, d(j, t) = c0 + sum_q w2_q |P_j,q|^2 - Re(P_j,q conj(cvec_q ab_t,q))
 // (the coarse diff2 restricted to the ring plus the particle's constant) and
-// score_j = log sum_t pdf_t(t) exp(dmin - d(j, t)) + log pdf_o(j), the log of
-// the particle's low-resolution posterior of orientation j up to a constant.
+// score_j = log sum_t pdf_t(t) exp(-d(j, t)) + log pdf_o(j), the log of the
+// particle's low-resolution posterior of orientation j up to a constant.
 // The contraction runs on the tensor cores (tc_launch_rescore: split-BF16, one
-// 128 x 96 tile per 128 candidates of a particle); its operands are the ring
-// pixels as K = 2 x ring (re, im interleaved), zero padded to kr.
+// 128 x 96 tile per 128 candidates of a particle) and its epilogue reduces each
+// candidate's row to the score; the operands are the ring pixels as
+// K = 2 x ring (re, im interleaved), zero padded to kr.
 constexpr int RS_TMAX = 96;            // translations of one rescoring tile
 
 // projections of every coarse orientation at the ring pixels: FP32 (norms) and
@@ -362,13 +363,12 @@ __global__ void __launch_bounds__(128) k_ring_images(Tables tb, Work w, const in
     }
 }
 
-// candidate rows (b*K1 + j) of the A operand, their ring norms, and the reset of
-// the per-particle minimum; one warp per candidate
+// candidate rows (b*K1 + j) of the A operand and their ring norms; one warp per candidate
 __global__ void __launch_bounds__(256) k_rescore_gather(int n, int k1, int nring, int kr, const int* __restrict__ cand,
                                                         const float2* __restrict__ projR, const bf16* __restrict__ rh,
                                                         const bf16* __restrict__ rl, const float* __restrict__ w2r,
                                                         bf16* __restrict__ ah, bf16* __restrict__ al,
-                                                        float* __restrict__ rnorm, unsigned* __restrict__ rmin)
+                                                        float* __restrict__ rnorm)
 {
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -398,34 +398,7 @@ __global__ void __launch_bounds__(256) k_rescore_gather(int n, int k1, int nring
     }
     (void)projR;
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) {
-        rnorm[gw] = acc;
-        if (gw % k1 == 0) rmin[b] = 0xffffffffu;
-    }
-}
-
-// score of every candidate from its T ring diff2 values; one warp per candidate
-__global__ void __launch_bounds__(256) k_rescore_reduce(Tables tb, Work w, int k1, const int* __restrict__ cand,
-                                                        const float* __restrict__ d2, const unsigned* __restrict__ rmin,
-                                                        float* __restrict__ score)
-{
-    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (gw >= (long long)w.n * k1) return;
-    const int b = (int)(gw / k1), T = tb.T;
-    const float mn = key2f(rmin[b]);
-    const float* d = d2 + (size_t)gw * T;
-    float se = 0.f;   // FP32: a ranking score (terms below e^-80 of the particle's best are dropped)
-    for (int t = lane; t < T; t += 32) {
-        const float v = d[t];
-        if (v < 0.f || v - mn > 80.f) continue;
-        se += (float)w.pdf_t[(size_t)b * T + t] * __expf(mn - v);
-    }
-    for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
-    if (lane == 0) {
-        const int oc = cand[gw];
-        score[gw] = (tb.skip[oc] || !(se > 0.f)) ? -INFINITY : __logf(se) + (float)log(tb.pdf_oc[oc]);
-    }
+    if (lane == 0) rnorm[gw] = acc;
 }
 
 // the k best-scored candidates of each particle, ranked (ties by rank in the network's list)
@@ -1391,8 +1364,6 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.rbh, 0, rb_rows * N.kr * sizeof(bf16)));
     T2B_CUDA(cudaMemset(N.rbl, 0, rb_rows * N.kr * sizeof(bf16)));
     N.rnorm = (float*)net_dalloc(W, ra_rows * sizeof(float));
-    N.rd2 = (float*)net_dalloc(W, ra_rows * tb.T * sizeof(float));
-    N.rmin = (unsigned*)net_dalloc(W, (size_t)B * sizeof(unsigned));
     const int rs = tc_slot_rescore();
     tc_set_map_box(c->tc, rs, N.rah, (int)ra_rows, N.kr, 128);
     tc_set_map_box(c->tc, rs + 1, N.ral, (int)ra_rows, N.kr, 128);
@@ -1584,11 +1555,10 @@ void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st)
         k_ring_images<<<w.n * tb.T, 128, 0, st>>>(tb, w, N.ring, N.nring, N.kr, (bf16*)N.rbh, (bf16*)N.rbl, N.w2r);
         k_rescore_gather<<<(int)((nc * 32 + 255) / 256), 256, 0, st>>>(w.n, N.k1, N.nring, N.kr, N.cand1, N.projR,
                                                                        (const bf16*)N.rth, (const bf16*)N.rtl, N.w2r,
-                                                                       (bf16*)N.rah, (bf16*)N.ral, N.rnorm, N.rmin);
+                                                                       (bf16*)N.rah, (bf16*)N.ral, N.rnorm);
         T2B_CUDA(cudaGetLastError());
-        tc_launch_rescore(w.n, N.k1, tb.T, N.kr, c->tc, w.c0, N.rnorm, tb.skip, N.cand1, N.rd2, N.rmin, w.err, nullptr,
+        tc_launch_rescore(w.n, N.k1, tb.T, N.kr, c->tc, N.rnorm, tb.skip, N.cand1, w.pdf_t, tb.pdf_oc, N.score1, w.err,
                           st);
-        k_rescore_reduce<<<(int)((nc * 32 + 255) / 256), 256, 0, st>>>(tb, w, N.k1, N.cand1, N.rd2, N.rmin, N.score1);
         k_rescore_select<<<w.n, 1024, 0, st>>>(N.cand1, N.score1, N.k1, N.kprop, N.prop);
     } else {
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO,

@@ -54,8 +54,7 @@ struct ProposalNet {
     float* w2r = nullptr;              // B x nring
     void *rah = nullptr, *ral = nullptr;  // B*NET_MAX_K1 x kr: gathered candidate rows
     void *rbh = nullptr, *rbl = nullptr;  // B*T x kr: shifted ring images
-    float *rnorm = nullptr, *rd2 = nullptr;  // B*K1 ring norms, B*K1*T ring diff2
-    unsigned* rmin = nullptr;          // B
+    float* rnorm = nullptr;            // B*K1 ring norms
     int* cand1 = nullptr;              // B x k1 network candidates
     float* score1 = nullptr;           // B x k1 low-resolution scores
     double thr = 0.999;

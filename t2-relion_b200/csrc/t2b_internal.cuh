@@ -221,9 +221,9 @@ int tc_slot_proposals();
 int tc_slot_audit();
 int tc_slot_rescore();
 void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows);
-void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* c0, const float* norms,
-                       const unsigned char* skip, const int* cand, float* d2, unsigned* minkey, int* err,
-                       const int* gate, cudaStream_t st);
+void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* norms, const unsigned char* skip,
+                       const int* cand, const double* pdf_t, const double* pdf_oc, float* score, int* err,
+                       cudaStream_t st);
 void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, int tn, const float* nprop,
                     cudaStream_t st);
 void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
