@@ -31,7 +31,8 @@ namespace t2b {
 namespace {
 
 constexpr int TM = 128, TN = 256, TK = 64;
-constexpr int STAGES = 2;
+constexpr int STAGES = 2;       // pipeline stages of 128 x 256 tiles (96 KB each)
+constexpr int MAXSTAGES = 3;    // 128 x 96 tiles: 56 KB stages, three fit in the same space
 constexpr uint32_t A_BYTES = TM * TK * 2;              // 16 KB
 constexpr uint32_t B_BYTES = TN * TK * 2;              // 32 KB
 constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
@@ -200,18 +201,23 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
     const CUtensorMap* mIh = maps + ib;
     const CUtensorMap* mIl = maps + ib + 1;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], tfull_bar[2], tempty_bar[2], drain_bar;
+    __shared__ __align__(8) uint64_t full_bar[MAXSTAGES], empty_bar[MAXSTAGES], tfull_bar[2], tempty_bar[2], drain_bar;
     __shared__ uint32_t tmem_base_slot;
     __shared__ volatile int abort_flag;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // stage geometry of this launch: B box of tn rows; narrow tiles get a third stage
+    const int tn_l = p.tn ? p.tn : TN;
+    const uint32_t bbytes = (uint32_t)tn_l * TK * 2;                 // multiple of 1024
+    const uint32_t sbytes = 2 * A_BYTES + 2 * bbytes;
+    const int nst = (2 * A_BYTES + 2 * bbytes) * MAXSTAGES <= STAGES * STAGE_BYTES ? MAXSTAGES : STAGES;
     const uint32_t base = (su32(smem_raw) + 1023u) & ~1023u;
     uint8_t* gbase = smem_raw + (base - su32(smem_raw));
     float* epi = reinterpret_cast<float*>(gbase + STAGES * STAGE_BYTES);          // 4 x 32 x 33
     unsigned* smin = reinterpret_cast<unsigned*>(epi + 4 * 32 * EPI_LD);          // 4 x (TN+2)
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; s++) { mbar_init(&full_bar[s], 1); mbar_init(&empty_bar[s], 1); }
+        for (int s = 0; s < MAXSTAGES; s++) { mbar_init(&full_bar[s], 1); mbar_init(&empty_bar[s], 1); }
         for (int s = 0; s < 2; s++) { mbar_init(&tfull_bar[s], 1); mbar_init(&tempty_bar[s], 4); }
         mbar_init(&drain_bar, 1);
         abort_flag = 0;
@@ -238,10 +244,9 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             asm volatile("prefetch.tensormap [%0];" ::"l"(ms[j]) : "memory");
         }
         int it = 0;
-        int issued[STAGES] = {0, 0};
-        uint32_t last_par[STAGES] = {0, 0};
-        const uint32_t b_bytes = (uint32_t)(p.tn ? p.tn : TN) * TK * 2;
-        const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + b_bytes * (p.products >= 2 ? 2u : 1u);
+        int issued[MAXSTAGES] = {0, 0, 0};
+        uint32_t last_par[MAXSTAGES] = {0, 0, 0};
+        const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + bbytes * (p.products >= 2 ? 2u : 1u);
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
             int ya, yb;
             if (p.mode == 0) {
@@ -250,19 +255,19 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 ya = mt * TM;
                 yb = nt * TN;
             } else {
-                ya = tile * TM;
+                ya = (p.mtp > 1) ? tile * TM : tile * p.ppt * p.kslot;
                 yb = (tile / (p.mtp ? p.mtp : 1)) * p.ppt * p.T;
             }
             for (int kb = 0; kb < p.kblocks; kb++, it++) {
-                const int s = it % STAGES;
-                const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+                const int s = it % nst;
+                const uint32_t ph = (uint32_t)(it / nst) & 1u;
                 if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
-                uint8_t* st = gbase + s * STAGE_BYTES;
+                uint8_t* st = gbase + s * sbytes;
                 mbar_expect_tx(&full_bar[s], tx_bytes);
                 tma_load(st, mPh, &full_bar[s], kb * TK, ya);
                 if (p.products == 3) tma_load(st + A_BYTES, mPl, &full_bar[s], kb * TK, ya);
                 tma_load(st + 2 * A_BYTES, mIh, &full_bar[s], kb * TK, yb);
-                if (p.products >= 2) tma_load(st + 2 * A_BYTES + B_BYTES, mIl, &full_bar[s], kb * TK, yb);
+                if (p.products >= 2) tma_load(st + 2 * A_BYTES + bbytes, mIl, &full_bar[s], kb * TK, yb);
                 issued[s] = 1;
                 last_par[s] = ph;
             }
@@ -270,7 +275,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         if (abort_flag) {
             // let the copies already in flight land before the CTA exits
             volatile int never = 0;
-            for (int s = 0; s < STAGES; s++)
+            for (int s = 0; s < nst; s++)
                 if (issued[s]) mbar_wait(&full_bar[s], last_par[s], &never);
         }
     } else if (warp == 1 && lane == 0) {
@@ -285,13 +290,13 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             const uint32_t dt = tmem + (uint32_t)(abuf * TN);
             bool ok = true;
             for (int kb = 0; kb < p.kblocks; kb++, it++) {
-                const int s = it % STAGES;
-                const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+                const int s = it % nst;
+                const uint32_t ph = (uint32_t)(it / nst) & 1u;
                 if (!mbar_wait(&full_bar[s], ph, &abort_flag)) { ok = false; break; }
                 tc_fence_after();
-                const uint32_t sa = base + s * STAGE_BYTES;
+                const uint32_t sa = base + s * sbytes;
                 const uint64_t dPh = sdesc(sa), dPl = sdesc(sa + A_BYTES);
-                const uint64_t dIh = sdesc(sa + 2 * A_BYTES), dIl = sdesc(sa + 2 * A_BYTES + B_BYTES);
+                const uint64_t dIh = sdesc(sa + 2 * A_BYTES), dIl = sdesc(sa + 2 * A_BYTES + bbytes);
 #pragma unroll
                 for (int k = 0; k < TK / 16; k++) {
                     const uint64_t ko = (uint64_t)(k * 32) >> 4;  // 32 bytes per K=16 step
@@ -759,7 +764,7 @@ void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float
 void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, int tn, const float* nprop,
                     cudaStream_t st)
 {
-    T2B_REQUIRE(ppt >= 1 && ppt * kslot == TM && ppt * tb.T <= tn && w.kprop <= kslot && (tn == 96 || tn == TN),
+    T2B_REQUIRE(ppt >= 1 && ppt * kslot <= TM && ppt * tb.T <= tn && w.kprop <= kslot && (tn == 96 || tn == TN),
                 T2B_ERR_STATE, "proposal tile shape");
     TcParams p{};
     p.mode = 1;

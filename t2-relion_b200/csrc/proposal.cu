@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(1024) k_rescore_select(const int* __restrict__
 // from the configuration's coarse operand (16-byte copies), and its norm
 // N = sum_k w2_k |P|^2_k from the same split-BF16 operands the full pass's norm
 // contraction reads (|P|^2 hi + lo per orientation, w2 hi + lo per particle).
-// Row of (b, j) in the A operand: (b / ppt) * 128 + (b % ppt) * kslot + j.
+// Row of (b, j) in the A operand: b * kslot + j (tile i starts at row i * ppt * kslot).
 // Runs while *gate != 0.
 __global__ void __launch_bounds__(256) k_prop_gather(Work w, int ppt, int kslot, int kdim, int kn,
                                                      const bf16* __restrict__ bh, const bf16* __restrict__ bl,
@@ -449,7 +449,8 @@ __global__ void __launch_bounds__(256) k_prop_gather(Work w, int ppt, int kslot,
     const int b = blockIdx.y, j = blockIdx.x;
     if (b >= w.n || j >= w.kprop) return;
     const size_t oc = (size_t)w.prop[(size_t)b * w.kprop + j];
-    const size_t row = (size_t)(b / ppt) * 128 + (size_t)(b % ppt) * kslot + j;
+    const size_t row = (size_t)b * kslot + j;
+    (void)ppt;
     {
         const uint4* sh = reinterpret_cast<const uint4*>(bh + oc * kdim);
         const uint4* sl = reinterpret_cast<const uint4*>(bl + oc * kdim);
@@ -1415,14 +1416,16 @@ void net_setup(t2b_ctx* c, int na_max)
     N.ready = true;
 }
 
-// Proposal tiles: one particle per 128 x 96 tile (up to 128 proposals x its
-// translations) when T <= 96; otherwise 128 x 256 tiles of two particles with
-// up to 64 proposals each, or of one particle.
+// Proposal tiles: one particle per 128 x 96 tile (its proposals x its
+// translations) when T <= 96, with 64 rows per particle in the gathered operand
+// when k <= 64 (the tile's other 64 rows are the next particle's, read from L2
+// and discarded); otherwise 128 x 256 tiles of two particles with up to 64
+// proposals each, or of one particle.
 void set_tile_shape(ProposalNet& N, int T)
 {
     if (T <= 96) {
         N.ppt = 1;
-        N.kslot = 128;
+        N.kslot = N.kprop <= 64 ? 64 : 128;
         N.tn = 96;
     } else if (N.kprop <= 64 && 2 * T <= 256) {
         N.ppt = 2;
