@@ -295,6 +295,79 @@ int t2b_proposal_logits(t2b_ctx* ctx, const float* imgs, int n, float* logits);
 int t2b_proposal_grad(t2b_ctx* ctx, const float* imgs, const int* tgt_oc, const float* tgt_w, int n, double* loss,
                       float* grad);
 
+/* ---------------------------------------------------------------------------
+ * Image preparation: real-space particles -> the t2b_batch inputs, on the device.
+ *
+ * MlOptimiser::getFourierTransformsAndCtfs (src/ml_optimiser.cpp:5689-6390;
+ * accelerated counterpart src/acc/acc_ml_optimiser_impl.h:96-1030) for 2D
+ * particle images, and the Minvsigma2 image of
+ * precalculateShiftedImagesCtfsAndInvSigma2s (src/ml_optimiser.cpp:6680-6720):
+ * norm correction, rounded old offset as an integer shift with zero fill,
+ * the unmasked and the soft-masked image (average or noise background)
+ * Fourier transformed (forward divided by N^2), windowed to current_size and
+ * centred by sign, the masked image's power spectrum and highres_Xi2, the CTF
+ * image (CTF::getFftwImage without padding) and Minvsigma2.  One optics group
+ * per configuration; no helical, multi-body or subtomogram paths.
+ * The noise background has the reference's spectrum but its own
+ * counter-based generator (seed random_seed + part_id): the reference's
+ * rand() / curand draws are not reproducible across thread schedules.
+ * ------------------------------------------------------------------------- */
+typedef struct t2b_prep_config {
+    int image_size;             /* N: particle box (even, a product of 2, 3, 5; 8..512)   */
+    int current_size;           /* s: window handed to the E-step (even, <= N)            */
+    int max_batch;              /* particles per call                                     */
+    int zero_mask;              /* 1: average background outside the mask (--zero_mask);
+                                   0: noise background of spectrum sigma2_noise           */
+    int random_seed;            /* noise of a particle: random_seed + its part_id         */
+    int do_norm_correction;
+    int do_ctf_correction;
+    int ctf_premultiplied;      /* CTF image squared                                      */
+    int ctf_phase_flipped;      /* |CTF| (do_abs)                                          */
+    int only_flip_phases;       /* sign of the CTF                                        */
+    int intact_ctf_first_peak;  /* 1 until the first peak                                 */
+    int n_sigma2;               /* length of sigma2_noise (model ori_size/2 + 1)          */
+    const double* sigma2_noise; /* mymodel.sigma2_noise[optics_group], host               */
+    double pixel_size;          /* Angstrom per pixel of the particles                    */
+    double mask_radius;         /* pixels: particle_diameter / (2 pixel_size)             */
+    double width_mask_edge;     /* pixels                                                 */
+    double avg_norm_correction;
+    double sigma2_fudge;
+    double remap_noise;         /* (image_size*pixel_size) / (ori_size*model pixel size)  */
+    double remap_minv;          /* (ori_size*model pixel size) / (image_size*pixel_size)  */
+    double voltage, cs, q0;     /* optics group: kV, mm, amplitude contrast               */
+} t2b_prep_config;
+
+/* Per-particle parameters, T2B_PREP_NPARAM doubles each: old offset x, y
+ * (METADATA_XOFF/YOFF, pixels), offset prior x, y (999 = none), METADATA_NORM,
+ * defocus U, V (Angstrom), defocus angle (deg), CTF B-factor, CTF scale
+ * (k-factor), phase shift (deg), scale correction (mymodel.scale_correction). */
+#define T2B_PREP_NPARAM 12
+
+typedef struct t2b_prep_batch {
+    int n;                      /* particles (<= max_batch)                               */
+    int _pad;
+    const float* images;        /* n x N x N real space, row-major, centre at (N/2, N/2)  */
+    const double* params;       /* n x T2B_PREP_NPARAM                                    */
+    const long long* part_id;   /* n (noise seeds; may be NULL with zero_mask)            */
+} t2b_prep_batch;
+
+typedef struct t2b_prep_out {   /* P = s*(s/2+1); layouts of t2b_batch                    */
+    float* fimg;                /* n x 2P masked image                                    */
+    float* fimg_nomask;         /* n x 2P unmasked image                                  */
+    float* ctf;                 /* n x P                                                  */
+    float* minvsigma2;          /* n x P                                                  */
+    double* scalars;            /* n x 8: t2b_batch.scalars                               */
+    double* power;              /* n x (N/2+1) power spectrum of the masked image
+                                   (exp_power_img), or NULL                              */
+} t2b_prep_out;
+
+/* Upload the per-iteration state (noise spectrum, optics) and size the workspace. */
+int t2b_prep_configure(t2b_ctx* ctx, const t2b_prep_config* cfg);
+/* Host variant: host buffers in and out, returns when done.  Device variant:
+ * device buffers, enqueued on `stream` (cudaStream_t, NULL = the context's). */
+int t2b_prep_batch_host(t2b_ctx* ctx, const t2b_prep_batch* batch, const t2b_prep_out* out);
+int t2b_prep_batch_device(t2b_ctx* ctx, const t2b_prep_batch* batch, const t2b_prep_out* out, void* stream);
+
 /* Host sampling (HealpixSampling, src/healpix_sampling.cpp:534-640,
  * 1787-2040), C1 symmetry, no perturbation.  Fills Euler matrices of the
  * coarse orientations (idir*n_psi + ipsi), of the fine orientations

@@ -39,6 +39,7 @@ ABI_SYMBOLS = (
     "t2b_sampling", "t2b_reconstruct_divide_noalloc", "t2b_last_launch_count",
     "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
+    "t2b_prep_configure", "t2b_prep_batch_host", "t2b_prep_batch_device",
 )
 
 
@@ -108,6 +109,30 @@ class ProposalReport(ctypes.Structure):
                 ("params", ctypes.c_longlong)]
 
 
+class PrepConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "image_size", "current_size", "max_batch", "zero_mask", "random_seed", "do_norm_correction",
+        "do_ctf_correction", "ctf_premultiplied", "ctf_phase_flipped", "only_flip_phases",
+        "intact_ctf_first_peak", "n_sigma2")] + [("sigma2_noise", _p)] + [(n, ctypes.c_double) for n in (
+            "pixel_size", "mask_radius", "width_mask_edge", "avg_norm_correction", "sigma2_fudge",
+            "remap_noise", "remap_minv", "voltage", "cs", "q0")]
+
+
+class PrepBatch(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("_pad", ctypes.c_int), ("images", _p), ("params", _p), ("part_id", _p)]
+
+
+class PrepOut(ctypes.Structure):
+    _fields_ = [(n, _p) for n in ("fimg", "fimg_nomask", "ctf", "minvsigma2", "scalars", "power")]
+
+
+PREP_NPARAM = 12
+PREP_DEFAULTS = dict(zero_mask=0, random_seed=0, do_norm_correction=0, do_ctf_correction=1, ctf_premultiplied=0,
+                     ctf_phase_flipped=0, only_flip_phases=0, intact_ctf_first_peak=0, avg_norm_correction=1.0,
+                     sigma2_fudge=1.0, remap_noise=1.0, remap_minv=1.0, voltage=300.0, cs=2.7, q0=0.1,
+                     width_mask_edge=5.0)
+
+
 def _setup_prototypes():
     i, v, c = ctypes.c_int, ctypes.c_void_p, ctypes.c_char_p
     lib.t2b_create.argtypes = [i, ctypes.POINTER(v)]
@@ -139,6 +164,9 @@ def _setup_prototypes():
     lib.t2b_proposal_features.argtypes = [v, ctypes.POINTER(Batch), v]
     lib.t2b_proposal_logits.argtypes = [v, v, i, v]
     lib.t2b_proposal_grad.argtypes = [v, v, v, v, i, ctypes.POINTER(ctypes.c_double), v]
+    lib.t2b_prep_configure.argtypes = [v, ctypes.POINTER(PrepConfig)]
+    lib.t2b_prep_batch_host.argtypes = [v, ctypes.POINTER(PrepBatch), ctypes.POINTER(PrepOut)]
+    lib.t2b_prep_batch_device.argtypes = [v, ctypes.POINTER(PrepBatch), ctypes.POINTER(PrepOut), v]
 
 
 _setup_prototypes()
@@ -320,6 +348,48 @@ class EStep:
         r = Result(*[result_ptrs.get(name) for name, _ in Result._fields_])
         _check(lib.t2b_estep_batch_device(self._h, ctypes.byref(b), ctypes.byref(r),
                                           ctypes.c_void_p(stream)))
+
+    # ---------------------------------------------- image preparation
+    def configure_prep(self, *, image_size, current_size, max_batch, sigma2_noise, pixel_size, mask_radius, **kw):
+        """t2b_prep_configure (getFourierTransformsAndCtfs state of one optics group)."""
+        opts = dict(PREP_DEFAULTS)
+        unknown = set(kw) - set(opts)
+        if unknown:
+            raise TypeError(f"unknown image-preparation settings: {sorted(unknown)}")
+        opts.update(kw)
+        sig = np.ascontiguousarray(sigma2_noise, np.float64)
+        self._prep_keep = sig
+        c = PrepConfig(image_size=image_size, current_size=current_size, max_batch=max_batch,
+                       n_sigma2=sig.size, sigma2_noise=_ptr(sig), pixel_size=pixel_size, mask_radius=mask_radius,
+                       **opts)
+        _check(lib.t2b_prep_configure(self._h, ctypes.byref(c)))
+        self.prep_cfg = dict(image_size=image_size, current_size=current_size, max_batch=max_batch,
+                             sigma2_noise=sig.copy(), pixel_size=pixel_size, mask_radius=mask_radius, **opts)
+        return self.prep_cfg
+
+    def prepare_images(self, images, params, part_id=None):
+        """t2b_prep_batch_host: real-space images (n, N, N) and per-particle
+        parameters (n, 12) -> dict(fimg, fimg_nomask, ctf, minvsigma2, scalars, power)."""
+        pc = self.prep_cfg
+        N, s = pc["image_size"], pc["current_size"]
+        img = np.ascontiguousarray(images, np.float32)
+        n = img.shape[0]
+        par = np.ascontiguousarray(params, np.float64).reshape(n, PREP_NPARAM)
+        pid = None if part_id is None else np.ascontiguousarray(part_id, np.int64)
+        P = s * (s // 2 + 1)
+        out = dict(fimg=np.zeros((n, P), np.complex64), fimg_nomask=np.zeros((n, P), np.complex64),
+                   ctf=np.zeros((n, P), np.float32), minvsigma2=np.zeros((n, P), np.float32),
+                   scalars=np.zeros((n, 8)), power=np.zeros((n, N // 2 + 1)))
+        b = PrepBatch(n, 0, _ptr(img), _ptr(par), _ptr(pid))
+        o = PrepOut(*[_ptr(out[k]) for k, _ in PrepOut._fields_])
+        _check(lib.t2b_prep_batch_host(self._h, ctypes.byref(b), ctypes.byref(o)))
+        return out
+
+    def prepare_images_device(self, n, images_ptr, params_ptr, part_id_ptr, out_ptrs, stream=0):
+        """t2b_prep_batch_device; pointers are device memory (ctypes.c_void_p)."""
+        b = PrepBatch(n, 0, images_ptr, params_ptr, part_id_ptr)
+        o = PrepOut(*[out_ptrs.get(k) for k, _ in PrepOut._fields_])
+        _check(lib.t2b_prep_batch_device(self._h, ctypes.byref(b), ctypes.byref(o), ctypes.c_void_p(stream)))
 
     # ---------------------------------------------- learned orientation proposals
     def train_proposals(self, minvsigma2, n_train=200000, n_posterior=20000, n_val=1024, epochs=4, batch=256,

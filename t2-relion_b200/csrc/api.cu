@@ -91,6 +91,7 @@ void t2b_destroy(t2b_ctx* c)
         cudaStreamSynchronize(c->stream);
         free_allocs(c);
         proposal_release(c);
+        imageprep_release(c);
         for (auto p : c->mdl) cudaFree(p);
         for (auto p : c->gdata) cudaFree(p);
         for (auto p : c->gweight) cudaFree(p);

@@ -13,6 +13,7 @@
 namespace t2b {
 
 struct ProposalNet;
+struct ImagePrep;
 
 // ---------------------------------------------------------------- errors
 void set_error(const std::string& msg);
@@ -239,6 +240,10 @@ namespace t2b {
 void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool allow_prop);
 }
 
+namespace t2b {
+void imageprep_release(t2b_ctx* c);   // context destruction (imageprep.cu)
+}
+
 struct t2b_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -277,4 +282,5 @@ struct t2b_ctx {
     float stage_ms[9]{};
     bool prop_events = false;                 // the last timed batch recorded ev[8..11]
     t2b::ProposalNet* net = nullptr;          // learned orientation proposals (proposal.cu)
+    t2b::ImagePrep* prep = nullptr;           // image preparation state (imageprep.cu)
 };

@@ -230,7 +230,7 @@ def make_particles(fmap, n, *, ori_size, s, r_max, angpix, snr, seed, max_shift=
     scal[:, 1] = xi2
     scal[:, 6] = 1.0
     return dict(fimg=fimg, ctf=ctf, minv=minv, scalars=scal, sigma2=sigma2,
-                rot=rot, tilt=tilt, psi=psi, shifts=shifts, A=A, classes=cls)
+                rot=rot, tilt=tilt, psi=psi, shifts=shifts, A=A, classes=cls, defU=defU, defV=defV, dang=dang)
 
 
 # Named workloads.  Sizes only; seeds are per call.
