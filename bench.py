@@ -372,6 +372,112 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+PREP_WORKLOAD = dict(name="prep_box128_s80_noise_background", image_size=128, current_size=80, pixel_size=1.3,
+                     mask_radius=50.0, width_mask_edge=5.0, zero_mask=0, random_seed=11, sigma2_fudge=1.0,
+                     voltage=300.0, cs=2.7, q0=0.1)
+
+
+def run_prep(args):
+    """Image preparation (t2b_prep_batch_*) of box-128 real-space particles to the
+    80-pixel E-step window with the noise background: particles/s."""
+    import torch
+    t2b = load_package()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    W = PREP_WORKLOAD
+    N, s, B = W["image_size"], W["current_size"], args.prep_batch
+    rng = np.random.default_rng(W["random_seed"])
+    imgs = rng.standard_normal((B, N, N)).astype(np.float32)
+    par = np.zeros((B, t2b.PREP_NPARAM))
+    par[:, 0:2] = rng.uniform(-5, 5, (B, 2))
+    par[:, 2:4] = 999.
+    par[:, 4] = 1.0
+    par[:, 5] = rng.uniform(10000, 30000, B)
+    par[:, 6] = par[:, 5] - rng.uniform(0, 1000, B)
+    par[:, 7] = rng.uniform(0, 180, B)
+    par[:, 9] = par[:, 11] = 1.0
+    pid = np.arange(B, dtype=np.int64)
+    sig = 0.2 + np.linspace(1.0, 0.05, N // 2 + 1) ** 2
+    es = t2b.EStep(0)
+    cfg = {k: v for k, v in W.items() if k != "name"}
+    es.configure_prep(max_batch=B, sigma2_noise=sig, **cfg)
+    dev = torch.device("cuda", 0)
+    P, h = s * (s // 2 + 1), N // 2 + 1
+    ti, tp, tq = (torch.from_numpy(a).to(dev) for a in (imgs, par, pid))
+    out = dict(fimg=torch.zeros(B, 2 * P, device=dev), fimg_nomask=torch.zeros(B, 2 * P, device=dev),
+               ctf=torch.zeros(B, P, device=dev), minvsigma2=torch.zeros(B, P, device=dev),
+               scalars=torch.zeros(B, 8, dtype=torch.float64, device=dev),
+               power=torch.zeros(B, h, dtype=torch.float64, device=dev))
+    optr = {k: ctypes.c_void_p(v.data_ptr()) for k, v in out.items()}
+    stream = torch.cuda.Stream(dev)
+
+    def step():
+        es.prepare_images_device(B, ctypes.c_void_p(ti.data_ptr()), ctypes.c_void_p(tp.data_ptr()),
+                                 ctypes.c_void_p(tq.data_ptr()), optr, stream=stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        torch.cuda.nvtx.range_push("timed_steps")
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    value = B / (ms / 1000.0)
+    # end to end through the host entry point (host images in, host E-step inputs out)
+    pin_img = torch.from_numpy(imgs).pin_memory()
+    pin_par = torch.from_numpy(par).pin_memory()
+    pin_pid = torch.from_numpy(pid).pin_memory()
+    hout = {k: torch.zeros(v.shape, dtype=v.dtype).pin_memory() for k, v in out.items()}
+    b = t2b.PrepBatch(B, 0, ctypes.c_void_p(pin_img.data_ptr()), ctypes.c_void_p(pin_par.data_ptr()),
+                      ctypes.c_void_p(pin_pid.data_ptr()))
+    o = t2b.PrepOut(*[ctypes.c_void_p(hout[k].data_ptr()) for k, _ in t2b.PrepOut._fields_])
+    for _ in range(2):
+        t2b._check(t2b.lib.t2b_prep_batch_host(es._h, ctypes.byref(b), ctypes.byref(o)))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        t2b._check(t2b.lib.t2b_prep_batch_host(es._h, ctypes.byref(b), ctypes.byref(o)))
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    h2d = pin_img.numel() * 4 + pin_par.numel() * 8 + pin_pid.numel() * 8
+    d2h = sum(v.numel() * v.element_size() for v in hout.values())
+    # algorithmic bytes per particle: the image and its parameters in, the E-step inputs out
+    per = N * N * 4 + t2b.PREP_NPARAM * 8 + 8 + 2 * (2 * P * 4) + 2 * (P * 4) + 8 * 8 + h * 8
+    peaks, src = measured_peaks()
+    achieved = per * B / (ms / 1000.0) / 1e9
+    peak = peaks.get("hbm_gbs", 6650.0)
+    line = {"metric": "image preparation particles/s box128 -> 80-pixel window, noise background",
+            "value": value, "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (FFT) / f64 (sums, noise, CTF)", "data": "synthetic",
+            "config": {"workload": W["name"], "particles_per_step": B,
+                       "l2": "inputs (%.0f MB) larger than L2" % (B * N * N * 4 / 1e6)},
+            "e2e": {"value": B / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            # the box-128 workload takes the fused path: k_noise_fused + k_prep_fused per call
+            "gpu_launches": 2 * args.steps, "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "kernel": "the preparation pass (k_noise_fused, k_prep_fused)",
+                         "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": src, "traffic": None,
+                         "bytes_per_particle": per}}
+    if not args.no_cpu_baseline:
+        import imageprep_oracle as ipo
+        ocfg = dict(cfg, sigma2_noise=sig, do_norm_correction=0, avg_norm_correction=1.0, remap_noise=1.0,
+                    remap_minv=1.0, do_ctf_correction=1, ctf_premultiplied=0, ctf_phase_flipped=0,
+                    only_flip_phases=0, intact_ctf_first_peak=0)
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < min(args.ref_seconds, 10.0):
+            ipo.prepare(imgs[k:k + 8].astype(np.float64), par[k:k + 8], pid[k:k + 8], ocfg)
+            k += 8
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": k / dt, "unit": "particles/s", "cores": 1, "kind": "port",
+                                "sample": f"{k} particles through the FP64 numpy oracle"}
+    print(json.dumps(line), flush=True)
+    es.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -390,7 +496,14 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--profile-case", action="store_true",
                     help="HEALPix order 2 instead of 3 (for ncu captures; not a bench number)")
+    ap.add_argument("--stage", default="estep", choices=["estep", "prep"],
+                    help="estep: the E-step (the headline); prep: the image preparation before it "
+                         "(real-space particles -> E-step inputs), its own JSON line")
+    ap.add_argument("--prep-batch", type=int, default=1024, help="prep: particles per call")
     args = ap.parse_args()
+    if args.stage == "prep":
+        run_prep(args)
+        return
     if args.profile_case:
         WORKLOAD.update(PROFILE_WORKLOAD)
     PROP.update(topk=args.topk, rescore=args.rescore)

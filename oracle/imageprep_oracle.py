@@ -37,9 +37,10 @@ Noise background.  The reference draws the noise spectrum from the process-wide
 rand() stream (CPU path, src/funcs.cpp:570-620) or from curand (GPU path,
 src/acc/utilities_impl.h:219-300), neither reproducible across thread
 schedules.  The library and this oracle use one counter-based generator instead
-(SplitMix64 of the particle's seed random_seed + part_id and the element index,
-Box-Muller in FP64), so that the noise image is a function of the particle
-alone; its spectrum is the reference's: N(0, sigma2_fudge * sigma2_noise[ires])
+(one SplitMix64 draw per half-transform element from the particle's key
+random_seed + part_id and the element index; two 24-bit uniforms; Box-Muller,
+FP32 on the device, FP64 here), so that the noise image is a function of the
+particle alone; its spectrum is the reference's: N(0, sigma2_fudge * sigma2_noise[ires])
 for the real and imaginary part of every half-transform element with
 ires < N/2 + 1, zero elsewhere, transformed back unnormalised (c2r).
 """
@@ -90,10 +91,9 @@ def noise_spectrum(seed, N, sigma2_fudge, remapped):
     with np.errstate(over="ignore"):
         key = splitmix64(np.array([np.int64(seed)]).astype(np.uint64))[0]
         c = (ky % N * h + kx).astype(np.uint64)           # element index i * h + j
-        x1 = splitmix64(key + np.uint64(2) * c)
-        x2 = splitmix64(key + np.uint64(2) * c + np.uint64(1))
-    u1 = ((x1 >> np.uint64(11)).astype(np.float64) + 1.0) * 2.0 ** -53   # (0, 1]
-    u2 = (x2 >> np.uint64(11)).astype(np.float64) * 2.0 ** -53           # [0, 1)
+        x = splitmix64(key + c)
+    u1 = ((x >> np.uint64(40)).astype(np.float64) + 1.0) * 2.0 ** -24                  # (0, 1]
+    u2 = ((x >> np.uint64(8)) & np.uint64(0xFFFFFF)).astype(np.float64) * 2.0 ** -24    # [0, 1)
     rad = np.sqrt(-2.0 * np.log(u1))
     ires = ring_index(ky, kx)
     sig = np.zeros(ky.shape)

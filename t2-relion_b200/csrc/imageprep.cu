@@ -24,9 +24,10 @@
 //
 // Noise background: the reference draws the noise spectrum from rand() (CPU)
 // or curand (GPU), neither reproducible across thread schedules; here it is a
-// counter-based generator (SplitMix64 of random_seed + part_id and the element
-// index, Box-Muller in FP64) with the reference's spectrum, transformed back
-// unnormalised like FFTW's c2r.
+// counter-based generator (one SplitMix64 draw per element from the particle's
+// key random_seed + part_id and the element index, two 24-bit uniforms,
+// Box-Muller) with the reference's spectrum, transformed back unnormalised like
+// FFTW's c2r.
 #include "t2b_internal.cuh"
 
 #include <cmath>
@@ -49,6 +50,7 @@ struct ImagePrep {
     t2b_prep_config cfg{};
     int N = 0, h = 0, s = 0, hs = 0, P = 0, max_batch = 0;
     int rpb = 0, cpb = 0, ncol_blocks = 0;
+    bool fused = false;            // one CTA per particle (k_noise_fused, k_prep_fused)
     FftPlan plan{};
     double minv_dc = 0.;
     float2* tw = nullptr;          // N twiddles e^{-2 pi i t / N}
@@ -110,6 +112,36 @@ __device__ __forceinline__ void dft_small(float2* v, const float2* tw, int NR)
         v[2] = csub(a, c);
         v[1] = cadd(b, mid);
         v[3] = csub(b, mid);
+    } else if (R == 8) {
+        // 8 = 2 x 4: DFT4 of the even and odd points, X[k] = E[k] + W8^k O[k], X[k+4] = E[k] - W8^k O[k]
+        float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        dft_small<4, INV>(e, tw, NR);
+        dft_small<4, INV>(o, tw, NR);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float2 t = k == 0 ? o[0] : cmul(o[k], twid<INV>(tw, k * NR));
+            v[k] = cadd(e[k], t);
+            v[k + 4] = csub(e[k], t);
+        }
+    } else if (R == 16) {
+        // 16 = 4 x 4: Y_l = DFT4 over m of v[4m + l]; X[k1 + 4 k2] = DFT4 over l of W16^{l k1} Y_l[k1]
+        float2 y[4][4];
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            float2 t[4] = {v[l], v[4 + l], v[8 + l], v[12 + l]};
+            dft_small<4, INV>(t, tw, NR);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) y[l][k1] = t[k1];
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            float2 z[4];
+#pragma unroll
+            for (int l = 0; l < 4; ++l) z[l] = (l * k1 == 0) ? y[l][k1] : cmul(y[l][k1], twid<INV>(tw, l * k1 * NR));
+            dft_small<4, INV>(z, tw, NR);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = z[k2];
+        }
     } else {
         float2 o[R];
 #pragma unroll
@@ -169,6 +201,72 @@ __device__ float2* fft_smem(float2* a, float2* b, int nfft, const FftPlan& pl, c
     return a;
 }
 
+
+// ---- the same FFT with the size known at compile time (the common box sizes):
+// constant radix plan (radix-16 and radix-8 register butterflies first), constant
+// index arithmetic, unrolled stage sequence
+constexpr int ct_radix(int N, int st)
+{
+    int n = N, k = 0;
+    for (int r : {16, 8, 4, 2, 3, 5})
+        while (n % r == 0) {
+            if (k == st) return r;
+            n /= r;
+            ++k;
+        }
+    return 0;
+}
+constexpr int ct_ns(int N, int st)
+{
+    int ns = 1;
+    for (int k = 0; k < st; ++k) ns *= ct_radix(N, k);
+    return ns;
+}
+
+template <int R, bool INV, int N, int Ns>
+__device__ __forceinline__ void fft_stage_ct(const float2* a, float2* b, int nfft, const float2* tw)
+{
+    constexpr int NR = N / R;
+    constexpr int tstride = N / (Ns * R);
+    for (int e = threadIdx.x; e < nfft * NR; e += blockDim.x) {
+        const int f = e / NR, j = e - f * NR;
+        const float2* in = a + f * N;
+        float2* out = b + f * N;
+        const int k = j % Ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = in[j + r * NR];
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid<INV>(tw, k * r * tstride));
+        }
+        dft_small<R, INV>(v, tw, NR);
+        const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) out[base + r * Ns] = v[r];
+    }
+}
+
+template <int N, bool INV, int ST>
+__device__ __forceinline__ float2* fft_ct(float2* a, float2* b, int nfft, const float2* tw)
+{
+    if constexpr (ct_radix(N, ST) == 0) {
+        return a;
+    } else {
+        fft_stage_ct<ct_radix(N, ST), INV, N, ct_ns(N, ST)>(a, b, nfft, tw);
+        __syncthreads();
+        return fft_ct<N, INV, ST + 1>(b, a, nfft, tw);
+    }
+}
+
+// compile-time size when NC > 0, the runtime plan otherwise
+template <int NC, bool INV>
+__device__ __forceinline__ float2* fft_any(float2* a, float2* b, int nfft, const FftPlan& pl, const float2* tw)
+{
+    if constexpr (NC > 0) return fft_ct<NC, INV, 0>(a, b, nfft, tw);
+    else return fft_smem<INV>(a, b, nfft, pl, tw);
+}
+
 __device__ __forceinline__ int relion_round(double x) { return x > 0 ? (int)(x + 0.5) : (int)(x - 0.5); }
 
 __device__ __forceinline__ unsigned long long splitmix64(unsigned long long z)
@@ -177,6 +275,26 @@ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long z)
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
+}
+
+// ring index ROUND(sqrt(ky^2 + kx^2)): FP32 sqrt decides the rounding exactly for the
+// integer radii of a box <= 512 (sqrt(r2) is never within 3e-4 of a half-integer)
+__device__ __forceinline__ int ring_of(int ky, int kx)
+{
+    return (int)(sqrtf((float)(ky * ky + kx * kx)) + 0.5f);
+}
+
+// noise spectrum element: one SplitMix64 draw of the particle's key and the element
+// index; two 24-bit uniforms u1 in (0, 1], u2 in [0, 1); Box-Muller
+__device__ __forceinline__ float2 noise_value(unsigned long long key, unsigned long long c, float sig)
+{
+    const unsigned long long x = splitmix64(key + c);
+    const float u1 = (float)((x >> 40) + 1ull) * 0x1.0p-24f;
+    const float u2 = (float)((x >> 8) & 0xFFFFFFull) * 0x1.0p-24f;
+    const float rad = sqrtf(-2.f * logf(u1)) * sig;
+    float sn, cs;
+    sincospif(2.f * u2, &sn, &cs);
+    return make_float2(rad * cs, rad * sn);
 }
 
 struct PrepArgs {
@@ -236,19 +354,8 @@ __global__ void __launch_bounds__(PREP_THREADS) k_noise_cols(PrepArgs a)
         float2 v = make_float2(0.f, 0.f);
         if (j < h) {
             const int ky = i < h ? i : i - N;
-            const int ires = relion_round(sqrt((double)(ky * ky + j * j)));
-            if (ires < h) {
-                const double sig = a.noise_sig[ires];
-                const unsigned long long cidx = (unsigned long long)i * h + j;
-                const unsigned long long x1 = splitmix64(key + 2ull * cidx);
-                const unsigned long long x2 = splitmix64(key + 2ull * cidx + 1ull);
-                const double u1 = ((double)(x1 >> 11) + 1.0) * 0x1.0p-53;
-                const double u2 = (double)(x2 >> 11) * 0x1.0p-53;
-                const double rad = sqrt(-2.0 * log(u1)) * sig;
-                double sn, cs;
-                sincospi(2.0 * u2, &sn, &cs);
-                v = make_float2((float)(rad * cs), (float)(rad * sn));
-            }
+            const int ires = ring_of(ky, j);
+            if (ires < h) v = noise_value(key, (unsigned long long)i * h + j, (float)a.noise_sig[ires]);
         }
         b0[c * N + i] = v;
     }
@@ -478,18 +585,31 @@ __global__ void __launch_bounds__(PREP_THREADS) k_cols(PrepArgs a)
     }
 }
 
+// power spectrum of the masked transform: one warp per ring, lanes over the
+// ring's pixels, fixed-order shuffle reduction (deterministic)
+__device__ __forceinline__ void ring_sums(const float* pw, const int* off, const int* pix, int h, double* spec,
+                                          double* power)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int r = warp; r < h; r += nw) {
+        double acc = 0.;
+        for (int q = off[r] + lane; q < off[r + 1]; q += 32) acc += pw[pix[q]];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            spec[r] = acc;
+            if (power) power[r] = acc;
+        }
+    }
+}
+
 // ------------------------------------------------------------ spectrum and scalars
 __global__ void __launch_bounds__(PREP_THREADS) k_final(PrepArgs a)
 {
     __shared__ double s_spec[PREP_MAX_N / 2 + 1];
     const int p = blockIdx.x, h = a.h;
     const float* pw = a.pw + (size_t)p * a.N * h;
-    for (int r = threadIdx.x; r < h; r += blockDim.x) {
-        double acc = 0.;
-        for (int q = a.ring_off[r]; q < a.ring_off[r + 1]; ++q) acc += pw[a.ring_pix[q]];
-        s_spec[r] = acc;
-        if (a.power) a.power[(size_t)p * h + r] = acc;
-    }
+    ring_sums(pw, a.ring_off, a.ring_pix, h, s_spec, a.power ? a.power + (size_t)p * h : nullptr);
     __syncthreads();
     if (threadIdx.x != 0) return;
     double xi2 = 0.;
@@ -507,7 +627,249 @@ __global__ void __launch_bounds__(PREP_THREADS) k_final(PrepArgs a)
     sc[7] = 0.;
 }
 
+// ------------------------------------------------------------ fused path: one CTA per particle
+// When the particle's two half spectra fit in shared memory (N <= 136), the row
+// and column passes run in one CTA per particle and the half spectra never
+// leave the SM: rows in chunks of FQ (ping-pong scratch), unpacked into the
+// masked and unmasked half spectra; then columns in chunks of FQ/2 of each.
+constexpr int FQ = 16;
+constexpr int FUSED_THREADS = 512;
+
+size_t fused_prep_smem(int N)
+{
+    const size_t h = N / 2 + 1;
+    return sizeof(float2) * (N + 2 * h * N + 2 * (size_t)FQ * N) + sizeof(float) * h * N + sizeof(double) * h;
+}
+size_t fused_noise_smem(int N)
+{
+    const size_t h = N / 2 + 1;
+    return sizeof(float2) * (N + h * N + 2 * (size_t)FQ * N);
+}
+
+// noise image of one particle: spectrum -> inverse over y (columns) -> c2r over x (rows)
+template <int NC>
+__global__ void __launch_bounds__(FUSED_THREADS) k_noise_fused(PrepArgs a)
+{
+    extern __shared__ float2 sm[];
+    const int N = NC > 0 ? NC : a.N, h = N / 2 + 1, p = blockIdx.x;
+    float2* s_tw = sm;
+    float2* S = s_tw + N;
+    float2* A = S + (size_t)N * h;
+    float2* B = A + FQ * N;
+    load_tw(s_tw, a.tw, N);
+    const unsigned long long key = splitmix64((unsigned long long)(a.seed + a.pid[p]));
+    for (int e = threadIdx.x; e < N * h; e += blockDim.x) {
+        const int i = e / h, j = e - i * h;
+        const int ky = i < h ? i : i - N;
+        const int ires = ring_of(ky, j);
+        float2 v = make_float2(0.f, 0.f);
+        if (ires < h) v = noise_value(key, (unsigned long long)e, (float)a.noise_sig[ires]);
+        S[e] = v;
+    }
+    __syncthreads();
+    for (int j0 = 0; j0 < h; j0 += FQ) {
+        for (int e = threadIdx.x; e < FQ * N; e += blockDim.x) {
+            const int i = e % N, c = e / N, j = j0 + c;
+            A[e] = j < h ? S[(size_t)i * h + j] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        const float2* r = fft_any<NC, true>(A, B, FQ, a.plan, s_tw);
+        for (int e = threadIdx.x; e < FQ * N; e += blockDim.x) {
+            const int i = e % N, c = e / N, j = j0 + c;
+            if (j < h) S[(size_t)i * h + j] = r[e];
+        }
+        __syncthreads();
+    }
+    float* out = a.noise + (size_t)p * N * N;
+    for (int y0 = 0; y0 < N; y0 += FQ) {
+        for (int e = threadIdx.x; e < FQ * N; e += blockDim.x) {
+            const int rr = e / N, k = e - rr * N, y = y0 + rr;
+            float2 v = make_float2(0.f, 0.f);
+            if (y < N) {
+                const float2* g = S + (size_t)y * h;
+                if (k == 0 || k == N / 2) v = make_float2(g[k].x, 0.f);
+                else if (k < N / 2) v = g[k];
+                else v = make_float2(g[N - k].x, -g[N - k].y);
+            }
+            A[e] = v;
+        }
+        __syncthreads();
+        const float2* r = fft_any<NC, true>(A, B, FQ, a.plan, s_tw);
+        for (int e = threadIdx.x; e < FQ * N; e += blockDim.x) {
+            const int rr = e / N, x = e - rr * N, y = y0 + rr;
+            if (y < N) out[(size_t)y * N + x] = r[e].x;
+        }
+        __syncthreads();
+    }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(FUSED_THREADS) k_prep_fused(PrepArgs a)
+{
+    extern __shared__ float2 sm[];
+    __shared__ double s_w[FUSED_THREADS], s_v[FUSED_THREADS];
+    const int N = NC > 0 ? NC : a.N, h = N / 2 + 1, p = blockIdx.x;
+    constexpr int C = FQ / 2;
+    float2* s_tw = sm;
+    float2* SM = s_tw + N;
+    float2* SU = SM + (size_t)N * h;
+    float2* A = SU + (size_t)N * h;
+    float2* B = A + FQ * N;
+    float* PW = reinterpret_cast<float*>(B + FQ * N);
+    load_tw(s_tw, a.tw, N);
+    const PixelCtx pc = pixel_ctx(a, p);
+    const float* img = a.img + (size_t)p * N * N;
+    const float* noise = a.zero_mask ? nullptr : a.noise + (size_t)p * N * N;
+    // average background (zero-mask path): fixed-order FP64 reduction
+    float bgv = 0.f;
+    if (a.zero_mask) {
+        double sw = 0., sv = 0.;
+        for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+            const int y = e / N, x = e - y * N;
+            const float w = mask_weight(a, x, y);
+            if (w < 0.f) continue;
+            sw += w;
+            sv += (double)w * shifted_pixel(a, img, pc, x, y);
+        }
+        s_w[threadIdx.x] = sw;
+        s_v[threadIdx.x] = sv;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) {
+                s_w[threadIdx.x] += s_w[threadIdx.x + o];
+                s_v[threadIdx.x] += s_v[threadIdx.x + o];
+            }
+            __syncthreads();
+        }
+        bgv = s_w[0] > 0. ? (float)(s_v[0] / s_w[0]) : 0.f;
+    }
+    // rows: masked + i * unmasked, forward FFT over x, split into the two half spectra.
+    // The pixels (and the noise outside the mask) of the next FQ rows are loaded into
+    // registers before the current rows' FFT, so their latency overlaps it.
+    constexpr int PMAX = (FQ * (NC > 0 ? NC : 136) + FUSED_THREADS - 1) / FUSED_THREADS;
+    float ru[PMAX], rn[PMAX];
+    auto fetch = [&](int y0) {
+#pragma unroll
+        for (int t = 0; t < PMAX; ++t) {
+            const int e = threadIdx.x + t * FUSED_THREADS;
+            const int rr = e / N, x = e - rr * N, y = y0 + rr;
+            ru[t] = 0.f;
+            rn[t] = 0.f;
+            if (e < FQ * N && y < N) {
+                ru[t] = shifted_pixel(a, img, pc, x, y);
+                if (!a.zero_mask && mask_weight(a, x, y) >= 0.f) rn[t] = noise[(size_t)y * N + x];
+            }
+        }
+    };
+    fetch(0);
+    for (int y0 = 0; y0 < N; y0 += FQ) {
+#pragma unroll
+        for (int t = 0; t < PMAX; ++t) {
+            const int e = threadIdx.x + t * FUSED_THREADS;
+            if (e >= FQ * N) continue;
+            const int rr = e / N, x = e - rr * N, y = y0 + rr;
+            const float u = ru[t];
+            const float w = mask_weight(a, x, y);
+            float m = u;
+            if (w >= 0.f) {
+                const float fill = a.zero_mask ? bgv : rn[t];
+                m = (w >= 1.f) ? fill : (1.f - w) * u + w * fill;
+            }
+            A[e] = y < N ? make_float2(m, u) : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        if (y0 + FQ < N) fetch(y0 + FQ);
+        const float2* r = fft_any<NC, false>(A, B, FQ, a.plan, s_tw);
+        for (int e = threadIdx.x; e < FQ * h; e += blockDim.x) {
+            const int rr = e / h, k = e - rr * h, y = y0 + rr;
+            if (y >= N) continue;
+            const float2 zk = r[rr * N + k];
+            const float2 zc = r[rr * N + (N - k) % N];
+            SM[(size_t)y * h + k] = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y - zc.y));
+            SU[(size_t)y * h + k] = make_float2(0.5f * (zk.y + zc.y), -0.5f * (zk.x - zc.x));
+        }
+        __syncthreads();
+    }
+    // columns: C of each half spectrum per chunk, forward FFT over y
+    const double* par = a.par + (size_t)p * NPAR;
+    const double az = par[7] * (PI_D / 180.);
+    const double ca = cos(az), sa = sin(az);
+    const double Axx = -par[5] * ca * ca - par[6] * sa * sa;
+    const double Axy = (par[6] - par[5]) * ca * sa;
+    const double Ayy = -par[5] * sa * sa - par[6] * ca * ca;
+    const float inv = 1.f / ((float)N * (float)N);
+    const int s = a.s, hs = a.hs;
+    const size_t o = (size_t)p * a.P;
+    for (int j0 = 0; j0 < h; j0 += C) {
+        for (int e = threadIdx.x; e < 2 * C * N; e += blockDim.x) {
+            const int i = e % N, q = e / N, half = q / C, j = j0 + (q - half * C);
+            A[e] = j < h ? (half ? SU : SM)[(size_t)i * h + j] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        const float2* r = fft_any<NC, false>(A, B, 2 * C, a.plan, s_tw);
+        for (int e = threadIdx.x; e < C * N; e += blockDim.x) {
+            const int i = e % N, c = e / N, j = j0 + c;
+            if (j >= h) continue;
+            const float2 f = r[e];
+            const float fr = f.x * inv, fi = f.y * inv;
+            PW[(size_t)i * h + j] = fr * fr + fi * fi;
+        }
+        if (j0 < hs)
+            for (int e = threadIdx.x; e < C * s; e += blockDim.x) {
+                const int c = e % C, iw = e / C, j = j0 + c;
+                if (j >= hs) continue;
+                const int ky = iw < hs ? iw : iw - s;
+                const int i = ky >= 0 ? ky : ky + N;
+                const float sg = ((iw ^ j) & 1) ? -inv : inv;
+                const float2 fm = r[c * N + i], fu = r[(C + c) * N + i];
+                const size_t w = o + (size_t)iw * hs + j;
+                reinterpret_cast<float2*>(a.fimg)[w] = make_float2(fm.x * sg, fm.y * sg);
+                reinterpret_cast<float2*>(a.fnm)[w] = make_float2(fu.x * sg, fu.y * sg);
+                a.ctf[w] = a.do_ctf ? ctf_value(a, par, Axx, Axy, Ayy, j, ky) : 1.f;
+                a.minv[w] = a.minv_img[(size_t)iw * hs + j];
+            }
+        __syncthreads();
+    }
+    // ring sums (fixed order per ring) and the scalars; the ring lists are staged in
+    // the free row scratch (they fit for every N of this kernel)
+    int* s_pix = reinterpret_cast<int*>(A);
+    double* spec = reinterpret_cast<double*>(PW + (size_t)N * h);
+    const int npix = a.ring_off[h];
+    for (int q = threadIdx.x; q < npix; q += blockDim.x) s_pix[q] = a.ring_pix[q];
+    __syncthreads();
+    ring_sums(PW, a.ring_off, s_pix, h, spec, a.power ? a.power + (size_t)p * h : nullptr);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double xi2 = 0.;
+        if (s < N)
+            for (int r = hs; r < h; ++r) xi2 += spec[r];
+        double* sc = a.sc + (size_t)p * 8;
+        sc[0] = a.minv_dc;
+        sc[1] = xi2;
+        sc[2] = pc.tx;
+        sc[3] = pc.ty;
+        sc[4] = (par[2] > 998.99 && par[2] < 999.01) ? 0. : par[2];
+        sc[5] = (par[3] > 998.99 && par[3] < 999.01) ? 0. : par[3];
+        sc[6] = par[11];
+        sc[7] = 0.;
+    }
+}
+
 // ------------------------------------------------------------ host side
+
+// compile-time sizes of the fused kernels (other sizes run the same kernels with the runtime plan)
+#define T2B_PREP_SIZES(X) X(64) X(72) X(80) X(96) X(100) X(120) X(128)
+
+using PrepKernel = void (*)(PrepArgs);
+PrepKernel fused_kernel(int N, bool noise)
+{
+#define T2B_CASE(n) \
+    if (N == n) return noise ? (PrepKernel)k_noise_fused<n> : (PrepKernel)k_prep_fused<n>;
+    T2B_PREP_SIZES(T2B_CASE)
+#undef T2B_CASE
+    return noise ? (PrepKernel)k_noise_fused<0> : (PrepKernel)k_prep_fused<0>;
+}
+
 double host_round(double x) { return x > 0 ? (double)(int)(x + 0.5) : (double)(int)(x - 0.5); }
 
 FftPlan make_plan(int N)
@@ -609,6 +971,15 @@ PrepArgs make_args(const ImagePrep& G, int n, const float* img, const double* pa
 int enqueue_prep(const ImagePrep& G, const PrepArgs& a, int n, cudaStream_t st)
 {
     int launches = 0;
+    if (G.fused) {
+        if (!G.cfg.zero_mask) {
+            fused_kernel(G.N, true)<<<n, FUSED_THREADS, fused_noise_smem(G.N), st>>>(a);
+            ++launches;
+        }
+        fused_kernel(G.N, false)<<<n, FUSED_THREADS, fused_prep_smem(G.N), st>>>(a);
+        T2B_CUDA(cudaGetLastError());
+        return launches + 1;
+    }
     const dim3 grow(n, (G.N + G.rpb - 1) / G.rpb), gcol(n, G.ncol_blocks);
     if (!G.cfg.zero_mask) {
         k_noise_cols<<<gcol, PREP_THREADS, smem_noise_cols(G), st>>>(a);
@@ -719,29 +1090,42 @@ int t2b_prep_configure(t2b_ctx* c, const t2b_prep_config* cf)
             }
             off[h] = (int)pix.size();
             const size_t B = cf->max_batch, NH = (size_t)N * h;
+            int optin = 0;
+            T2B_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+            // static shared memory of k_prep_fused: the two FP64 reduction arrays
+            // (the fused kernel stages the ring lists in its row scratch: 2 FQ N float2)
+            G->fused = fused_prep_smem(N) + 2 * FUSED_THREADS * sizeof(double) <= (size_t)optin &&
+                       pix.size() <= (size_t)4 * FQ * N;
             G->tw = dalloc<float2>(*G, N);
             G->noise_sig = dalloc<double>(*G, h);
             G->minv = dalloc<float>(*G, G->P);
             G->ring_off = dalloc<int>(*G, h + 1);
             G->ring_pix = dalloc<int>(*G, pix.size());
-            G->gm = dalloc<float2>(*G, B * NH);
-            G->gu = dalloc<float2>(*G, B * NH);
-            G->pw = dalloc<float>(*G, B * NH);
             G->bg = dalloc<double>(*G, B);
-            if (!cf->zero_mask) {
-                G->gn = dalloc<float2>(*G, B * NH);
-                G->noise = dalloc<float>(*G, B * (size_t)N * N);
+            if (!G->fused) {
+                G->gm = dalloc<float2>(*G, B * NH);
+                G->gu = dalloc<float2>(*G, B * NH);
+                G->pw = dalloc<float>(*G, B * NH);
+                if (!cf->zero_mask) G->gn = dalloc<float2>(*G, B * NH);
             }
+            if (!cf->zero_mask) G->noise = dalloc<float>(*G, B * (size_t)N * N);
             T2B_CUDA(cudaMemcpy(G->tw, tw.data(), N * sizeof(float2), cudaMemcpyHostToDevice));
             T2B_CUDA(cudaMemcpy(G->noise_sig, nsig.data(), h * sizeof(double), cudaMemcpyHostToDevice));
             T2B_CUDA(cudaMemcpy(G->minv, minv.data(), G->P * sizeof(float), cudaMemcpyHostToDevice));
             T2B_CUDA(cudaMemcpy(G->ring_off, off.data(), (h + 1) * sizeof(int), cudaMemcpyHostToDevice));
             if (!pix.empty())
                 T2B_CUDA(cudaMemcpy(G->ring_pix, pix.data(), pix.size() * sizeof(int), cudaMemcpyHostToDevice));
-            const int big = (int)std::max(smem_rows(*G), std::max(smem_cols(*G), smem_noise_cols(*G)));
-            for (const void* k : {(const void*)k_rows, (const void*)k_cols, (const void*)k_noise_cols,
-                                  (const void*)k_noise_rows})
-                T2B_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+            if (G->fused) {
+                T2B_CUDA(cudaFuncSetAttribute((const void*)fused_kernel(N, false),
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_prep_smem(N)));
+                T2B_CUDA(cudaFuncSetAttribute((const void*)fused_kernel(N, true),
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_noise_smem(N)));
+            } else {
+                const int big = (int)std::max(smem_rows(*G), std::max(smem_cols(*G), smem_noise_cols(*G)));
+                for (const void* k : {(const void*)k_rows, (const void*)k_cols, (const void*)k_noise_cols,
+                                      (const void*)k_noise_rows})
+                    T2B_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+            }
         } catch (...) {
             free_prep(G);
             throw;

@@ -31,6 +31,9 @@ CASES = {
     "n60_s32_flip_noctf_edge": (60, 32, dict(zero_mask=1, mask_radius=20.0, only_flip_phases=1,
                                              width_mask_edge=3.0)),
     "n64_s64_noctf": (64, 64, dict(zero_mask=0, mask_radius=24.0, do_ctf_correction=0, random_seed=-3)),
+    # boxes whose two half spectra exceed shared memory take the two-pass kernels
+    "n192_s120_noise_twopass": (192, 120, dict(zero_mask=0, mask_radius=80.0)),
+    "n160_s96_zeromask_twopass": (160, 96, dict(zero_mask=1, mask_radius=60.0)),
 }
 
 
