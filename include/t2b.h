@@ -196,6 +196,31 @@ int t2b_project(t2b_ctx* ctx, int iclass, const double* eulers, int n, int curre
 int t2b_debug_coarse_diff2(t2b_ctx* ctx, int b, float* out);
 int t2b_debug_fine(t2b_ctx* ctx, int b, long long* pairs, float* diff2, long long cap, long long* count);
 
+/* Tile-shape autotuner (no counterpart in the reference; the reference's
+ * kernels have fixed tile shapes).  Times candidate shapes on the caller's
+ * batch (host buffers, as t2b_estep_batch_host) with CUDA events and keeps the
+ * fastest of each for later batches and configurations:
+ *   contraction tile of the dense coarse pass: N = 256 or 128 columns x raster
+ *     groups of 4, 8, 16, 32 orientation tiles (diff2_ms[i]: N = 256 for i < 4);
+ *   fine pass and weighted sums + backprojection: 1..4 persistent CTAs per SM;
+ *   projection tile: 128, 256, 512 pixels x 1, 2, 4 orientations per CTA
+ *     (project_ms[3 * ipx + ior]), on up to 16384 table rows.
+ * None of the shapes changes a value the E-step computes (the backprojection's
+ * FP32 atomics aside, whose order is never fixed).  The grids are restored
+ * after the tuning batches; the learned proposals and their audit stream are
+ * not used.  A few seconds at the box-128 workload.  t2b_tune_set installs
+ * shapes directly (e.g. from an earlier run). */
+typedef struct t2b_tune_report {
+    int diff2_tn, diff2_group;              /* chosen shapes                                */
+    int fine_ctas_per_sm, wsum_ctas_per_sm;
+    int project_pixels, project_orients;
+    float diff2_ms[8];                      /* coarse contraction per candidate (-1: n/a)   */
+    float fine_ms[4], wsum_ms[4];           /* per CTAs-per-SM 1..4 (-1: no fine pass)      */
+    float project_ms[9];
+} t2b_tune_report;
+int t2b_autotune(t2b_ctx* ctx, const t2b_batch* batch, t2b_tune_report* report);
+int t2b_tune_set(t2b_ctx* ctx, const t2b_tune_report* shapes);
+
 /* Kernel launches of the last batch (the kernel nodes of its CUDA graph);
  * -1 when the last batch did not run as a graph.  With use_graph set, both
  * entry points replay a graph captured once per batch shape. */

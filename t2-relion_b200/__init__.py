@@ -39,7 +39,7 @@ ABI_SYMBOLS = (
     "t2b_sampling", "t2b_reconstruct_divide_noalloc", "t2b_last_launch_count",
     "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
-    "t2b_prep_configure", "t2b_prep_batch_host", "t2b_prep_batch_device",
+    "t2b_prep_configure", "t2b_prep_batch_host", "t2b_prep_batch_device", "t2b_autotune", "t2b_tune_set",
 )
 
 
@@ -126,6 +126,13 @@ class PrepOut(ctypes.Structure):
     _fields_ = [(n, _p) for n in ("fimg", "fimg_nomask", "ctf", "minvsigma2", "scalars", "power")]
 
 
+class TuneReport(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("diff2_tn", "diff2_group", "fine_ctas_per_sm", "wsum_ctas_per_sm",
+                                            "project_pixels", "project_orients")] + [
+        ("diff2_ms", ctypes.c_float * 8), ("fine_ms", ctypes.c_float * 4), ("wsum_ms", ctypes.c_float * 4),
+        ("project_ms", ctypes.c_float * 9)]
+
+
 PREP_NPARAM = 12
 PREP_DEFAULTS = dict(zero_mask=0, random_seed=0, do_norm_correction=0, do_ctf_correction=1, ctf_premultiplied=0,
                      ctf_phase_flipped=0, only_flip_phases=0, intact_ctf_first_peak=0, avg_norm_correction=1.0,
@@ -165,6 +172,8 @@ def _setup_prototypes():
     lib.t2b_proposal_logits.argtypes = [v, v, i, v]
     lib.t2b_proposal_grad.argtypes = [v, v, v, v, i, ctypes.POINTER(ctypes.c_double), v]
     lib.t2b_prep_configure.argtypes = [v, ctypes.POINTER(PrepConfig)]
+    lib.t2b_autotune.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(TuneReport)]
+    lib.t2b_tune_set.argtypes = [v, ctypes.POINTER(TuneReport)]
     lib.t2b_prep_batch_host.argtypes = [v, ctypes.POINTER(PrepBatch), ctypes.POINTER(PrepOut)]
     lib.t2b_prep_batch_device.argtypes = [v, ctypes.POINTER(PrepBatch), ctypes.POINTER(PrepOut), v]
 
@@ -348,6 +357,27 @@ class EStep:
         r = Result(*[result_ptrs.get(name) for name, _ in Result._fields_])
         _check(lib.t2b_estep_batch_device(self._h, ctypes.byref(b), ctypes.byref(r),
                                           ctypes.c_void_p(stream)))
+
+    # ---------------------------------------------- tile-shape autotuner
+    def autotune(self, fimg, ctf, minvsigma2, scalars, fimg_nomask=None):
+        """t2b_autotune on a host batch; returns the report as a dict (shapes and timings)."""
+        fimg = np.ascontiguousarray(fimg, np.complex64)
+        arrs = [np.ascontiguousarray(ctf, np.float32), np.ascontiguousarray(minvsigma2, np.float32),
+                np.ascontiguousarray(scalars, np.float64)]
+        fnm = None if fimg_nomask is None else np.ascontiguousarray(fimg_nomask, np.complex64)
+        b = Batch(fimg.shape[0], 0, _ptr(fimg), _ptr(fnm), _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]))
+        rep = TuneReport()
+        _check(lib.t2b_autotune(self._h, ctypes.byref(b), ctypes.byref(rep)))
+        return {k: (list(getattr(rep, k)) if isinstance(getattr(rep, k), ctypes.Array) else getattr(rep, k))
+                for k, _ in TuneReport._fields_}
+
+    def tune_set(self, diff2_tn=256, diff2_group=16, fine_ctas_per_sm=4, wsum_ctas_per_sm=4, project_pixels=256,
+                 project_orients=1):
+        """t2b_tune_set: install tile shapes (the defaults are the untuned ones)."""
+        rep = TuneReport(diff2_tn=diff2_tn, diff2_group=diff2_group, fine_ctas_per_sm=fine_ctas_per_sm,
+                         wsum_ctas_per_sm=wsum_ctas_per_sm, project_pixels=project_pixels,
+                         project_orients=project_orients)
+        _check(lib.t2b_tune_set(self._h, ctypes.byref(rep)))
 
     # ---------------------------------------------- image preparation
     def configure_prep(self, *, image_size, current_size, max_batch, sigma2_noise, pixel_size, mask_radius, **kw):

@@ -319,13 +319,15 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         for (int k = 0; k < K; k++) {
             const Volume& v = c->mvol[k];
             T2B_REQUIRE(v.r_max * v.pad + 1 < v.xdim, T2B_ERR_ARG, "projector too small");
-            launch_project_table(v, c->mdl[k], tb.eul_c, O, s, pc + (size_t)k * O * P, st);
+            launch_project_table(v, c->mdl[k], tb.eul_c, O, s, pc + (size_t)k * O * P, st, c->tune.proj_px,
+                                 c->tune.proj_orients);
         }
         tb.proj_c = pc;
         if (tb.ovs) {
             float2* pf = dalloc<float2>(c, (size_t)KO * R * P);
             for (int k = 0; k < K; k++)
-                launch_project_table(c->mvol[k], c->mdl[k], tb.eul_f, O * R, s, pf + (size_t)k * O * R * P, st);
+                launch_project_table(c->mvol[k], c->mdl[k], tb.eul_f, O * R, s, pf + (size_t)k * O * R * P, st,
+                                     c->tune.proj_px, c->tune.proj_orients);
             tb.proj_f = pf;
         } else {
             tb.proj_f = pc;
@@ -343,6 +345,8 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         // workspace
         Work& w = c->wk;
         w = Work{};
+        w.fine_ctas = c->tune.fine_ctas;
+        w.wsum_ctas = c->tune.wsum_ctas;
         const long long KOT = KO * T;
         w.cvec = dalloc<float2>(c, (size_t)B * P);
         w.w2 = dalloc<float>(c, (size_t)B * P);
@@ -403,6 +407,8 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         c->gd_table = gd;
         c->gw_table = gw;
         c->tc = TcOperands{};
+        c->tc.dense_tn = c->tune.dense_tn;
+        c->tc.group_m = c->tune.group_m;
         if (f.diff2_mode == T2B_DIFF2_SPLIT_BF16) {
             TcOperands& op = c->tc;
             op.kdim = (int)tc_kdim(tb.nk);
@@ -647,6 +653,168 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
     });
 }
 
+int t2b_autotune(t2b_ctx* c, const t2b_batch* b, t2b_tune_report* rep)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && b && rep, T2B_ERR_ARG, "null argument");
+        T2B_REQUIRE(c->configured, T2B_ERR_STATE, "t2b_configure must be called before t2b_autotune");
+        T2B_REQUIRE(b->n >= 1 && b->n <= c->cfg.max_batch, T2B_ERR_ARG, "batch size out of range");
+        T2B_REQUIRE(b->fimg && b->ctf && b->minvsigma2 && b->scalars, T2B_ERR_ARG, "missing batch inputs");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        cudaStream_t st = c->stream;
+        Work w = c->wk;
+        const int n = b->n, P = c->tb.P, K = c->tb.K;
+        w.n = n;
+        T2B_CUDA(cudaMemcpyAsync((void*)w.fimg, b->fimg, (size_t)n * P * sizeof(float2), cudaMemcpyHostToDevice, st));
+        if (b->fimg_nomask)
+            T2B_CUDA(cudaMemcpyAsync((void*)w.fimg_nm, b->fimg_nomask, (size_t)n * P * sizeof(float2),
+                                     cudaMemcpyHostToDevice, st));
+        else
+            w.fimg_nm = w.fimg;
+        T2B_CUDA(cudaMemcpyAsync((void*)w.ctf, b->ctf, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
+        T2B_CUDA(cudaMemcpyAsync((void*)w.minv, b->minvsigma2, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
+        T2B_CUDA(cudaMemcpyAsync((void*)w.scal, b->scalars, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, st));
+        // the tuning batches backproject like real ones: keep the grids and put them back after
+        std::vector<void*> saved;
+        struct Restore {
+            t2b_ctx* c;
+            std::vector<void*>& saved;
+            ~Restore()
+            {
+                for (size_t k = 0; k < saved.size() / 2; k++) {
+                    const size_t nv = (size_t)c->gvol[k].xdim * c->gvol[k].ydim * c->gvol[k].zdim;
+                    if (saved[2 * k]) cudaMemcpy(c->gdata[k], saved[2 * k], nv * sizeof(float2), cudaMemcpyDeviceToDevice);
+                    if (saved[2 * k + 1])
+                        cudaMemcpy(c->gweight[k], saved[2 * k + 1], nv * sizeof(float), cudaMemcpyDeviceToDevice);
+                    cudaFree(saved[2 * k]);
+                    cudaFree(saved[2 * k + 1]);
+                }
+            }
+        } restore{c, saved};
+        T2B_CUDA(cudaStreamSynchronize(st));
+        for (int k = 0; k < K; k++) {
+            const size_t nv = (size_t)c->gvol[k].xdim * c->gvol[k].ydim * c->gvol[k].zdim;
+            void *d = nullptr, *wt = nullptr;
+            saved.push_back(nullptr);
+            saved.push_back(nullptr);
+            T2B_CUDA(cudaMalloc(&d, nv * sizeof(float2)));
+            saved[2 * k] = d;
+            T2B_CUDA(cudaMalloc(&wt, nv * sizeof(float)));
+            saved[2 * k + 1] = wt;
+            T2B_CUDA(cudaMemcpy(d, c->gdata[k], nv * sizeof(float2), cudaMemcpyDeviceToDevice));
+            T2B_CUDA(cudaMemcpy(wt, c->gweight[k], nv * sizeof(float), cudaMemcpyDeviceToDevice));
+        }
+        // one E-step of the batch with stage events; the faster of two runs (the first also warms)
+        auto run = [&](int stage, int stage2) {
+            float best = 1e30f;
+            for (int rep_i = 0; rep_i < 2; rep_i++) {
+                Work wr = w;
+                wr.fine_ctas = c->wk.fine_ctas;
+                wr.wsum_ctas = c->wk.wsum_ctas;
+                enqueue_estep(c, wr, st, true, false);   // full coarse pass; the audit stream is not advanced
+                T2B_CUDA(cudaStreamSynchronize(st));
+                c->last_kernels = -1;
+                collect_stage_ms(c);
+                float t = c->stage_ms[stage];
+                if (stage2 >= 0 && c->stage_ms[stage2] > 0.f) t += c->stage_ms[stage2];
+                best = std::min(best, t);
+            }
+            return best;
+        };
+        *rep = t2b_tune_report{};
+        // 1. contraction tile: N columns x raster group, timed on the full coarse pass (the
+        // audit's full pass of the learned mode runs the same dense tiles with the same group)
+        const bool tc = c->cfg.diff2_mode == T2B_DIFF2_SPLIT_BF16;
+        const int tns[2] = {256, 128}, groups[4] = {4, 8, 16, 32};
+        int best_i = -1;
+        for (int i = 0; i < 8; i++) {
+            if (!tc) { rep->diff2_ms[i] = -1.f; continue; }
+            c->tc.dense_tn = tns[i / 4];
+            c->tc.group_m = groups[i % 4];
+            rep->diff2_ms[i] = run(2, -1);
+            if (best_i < 0 || rep->diff2_ms[i] < rep->diff2_ms[best_i]) best_i = i;
+        }
+        if (tc) {
+            c->tune.dense_tn = c->tc.dense_tn = tns[best_i / 4];
+            c->tune.group_m = c->tc.group_m = groups[best_i % 4];
+        }
+        // 2. fine pass and 3. weighted sums + backprojection: CTAs per SM of the persistent kernels
+        int bf = 0, bw = 0;
+        for (int k = 1; k <= 4; k++) {
+            c->wk.fine_ctas = k;
+            rep->fine_ms[k - 1] = c->tb.ovs ? run(4, -1) : -1.f;
+            if (c->tb.ovs && (bf == 0 || rep->fine_ms[k - 1] < rep->fine_ms[bf - 1])) bf = k;
+        }
+        c->tune.fine_ctas = c->wk.fine_ctas = bf ? bf : 4;
+        for (int k = 1; k <= 4; k++) {
+            c->wk.wsum_ctas = k;
+            rep->wsum_ms[k - 1] = run(6, -1);
+            if (bw == 0 || rep->wsum_ms[k - 1] < rep->wsum_ms[bw - 1]) bw = k;
+        }
+        c->tune.wsum_ctas = c->wk.wsum_ctas = bw;
+        // 4. projection tile: pixels x orientations per CTA, on the first (up to 16384) rows of
+        // the fine (else coarse) table of class 0, rewritten with identical values
+        {
+            const int rows = std::min(16384, c->tb.ovs ? c->tb.O * c->tb.R : c->tb.O);
+            float2* out = const_cast<float2*>(c->tb.ovs ? c->tb.proj_f : c->tb.proj_c);
+            const double* eul = c->tb.ovs ? c->tb.eul_f : c->tb.eul_c;
+            const int pxs[3] = {128, 256, 512}, ors[3] = {1, 2, 4};
+            cudaEvent_t e0, e1;
+            T2B_CUDA(cudaEventCreate(&e0));
+            T2B_CUDA(cudaEventCreate(&e1));
+            int bp = -1;
+            for (int i = 0; i < 9; i++) {
+                float best = 1e30f;
+                for (int r = 0; r < 2; r++) {
+                    T2B_CUDA(cudaEventRecord(e0, st));
+                    launch_project_table(c->mvol[0], c->mdl[0], eul, rows, c->tb.s, out, st, pxs[i / 3], ors[i % 3]);
+                    T2B_CUDA(cudaEventRecord(e1, st));
+                    T2B_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    T2B_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    best = std::min(best, ms);
+                }
+                rep->project_ms[i] = best;
+                if (bp < 0 || best < rep->project_ms[bp]) bp = i;
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            c->tune.proj_px = pxs[bp / 3];
+            c->tune.proj_orients = ors[bp % 3];
+        }
+        rep->diff2_tn = c->tune.dense_tn;
+        rep->diff2_group = c->tune.group_m;
+        rep->fine_ctas_per_sm = c->tune.fine_ctas;
+        rep->wsum_ctas_per_sm = c->tune.wsum_ctas;
+        rep->project_pixels = c->tune.proj_px;
+        rep->project_orients = c->tune.proj_orients;
+        c->drop_graphs();   // the next batch captures with the chosen shapes
+    });
+}
+
+int t2b_tune_set(t2b_ctx* c, const t2b_tune_report* shapes)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && shapes, T2B_ERR_ARG, "null argument");
+        T2B_REQUIRE((shapes->diff2_tn == 256 || shapes->diff2_tn == 128) && shapes->diff2_group >= 1 &&
+                        shapes->fine_ctas_per_sm >= 1 && shapes->fine_ctas_per_sm <= 4 &&
+                        shapes->wsum_ctas_per_sm >= 1 && shapes->wsum_ctas_per_sm <= 4 &&
+                        shapes->project_pixels >= 32 && shapes->project_pixels <= 1024 &&
+                        shapes->project_pixels % 32 == 0 && shapes->project_orients >= 1 &&
+                        shapes->project_orients <= 64,
+                    T2B_ERR_ARG, "tile shapes out of range");
+        std::lock_guard<std::mutex> lk(c->mu);
+        c->tune.dense_tn = c->tc.dense_tn = shapes->diff2_tn;
+        c->tune.group_m = c->tc.group_m = shapes->diff2_group;
+        c->tune.fine_ctas = c->wk.fine_ctas = shapes->fine_ctas_per_sm;
+        c->tune.wsum_ctas = c->wk.wsum_ctas = shapes->wsum_ctas_per_sm;
+        c->tune.proj_px = shapes->project_pixels;
+        c->tune.proj_orients = shapes->project_orients;
+        c->drop_graphs();
+    });
+}
+
 int t2b_stage_timing(t2b_ctx* c, int on)
 {
     return guarded([&] {
@@ -760,7 +928,8 @@ int t2b_project(t2b_ctx* c, int iclass, const double* eulers, int n, int current
         }
         try {
             T2B_CUDA(cudaMemcpyAsync(de, eulers, (size_t)n * 9 * sizeof(double), cudaMemcpyHostToDevice, st));
-            launch_project_table(c->mvol[iclass], c->mdl[iclass], de, n, current_size, dout, st);
+            launch_project_table(c->mvol[iclass], c->mdl[iclass], de, n, current_size, dout, st, c->tune.proj_px,
+                                 c->tune.proj_orients);
             T2B_CUDA(cudaMemcpyAsync(out, dout, (size_t)n * P * sizeof(float2), cudaMemcpyDeviceToHost, st));
             T2B_CUDA(cudaStreamSynchronize(st));
         } catch (...) {

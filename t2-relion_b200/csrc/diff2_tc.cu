@@ -146,15 +146,15 @@ __device__ __forceinline__ unsigned f2key(float f)
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-// Tile order: groups of GROUP_M orientation tiles, the batch columns inside a
-// group, so the 148 tiles that run together share few operand strips.
-constexpr int GROUP_M = 16;
-__device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, int& mt, int& nt)
+// Tile order: groups of `group` orientation tiles, the batch columns inside a
+// group, so the 148 tiles that run together share few operand strips (the group
+// size is chosen by t2b_autotune; 16 by default).
+__device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, int group, int& mt, int& nt)
 {
-    const int per_group = GROUP_M * n_tiles;
+    const int per_group = group * n_tiles;
     const int g = tile / per_group;
-    const int first = g * GROUP_M;
-    const int gm = min(GROUP_M, m_tiles - first);
+    const int first = g * group;
+    const int gm = min(group, m_tiles - first);
     const int r = tile - g * per_group;
     mt = first + r % gm;
     nt = r / gm;
@@ -162,6 +162,7 @@ __device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, 
 
 struct TcParams {
     int m_tiles, n_tiles, kblocks;
+    int group;                // dense tiles: orientation tiles per raster group (0: 16)
     int raw;                  // 1: store the contraction itself (norm and network GEMMs), 0: diff2 epilogue
     int KO, T, ncols;
     const float* c0;
@@ -251,9 +252,9 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             int ya, yb;
             if (p.mode == 0) {
                 int mt, nt;
-                tile_coords(tile, p.m_tiles, p.n_tiles, mt, nt);
+                tile_coords(tile, p.m_tiles, p.n_tiles, p.group ? p.group : 16, mt, nt);
                 ya = mt * TM;
-                yb = nt * TN;
+                yb = nt * tn_l;
             } else {
                 ya = (p.mtp > 1) ? tile * TM : tile * p.ppt * p.kslot;
                 yb = (tile / (p.mtp ? p.mtp : 1)) * p.ppt * p.T;
@@ -322,12 +323,12 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         int tl = 0;
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x, tl++) {
             int mt = 0, nt = 0;
-            if (p.mode == 0) tile_coords(tile, p.m_tiles, p.n_tiles, mt, nt);
+            if (p.mode == 0) tile_coords(tile, p.m_tiles, p.n_tiles, p.group ? p.group : 16, mt, nt);
             const int abuf = tl & 1;
             const uint32_t aph = (uint32_t)(tl >> 1) & 1u;
             if (!mbar_wait(&tfull_bar[abuf], aph, &abort_flag)) { abort_flag = 1; break; }
             tc_fence_after();
-            const int n0 = nt * TN;
+            const int n0 = nt * tn_l;
             const int mtp = p.mtp ? p.mtp : 1;
             const int bfirst = p.mode == 0 ? n0 / p.T : (tile / mtp) * p.ppt;
             const int jbase = p.mode == 0 ? 0 : (tile % mtp) * TM;
@@ -588,7 +589,8 @@ size_t tc_kn(int nk) { return (size_t)((nk + TK - 1) / TK) * TK; }
 
 // descriptor slots in op.maps (TC_MAP_SLOTS of 128 bytes)
 enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL,
-       MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_IH96, MAP_IL96, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL, MAP_COUNT };
+       MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_IH96, MAP_IL96, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL,
+       MAP_IH128, MAP_IL128, MAP_COUNT };
 static_assert(MAP_COUNT <= TC_MAP_SLOTS, "tensor-map slots");
 static_assert(sizeof(CUtensorMap) == 128, "tensor-map size");
 
@@ -615,6 +617,10 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
     // the image operand with a 96-row box: one particle's translations per tile (proposal pass)
     CUtensorMap h96[2] = {make_map(op.ah, op.n_pad, op.kdim, 96), make_map(op.al, op.n_pad, op.kdim, 96)};
     T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * MAP_IH96, h96, sizeof(h96), cudaMemcpyHostToDevice));
+    // and with a 128-row box: dense coarse tiles of 128 columns (t2b_autotune)
+    CUtensorMap h128[2] = {make_map(op.ah, op.n_pad, op.kdim, 128), make_map(op.al, op.n_pad, op.kdim, 128)};
+    T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * MAP_IH128, h128, sizeof(h128),
+                        cudaMemcpyHostToDevice));
     const int rows = tb.K * tb.O;
     // sizes were fixed when the operand buffers were allocated
     T2B_REQUIRE(op.m_pad == (rows + TM - 1) / TM * TM && op.kdim == (int)tc_kdim(tb.nk), T2B_ERR_STATE,
@@ -685,10 +691,13 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     const int ncols = w.n * tb.T;
     const int n_pad = (ncols + TN - 1) / TN * TN;
     T2B_REQUIRE(n_pad <= op.n_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
+    T2B_REQUIRE(op.dense_tn == 256 || op.dense_tn == 128, T2B_ERR_ARG, "dense tile width");
     TcParams p{};
     p.raw = 0;
     p.m_tiles = op.m_pad / TM;
-    p.n_tiles = n_pad / TN;
+    p.n_tiles = (ncols + op.dense_tn - 1) / op.dense_tn;
+    p.tn = op.dense_tn == TN ? 0 : op.dense_tn;
+    p.group = op.group_m;
     p.kblocks = op.kdim / TK;
     p.KO = tb.K * tb.O;
     p.T = tb.T;
@@ -702,7 +711,7 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     p.products = 3;
     p.gate = gate;
     p.gate_run = gate_run;
-    launch_gemm(op, MAP_PH, MAP_IH, p, st);
+    launch_gemm(op, MAP_PH, op.dense_tn == TN ? MAP_IH : MAP_IH128, p, st);
 }
 
 void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_side)
@@ -809,6 +818,7 @@ void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* 
     p.minkey = minkeya;
     p.err = err;
     p.products = 3;
+    p.group = op.group_m;
     launch_gemm(op, MAP_PH, MAP_IAH, p, st);
 }
 

@@ -1585,7 +1585,7 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
 
 void launch_fine(const Tables& tb, const Work& w, cudaStream_t st)
 {
-    k_fine<<<4 * sm_count(), 256, 0, st>>>(tb, w);   // <= 64 registers: 4 CTAs per SM
+    k_fine<<<(w.fine_ctas > 0 ? w.fine_ctas : 4) * sm_count(), 256, 0, st>>>(tb, w);   // <= 64 registers: <= 4 CTAs per SM
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -1604,7 +1604,7 @@ void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* co
 {
     GridPtrs gp{grid_data, grid_weight};
     k_group_starts<<<2 * sm_count(), 256, 0, st>>>(tb, w);
-    k_wsum_bp<<<4 * sm_count(), 256, 0, st>>>(tb, w, g, gp);   // 64 registers: 4 CTAs per SM
+    k_wsum_bp<<<(w.wsum_ctas > 0 ? w.wsum_ctas : 4) * sm_count(), 256, 0, st>>>(tb, w, g, gp);   // 64 registers: <= 4 CTAs per SM
     k_results<<<(w.n + 127) / 128, 128, 0, st>>>(tb, w);
     T2B_CUDA(cudaGetLastError());
 }

@@ -18,21 +18,22 @@
 namespace t2b {
 namespace {
 
-// one table row per orientation (blockIdx.y), one window pixel per thread
+// projection tile: blockDim.x window pixels x `orients` orientations per CTA (rows
+// blockIdx.y * orients ...), one pixel per thread; the tile shape is chosen by
+// t2b_autotune and does not change any value
 __global__ void k_project(const float2* __restrict__ mdl, Volume v, const double* __restrict__ eul,
-                          int s, float2* __restrict__ out)
+                          int s, int n, int orients, float2* __restrict__ out)
 {
     const int xh = s / 2 + 1, P = s * xh;
-    const int o = blockIdx.y;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= P) return;
-    const int i = n / xh, x = n - i * xh;
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    if (px >= P) return;
+    const int i = px / xh, x = px - i * xh;
     const int y = (i < xh) ? i : i - s;
     const int rmo = s / 2;
-    float2 res = make_float2(0.f, 0.f);
-    if (x * x + y * y <= rmo * rmo && x * x + y * y <= v.r_max * v.r_max)
-        res = project_pixel(mdl, v, eul + 9 * (size_t)o, x, y);
-    out[(size_t)o * P + n] = res;
+    const bool inside = x * x + y * y <= rmo * rmo && x * x + y * y <= v.r_max * v.r_max;
+    const int o0 = blockIdx.y * orients, o1 = min(n, o0 + orients);
+    for (int o = o0; o < o1; ++o)
+        out[(size_t)o * P + px] = inside ? project_pixel(mdl, v, eul + 9 * (size_t)o, x, y) : make_float2(0.f, 0.f);
 }
 
 // e^{-2 pi i (kx sx + ky sy)/N} for every pixel of the window
@@ -56,13 +57,16 @@ __global__ void k_phase(const double* __restrict__ shifts, int s, int ori, float
 }  // namespace
 
 void launch_project_table(const Volume& v, const float2* mdl, const double* eul9, int n, int s,
-                          float2* out, cudaStream_t st)
+                          float2* out, cudaStream_t st, int px, int orients)
 {
     const int P = s * (s / 2 + 1);
-    for (int o0 = 0; o0 < n; o0 += 65535) {
-        const int cnt = std::min(65535, n - o0);
-        dim3 grid((P + 255) / 256, cnt);
-        k_project<<<grid, 256, 0, st>>>(mdl, v, eul9 + 9 * (size_t)o0, s, out + (size_t)o0 * P);
+    T2B_REQUIRE(px >= 32 && px <= 1024 && px % 32 == 0 && orients >= 1 && orients <= 64, T2B_ERR_ARG,
+                "projection tile shape");
+    const int per_launch = 65535 * orients;
+    for (int o0 = 0; o0 < n; o0 += per_launch) {
+        const int cnt = std::min(per_launch, n - o0);
+        dim3 grid((P + px - 1) / px, (cnt + orients - 1) / orients);
+        k_project<<<grid, px, 0, st>>>(mdl, v, eul9 + 9 * (size_t)o0, s, cnt, orients, out + (size_t)o0 * P);
     }
     T2B_CUDA(cudaGetLastError());
 }

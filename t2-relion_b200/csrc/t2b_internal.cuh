@@ -163,6 +163,7 @@ struct Work {
     const int* prop;          // n x kprop: global orientation of each proposal (ranked)
     int kprop;
     int no_bp;                // 1: weighted sums only, the grids are not touched
+    int fine_ctas, wsum_ctas; // CTAs per SM of the fine pass and of the weighted sums (0: 4; t2b_autotune)
     int* r_learned;           // n (optional): 1 if the particle's coarse pass used the proposals
     double* r_audit;          // n (optional): posterior mass in the proposals (audited), else -1
     // results (device)
@@ -175,7 +176,7 @@ struct Work {
 // ------------------------------------------------------------- kernels
 // projection tables (project.cu)
 void launch_project_table(const Volume& v, const float2* mdl, const double* eul9, int n, int s,
-                          float2* out, cudaStream_t st);
+                          float2* out, cudaStream_t st, int px = 256, int orients = 1);
 void launch_phase_table(const double* shifts, int n, int s, int ori_size, float2* out, cudaStream_t st);
 
 // E-step stages (estep.cu)
@@ -205,6 +206,8 @@ struct TcOperands {
     int m_pad, n_pad, kdim;   // padded sizes of the cross-term operands
     int kn, b_pad;            // padded sizes of the norm operands
     void* maps;               // TC_MAP_SLOTS CUtensorMap descriptors (128 B each) in device memory
+    int dense_tn = 256;       // N columns of a dense coarse-pass tile (256 or 128; t2b_autotune)
+    int group_m = 16;         // orientation tiles per raster group of the dense and audit tiles
 };
 constexpr int TC_MAP_SLOTS = 24;
 size_t tc_kdim(int nk);
@@ -283,4 +286,9 @@ struct t2b_ctx {
     bool prop_events = false;                 // the last timed batch recorded ev[8..11]
     t2b::ProposalNet* net = nullptr;          // learned orientation proposals (proposal.cu)
     t2b::ImagePrep* prep = nullptr;           // image preparation state (imageprep.cu)
+    struct Tune {                             // tile and launch shapes (t2b_autotune); kept across t2b_configure
+        int dense_tn = 256, group_m = 16;     // dense contraction tile: N columns, raster group
+        int fine_ctas = 4, wsum_ctas = 4;     // CTAs per SM: fine pass, weighted sums + backprojection
+        int proj_px = 256, proj_orients = 1;  // projection tile: pixels x orientations per CTA
+    } tune;
 };
