@@ -163,6 +163,49 @@ int t2b_estep_batch_device(t2b_ctx* ctx, const t2b_batch* batch, const t2b_resul
  * double, host memory. */
 int t2b_reconstruct_divide(t2b_ctx* ctx, int iclass, double* fconv);
 
+/* M-step reconstruction of a 3D grid on the device (BackProjector::reconstruct,
+ * src/backprojector.cpp:1344-1530, on the reference's default skip-gridding
+ * path, followed by windowToOridimRealSpace :2486-2620 and
+ * Projector::griddingCorrect, src/projector.cpp:489-522): decenter, optional
+ * MAP term 1 / (pad^3 tau2_fudge tau2[ires]) on the weights for shells >=
+ * minres_map, FP64 division by max(weight, radial average / 1000), window to
+ * pad * ori_size, inverse 3D FFT (FP32), real-space window to ori_size,
+ * normalisation for 2D particles (pad^3 ori_size), soft mask (radius ori/2,
+ * width 3, average background), sinc^2 gridding correction.  vol: host,
+ * ori_size^3 doubles [z][y][x], centre at ori_size/2.  pad * ori_size must be
+ * a product of 2, 3, 5 and <= 512.  The gridding iterations
+ * (--dont_skip_gridding) are not implemented. */
+typedef struct t2b_recon_config {
+    int ori_size;               /* model box                                       */
+    int do_map;                 /* add the inverse tau2 spectrum to the weights    */
+    int minres_map;             /* first shell that gets the MAP term              */
+    int _pad;
+    double tau2_fudge;
+    const double* tau2;         /* ori_size/2+1 (host); required with do_map       */
+} t2b_recon_config;
+int t2b_reconstruct(t2b_ctx* ctx, int iclass, const t2b_recon_config* cfg, double* vol);
+
+/* Fourier shell correlation of two grids (two half-sets) after down-sampling to
+ * the unpadded box (BackProjector::getDownsampledAverage +
+ * calculateDownSampledFourierShellCorrelation, src/backprojector.cpp:933-1040);
+ * fsc: host, ori_size/2+1 doubles, fsc[0] = 1. */
+int t2b_fsc_halves(t2b_ctx* ctx, int grid_a, int grid_b, int ori_size, double* fsc);
+
+/* BackProjector::updateSSNRarrays (src/backprojector.cpp:1041-1205) of a grid:
+ * tau2 (in/out), sigma2, data_vs_prior and fourier_coverage, ori_size/2+1
+ * doubles each (host). */
+typedef struct t2b_ssnr_config {
+    int ori_size;
+    int update_tau2_with_fsc;
+    int is_whole_instead_of_half;
+    int correct_tau2_by_avgctf2;
+    double tau2_fudge;
+    const double* fsc;          /* ori_size/2+1, with update_tau2_with_fsc         */
+    const double* avgctf2;      /* ori_size/2+1, with correct_tau2_by_avgctf2      */
+} t2b_ssnr_config;
+int t2b_update_ssnr(t2b_ctx* ctx, int iclass, const t2b_ssnr_config* cfg, double* tau2, double* sigma2,
+                    double* data_vs_prior, double* fourier_coverage);
+
 /* Maximum r_max of t2b_reconstruct_divide_noalloc. */
 #define T2B_NOALLOC_MAX_RMAX 2048
 

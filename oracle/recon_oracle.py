@@ -1,0 +1,215 @@
+"""FP64 oracle of the M-step reconstruction on the device (test infrastructure).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/ as the checker of
+t2-relion_b200/csrc/recon.cu.  The shipped library never uses it.
+
+Restates in numpy, on a centred half-complex backprojection grid (data
+complex, weight real; z, y centred at -initz, -inity; x from 0):
+
+  reconstruct_map   BackProjector::reconstruct (src/backprojector.cpp:1344-1530),
+                    the skip-gridding path (the reference's default:
+                    skip_gridding = !--dont_skip_gridding, src/ml_optimiser.cpp:525):
+                    Projector::decenter to the FFTW layout of the pad_size box
+                    (r^2 <= ROUND(r_max pad)^2), the MAP term
+                    1 / (pad^3 tau2_fudge tau2[ROUND(r / pad)]) added to the
+                    weight for r^2 < max_r2 and shells >= minres_map (:1412-1455),
+                    the division by max(weight, radial average / 1000) (:1463-1531);
+                    then windowToOridimRealSpace (:2486-2620): window the transform
+                    to pad * ori_size (src/fftw.h:736-790), CenterFFTbySign, unnormalised inverse FFT,
+                    real-space window to ori_size, divide by pad^3 ori_size (2D
+                    particles), softMaskOutsideMap (src/mask.cpp:43-96; radius
+                    ori_size / 2, cosine width 3, average background); and
+                    Projector::griddingCorrect (src/projector.cpp:489-522:
+                    divide by sinc^2 of r / (ori_size pad), trilinear)
+  downsampled_fsc   getDownsampledAverage + calculateDownSampledFourierShellCorrelation
+                    (src/backprojector.cpp:933-1040)
+  update_ssnr       BackProjector::updateSSNRarrays (src/backprojector.cpp:1041-1205)
+"""
+import numpy as np
+
+PI = 3.14159265358979323846
+
+
+def relion_round(x):
+    x = np.asarray(x, float)
+    return np.where(x > 0, np.floor(x + 0.5), -np.floor(-x + 0.5)).astype(np.int64)
+
+
+def _logical(shape, initz, inity):
+    zd, yd, xd = shape
+    k = np.arange(zd)[:, None, None] + initz
+    i = np.arange(yd)[None, :, None] + inity
+    j = np.arange(xd)[None, None, :]
+    return k, i, j
+
+
+def decenter_divide(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_map=0):
+    """Fconv of the pad_size box (FFTW layout [ps][ps][ps/2+1]) after the MAP term and the
+    skip-gridding division, FP64."""
+    zd, yd, xd = weight.shape
+    ps = yd
+    fx = ps // 2 + 1
+    initz, inity = -(zd // 2), -(yd // 2)
+    rp = int(relion_round(r_max * pad))
+    max_r2 = rp * rp
+    k = np.arange(ps)
+    kp = np.where(k < fx, k, k - ps)
+    KP, IP, JP = np.meshgrid(kp, kp, np.arange(fx), indexing="ij")
+    r2 = KP * KP + IP * IP + JP * JP
+    inside = r2 <= max_r2
+    zs, ys = KP - initz, IP - inity
+    F = np.zeros((ps, ps, fx), complex)
+    W = np.zeros((ps, ps, fx))
+    F[inside] = data[zs[inside], ys[inside], JP[inside]]
+    W[inside] = weight[zs[inside], ys[inside], JP[inside]]
+    oc = float(pad) ** 3
+    if tau2 is not None:
+        m = r2 < max_r2
+        ires = relion_round(np.sqrt(r2[m].astype(float)) / pad)
+        t = np.asarray(tau2, float)[ires]
+        invw = W[m]
+        invtau2 = np.where(t > 0, 1.0 / (oc * tau2_fudge * np.where(t > 0, t, 1.0)),
+                           np.where(invw > 1e-20, 1.0 / (0.001 * np.where(invw > 1e-20, invw, 1.0)), 0.0))
+        W[m] = np.where(ires >= minres_map, invw + invtau2, invw)
+    # radial averages below ROUND((r_max pad)^2)
+    rr2 = int(relion_round(r_max * pad * r_max * pad))
+    m = r2 < rr2
+    ires = np.floor(np.sqrt(r2[m].astype(float)) / pad).astype(int)
+    rad = np.bincount(ires, W[m], r_max)[:r_max]
+    cnt = np.bincount(ires, minlength=r_max)[:r_max]
+    rad = np.where((cnt > 0) | (rad > 0), rad / (1000. * np.maximum(cnt, 1)), rad)
+    iall = np.floor(np.sqrt(r2.astype(float)) / pad).astype(int)
+    wfin = np.maximum(W, rad[np.minimum(iall, r_max - 1)])
+    out = np.where(wfin != 0, F / np.where(wfin != 0, wfin, 1.0), F)
+    return out
+
+
+def soft_mask_bg(vol, radius, width):
+    n = vol.shape[0]
+    c = np.arange(n) - n // 2
+    r = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2)
+    rp = radius + width
+    rc = 0.5 + 0.5 * np.cos(PI * (rp - r) / width)
+    edge = (r >= radius) & (r <= rp)
+    out_ = r > rp
+    s = np.sum(out_) + np.sum(rc[edge])
+    bg = (np.sum(vol[out_]) + np.sum(rc[edge] * vol[edge])) / s if s > 0 else 0.0
+    res = vol.copy()
+    res[out_] = bg
+    res[edge] = (1 - rc[edge]) * vol[edge] + rc[edge] * bg
+    return res
+
+
+def reconstruct_map(data, weight, r_max, pad, ori_size, tau2=None, tau2_fudge=1.0, minres_map=0):
+    """Real-space map (ori_size^3, FP64) of the skip-gridding reconstruction."""
+    F = decenter_divide(data, weight, r_max, pad, tau2, tau2_fudge, minres_map)
+    ps = F.shape[0]
+    N = int(relion_round(pad * ori_size))
+    N += N % 2
+    h = N // 2 + 1
+    k = np.arange(N)
+    kp = np.where(k < h, k, k - N)
+    half = ps // 2
+    # windowFourierTransform (src/fftw.h:736-790): shrinking copies every output element;
+    # enlarging copies the input elements with r^2 <= (XSIZE(in) - 1)^2 and zeros the rest
+    ok = (kp >= -half) & (kp <= half)
+    src = np.where(kp < 0, kp + ps, kp)
+    jj = np.arange(h)
+    sel = ok[:, None, None] & ok[None, :, None] & (jj <= half)[None, None, :]
+    if N > ps:
+        sel &= (kp[:, None, None] ** 2 + kp[None, :, None] ** 2 + jj[None, None, :] ** 2) <= half * half
+    Z, Y, X = np.broadcast_arrays(src[:, None, None], src[None, :, None], np.minimum(jj, half)[None, None, :])
+    G = np.zeros((N, N, h), complex)
+    G[sel] = F[Z[sel], Y[sel], X[sel]]
+    sign = np.where(((k[:, None, None] ^ k[None, :, None] ^ jj[None, None, :]) & 1) != 0, -1.0, 1.0)
+    G = G * sign
+    big = np.fft.irfftn(G, s=(N, N, N), axes=(0, 1, 2)) * float(N) ** 3
+    o0 = N // 2 - ori_size // 2
+    vol = big[o0:o0 + ori_size, o0:o0 + ori_size, o0:o0 + ori_size] / (float(pad) ** 3 * ori_size)
+    vol = soft_mask_bg(vol, ori_size / 2.0, 3.0)
+    c = np.arange(ori_size) - ori_size // 2
+    r = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2)
+    rval = r / (ori_size * pad)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        sinc = np.where(r > 0, np.sin(PI * rval) / (PI * np.where(r > 0, rval, 1.0)), 1.0)
+    return vol / (sinc * sinc)
+
+
+def downsampled_average(data, weight, r_max, pad):
+    zd, yd, xd = weight.shape
+    K, I, J = _logical(weight.shape, -(zd // 2), -(yd // 2))
+    K, I, J = np.broadcast_arrays(K, I, J)
+    ds = 2 * (r_max + 1) + 1
+    dh = ds // 2
+    kp = relion_round(K / pad) + dh
+    ip = relion_round(I / pad) + dh
+    jp = relion_round(J / pad)
+    idx = (kp * ds + ip) * (dh + 1) + jp
+    n = ds * ds * (dh + 1)
+    ar = np.bincount(idx.ravel(), data.real.ravel(), n)
+    ai = np.bincount(idx.ravel(), data.imag.ravel(), n)
+    w = np.bincount(idx.ravel(), weight.ravel(), n)
+    avg = np.where(w > 0, (ar + 1j * ai) / np.where(w > 0, w, 1.0), 0.0)
+    return avg.reshape(ds, ds, dh + 1)
+
+
+def downsampled_fsc(data1, w1, data2, w2, r_max, pad, ori_size):
+    a1 = downsampled_average(data1, w1, r_max, pad)
+    a2 = downsampled_average(data2, w2, r_max, pad)
+    ds = a1.shape[0]
+    dh = ds // 2
+    c = np.arange(ds) - dh
+    R = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + np.arange(dh + 1)[None, None, :] ** 2)
+    m = R <= r_max
+    idx = relion_round(R[m])
+    nb = ori_size // 2 + 1
+    num = np.bincount(idx, (a1[m] * np.conj(a2[m])).real, nb)
+    d1 = np.bincount(idx, np.abs(a1[m]) ** 2, nb)
+    d2 = np.bincount(idx, np.abs(a2[m]) ** 2, nb)
+    fsc = np.where(d1 * d2 > 0, num / np.sqrt(np.where(d1 * d2 > 0, d1 * d2, 1.0)), 0.0)
+    fsc[0] = 1.0
+    return fsc
+
+
+def update_ssnr(weight, r_max, pad, ori_size, tau2_fudge, tau2, fsc, avgctf2=None, update_tau2_with_fsc=True,
+                is_whole_instead_of_half=False, correct_tau2_by_avgctf2=False):
+    """Returns tau2, sigma2, data_vs_prior, fourier_coverage (FP64)."""
+    zd, yd, xd = weight.shape
+    K, I, J = np.broadcast_arrays(*_logical(weight.shape, -(zd // 2), -(yd // 2)))
+    r2 = K * K + I * I + J * J
+    rp = int(relion_round(r_max * pad))
+    m = r2 < rp * rp
+    ires = relion_round(np.sqrt(r2[m].astype(float)) / pad)
+    nb = ori_size // 2 + 1
+    oc = float(pad) ** 3
+    wv = weight[m]
+    s2 = np.bincount(ires, oc * wv, nb)
+    cnt = np.bincount(ires, minlength=nb).astype(float)
+    sigma2 = np.where(s2 > 1e-10, cnt / np.where(s2 > 1e-10, s2, 1.0), 0.0)
+    tau2 = np.array(tau2, float).copy()
+    dvp = np.zeros(nb)
+    cov = np.zeros(nb)
+    if update_tau2_with_fsc:
+        myfsc = np.maximum(0.001, np.asarray(fsc, float))
+        if is_whole_instead_of_half:
+            myfsc = np.sqrt(2. * myfsc / (myfsc + 1.))
+        myfsc = np.minimum(0.999, myfsc)
+        ssnr = myfsc / (1. - myfsc) * tau2_fudge
+        tau2 = ssnr * sigma2
+        dvp = ssnr.copy()
+    t = tau2[ires]
+    with np.errstate(divide="ignore"):
+        invtau2 = np.where(t > 0, 1.0 / (oc * tau2_fudge * np.where(t > 0, t, 1.0)), 1.0 / (0.001 * wv))
+    if correct_tau2_by_avgctf2 and avgctf2 is not None:
+        a = np.asarray(avgctf2, float)[ires]
+        invtau2 = np.where((t > 0) & (a > 0), invtau2 / np.where(a > 0, a, 1.0), invtau2)
+    ratio = wv / invtau2
+    if not update_tau2_with_fsc:
+        dvp = np.bincount(ires, ratio, nb)
+    cov = np.bincount(ires, (ratio >= 1.).astype(float), nb)
+    cnt2 = np.bincount(ires, minlength=nb).astype(float)
+    if not update_tau2_with_fsc:
+        i = np.arange(nb)
+        dvp = np.where(i > r_max, 0.0, np.where(cnt2 < 0.001, 999., dvp / np.maximum(cnt2, 1e-300)))
+    cov = np.where(cnt2 > 0, cov / np.maximum(cnt2, 1e-300), cov)
+    return tau2, sigma2, dvp, cov

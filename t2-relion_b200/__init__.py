@@ -40,6 +40,7 @@ ABI_SYMBOLS = (
     "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
     "t2b_prep_configure", "t2b_prep_batch_host", "t2b_prep_batch_device", "t2b_autotune", "t2b_tune_set",
+    "t2b_reconstruct", "t2b_fsc_halves", "t2b_update_ssnr",
 )
 
 
@@ -126,6 +127,17 @@ class PrepOut(ctypes.Structure):
     _fields_ = [(n, _p) for n in ("fimg", "fimg_nomask", "ctf", "minvsigma2", "scalars", "power")]
 
 
+class ReconConfig(ctypes.Structure):
+    _fields_ = [("ori_size", ctypes.c_int), ("do_map", ctypes.c_int), ("minres_map", ctypes.c_int),
+                ("_pad", ctypes.c_int), ("tau2_fudge", ctypes.c_double), ("tau2", _p)]
+
+
+class SsnrConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("ori_size", "update_tau2_with_fsc", "is_whole_instead_of_half",
+                                            "correct_tau2_by_avgctf2")] + [
+        ("tau2_fudge", ctypes.c_double), ("fsc", _p), ("avgctf2", _p)]
+
+
 class TuneReport(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("diff2_tn", "diff2_group", "fine_ctas_per_sm", "wsum_ctas_per_sm",
                                             "project_pixels", "project_orients")] + [
@@ -173,6 +185,9 @@ def _setup_prototypes():
     lib.t2b_proposal_grad.argtypes = [v, v, v, v, i, ctypes.POINTER(ctypes.c_double), v]
     lib.t2b_prep_configure.argtypes = [v, ctypes.POINTER(PrepConfig)]
     lib.t2b_autotune.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(TuneReport)]
+    lib.t2b_reconstruct.argtypes = [v, i, ctypes.POINTER(ReconConfig), v]
+    lib.t2b_fsc_halves.argtypes = [v, i, i, i, v]
+    lib.t2b_update_ssnr.argtypes = [v, i, ctypes.POINTER(SsnrConfig), v, v, v, v]
     lib.t2b_tune_set.argtypes = [v, ctypes.POINTER(TuneReport)]
     lib.t2b_prep_batch_host.argtypes = [v, ctypes.POINTER(PrepBatch), ctypes.POINTER(PrepOut)]
     lib.t2b_prep_batch_device.argtypes = [v, ctypes.POINTER(PrepBatch), ctypes.POINTER(PrepOut), v]
@@ -357,6 +372,34 @@ class EStep:
         r = Result(*[result_ptrs.get(name) for name, _ in Result._fields_])
         _check(lib.t2b_estep_batch_device(self._h, ctypes.byref(b), ctypes.byref(r),
                                           ctypes.c_void_p(stream)))
+
+    # ---------------------------------------------- M-step reconstruction
+    def reconstruct(self, iclass, ori_size, tau2=None, tau2_fudge=1.0, minres_map=0):
+        """t2b_reconstruct: the real-space map (ori_size^3, FP64) of grid `iclass`."""
+        t = None if tau2 is None else np.ascontiguousarray(tau2, np.float64)
+        cfg = ReconConfig(ori_size, 0 if t is None else 1, minres_map, 0, tau2_fudge, _ptr(t))
+        vol = np.zeros((ori_size,) * 3)
+        _check(lib.t2b_reconstruct(self._h, iclass, ctypes.byref(cfg), _ptr(vol)))
+        return vol
+
+    def fsc_halves(self, grid_a, grid_b, ori_size):
+        """t2b_fsc_halves: down-sampled FSC of two grids (ori_size/2+1)."""
+        f = np.zeros(ori_size // 2 + 1)
+        _check(lib.t2b_fsc_halves(self._h, grid_a, grid_b, ori_size, _ptr(f)))
+        return f
+
+    def update_ssnr(self, iclass, ori_size, tau2, tau2_fudge=1.0, fsc=None, avgctf2=None,
+                    is_whole_instead_of_half=False):
+        """t2b_update_ssnr: returns (tau2, sigma2, data_vs_prior, fourier_coverage)."""
+        nb = ori_size // 2 + 1
+        t = np.array(tau2, np.float64).reshape(nb)
+        f = None if fsc is None else np.ascontiguousarray(fsc, np.float64)
+        a = None if avgctf2 is None else np.ascontiguousarray(avgctf2, np.float64)
+        cfg = SsnrConfig(ori_size, f is not None, int(is_whole_instead_of_half), a is not None, tau2_fudge,
+                         _ptr(f), _ptr(a))
+        out = [np.zeros(nb) for _ in range(3)]
+        _check(lib.t2b_update_ssnr(self._h, iclass, ctypes.byref(cfg), _ptr(t), *[_ptr(o) for o in out]))
+        return (t, *out)
 
     # ---------------------------------------------- tile-shape autotuner
     def autotune(self, fimg, ctf, minvsigma2, scalars, fimg_nomask=None):

@@ -1439,7 +1439,8 @@ __global__ void k_results(Tables tb, Work w)
 
 // --------------------------------------------------- reconstruction (FP64)
 __global__ void k_decenter(Volume g, const float2* __restrict__ data, const float* __restrict__ weight,
-                           double2* __restrict__ fconv, double* __restrict__ fw, double* rad, double* cnt)
+                           double2* __restrict__ fconv, double* __restrict__ fw, double* rad, double* cnt,
+                           const double* __restrict__ tau2, double tscale, int minres_map)
 {
     const int ps = g.ydim, fx = ps / 2 + 1;
     const long long total = (long long)ps * ps * fx;
@@ -1458,6 +1459,14 @@ __global__ void k_decenter(Volume g, const float2* __restrict__ data, const floa
         const float2 d = data[src];
         v = make_double2(d.x, d.y);
         wv = weight[src];
+    }
+    // MAP term: the inverse tau2 spectrum added to the weight (src/backprojector.cpp:1412-1455)
+    if (tau2 && r2 < rp * rp) {
+        const double rr = sqrt((double)r2) / g.pad;
+        const int im = rr > 0 ? (int)(rr + 0.5) : (int)(rr - 0.5);
+        const double t = tau2[im];
+        const double invtau2 = t > 0. ? 1. / (tscale * t) : (wv > 1e-20 ? 1. / (0.001 * wv) : 0.);
+        if (im >= minres_map) wv += invtau2;
     }
     fconv[n] = v;
     fw[n] = wv;
@@ -1610,14 +1619,15 @@ void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* co
 }
 
 void launch_reconstruct(const Volume& g, const float2* data, const float* weight, double2* fconv,
-                        double* fw, double* rad, double* cnt, cudaStream_t st)
+                        double* fw, double* rad, double* cnt, cudaStream_t st, const double* tau2, double tscale,
+                        int minres_map)
 {
     const int ps = g.ydim, fx = ps / 2 + 1;
     const long long total = (long long)ps * ps * fx;
     T2B_CUDA(cudaMemsetAsync(rad, 0, sizeof(double) * g.r_max, st));
     T2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(double) * g.r_max, st));
     const int nb = (int)((total + 255) / 256);
-    k_decenter<<<nb, 256, 0, st>>>(g, data, weight, fconv, fw, rad, cnt);
+    k_decenter<<<nb, 256, 0, st>>>(g, data, weight, fconv, fw, rad, cnt, tau2, tscale, minres_map);
     k_radnorm<<<(g.r_max + 255) / 256, 256, 0, st>>>(g.r_max, rad, cnt);
     k_divide<<<nb, 256, 0, st>>>(g, fconv, fw, rad);
     T2B_CUDA(cudaGetLastError());

@@ -29,6 +29,7 @@
 // Box-Muller) with the reference's spectrum, transformed back unnormalised like
 // FFTW's c2r.
 #include "t2b_internal.cuh"
+#include "fft_smem.cuh"
 
 #include <cmath>
 #include <cstring>
@@ -38,13 +39,6 @@ namespace t2b {
 constexpr double PI_D = 3.14159265358979323846;
 constexpr int PREP_MAX_N = 512;
 constexpr int PREP_THREADS = 256;
-constexpr int PREP_MAX_STAGES = 12;
-
-struct FftPlan {
-    int n = 0;
-    int nst = 0;
-    int rad[PREP_MAX_STAGES] = {};
-};
 
 struct ImagePrep {
     t2b_prep_config cfg{};
@@ -78,194 +72,6 @@ struct ImagePrep {
 };
 
 namespace {
-
-// ------------------------------------------------------------ shared-memory FFT
-__device__ __forceinline__ float2 cmul(float2 a, float2 b)
-{
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-
-template <bool INV>
-__device__ __forceinline__ float2 twid(const float2* tw, int t)
-{
-    const float2 w = tw[t];
-    return INV ? make_float2(w.x, -w.y) : w;
-}
-
-// DFT of R points in registers: out[q] = sum_r v[r] W^{q r}, W = e^{-+2 pi i / R}
-// (tw[t] = e^{-2 pi i t / N}, NR = N / R).
-template <int R, bool INV>
-__device__ __forceinline__ void dft_small(float2* v, const float2* tw, int NR)
-{
-    if (R == 2) {
-        const float2 a = v[0], b = v[1];
-        v[0] = cadd(a, b);
-        v[1] = csub(a, b);
-    } else if (R == 4) {
-        const float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
-        const float2 c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
-        // forward: X1 = b - i d, X3 = b + i d; inverse swaps them
-        const float2 mid = INV ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);   // -+ i d
-        v[0] = cadd(a, c);
-        v[2] = csub(a, c);
-        v[1] = cadd(b, mid);
-        v[3] = csub(b, mid);
-    } else if (R == 8) {
-        // 8 = 2 x 4: DFT4 of the even and odd points, X[k] = E[k] + W8^k O[k], X[k+4] = E[k] - W8^k O[k]
-        float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
-        dft_small<4, INV>(e, tw, NR);
-        dft_small<4, INV>(o, tw, NR);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const float2 t = k == 0 ? o[0] : cmul(o[k], twid<INV>(tw, k * NR));
-            v[k] = cadd(e[k], t);
-            v[k + 4] = csub(e[k], t);
-        }
-    } else if (R == 16) {
-        // 16 = 4 x 4: Y_l = DFT4 over m of v[4m + l]; X[k1 + 4 k2] = DFT4 over l of W16^{l k1} Y_l[k1]
-        float2 y[4][4];
-#pragma unroll
-        for (int l = 0; l < 4; ++l) {
-            float2 t[4] = {v[l], v[4 + l], v[8 + l], v[12 + l]};
-            dft_small<4, INV>(t, tw, NR);
-#pragma unroll
-            for (int k1 = 0; k1 < 4; ++k1) y[l][k1] = t[k1];
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1) {
-            float2 z[4];
-#pragma unroll
-            for (int l = 0; l < 4; ++l) z[l] = (l * k1 == 0) ? y[l][k1] : cmul(y[l][k1], twid<INV>(tw, l * k1 * NR));
-            dft_small<4, INV>(z, tw, NR);
-#pragma unroll
-            for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = z[k2];
-        }
-    } else {
-        float2 o[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-            float2 acc = v[0];
-#pragma unroll
-            for (int r = 1; r < R; ++r) acc = cadd(acc, cmul(v[r], twid<INV>(tw, ((q * r) % R) * NR)));
-            o[q] = acc;
-        }
-#pragma unroll
-        for (int q = 0; q < R; ++q) v[q] = o[q];
-    }
-}
-
-// One Stockham stage over nfft sequences of length N: a -> b.
-template <int R, bool INV>
-__device__ __forceinline__ void fft_stage(const float2* a, float2* b, int nfft, int N, int Ns, const float2* tw)
-{
-    const int NR = N / R;
-    const int tstride = N / (Ns * R);
-    for (int e = threadIdx.x; e < nfft * NR; e += blockDim.x) {
-        const int f = e / NR, j = e - f * NR;
-        const float2* in = a + f * N;
-        float2* out = b + f * N;
-        const int k = j % Ns;
-        float2 v[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = in[j + r * NR];
-#pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid<INV>(tw, k * r * tstride));
-        dft_small<R, INV>(v, tw, NR);
-        const int base = (j / Ns) * Ns * R + k;
-#pragma unroll
-        for (int r = 0; r < R; ++r) out[base + r * Ns] = v[r];
-    }
-}
-
-// All stages; returns the buffer holding the transform (natural order).
-template <bool INV>
-__device__ float2* fft_smem(float2* a, float2* b, int nfft, const FftPlan& pl, const float2* tw)
-{
-    int Ns = 1;
-    for (int st = 0; st < pl.nst; ++st) {
-        const int R = pl.rad[st];
-        switch (R) {
-        case 4: fft_stage<4, INV>(a, b, nfft, pl.n, Ns, tw); break;
-        case 2: fft_stage<2, INV>(a, b, nfft, pl.n, Ns, tw); break;
-        case 3: fft_stage<3, INV>(a, b, nfft, pl.n, Ns, tw); break;
-        default: fft_stage<5, INV>(a, b, nfft, pl.n, Ns, tw); break;
-        }
-        __syncthreads();
-        float2* t = a;
-        a = b;
-        b = t;
-        Ns *= R;
-    }
-    return a;
-}
-
-
-// ---- the same FFT with the size known at compile time (the common box sizes):
-// constant radix plan (radix-16 and radix-8 register butterflies first), constant
-// index arithmetic, unrolled stage sequence
-constexpr int ct_radix(int N, int st)
-{
-    int n = N, k = 0;
-    for (int r : {16, 8, 4, 2, 3, 5})
-        while (n % r == 0) {
-            if (k == st) return r;
-            n /= r;
-            ++k;
-        }
-    return 0;
-}
-constexpr int ct_ns(int N, int st)
-{
-    int ns = 1;
-    for (int k = 0; k < st; ++k) ns *= ct_radix(N, k);
-    return ns;
-}
-
-template <int R, bool INV, int N, int Ns>
-__device__ __forceinline__ void fft_stage_ct(const float2* a, float2* b, int nfft, const float2* tw)
-{
-    constexpr int NR = N / R;
-    constexpr int tstride = N / (Ns * R);
-    for (int e = threadIdx.x; e < nfft * NR; e += blockDim.x) {
-        const int f = e / NR, j = e - f * NR;
-        const float2* in = a + f * N;
-        float2* out = b + f * N;
-        const int k = j % Ns;
-        float2 v[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = in[j + r * NR];
-        if (Ns > 1) {
-#pragma unroll
-            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid<INV>(tw, k * r * tstride));
-        }
-        dft_small<R, INV>(v, tw, NR);
-        const int base = (j / Ns) * Ns * R + k;
-#pragma unroll
-        for (int r = 0; r < R; ++r) out[base + r * Ns] = v[r];
-    }
-}
-
-template <int N, bool INV, int ST>
-__device__ __forceinline__ float2* fft_ct(float2* a, float2* b, int nfft, const float2* tw)
-{
-    if constexpr (ct_radix(N, ST) == 0) {
-        return a;
-    } else {
-        fft_stage_ct<ct_radix(N, ST), INV, N, ct_ns(N, ST)>(a, b, nfft, tw);
-        __syncthreads();
-        return fft_ct<N, INV, ST + 1>(b, a, nfft, tw);
-    }
-}
-
-// compile-time size when NC > 0, the runtime plan otherwise
-template <int NC, bool INV>
-__device__ __forceinline__ float2* fft_any(float2* a, float2* b, int nfft, const FftPlan& pl, const float2* tw)
-{
-    if constexpr (NC > 0) return fft_ct<NC, INV, 0>(a, b, nfft, tw);
-    else return fft_smem<INV>(a, b, nfft, pl, tw);
-}
 
 __device__ __forceinline__ int relion_round(double x) { return x > 0 ? (int)(x + 0.5) : (int)(x - 0.5); }
 
@@ -872,25 +678,6 @@ PrepKernel fused_kernel(int N, bool noise)
 
 double host_round(double x) { return x > 0 ? (double)(int)(x + 0.5) : (double)(int)(x - 0.5); }
 
-FftPlan make_plan(int N)
-{
-    FftPlan pl;
-    pl.n = N;
-    int n = N;
-    auto take = [&](int r) {
-        while (n % r == 0 && pl.nst < PREP_MAX_STAGES) {
-            pl.rad[pl.nst++] = r;
-            n /= r;
-        }
-    };
-    take(4);
-    take(2);
-    take(3);
-    take(5);
-    T2B_REQUIRE(n == 1, T2B_ERR_UNSUPPORTED, "image_size must be a product of 2, 3 and 5");
-    return pl;
-}
-
 template <typename T>
 T* dalloc(ImagePrep& G, size_t count)
 {
@@ -1033,7 +820,7 @@ int t2b_prep_configure(t2b_ctx* c, const t2b_prep_config* cf)
         T2B_REQUIRE(cf->q0 >= 0. && cf->q0 < 1. && cf->voltage > 0., T2B_ERR_ARG, "bad optics (voltage, q0)");
         T2B_REQUIRE(!cf->do_norm_correction || cf->avg_norm_correction > 0., T2B_ERR_ARG,
                     "avg_norm_correction must be positive");
-        const FftPlan plan = make_plan(N);
+        const FftPlan plan = fft_plan(N);
         free_prep(c->prep);
         c->prep = nullptr;
         ImagePrep* G = new ImagePrep();

@@ -1,0 +1,508 @@
+// M-step reconstruction on the device: the real-space map of a backprojection
+// grid, the half-map FSC and the SSNR arrays.
+//
+// t2b_reconstruct follows BackProjector::reconstruct on the reference's default
+// skip-gridding path (src/backprojector.cpp:1344-1530; skip_gridding =
+// !--dont_skip_gridding, src/ml_optimiser.cpp:525): decenter (r^2 <= ROUND(r_max
+// pad)^2), the MAP term 1 / (pad^3 tau2_fudge tau2) added to the weights
+// (:1412-1455), the FP64 division by max(weight, radial average / 1000)
+// (:1463-1531; the kernels of t2b_reconstruct_divide), then
+// windowToOridimRealSpace (:2486-2620) and Projector::griddingCorrect
+// (src/projector.cpp:489-522):
+//   window the pad_size transform to pad * ori_size (src/fftw.h:736-790),
+//   CenterFFTbySign, unnormalised inverse 3D FFT, real-space window to
+//   ori_size, divide by pad^3 ori_size (2D particles), softMaskOutsideMap
+//   (radius ori_size / 2, cosine width 3, average background), divide by
+//   sinc^2(r / (ori_size pad)).
+// The inverse transform is three passes of batched 1D FFTs in shared memory
+// (fft_smem.cuh): columns along z, columns along y of the planes inside the
+// real-space window, and the c2r rows of the window only; FP32 (the division
+// before it and every sum after it are FP64).
+//
+// t2b_fsc_halves: getDownsampledAverage + calculateDownSampledFourierShellCorrelation
+// (src/backprojector.cpp:933-1040).  t2b_update_ssnr: updateSSNRarrays
+// (:1041-1205).  Both reduce the grid on the device (FP64 atomics into shell
+// and down-sampled bins) and finish the per-shell arithmetic on the host.
+#include "t2b_internal.cuh"
+#include "fft_smem.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace t2b {
+
+constexpr double PI_R = 3.14159265358979323846;
+
+namespace {
+
+constexpr int RC_THREADS = 256;
+constexpr int RC_CX = 16;   // columns per CTA in the z and y passes
+constexpr int RC_ROWS = 8;  // rows per CTA in the x pass
+
+__device__ __forceinline__ int rround(double x) { return x > 0 ? (int)(x + 0.5) : (int)(x - 0.5); }
+
+// the pad_size transform (FFTW layout, double2) -> the N = pad * ori_size half
+// transform (float2), windowed (shrink: every output element; enlarge: input
+// elements with r^2 <= (ps/2)^2) and centred by sign
+__global__ void k_window(const double2* __restrict__ fc, int ps, int N, float2* __restrict__ G)
+{
+    const int h = N / 2 + 1, half = ps / 2, fx = ps / 2 + 1;
+    const long long total = (long long)N * N * h;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % h);
+        const int i = (int)((n / h) % N);
+        const int k = (int)(n / ((long long)h * N));
+        const int kp = k < h ? k : k - N, ip = i < h ? i : i - N;
+        float2 v = make_float2(0.f, 0.f);
+        bool ok = kp >= -half && kp <= half && ip >= -half && ip <= half && j <= half;
+        if (ok && N > ps) ok = kp * kp + ip * ip + j * j <= half * half;
+        if (ok) {
+            const double2 d = fc[((size_t)(kp < 0 ? kp + ps : kp) * ps + (ip < 0 ? ip + ps : ip)) * fx + j];
+            const float sg = ((k ^ i ^ j) & 1) ? -1.f : 1.f;
+            v = make_float2((float)d.x * sg, (float)d.y * sg);
+        }
+        G[n] = v;
+    }
+}
+
+// inverse FFT of RC_CX columns along one axis: axis 0 = z (line index y = blockIdx.x),
+// axis 1 = y (plane z = z0 + blockIdx.x); x tile = blockIdx.y
+template <int NC>
+__global__ void __launch_bounds__(RC_THREADS) k_cols3(float2* __restrict__ G, int Nrt, int axis, int z0,
+                                                      const float2* __restrict__ tw, FftPlan plan)
+{
+    extern __shared__ float2 sm[];
+    const int N = NC > 0 ? NC : Nrt, h = N / 2 + 1;
+    float2* s_tw = sm;
+    float2* A = sm + N;
+    float2* B = A + RC_CX * N;
+    for (int t = threadIdx.x; t < N; t += blockDim.x) s_tw[t] = tw[t];
+    const int x0 = blockIdx.y * RC_CX;
+    const size_t line = blockIdx.x;
+    // element q of column c: axis 0: (q, line, x0 + c); axis 1: (z0 + line, q, x0 + c)
+    auto idx = [&](int q, int c) -> size_t {
+        return axis == 0 ? ((size_t)q * N + line) * h + x0 + c : (((size_t)z0 + line) * N + q) * h + x0 + c;
+    };
+    for (int e = threadIdx.x; e < RC_CX * N; e += blockDim.x) {
+        const int c = e % RC_CX, q = e / RC_CX;
+        A[c * N + q] = x0 + c < h ? G[idx(q, c)] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2* r = fft_any<NC, true>(A, B, RC_CX, plan, s_tw);
+    for (int e = threadIdx.x; e < RC_CX * N; e += blockDim.x) {
+        const int c = e % RC_CX, q = e / RC_CX;
+        if (x0 + c < h) G[idx(q, c)] = r[c * N + q];
+    }
+}
+
+// c2r rows (imaginary parts of x = 0 and N/2 dropped) of the real-space window:
+// row (z0 + zw, z0 + yw) -> vol[zw][yw][0..ori), divided by the FFT normalisation
+template <int NC>
+__global__ void __launch_bounds__(RC_THREADS) k_rows3(const float2* __restrict__ G, int Nrt, int ori, int z0,
+                                                      float norm, const float2* __restrict__ tw, FftPlan plan,
+                                                      float* __restrict__ vol)
+{
+    extern __shared__ float2 sm[];
+    const int N = NC > 0 ? NC : Nrt, h = N / 2 + 1;
+    float2* s_tw = sm;
+    float2* A = sm + N;
+    float2* B = A + RC_ROWS * N;
+    for (int t = threadIdx.x; t < N; t += blockDim.x) s_tw[t] = tw[t];
+    const int row0 = blockIdx.x * RC_ROWS;
+    for (int e = threadIdx.x; e < RC_ROWS * N; e += blockDim.x) {
+        const int rr = e / N, k = e - rr * N, row = row0 + rr;
+        float2 v = make_float2(0.f, 0.f);
+        if (row < ori * ori) {
+            const int zw = row / ori, yw = row - zw * ori;
+            const float2* g = G + (((size_t)z0 + zw) * N + z0 + yw) * h;
+            if (k == 0 || k == N / 2) v = make_float2(g[k].x, 0.f);
+            else if (k < N / 2) v = g[k];
+            else v = make_float2(g[N - k].x, -g[N - k].y);
+        }
+        A[e] = v;
+    }
+    __syncthreads();
+    const float2* r = fft_any<NC, true>(A, B, RC_ROWS, plan, s_tw);
+    for (int e = threadIdx.x; e < RC_ROWS * ori; e += blockDim.x) {
+        const int rr = e / ori, x = e - rr * ori, row = row0 + rr;
+        if (row < ori * ori) vol[(size_t)row * ori + x] = r[rr * N + z0 + x].x / norm;
+    }
+}
+
+// soft-mask background (softMaskOutsideMap without a noise image), fixed-order FP64
+// partial sums per block
+__global__ void __launch_bounds__(RC_THREADS) k_mask_partial(const float* __restrict__ vol, int ori, double radius,
+                                                             double width, double2* __restrict__ part)
+{
+    __shared__ double sw[RC_THREADS], sv[RC_THREADS];
+    const long long total = (long long)ori * ori * ori;
+    double aw = 0., av = 0.;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(n % ori), y = (int)((n / ori) % ori), z = (int)(n / ((long long)ori * ori));
+        const double xl = x - ori / 2, yl = y - ori / 2, zl = z - ori / 2;
+        const double r = sqrt(xl * xl + yl * yl + zl * zl);
+        if (r < radius) continue;
+        const double rp = radius + width;
+        const double w = r > rp ? 1. : 0.5 + 0.5 * cos(PI_R * (rp - r) / width);
+        aw += w;
+        av += w * vol[n];
+    }
+    sw[threadIdx.x] = aw;
+    sv[threadIdx.x] = av;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sw[threadIdx.x] += sw[threadIdx.x + o];
+            sv[threadIdx.x] += sv[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = make_double2(sw[0], sv[0]);
+}
+
+// soft mask with the background, then the gridding correction (trilinear: sinc^2)
+__global__ void k_mask_grid(const float* __restrict__ vol, int ori, int pad, double radius, double width,
+                            const double2* __restrict__ part, int nparts, double* __restrict__ out)
+{
+    __shared__ double s_bg;
+    if (threadIdx.x == 0) {
+        double w = 0., v = 0.;
+        for (int b = 0; b < nparts; ++b) {
+            w += part[b].x;
+            v += part[b].y;
+        }
+        s_bg = w > 0. ? v / w : 0.;
+    }
+    __syncthreads();
+    const double bg = s_bg;
+    const long long total = (long long)ori * ori * ori;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(n % ori), y = (int)((n / ori) % ori), z = (int)(n / ((long long)ori * ori));
+        const double xl = x - ori / 2, yl = y - ori / 2, zl = z - ori / 2;
+        const double r = sqrt(xl * xl + yl * yl + zl * zl);
+        double v = vol[n];
+        if (r >= radius) {
+            const double rp = radius + width;
+            if (r > rp) v = bg;
+            else {
+                const double w = 0.5 + 0.5 * cos(PI_R * (rp - r) / width);
+                v = (1. - w) * v + w * bg;
+            }
+        }
+        if (r > 0.) {
+            const double rv = r / ((double)ori * pad);
+            const double sn = sin(PI_R * rv) / (PI_R * rv);
+            v /= sn * sn;
+        }
+        out[n] = v;
+    }
+}
+
+// ---------------------------------------------------------------- FSC and SSNR
+__global__ void k_downsample(Volume g, const float2* __restrict__ data, const float* __restrict__ weight,
+                             double* __restrict__ acc /* bins x 3 */)
+{
+    const int ds = 2 * (g.r_max + 1) + 1, dh = ds / 2;
+    const long long total = (long long)g.zdim * g.ydim * g.xdim;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % g.xdim), i = (int)((n / g.xdim) % g.ydim), k = (int)(n / ((long long)g.xdim * g.ydim));
+        const int kp = rround((double)(k + g.initz) / g.pad) + dh, ip = rround((double)(i + g.inity) / g.pad) + dh;
+        const int jp = rround((double)j / g.pad);
+        if (kp < 0 || kp >= ds || ip < 0 || ip >= ds || jp > dh) continue;   // a grid larger than pad_size
+        const size_t b = (((size_t)kp * ds + ip) * (dh + 1) + jp) * 3;
+        const float2 d = data[n];
+        const float w = weight[n];
+        if (d.x != 0.f) atomicAdd(&acc[b], (double)d.x);
+        if (d.y != 0.f) atomicAdd(&acc[b + 1], (double)d.y);
+        if (w != 0.f) atomicAdd(&acc[b + 2], (double)w);
+    }
+}
+
+// shell sums: FP64 shared-memory bins per block, one global atomic per bin and block
+__device__ __forceinline__ void shell_init(double* sb, int n)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sb[i] = 0.;
+    __syncthreads();
+}
+__device__ __forceinline__ void shell_flush(const double* sb, int n, double* acc)
+{
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (sb[i] != 0.) atomicAdd(&acc[i], sb[i]);
+}
+
+__global__ void k_fsc_shells(int r_max, int nb, const double* __restrict__ a1, const double* __restrict__ a2,
+                             double* __restrict__ sh /* nb x 3 */)
+{
+    extern __shared__ double sb[];
+    shell_init(sb, 3 * nb);
+    const int ds = 2 * (r_max + 1) + 1, dh = ds / 2;
+    const long long total = (long long)ds * ds * (dh + 1);
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % (dh + 1)), i = (int)((n / (dh + 1)) % ds) - dh, k = (int)(n / ((long long)(dh + 1) * ds)) - dh;
+        const double R = sqrt((double)(k * k + i * i + j * j));
+        if (R > r_max) continue;
+        const int idx = rround(R);
+        const double w1 = a1[3 * n + 2], w2 = a2[3 * n + 2];
+        const double r1 = w1 > 0. ? a1[3 * n] / w1 : 0., i1 = w1 > 0. ? a1[3 * n + 1] / w1 : 0.;
+        const double r2 = w2 > 0. ? a2[3 * n] / w2 : 0., i2 = w2 > 0. ? a2[3 * n + 1] / w2 : 0.;
+        atomicAdd(&sb[3 * idx], r1 * r2 + i1 * i2);
+        atomicAdd(&sb[3 * idx + 1], r1 * r1 + i1 * i1);
+        atomicAdd(&sb[3 * idx + 2], r2 * r2 + i2 * i2);
+    }
+    shell_flush(sb, 3 * nb, sh);
+}
+
+// pass 1 of updateSSNRarrays: per shell, sum of pad^3 weight and count (r^2 < max_r2)
+__global__ void k_ssnr_sigma(Volume g, int nb, const float* __restrict__ weight, double oc, double* __restrict__ acc)
+{
+    extern __shared__ double sb[];
+    shell_init(sb, 2 * nb);
+    const int rp = g.r_max * g.pad;
+    const long long total = (long long)g.zdim * g.ydim * g.xdim;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % g.xdim), i = (int)((n / g.xdim) % g.ydim) + g.inity, k = (int)(n / ((long long)g.xdim * g.ydim)) + g.initz;
+        const int r2 = k * k + i * i + j * j;
+        if (r2 >= rp * rp) continue;
+        const int ires = rround(sqrt((double)r2) / g.pad);
+        atomicAdd(&sb[2 * ires], oc * weight[n]);
+        atomicAdd(&sb[2 * ires + 1], 1.);
+    }
+    shell_flush(sb, 2 * nb, acc);
+}
+
+// pass 2: per shell, sum of weight / invtau2 (data vs prior), coverage count, count
+__global__ void k_ssnr_prior(Volume g, int nb, const float* __restrict__ weight, double oc, double tau2_fudge,
+                             const double* __restrict__ tau2, const double* __restrict__ avgctf2, int correct_ctf2,
+                             double* __restrict__ acc)
+{
+    extern __shared__ double sb[];
+    shell_init(sb, 3 * nb);
+    const int rp = g.r_max * g.pad;
+    const long long total = (long long)g.zdim * g.ydim * g.xdim;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % g.xdim), i = (int)((n / g.xdim) % g.ydim) + g.inity, k = (int)(n / ((long long)g.xdim * g.ydim)) + g.initz;
+        const int r2 = k * k + i * i + j * j;
+        if (r2 >= rp * rp) continue;
+        const int ires = rround(sqrt((double)r2) / g.pad);
+        const double invw = weight[n];
+        double invtau2;
+        if (tau2[ires] > 0.) {
+            invtau2 = 1. / (oc * tau2_fudge * tau2[ires]);
+            if (correct_ctf2 && avgctf2[ires] > 0.) invtau2 *= 1. / avgctf2[ires];
+        } else {
+            invtau2 = 1. / (0.001 * invw);
+        }
+        const double ratio = invw / invtau2;
+        atomicAdd(&sb[3 * ires], ratio);
+        if (ratio >= 1.) atomicAdd(&sb[3 * ires + 1], 1.);
+        atomicAdd(&sb[3 * ires + 2], 1.);
+    }
+    shell_flush(sb, 3 * nb, acc);
+}
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    explicit DevBuf(size_t n)
+    {
+        if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            throw Error{T2B_ERR_NOMEM, "reconstruction buffers"};
+        }
+    }
+    ~DevBuf() { cudaFree(p); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+using ColKernel = void (*)(float2*, int, int, int, const float2*, FftPlan);
+using RowKernel = void (*)(const float2*, int, int, int, float, const float2*, FftPlan, float*);
+
+void recon_kernels(int N, ColKernel& col, RowKernel& row)
+{
+    if (N == 256) { col = k_cols3<256>; row = k_rows3<256>; }
+    else if (N == 128) { col = k_cols3<128>; row = k_rows3<128>; }
+    else { col = k_cols3<0>; row = k_rows3<0>; }
+}
+
+int grid_of(long long total)
+{
+    return (int)std::min<long long>((total + RC_THREADS - 1) / RC_THREADS, 148LL * 16);
+}
+
+const Volume& grid_volume(t2b_ctx* c, int ig)
+{
+    T2B_REQUIRE(ig >= 0 && ig < (int)c->gvol.size() && c->gdata[ig], T2B_ERR_ARG, "no such grid");
+    const Volume& v = c->gvol[ig];
+    T2B_REQUIRE(v.ref_dim == 3, T2B_ERR_UNSUPPORTED, "the reconstruction is implemented for 3D grids");
+    return v;
+}
+
+}  // namespace
+}  // namespace t2b
+
+using namespace t2b;
+
+extern "C" {
+
+int t2b_reconstruct(t2b_ctx* c, int iclass, const t2b_recon_config* cf, double* vol_out)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && cf && vol_out, T2B_ERR_ARG, "null argument");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard dg(c->device);
+        const Volume& v = grid_volume(c, iclass);
+        const int ori = cf->ori_size, pad = v.pad;
+        T2B_REQUIRE(ori >= 8 && ori % 2 == 0, T2B_ERR_ARG, "ori_size must be even and >= 8");
+        T2B_REQUIRE(v.r_max <= ori / 2, T2B_ERR_ARG, "the grid's r_max exceeds ori_size / 2");
+        T2B_REQUIRE(!cf->do_map || (cf->tau2 && cf->tau2_fudge > 0.), T2B_ERR_ARG, "do_map needs tau2 and tau2_fudge");
+        int N = pad * ori;
+        N += N % 2;
+        T2B_REQUIRE(N <= 512, T2B_ERR_UNSUPPORTED, "pad * ori_size must be <= 512");
+        const FftPlan plan = fft_plan(N);
+        const int ps = v.ydim, fx = ps / 2 + 1, h = N / 2 + 1;
+        const size_t nps = (size_t)ps * ps * fx;
+        cudaStream_t st = c->stream;
+        DevBuf<double2> fc(nps);
+        DevBuf<double> fw(nps), rad(2 * (size_t)v.r_max), t2(ori / 2 + 1);
+        if (cf->do_map)
+            T2B_CUDA(cudaMemcpyAsync(t2.p, cf->tau2, (ori / 2 + 1) * sizeof(double), cudaMemcpyHostToDevice, st));
+        const double tscale = (double)pad * pad * pad * cf->tau2_fudge;
+        launch_reconstruct(v, c->gdata[iclass], c->gweight[iclass], fc.p, fw.p, rad.p, rad.p + v.r_max, st,
+                           cf->do_map ? t2.p : nullptr, tscale, cf->minres_map);
+        // window + centre by sign, inverse 3D FFT, real-space window
+        DevBuf<float2> G((size_t)N * N * h), tw(N);
+        std::vector<float2> htw(N);
+        for (int t = 0; t < N; ++t) {
+            const double a = -2.0 * PI_R * (double)t / (double)N;
+            htw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        T2B_CUDA(cudaMemcpyAsync(tw.p, htw.data(), N * sizeof(float2), cudaMemcpyHostToDevice, st));
+        k_window<<<grid_of((long long)N * N * h), RC_THREADS, 0, st>>>(fc.p, ps, N, G.p);
+        ColKernel col;
+        RowKernel row;
+        recon_kernels(N, col, row);
+        const size_t smc = sizeof(float2) * ((size_t)N + 2 * (size_t)RC_CX * N);
+        const size_t smr = sizeof(float2) * ((size_t)N + 2 * (size_t)RC_ROWS * N);
+        T2B_CUDA(cudaFuncSetAttribute((const void*)col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc));
+        T2B_CUDA(cudaFuncSetAttribute((const void*)row, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr));
+        const int z0 = N / 2 - ori / 2, xt = (h + RC_CX - 1) / RC_CX;
+        col<<<dim3(N, xt), RC_THREADS, smc, st>>>(G.p, N, 0, 0, tw.p, plan);              // along z, every (y, x)
+        col<<<dim3(ori, xt), RC_THREADS, smc, st>>>(G.p, N, 1, z0, tw.p, plan);           // along y, window planes
+        DevBuf<float> vol((size_t)ori * ori * ori);
+        const float norm = (float)((double)pad * pad * pad * ori);                        // 2D particles
+        row<<<(ori * ori + RC_ROWS - 1) / RC_ROWS, RC_THREADS, smr, st>>>(G.p, N, ori, z0, norm, tw.p, plan, vol.p);
+        // soft mask (radius ori/2, width 3, average background) and gridding correction
+        const long long nv = (long long)ori * ori * ori;
+        const int nb = grid_of(nv);
+        DevBuf<double2> part(nb);
+        DevBuf<double> out(nv);
+        k_mask_partial<<<nb, RC_THREADS, 0, st>>>(vol.p, ori, ori / 2.0, 3.0, part.p);
+        k_mask_grid<<<nb, RC_THREADS, 0, st>>>(vol.p, ori, pad, ori / 2.0, 3.0, part.p, nb, out.p);
+        T2B_CUDA(cudaGetLastError());
+        T2B_CUDA(cudaMemcpyAsync(vol_out, out.p, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
+        T2B_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int t2b_fsc_halves(t2b_ctx* c, int grid_a, int grid_b, int ori_size, double* fsc)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && fsc && ori_size >= 2, T2B_ERR_ARG, "bad argument");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard dg(c->device);
+        const Volume& a = grid_volume(c, grid_a);
+        const Volume& b = grid_volume(c, grid_b);
+        T2B_REQUIRE(a.xdim == b.xdim && a.ydim == b.ydim && a.zdim == b.zdim && a.r_max == b.r_max && a.pad == b.pad,
+                    T2B_ERR_ARG, "the two grids differ in shape");
+        T2B_REQUIRE(a.r_max <= ori_size / 2, T2B_ERR_ARG, "r_max exceeds ori_size / 2");
+        const int ds = 2 * (a.r_max + 1) + 1, dh = ds / 2, nb = ori_size / 2 + 1;
+        T2B_REQUIRE(nb <= 1024, T2B_ERR_ARG, "ori_size too large");
+        const size_t bins = (size_t)ds * ds * (dh + 1);
+        cudaStream_t st = c->stream;
+        DevBuf<double> aa(3 * bins), ab(3 * bins), sh(3 * (size_t)nb);
+        T2B_CUDA(cudaMemsetAsync(aa.p, 0, 3 * bins * sizeof(double), st));
+        T2B_CUDA(cudaMemsetAsync(ab.p, 0, 3 * bins * sizeof(double), st));
+        T2B_CUDA(cudaMemsetAsync(sh.p, 0, 3 * (size_t)nb * sizeof(double), st));
+        const long long nvox = (long long)a.zdim * a.ydim * a.xdim;
+        k_downsample<<<grid_of(nvox), RC_THREADS, 0, st>>>(a, c->gdata[grid_a], c->gweight[grid_a], aa.p);
+        k_downsample<<<grid_of(nvox), RC_THREADS, 0, st>>>(b, c->gdata[grid_b], c->gweight[grid_b], ab.p);
+        k_fsc_shells<<<grid_of((long long)bins), RC_THREADS, 3 * nb * sizeof(double), st>>>(a.r_max, nb, aa.p, ab.p,
+                                                                                             sh.p);
+        T2B_CUDA(cudaGetLastError());
+        std::vector<double> h(3 * (size_t)nb);
+        T2B_CUDA(cudaMemcpyAsync(h.data(), sh.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        T2B_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < nb; ++i) {
+            const double d = h[3 * i + 1] * h[3 * i + 2];
+            fsc[i] = d > 0. ? h[3 * i] / std::sqrt(d) : 0.;
+        }
+        fsc[0] = 1.;
+    });
+}
+
+int t2b_update_ssnr(t2b_ctx* c, int iclass, const t2b_ssnr_config* cf, double* tau2, double* sigma2,
+                    double* data_vs_prior, double* fourier_coverage)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && cf && tau2 && sigma2 && data_vs_prior && fourier_coverage, T2B_ERR_ARG, "null argument");
+        T2B_REQUIRE(!cf->update_tau2_with_fsc || cf->fsc, T2B_ERR_ARG, "update_tau2_with_fsc needs the FSC");
+        T2B_REQUIRE(!cf->correct_tau2_by_avgctf2 || cf->avgctf2, T2B_ERR_ARG, "correct_tau2_by_avgctf2 needs avgctf2");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard dg(c->device);
+        const Volume& v = grid_volume(c, iclass);
+        const int nb = cf->ori_size / 2 + 1;
+        T2B_REQUIRE(v.r_max < nb && nb <= 1024, T2B_ERR_ARG, "r_max exceeds ori_size / 2 (or ori_size too large)");
+        const double oc = (double)v.pad * v.pad * v.pad;
+        cudaStream_t st = c->stream;
+        DevBuf<double> acc(3 * (size_t)nb), t2d(nb), actf(nb);
+        const long long nvox = (long long)v.zdim * v.ydim * v.xdim;
+        // pass 1: sigma2 = count / sum(pad^3 weight) per shell (src/backprojector.cpp:1058-1088)
+        T2B_CUDA(cudaMemsetAsync(acc.p, 0, 3 * (size_t)nb * sizeof(double), st));
+        k_ssnr_sigma<<<grid_of(nvox), RC_THREADS, 2 * nb * sizeof(double), st>>>(v, nb, c->gweight[iclass], oc, acc.p);
+        std::vector<double> h(3 * (size_t)nb);
+        T2B_CUDA(cudaMemcpyAsync(h.data(), acc.p, 2 * (size_t)nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+        T2B_CUDA(cudaStreamSynchronize(st));
+        std::vector<double> s2(nb), t(tau2, tau2 + nb), dvp(nb, 0.), cov(nb, 0.);
+        for (int i = 0; i < nb; ++i) {
+            const double sw = h[2 * i], cn = h[2 * i + 1];
+            s2[i] = sw > 1e-10 ? cn / sw : 0.;
+        }
+        // tau2 from the FSC (:1101-1125)
+        if (cf->update_tau2_with_fsc)
+            for (int i = 0; i < nb; ++i) {
+                double f = std::max(0.001, cf->fsc[i]);
+                if (cf->is_whole_instead_of_half) f = std::sqrt(2. * f / (f + 1.));
+                f = std::min(0.999, f);
+                const double ssnr = f / (1. - f) * cf->tau2_fudge;
+                t[i] = ssnr * s2[i];
+                dvp[i] = ssnr;
+            }
+        // pass 2: data vs prior and Fourier coverage (:1127-1190)
+        T2B_CUDA(cudaMemcpyAsync(t2d.p, t.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        if (cf->correct_tau2_by_avgctf2)
+            T2B_CUDA(cudaMemcpyAsync(actf.p, cf->avgctf2, nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        T2B_CUDA(cudaMemsetAsync(acc.p, 0, 3 * (size_t)nb * sizeof(double), st));
+        k_ssnr_prior<<<grid_of(nvox), RC_THREADS, 3 * nb * sizeof(double), st>>>(v, nb, c->gweight[iclass], oc,
+                                                                                  cf->tau2_fudge, t2d.p, actf.p,
+                                                                                  cf->correct_tau2_by_avgctf2, acc.p);
+        T2B_CUDA(cudaGetLastError());
+        T2B_CUDA(cudaMemcpyAsync(h.data(), acc.p, 3 * (size_t)nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+        T2B_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < nb; ++i) {
+            const double ratio = h[3 * i], ncov = h[3 * i + 1], cn = h[3 * i + 2];
+            if (!cf->update_tau2_with_fsc) dvp[i] = i > v.r_max ? 0. : (cn < 0.001 ? 999. : ratio / cn);
+            cov[i] = cn > 0. ? ncov / cn : ncov;
+        }
+        for (int i = 0; i < nb; ++i) {
+            tau2[i] = t[i];
+            sigma2[i] = s2[i];
+            data_vs_prior[i] = dvp[i];
+            fourier_coverage[i] = cov[i];
+        }
+    });
+}
+
+}  // extern "C"

@@ -191,7 +191,8 @@ void launch_weights_fine(const Tables& tb, const Work& w, cudaStream_t st);
 void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* const* grid_data,
                     float* const* grid_weight, cudaStream_t st);
 void launch_reconstruct(const Volume& g, const float2* data, const float* weight, double2* fconv,
-                        double* fw, double* rad, double* cnt, cudaStream_t st);
+                        double* fw, double* rad, double* cnt, cudaStream_t st, const double* tau2 = nullptr,
+                        double tscale = 1., int minres_map = 0);
 
 // tcgen05 split-BF16 coarse diff2 (diff2_tc.cu)
 struct TcOperands {

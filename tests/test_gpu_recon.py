@@ -1,0 +1,93 @@
+"""M-step reconstruction on the GPU (t2b_reconstruct, t2b_fsc_halves,
+t2b_update_ssnr) against the FP64 oracle (oracle/recon_oracle.py), on the
+backprojection grids the E-step filled.
+
+Tolerances: the map within 2e-5 of its largest value (the inverse 3D FFT is
+FP32; the division before it and the sums after it are FP64); FSC and SSNR
+arrays 1e-9 relative (FP64 sums in a different order)."""
+import numpy as np
+import pytest
+
+import problems
+import recon_oracle as ro
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def two_classes():
+    pb = problems.build("refine_o2", n_particles=32, seed=23, nr_classes=2)
+    P = pb["parts"]
+    es = pb["product"]()
+    es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    pb["es"] = es
+    pb["grids"] = [es.get_backprojector(k) for k in range(2)]
+    yield pb
+    es.close()
+
+
+def _map_close(got, ref):
+    err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+    assert err <= 2e-5, err
+    c = np.corrcoef(got.ravel(), ref.ravel())[0, 1]
+    assert c >= 0.999999, c
+
+
+@pytest.mark.parametrize("with_map", [False, True], ids=["plain", "map_tau2"])
+def test_reconstruction_matches_oracle(two_classes, with_map):
+    pb, es = two_classes, two_classes["es"]
+    N, r = pb["N"], pb["r"]
+    data, w = pb["grids"][0]
+    tau2 = None
+    if with_map:
+        tau2 = np.random.default_rng(3).uniform(0.5, 2.0, N // 2 + 1) * np.mean(w)
+    got = es.reconstruct(0, N, tau2=tau2, tau2_fudge=1.3, minres_map=2)
+    ref = ro.reconstruct_map(data.astype(np.complex128), w.astype(np.float64), r, 2, N, tau2=tau2, tau2_fudge=1.3,
+                             minres_map=2)
+    _map_close(got, ref)
+
+
+def test_reconstruction_of_a_larger_grid_window_shrinks(t2b):
+    """A grid whose pad_size (131) exceeds pad * ori_size (128): the transform is cut down."""
+    pb = problems.build("refine_o2", n_particles=16, seed=29)
+    P, samp = pb["parts"], pb["samp"]
+    es = t2b.EStep(0)
+    es.set_projector(0, pb["maps"][0], 3, pb["r"], 2)
+    big_r = pb["N"] // 2
+    es.init_backprojector(0, 3, 2 * (2 * big_r + 1) + 1, big_r, 2)
+    es.configure(ori_size=pb["N"], current_size=pb["s"], ref_dim=3, nr_classes=1, samp=samp,
+                 pdf_direction=np.ones((1, samp["n_dir"])) / samp["n_dir"], pdf_class=np.ones(1),
+                 sigma2_offset=36.0, pixel_size=2.0, adaptive_oversampling=0, diff2_mode=0, max_batch=16)
+    es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    data, w = es.get_backprojector(0)
+    got = es.reconstruct(0, pb["N"])
+    es.close()
+    ref = ro.reconstruct_map(data.astype(np.complex128), w.astype(np.float64), big_r, 2, pb["N"])
+    _map_close(got, ref)
+
+
+def test_fsc_matches_oracle(two_classes):
+    pb, es = two_classes, two_classes["es"]
+    (d1, w1), (d2, w2) = pb["grids"]
+    got = es.fsc_halves(0, 1, pb["N"])
+    ref = ro.downsampled_fsc(d1.astype(np.complex128), w1.astype(np.float64), d2.astype(np.complex128),
+                             w2.astype(np.float64), pb["r"], 2, pb["N"])
+    assert np.allclose(got, ref, rtol=1e-9, atol=1e-12)
+    same = es.fsc_halves(0, 0, pb["N"])
+    assert np.allclose(same[:pb["r"] + 1], 1.0, atol=1e-12)
+
+
+@pytest.mark.parametrize("with_fsc", [True, False], ids=["tau2_from_fsc", "keep_tau2"])
+def test_ssnr_matches_oracle(two_classes, with_fsc):
+    pb, es = two_classes, two_classes["es"]
+    N, r = pb["N"], pb["r"]
+    _, w = pb["grids"][0]
+    nb = N // 2 + 1
+    tau2 = np.random.default_rng(7).uniform(0.1, 1.0, nb) * np.mean(w)
+    tau2[-3:] = 0.0
+    fsc = np.clip(1.0 - np.linspace(0, 1.1, nb), -0.05, 1.0) if with_fsc else None
+    got = es.update_ssnr(0, N, tau2, tau2_fudge=1.2, fsc=fsc)
+    ref = ro.update_ssnr(w.astype(np.float64), r, 2, N, 1.2, tau2, fsc if with_fsc else np.zeros(nb),
+                         update_tau2_with_fsc=with_fsc)
+    for g, rr in zip(got, ref):
+        assert np.allclose(g, rr, rtol=1e-9, atol=1e-14)

@@ -1,0 +1,107 @@
+"""The FP64 reconstruction oracle (oracle/recon_oracle.py) on the CPU: its
+skip-gridding division against the C++ E-step oracle's, its real-space chain
+(window, CenterFFTbySign, inverse FFT, normalisation, gridding correction) on
+the Fourier map of a known volume, and the FSC / SSNR arrays against direct
+sums."""
+import numpy as np
+import pytest
+
+import recon_oracle as ro
+
+
+def _grid(rng, r_max, pad=2):
+    ps = 2 * (r_max * pad + 1) + 1
+    data = (rng.standard_normal((ps, ps, ps // 2 + 1)) + 1j * rng.standard_normal((ps, ps, ps // 2 + 1)))
+    weight = rng.uniform(0.5, 2.0, (ps, ps, ps // 2 + 1))
+    return data.astype(np.complex64).astype(np.complex128), weight.astype(np.float32).astype(np.float64)
+
+
+def test_division_matches_cpp_oracle(oracle):
+    rng = np.random.default_rng(1)
+    data, weight = _grid(rng, 8)
+    got = ro.decenter_divide(data, weight, 8, 2)
+    ref = oracle.reconstruct_divide(data, weight, 8, 2)
+    assert np.max(np.abs(got - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+def test_map_term_raises_the_weights():
+    rng = np.random.default_rng(2)
+    data, weight = _grid(rng, 8)
+    tau2 = np.full(17, 0.5)
+    plain = ro.decenter_divide(data, weight, 8, 2)
+    reg = ro.decenter_divide(data, weight, 8, 2, tau2=tau2, tau2_fudge=1.0, minres_map=0)
+    # inside the sphere the weight grows by 1/(pad^3 tau2) = 0.25: |F| shrinks
+    m = np.abs(plain) > 0
+    assert np.all(np.abs(reg[m]) <= np.abs(plain[m]) * (1 + 1e-12))
+    assert np.any(np.abs(reg[m]) < 0.9 * np.abs(plain[m]))
+
+
+@pytest.mark.parametrize("ori,r_max", [(32, 16), (32, 8)], ids=["shrink", "enlarge"])
+def test_reconstruction_of_a_known_volume(synth, ori, r_max):
+    """Grid = the padded Fourier map of a band-limited volume V with weight 1: the map is
+    V / ori (normalisation of 2D particles) over sinc^2 (gridding correction), low-passed
+    at r_max."""
+    vol = synth.blob_volume(ori, 8, sigma=(2.5, 4.0), seed=3)
+    # the map a projector holds: centred half-complex of the 2x padded volume (weights 1),
+    # on the pad_size box 2 (2 r_max + 1) + 1 (which exceeds the padded box when r_max = ori/2)
+    m = 2 * ori
+    big0 = np.zeros((m,) * 3)
+    big0[ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori] = vol
+    F0 = np.fft.rfftn(np.fft.ifftshift(big0)) / float(ori) ** 3
+    ps = 2 * (2 * r_max + 1) + 1
+    kk = np.arange(ps) - ps // 2
+    KZ, KY, KX = np.meshgrid(kk, kk, np.arange(ps // 2 + 1), indexing="ij")
+    keep = KZ * KZ + KY * KY + KX * KX <= (2 * r_max) ** 2
+    fmap = np.where(keep, F0[KZ % m, KY % m, np.minimum(KX, m // 2)], 0)
+    weight = np.ones(fmap.shape)
+    got = ro.reconstruct_map(fmap, weight, r_max, 2, ori)
+    c = np.arange(ori) - ori // 2
+    r = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2)
+    rv = r / (2 * ori)
+    sinc = np.where(r > 0, np.sin(np.pi * rv) / (np.pi * np.where(r > 0, rv, 1)), 1.0)
+    # the same low-pass applied to V directly
+    N = 2 * ori
+    big = np.zeros((N,) * 3)
+    big[ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori] = vol
+    F = np.fft.rfftn(np.fft.ifftshift(big))
+    k = np.fft.fftfreq(N) * N
+    kx = np.arange(N // 2 + 1)
+    r2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kx[None, None, :] ** 2
+    F[r2 > (2 * r_max) ** 2] = 0
+    lp = np.fft.fftshift(np.fft.irfftn(F, s=(N,) * 3, axes=(0, 1, 2)))[ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori,
+                                                        ori // 2:ori // 2 + ori]
+    want = ro.soft_mask_bg(lp / ori, ori / 2.0, 3.0) / (sinc * sinc)
+    assert np.max(np.abs(got - want)) <= 1e-10 * np.max(np.abs(want))
+
+
+def test_fsc_of_identical_and_independent_halves():
+    rng = np.random.default_rng(4)
+    d1, w1 = _grid(rng, 8)
+    f_same = ro.downsampled_fsc(d1, w1, d1, w1, 8, 2, 32)
+    assert np.allclose(f_same[:9], 1.0, atol=1e-12) and np.all(f_same[9:] == 0)
+    d2, w2 = _grid(rng, 8)
+    f_ind = ro.downsampled_fsc(d1, w1, d2, w2, 8, 2, 32)
+    assert f_ind[0] == 1.0 and np.all(np.abs(f_ind[2:9]) < 0.3)
+
+
+def test_ssnr_arrays_against_direct_sums():
+    rng = np.random.default_rng(5)
+    _, w = _grid(rng, 8)
+    ori, nb = 32, 17
+    tau2 = rng.uniform(0.1, 1.0, nb)
+    fsc = np.clip(1.0 - np.linspace(0, 1.2, nb), -0.1, 1.0)
+    t, s2, dvp, cov = ro.update_ssnr(w, 8, 2, ori, 1.5, tau2, fsc)
+    # direct: shell of every voxel with r^2 < (r_max pad)^2, ires = ROUND(r / pad)
+    ps = w.shape[0]
+    k = np.arange(ps) - ps // 2
+    K, I, J = np.meshgrid(k, k, np.arange(w.shape[2]), indexing="ij")
+    r2 = K * K + I * I + J * J
+    m = r2 < 16 * 16
+    ires = np.floor(np.sqrt(r2[m]) / 2 + 0.5).astype(int)
+    s = np.bincount(ires, 8 * w[m], nb)
+    n = np.bincount(ires, minlength=nb)
+    assert np.allclose(s2[n > 0], n[n > 0] / s[n > 0], rtol=1e-12)
+    f = np.minimum(0.999, np.maximum(0.001, fsc))
+    assert np.allclose(dvp, f / (1 - f) * 1.5, rtol=1e-12)
+    assert np.allclose(t, f / (1 - f) * 1.5 * s2, rtol=1e-12)
+    assert np.all((cov >= 0) & (cov <= 1))
