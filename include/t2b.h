@@ -436,6 +436,35 @@ int t2b_prep_configure(t2b_ctx* ctx, const t2b_prep_config* cfg);
 int t2b_prep_batch_host(t2b_ctx* ctx, const t2b_prep_batch* batch, const t2b_prep_out* out);
 int t2b_prep_batch_device(t2b_ctx* ctx, const t2b_prep_batch* batch, const t2b_prep_out* out, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * On-disk formats of real data (host code, no GPU).
+ *
+ * MRC image stacks (src/rwMRC.h): modes 0 (int8), 1 (int16), 2 (float32),
+ * 6 (uint16), 12 (half); byte-swapped files are recognised as the reference
+ * does; the pixel size is cella.x / mx.  t2b_mrc_read converts sections
+ * [first, first + count) of a stack (nx * ny floats each) to float;
+ * t2b_mrc_write writes mode 2.
+ *
+ * STAR metadata (MetaDataTable::read, src/metadata_table.cpp:959-1262): one
+ * data block (the first, or data_<block>), a loop_ table or label-value pairs;
+ * values are kept as text (t2b_star_value) or converted to numbers column by
+ * column (t2b_star_column).  Labels are given without the leading '_'.
+ * t2b_star_write writes a numeric loop_ block (append: after the file's blocks).
+ * ------------------------------------------------------------------------- */
+int t2b_mrc_info(const char* path, int* nx, int* ny, int* nz, int* mode, double* pixel_size);
+int t2b_mrc_read(const char* path, long long first, long long count, float* out);
+int t2b_mrc_write(const char* path, const float* data, int nx, int ny, int nz, double pixel_size);
+
+typedef struct t2b_star t2b_star;
+int t2b_star_open(const char* path, const char* block, t2b_star** table);
+int t2b_star_shape(const t2b_star* table, long long* rows, int* cols);
+int t2b_star_label(const t2b_star* table, int col, char* buf, int cap);
+int t2b_star_column(const t2b_star* table, const char* label, double* out);
+int t2b_star_value(const t2b_star* table, const char* label, long long row, char* buf, int cap);
+void t2b_star_close(t2b_star* table);
+int t2b_star_write(const char* path, const char* block, int ncols, const char* const* labels, long long nrows,
+                   const double* values, int append);
+
 /* Host sampling (HealpixSampling, src/healpix_sampling.cpp:534-640,
  * 1787-2040), C1 symmetry, no perturbation.  Fills Euler matrices of the
  * coarse orientations (idir*n_psi + ipsi), of the fine orientations

@@ -41,6 +41,8 @@ ABI_SYMBOLS = (
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
     "t2b_prep_configure", "t2b_prep_batch_host", "t2b_prep_batch_device", "t2b_autotune", "t2b_tune_set",
     "t2b_reconstruct", "t2b_fsc_halves", "t2b_update_ssnr",
+    "t2b_mrc_info", "t2b_mrc_read", "t2b_mrc_write", "t2b_star_open", "t2b_star_shape", "t2b_star_label",
+    "t2b_star_column", "t2b_star_value", "t2b_star_close", "t2b_star_write",
 )
 
 
@@ -186,6 +188,18 @@ def _setup_prototypes():
     lib.t2b_prep_configure.argtypes = [v, ctypes.POINTER(PrepConfig)]
     lib.t2b_autotune.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(TuneReport)]
     lib.t2b_reconstruct.argtypes = [v, i, ctypes.POINTER(ReconConfig), v]
+    ll = ctypes.c_longlong
+    lib.t2b_mrc_info.argtypes = [c] + [ctypes.POINTER(i)] * 4 + [ctypes.POINTER(ctypes.c_double)]
+    lib.t2b_mrc_read.argtypes = [c, ll, ll, v]
+    lib.t2b_mrc_write.argtypes = [c, v, i, i, i, ctypes.c_double]
+    lib.t2b_star_open.argtypes = [c, c, ctypes.POINTER(v)]
+    lib.t2b_star_shape.argtypes = [v, ctypes.POINTER(ll), ctypes.POINTER(i)]
+    lib.t2b_star_label.argtypes = [v, i, c, i]
+    lib.t2b_star_column.argtypes = [v, c, v]
+    lib.t2b_star_value.argtypes = [v, c, ll, c, i]
+    lib.t2b_star_close.argtypes = [v]
+    lib.t2b_star_close.restype = None
+    lib.t2b_star_write.argtypes = [c, c, i, ctypes.POINTER(c), ll, v, i]
     lib.t2b_fsc_halves.argtypes = [v, i, i, i, v]
     lib.t2b_update_ssnr.argtypes = [v, i, ctypes.POINTER(SsnrConfig), v, v, v, v]
     lib.t2b_tune_set.argtypes = [v, ctypes.POINTER(TuneReport)]
@@ -207,6 +221,106 @@ def _ptr(a):
 
 def version():
     return lib.t2b_version().decode()
+
+
+# ------------------------------------------------------------------ on-disk formats
+def mrc_info(path):
+    """(nx, ny, nz, mode, pixel size) of an MRC file (t2b_mrc_info)."""
+    v = [ctypes.c_int() for _ in range(4)]
+    px = ctypes.c_double()
+    _check(lib.t2b_mrc_info(os.fsencode(path), *[ctypes.byref(x) for x in v], ctypes.byref(px)))
+    return v[0].value, v[1].value, v[2].value, v[3].value, px.value
+
+
+def read_mrc(path, first=0, count=None):
+    """Sections [first, first + count) of an MRC stack as float32 (count, ny, nx)."""
+    nx, ny, nz, _, _ = mrc_info(path)
+    count = nz - first if count is None else count
+    out = np.zeros((count, ny, nx), np.float32)
+    _check(lib.t2b_mrc_read(os.fsencode(path), first, count, _ptr(out)))
+    return out
+
+
+def write_mrc(path, data, pixel_size):
+    """Write (nz, ny, nx) or (ny, nx) float32 data as mode-2 MRC."""
+    d = np.ascontiguousarray(data, np.float32)
+    if d.ndim == 2:
+        d = d[None]
+    _check(lib.t2b_mrc_write(os.fsencode(path), _ptr(d), d.shape[2], d.shape[1], d.shape[0], float(pixel_size)))
+
+
+class StarTable:
+    """One data block of a STAR file (t2b_star_*): labels, text values, numeric columns."""
+
+    def __init__(self, path, block=None):
+        self._h = ctypes.c_void_p()
+        _check(lib.t2b_star_open(os.fsencode(path), None if block is None else block.encode(), ctypes.byref(self._h)))
+        rows, cols = ctypes.c_longlong(), ctypes.c_int()
+        _check(lib.t2b_star_shape(self._h, ctypes.byref(rows), ctypes.byref(cols)))
+        self.rows = rows.value
+        buf = ctypes.create_string_buffer(256)
+        self.labels = []
+        for k in range(cols.value):
+            _check(lib.t2b_star_label(self._h, k, buf, 256))
+            self.labels.append(buf.value.decode())
+
+    def column(self, label):
+        out = np.zeros(self.rows)
+        _check(lib.t2b_star_column(self._h, label.encode(), _ptr(out)))
+        return out
+
+    def value(self, label, row):
+        buf = ctypes.create_string_buffer(4096)
+        _check(lib.t2b_star_value(self._h, label.encode(), row, buf, 4096))
+        return buf.value.decode()
+
+    def strings(self, label):
+        return [self.value(label, r) for r in range(self.rows)]
+
+    def close(self):
+        if self._h:
+            lib.t2b_star_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_star(path, block, columns, append=False):
+    """Write a numeric loop_ block: columns = {label: array of rows}."""
+    labels = list(columns)
+    vals = np.ascontiguousarray(np.stack([np.asarray(columns[k], np.float64) for k in labels], 1))
+    arr = (ctypes.c_char_p * len(labels))(*[k.encode() for k in labels])
+    _check(lib.t2b_star_write(os.fsencode(path), block.encode(), len(labels), arr, vals.shape[0], _ptr(vals),
+                              int(append)))
+
+
+def prep_params_from_star(particles, pixel_size, scale_correction=1.0):
+    """Per-particle t2b_prep_batch parameters (n x 12) from a RELION particles block:
+    offsets rlnOriginX/YAngst / pixel size (METADATA_XOFF/YOFF in pixels), priors (999: none),
+    rlnNormCorrection, defocus U/V/angle, CTF B-factor, scale, phase shift."""
+    n = particles.rows
+    have = set(particles.labels)
+
+    def col(name, default):
+        return particles.column(name) if name in have else np.full(n, default)
+    par = np.zeros((n, PREP_NPARAM))
+    par[:, 0] = col("rlnOriginXAngst", 0.0) / pixel_size
+    par[:, 1] = col("rlnOriginYAngst", 0.0) / pixel_size
+    par[:, 2] = col("rlnOriginXPriorAngst", 999.0 * pixel_size) / pixel_size
+    par[:, 3] = col("rlnOriginYPriorAngst", 999.0 * pixel_size) / pixel_size
+    par[:, 4] = col("rlnNormCorrection", 1.0)
+    par[:, 5] = col("rlnDefocusU", 0.0)
+    par[:, 6] = col("rlnDefocusV", 0.0)
+    par[:, 7] = col("rlnDefocusAngle", 0.0)
+    par[:, 8] = col("rlnCtfBfactor", 0.0)
+    par[:, 9] = col("rlnCtfScalefactor", 1.0)
+    par[:, 10] = col("rlnPhaseShift", 0.0)
+    par[:, 11] = scale_correction
+    return par
 
 
 def sampling(ref_dim, healpix_order, psi_step, adaptive_oversampling, offset_range_px,

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libt2b.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["api.cu", "project.cu", "estep.cu", "diff2_tc.cu", "proposal.cu", "imageprep.cu", "recon.cu", "noalloc.cu", "sampling.cpp"]
+SOURCES = ["api.cu", "project.cu", "estep.cu", "diff2_tc.cu", "proposal.cu", "imageprep.cu", "recon.cu", "noalloc.cu", "sampling.cpp", "io.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -170,3 +170,41 @@ def test_device_particle_path_matches_oracle_preparation():
     same = np.all(a["pose"] == b["pose"], axis=1)
     assert same.mean() >= 0.95, same.mean()
     assert np.allclose(a["min_diff2"], b["min_diff2"], rtol=1e-4)
+
+
+def test_particles_from_star_and_mrc_files(tmp_path):
+    """The real-data path: a STAR particles block and an MRC stack on disk -> the library's
+    readers -> device preparation -> E-step; the same poses as the in-memory batch."""
+    pb = problems.build("refine_o2", n_particles=16, seed=31)
+    t2b, sy, N, s, r = pb["t2b"], pb["sy"], pb["N"], pb["s"], pb["r"]
+    full = sy.make_particles(pb["maps"][0], 16, ori_size=N, s=N, r_max=r, angpix=2.0, snr=0.05, seed=31,
+                             max_shift=3.0)
+    imgs = np.stack([real_space_from_window(full["fimg"][b].astype(np.complex128), N)
+                     for b in range(16)]).astype(np.float32)
+    stack = tmp_path / "particles.mrcs"
+    t2b.write_mrc(str(stack), imgs, 2.0)
+    star = tmp_path / "particles.star"
+    t2b.write_star(str(star), "particles", {"rlnDefocusU": full["defU"], "rlnDefocusV": full["defV"],
+                                            "rlnDefocusAngle": full["dang"], "rlnOriginXAngst": np.zeros(16),
+                                            "rlnOriginYAngst": np.zeros(16)})
+    tab = t2b.StarTable(str(star), "particles")
+    par = t2b.prep_params_from_star(tab, 2.0)
+    nx, ny, nz, mode, px = t2b.mrc_info(str(stack))
+    assert (nx, ny, nz, mode) == (N, N, 16, 2) and px == pytest.approx(2.0)
+    disk = t2b.read_mrc(str(stack))
+    assert np.array_equal(disk, imgs)
+    cfg = base_cfg(N, s, sigma2_noise=np.full(N // 2 + 1, full["sigma2"]), pixel_size=px, mask_radius=28.0,
+                   zero_mask=0, random_seed=5)
+    es = pb["product"]()
+    es.configure_prep(max_batch=16, **cfg)
+    a_in = es.prepare_images(disk, par, np.arange(16))
+    direct_par = params(16, np.random.default_rng(0))
+    direct_par[:, ipo.P_DEFU], direct_par[:, ipo.P_DEFV], direct_par[:, ipo.P_DEFANG] = full["defU"], full["defV"], \
+        full["dang"]
+    direct_par[:, ipo.P_XPRIOR] = direct_par[:, ipo.P_YPRIOR] = 999.0
+    b_in = es.prepare_images(imgs, direct_par, np.arange(16))
+    for k in ("fimg", "fimg_nomask", "ctf", "minvsigma2", "scalars"):
+        assert np.array_equal(a_in[k], b_in[k]), k
+    a = es.expectation(a_in["fimg"], a_in["ctf"], a_in["minvsigma2"], a_in["scalars"], fimg_nomask=a_in["fimg_nomask"])
+    es.close()
+    assert np.all(a["status"] == 0)
