@@ -378,6 +378,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         w.d2f = dalloc<float>(c, (size_t)w.pair_cap * R * V);
         w.wf = dalloc<double>(c, (size_t)w.pair_cap * R * V);
         w.groups = dalloc<long long>(c, w.pair_cap);
+        w.group_end = dalloc<long long>(c, w.pair_cap);
         w.group_b = dalloc<int>(c, w.pair_cap);
         w.group_off = dalloc<long long>(c, B + 1);
         w.counters = dalloc<unsigned long long>(c, 16);

@@ -1214,9 +1214,15 @@ __global__ void k_group_starts(Tables tb, Work w)
     const long long npairs = w.pair_off[w.n];
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < npairs; q += (long long)gridDim.x * blockDim.x) {
         const int b = w.pair_b[q];
-        if (q == w.pair_off[b] || w.pairs[q - 1] / tb.T != w.pairs[q] / tb.T) {
+        const long long oc = w.pairs[q] / tb.T;
+        if (q == w.pair_off[b] || w.pairs[q - 1] / tb.T != oc) {
             const unsigned long long i = atomicAdd(&w.counters[3], 1ull);
             w.groups[i] = q;
+            // the group's end, found here (one thread per group) rather than by the consumer
+            long long e = q + 1;
+            const long long pend = w.pair_off[b + 1];
+            while (e < pend && w.pairs[e] / tb.T == oc) e++;
+            w.group_end[i] = e;
         }
     }
 }
@@ -1243,14 +1249,8 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
             // a work item is (orientation group, fine rotation); find the group's end
             grp_end = -1;
             if ((unsigned long long)item < nitems) {
-                const long long q = w.groups[item / R];
-                const int bq = w.pair_b[q];
-                const long long oc = w.pairs[q] / T;
-                long long e = q + 1;
-                const long long pend = w.pair_off[bq + 1];
-                while (e < pend && w.pairs[e] / T == oc) e++;
-                grp_end = e;
-                grp_beg = q;
+                grp_beg = w.groups[item / R];
+                grp_end = w.group_end[item / R];
             }
         }
         __syncthreads();

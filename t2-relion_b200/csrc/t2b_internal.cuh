@@ -153,6 +153,7 @@ struct Work {
     float* d2f;               // pair_cap * R*V
     double* wf;               // pair_cap * R*V (final weights when ovs; coarse gathered otherwise)
     long long* groups;        // pair_cap: first pair of each orientation group
+    long long* group_end;     // pair_cap: one past its last pair
     int* group_b;             // pair_cap
     long long* group_off;     // n+1
     unsigned long long* counters; // queue heads etc. (16)
