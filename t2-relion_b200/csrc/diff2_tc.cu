@@ -163,6 +163,8 @@ __device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, 
 struct TcParams {
     int m_tiles, n_tiles, kblocks;
     int group;                // dense tiles: orientation tiles per raster group (0: 16)
+    int ksplit;               // raw GEMMs: K split into this many slices (0/1: none); slice s writes
+                              // its partial product at out + s * ncols * KO
     int raw;                  // 1: store the contraction itself (norm and network GEMMs), 0: diff2 epilogue
     int KO, T, ncols;
     const float* c0;
@@ -233,7 +235,9 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base_slot;
-    const int ntiles = p.m_tiles * p.n_tiles;
+    const int ksp = p.ksplit > 1 ? p.ksplit : 1;
+    const int ntiles = p.m_tiles * p.n_tiles * ksp;
+    const int kper = (p.kblocks + ksp - 1) / ksp;   // k-blocks per slice
 
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer
@@ -250,16 +254,17 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + bbytes * (p.products >= 2 ? 2u : 1u);
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
             int ya, yb;
+            const int kb0 = (tile % ksp) * kper, kb1 = min(p.kblocks, kb0 + kper);
             if (p.mode == 0) {
                 int mt, nt;
-                tile_coords(tile, p.m_tiles, p.n_tiles, p.group ? p.group : 16, mt, nt);
+                tile_coords(tile / ksp, p.m_tiles, p.n_tiles, p.group ? p.group : 16, mt, nt);
                 ya = mt * TM;
                 yb = nt * tn_l;
             } else {
                 ya = (p.mtp > 1) ? tile * TM : tile * p.ppt * p.kslot;
                 yb = (tile / (p.mtp ? p.mtp : 1)) * p.ppt * p.T;
             }
-            for (int kb = 0; kb < p.kblocks; kb++, it++) {
+            for (int kb = kb0; kb < kb1; kb++, it++) {
                 const int s = it % nst;
                 const uint32_t ph = (uint32_t)(it / nst) & 1u;
                 if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
@@ -290,7 +295,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             tc_fence_after();
             const uint32_t dt = tmem + (uint32_t)(abuf * TN);
             bool ok = true;
-            for (int kb = 0; kb < p.kblocks; kb++, it++) {
+            const int kb0 = (tile % ksp) * kper, kb1 = min(p.kblocks, kb0 + kper);
+            for (int kb = kb0; kb < kb1; kb++, it++) {
                 const int s = it % nst;
                 const uint32_t ph = (uint32_t)(it / nst) & 1u;
                 if (!mbar_wait(&full_bar[s], ph, &abort_flag)) { ok = false; break; }
@@ -301,7 +307,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
 #pragma unroll
                 for (int k = 0; k < TK / 16; k++) {
                     const uint64_t ko = (uint64_t)(k * 32) >> 4;  // 32 bytes per K=16 step
-                    umma(dt, dPh + ko, dIh + ko, idesc, (kb | k) != 0);
+                    umma(dt, dPh + ko, dIh + ko, idesc, (kb != kb0 || k != 0));
                     if (p.products >= 2) umma(dt, dPh + ko, dIl + ko, idesc, 1);
                     if (p.products == 3) umma(dt, dPl + ko, dIh + ko, idesc, 1);
                 }
@@ -323,7 +329,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         int tl = 0;
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x, tl++) {
             int mt = 0, nt = 0;
-            if (p.mode == 0) tile_coords(tile, p.m_tiles, p.n_tiles, p.group ? p.group : 16, mt, nt);
+            if (p.mode == 0) tile_coords(tile / ksp, p.m_tiles, p.n_tiles, p.group ? p.group : 16, mt, nt);
+            float* const outp = p.d2c + (size_t)(tile % ksp) * p.ncols * p.KO * p.T;   // raw: the slice's partial
             const int abuf = tl & 1;
             const uint32_t aph = (uint32_t)(tl >> 1) & 1u;
             if (!mbar_wait(&tfull_bar[abuf], aph, &abort_flag)) { abort_flag = 1; break; }
@@ -402,7 +409,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                             d = c0 + p.norms[(size_t)b * p.KO + oc] - sbuf[r * EPI_LD + lane];
                             lmin = min(lmin, f2key(d));
                         }
-                        p.d2c[((size_t)b * p.KO + oc) * p.T + t] = d;
+                        outp[((size_t)b * p.KO + oc) * p.T + t] = d;
                     }
                 } else {
                     // proposal tile: column -> (particle slot, translation), row -> (slot, proposal)
@@ -594,9 +601,9 @@ enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL,
 static_assert(MAP_COUNT <= TC_MAP_SLOTS, "tensor-map slots");
 static_assert(sizeof(CUtensorMap) == 128, "tensor-map size");
 
-void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128)
+void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128, int box_rows)
 {
-    const CUtensorMap m = make_map(ptr, rows, kdim, a_side ? TM : TN);
+    const CUtensorMap m = make_map(ptr, rows, kdim, box_rows > 0 ? box_rows : (a_side ? TM : TN));
     std::memcpy(out128, &m, sizeof(m));
 }
 
@@ -823,16 +830,24 @@ void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* 
 }
 
 // out[n][m] = sum_k A[m][k] B[n][k]: both operands K-major BF16 behind the
-// tensor maps maps[ia] (A, 128-row box) and maps[ib] (B, 256-row box); K a
-// multiple of 64; products = 1 is one BF16 product (the lo halves are not read).
-void tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* out, int products, int* err,
-                 cudaStream_t st)
+// tensor maps maps[ia] (A, 128-row box) and maps[ib] (B, a tn-row box: 256 or
+// 128); K a multiple of 64; products = 1 is one BF16 product (the lo halves are
+// not read).  ksplit > 1 splits K into slices (more tiles for a small M x N):
+// slice s writes its partial product at out + s * N * M, to be summed in a fixed
+// order by the caller; returns the number of slices written.
+int tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* out, int products, int* err,
+                cudaStream_t st, int ksplit, int tn)
 {
     T2B_REQUIRE(K % TK == 0 && M > 0 && N > 0 && products >= 1 && products <= 3, T2B_ERR_ARG, "tensor-core GEMM shape");
+    T2B_REQUIRE(tn == 256 || tn == 128, T2B_ERR_ARG, "tensor-core GEMM tile width");
     TcParams p{};
     p.m_tiles = (M + TM - 1) / TM;
-    p.n_tiles = (N + TN - 1) / TN;
+    p.n_tiles = (N + tn - 1) / tn;
     p.kblocks = K / TK;
+    // no empty slice: ceil(kblocks / kper) slices of kper = ceil(kblocks / ksplit) k-blocks
+    const int kper = (p.kblocks + std::max(1, ksplit) - 1) / std::max(1, ksplit);
+    p.ksplit = (p.kblocks + kper - 1) / kper;
+    p.tn = tn == TN ? 0 : tn;
     p.raw = 1;
     p.KO = M;
     p.T = 1;
@@ -840,9 +855,10 @@ void tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* o
     p.d2c = out;
     p.err = err;
     p.products = products;
-    const int grid = std::min(sms(), p.m_tiles * p.n_tiles);
+    const int grid = std::min(sms(), p.m_tiles * p.n_tiles * p.ksplit);
     k_diff2_tc<<<grid, NTHREADS, SMEM_BYTES, st>>>(static_cast<const CUtensorMap*>(maps), ia, ib, p);
     T2B_CUDA(cudaGetLastError());
+    return p.ksplit;
 }
 
 }  // namespace t2b

@@ -194,13 +194,16 @@ __global__ void __launch_bounds__(256) k_conv_fwd(const float* __restrict__ img,
     }
 }
 
-// out = act(y + bias) as FP32 and / or BF16 (rows x cols, row-major)
+// out = act(sum_s y_s + bias) as FP32 and / or BF16 (rows x cols, row-major; the
+// `slices` partial products of a split-K GEMM, rows * cols apart, summed in order)
 __global__ void k_bias_act(const float* __restrict__ y, const bf16* __restrict__ bias, int rows, int cols, int relu,
-                           float* __restrict__ outf, bf16* __restrict__ outb)
+                           float* __restrict__ outf, bf16* __restrict__ outb, int slices = 1)
 {
     const size_t total = (size_t)rows * cols;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        float v = y[i] + __bfloat162float(bias[i % cols]);
+        float acc = y[i];
+        for (int s = 1; s < slices; ++s) acc += y[(size_t)s * total + i];
+        float v = acc + __bfloat162float(bias[i % cols]);
         if (relu) v = fmaxf(v, 0.f);
         if (outf) outf[i] = v;
         if (outb) outb[i] = __float2bfloat16_rn(v);
@@ -1342,8 +1345,8 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.x0b, 0, (size_t)N.b_pad * NET_H0 * sizeof(bf16)));
     T2B_CUDA(cudaMemset(N.h1b, 0, (size_t)N.b_pad * NET_H1 * sizeof(bf16)));
     T2B_CUDA(cudaMemset(N.h2b, 0, (size_t)N.b_pad * NET_H2 * sizeof(bf16)));
-    N.y1 = (float*)net_dalloc(W, (size_t)B * NET_H1 * sizeof(float));
-    N.y2 = (float*)net_dalloc(W, (size_t)B * NET_H2 * sizeof(float));
+    N.y1 = (float*)net_dalloc(W, (size_t)NET_KSPLIT * B * NET_H1 * sizeof(float));   // split-K partials
+    N.y2 = (float*)net_dalloc(W, (size_t)NET_KSPLIT * B * NET_H2 * sizeof(float));
     N.logits = (float*)net_dalloc(W, (size_t)B * KO * sizeof(float));
     N.prop = (int*)net_dalloc(W, (size_t)B * 128 * sizeof(int));
     T2B_CUDA(cudaMemset(N.prop, 0, (size_t)B * 128 * sizeof(int)));
@@ -1370,8 +1373,9 @@ void net_setup(t2b_ctx* c, int na_max)
     tc_set_map_box(c->tc, rs + 1, N.ral, (int)ra_rows, N.kr, 128);
     tc_set_map_box(c->tc, rs + 2, N.rbh, (int)rb_rows, N.kr, RS_TMAX);
     tc_set_map_box(c->tc, rs + 3, N.rbl, (int)rb_rows, N.kr, RS_TMAX);
-    // tensor maps of the dense layers: W1, X0b, W2, H1b, W3, H2b
-    unsigned char blobs[6][128];
+    // tensor maps of the dense layers: W1, X0b, W2, H1b, W3, H2b, then the three activations
+    // again with a 128-row box (batches of <= 128 particles: 128-column tiles)
+    unsigned char blobs[9][128];
     const bf16* thb = (const bf16*)N.thb;
     tc_encode((void*)(thb + N.L.w1), NET_H1, NET_H0, true, blobs[0]);
     tc_encode(N.x0b, N.b_pad, NET_H0, false, blobs[1]);
@@ -1379,6 +1383,9 @@ void net_setup(t2b_ctx* c, int na_max)
     tc_encode(N.h1b, N.b_pad, NET_H1, false, blobs[3]);
     tc_encode((void*)(thb + N.L.w3), N.L.KOpad, NET_H2, true, blobs[4]);
     tc_encode(N.h2b, N.b_pad, NET_H2, false, blobs[5]);
+    tc_encode(N.x0b, N.b_pad, NET_H0, false, blobs[6], 128);
+    tc_encode(N.h1b, N.b_pad, NET_H1, false, blobs[7], 128);
+    tc_encode(N.h2b, N.b_pad, NET_H2, false, blobs[8], 128);
     N.maps = net_dalloc(W, sizeof(blobs));
     T2B_CUDA(cudaMemcpy(N.maps, blobs, sizeof(blobs), cudaMemcpyHostToDevice));
     // restricted coarse pass operands: up to 128 proposal rows per particle
@@ -1439,14 +1446,19 @@ void set_tile_shape(ProposalNet& N, int T)
 }
 
 // dense layers of the inference path: x0b (n rows) -> logits (n x KO, no bias)
+// fc1 and fc2 have only 8 output tiles of 128 features: K is split into NET_KSPLIT
+// slices (128 CTAs), the partial products summed in a fixed order with the bias;
+// batches of <= 128 particles use 128-column tiles
 void infer_dense(ProposalNet& N, int n, int* err, cudaStream_t st)
 {
     const bf16* thb = (const bf16*)N.thb;
-    tc_gemm_raw(N.maps, 0, 1, NET_H1, n, NET_H0, N.y1, 1, err, st);
-    k_bias_act<<<gridsz((size_t)n * NET_H1), 256, 0, st>>>(N.y1, thb + N.L.b1, n, NET_H1, 1, nullptr, (bf16*)N.h1b);
-    tc_gemm_raw(N.maps, 2, 3, NET_H2, n, NET_H1, N.y2, 1, err, st);
-    k_bias_act<<<gridsz((size_t)n * NET_H2), 256, 0, st>>>(N.y2, thb + N.L.b2, n, NET_H2, 1, nullptr, (bf16*)N.h2b);
-    tc_gemm_raw(N.maps, 4, 5, N.KO, n, NET_H2, N.logits, 1, err, st);
+    const bool narrow = n <= 128;
+    const int tn = narrow ? 128 : 256;
+    const int s1 = tc_gemm_raw(N.maps, 0, narrow ? 6 : 1, NET_H1, n, NET_H0, N.y1, 1, err, st, NET_KSPLIT, tn);
+    k_bias_act<<<gridsz((size_t)n * NET_H1), 256, 0, st>>>(N.y1, thb + N.L.b1, n, NET_H1, 1, nullptr, (bf16*)N.h1b, s1);
+    const int s2 = tc_gemm_raw(N.maps, 2, narrow ? 7 : 3, NET_H2, n, NET_H1, N.y2, 1, err, st, NET_KSPLIT, tn);
+    k_bias_act<<<gridsz((size_t)n * NET_H2), 256, 0, st>>>(N.y2, thb + N.L.b2, n, NET_H2, 1, nullptr, (bf16*)N.h2b, s2);
+    tc_gemm_raw(N.maps, 4, narrow ? 8 : 5, N.KO, n, NET_H2, N.logits, 1, err, st, 1, tn);
     T2B_CUDA(cudaGetLastError());
 }
 

@@ -13,6 +13,7 @@ constexpr int NET_NPOST = 8;       // posterior labels kept per training particl
 constexpr int NET_NTGT = 1 + NET_NPOST;
 constexpr int NET_TOPK_CAND = 2048;
 constexpr int NET_MAX_KO = 49152;  // logits of one particle held in shared memory by the top-k
+constexpr int NET_KSPLIT = 16;     // K slices of the fc1 / fc2 inference GEMMs
 constexpr int NET_MAX_K1 = 1024;   // network candidates rescored at low resolution
 
 // offsets (elements) of the parameters in the flat FP32 / BF16 vectors;

@@ -221,7 +221,7 @@ size_t tc_kn(int nk);
 void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate = nullptr,
                      int gate_run = 0);
 bool tc_supported();
-void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128);
+void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128, int box_rows = 0);
 void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_side);
 int tc_slot_proposals();
 int tc_slot_audit();
@@ -234,8 +234,8 @@ void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, in
                     cudaStream_t st);
 void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
                      unsigned* minkeya, int* err, cudaStream_t st);
-void tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* out, int products, int* err,
-                 cudaStream_t st);
+int tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* out, int products, int* err,
+                cudaStream_t st, int ksplit = 1, int tn = 256);
 
 }  // namespace t2b
 
