@@ -220,30 +220,56 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
                                                int* __restrict__ prop, int ranked)
 {
     extern __shared__ unsigned keys[];
-    __shared__ unsigned hist[256];
+    __shared__ unsigned whist[8][256];   // sub-histograms: warps w and w + 8, + 16, + 24 share one
     __shared__ unsigned s_prefix, s_want, s_n;
     __shared__ unsigned long long cand[NET_TOPK_CAND];
-    const int b = blockIdx.x;
+    const int b = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < KO; i += blockDim.x)
         keys[i] = skip[i] ? 0u : f2key(logits[(size_t)b * KO + i] + __bfloat162float(bias[i]));
     if (threadIdx.x == 0) { s_prefix = 0; s_want = (unsigned)k; s_n = 0; }
     __syncthreads();
     unsigned mask = 0;
     for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+        for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&whist[0][0])[i] = 0;
         __syncthreads();
         const unsigned prefix = s_prefix;
+        unsigned* hw = whist[wid & 7];
         for (int i = threadIdx.x; i < KO; i += blockDim.x)
-            if ((keys[i] & mask) == prefix) atomicAdd(&hist[(keys[i] >> shift) & 255u], 1u);
+            if ((keys[i] & mask) == prefix) atomicAdd(&hw[(keys[i] >> shift) & 255u], 1u);
         __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned want = s_want, d = 0;
-            for (int dg = 255; dg >= 0; dg--) {
-                if (hist[dg] >= want) { d = (unsigned)dg; break; }
-                want -= hist[dg];
+        if (wid == 0) {
+            // digit of the k-th largest: lane l holds bins 255-8l .. 248-8l (descending); a suffix
+            // scan over the lanes finds the lane whose bins cross `want`, then the lane walks them
+            const unsigned want0 = s_want;
+            unsigned c[8], tot = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int dg = 255 - 8 * lane - j;
+                unsigned v = 0;
+#pragma unroll
+                for (int h = 0; h < 8; h++) v += whist[h][dg];
+                c[j] = v;
+                tot += v;
             }
-            s_want = want;
-            s_prefix = prefix | (d << shift);
+            unsigned incl = tot;   // inclusive prefix over lanes 0..lane (higher digits first)
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned x = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += x;
+            }
+            const unsigned excl = incl - tot;
+            const bool here = excl < want0 && incl >= want0;
+            const unsigned ball = __ballot_sync(0xffffffffu, here);
+            if (here && lane == __ffs(ball) - 1) {
+                unsigned want = want0 - excl, d = 0;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    if (c[j] >= want) { d = 255u - 8u * lane - j; break; }
+                    want -= c[j];
+                }
+                s_want = want;
+                s_prefix = prefix | (d << shift);
+            }
         }
         mask |= 255u << shift;
         __syncthreads();
