@@ -104,7 +104,7 @@ class Problem:
     """Holds the numpy arrays an OrcSetup points to (keeps them alive)."""
 
     def __init__(self, *, ori_size, s, ref_dim, maps, r_max, pad, samp, pdf_direction, pdf_class,
-                 sigma2_offset, pixel_size, adaptive_fraction, ovs, bp_pad_size, bp_r_max):
+                 sigma2_offset, pixel_size, adaptive_fraction, ovs, bp_pad_size, bp_r_max, maximum_significants=-1):
         self.maps = np.ascontiguousarray(np.stack(maps), np.complex64)
         self.eul_coarse = np.ascontiguousarray(samp["eul_coarse"], np.float64)
         self.eul_fine = np.ascontiguousarray(samp["eul_fine"], np.float64)
@@ -132,7 +132,7 @@ class Problem:
         S.n_dir, S.n_psi, S.n_trans = samp["n_dir"], samp["n_psi"], samp["n_trans"]
         S.nover_rot = samp["nover_rot"] if ovs else 1
         S.nover_trans = samp["nover_trans"] if ovs else 1
-        S.adaptive_oversampling, S.maximum_significants = ovs, -1
+        S.adaptive_oversampling, S.maximum_significants = ovs, maximum_significants
         S.maps = _ptr(self.maps)
         S.mxdim, S.mydim, S.mzdim = mx, my, mz
         S.minity, S.minitz = -(my // 2), (-(mz // 2) if ref_dim == 3 else 0)

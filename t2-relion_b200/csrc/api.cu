@@ -222,7 +222,6 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
                     "adaptive_oversampling must be 0 or 1");
         const int R = f.adaptive_oversampling ? f.nover_rot : 1, V = f.adaptive_oversampling ? f.nover_trans : 1;
         T2B_REQUIRE(R >= 1 && R <= 8 && V >= 1 && V <= 4, T2B_ERR_ARG, "oversampling factors must be <= 8 (rot), <= 4 (trans)");
-        T2B_REQUIRE(f.maximum_significants <= 0, T2B_ERR_UNSUPPORTED, "maximum_significants > 0 is not supported");
         T2B_REQUIRE(f.diff2_mode == T2B_DIFF2_PLAIN_FP32 || f.diff2_mode == T2B_DIFF2_SPLIT_BF16, T2B_ERR_ARG, "bad diff2_mode");
         T2B_REQUIRE(f.diff2_mode != T2B_DIFF2_SPLIT_BF16 || tc_supported(), T2B_ERR_UNSUPPORTED,
                     "split-BF16 tcgen05 contraction unavailable in this build");
@@ -257,6 +256,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         tb.K = K; tb.n_dir = f.n_dir; tb.n_psi = f.n_psi; tb.O = O; tb.T = T;
         tb.R = R; tb.V = V; tb.ovs = f.adaptive_oversampling; tb.ref_dim = f.ref_dim;
         tb.sigma2_offset = f.sigma2_offset; tb.pixel_size = f.pixel_size; tb.adaptive_fraction = f.adaptive_fraction;
+        tb.maxsig = f.maximum_significants > 0 ? f.maximum_significants : 0;
         cudaStream_t st = c->stream;
         // host-side tables: normalised pdf_orientation and the skip mask
         std::vector<double> pdf_o((size_t)K * f.n_dir);

@@ -534,7 +534,10 @@ __global__ void k_sel_init(Work w, int fine, double frac)
 // Choose the digit bin that contains the crossing of the descending
 // cumulative sum; narrow the prefix or move on to the gather.  One CTA per
 // particle; bins are visited from the largest digit down.
-__global__ void __launch_bounds__(1024) k_select(Work w, int fine)
+// maxsig > 0 (coarse pass only, src/ml_optimiser.cpp:7945-7966): the walk also stops at
+// the maxsig-th largest weight, so the threshold is the weight at rank
+// min(crossing, maxsig - 1)
+__global__ void __launch_bounds__(1024) k_select(Work w, int fine, int maxsig)
 {
     __shared__ double ssum[1024];
     __shared__ unsigned long long scnt[1024];
@@ -568,16 +571,23 @@ __global__ void __launch_bounds__(1024) k_select(Work w, int fine)
         __syncthreads();
     }
     const double base = sel->cum_above, target = sel->target;
+    const unsigned long long cbase = sel->count_above;
     double before = threadIdx.x ? ssum[threadIdx.x - 1] : 0.;
+    unsigned long long beforec = threadIdx.x ? scnt[threadIdx.x - 1] : 0;
     for (int j = 0; j < per; j++) {
         const int pos = threadIdx.x * per + j;
         if (pos >= nb) break;
         const double s = hs[nb - 1 - pos];
-        if (hc[nb - 1 - pos] > 0) {
+        const unsigned long long cn = hc[nb - 1 - pos];
+        if (cn > 0) {
             atomicMax(&lastne, pos);
-            if (base + before + s > target) { atomicMin(&chosen, pos); break; }
+            if (base + before + s > target || (maxsig > 0 && cbase + beforec + cn >= (unsigned long long)maxsig)) {
+                atomicMin(&chosen, pos);
+                break;
+            }
         }
         before += s;
+        beforec += cn;
     }
     __syncthreads();
     // no crossing (adaptive_fraction ~ 1 under rounding): the lowest non-empty bin
@@ -707,7 +717,7 @@ __global__ void __launch_bounds__(256) k_gather(Tables tb, Work w, int fine)
 
 // Sort the candidates (descending) and walk the cumulative sum
 // (src/ml_optimiser.cpp:7905-7935).
-__global__ void __launch_bounds__(1024) k_final(Work w, int fine, int ipass)
+__global__ void __launch_bounds__(1024) k_final(Work w, int fine, int ipass, int maxsig)
 {
     __shared__ double c[CAND_CAP];
     const int b = blockIdx.x;
@@ -724,6 +734,7 @@ __global__ void __launch_bounds__(1024) k_final(Work w, int fine, int ipass)
             const double v = w.cand[(size_t)b * CAND_CAP];
             long long need = (long long)floor((sel->target - sel->cum_above) / v) + 1;
             need = max(1LL, min(need, nc));
+            if (maxsig > 0) need = max(1LL, min(need, (long long)maxsig - (long long)sel->count_above));
             sel->thr = v;
             sel->nr_sign = (long long)sel->count_above + need;
             sel->phase = 2;
@@ -752,7 +763,7 @@ __global__ void __launch_bounds__(1024) k_final(Work w, int fine, int ipass)
         long long k = -1;
         for (long long i = 0; i < nc; i++) {
             cum += c[i];
-            if (cum > sel->target) { k = i; break; }
+            if (cum > sel->target || (maxsig > 0 && (long long)sel->count_above + i + 1 >= maxsig)) { k = i; break; }
         }
         if (k < 0) k = nc - 1;
         sel->thr = c[k];
@@ -834,7 +845,7 @@ __device__ void bitonic_pairs(double* kw, long long* ki, int n2, bool by_weight)
         }
 }
 
-__global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass)
+__global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass, int maxsig)
 {
     extern __shared__ unsigned char smem_raw[];
     double* sw = reinterpret_cast<double*>(smem_raw);
@@ -861,7 +872,7 @@ __global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass
         long long k = -1;
         for (long long i = 0; i < nc; i++) {
             cum += sw[i];
-            if (cum > sel->target) { k = i; break; }
+            if (cum > sel->target || (maxsig > 0 && i + 1 >= maxsig)) { k = i; break; }
         }
         if (k < 0) k = nc - 1;
         const double thr = sw[k];
@@ -1529,16 +1540,17 @@ void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStr
 {
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
+    const int maxsig = fine ? 0 : tb.maxsig;   // the reference's count only grows in the coarse pass
     k_sel_init<<<(w.n + 127) / 128, 128, 0, st>>>(w, fine, tb.adaptive_fraction);
-    k_select<<<w.n, 1024, 0, st>>>(w, fine);
+    k_select<<<w.n, 1024, 0, st>>>(w, fine, maxsig);
     for (int level = 1; level < 6; level++) {
         k_hist_level<<<grid, 256, HIST_SMEM, st>>>(tb, w, fine);
-        k_select<<<w.n, 1024, 0, st>>>(w, fine);
+        k_select<<<w.n, 1024, 0, st>>>(w, fine, maxsig);
     }
     k_gather<<<grid, 256, 0, st>>>(tb, w, fine);
-    k_final<<<w.n, 1024, 0, st>>>(w, fine, ipass);
+    k_final<<<w.n, 1024, 0, st>>>(w, fine, ipass, maxsig);
     k_gather_fast<<<grid, 256, 0, st>>>(tb, w, fine);
-    k_final_fast<<<w.n, 1024, FAST_SMEM, st>>>(w, fine, ipass);
+    k_final_fast<<<w.n, 1024, FAST_SMEM, st>>>(w, fine, ipass, maxsig);
 }
 
 }  // namespace
@@ -1576,7 +1588,7 @@ void estep_init_attributes()
 
 void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStream_t st)
 {
-    (void)maxsig;
+    (void)maxsig;   // tb.maxsig
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
     k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 0);

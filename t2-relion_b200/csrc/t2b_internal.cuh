@@ -97,6 +97,7 @@ constexpr int FAST_CAP = 4096;   // weights gathered by the fast selection path
 struct Tables {
     int s, xh, P, ori_size;
     int K, n_dir, n_psi, O, T, R, V, ovs, ref_dim;
+    int maxsig;               // maximum_significants of the coarse pass (<= 0: off)
     const float2* proj_c;     // K*O x P
     const float2* proj_f;     // K*O*R x P (ovs) else == proj_c
     const float2* ab_c;       // T x P phase factors

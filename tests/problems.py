@@ -4,7 +4,7 @@ import numpy as np
 from conftest import load_package
 
 
-def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=None, ref_dim=3):
+def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=None, ref_dim=3, maxsig=-1):
     t2b = load_package()
     import t2relion_b200.synthetic as sy
     import oracle as orc
@@ -38,7 +38,7 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
     prob = orc.Problem(ori_size=N, s=s, ref_dim=ref_dim, maps=maps, r_max=r, pad=2, samp=samp,
                        pdf_direction=pdf_dir, pdf_class=pdf_cls, sigma2_offset=sigma2_offset,
                        pixel_size=p["angpix"], adaptive_fraction=0.999, ovs=p["ovs"], bp_pad_size=ps,
-                       bp_r_max=r)
+                       bp_r_max=r, maximum_significants=maxsig)
     mres = sy.mresol(s)
     oparts = prob.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], mres)
 
@@ -50,7 +50,7 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
         es.configure(ori_size=N, current_size=s, ref_dim=ref_dim, nr_classes=nr_classes, samp=samp,
                      pdf_direction=pdf_dir, pdf_class=pdf_cls, sigma2_offset=sigma2_offset,
                      pixel_size=p["angpix"], adaptive_oversampling=p["ovs"], diff2_mode=diff2_mode,
-                     max_batch=max_batch or n_particles)
+                     max_batch=max_batch or n_particles, maximum_significants=maxsig)
         return es
 
     return dict(t2b=t2b, sy=sy, maps=maps, samp=samp, parts=parts, prob=prob, oparts=oparts,

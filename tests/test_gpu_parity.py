@@ -144,3 +144,28 @@ def test_splitbf16_matches_plain_with_many_tiles_per_cta():
     assert np.all(r0["status"] == 0) and np.all(r1["status"] == 0)
     assert np.max(np.abs(d1.astype(np.float64) - d0) / np.abs(d0)) <= 2 * DIFF2_RTOL
     assert np.mean(np.all(r0["pose"] == r1["pose"], axis=1)) >= 0.98
+
+
+@pytest.mark.parametrize("name,maxsig", [("refine_o2", 40), ("refine_o1_ovs", 25), ("refine_o2", 3000)],
+                         ids=["o2-maxsig40", "o1ovs-maxsig25", "o2-maxsig3000"])
+def test_maximum_significants_matches_oracle(name, maxsig):
+    """--maxsig: the coarse threshold is the weight of rank min(crossing, maxsig - 1)
+    (src/ml_optimiser.cpp:7945-7966); the fine pass is unaffected."""
+    pb = problems.build(name, n_particles=12, seed=41, diff2_mode=1, maxsig=maxsig)
+    P = pb["parts"]
+    es = pb["product"]()
+    res = es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    ores = pb["prob"].estep(pb["oparts"])
+    for b in range(4):
+        d2 = es.coarse_diff2(b).astype(np.float64)
+        mn = d2[d2 >= 0].min()
+        rc, wts, sw, sig, ns = pb["prob"].weights(pb["oparts"], b, 0, d2, np.arange(d2.size), mn)
+        assert rc == 0
+        assert res["nr_sign"][b] == ns and ns <= maxsig
+        assert res["coarse_sig_weight"][b] == pytest.approx(sig, rel=1e-12)
+        assert res["n_coarse_sig"][b] == int(np.sum(wts >= sig))
+    es.close()
+    assert np.all(res["status"] == 0)
+    assert np.all(res["nr_sign"] <= maxsig)
+    same = np.all(res["pose"] == ores["pose"], axis=1)
+    assert same.mean() >= 0.9, same.mean()
