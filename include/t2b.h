@@ -87,7 +87,7 @@ typedef struct t2b_config {
     int n_trans;               /* coarse translations                                 */
     int adaptive_oversampling; /* 0: single pass; 1: coarse + fine pass               */
     int nover_rot, nover_trans;/* oversampling factors of the fine pass (1 if none)   */
-    int maximum_significants;  /* <= 0: off (only 0/-1 supported)                     */
+    int maximum_significants;  /* > 0: cap of the coarse-pass significant samples (--maxsig) */
     int diff2_mode;            /* T2B_DIFF2_*                                         */
     int max_batch;             /* particles per t2b_estep_* call                      */
     int use_graph;             /* 1: t2b_estep_batch_device captures the batch into a CUDA
