@@ -163,7 +163,7 @@ int t2b_estep_batch_device(t2b_ctx* ctx, const t2b_batch* batch, const t2b_resul
  * double, host memory. */
 int t2b_reconstruct_divide(t2b_ctx* ctx, int iclass, double* fconv);
 
-/* M-step reconstruction of a 3D grid on the device (BackProjector::reconstruct,
+/* M-step reconstruction of a grid on the device (BackProjector::reconstruct,
  * src/backprojector.cpp:1344-1530, on the reference's default skip-gridding
  * path, followed by windowToOridimRealSpace :2486-2620 and
  * Projector::griddingCorrect, src/projector.cpp:489-522): decenter, optional
@@ -172,7 +172,8 @@ int t2b_reconstruct_divide(t2b_ctx* ctx, int iclass, double* fconv);
  * pad * ori_size, inverse 3D FFT (FP32), real-space window to ori_size,
  * normalisation for 2D particles (pad^3 ori_size), soft mask (radius ori/2,
  * width 3, average background), sinc^2 gridding correction.  vol: host,
- * ori_size^3 doubles [z][y][x], centre at ori_size/2.  pad * ori_size must be
+ * ori_size^3 doubles [z][y][x] (a 2D grid of 2D classification: ori_size^2,
+ * normalisation pad^2), centre at ori_size/2.  pad * ori_size must be
  * a product of 2, 3, 5 and <= 512.  The gridding iterations
  * (--dont_skip_gridding) are not implemented. */
 typedef struct t2b_recon_config {

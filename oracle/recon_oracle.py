@@ -4,7 +4,8 @@ TEST INFRASTRUCTURE ONLY: imported by tests/ as the checker of
 t2-relion_b200/csrc/recon.cu.  The shipped library never uses it.
 
 Restates in numpy, on a centred half-complex backprojection grid (data
-complex, weight real; z, y centred at -initz, -inity; x from 0):
+complex, weight real; z, y centred at -initz, -inity; x from 0; 3D grids of
+3D refinements or 2D grids of 2D classes):
 
   reconstruct_map   BackProjector::reconstruct (src/backprojector.cpp:1344-1530),
                     the skip-gridding path (the reference's default:
@@ -44,8 +45,11 @@ def _logical(shape, initz, inity):
 
 
 def decenter_divide(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_map=0):
-    """Fconv of the pad_size box (FFTW layout [ps][ps][ps/2+1]) after the MAP term and the
-    skip-gridding division, FP64."""
+    """Fconv of the pad_size box (FFTW layout [ps][ps][ps/2+1], 2D: [ps][ps/2+1]) after the MAP
+    term and the skip-gridding division, FP64."""
+    two_d = weight.ndim == 2
+    if two_d:
+        data, weight = data[None], weight[None]
     zd, yd, xd = weight.shape
     ps = yd
     fx = ps // 2 + 1
@@ -54,15 +58,16 @@ def decenter_divide(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_
     max_r2 = rp * rp
     k = np.arange(ps)
     kp = np.where(k < fx, k, k - ps)
-    KP, IP, JP = np.meshgrid(kp, kp, np.arange(fx), indexing="ij")
+    kz = np.zeros(1, np.int64) if two_d else kp
+    KP, IP, JP = np.meshgrid(kz, kp, np.arange(fx), indexing="ij")
     r2 = KP * KP + IP * IP + JP * JP
     inside = r2 <= max_r2
     zs, ys = KP - initz, IP - inity
-    F = np.zeros((ps, ps, fx), complex)
-    W = np.zeros((ps, ps, fx))
+    F = np.zeros(KP.shape, complex)
+    W = np.zeros(KP.shape)
     F[inside] = data[zs[inside], ys[inside], JP[inside]]
     W[inside] = weight[zs[inside], ys[inside], JP[inside]]
-    oc = float(pad) ** 3
+    oc = float(pad) ** (2 if two_d else 3)
     if tau2 is not None:
         m = r2 < max_r2
         ires = relion_round(np.sqrt(r2[m].astype(float)) / pad)
@@ -81,13 +86,18 @@ def decenter_divide(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_
     iall = np.floor(np.sqrt(r2.astype(float)) / pad).astype(int)
     wfin = np.maximum(W, rad[np.minimum(iall, r_max - 1)])
     out = np.where(wfin != 0, F / np.where(wfin != 0, wfin, 1.0), F)
-    return out
+    return out[0] if two_d else out
+
+
+def _radius(n, nd):
+    c = np.arange(n) - n // 2
+    if nd == 2:
+        return np.sqrt(c[:, None] ** 2 + c[None, :] ** 2)
+    return np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2)
 
 
 def soft_mask_bg(vol, radius, width):
-    n = vol.shape[0]
-    c = np.arange(n) - n // 2
-    r = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2)
+    r = _radius(vol.shape[0], vol.ndim)
     rp = radius + width
     rc = 0.5 + 0.5 * np.cos(PI * (rp - r) / width)
     edge = (r >= radius) & (r <= rp)
@@ -101,9 +111,13 @@ def soft_mask_bg(vol, radius, width):
 
 
 def reconstruct_map(data, weight, r_max, pad, ori_size, tau2=None, tau2_fudge=1.0, minres_map=0):
-    """Real-space map (ori_size^3, FP64) of the skip-gridding reconstruction."""
+    """Real-space map (ori_size^3, or ori_size^2 for a 2D grid; FP64) of the skip-gridding
+    reconstruction (2D particles)."""
+    nd = weight.ndim
     F = decenter_divide(data, weight, r_max, pad, tau2, tau2_fudge, minres_map)
-    ps = F.shape[0]
+    if nd == 2:
+        F = F[None]
+    ps = F.shape[1]
     N = int(relion_round(pad * ori_size))
     N += N % 2
     h = N // 2 + 1
@@ -115,20 +129,25 @@ def reconstruct_map(data, weight, r_max, pad, ori_size, tau2=None, tau2_fudge=1.
     ok = (kp >= -half) & (kp <= half)
     src = np.where(kp < 0, kp + ps, kp)
     jj = np.arange(h)
-    sel = ok[:, None, None] & ok[None, :, None] & (jj <= half)[None, None, :]
+    kz, okz, srcz = (np.zeros(1, np.int64), np.ones(1, bool), np.zeros(1, np.int64)) if nd == 2 else (kp, ok, src)
+    sel = okz[:, None, None] & ok[None, :, None] & (jj <= half)[None, None, :]
     if N > ps:
-        sel &= (kp[:, None, None] ** 2 + kp[None, :, None] ** 2 + jj[None, None, :] ** 2) <= half * half
-    Z, Y, X = np.broadcast_arrays(src[:, None, None], src[None, :, None], np.minimum(jj, half)[None, None, :])
-    G = np.zeros((N, N, h), complex)
+        sel &= (kz[:, None, None] ** 2 + kp[None, :, None] ** 2 + jj[None, None, :] ** 2) <= half * half
+    Z, Y, X = np.broadcast_arrays(srcz[:, None, None], src[None, :, None], np.minimum(jj, half)[None, None, :])
+    G = np.zeros(sel.shape, complex)
     G[sel] = F[Z[sel], Y[sel], X[sel]]
-    sign = np.where(((k[:, None, None] ^ k[None, :, None] ^ jj[None, None, :]) & 1) != 0, -1.0, 1.0)
+    kk = np.arange(G.shape[0])
+    sign = np.where(((kk[:, None, None] ^ k[None, :, None] ^ jj[None, None, :]) & 1) != 0, -1.0, 1.0)
     G = G * sign
-    big = np.fft.irfftn(G, s=(N, N, N), axes=(0, 1, 2)) * float(N) ** 3
     o0 = N // 2 - ori_size // 2
-    vol = big[o0:o0 + ori_size, o0:o0 + ori_size, o0:o0 + ori_size] / (float(pad) ** 3 * ori_size)
+    if nd == 3:
+        big = np.fft.irfftn(G, s=(N, N, N), axes=(0, 1, 2)) * float(N) ** 3
+        vol = big[o0:o0 + ori_size, o0:o0 + ori_size, o0:o0 + ori_size] / (float(pad) ** 3 * ori_size)
+    else:
+        big = np.fft.irfftn(G[0], s=(N, N), axes=(0, 1)) * float(N) ** 2
+        vol = big[o0:o0 + ori_size, o0:o0 + ori_size] / float(pad) ** 2
     vol = soft_mask_bg(vol, ori_size / 2.0, 3.0)
-    c = np.arange(ori_size) - ori_size // 2
-    r = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2)
+    r = _radius(ori_size, nd)
     rval = r / (ori_size * pad)
     with np.errstate(invalid="ignore", divide="ignore"):
         sinc = np.where(r > 0, np.sin(PI * rval) / (PI * np.where(r > 0, rval, 1.0)), 1.0)
@@ -136,30 +155,35 @@ def reconstruct_map(data, weight, r_max, pad, ori_size, tau2=None, tau2_fudge=1.
 
 
 def downsampled_average(data, weight, r_max, pad):
+    two_d = weight.ndim == 2
+    if two_d:
+        data, weight = data[None], weight[None]
     zd, yd, xd = weight.shape
     K, I, J = _logical(weight.shape, -(zd // 2), -(yd // 2))
     K, I, J = np.broadcast_arrays(K, I, J)
     ds = 2 * (r_max + 1) + 1
     dh = ds // 2
-    kp = relion_round(K / pad) + dh
+    nzb = 1 if two_d else ds
+    kp = np.zeros_like(K) if two_d else relion_round(K / pad) + dh
     ip = relion_round(I / pad) + dh
     jp = relion_round(J / pad)
     idx = (kp * ds + ip) * (dh + 1) + jp
-    n = ds * ds * (dh + 1)
+    n = nzb * ds * (dh + 1)
     ar = np.bincount(idx.ravel(), data.real.ravel(), n)
     ai = np.bincount(idx.ravel(), data.imag.ravel(), n)
     w = np.bincount(idx.ravel(), weight.ravel(), n)
     avg = np.where(w > 0, (ar + 1j * ai) / np.where(w > 0, w, 1.0), 0.0)
-    return avg.reshape(ds, ds, dh + 1)
+    return avg.reshape(nzb, ds, dh + 1)
 
 
 def downsampled_fsc(data1, w1, data2, w2, r_max, pad, ori_size):
     a1 = downsampled_average(data1, w1, r_max, pad)
     a2 = downsampled_average(data2, w2, r_max, pad)
-    ds = a1.shape[0]
+    ds = a1.shape[1]
     dh = ds // 2
     c = np.arange(ds) - dh
-    R = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + np.arange(dh + 1)[None, None, :] ** 2)
+    kz = np.zeros(1) if a1.shape[0] == 1 else c
+    R = np.sqrt(kz[:, None, None] ** 2 + c[None, :, None] ** 2 + np.arange(dh + 1)[None, None, :] ** 2)
     m = R <= r_max
     idx = relion_round(R[m])
     nb = ori_size // 2 + 1
@@ -174,21 +198,22 @@ def downsampled_fsc(data1, w1, data2, w2, r_max, pad, ori_size):
 def update_ssnr(weight, r_max, pad, ori_size, tau2_fudge, tau2, fsc, avgctf2=None, update_tau2_with_fsc=True,
                 is_whole_instead_of_half=False, correct_tau2_by_avgctf2=False):
     """Returns tau2, sigma2, data_vs_prior, fourier_coverage (FP64)."""
-    zd, yd, xd = weight.shape
-    K, I, J = np.broadcast_arrays(*_logical(weight.shape, -(zd // 2), -(yd // 2)))
+    two_d = weight.ndim == 2
+    w3 = weight[None] if two_d else weight
+    zd, yd, xd = w3.shape
+    K, I, J = np.broadcast_arrays(*_logical(w3.shape, -(zd // 2), -(yd // 2)))
     r2 = K * K + I * I + J * J
     rp = int(relion_round(r_max * pad))
     m = r2 < rp * rp
     ires = relion_round(np.sqrt(r2[m].astype(float)) / pad)
     nb = ori_size // 2 + 1
-    oc = float(pad) ** 3
-    wv = weight[m]
+    oc = float(pad) ** (2 if two_d else 3)
+    wv = w3[m]
     s2 = np.bincount(ires, oc * wv, nb)
     cnt = np.bincount(ires, minlength=nb).astype(float)
     sigma2 = np.where(s2 > 1e-10, cnt / np.where(s2 > 1e-10, s2, 1.0), 0.0)
     tau2 = np.array(tau2, float).copy()
     dvp = np.zeros(nb)
-    cov = np.zeros(nb)
     if update_tau2_with_fsc:
         myfsc = np.maximum(0.001, np.asarray(fsc, float))
         if is_whole_instead_of_half:

@@ -401,6 +401,9 @@ class EStep:
         xdim, ydim = pad_size // 2 + 1, pad_size
         zdim = pad_size if ref_dim == 3 else 1
         self._grid_shape = (zdim, ydim, xdim) if ref_dim == 3 else (ydim, xdim)
+        if not hasattr(self, "_grid_dims"):
+            self._grid_dims = {}
+        self._grid_dims[iclass] = ref_dim
         _check(lib.t2b_backprojector_init(self._h, iclass, ref_dim, xdim, ydim, zdim, -(ydim // 2),
                                           -(zdim // 2) if ref_dim == 3 else 0, r_max, padding_factor))
 
@@ -489,10 +492,10 @@ class EStep:
 
     # ---------------------------------------------- M-step reconstruction
     def reconstruct(self, iclass, ori_size, tau2=None, tau2_fudge=1.0, minres_map=0):
-        """t2b_reconstruct: the real-space map (ori_size^3, FP64) of grid `iclass`."""
+        """t2b_reconstruct: the real-space map (ori_size^3, or ori_size^2 of a 2D class; FP64) of grid `iclass`."""
         t = None if tau2 is None else np.ascontiguousarray(tau2, np.float64)
         cfg = ReconConfig(ori_size, 0 if t is None else 1, minres_map, 0, tau2_fudge, _ptr(t))
-        vol = np.zeros((ori_size,) * 3)
+        vol = np.zeros((ori_size,) * getattr(self, "_grid_dims", {}).get(iclass, 3))
         _check(lib.t2b_reconstruct(self._h, iclass, ctypes.byref(cfg), _ptr(vol)))
         return vol
 

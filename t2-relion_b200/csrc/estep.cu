@@ -1453,8 +1453,8 @@ __global__ void k_decenter(Volume g, const float2* __restrict__ data, const floa
                            double2* __restrict__ fconv, double* __restrict__ fw, double* rad, double* cnt,
                            const double* __restrict__ tau2, double tscale, int minres_map)
 {
-    const int ps = g.ydim, fx = ps / 2 + 1;
-    const long long total = (long long)ps * ps * fx;
+    const int ps = g.ydim, fx = ps / 2 + 1, nz = g.ref_dim == 3 ? ps : 1;   // 2D grids: one plane
+    const long long total = (long long)nz * ps * fx;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= total) return;
     const int j = (int)(n % fx);
@@ -1496,8 +1496,8 @@ __global__ void k_radnorm(int r_max, double* rad, const double* cnt)
 
 __global__ void k_divide(Volume g, double2* __restrict__ fconv, const double* __restrict__ fw, const double* rad)
 {
-    const int ps = g.ydim, fx = ps / 2 + 1;
-    const long long total = (long long)ps * ps * fx;
+    const int ps = g.ydim, fx = ps / 2 + 1, nz = g.ref_dim == 3 ? ps : 1;
+    const long long total = (long long)nz * ps * fx;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= total) return;
     const int j = (int)(n % fx);
@@ -1634,8 +1634,8 @@ void launch_reconstruct(const Volume& g, const float2* data, const float* weight
                         double* fw, double* rad, double* cnt, cudaStream_t st, const double* tau2, double tscale,
                         int minres_map)
 {
-    const int ps = g.ydim, fx = ps / 2 + 1;
-    const long long total = (long long)ps * ps * fx;
+    const int ps = g.ydim, fx = ps / 2 + 1, nz = g.ref_dim == 3 ? ps : 1;
+    const long long total = (long long)nz * ps * fx;
     T2B_CUDA(cudaMemsetAsync(rad, 0, sizeof(double) * g.r_max, st));
     T2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(double) * g.r_max, st));
     const int nb = (int)((total + 255) / 256);

@@ -44,10 +44,10 @@ __device__ __forceinline__ int rround(double x) { return x > 0 ? (int)(x + 0.5) 
 // the pad_size transform (FFTW layout, double2) -> the N = pad * ori_size half
 // transform (float2), windowed (shrink: every output element; enlarge: input
 // elements with r^2 <= (ps/2)^2) and centred by sign
-__global__ void k_window(const double2* __restrict__ fc, int ps, int N, float2* __restrict__ G)
+__global__ void k_window(const double2* __restrict__ fc, int ps, int N, int dim, float2* __restrict__ G)
 {
     const int h = N / 2 + 1, half = ps / 2, fx = ps / 2 + 1;
-    const long long total = (long long)N * N * h;
+    const long long total = (long long)(dim == 3 ? N : 1) * N * h;   // 2D: one plane
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(n % h);
         const int i = (int)((n / h) % N);
@@ -96,11 +96,12 @@ __global__ void __launch_bounds__(RC_THREADS) k_cols3(float2* __restrict__ G, in
 }
 
 // c2r rows (imaginary parts of x = 0 and N/2 dropped) of the real-space window:
-// row (z0 + zw, z0 + yw) -> vol[zw][yw][0..ori), divided by the FFT normalisation
+// row (z0 + zw, z0 + yw) -> vol[zw][yw][0..ori) (2D: row z0 + yw of the single plane),
+// divided by the FFT normalisation
 template <int NC>
 __global__ void __launch_bounds__(RC_THREADS) k_rows3(const float2* __restrict__ G, int Nrt, int ori, int z0,
                                                       float norm, const float2* __restrict__ tw, FftPlan plan,
-                                                      float* __restrict__ vol)
+                                                      float* __restrict__ vol, int dim)
 {
     extern __shared__ float2 sm[];
     const int N = NC > 0 ? NC : Nrt, h = N / 2 + 1;
@@ -109,12 +110,13 @@ __global__ void __launch_bounds__(RC_THREADS) k_rows3(const float2* __restrict__
     float2* B = A + RC_ROWS * N;
     for (int t = threadIdx.x; t < N; t += blockDim.x) s_tw[t] = tw[t];
     const int row0 = blockIdx.x * RC_ROWS;
+    const int nrows = dim == 3 ? ori * ori : ori;
     for (int e = threadIdx.x; e < RC_ROWS * N; e += blockDim.x) {
         const int rr = e / N, k = e - rr * N, row = row0 + rr;
         float2 v = make_float2(0.f, 0.f);
-        if (row < ori * ori) {
+        if (row < nrows) {
             const int zw = row / ori, yw = row - zw * ori;
-            const float2* g = G + (((size_t)z0 + zw) * N + z0 + yw) * h;
+            const float2* g = G + ((dim == 3 ? (size_t)z0 + zw : (size_t)0) * N + z0 + yw) * h;
             if (k == 0 || k == N / 2) v = make_float2(g[k].x, 0.f);
             else if (k < N / 2) v = g[k];
             else v = make_float2(g[N - k].x, -g[N - k].y);
@@ -125,21 +127,21 @@ __global__ void __launch_bounds__(RC_THREADS) k_rows3(const float2* __restrict__
     const float2* r = fft_any<NC, true>(A, B, RC_ROWS, plan, s_tw);
     for (int e = threadIdx.x; e < RC_ROWS * ori; e += blockDim.x) {
         const int rr = e / ori, x = e - rr * ori, row = row0 + rr;
-        if (row < ori * ori) vol[(size_t)row * ori + x] = r[rr * N + z0 + x].x / norm;
+        if (row < nrows) vol[(size_t)row * ori + x] = r[rr * N + z0 + x].x / norm;
     }
 }
 
 // soft-mask background (softMaskOutsideMap without a noise image), fixed-order FP64
 // partial sums per block
-__global__ void __launch_bounds__(RC_THREADS) k_mask_partial(const float* __restrict__ vol, int ori, double radius,
-                                                             double width, double2* __restrict__ part)
+__global__ void __launch_bounds__(RC_THREADS) k_mask_partial(const float* __restrict__ vol, int ori, int dim,
+                                                             double radius, double width, double2* __restrict__ part)
 {
     __shared__ double sw[RC_THREADS], sv[RC_THREADS];
-    const long long total = (long long)ori * ori * ori;
+    const long long total = (long long)ori * ori * (dim == 3 ? ori : 1);
     double aw = 0., av = 0.;
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(n % ori), y = (int)((n / ori) % ori), z = (int)(n / ((long long)ori * ori));
-        const double xl = x - ori / 2, yl = y - ori / 2, zl = z - ori / 2;
+        const double xl = x - ori / 2, yl = y - ori / 2, zl = dim == 3 ? z - ori / 2 : 0;
         const double r = sqrt(xl * xl + yl * yl + zl * zl);
         if (r < radius) continue;
         const double rp = radius + width;
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(RC_THREADS) k_mask_partial(const float* __rest
 }
 
 // soft mask with the background, then the gridding correction (trilinear: sinc^2)
-__global__ void k_mask_grid(const float* __restrict__ vol, int ori, int pad, double radius, double width,
+__global__ void k_mask_grid(const float* __restrict__ vol, int ori, int dim, int pad, double radius, double width,
                             const double2* __restrict__ part, int nparts, double* __restrict__ out)
 {
     __shared__ double s_bg;
@@ -175,10 +177,10 @@ __global__ void k_mask_grid(const float* __restrict__ vol, int ori, int pad, dou
     }
     __syncthreads();
     const double bg = s_bg;
-    const long long total = (long long)ori * ori * ori;
+    const long long total = (long long)ori * ori * (dim == 3 ? ori : 1);
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(n % ori), y = (int)((n / ori) % ori), z = (int)(n / ((long long)ori * ori));
-        const double xl = x - ori / 2, yl = y - ori / 2, zl = z - ori / 2;
+        const double xl = x - ori / 2, yl = y - ori / 2, zl = dim == 3 ? z - ori / 2 : 0;
         const double r = sqrt(xl * xl + yl * yl + zl * zl);
         double v = vol[n];
         if (r >= radius) {
@@ -206,9 +208,10 @@ __global__ void k_downsample(Volume g, const float2* __restrict__ data, const fl
     const long long total = (long long)g.zdim * g.ydim * g.xdim;
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(n % g.xdim), i = (int)((n / g.xdim) % g.ydim), k = (int)(n / ((long long)g.xdim * g.ydim));
-        const int kp = rround((double)(k + g.initz) / g.pad) + dh, ip = rround((double)(i + g.inity) / g.pad) + dh;
+        const int kp = g.ref_dim == 3 ? rround((double)(k + g.initz) / g.pad) + dh : 0;   // 2D: one plane
+        const int ip = rround((double)(i + g.inity) / g.pad) + dh;
         const int jp = rround((double)j / g.pad);
-        if (kp < 0 || kp >= ds || ip < 0 || ip >= ds || jp > dh) continue;   // a grid larger than pad_size
+        if (kp < 0 || kp >= (g.ref_dim == 3 ? ds : 1) || ip < 0 || ip >= ds || jp > dh) continue;   // a grid larger than pad_size
         const size_t b = (((size_t)kp * ds + ip) * (dh + 1) + jp) * 3;
         const float2 d = data[n];
         const float w = weight[n];
@@ -231,15 +234,16 @@ __device__ __forceinline__ void shell_flush(const double* sb, int n, double* acc
         if (sb[i] != 0.) atomicAdd(&acc[i], sb[i]);
 }
 
-__global__ void k_fsc_shells(int r_max, int nb, const double* __restrict__ a1, const double* __restrict__ a2,
+__global__ void k_fsc_shells(int r_max, int nb, int dim, const double* __restrict__ a1, const double* __restrict__ a2,
                              double* __restrict__ sh /* nb x 3 */)
 {
     extern __shared__ double sb[];
     shell_init(sb, 3 * nb);
     const int ds = 2 * (r_max + 1) + 1, dh = ds / 2;
-    const long long total = (long long)ds * ds * (dh + 1);
+    const long long total = (long long)(dim == 3 ? ds : 1) * ds * (dh + 1);
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(n % (dh + 1)), i = (int)((n / (dh + 1)) % ds) - dh, k = (int)(n / ((long long)(dh + 1) * ds)) - dh;
+        const int j = (int)(n % (dh + 1)), i = (int)((n / (dh + 1)) % ds) - dh;
+        const int k = dim == 3 ? (int)(n / ((long long)(dh + 1) * ds)) - dh : 0;
         const double R = sqrt((double)(k * k + i * i + j * j));
         if (R > r_max) continue;
         const int idx = rround(R);
@@ -318,7 +322,7 @@ struct DevBuf {
 };
 
 using ColKernel = void (*)(float2*, int, int, int, const float2*, FftPlan);
-using RowKernel = void (*)(const float2*, int, int, int, float, const float2*, FftPlan, float*);
+using RowKernel = void (*)(const float2*, int, int, int, float, const float2*, FftPlan, float*, int);
 
 void recon_kernels(int N, ColKernel& col, RowKernel& row)
 {
@@ -336,7 +340,7 @@ const Volume& grid_volume(t2b_ctx* c, int ig)
 {
     T2B_REQUIRE(ig >= 0 && ig < (int)c->gvol.size() && c->gdata[ig], T2B_ERR_ARG, "no such grid");
     const Volume& v = c->gvol[ig];
-    T2B_REQUIRE(v.ref_dim == 3, T2B_ERR_UNSUPPORTED, "the reconstruction is implemented for 3D grids");
+    T2B_REQUIRE(v.ref_dim == 3 || v.ref_dim == 2, T2B_ERR_UNSUPPORTED, "grids are 2D or 3D");
     return v;
 }
 
@@ -362,25 +366,26 @@ int t2b_reconstruct(t2b_ctx* c, int iclass, const t2b_recon_config* cf, double* 
         N += N % 2;
         T2B_REQUIRE(N <= 512, T2B_ERR_UNSUPPORTED, "pad * ori_size must be <= 512");
         const FftPlan plan = fft_plan(N);
+        const int dim = v.ref_dim;
         const int ps = v.ydim, fx = ps / 2 + 1, h = N / 2 + 1;
-        const size_t nps = (size_t)ps * ps * fx;
+        const size_t nps = (size_t)(dim == 3 ? ps : 1) * ps * fx;
         cudaStream_t st = c->stream;
         DevBuf<double2> fc(nps);
         DevBuf<double> fw(nps), rad(2 * (size_t)v.r_max), t2(ori / 2 + 1);
         if (cf->do_map)
             T2B_CUDA(cudaMemcpyAsync(t2.p, cf->tau2, (ori / 2 + 1) * sizeof(double), cudaMemcpyHostToDevice, st));
-        const double tscale = (double)pad * pad * pad * cf->tau2_fudge;
+        const double tscale = (dim == 3 ? (double)pad * pad * pad : (double)pad * pad) * cf->tau2_fudge;
         launch_reconstruct(v, c->gdata[iclass], c->gweight[iclass], fc.p, fw.p, rad.p, rad.p + v.r_max, st,
                            cf->do_map ? t2.p : nullptr, tscale, cf->minres_map);
         // window + centre by sign, inverse 3D FFT, real-space window
-        DevBuf<float2> G((size_t)N * N * h), tw(N);
+        DevBuf<float2> G((size_t)(dim == 3 ? N : 1) * N * h), tw(N);
         std::vector<float2> htw(N);
         for (int t = 0; t < N; ++t) {
             const double a = -2.0 * PI_R * (double)t / (double)N;
             htw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
         }
         T2B_CUDA(cudaMemcpyAsync(tw.p, htw.data(), N * sizeof(float2), cudaMemcpyHostToDevice, st));
-        k_window<<<grid_of((long long)N * N * h), RC_THREADS, 0, st>>>(fc.p, ps, N, G.p);
+        k_window<<<grid_of((long long)(dim == 3 ? N : 1) * N * h), RC_THREADS, 0, st>>>(fc.p, ps, N, dim, G.p);
         ColKernel col;
         RowKernel row;
         recon_kernels(N, col, row);
@@ -389,18 +394,24 @@ int t2b_reconstruct(t2b_ctx* c, int iclass, const t2b_recon_config* cf, double* 
         T2B_CUDA(cudaFuncSetAttribute((const void*)col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc));
         T2B_CUDA(cudaFuncSetAttribute((const void*)row, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr));
         const int z0 = N / 2 - ori / 2, xt = (h + RC_CX - 1) / RC_CX;
-        col<<<dim3(N, xt), RC_THREADS, smc, st>>>(G.p, N, 0, 0, tw.p, plan);              // along z, every (y, x)
-        col<<<dim3(ori, xt), RC_THREADS, smc, st>>>(G.p, N, 1, z0, tw.p, plan);           // along y, window planes
-        DevBuf<float> vol((size_t)ori * ori * ori);
-        const float norm = (float)((double)pad * pad * pad * ori);                        // 2D particles
-        row<<<(ori * ori + RC_ROWS - 1) / RC_ROWS, RC_THREADS, smr, st>>>(G.p, N, ori, z0, norm, tw.p, plan, vol.p);
+        if (dim == 3) {
+            col<<<dim3(N, xt), RC_THREADS, smc, st>>>(G.p, N, 0, 0, tw.p, plan);          // along z, every (y, x)
+            col<<<dim3(ori, xt), RC_THREADS, smc, st>>>(G.p, N, 1, z0, tw.p, plan);       // along y, window planes
+        } else {
+            col<<<dim3(1, xt), RC_THREADS, smc, st>>>(G.p, N, 1, 0, tw.p, plan);          // along y, the one plane
+        }
+        const long long nv = (long long)ori * ori * (dim == 3 ? ori : 1);
+        DevBuf<float> vol(nv);
+        // normalisation of windowToOridimRealSpace for 2D particles: pad^3 ori (3D maps), pad^2 (2D)
+        const float norm = dim == 3 ? (float)((double)pad * pad * pad * ori) : (float)((double)pad * pad);
+        const int nrows = dim == 3 ? ori * ori : ori;
+        row<<<(nrows + RC_ROWS - 1) / RC_ROWS, RC_THREADS, smr, st>>>(G.p, N, ori, z0, norm, tw.p, plan, vol.p, dim);
         // soft mask (radius ori/2, width 3, average background) and gridding correction
-        const long long nv = (long long)ori * ori * ori;
         const int nb = grid_of(nv);
         DevBuf<double2> part(nb);
         DevBuf<double> out(nv);
-        k_mask_partial<<<nb, RC_THREADS, 0, st>>>(vol.p, ori, ori / 2.0, 3.0, part.p);
-        k_mask_grid<<<nb, RC_THREADS, 0, st>>>(vol.p, ori, pad, ori / 2.0, 3.0, part.p, nb, out.p);
+        k_mask_partial<<<nb, RC_THREADS, 0, st>>>(vol.p, ori, dim, ori / 2.0, 3.0, part.p);
+        k_mask_grid<<<nb, RC_THREADS, 0, st>>>(vol.p, ori, dim, pad, ori / 2.0, 3.0, part.p, nb, out.p);
         T2B_CUDA(cudaGetLastError());
         T2B_CUDA(cudaMemcpyAsync(vol_out, out.p, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
         T2B_CUDA(cudaStreamSynchronize(st));
@@ -415,12 +426,13 @@ int t2b_fsc_halves(t2b_ctx* c, int grid_a, int grid_b, int ori_size, double* fsc
         DeviceGuard dg(c->device);
         const Volume& a = grid_volume(c, grid_a);
         const Volume& b = grid_volume(c, grid_b);
-        T2B_REQUIRE(a.xdim == b.xdim && a.ydim == b.ydim && a.zdim == b.zdim && a.r_max == b.r_max && a.pad == b.pad,
+        T2B_REQUIRE(a.xdim == b.xdim && a.ydim == b.ydim && a.zdim == b.zdim && a.r_max == b.r_max && a.pad == b.pad &&
+                        a.ref_dim == b.ref_dim,
                     T2B_ERR_ARG, "the two grids differ in shape");
         T2B_REQUIRE(a.r_max <= ori_size / 2, T2B_ERR_ARG, "r_max exceeds ori_size / 2");
         const int ds = 2 * (a.r_max + 1) + 1, dh = ds / 2, nb = ori_size / 2 + 1;
         T2B_REQUIRE(nb <= 1024, T2B_ERR_ARG, "ori_size too large");
-        const size_t bins = (size_t)ds * ds * (dh + 1);
+        const size_t bins = (size_t)(a.ref_dim == 3 ? ds : 1) * ds * (dh + 1);
         cudaStream_t st = c->stream;
         DevBuf<double> aa(3 * bins), ab(3 * bins), sh(3 * (size_t)nb);
         T2B_CUDA(cudaMemsetAsync(aa.p, 0, 3 * bins * sizeof(double), st));
@@ -429,8 +441,8 @@ int t2b_fsc_halves(t2b_ctx* c, int grid_a, int grid_b, int ori_size, double* fsc
         const long long nvox = (long long)a.zdim * a.ydim * a.xdim;
         k_downsample<<<grid_of(nvox), RC_THREADS, 0, st>>>(a, c->gdata[grid_a], c->gweight[grid_a], aa.p);
         k_downsample<<<grid_of(nvox), RC_THREADS, 0, st>>>(b, c->gdata[grid_b], c->gweight[grid_b], ab.p);
-        k_fsc_shells<<<grid_of((long long)bins), RC_THREADS, 3 * nb * sizeof(double), st>>>(a.r_max, nb, aa.p, ab.p,
-                                                                                             sh.p);
+        k_fsc_shells<<<grid_of((long long)bins), RC_THREADS, 3 * nb * sizeof(double), st>>>(a.r_max, nb, a.ref_dim, aa.p,
+                                                                                             ab.p, sh.p);
         T2B_CUDA(cudaGetLastError());
         std::vector<double> h(3 * (size_t)nb);
         T2B_CUDA(cudaMemcpyAsync(h.data(), sh.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -455,7 +467,7 @@ int t2b_update_ssnr(t2b_ctx* c, int iclass, const t2b_ssnr_config* cf, double* t
         const Volume& v = grid_volume(c, iclass);
         const int nb = cf->ori_size / 2 + 1;
         T2B_REQUIRE(v.r_max < nb && nb <= 1024, T2B_ERR_ARG, "r_max exceeds ori_size / 2 (or ori_size too large)");
-        const double oc = (double)v.pad * v.pad * v.pad;
+        const double oc = v.ref_dim == 3 ? (double)v.pad * v.pad * v.pad : (double)v.pad * v.pad;
         cudaStream_t st = c->stream;
         DevBuf<double> acc(3 * (size_t)nb), t2d(nb), actf(nb);
         const long long nvox = (long long)v.zdim * v.ydim * v.xdim;

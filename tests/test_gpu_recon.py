@@ -91,3 +91,46 @@ def test_ssnr_matches_oracle(two_classes, with_fsc):
                          update_tau2_with_fsc=with_fsc)
     for g, rr in zip(got, ref):
         assert np.allclose(g, rr, rtol=1e-9, atol=1e-14)
+
+
+@pytest.fixture(scope="module")
+def classes_2d():
+    pb = problems.build("class2d", n_particles=24, seed=37, nr_classes=2)
+    P = pb["parts"]
+    es = pb["product"]()
+    es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    pb["es"] = es
+    pb["grids"] = [es.get_backprojector(k) for k in range(2)]
+    yield pb
+    es.close()
+
+
+@pytest.mark.parametrize("with_map", [False, True], ids=["plain", "map_tau2"])
+def test_2d_class_reconstruction_matches_oracle(classes_2d, with_map):
+    pb, es = classes_2d, classes_2d["es"]
+    N, r = pb["N"], pb["r"]
+    for k in range(2):
+        data, w = pb["grids"][k]
+        assert w.ndim == 2
+        tau2 = np.random.default_rng(9).uniform(0.5, 2.0, N // 2 + 1) * np.mean(w) if with_map else None
+        got = es.reconstruct(k, N, tau2=tau2, tau2_fudge=2.0, minres_map=1)
+        assert got.shape == (N, N)
+        ref = ro.reconstruct_map(data.astype(np.complex128), w.astype(np.float64), r, 2, N, tau2=tau2,
+                                 tau2_fudge=2.0, minres_map=1)
+        _map_close(got, ref)
+
+
+def test_2d_fsc_and_ssnr_match_oracle(classes_2d):
+    pb, es = classes_2d, classes_2d["es"]
+    N, r = pb["N"], pb["r"]
+    (d1, w1), (d2, w2) = pb["grids"]
+    got = es.fsc_halves(0, 1, N)
+    ref = ro.downsampled_fsc(d1.astype(np.complex128), w1.astype(np.float64), d2.astype(np.complex128),
+                             w2.astype(np.float64), r, 2, N)
+    assert np.allclose(got, ref, rtol=1e-9, atol=1e-12)
+    nb = N // 2 + 1
+    tau2 = np.random.default_rng(8).uniform(0.1, 1.0, nb) * np.mean(w1)
+    g = es.update_ssnr(0, N, tau2, tau2_fudge=1.5, fsc=got)
+    rr = ro.update_ssnr(w1.astype(np.float64), r, 2, N, 1.5, tau2, got)
+    for a, b in zip(g, rr):
+        assert np.allclose(a, b, rtol=1e-9, atol=1e-14)

@@ -105,3 +105,35 @@ def test_ssnr_arrays_against_direct_sums():
     assert np.allclose(dvp, f / (1 - f) * 1.5, rtol=1e-12)
     assert np.allclose(t, f / (1 - f) * 1.5 * s2, rtol=1e-12)
     assert np.all((cov >= 0) & (cov <= 1))
+
+
+@pytest.mark.parametrize("ori,r_max", [(32, 16), (32, 8)], ids=["shrink", "enlarge"])
+def test_reconstruction_of_a_known_image_2d(synth, ori, r_max):
+    """2D classes: the padded Fourier map of a band-limited image with weight 1 gives the
+    image itself (normalisation pad^2 of 2D maps from 2D particles) over sinc^2, low-passed
+    at r_max."""
+    img = synth.blob_volume(ori, 6, sigma=(2.5, 4.0), seed=5, ndim=2)
+    m = 2 * ori
+    big0 = np.zeros((m, m))
+    big0[ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori] = img
+    F0 = np.fft.rfft2(np.fft.ifftshift(big0)) / float(ori) ** 2
+    ps = 2 * (2 * r_max + 1) + 1
+    kk = np.arange(ps) - ps // 2
+    KY, KX = np.meshgrid(kk, np.arange(ps // 2 + 1), indexing="ij")
+    keep = KY * KY + KX * KX <= (2 * r_max) ** 2
+    fmap = np.where(keep, F0[KY % m, np.minimum(KX, m // 2)], 0)
+    got = ro.reconstruct_map(fmap, np.ones(fmap.shape), r_max, 2, ori)
+    assert got.shape == (ori, ori)
+    big = np.zeros((m, m))
+    big[ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori] = img
+    F = np.fft.rfft2(np.fft.ifftshift(big))
+    k = np.fft.fftfreq(m) * m
+    r2 = k[:, None] ** 2 + np.arange(m // 2 + 1)[None, :] ** 2
+    F[r2 > (2 * r_max) ** 2] = 0
+    lp = np.fft.fftshift(np.fft.irfft2(F, s=(m, m)))[ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori]
+    c = np.arange(ori) - ori // 2
+    r = np.sqrt(c[:, None] ** 2 + c[None, :] ** 2)
+    rv = r / (2 * ori)
+    sinc = np.where(r > 0, np.sin(np.pi * rv) / (np.pi * np.where(r > 0, rv, 1)), 1.0)
+    want = ro.soft_mask_bg(lp, ori / 2.0, 3.0) / (sinc * sinc)
+    assert np.max(np.abs(got - want)) <= 1e-10 * np.max(np.abs(want))
