@@ -535,8 +535,13 @@ static int replay_graph(t2b_ctx* c, Work& w, cudaStream_t st, const std::vector<
         T2B_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
         int kn = 0;
         for (auto nd : nodes) {
+            // this runtime reports conditional nodes (the selection's multi-level search) as an
+            // error: they are not kernel nodes either way
             cudaGraphNodeType ty;
-            T2B_CUDA(cudaGraphNodeGetType(nd, &ty));
+            if (cudaGraphNodeGetType(nd, &ty) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
             if (ty == cudaGraphNodeTypeKernel) kn++;
         }
         const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);

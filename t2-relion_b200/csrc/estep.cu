@@ -18,6 +18,7 @@
 //             prior sums, then trilinear backprojection with float2 atomics
 //             (src/ml_optimiser.cpp:8153-8700, src/backprojector.cpp:55-230)
 #include "t2b_internal.cuh"
+#include <map>
 #include <algorithm>
 #include <cfloat>
 
@@ -537,7 +538,9 @@ __global__ void k_sel_init(Work w, int fine, double frac)
 // maxsig > 0 (coarse pass only, src/ml_optimiser.cpp:7945-7966): the walk also stops at
 // the maxsig-th largest weight, so the threshold is the weight at rank
 // min(crossing, maxsig - 1)
-__global__ void __launch_bounds__(1024) k_select(Work w, int fine, int maxsig)
+// cond (non-zero during graph capture, level 0 only): set when a particle still needs the
+// multi-level search or the candidate gather, the condition of the graph node that holds them
+__global__ void __launch_bounds__(1024) k_select(Work w, int fine, int maxsig, cudaGraphConditionalHandle cond)
 {
     __shared__ double ssum[1024];
     __shared__ unsigned long long scnt[1024];
@@ -613,6 +616,7 @@ __global__ void __launch_bounds__(1024) k_select(Work w, int fine, int maxsig)
     }
     if (pos < 0 && threadIdx.x == 0) { sel->phase = 3; w.status[b] = T2B_ERR_NOSIGNIF; }
     __syncthreads();
+    if (cond && threadIdx.x == 0 && (sel->phase == 0 || sel->phase == 1)) cudaGraphSetConditional(cond, 1u);
     for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
 }
 
@@ -1536,19 +1540,70 @@ int grid_x_for(int nb)
 const size_t HIST_SMEM = HIST_BINS * (sizeof(unsigned) + sizeof(double));
 const size_t FAST_SMEM = FAST_CAP * (sizeof(double) + sizeof(long long));
 
+// a stream per device to capture conditional-node bodies on
+cudaStream_t body_stream()
+{
+    static std::mutex mu;
+    static std::map<int, cudaStream_t> streams;
+    int dev = 0;
+    T2B_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    cudaStream_t& bs = streams[dev];
+    if (!bs) T2B_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+    return bs;
+}
+
 void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStream_t st)
 {
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
     const int maxsig = fine ? 0 : tb.maxsig;   // the reference's count only grows in the coarse pass
+    // under graph capture the multi-level search (levels 1-5, the candidate gather and sort)
+    // is the body of an IF node whose condition the level-0 select sets when a particle needs
+    // it, so the usual batch (every particle on the fast path) launches none of it
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    T2B_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
+    const bool cond = cs == cudaStreamCaptureStatusActive && g != nullptr;
+    cudaGraphConditionalHandle h = 0;
+    if (cond) T2B_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
     k_sel_init<<<(w.n + 127) / 128, 128, 0, st>>>(w, fine, tb.adaptive_fraction);
-    k_select<<<w.n, 1024, 0, st>>>(w, fine, maxsig);
-    for (int level = 1; level < 6; level++) {
-        k_hist_level<<<grid, 256, HIST_SMEM, st>>>(tb, w, fine);
-        k_select<<<w.n, 1024, 0, st>>>(w, fine, maxsig);
+    k_select<<<w.n, 1024, 0, st>>>(w, fine, maxsig, h);
+    auto multilevel = [&](cudaStream_t s2) {
+        for (int level = 1; level < 6; level++) {
+            k_hist_level<<<grid, 256, HIST_SMEM, s2>>>(tb, w, fine);
+            k_select<<<w.n, 1024, 0, s2>>>(w, fine, maxsig, 0);
+        }
+        k_gather<<<grid, 256, 0, s2>>>(tb, w, fine);
+        k_final<<<w.n, 1024, 0, s2>>>(w, fine, ipass, maxsig);
+    };
+    if (cond) {
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        T2B_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeIf;
+        np.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        T2B_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        T2B_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+        cudaStream_t bs = body_stream();
+        T2B_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        try {
+            multilevel(bs);
+        } catch (...) {
+            cudaGraph_t dummy = nullptr;
+            cudaStreamEndCapture(bs, &dummy);
+            throw;
+        }
+        cudaGraph_t done = nullptr;
+        T2B_CUDA(cudaStreamEndCapture(bs, &done));
+    } else {
+        multilevel(st);
     }
-    k_gather<<<grid, 256, 0, st>>>(tb, w, fine);
-    k_final<<<w.n, 1024, 0, st>>>(w, fine, ipass, maxsig);
     k_gather_fast<<<grid, 256, 0, st>>>(tb, w, fine);
     k_final_fast<<<w.n, 1024, FAST_SMEM, st>>>(w, fine, ipass, maxsig);
 }
