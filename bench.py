@@ -12,8 +12,10 @@ FP64 weights, weighted sums and backprojection.
 
 value: particles/s with inputs resident in HBM (device entry point, CUDA events
 on the launching stream, max over ranks).  e2e: the same metric through the
-host entry point with pinned host buffers (H2D of the batch and D2H of the
-results inside the timed region).  `--impl reference` times the reference's CPU
+host entry points with pinned host buffers (H2D of the batch and D2H of the
+results inside the timed region, host wall clock): the pipelined pair
+t2b_estep_submit_host / t2b_estep_wait, step i's inputs copying while step i-1
+computes (`synchronous_value`: t2b_estep_batch_host, one blocking call per step).  `--impl reference` times the reference's CPU
 E-step on the host cores instead: the reference's own CPU diff2 kernel compiled
 from its sources (oracle/_ref) when built, else the FP64 port in oracle/.
 """
@@ -672,14 +674,34 @@ def main():
     def e2e_step():
         t2b._check(lib.t2b_estep_batch_host(es._h, ctypes.byref(batch), ctypes.byref(result)))
 
+    ticket = ctypes.c_longlong(-1)
+
+    def e2e_submit():
+        t2b._check(lib.t2b_estep_submit_host(es._h, ctypes.byref(batch), ctypes.byref(result), ctypes.byref(ticket)))
+        return ticket.value
+
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
+    # one call per step, each waiting for its own results
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
+    sync_s = max_over_ranks(time.perf_counter() - t0, world)
+    if world > 1:
+        torch.distributed.barrier()
+    # pipelined: step i is submitted (its inputs copy in while step i-1 computes), then the
+    # host waits for the results of step i-1; after the loop, for the last step's
+    t0 = time.perf_counter()
+    prev = None
+    for _ in range(args.steps):
+        cur = e2e_submit()
+        if prev is not None:
+            t2b._check(lib.t2b_estep_wait(es._h, prev))
+        prev = cur
+    t2b._check(lib.t2b_estep_wait(es._h, prev))
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     # per-stage device times (CUDA events around each stage) of separately synchronised
     # host-path steps; not part of `value`
@@ -693,7 +715,8 @@ def main():
     h2d = sum(v.numel() * v.element_size() for v in pin.values())
     d2h = sum(v.numel() * v.element_size() for v in hres.values())
     e2e = {"value": B * args.steps * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h}
+           "d2h_bytes_per_step": d2h, "api": "t2b_estep_submit_host + t2b_estep_wait (one step in flight)",
+           "synchronous_value": B * args.steps * world / sync_s}
 
     # roofline of the dominant kernel (the tcgen05 contraction k_diff2_tc)
     O, T = samp["n_dir"] * samp["n_psi"], samp["n_trans"]

@@ -34,7 +34,8 @@ ABI_SYMBOLS = (
     "t2b_create", "t2b_destroy", "t2b_last_error", "t2b_version",
     "t2b_projector_set", "t2b_backprojector_init", "t2b_backprojector_clear",
     "t2b_backprojector_get", "t2b_backprojector_device_ptrs", "t2b_configure",
-    "t2b_estep_batch_host", "t2b_estep_batch_device", "t2b_reconstruct_divide",
+    "t2b_estep_batch_host", "t2b_estep_batch_device", "t2b_estep_submit_host", "t2b_estep_wait",
+    "t2b_reconstruct_divide",
     "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_last_stage_ms",
     "t2b_sampling", "t2b_reconstruct_divide_noalloc", "t2b_last_launch_count",
     "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
@@ -169,6 +170,9 @@ def _setup_prototypes():
     lib.t2b_configure.argtypes = [v, ctypes.POINTER(Config)]
     lib.t2b_estep_batch_host.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(Result)]
     lib.t2b_estep_batch_device.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(Result), v]
+    lib.t2b_estep_submit_host.argtypes = [v, ctypes.POINTER(Batch), ctypes.POINTER(Result),
+                                          ctypes.POINTER(ctypes.c_longlong)]
+    lib.t2b_estep_wait.argtypes = [v, ctypes.c_longlong]
     lib.t2b_reconstruct_divide.argtypes = [v, i, v]
     lib.t2b_reconstruct_divide_noalloc.argtypes = [v, v, i, i, i, i, i, i, i, v, v]
     lib.t2b_project.argtypes = [v, i, v, i, i, v]
@@ -365,6 +369,7 @@ class EStep:
         self._h = ctypes.c_void_p()
         _check(lib.t2b_create(device, ctypes.byref(self._h)))
         self._keep = []
+        self._inflight = {}   # ticket -> the arrays a submitted host batch reads and writes
         self.cfg = None
 
     def close(self):
@@ -481,6 +486,27 @@ class EStep:
         r = Result(*[_ptr(res[name]) for name, _ in Result._fields_])
         _check(lib.t2b_estep_batch_host(self._h, ctypes.byref(b), ctypes.byref(r)))
         return res
+
+    # pipelined host batches: submit returns a ticket at once; the batch's arrays (inputs
+    # and the returned result dict) must stay alive until wait(ticket) returns
+    def expectation_submit(self, fimg, ctf, minvsigma2, scalars, fimg_nomask=None, out=None):
+        fimg = np.ascontiguousarray(fimg, np.complex64)
+        n = fimg.shape[0]
+        arrs = [fimg, np.ascontiguousarray(ctf, np.float32), np.ascontiguousarray(minvsigma2, np.float32),
+                np.ascontiguousarray(scalars, np.float64)]
+        fnm = None if fimg_nomask is None else np.ascontiguousarray(fimg_nomask, np.complex64)
+        b = Batch(n, 0, _ptr(arrs[0]), _ptr(fnm), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(arrs[3]))
+        res = self._result_arrays(n) if out is None else out
+        r = Result(*[_ptr(res[name]) for name, _ in Result._fields_])
+        t = ctypes.c_longlong(-1)
+        _check(lib.t2b_estep_submit_host(self._h, ctypes.byref(b), ctypes.byref(r), ctypes.byref(t)))
+        self._inflight[t.value] = (arrs, fnm, res)
+        return t.value, res
+
+    def wait(self, ticket=-1):
+        _check(lib.t2b_estep_wait(self._h, ticket))
+        for k in [k for k in self._inflight if ticket < 0 or k <= ticket]:
+            del self._inflight[k]
 
     # device-resident variant: arguments are objects with .data_ptr() (e.g. torch tensors)
     def expectation_device(self, n, fimg_ptr, ctf_ptr, minv_ptr, scal_ptr, result_ptrs, stream=0,

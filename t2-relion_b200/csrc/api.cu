@@ -75,7 +75,19 @@ int t2b_create(int device, t2b_ctx** out)
         auto* c = new t2b_ctx();
         c->device = device;
         cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-        if (e != cudaSuccess) { delete c; T2B_CUDA(e); }
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+        for (auto& s : c->in)
+            for (cudaEvent_t* ev : {&s.copied, &s.consumed, &s.done})
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            for (auto& s : c->in)
+                for (cudaEvent_t ev : {s.copied, s.consumed, s.done})
+                    if (ev) cudaEventDestroy(ev);
+            if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+            if (c->stream) cudaStreamDestroy(c->stream);
+            delete c;
+            T2B_CUDA(e);
+        }
         for (auto& ev : c->ev) cudaEventCreate(&ev);
         *out = c;
     });
@@ -88,6 +100,7 @@ void t2b_destroy(t2b_ctx* c)
         int prev = -1;
         cudaGetDevice(&prev);
         cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->copy_stream);
         cudaStreamSynchronize(c->stream);
         free_allocs(c);
         proposal_release(c);
@@ -96,6 +109,9 @@ void t2b_destroy(t2b_ctx* c)
         for (auto p : c->gdata) cudaFree(p);
         for (auto p : c->gweight) cudaFree(p);
         for (auto& ev : c->ev) cudaEventDestroy(ev);
+        for (auto& s : c->in)
+            for (cudaEvent_t ev : {s.copied, s.consumed, s.done}) cudaEventDestroy(ev);
+        cudaStreamDestroy(c->copy_stream);
         cudaStreamDestroy(c->stream);
         if (prev >= 0) cudaSetDevice(prev);
     }
@@ -241,6 +257,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         }
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard g(c->device);
+        T2B_CUDA(cudaStreamSynchronize(c->copy_stream));
         T2B_CUDA(cudaStreamSynchronize(c->stream));
         free_allocs(c);
         proposal_invalidate(c);
@@ -392,6 +409,16 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         w.ctf = dalloc<float>(c, (size_t)B * P);
         w.minv = dalloc<float>(c, (size_t)B * P);
         w.scal = dalloc<double>(c, (size_t)B * 8);
+        c->in[0].fimg = const_cast<float2*>(w.fimg);
+        c->in[0].fimg_nm = const_cast<float2*>(w.fimg_nm);
+        c->in[0].ctf = const_cast<float*>(w.ctf);
+        c->in[0].minv = const_cast<float*>(w.minv);
+        c->in[0].scal = const_cast<double*>(w.scal);
+        c->in[1].fimg = dalloc<float2>(c, (size_t)B * P);
+        c->in[1].fimg_nm = dalloc<float2>(c, (size_t)B * P);
+        c->in[1].ctf = dalloc<float>(c, (size_t)B * P);
+        c->in[1].minv = dalloc<float>(c, (size_t)B * P);
+        c->in[1].scal = dalloc<double>(c, (size_t)B * 8);
         w.r_min = dalloc<double>(c, B); w.r_sum = dalloc<double>(c, B); w.r_sig = dalloc<double>(c, B);
         w.r_csum = dalloc<double>(c, B); w.r_csig = dalloc<double>(c, B); w.r_pmax = dalloc<double>(c, B);
         w.r_nsign = dalloc<long long>(c, B); w.r_ncsig = dalloc<long long>(c, B);
@@ -554,6 +581,84 @@ static int replay_graph(t2b_ctx* c, Work& w, cudaStream_t st, const std::vector<
     return g.kernels;
 }
 
+// Enqueue one host batch: inputs into staging slot (ticket & 1) on the copy stream once
+// that slot's previous batch has read its own, the batch on the context's stream once
+// they are in, the results back to host memory after it.  Returns the ticket.
+static long long submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
+{
+    cudaStream_t st = c->stream, cs = c->copy_stream;
+    const long long ticket = c->submitted;
+    t2b_ctx::InSlot& in = c->in[ticket & 1];
+    Work w = c->wk;
+    const int n = b->n, P = c->tb.P;
+    w.n = n;
+    w.fimg = in.fimg;
+    w.fimg_nm = b->fimg_nomask ? in.fimg_nm : in.fimg;   // no separate unmasked image: the masked one serves both
+    w.ctf = in.ctf;
+    w.minv = in.minv;
+    w.scal = in.scal;
+    T2B_CUDA(cudaStreamWaitEvent(cs, in.consumed, 0));
+    T2B_CUDA(cudaMemcpyAsync(in.fimg, b->fimg, (size_t)n * P * sizeof(float2), cudaMemcpyHostToDevice, cs));
+    if (b->fimg_nomask)
+        T2B_CUDA(cudaMemcpyAsync(in.fimg_nm, b->fimg_nomask, (size_t)n * P * sizeof(float2), cudaMemcpyHostToDevice, cs));
+    T2B_CUDA(cudaMemcpyAsync(in.ctf, b->ctf, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, cs));
+    T2B_CUDA(cudaMemcpyAsync(in.minv, b->minvsigma2, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, cs));
+    T2B_CUDA(cudaMemcpyAsync(in.scal, b->scalars, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, cs));
+    T2B_CUDA(cudaEventRecord(in.copied, cs));
+    T2B_CUDA(cudaStreamWaitEvent(st, in.copied, 0));
+    // the batch computation itself: a replayed graph unless stage timing is on
+    const bool graph = c->cfg.use_graph && !c->stage_timing;
+    if (graph) {
+        const std::vector<const void*> key = {(const void*)(intptr_t)n, (const void*)st, (const void*)w.fimg_nm,
+                                              (const void*)(intptr_t)(c->net && c->net->enabled ? c->net->kprop : 0)};
+        c->last_kernels = replay_graph(c, w, st, key, in.g);
+    } else {
+        enqueue_estep(c, w, st, true, true);
+        c->last_kernels = -1;
+    }
+    T2B_CUDA(cudaEventRecord(in.consumed, st));
+    const int K = c->tb.K, half = c->cfg.ori_size / 2 + 1;
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        if (dst) T2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    };
+    d2h(r->min_diff2, w.r_min, n * sizeof(double));
+    d2h(r->sum_weight, w.r_sum, n * sizeof(double));
+    d2h(r->sig_weight, w.r_sig, n * sizeof(double));
+    d2h(r->coarse_sum_weight, w.r_csum, n * sizeof(double));
+    d2h(r->coarse_sig_weight, w.r_csig, n * sizeof(double));
+    d2h(r->nr_sign, w.r_nsign, n * sizeof(long long));
+    d2h(r->n_coarse_sig, w.r_ncsig, n * sizeof(long long));
+    d2h(r->pmax, w.r_pmax, n * sizeof(double));
+    d2h(r->pose, w.r_pose, n * 5 * sizeof(int));
+    d2h(r->wsum_norm, w.r_norm, n * sizeof(double));
+    d2h(r->sumw, w.r_sumw, n * sizeof(double));
+    d2h(r->wsum_sigma2_offset, w.r_sig_off, n * sizeof(double));
+    d2h(r->wsum_sigma2, w.r_sigma2, (size_t)n * half * sizeof(double));
+    d2h(r->wsum_pdf_class, w.r_pdf_class, (size_t)n * K * sizeof(double));
+    d2h(r->wsum_pdf_dir, w.r_pdf_dir, (size_t)n * K * c->tb.n_dir * sizeof(double));
+    d2h(r->status, w.status, n * sizeof(int));
+    d2h(r->learned, w.r_learned, n * sizeof(int));
+    d2h(r->audit_mass, w.r_audit, n * sizeof(double));
+    T2B_CUDA(cudaEventRecord(in.done, st));
+    c->last_n = n;
+    return c->submitted++;
+}
+
+// Block until the batch of `ticket` (every batch when ticket < 0) is done.
+static void wait_host(t2b_ctx* c, long long ticket)
+{
+    cudaEvent_t ev = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        T2B_REQUIRE(ticket < c->submitted, T2B_ERR_ARG, "no batch was submitted with this ticket");
+        if (ticket >= 0) ev = c->in[ticket & 1].done;
+    }
+    DeviceGuard g(c->device);
+    // a slot's event recorded again by a later batch completes after this one: stream order
+    if (ev) T2B_CUDA(cudaEventSynchronize(ev));
+    else T2B_CUDA(cudaStreamSynchronize(c->stream));
+}
+
 }  // namespace t2b
 
 extern "C" {
@@ -562,56 +667,34 @@ int t2b_estep_batch_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
 {
     return guarded([&] {
         check_batch(c, b, r);
+        long long ticket;
+        {
+            std::lock_guard<std::mutex> lk(c->mu);
+            DeviceGuard g(c->device);
+            ticket = submit_host(c, b, r);
+        }
+        wait_host(c, ticket);
+        std::lock_guard<std::mutex> lk(c->mu);
+        collect_stage_ms(c);
+    });
+}
+
+int t2b_estep_submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, long long* ticket)
+{
+    return guarded([&] {
+        check_batch(c, b, r);
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard g(c->device);
-        cudaStream_t st = c->stream;
-        Work w = c->wk;
-        const int n = b->n, P = c->tb.P;
-        w.n = n;
-        T2B_CUDA(cudaMemcpyAsync((void*)w.fimg, b->fimg, (size_t)n * P * sizeof(float2), cudaMemcpyHostToDevice, st));
-        if (b->fimg_nomask)
-            T2B_CUDA(cudaMemcpyAsync((void*)w.fimg_nm, b->fimg_nomask, (size_t)n * P * sizeof(float2),
-                                     cudaMemcpyHostToDevice, st));
-        else
-            w.fimg_nm = w.fimg;   // no separate unmasked image: the masked one serves both
-        T2B_CUDA(cudaMemcpyAsync((void*)w.ctf, b->ctf, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
-        T2B_CUDA(cudaMemcpyAsync((void*)w.minv, b->minvsigma2, (size_t)n * P * sizeof(float), cudaMemcpyHostToDevice, st));
-        T2B_CUDA(cudaMemcpyAsync((void*)w.scal, b->scalars, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, st));
-        // the batch computation itself: a replayed graph unless stage timing is on
-        const bool graph = c->cfg.use_graph && !c->stage_timing;
-        if (graph) {
-            const std::vector<const void*> key = {(const void*)(intptr_t)n, (const void*)st, (const void*)w.fimg_nm,
-                                                  (const void*)(intptr_t)(c->net && c->net->enabled ? c->net->kprop : 0)};
-            c->last_kernels = replay_graph(c, w, st, key, c->g_host);
-        } else {
-            enqueue_estep(c, w, st, true, true);
-            c->last_kernels = -1;
-        }
-        const int K = c->tb.K, half = c->cfg.ori_size / 2 + 1;
-        auto d2h = [&](void* dst, const void* src, size_t bytes) {
-            if (dst) T2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
-        };
-        d2h(r->min_diff2, w.r_min, n * sizeof(double));
-        d2h(r->sum_weight, w.r_sum, n * sizeof(double));
-        d2h(r->sig_weight, w.r_sig, n * sizeof(double));
-        d2h(r->coarse_sum_weight, w.r_csum, n * sizeof(double));
-        d2h(r->coarse_sig_weight, w.r_csig, n * sizeof(double));
-        d2h(r->nr_sign, w.r_nsign, n * sizeof(long long));
-        d2h(r->n_coarse_sig, w.r_ncsig, n * sizeof(long long));
-        d2h(r->pmax, w.r_pmax, n * sizeof(double));
-        d2h(r->pose, w.r_pose, n * 5 * sizeof(int));
-        d2h(r->wsum_norm, w.r_norm, n * sizeof(double));
-        d2h(r->sumw, w.r_sumw, n * sizeof(double));
-        d2h(r->wsum_sigma2_offset, w.r_sig_off, n * sizeof(double));
-        d2h(r->wsum_sigma2, w.r_sigma2, (size_t)n * half * sizeof(double));
-        d2h(r->wsum_pdf_class, w.r_pdf_class, (size_t)n * K * sizeof(double));
-        d2h(r->wsum_pdf_dir, w.r_pdf_dir, (size_t)n * K * c->tb.n_dir * sizeof(double));
-        d2h(r->status, w.status, n * sizeof(int));
-        d2h(r->learned, w.r_learned, n * sizeof(int));
-        d2h(r->audit_mass, w.r_audit, n * sizeof(double));
-        T2B_CUDA(cudaStreamSynchronize(st));
-        collect_stage_ms(c);
-        c->last_n = n;
+        const long long t = submit_host(c, b, r);
+        if (ticket) *ticket = t;
+    });
+}
+
+int t2b_estep_wait(t2b_ctx* c, long long ticket)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c, T2B_ERR_ARG, "null argument");
+        wait_host(c, ticket);
     });
 }
 

@@ -519,10 +519,11 @@ __global__ void k_audit_begin(PropState* ps, int* audit_b, int n, int every, int
                               double* asum, double* r_audit)
 {
     if (threadIdx.x == 0) {
+        // the stream positions seen + b that are multiples of `every`: an arithmetic progression
         int na = 0;
         const long long seen = ps->seen;
-        for (int b = 0; b < n && na < na_max; b++)
-            if ((seen + b) % every == 0) audit_b[na++] = b;
+        const long long first = (every - seen % every) % every;
+        for (long long b = first; b < n && na < na_max; b += every) audit_b[na++] = (int)b;
         ps->na = na;
         ps->seen = seen + n;
         ps->gate = 1;

@@ -273,11 +273,27 @@ struct t2b_ctx {
         std::vector<const void*> key;         // shape / buffers / stream / proposal settings
         int kernels = -1;                     // its kernel nodes
     };
-    GraphSlot g_dev, g_host;                  // device and host entry points
+    GraphSlot g_dev;                          // device entry point
+    // Host entry points: two staging slots for the batch inputs.  A batch's inputs are
+    // copied into its slot on copy_stream while the previous batch computes on `stream`;
+    // slot 0 is the workspace's own input buffers, slot 1 a second set.
+    struct InSlot {
+        float2* fimg = nullptr;
+        float2* fimg_nm = nullptr;
+        float* ctf = nullptr;
+        float* minv = nullptr;
+        double* scal = nullptr;
+        cudaEvent_t copied = nullptr;         // inputs in the slot (copy_stream)
+        cudaEvent_t consumed = nullptr;       // the slot's batch has read them (stream)
+        cudaEvent_t done = nullptr;           // the slot's results are in host memory (stream)
+        GraphSlot g;                          // the captured batch reading this slot
+    } in[2];
+    cudaStream_t copy_stream = nullptr;
+    long long submitted = 0;                  // host batches submitted: the next ticket
     bool stage_timing = false;                // host batches run uncaptured with stage events
     void drop_graphs()
     {
-        for (GraphSlot* g : {&g_dev, &g_host}) {
+        for (GraphSlot* g : {&g_dev, &in[0].g, &in[1].g}) {
             if (g->exec) cudaGraphExecDestroy(g->exec);
             g->exec = nullptr;
             g->key.clear();

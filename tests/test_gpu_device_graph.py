@@ -43,3 +43,39 @@ def test_graph_replay_matches_host_path(mode):
         assert np.allclose(got["wsum_norm"], ref["wsum_norm"], rtol=1e-5, atol=0)
     assert es.launch_count() > 20
     es.close()
+
+
+def test_pipelined_host_batches_match_synchronous_ones(t2b):
+    """t2b_estep_submit_host / t2b_estep_wait: three batches of different sizes in flight
+    at once (inputs copied while the previous batch computes, two staging slots) give
+    the results and the backprojection of the same batches run one at a time."""
+    pb = problems.build("refine_o1_ovs", n_particles=14, seed=12, diff2_mode=1)
+    P = pb["parts"]
+    es = pb["product"]()
+    cuts = [(0, 6), (6, 9), (9, 14)]
+
+    def part(a, b):
+        return P["fimg"][a:b], P["ctf"][a:b], P["minv"][a:b], P["scalars"][a:b]
+
+    es.clear_backprojector(0)
+    sync = [es.expectation(*part(a, b)) for a, b in cuts]
+    g_sync = [x.copy() for x in es.get_backprojector(0)]
+    es.clear_backprojector(0)
+    tickets = [es.expectation_submit(*part(a, b)) for a, b in cuts]
+    assert [t for t, _ in tickets] == [tickets[0][0] + i for i in range(3)]
+    es.wait(tickets[1][0])          # the first two are done, the third may still run
+    for (t, got), ref in zip(tickets[:2], sync[:2]):
+        assert np.array_equal(got["pose"], ref["pose"])
+    es.wait()
+    for (t, got), ref in zip(tickets, sync):
+        assert np.all(got["status"] == 0)
+        assert np.array_equal(got["pose"], ref["pose"])
+        assert np.array_equal(got["nr_sign"], ref["nr_sign"])
+        for k in ("min_diff2", "sum_weight", "sig_weight", "pmax", "sumw"):
+            assert np.allclose(got[k], ref[k], rtol=1e-9, atol=0), k
+        assert np.allclose(got["wsum_norm"], ref["wsum_norm"], rtol=1e-5, atol=0)
+    for a, b in zip(es.get_backprojector(0), g_sync):
+        assert np.allclose(a, b, rtol=1e-4, atol=1e-4 * np.max(np.abs(b)))
+    with pytest.raises(t2b.T2BError):
+        es.wait(tickets[-1][0] + 1)
+    es.close()
