@@ -99,6 +99,15 @@ public:
     {
         check(t2b_estep_batch_device(b_.ctx(), &in, &out, stream));
     }
+    // pipelined host batches: submit returns a ticket at once (the batch's inputs copy in
+    // while the previous batch computes); its buffers stay untouched until wait(ticket)
+    long long submitBatch(const t2b_batch& in, const t2b_result& out)
+    {
+        long long t = -1;
+        check(t2b_estep_submit_host(b_.ctx(), &in, &out, &t));
+        return t;
+    }
+    void wait(long long ticket = -1) { check(t2b_estep_wait(b_.ctx(), ticket)); }
 
 private:
     MlDeviceBundle& b_;
