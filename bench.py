@@ -56,6 +56,8 @@ METRIC = "E-step particles/s box128: learned+split-BF16 vs plain FP32 GPU; roofl
 # learned proposals: network top-1024 rescored at low resolution, best 64 to the coarse
 # pass; every 50th particle (2 %) audited by the full coarse pass (>= 0.999 of its mass)
 PROP = dict(topk=64, rescore=1024, audit_every=50, audit_mass=0.999)
+# end-to-end timing: at least this many steps per timed run
+E2E_STEPS = 30
 # DRAM bytes (read + write) of the audit + proposal k_diff2_tc launches of one learned step
 # at 128 particles, from one ncu capture
 # (audit 766.02 MB read + 18.59 MB written, proposal pass 548.33 MB + 0.46 MB;
@@ -75,7 +77,7 @@ def build_problem(t2b, sy, n_particles, seed):
     return fmap, samp, parts
 
 
-def setup_context(t2b, sy, fmap, samp, mode, batch, device=0):
+def setup_context(t2b, sy, fmap, samp, mode, batch, device=0, use_graph=1):
     w = WORKLOAD
     es = t2b.EStep(device)
     es.set_projector(0, fmap, 3, w["r_max"], 2)
@@ -83,7 +85,7 @@ def setup_context(t2b, sy, fmap, samp, mode, batch, device=0):
     es.configure(ori_size=w["ori_size"], current_size=2 * w["r_max"], ref_dim=3, nr_classes=1, samp=samp,
                  pdf_direction=np.full((1, samp["n_dir"]), 1.0 / samp["n_dir"]), pdf_class=np.ones(1),
                  sigma2_offset=(w["offset_range"] * w["angpix"]) ** 2, pixel_size=w["angpix"],
-                 adaptive_oversampling=1, diff2_mode=mode, max_batch=batch)
+                 adaptive_oversampling=1, diff2_mode=mode, max_batch=batch, use_graph=use_graph)
     return es
 
 
@@ -554,6 +556,9 @@ def main():
                          "(real-space particles -> E-step inputs), its own JSON line")
     ap.add_argument("--prep-batch", type=int, default=1024, help="prep: particles per call")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tile shapes")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch each step's kernels one by one instead of replaying its CUDA graph (ncu cannot "
+                         "profile the kernel nodes of a graph with conditional nodes; not a bench number)")
     args = ap.parse_args()
     if args.stage == "prep":
         run_prep(args)
@@ -578,7 +583,7 @@ def main():
     B = args.batch
     fmap, samp, parts = build_problem(t2b, sy, B, WORKLOAD["seed"] + 1000 * rank)
     mode = t2b.DIFF2_PLAIN_FP32 if args.mode == "plain" else t2b.DIFF2_SPLIT_BF16
-    es = setup_context(t2b, sy, fmap, samp, mode, B, device=local)
+    es = setup_context(t2b, sy, fmap, samp, mode, B, device=local, use_graph=0 if args.no_graph else 1)
     tuned = None
     if not args.no_autotune:
         # once per configuration, before the timed region: the library's tile-shape autotuner
@@ -683,26 +688,38 @@ def main():
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    # one call per step, each waiting for its own results
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    sync_s = max_over_ranks(time.perf_counter() - t0, world)
-    if world > 1:
-        torch.distributed.barrier()
-    # pipelined: step i is submitted (its inputs copy in while step i-1 computes), then the
-    # host waits for the results of step i-1; after the loop, for the last step's
-    t0 = time.perf_counter()
-    prev = None
-    for _ in range(args.steps):
-        cur = e2e_submit()
-        if prev is not None:
-            t2b._check(lib.t2b_estep_wait(es._h, prev))
-        prev = cur
-    t2b._check(lib.t2b_estep_wait(es._h, prev))
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    # host wall clock over E2E_STEPS steps, the median of three runs (a run of a few
+    # milliseconds is at the mercy of one host scheduling hiccup)
+    n_e2e = max(args.steps, E2E_STEPS)
+
+    def timed(loop):
+        runs = []
+        for _ in range(3):
+            if world > 1:
+                torch.distributed.barrier()
+            t0 = time.perf_counter()
+            loop()
+            runs.append(max_over_ranks(time.perf_counter() - t0, world))
+        return float(np.median(runs))
+
+    def sync_loop():
+        # one call per step, each waiting for its own results
+        for _ in range(n_e2e):
+            e2e_step()
+
+    def pipelined_loop():
+        # step i is submitted (its inputs copy in while step i-1 computes), then the host
+        # waits for the results of step i-1; after the loop, for the last step's
+        prev = None
+        for _ in range(n_e2e):
+            cur = e2e_submit()
+            if prev is not None:
+                t2b._check(lib.t2b_estep_wait(es._h, prev))
+            prev = cur
+        t2b._check(lib.t2b_estep_wait(es._h, prev))
+
+    sync_s = timed(sync_loop)
+    e2e_s = timed(pipelined_loop)
     # per-stage device times (CUDA events around each stage) of separately synchronised
     # host-path steps; not part of `value`
     stages = []
@@ -714,9 +731,10 @@ def main():
     stages = np.mean(np.array(stages), axis=0)
     h2d = sum(v.numel() * v.element_size() for v in pin.values())
     d2h = sum(v.numel() * v.element_size() for v in hres.values())
-    e2e = {"value": B * args.steps * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
+    e2e = {"value": B * n_e2e * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "api": "t2b_estep_submit_host + t2b_estep_wait (one step in flight)",
-           "synchronous_value": B * args.steps * world / sync_s}
+           "steps": n_e2e, "timing": "host wall clock, median of 3 runs",
+           "synchronous_value": B * n_e2e * world / sync_s}
 
     # roofline of the dominant kernel (the tcgen05 contraction k_diff2_tc)
     O, T = samp["n_dir"] * samp["n_psi"], samp["n_trans"]

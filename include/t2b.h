@@ -250,6 +250,11 @@ int t2b_project(t2b_ctx* ctx, int iclass, const double* eulers, int n, int curre
  * nover_rot*nover_trans).  *count receives the number of pairs. */
 int t2b_debug_coarse_diff2(t2b_ctx* ctx, int b, float* out);
 int t2b_debug_fine(t2b_ctx* ctx, int b, long long* pairs, float* diff2, long long cap, long long* count);
+/* Learned proposals of particle b in the last batch (valid where that batch's
+ * `learned` result is 1): *kprop receives the proposals per particle; prop
+ * (kprop ints, may be NULL) their orientation indices k*n_dir*n_psi + o, and
+ * diff2 (kprop x n_trans floats, may be NULL) their coarse diff2. */
+int t2b_debug_proposals(t2b_ctx* ctx, int b, int* prop, float* diff2, int* kprop);
 
 /* Tile-shape autotuner (no counterpart in the reference; the reference's
  * kernels have fixed tile shapes).  Times candidate shapes on the caller's

@@ -36,7 +36,7 @@ ABI_SYMBOLS = (
     "t2b_backprojector_get", "t2b_backprojector_device_ptrs", "t2b_configure",
     "t2b_estep_batch_host", "t2b_estep_batch_device", "t2b_estep_submit_host", "t2b_estep_wait",
     "t2b_reconstruct_divide",
-    "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_last_stage_ms",
+    "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_debug_proposals", "t2b_last_stage_ms",
     "t2b_sampling", "t2b_reconstruct_divide_noalloc", "t2b_last_launch_count",
     "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
@@ -178,6 +178,7 @@ def _setup_prototypes():
     lib.t2b_project.argtypes = [v, i, v, i, i, v]
     lib.t2b_debug_coarse_diff2.argtypes = [v, i, v]
     lib.t2b_debug_fine.argtypes = [v, i, v, v, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+    lib.t2b_debug_proposals.argtypes = [v, i, v, v, ctypes.POINTER(ctypes.c_int)]
     lib.t2b_last_stage_ms.argtypes = [v, v, i]
     lib.t2b_last_launch_count.argtypes = [v, ctypes.POINTER(i)]
     lib.t2b_stage_timing.argtypes = [v, i]
@@ -688,6 +689,15 @@ class EStep:
         out = np.zeros(cfg["nr_classes"] * cfg["n_dir"] * cfg["n_psi"] * cfg["n_trans"], np.float32)
         _check(lib.t2b_debug_coarse_diff2(self._h, b, _ptr(out)))
         return out
+
+    def proposals(self, b):
+        """Learned proposals of particle b in the last batch: (orientations, coarse diff2 kprop x n_trans)."""
+        k = ctypes.c_int(0)
+        _check(lib.t2b_debug_proposals(self._h, b, None, None, ctypes.byref(k)))
+        prop = np.zeros(k.value, np.int32)
+        d2 = np.zeros((k.value, self.cfg["n_trans"]), np.float32)
+        _check(lib.t2b_debug_proposals(self._h, b, _ptr(prop), _ptr(d2), ctypes.byref(k)))
+        return prop, d2
 
     def fine(self, b, cap=1 << 20):
         cfg = self.cfg

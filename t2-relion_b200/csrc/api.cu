@@ -489,8 +489,8 @@ void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool
     launch_prep(tb, w, st);
     if (pm) proposal_infer(c, w, st);
     if (stage_events) cudaEventRecord(c->ev[1], st);
-    if (tc) tc_split_images(tb, w, c->tc, st);
     if (pm) proposal_audit(c, w, st, stage_events ? c->ev + 8 : nullptr);
+    if (tc) tc_split_images(tb, w, c->tc, st, w.gate);   // the full pass's operand: skipped while proposals hold
     if (tc) tc_launch_norms(tb, w, c->tc, st, w.gate, 0);
     else launch_norms(tb, w, st);
     if (stage_events) cudaEventRecord(c->ev[2], st);
@@ -942,6 +942,24 @@ int t2b_debug_coarse_diff2(t2b_ctx* c, int b, float* out)
         const size_t n = (size_t)c->tb.K * c->tb.O * c->tb.T;
         T2B_CUDA(cudaStreamSynchronize(c->stream));
         T2B_CUDA(cudaMemcpy(out, c->wk.d2c + (size_t)b * n, n * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+int t2b_debug_proposals(t2b_ctx* c, int b, int* prop, float* diff2, int* kprop)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && kprop && c->configured && b >= 0 && b < c->last_n, T2B_ERR_ARG, "bad particle index");
+        T2B_REQUIRE(c->net && c->net->enabled, T2B_ERR_STATE, "learned proposals are not enabled");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        const int k = c->net->kprop, T = c->tb.T;
+        *kprop = k;
+        if (prop)
+            T2B_CUDA(cudaMemcpy(prop, c->net->prop + (size_t)b * k, k * sizeof(int), cudaMemcpyDeviceToHost));
+        if (diff2)
+            T2B_CUDA(cudaMemcpy(diff2, c->wk.d2c + (size_t)b * k * T, (size_t)k * T * sizeof(float),
+                                cudaMemcpyDeviceToHost));
     });
 }
 

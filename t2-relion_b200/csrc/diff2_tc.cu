@@ -174,17 +174,19 @@ struct TcParams {
     unsigned* minkey;
     int* err;
     int products;             // 1: hi.hi, 2: + hi(A).lo(B), 3: + lo(A).hi(B) (split-BF16)
-    // proposal tiles (mode 1): tile i holds particles [i*ppt, i*ppt + ppt); A rows
-    // [i*128, i*128+128) are their gathered proposals (kslot rows each, the first
-    // KO of them used), B rows from i*ppt*T are their shifted images; norms and
-    // d2c are per (particle, proposal); ncols = particles of the batch
+    // proposal tiles (mode 1): tile i holds particles [i*ppt, i*ppt + ppt) (ppt * kslot
+    // = 128); A rows [i*128, i*128+128) are their proposals premultiplied by the
+    // conjugate particle image (kslot rows each, the first KO of them used), B the T
+    // phase rows of the translations, the same for every tile; norms and d2c are per
+    // (particle, proposal); ncols = particles of the batch.
+    // mode 2 tiles hold one particle (ppt = 1): B rows from tile*T (its own images).
     int mode, ppt, kslot;
     const int* prop;          // mode 1: global orientation of every (particle, proposal)
     const int* gate;          // run only when (*gate != 0) == gate_run (null: always)
     int gate_run;
     int tn;                   // N of the tile (multiple of 32, <= 256; 0 = 256); B maps with a tn-row box
-    int mtp;                  // mode 1 with ppt = 1: consecutive tiles per particle (0 = 1); A rows of
-                              // tile i are rows [i*128, i*128+128), proposal j = (i % mtp)*128 + row
+    int mtp;                  // mode 2: consecutive tiles per particle (0 = 1); A rows of tile i are
+                              // rows [i*128, i*128+128), candidate j = (i % mtp)*128 + row
     // mode 2 (low-resolution rescoring, tiles as mode 1 with ppt = 1): no diff2 is stored;
     // each epilogue thread reduces its own row (candidate j) over the translations,
     // d2c[b*KO + j] = log sum_t pdf_t exp(C_t) - norm_j + log pdf_o(j)  (c0 omitted)
@@ -260,9 +262,12 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 tile_coords(tile / ksp, p.m_tiles, p.n_tiles, p.group ? p.group : 16, mt, nt);
                 ya = mt * TM;
                 yb = nt * tn_l;
+            } else if (p.mode == 1) {
+                ya = tile * TM;
+                yb = 0;
             } else {
-                ya = (p.mtp > 1) ? tile * TM : tile * p.ppt * p.kslot;
-                yb = (tile / (p.mtp ? p.mtp : 1)) * p.ppt * p.T;
+                ya = tile * TM;
+                yb = (tile / (p.mtp ? p.mtp : 1)) * p.T;
             }
             for (int kb = kb0; kb < kb1; kb++, it++) {
                 const int s = it % nst;
@@ -352,6 +357,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                     const size_t pj = (size_t)bb * p.KO + j;
                     my_skip = p.skip[p.prop[pj]] ? 1 : 0;
                     my_norm = p.norms[pj];
+                    if (p.mode == 1) my_norm = p.c0[bb] + my_norm;   // diff2 = (c0 + norm) - C
                 }
             }
             __syncwarp();
@@ -412,25 +418,23 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                         outp[((size_t)b * p.KO + oc) * p.T + t] = d;
                     }
                 } else {
-                    // proposal tile: column -> (particle slot, translation), row -> (slot, proposal)
-                    const int col = c * 32 + lane;
-                    const int bc = col / p.T;
-                    const int t = col - bc * p.T;
-                    b = bfirst + bc;
-                    const bool cok = bc < p.ppt && b < p.ncols;
-                    const float c0 = cok ? p.c0[b] : 0.f;
+                    // proposal tile: column = translation; the warp's 32 rows are proposals of
+                    // one particle (kslot a multiple of 32)
+                    const int t = c * 32 + lane;
+                    const int bp = (q * 32) / p.kslot;
+                    b = bfirst + bp;
+                    const bool cok = t < p.T && bp < p.ppt && b < p.ncols;
                     for (int r = 0; r < 32; r++) {
-                        const int row = q * 32 + r;
-                        const int bp = row / p.kslot, j = jbase + row - bp * p.kslot;
+                        const int j = q * 32 + r - bp * p.kslot;
                         const int skip_r = __shfl_sync(0xffffffffu, my_skip, r);
-                        const float norm_r = __shfl_sync(0xffffffffu, my_norm, r);
-                        if (!cok || bp != bc || j >= p.KO) continue;
+                        const float cn_r = __shfl_sync(0xffffffffu, my_norm, r);
+                        if (!cok || j >= p.KO) continue;
                         const size_t pj = (size_t)b * p.KO + j;
                         float d;
                         if (skip_r) {
                             d = -999.f;
                         } else {
-                            d = c0 + norm_r - sbuf[r * EPI_LD + lane];
+                            d = cn_r - sbuf[r * EPI_LD + lane];
                             lmin = min(lmin, f2key(d));
                         }
                         p.d2c[pj * p.T + t] = d;
@@ -481,17 +485,20 @@ __global__ void k_split_proj(const float2* __restrict__ proj, int rows, int P, c
 }
 
 // shifted, CTF- and sigma-weighted images: column b*T+t, value cvec_b[p] * ab_t[p];
-// one operand row per CTA iteration, 4 complex values (16-byte stores) per thread
+// one operand row per CTA iteration, 4 complex values (16-byte stores) per thread.
+// cvec = null: the phase rows ab_t themselves.  Returns at once while *gate != 0
+// (learned proposals in use: only the full coarse pass reads these rows).
 __global__ void __launch_bounds__(128) k_split_img(const float2* __restrict__ cvec, const float2* __restrict__ ab,
                                                    int ncols, int nrows, int T, int P, const int* __restrict__ kpix,
                                                    int nk, int kdim, __nv_bfloat16* __restrict__ hi,
-                                                   __nv_bfloat16* __restrict__ lo)
+                                                   __nv_bfloat16* __restrict__ lo, const int* gate)
 {
+    if (gate && *gate != 0) return;
     const int nv = kdim / 8;  // groups of 4 complex values
     for (int col = blockIdx.x; col < nrows; col += gridDim.x) {
         const bool ok = col < ncols;
         const int b = ok ? col / T : 0, t = ok ? col - b * T : 0;
-        const float2* cb = cvec + (size_t)b * P;
+        const float2* cb = cvec ? cvec + (size_t)b * P : nullptr;
         const float2* at = ab + (size_t)t * P;
         uint4* dh = reinterpret_cast<uint4*>(hi + (size_t)col * kdim);
         uint4* dl = reinterpret_cast<uint4*>(lo + (size_t)col * kdim);
@@ -503,8 +510,13 @@ __global__ void __launch_bounds__(128) k_split_img(const float2* __restrict__ cv
                 float2 v = make_float2(0.f, 0.f);
                 if (ok && kk < nk) {
                     const int pp = kpix[kk];
-                    const float2 c = cb[pp], a = at[pp];
-                    v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+                    const float2 a = at[pp];
+                    if (cb) {
+                        const float2 c = cb[pp];
+                        v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+                    } else {
+                        v = a;
+                    }
                 }
                 __nv_bfloat16 h0, l0, h1, l1;
                 split_bf16(v.x, h0, l0);
@@ -596,7 +608,7 @@ size_t tc_kn(int nk) { return (size_t)((nk + TK - 1) / TK) * TK; }
 
 // descriptor slots in op.maps (TC_MAP_SLOTS of 128 bytes)
 enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL,
-       MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_IH96, MAP_IL96, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL,
+       MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_ABH, MAP_ABL, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL,
        MAP_IH128, MAP_IL128, MAP_COUNT };
 static_assert(MAP_COUNT <= TC_MAP_SLOTS, "tensor-map slots");
 static_assert(sizeof(CUtensorMap) == 128, "tensor-map size");
@@ -621,9 +633,6 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
     h[MAP_WL] = make_map(op.wl, op.b_pad, op.kn, TN);
     T2B_CUDA(cudaStreamSynchronize(st));
     T2B_CUDA(cudaMemcpy(op.maps, h, sizeof(h), cudaMemcpyHostToDevice));  // slots MAP_PH..MAP_WL
-    // the image operand with a 96-row box: one particle's translations per tile (proposal pass)
-    CUtensorMap h96[2] = {make_map(op.ah, op.n_pad, op.kdim, 96), make_map(op.al, op.n_pad, op.kdim, 96)};
-    T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * MAP_IH96, h96, sizeof(h96), cudaMemcpyHostToDevice));
     // and with a 128-row box: dense coarse tiles of 128 columns (t2b_autotune)
     CUtensorMap h128[2] = {make_map(op.ah, op.n_pad, op.kdim, 128), make_map(op.al, op.n_pad, op.kdim, 128)};
     T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * MAP_IH128, h128, sizeof(h128),
@@ -683,13 +692,22 @@ void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     launch_gemm(op, MAP_NH, MAP_WH, p, st);
 }
 
-void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st)
+void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate)
 {
     const int ncols = w.n * tb.T;
     const int n_pad = (ncols + TN - 1) / TN * TN;
     T2B_REQUIRE(n_pad <= op.n_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
     k_split_img<<<std::min(n_pad, 16 * sms()), 128, 0, st>>>(w.cvec, tb.ab_c, ncols, n_pad, tb.T, tb.P, tb.kpix, tb.nk,
-                                                            op.kdim, (__nv_bfloat16*)op.ah, (__nv_bfloat16*)op.al);
+                                                            op.kdim, (__nv_bfloat16*)op.ah, (__nv_bfloat16*)op.al,
+                                                            gate);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void tc_split_phases(const Tables& tb, const TcOperands& op, int rows, void* hi, void* lo, cudaStream_t st)
+{
+    T2B_REQUIRE(rows >= tb.T, T2B_ERR_ARG, "phase operand rows");
+    k_split_img<<<std::min(rows, 16 * sms()), 128, 0, st>>>(nullptr, tb.ab_c, tb.T, rows, tb.T, tb.P, tb.kpix, tb.nk,
+                                                           op.kdim, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, nullptr);
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -732,6 +750,7 @@ void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_
 int tc_slot_proposals() { return MAP_PGH; }
 int tc_slot_audit() { return MAP_IAH; }
 int tc_slot_rescore() { return MAP_RAH; }
+int tc_slot_phases() { return MAP_ABH; }
 
 void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows)
 {
@@ -773,20 +792,22 @@ void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float
 }
 
 // Restricted coarse pass: every particle against its own proposals only.
-// Tiles of ppt particles: A = gathered proposal projections (slots MAP_PGH/PGL,
-// 128 rows per tile), B = the particles' shifted images (rows from tile*ppt*T;
-// tn = 96: one particle per tile through the 96-row-box maps MAP_IH96/IL96,
-// tn = 256: MAP_IH/IL).  Runs while *w.gate != 0.
-void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, int tn, const float* nprop,
+// Cross term C[b, j][t] = Re sum_p P_oc(j)[p] conj(cvec_b[p] ab_t[p])
+//                       = Re sum_p (P_oc(j)[p] conj(cvec_b[p])) conj(ab_t[p]),
+// so the A rows (slots MAP_PGH/PGL, row b*kslot + j) hold the proposal times the
+// conjugate particle image (k_prop_gather) and B is the T phase rows ab_t (slots
+// MAP_ABH/ABL, a tn-row box), shared by every tile and resident in L2.  Tiles of
+// 128 / kslot particles.  Runs while *w.gate != 0.
+void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, int tn, const float* nprop,
                     cudaStream_t st)
 {
-    T2B_REQUIRE(ppt >= 1 && ppt * kslot <= TM && ppt * tb.T <= tn && w.kprop <= kslot && (tn == 96 || tn == TN),
+    T2B_REQUIRE((kslot == 64 || kslot == TM) && w.kprop <= kslot && tb.T <= tn && tn % 32 == 0 && tn <= TN,
                 T2B_ERR_STATE, "proposal tile shape");
     TcParams p{};
     p.mode = 1;
-    p.ppt = ppt;
+    p.ppt = TM / kslot;
     p.kslot = kslot;
-    p.m_tiles = (w.n + ppt - 1) / ppt;
+    p.m_tiles = (w.n + p.ppt - 1) / p.ppt;
     p.n_tiles = 1;
     p.kblocks = op.kdim / TK;
     p.KO = w.kprop;
@@ -803,7 +824,7 @@ void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, in
     p.gate = w.gate;
     p.gate_run = 1;
     p.tn = tn;
-    launch_gemm(op, MAP_PGH, tn == 96 ? MAP_IH96 : MAP_IH, p, st);
+    launch_gemm(op, MAP_PGH, MAP_ABH, p, st);
 }
 
 // Full coarse pass of the audited particles: dense tiles over every

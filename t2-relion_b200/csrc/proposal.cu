@@ -461,13 +461,15 @@ __global__ void __launch_bounds__(1024) k_rescore_select(const int* __restrict__
 }
 
 // ---------------------------------------------- proposal coarse operands
-// Gathered split-BF16 projection rows of every (particle, proposal), copied
-// from the configuration's coarse operand (16-byte copies), and its norm
-// N = sum_k w2_k |P|^2_k from the same split-BF16 operands the full pass's norm
-// contraction reads (|P|^2 hi + lo per orientation, w2 hi + lo per particle).
-// Row of (b, j) in the A operand: b * kslot + j (tile i starts at row i * ppt * kslot).
-// Runs while *gate != 0.
-__global__ void __launch_bounds__(256) k_prop_gather(Work w, int ppt, int kslot, int kdim, int kn,
+// A rows of the proposal contraction: for every (particle b, proposal j) the
+// projection of orientation oc = prop[b][j] times the conjugate particle image,
+// P_oc[p] conj(cvec_b[p]) over the in-radius pixels (P_oc = hi + lo of the
+// configuration's split-BF16 coarse operand), split again into hi + lo; and the
+// norm N = sum_k w2_k |P|^2_k from the same split-BF16 operands the full pass's
+// norm contraction reads (|P|^2 hi + lo per orientation, w2 hi + lo per particle).
+// Row of (b, j): b * kslot + j.  Runs while *gate != 0.
+__global__ void __launch_bounds__(128) k_prop_gather(Work w, int P, const int* __restrict__ kpix, int nk, int kslot,
+                                                     int kdim, int kn,
                                                      const bf16* __restrict__ bh, const bf16* __restrict__ bl,
                                                      const bf16* __restrict__ nh, const bf16* __restrict__ nl,
                                                      const bf16* __restrict__ wh, const bf16* __restrict__ wl,
@@ -479,15 +481,43 @@ __global__ void __launch_bounds__(256) k_prop_gather(Work w, int ppt, int kslot,
     if (b >= w.n || j >= w.kprop) return;
     const size_t oc = (size_t)w.prop[(size_t)b * w.kprop + j];
     const size_t row = (size_t)b * kslot + j;
-    (void)ppt;
     {
         const uint4* sh = reinterpret_cast<const uint4*>(bh + oc * kdim);
         const uint4* sl = reinterpret_cast<const uint4*>(bl + oc * kdim);
+        const int4* kp4 = reinterpret_cast<const int4*>(kpix);
+        const float2* cb = w.cvec + (size_t)b * P;
         uint4* dh = reinterpret_cast<uint4*>(ph + row * kdim);
         uint4* dl = reinterpret_cast<uint4*>(pl + row * kdim);
         for (int v = threadIdx.x; v < kdim / 8; v += blockDim.x) {
-            dh[v] = sh[v];
-            dl[v] = sl[v];
+            const uint4 hv = sh[v], lv = sl[v];
+            const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&hv);
+            const __nv_bfloat162* lp = reinterpret_cast<const __nv_bfloat162*>(&lv);
+            // pixel indices of these 4 values: one 16-byte load when all are in radius
+            int kk[4];
+            if (4 * v + 3 < nk) {
+                const int4 k4 = kp4[v];
+                kk[0] = k4.x; kk[1] = k4.y; kk[2] = k4.z; kk[3] = k4.w;
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; e++) kk[e] = 4 * v + e < nk ? kpix[4 * v + e] : 0;
+            }
+            __nv_bfloat162 h[4], l[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                float2 a = make_float2(0.f, 0.f);
+                if (4 * v + e < nk) {
+                    const float2 hf = __bfloat1622float2(hp[e]), lf = __bfloat1622float2(lp[e]);
+                    const float2 pv = make_float2(hf.x + lf.x, hf.y + lf.y);
+                    const float2 c = cb[kk[e]];
+                    a = make_float2(pv.x * c.x + pv.y * c.y, pv.y * c.x - pv.x * c.y);
+                }
+                const bf16 hx = __float2bfloat16_rn(a.x), hy = __float2bfloat16_rn(a.y);
+                h[e] = __halves2bfloat162(hx, hy);
+                l[e] = __halves2bfloat162(__float2bfloat16_rn(a.x - __bfloat162float(hx)),
+                                          __float2bfloat16_rn(a.y - __bfloat162float(hy)));
+            }
+            dh[v] = *reinterpret_cast<const uint4*>(h);
+            dl[v] = *reinterpret_cast<const uint4*>(l);
         }
     }
     const uint4* nhv = reinterpret_cast<const uint4*>(nh + oc * kn);
@@ -538,10 +568,12 @@ __global__ void k_audit_begin(PropState* ps, int* audit_b, int n, int every, int
         for (int b = threadIdx.x; b < n; b += blockDim.x) r_audit[b] = -1.;
 }
 
-// image operand rows, w2 and c0 of the audited particles into the audit slots
+// image operand rows of the audited particles (cvec_b ab_t over the in-radius
+// pixels, split-BF16, as the full pass's operand), their w2 and c0, into the
+// audit slots
 __global__ void __launch_bounds__(256) k_audit_operands(const PropState* ps, const int* audit_b, Work w, int T, int P,
                                                         const int* __restrict__ kpix, int nk, int kn,
-                                                        int kdim, const bf16* __restrict__ ih, const bf16* __restrict__ il,
+                                                        int kdim, const float2* __restrict__ ab,
                                                         bf16* __restrict__ iah, bf16* __restrict__ ial,
                                                         float* __restrict__ w2a, float* __restrict__ c0a)
 {
@@ -550,10 +582,22 @@ __global__ void __launch_bounds__(256) k_audit_operands(const PropState* ps, con
     const int b = audit_b[a];
     const int t = blockIdx.x;  // t == T: the w2 / c0 row
     if (t < T) {
-        const size_t src = ((size_t)b * T + t) * kdim, dst = ((size_t)a * T + t) * kdim;
-        for (int k = threadIdx.x; k < kdim / 8; k += blockDim.x) {
-            reinterpret_cast<uint4*>(iah + dst)[k] = reinterpret_cast<const uint4*>(ih + src)[k];
-            reinterpret_cast<uint4*>(ial + dst)[k] = reinterpret_cast<const uint4*>(il + src)[k];
+        const size_t dst = ((size_t)a * T + t) * kdim;
+        const float2* cb = w.cvec + (size_t)b * P;
+        const float2* at = ab + (size_t)t * P;
+        __nv_bfloat162* dh = reinterpret_cast<__nv_bfloat162*>(iah + dst);
+        __nv_bfloat162* dl = reinterpret_cast<__nv_bfloat162*>(ial + dst);
+        for (int k = threadIdx.x; k < kdim / 2; k += blockDim.x) {
+            float2 v = make_float2(0.f, 0.f);
+            if (k < nk) {
+                const int pp = kpix[k];
+                const float2 c = cb[pp], e = at[pp];
+                v = make_float2(c.x * e.x - c.y * e.y, c.x * e.y + c.y * e.x);
+            }
+            const bf16 hx = __float2bfloat16_rn(v.x), hy = __float2bfloat16_rn(v.y);
+            dh[k] = __halves2bfloat162(hx, hy);
+            dl[k] = __halves2bfloat162(__float2bfloat16_rn(v.x - __bfloat162float(hx)),
+                                       __float2bfloat16_rn(v.y - __bfloat162float(hy)));
         }
     } else {
         for (int k = threadIdx.x; k < kn; k += blockDim.x)
@@ -1424,6 +1468,13 @@ void net_setup(t2b_ctx* c, int na_max)
     N.nprop = (float*)net_dalloc(W, (size_t)B * 128 * sizeof(float));
     tc_set_map(c->tc, tc_slot_proposals(), N.pg_h, (int)pg_rows, op.kdim, true);
     tc_set_map(c->tc, tc_slot_proposals() + 1, N.pg_l, (int)pg_rows, op.kdim, true);
+    // the B operand of the proposal tiles: the phase rows, zero beyond T
+    const int ab_rows = (tb.T + 31) / 32 * 32;
+    N.ab_h = net_dalloc(W, (size_t)ab_rows * op.kdim * sizeof(bf16));
+    N.ab_l = net_dalloc(W, (size_t)ab_rows * op.kdim * sizeof(bf16));
+    tc_split_phases(tb, op, ab_rows, N.ab_h, N.ab_l, 0);
+    tc_set_map_box(c->tc, tc_slot_phases(), N.ab_h, ab_rows, op.kdim, ab_rows);
+    tc_set_map_box(c->tc, tc_slot_phases() + 1, N.ab_l, ab_rows, op.kdim, ab_rows);
     // audit
     N.na_max = std::max(1, std::min(B, na_max));
     const int ia_rows = (N.na_max * tb.T + 255) / 256 * 256;
@@ -1450,26 +1501,13 @@ void net_setup(t2b_ctx* c, int na_max)
     N.ready = true;
 }
 
-// Proposal tiles: one particle per 128 x 96 tile (its proposals x its
-// translations) when T <= 96, with 64 rows per particle in the gathered operand
-// when k <= 64 (the tile's other 64 rows are the next particle's, read from L2
-// and discarded); otherwise 128 x 256 tiles of two particles with up to 64
-// proposals each, or of one particle.
+// Proposal tiles: 128 rows of (particle, proposal), 64 rows per particle when
+// k <= 64 (two particles per tile), else 128, against the T phase rows padded to a
+// multiple of 32 columns.
 void set_tile_shape(ProposalNet& N, int T)
 {
-    if (T <= 96) {
-        N.ppt = 1;
-        N.kslot = N.kprop <= 64 ? 64 : 128;
-        N.tn = 96;
-    } else if (N.kprop <= 64 && 2 * T <= 256) {
-        N.ppt = 2;
-        N.kslot = 64;
-        N.tn = 256;
-    } else {
-        N.ppt = 1;
-        N.kslot = 128;
-        N.tn = 256;
-    }
+    N.kslot = N.kprop <= 64 ? 64 : 128;
+    N.tn = (T + 31) / 32 * 32;
 }
 
 // dense layers of the inference path: x0b (n rows) -> logits (n x KO, no bias)
@@ -1617,8 +1655,7 @@ void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev)
     const int KO = tb.K * tb.O;
     k_audit_begin<<<1, 256, 0, st>>>(N.ps, N.audit_b, w.n, N.every, N.na_max, N.minkeya, N.asum, w.r_audit);
     k_audit_operands<<<dim3(tb.T + 1, N.na_max), 256, 0, st>>>(N.ps, N.audit_b, w, tb.T, tb.P, tb.kpix, tb.nk, op.kn,
-                                                               op.kdim,
-                                                               (const bf16*)op.ah, (const bf16*)op.al, (bf16*)N.ia_h,
+                                                               op.kdim, tb.ab_c, (bf16*)N.ia_h,
                                                                (bf16*)N.ia_l, N.w2a, N.c0a);
     k_audit_norms<<<(KO * 32 + 255) / 256, 256, 0, st>>>(KO, op.kn, N.ps, (const bf16*)op.nh, (const bf16*)op.nl,
                                                         N.w2a, N.na_max, N.norma);
@@ -1637,14 +1674,15 @@ void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev
     ProposalNet& N = *c->net;
     const Tables& tb = c->tb;
     const TcOperands& op = c->tc;
-    k_prop_gather<<<dim3(N.kprop, w.n), 128, 0, st>>>(w, N.ppt, N.kslot, op.kdim, op.kn, (const bf16*)op.bh,
+    k_prop_gather<<<dim3(N.kprop, w.n), 128, 0, st>>>(w, tb.P, tb.kpix, tb.nk, N.kslot, op.kdim, op.kn,
+                                                      (const bf16*)op.bh,
                                                       (const bf16*)op.bl, (const bf16*)op.nh, (const bf16*)op.nl,
                                                       (const bf16*)op.wh, (const bf16*)op.wl, (bf16*)N.pg_h,
                                                       (bf16*)N.pg_l, N.nprop);
     (void)tb;
     T2B_CUDA(cudaGetLastError());
     if (ev) cudaEventRecord(ev[0], st);
-    tc_launch_prop(tb, w, c->tc, N.ppt, N.kslot, N.tn, N.nprop, st);
+    tc_launch_prop(tb, w, c->tc, N.kslot, N.tn, N.nprop, st);
     if (ev) cudaEventRecord(ev[1], st);
 }
 

@@ -47,7 +47,7 @@ struct ProposalNet {
     void* thb = nullptr;               // BF16 copy of th (every forward pass reads it)
     bool ready = false;                // workspace matches the configuration
     bool enabled = false;
-    int kprop = 64, every = 50, na_max = 0, ppt = 1, kslot = 128, tn = 256, b_pad = 0;
+    int kprop = 64, every = 50, na_max = 0, kslot = 128, tn = 96, b_pad = 0;
     int k1 = 0;                        // network candidates rescored at low resolution (0: none)
     int kr = 0;                        // K of the rescoring contraction (2 x ring pixels, padded)
     float2* projR = nullptr;           // K*O x nring: projections at the ring pixels (FP32)
@@ -67,6 +67,7 @@ struct ProposalNet {
     int* prop = nullptr;
     void* maps = nullptr;              // 6 tensor maps: W1, X0b, W2, H1b, W3, H2b
     void *pg_h = nullptr, *pg_l = nullptr;
+    void *ab_h = nullptr, *ab_l = nullptr;   // phase rows ab_t of the translations (split-BF16, tn rows)
     float* nprop = nullptr;
     PropState* ps = nullptr;
     int* audit_b = nullptr;

@@ -215,7 +215,7 @@ struct TcOperands {
 constexpr int TC_MAP_SLOTS = 24;
 size_t tc_kdim(int nk);
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
-void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st);
+void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate);
 void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate = nullptr,
                      int gate_run = 0);
 size_t tc_kn(int nk);
@@ -231,8 +231,10 @@ void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int
 void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* norms, const unsigned char* skip,
                        const int* cand, const double* pdf_t, const double* pdf_oc, float* score, int* err,
                        cudaStream_t st);
-void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int ppt, int kslot, int tn, const float* nprop,
+void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, int tn, const float* nprop,
                     cudaStream_t st);
+void tc_split_phases(const Tables& tb, const TcOperands& op, int rows, void* hi, void* lo, cudaStream_t st);
+int tc_slot_phases();
 void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
                      unsigned* minkeya, int* err, cudaStream_t st);
 int tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* out, int products, int* err,

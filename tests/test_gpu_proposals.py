@@ -177,3 +177,28 @@ def test_graph_batch_with_proposals_matches_host(trained):
     assert np.array_equal(got["pose"], ref["pose"])
     assert np.allclose(got["sum_weight"], ref["sum_weight"], rtol=1e-9)
     assert np.allclose(got["audit_mass"], ref["audit_mass"], rtol=1e-9)
+
+
+def test_proposal_diff2_matches_full_pass(trained):
+    """The restricted coarse pass (premultiplied proposal rows against the shared phase
+    rows) against the full coarse pass at the same (orientation, translation): both
+    split-BF16 contractions of the same sums, within 1e-5 of the diff2 scale."""
+    es, P = trained["es"], trained["parts"]
+    n = 16
+    es.enable_proposals(topk=64, rescore=512, audit_every=1000, audit_mass=1e-6)
+    got = es.expectation(P["fimg"][:n], P["ctf"][:n], P["minv"][:n], P["scalars"][:n])
+    assert np.all(got["learned"] == 1)
+    props = [es.proposals(b) for b in range(n)]
+    es.disable_proposals()
+    es.expectation(P["fimg"][:n], P["ctf"][:n], P["minv"][:n], P["scalars"][:n])
+    T = trained["samp"]["n_trans"]
+    worst = 0.0
+    for b, (prop, d2) in enumerate(props):
+        assert len(np.unique(prop)) == len(prop)
+        full = es.coarse_diff2(b).reshape(-1, T)[prop]
+        live = full > -998          # skipped orientations hold -999 in both
+        assert np.array_equal(live, d2 > -998)
+        scale = np.max(np.abs(full[live]))
+        worst = max(worst, np.max(np.abs(d2[live] - full[live])) / scale)
+    print("proposal diff2 vs full pass, max relative deviation:", worst)
+    assert worst <= 1e-5
