@@ -609,7 +609,7 @@ size_t tc_kn(int nk) { return (size_t)((nk + TK - 1) / TK) * TK; }
 // descriptor slots in op.maps (TC_MAP_SLOTS of 128 bytes)
 enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL,
        MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_ABH, MAP_ABL, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL,
-       MAP_IH128, MAP_IL128, MAP_COUNT };
+       MAP_IH128, MAP_IL128, MAP_WAH, MAP_WAL, MAP_COUNT };
 static_assert(MAP_COUNT <= TC_MAP_SLOTS, "tensor-map slots");
 static_assert(sizeof(CUtensorMap) == 128, "tensor-map size");
 
@@ -751,6 +751,7 @@ int tc_slot_proposals() { return MAP_PGH; }
 int tc_slot_audit() { return MAP_IAH; }
 int tc_slot_rescore() { return MAP_RAH; }
 int tc_slot_phases() { return MAP_ABH; }
+int tc_slot_audit_w2() { return MAP_WAH; }
 
 void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows)
 {
@@ -825,6 +826,29 @@ void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, 
     p.gate_run = 1;
     p.tn = tn;
     launch_gemm(op, MAP_PGH, MAP_ABH, p, st);
+}
+
+// Norms of the audited particles N[a][oc] = sum_k w2_a[k] |P_oc|^2_k: the full
+// pass's norm contraction (|P|^2 operand MAP_NH/NL) against the audit slots' w2
+// rows (MAP_WAH/WAL, split-BF16, 32-row box): 128 x 32 tiles, one pass over the
+// |P|^2 operand at the memory rate, the same sums as the full pass's norms.
+void tc_launch_audit_norms(const Tables& tb, TcOperands& op, int na_max, float* norma, int* err, cudaStream_t st)
+{
+    TcParams p{};
+    p.m_tiles = op.m_pad / TM;
+    p.n_tiles = (na_max + 31) / 32;
+    p.kblocks = op.kn / TK;
+    p.raw = 1;
+    p.KO = tb.K * tb.O;
+    p.T = 1;
+    p.ncols = na_max;
+    p.skip = tb.skip;
+    p.d2c = norma;
+    p.err = err;
+    p.products = 3;
+    p.group = op.group_m;
+    p.tn = 32;
+    launch_gemm(op, MAP_NH, MAP_WAH, p, st);
 }
 
 // Full coarse pass of the audited particles: dense tiles over every

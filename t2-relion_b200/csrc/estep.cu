@@ -1217,6 +1217,17 @@ __global__ void __launch_bounds__(256) k_argmax_fine(Tables tb, Work w)
 // ---------------------------------------------- weighted sums + backprojection
 constexpr int ENT_CAP = 512;
 
+// Fire-and-forget FP32 reductions into the grids (red: no value comes back, so the
+// warp does not hold a register for the reply as with an atomic whose result is unused)
+__device__ __forceinline__ void red_add(float* p, float v)
+{
+    asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ void red_add2(float2* p, float x, float y)
+{
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(x), "f"(y) : "memory");
+}
+
 struct GridPtrs {
     float2* const* data;
     float* const* weight;
@@ -1368,8 +1379,8 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
 #pragma unroll
                                 for (int cc = 0; cc < 8; cc++) {
                                     const size_t idx = ((size_t)(z0 + (cc >> 2)) * g.ydim + y0 + ((cc >> 1) & 1)) * g.xdim + x0 + (cc & 1);
-                                    atomicAdd(&gd[idx], make_float2(dd[cc] * vr, dd[cc] * vi));
-                                    atomicAdd(&gw[idx], dd[cc] * fw);
+                                    red_add2(&gd[idx], dd[cc] * vr, dd[cc] * vi);
+                                    red_add(&gw[idx], dd[cc] * fw);
                                 }
                             } else {
                                 if (x0 < 0 || x0 + 1 >= g.xdim || y0 < 0 || y0 + 1 >= g.ydim) continue;
@@ -1378,8 +1389,8 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
 #pragma unroll
                                 for (int cc = 0; cc < 4; cc++) {
                                     const size_t idx = (size_t)(y0 + (cc >> 1)) * g.xdim + x0 + (cc & 1);
-                                    atomicAdd(&gd[idx], make_float2(dd[cc] * vr, dd[cc] * vi));
-                                    atomicAdd(&gw[idx], dd[cc] * fw);
+                                    red_add2(&gd[idx], dd[cc] * vr, dd[cc] * vi);
+                                    red_add(&gw[idx], dd[cc] * fw);
                                 }
                             }
                         }

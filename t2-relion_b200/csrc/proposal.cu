@@ -575,7 +575,8 @@ __global__ void __launch_bounds__(256) k_audit_operands(const PropState* ps, con
                                                         const int* __restrict__ kpix, int nk, int kn,
                                                         int kdim, const float2* __restrict__ ab,
                                                         bf16* __restrict__ iah, bf16* __restrict__ ial,
-                                                        float* __restrict__ w2a, float* __restrict__ c0a)
+                                                        bf16* __restrict__ wah, bf16* __restrict__ wal,
+                                                        float* __restrict__ c0a)
 {
     const int a = blockIdx.y;
     if (a >= ps->na) return;
@@ -600,55 +601,13 @@ __global__ void __launch_bounds__(256) k_audit_operands(const PropState* ps, con
                                        __float2bfloat16_rn(v.y - __bfloat162float(hy)));
         }
     } else {
-        for (int k = threadIdx.x; k < kn; k += blockDim.x)
-            w2a[(size_t)a * kn + k] = k < nk ? w.w2[(size_t)b * P + kpix[k]] : 0.f;
+        for (int k = threadIdx.x; k < kn; k += blockDim.x) {
+            const float v = k < nk ? w.w2[(size_t)b * P + kpix[k]] : 0.f;
+            const bf16 h = __float2bfloat16_rn(v);
+            wah[(size_t)a * kn + k] = h;
+            wal[(size_t)a * kn + k] = __float2bfloat16_rn(v - __bfloat162float(h));
+        }
         if (threadIdx.x == 0) c0a[a] = w.c0[b];
-    }
-}
-
-// audit norms N[a][oc] = sum_k w2a[a][k] |P_oc|^2_k for every audit slot in one
-// pass over the split-BF16 |P|^2 operand (hi + lo, the norm GEMM's A operand;
-// k the in-radius pixel index, rows of kn elements, zero beyond nk); one warp
-// per orientation, 8 elements (16 bytes) per lane and load
-constexpr int AUDIT_NORM_SLOTS = 4;
-__global__ void __launch_bounds__(256) k_audit_norms(int KO, int kn, const PropState* ps, const bf16* __restrict__ nh,
-                                                     const bf16* __restrict__ nl, const float* __restrict__ w2a,
-                                                     int na_max, float* __restrict__ norma)
-{
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= KO) return;
-    const int na = min(ps->na, na_max);
-    const uint4* h = reinterpret_cast<const uint4*>(nh + (size_t)warp * kn);
-    const uint4* l = reinterpret_cast<const uint4*>(nl + (size_t)warp * kn);
-    const int nv = kn / 8;
-    for (int a0 = 0; a0 < na; a0 += AUDIT_NORM_SLOTS) {
-        float acc[AUDIT_NORM_SLOTS] = {};
-        for (int v = lane; v < nv; v += 32) {
-            const uint4 hv = h[v], lv = l[v];
-            const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&hv);
-            const __nv_bfloat162* lp = reinterpret_cast<const __nv_bfloat162*>(&lv);
-            float x[8];
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const float2 hf = __bfloat1622float2(hp[e]), lf = __bfloat1622float2(lp[e]);
-                x[2 * e] = hf.x + lf.x;
-                x[2 * e + 1] = hf.y + lf.y;
-            }
-#pragma unroll
-            for (int a = 0; a < AUDIT_NORM_SLOTS; a++) {
-                if (a0 + a >= na) break;
-                const float4* wp = reinterpret_cast<const float4*>(w2a + (size_t)(a0 + a) * kn + 8 * v);
-                const float4 w0 = wp[0], w1 = wp[1];
-                acc[a] += w0.x * x[0] + w0.y * x[1] + w0.z * x[2] + w0.w * x[3] + w1.x * x[4] + w1.y * x[5] +
-                          w1.z * x[6] + w1.w * x[7];
-            }
-        }
-#pragma unroll
-        for (int a = 0; a < AUDIT_NORM_SLOTS; a++) {
-            float v = acc[a];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0 && a0 + a < na) norma[(size_t)(a0 + a) * KO + warp] = v;
-        }
     }
 }
 
@@ -1487,13 +1446,18 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.ia_l, 0, (size_t)ia_rows * op.kdim * sizeof(bf16)));
     tc_set_map(c->tc, tc_slot_audit(), N.ia_h, ia_rows, op.kdim, false);
     tc_set_map(c->tc, tc_slot_audit() + 1, N.ia_l, ia_rows, op.kdim, false);
-    N.w2a = (float*)net_dalloc(W, (size_t)N.na_max * std::max(P, op.kn) * sizeof(float));
+    const int wa_rows = (N.na_max + 31) / 32 * 32;
+    N.wa_h = net_dalloc(W, (size_t)wa_rows * op.kn * sizeof(bf16));
+    N.wa_l = net_dalloc(W, (size_t)wa_rows * op.kn * sizeof(bf16));
+    T2B_CUDA(cudaMemset(N.wa_h, 0, (size_t)wa_rows * op.kn * sizeof(bf16)));
+    T2B_CUDA(cudaMemset(N.wa_l, 0, (size_t)wa_rows * op.kn * sizeof(bf16)));
+    tc_set_map_box(c->tc, tc_slot_audit_w2(), N.wa_h, wa_rows, op.kn, 32);
+    tc_set_map_box(c->tc, tc_slot_audit_w2() + 1, N.wa_l, wa_rows, op.kn, 32);
     N.c0a = (float*)net_dalloc(W, (size_t)N.na_max * sizeof(float));
     N.norma = (float*)net_dalloc(W, (size_t)N.na_max * KO * sizeof(float));
     N.d2a = (float*)net_dalloc(W, (size_t)N.na_max * KO * tb.T * sizeof(float));
     N.minkeya = (unsigned*)net_dalloc(W, (size_t)N.na_max * sizeof(unsigned));
     N.asum = (double*)net_dalloc(W, (size_t)N.na_max * 2 * sizeof(double));
-    T2B_CUDA(cudaMemset(N.w2a, 0, (size_t)N.na_max * std::max(P, op.kn) * sizeof(float)));
     T2B_CUDA(cudaMemset(N.c0a, 0, (size_t)N.na_max * sizeof(float)));
     T2B_CUDA(cudaMemset(N.norma, 0, (size_t)N.na_max * KO * sizeof(float)));
     T2B_CUDA(cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, KO * (int)sizeof(unsigned)));
@@ -1656,9 +1620,8 @@ void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev)
     k_audit_begin<<<1, 256, 0, st>>>(N.ps, N.audit_b, w.n, N.every, N.na_max, N.minkeya, N.asum, w.r_audit);
     k_audit_operands<<<dim3(tb.T + 1, N.na_max), 256, 0, st>>>(N.ps, N.audit_b, w, tb.T, tb.P, tb.kpix, tb.nk, op.kn,
                                                                op.kdim, tb.ab_c, (bf16*)N.ia_h,
-                                                               (bf16*)N.ia_l, N.w2a, N.c0a);
-    k_audit_norms<<<(KO * 32 + 255) / 256, 256, 0, st>>>(KO, op.kn, N.ps, (const bf16*)op.nh, (const bf16*)op.nl,
-                                                        N.w2a, N.na_max, N.norma);
+                                                               (bf16*)N.ia_l, (bf16*)N.wa_h, (bf16*)N.wa_l, N.c0a);
+    tc_launch_audit_norms(tb, op, N.na_max, N.norma, w.err, st);
     T2B_CUDA(cudaGetLastError());
     if (ev) cudaEventRecord(ev[0], st);
     tc_launch_audit(tb, op, N.na_max, N.c0a, N.norma, N.d2a, N.minkeya, w.err, st);

@@ -72,7 +72,8 @@ struct ProposalNet {
     PropState* ps = nullptr;
     int* audit_b = nullptr;
     void *ia_h = nullptr, *ia_l = nullptr;
-    float *w2a = nullptr, *c0a = nullptr, *norma = nullptr, *d2a = nullptr;
+    float *c0a = nullptr, *norma = nullptr, *d2a = nullptr;
+    void *wa_h = nullptr, *wa_l = nullptr;   // w2 of the audit slots (split-BF16, kn wide, 32-row padded)
     unsigned* minkeya = nullptr;
     double* asum = nullptr;
 };
