@@ -60,9 +60,9 @@ PROP = dict(topk=64, rescore=1024, audit_every=50, audit_mass=0.999)
 E2E_STEPS = 30
 # DRAM bytes (read + write) of the audit + proposal k_diff2_tc launches of one learned step
 # at 128 particles, from one ncu capture
-# (audit 766.02 MB read + 18.59 MB written, proposal pass 548.33 MB + 0.46 MB;
+# (audit 766.18 MB read + 18.58 MB written, proposal pass 169.91 MB + 0.40 MB;
 # profiles/k_diff2_tc_box128_learned_b128_dram.md)
-LEARNED_TRAFFIC = 766.02e6 + 18.59e6 + 548.33e6 + 0.46e6
+LEARNED_TRAFFIC = 766.18e6 + 18.58e6 + 169.91e6 + 0.40e6
 
 
 def build_problem(t2b, sy, n_particles, seed):
@@ -775,10 +775,9 @@ def main():
         f_prop = 8.0 * PROP["topk"] * T * P * B
         ntile_audit = ((K * O + 127) // 128) * ((int(np.ceil(B / PROP["audit_every"])) * T + 255) // 256)
         tile_flops = 128 * 256 * kdim * 2 * 3.0
-        if T <= 96:      # one particle per 128 x 96 tile
-            prop_exec = B * 128 * 96 * kdim * 2 * 3.0
-        else:
-            prop_exec = ((B + 1) // 2 if (PROP["topk"] <= 64 and 2 * T <= 256) else B) * tile_flops
+        # proposal tiles: 128 rows of 128 / kslot particles x T phase rows padded to 32 columns
+        ppt = 2 if PROP["topk"] <= 64 else 1
+        prop_exec = ((B + ppt - 1) // ppt) * 128 * ((T + 31) // 32 * 32) * kdim * 2 * 3.0
         executed = (ntile_audit * tile_flops + prop_exec) / ((t_audit + t_prop) / 1000.0) / 1e12
         peak = peaks.get("bf16_tflops_sustained", 1400.0)
         achieved = (f_audit + f_prop) / ((t_audit + t_prop) / 1000.0) / 1e12

@@ -363,22 +363,37 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             __syncwarp();
             const int nchunk = (p.tn ? p.tn : TN) / 32;
             if (p.mode == 2) {
-                // the thread's row straight from TMEM (32x32b: lane = row, 32 columns per load);
-                // online log-sum-exp over the translations
-                float m = -INFINITY, sacc = 0.f;
+                // the thread's row straight from TMEM (32x32b: lane = row, 32 columns per load):
+                // score = M + log sum_t pdf_t exp(C_t - M), M = max_t C_t, in two passes over
+                // TMEM (the max, then the sum) with no data-dependent branch; pdf_t of column
+                // c*32 + e is held by lane e (as FP32) and broadcast by a shuffle
                 const double* pt = p.pdf_t + (size_t)bfirst * p.T;
-                for (int c = 0; c < nchunk; c++) {
+                float wv[TN / 32];
+#pragma unroll
+                for (int c = 0; c < TN / 32; c++) {
+                    const int t = c * 32 + lane;
+                    wv[c] = (c < nchunk && t < p.T && bfirst < p.ncols) ? (float)pt[t] : 0.f;
+                }
+                float m = -INFINITY;
+#pragma unroll
+                for (int c = 0; c < TN / 32; c++) {
+                    if (c >= nchunk) break;
+                    uint32_t v[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
+#pragma unroll
+                    for (int e = 0; e < 32; e++)
+                        if (c * 32 + e < p.T) m = fmaxf(m, __uint_as_float(v[e]));
+                }
+                float sacc = 0.f;
+#pragma unroll
+                for (int c = 0; c < TN / 32; c++) {
+                    if (c >= nchunk) break;
                     uint32_t v[32];
                     tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
 #pragma unroll
                     for (int e = 0; e < 32; e++) {
-                        const int t = c * 32 + e;
-                        if (t < p.T) {
-                            const float x = __uint_as_float(v[e]);
-                            const float w = (float)pt[t];
-                            if (x > m) { sacc = sacc * __expf(m - x) + w; m = x; }
-                            else sacc += w * __expf(x - m);
-                        }
+                        const float w = __shfl_sync(0xffffffffu, wv[c], e);
+                        if (c * 32 + e < p.T) sacc += w * __expf(__uint_as_float(v[e]) - m);
                     }
                 }
                 const int j = jbase + q * 32 + lane;
