@@ -192,6 +192,12 @@ struct TcParams {
     // d2c[b*KO + j] = log sum_t pdf_t exp(C_t) - norm_j + log pdf_o(j)  (c0 omitted)
     const double* pdf_t;      // n x T
     const double* pdf_oc;     // K*O
+    // mode 1 with ksplit = 2: the two K slices of an m-tile run on two CTAs; each epilogue
+    // warp stores its slice's accumulator rows in part (per m-tile, slice, warp: nchunk x
+    // 32 x 32 floats, column-major in the lane), and the warp that arrives second on
+    // fix[m-tile * 4 + warp] (zero before the launch) adds the other slice's and emits
+    float* part;
+    int* fix;
 };
 
 // maps: device array of tensor-map descriptors (encoded once per configuration);
@@ -263,7 +269,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 ya = mt * TM;
                 yb = nt * tn_l;
             } else if (p.mode == 1) {
-                ya = tile * TM;
+                ya = (tile / ksp) * TM;
                 yb = 0;
             } else {
                 ya = tile * TM;
@@ -342,8 +348,9 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             tc_fence_after();
             const int n0 = nt * tn_l;
             const int mtp = p.mtp ? p.mtp : 1;
-            const int bfirst = p.mode == 0 ? n0 / p.T : (tile / mtp) * p.ppt;
-            const int jbase = p.mode == 0 ? 0 : (tile % mtp) * TM;
+            const int tt = tile / ksp;   // the m-tile (modes 1, 2)
+            const int bfirst = p.mode == 0 ? n0 / p.T : (tt / mtp) * p.ppt;
+            const int jbase = p.mode == 0 ? 0 : (tt % mtp) * TM;
             for (int i = lane; i < TN + 2; i += 32) wmin[i] = 0xffffffffu;
             // proposal tiles: the per-row data of the warp's 32 rows (orientation skip flag
             // and norm), one row per lane, broadcast by shuffles in the chunk loop below
@@ -362,6 +369,32 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             }
             __syncwarp();
             const int nchunk = (p.tn ? p.tn : TN) / 32;
+            // split-K proposal tiles: exchange the slices' partial sums through global memory;
+            // the sum own + other is the same whichever slice finishes second
+            const float* other = nullptr;
+            bool emit = true;
+            if (p.mode == 1 && ksp == 2) {
+                const int slice = tile % ksp;
+                const size_t wsz = (size_t)nchunk * 1024;
+                float* mine = p.part + (((size_t)tt * 2 + slice) * 4 + q) * wsz;
+                for (int c = 0; c < nchunk; c++) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
+#pragma unroll
+                    for (int e = 0; e < 32; e++) mine[(size_t)c * 1024 + e * 32 + lane] = __uint_as_float(v[e]);
+                }
+                __threadfence();
+                __syncwarp();
+                int first = 0;
+                if (lane == 0) first = atomicAdd(&p.fix[tt * 4 + q], 1) == 0;
+                first = __shfl_sync(0xffffffffu, first, 0);
+                if (first) {
+                    emit = false;
+                } else {
+                    __threadfence();
+                    other = p.part + (((size_t)tt * 2 + (1 - slice)) * 4 + q) * wsz;
+                }
+            }
             if (p.mode == 2) {
                 // the thread's row straight from TMEM (32x32b: lane = row, 32 columns per load):
                 // score = M + log sum_t pdf_t exp(C_t - M), M = max_t C_t, in two passes over
@@ -403,9 +436,14 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                                                            : m - my_norm + __logf(sacc) + (float)log(p.pdf_oc[p.prop[pj]]);
                 }
             }
-            for (int c = 0; c < (p.mode == 2 ? 0 : nchunk); c++) {
+            for (int c = 0; c < (p.mode == 2 || !emit ? 0 : nchunk); c++) {
                 uint32_t v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
+                if (other) {
+#pragma unroll
+                    for (int e = 0; e < 32; e++)
+                        v[e] = __float_as_uint(__uint_as_float(v[e]) + __ldcg(other + (size_t)c * 1024 + e * 32 + lane));
+                }
 #pragma unroll
                 for (int j = 0; j < 32; j++) sbuf[lane * EPI_LD + j] = __uint_as_float(v[j]);
                 __syncwarp();
@@ -676,7 +714,7 @@ void tc_init_attributes()
 
 static void launch_gemm(const TcOperands& op, int ia, int ib, TcParams& p, cudaStream_t st)
 {
-    const int grid = std::min(sms(), p.m_tiles * p.n_tiles);
+    const int grid = std::min(sms(), p.m_tiles * p.n_tiles * std::max(1, p.ksplit));
     k_diff2_tc<<<grid, NTHREADS, SMEM_BYTES, st>>>(static_cast<const CUtensorMap*>(op.maps), ia, ib, p);
     T2B_CUDA(cudaGetLastError());
 }
@@ -815,7 +853,7 @@ void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float
 // MAP_ABH/ABL, a tn-row box), shared by every tile and resident in L2.  Tiles of
 // 128 / kslot particles.  Runs while *w.gate != 0.
 void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, int tn, const float* nprop,
-                    cudaStream_t st)
+                    float* part, int* fix, int part_tiles, cudaStream_t st)
 {
     T2B_REQUIRE((kslot == 64 || kslot == TM) && w.kprop <= kslot && tb.T <= tn && tn % 32 == 0 && tn <= TN,
                 T2B_ERR_STATE, "proposal tile shape");
@@ -824,6 +862,14 @@ void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, 
     p.ppt = TM / kslot;
     p.kslot = kslot;
     p.m_tiles = (w.n + p.ppt - 1) / p.ppt;
+    // fewer m-tiles than half the SMs: two K slices per m-tile (the sum of the two partial
+    // accumulators is order-independent, so the result does not depend on the split)
+    if (part && fix && 2 * p.m_tiles <= sms() && p.m_tiles <= part_tiles && op.kdim / TK >= 2) {
+        p.ksplit = 2;
+        p.part = part;
+        p.fix = fix;
+        T2B_CUDA(cudaMemsetAsync(fix, 0, (size_t)p.m_tiles * 4 * sizeof(int), st));
+    }
     p.n_tiles = 1;
     p.kblocks = op.kdim / TK;
     p.KO = w.kprop;

@@ -1434,6 +1434,12 @@ void net_setup(t2b_ctx* c, int na_max)
     tc_split_phases(tb, op, ab_rows, N.ab_h, N.ab_l, 0);
     tc_set_map_box(c->tc, tc_slot_phases(), N.ab_h, ab_rows, op.kdim, ab_rows);
     tc_set_map_box(c->tc, tc_slot_phases() + 1, N.ab_l, ab_rows, op.kdim, ab_rows);
+    // split-K exchange buffers of the proposal tiles: up to half the SMs' worth of m-tiles
+    int nsm = 0;
+    T2B_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    N.part_tiles = std::max(1, nsm / 2);
+    N.part = (float*)net_dalloc(W, (size_t)N.part_tiles * 2 * 4 * (ab_rows / 32) * 1024 * sizeof(float));
+    N.fix = (int*)net_dalloc(W, (size_t)N.part_tiles * 4 * sizeof(int));
     // audit
     N.na_max = std::max(1, std::min(B, na_max));
     const int ia_rows = (N.na_max * tb.T + 255) / 256 * 256;
@@ -1645,7 +1651,7 @@ void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev
     (void)tb;
     T2B_CUDA(cudaGetLastError());
     if (ev) cudaEventRecord(ev[0], st);
-    tc_launch_prop(tb, w, c->tc, N.kslot, N.tn, N.nprop, st);
+    tc_launch_prop(tb, w, c->tc, N.kslot, N.tn, N.nprop, N.part, N.fix, N.part_tiles, st);
     if (ev) cudaEventRecord(ev[1], st);
 }
 

@@ -68,6 +68,9 @@ struct ProposalNet {
     void* maps = nullptr;              // 6 tensor maps: W1, X0b, W2, H1b, W3, H2b
     void *pg_h = nullptr, *pg_l = nullptr;
     void *ab_h = nullptr, *ab_l = nullptr;   // phase rows ab_t of the translations (split-BF16, tn rows)
+    float* part = nullptr;                   // split-K partial accumulators of the proposal tiles
+    int* fix = nullptr;                      // and their arrival counters
+    int part_tiles = 0;                      // m-tiles they cover
     float* nprop = nullptr;
     PropState* ps = nullptr;
     int* audit_b = nullptr;

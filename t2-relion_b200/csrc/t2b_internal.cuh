@@ -232,7 +232,7 @@ void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float
                        const int* cand, const double* pdf_t, const double* pdf_oc, float* score, int* err,
                        cudaStream_t st);
 void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, int tn, const float* nprop,
-                    cudaStream_t st);
+                    float* part, int* fix, int part_tiles, cudaStream_t st);
 void tc_split_phases(const Tables& tb, const TcOperands& op, int rows, void* hi, void* lo, cudaStream_t st);
 int tc_slot_phases();
 int tc_slot_audit_w2();
