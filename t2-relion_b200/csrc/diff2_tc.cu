@@ -100,6 +100,16 @@ __device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, uint
         : "memory");
 }
 
+// the same from a K-blocked operand ([k-block][row][64 elements]): one contiguous box
+__device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* map, uint64_t* bar, int y, int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
+            su32(dst)),
+        "l"(map), "r"(su32(bar)), "r"(0), "r"(y), "r"(z)
+        : "memory");
+}
+
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr)
 {
@@ -181,6 +191,7 @@ struct TcParams {
     // (particle, proposal); ncols = particles of the batch.
     // mode 2 tiles hold one particle (ppt = 1): B rows from tile*T (its own images).
     int mode, ppt, kslot;
+    int a3d;                  // the A maps are K-blocked 3D maps (coordinates (0, row, k-block))
     const int* prop;          // mode 1: global orientation of every (particle, proposal)
     const int* gate;          // run only when (*gate != 0) == gate_run (null: always)
     int gate_run;
@@ -281,8 +292,13 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
                 uint8_t* st = gbase + s * sbytes;
                 mbar_expect_tx(&full_bar[s], tx_bytes);
-                tma_load(st, mPh, &full_bar[s], kb * TK, ya);
-                if (p.products == 3) tma_load(st + A_BYTES, mPl, &full_bar[s], kb * TK, ya);
+                if (p.a3d) {
+                    tma_load3(st, mPh, &full_bar[s], ya, kb);
+                    if (p.products == 3) tma_load3(st + A_BYTES, mPl, &full_bar[s], ya, kb);
+                } else {
+                    tma_load(st, mPh, &full_bar[s], kb * TK, ya);
+                    if (p.products == 3) tma_load(st + A_BYTES, mPl, &full_bar[s], kb * TK, ya);
+                }
                 tma_load(st + 2 * A_BYTES, mIh, &full_bar[s], kb * TK, yb);
                 if (p.products >= 2) tma_load(st + 2 * A_BYTES + bbytes, mIl, &full_bar[s], kb * TK, yb);
                 issued[s] = 1;
@@ -644,6 +660,22 @@ CUtensorMap make_map(void* ptr, int rows, int kdim, int box_rows)
     return m;
 }
 
+// K-blocked operand: element (row, k) at ((k / 64) * rows + row) * 64 + k % 64, so a
+// 64-wide box of consecutive rows is one contiguous block of memory
+CUtensorMap make_map_blocked(void* ptr, int rows, int kdim, int box_rows)
+{
+    CUtensorMap m;
+    const cuuint64_t dims[3] = {(cuuint64_t)TK, (cuuint64_t)rows, (cuuint64_t)(kdim / TK)};
+    const cuuint64_t strides[2] = {(cuuint64_t)TK * 2, (cuuint64_t)rows * TK * 2};
+    const cuuint32_t box[3] = {(cuuint32_t)TK, (cuuint32_t)box_rows, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, ptr, dims, strides, box, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error{T2B_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    return m;
+}
+
 int sms()
 {
     int dev = 0, n = 0;
@@ -806,6 +838,13 @@ int tc_slot_rescore() { return MAP_RAH; }
 int tc_slot_phases() { return MAP_ABH; }
 int tc_slot_audit_w2() { return MAP_WAH; }
 
+void tc_set_map_blocked(TcOperands& op, int slot, void* ptr, int rows, int kdim)
+{
+    T2B_REQUIRE(slot >= MAP_PGH && slot < MAP_COUNT && op.maps && kdim % TK == 0, T2B_ERR_STATE, "bad tensor-map slot");
+    const CUtensorMap m = make_map_blocked(ptr, rows, kdim, TM);
+    T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * slot, &m, 128, cudaMemcpyHostToDevice));
+}
+
 void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows)
 {
     T2B_REQUIRE(slot >= MAP_PGH && slot < MAP_COUNT && op.maps, T2B_ERR_STATE, "bad tensor-map slot");
@@ -859,6 +898,7 @@ void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, 
                 T2B_ERR_STATE, "proposal tile shape");
     TcParams p{};
     p.mode = 1;
+    p.a3d = 1;
     p.ppt = TM / kslot;
     p.kslot = kslot;
     p.m_tiles = (w.n + p.ppt - 1) / p.ppt;

@@ -467,9 +467,11 @@ __global__ void __launch_bounds__(1024) k_rescore_select(const int* __restrict__
 // configuration's split-BF16 coarse operand), split again into hi + lo; and the
 // norm N = sum_k w2_k |P|^2_k from the same split-BF16 operands the full pass's
 // norm contraction reads (|P|^2 hi + lo per orientation, w2 hi + lo per particle).
-// Row of (b, j): b * kslot + j.  Runs while *gate != 0.
+// Row of (b, j): b * kslot + j, stored K-blocked (64-element k-blocks of all `rows`
+// rows one after the other: one contiguous tensor-core tile per k-block).
+// Runs while *gate != 0.
 __global__ void __launch_bounds__(128) k_prop_gather(Work w, int P, const int* __restrict__ kpix, int nk, int kslot,
-                                                     int kdim, int kn,
+                                                     int rows, int kdim, int kn,
                                                      const bf16* __restrict__ bh, const bf16* __restrict__ bl,
                                                      const bf16* __restrict__ nh, const bf16* __restrict__ nl,
                                                      const bf16* __restrict__ wh, const bf16* __restrict__ wl,
@@ -486,8 +488,10 @@ __global__ void __launch_bounds__(128) k_prop_gather(Work w, int P, const int* _
         const uint4* sl = reinterpret_cast<const uint4*>(bl + oc * kdim);
         const int4* kp4 = reinterpret_cast<const int4*>(kpix);
         const float2* cb = w.cvec + (size_t)b * P;
-        uint4* dh = reinterpret_cast<uint4*>(ph + row * kdim);
-        uint4* dl = reinterpret_cast<uint4*>(pl + row * kdim);
+        // 16-byte group v of the row: k-block v / 8, group v % 8 of its 64 elements
+        uint4* dh = reinterpret_cast<uint4*>(ph) + row * 8;
+        uint4* dl = reinterpret_cast<uint4*>(pl) + row * 8;
+        const size_t kstride = (size_t)rows * 8;
         for (int v = threadIdx.x; v < kdim / 8; v += blockDim.x) {
             const uint4 hv = sh[v], lv = sl[v];
             const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&hv);
@@ -516,8 +520,9 @@ __global__ void __launch_bounds__(128) k_prop_gather(Work w, int P, const int* _
                 l[e] = __halves2bfloat162(__float2bfloat16_rn(a.x - __bfloat162float(hx)),
                                           __float2bfloat16_rn(a.y - __bfloat162float(hy)));
             }
-            dh[v] = *reinterpret_cast<const uint4*>(h);
-            dl[v] = *reinterpret_cast<const uint4*>(l);
+            const size_t o = (size_t)(v >> 3) * kstride + (v & 7);
+            dh[o] = *reinterpret_cast<const uint4*>(h);
+            dl[o] = *reinterpret_cast<const uint4*>(l);
         }
     }
     const uint4* nhv = reinterpret_cast<const uint4*>(nh + oc * kn);
@@ -1425,8 +1430,9 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.pg_h, 0, pg_rows * op.kdim * sizeof(bf16)));
     T2B_CUDA(cudaMemset(N.pg_l, 0, pg_rows * op.kdim * sizeof(bf16)));
     N.nprop = (float*)net_dalloc(W, (size_t)B * 128 * sizeof(float));
-    tc_set_map(c->tc, tc_slot_proposals(), N.pg_h, (int)pg_rows, op.kdim, true);
-    tc_set_map(c->tc, tc_slot_proposals() + 1, N.pg_l, (int)pg_rows, op.kdim, true);
+    N.pg_rows = (int)pg_rows;
+    tc_set_map_blocked(c->tc, tc_slot_proposals(), N.pg_h, (int)pg_rows, op.kdim);
+    tc_set_map_blocked(c->tc, tc_slot_proposals() + 1, N.pg_l, (int)pg_rows, op.kdim);
     // the B operand of the proposal tiles: the phase rows, zero beyond T
     const int ab_rows = (tb.T + 31) / 32 * 32;
     N.ab_h = net_dalloc(W, (size_t)ab_rows * op.kdim * sizeof(bf16));
@@ -1643,7 +1649,7 @@ void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev
     ProposalNet& N = *c->net;
     const Tables& tb = c->tb;
     const TcOperands& op = c->tc;
-    k_prop_gather<<<dim3(N.kprop, w.n), 128, 0, st>>>(w, tb.P, tb.kpix, tb.nk, N.kslot, op.kdim, op.kn,
+    k_prop_gather<<<dim3(N.kprop, w.n), 128, 0, st>>>(w, tb.P, tb.kpix, tb.nk, N.kslot, N.pg_rows, op.kdim, op.kn,
                                                       (const bf16*)op.bh,
                                                       (const bf16*)op.bl, (const bf16*)op.nh, (const bf16*)op.nl,
                                                       (const bf16*)op.wh, (const bf16*)op.wl, (bf16*)N.pg_h,

@@ -71,6 +71,7 @@ struct ProposalNet {
     float* part = nullptr;                   // split-K partial accumulators of the proposal tiles
     int* fix = nullptr;                      // and their arrival counters
     int part_tiles = 0;                      // m-tiles they cover
+    int pg_rows = 0;                         // rows of the proposal A operand (K-blocked)
     float* nprop = nullptr;
     PropState* ps = nullptr;
     int* audit_b = nullptr;

@@ -228,6 +228,7 @@ int tc_slot_proposals();
 int tc_slot_audit();
 int tc_slot_rescore();
 void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows);
+void tc_set_map_blocked(TcOperands& op, int slot, void* ptr, int rows, int kdim);
 void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* norms, const unsigned char* skip,
                        const int* cand, const double* pdf_t, const double* pdf_oc, float* score, int* err,
                        cudaStream_t st);
