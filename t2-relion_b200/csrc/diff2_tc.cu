@@ -100,14 +100,14 @@ __device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, uint
         : "memory");
 }
 
-// the same from a K-blocked operand ([k-block][row][64 elements]): one contiguous box
-__device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* map, uint64_t* bar, int y, int z)
+// One contiguous block global -> shared (untiled bulk copy): the operand is stored
+// pre-swizzled, so the block lands in the layout the UMMA descriptor reads
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
-            su32(dst)),
-        "l"(map), "r"(su32(bar)), "r"(0), "r"(y), "r"(z)
-        : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     su32(dst)),
+                 "l"(src), "r"(bytes), "r"(su32(bar))
+                 : "memory");
 }
 
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
@@ -191,7 +191,13 @@ struct TcParams {
     // (particle, proposal); ncols = particles of the batch.
     // mode 2 tiles hold one particle (ppt = 1): B rows from tile*T (its own images).
     int mode, ppt, kslot;
-    int a3d;                  // the A maps are K-blocked 3D maps (coordinates (0, row, k-block))
+    // mode 1: A and B are stored pre-swizzled and K-blocked (swz_offset): the tile of rows
+    // [y, y + n) of k-block kb is one contiguous block, fetched by one bulk copy
+    const void* a_hi;
+    const void* a_lo;
+    const void* b_hi;
+    const void* b_lo;
+    int a_rows, b_rows;       // rows of each k-block layer
     const int* prop;          // mode 1: global orientation of every (particle, proposal)
     const int* gate;          // run only when (*gate != 0) == gate_run (null: always)
     int gate_run;
@@ -262,7 +268,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         // ---------------- TMA producer
         // only the descriptors this launch reads (the lo slots may not exist)
         const CUtensorMap* ms[4] = {mPh, mIh, mIl, mPl};
-        const int nmaps = 2 + (p.products >= 2 ? 1 : 0) + (p.products == 3 ? 1 : 0);
+        // (proposal tiles read no tensor map: their operands come by bulk copies)
+        const int nmaps = p.mode == 1 ? 0 : 2 + (p.products >= 2 ? 1 : 0) + (p.products == 3 ? 1 : 0);
         for (int j = 0; j < nmaps; j++) {
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(ms[j]) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(ms[j]) : "memory");
@@ -292,15 +299,18 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
                 uint8_t* st = gbase + s * sbytes;
                 mbar_expect_tx(&full_bar[s], tx_bytes);
-                if (p.a3d) {
-                    tma_load3(st, mPh, &full_bar[s], ya, kb);
-                    if (p.products == 3) tma_load3(st + A_BYTES, mPl, &full_bar[s], ya, kb);
+                if (p.mode == 1) {
+                    const size_t ao = ((size_t)kb * p.a_rows + ya) * (TK * 2), bo = ((size_t)kb * p.b_rows + yb) * (TK * 2);
+                    bulk_load(st, static_cast<const uint8_t*>(p.a_hi) + ao, A_BYTES, &full_bar[s]);
+                    bulk_load(st + A_BYTES, static_cast<const uint8_t*>(p.a_lo) + ao, A_BYTES, &full_bar[s]);
+                    bulk_load(st + 2 * A_BYTES, static_cast<const uint8_t*>(p.b_hi) + bo, bbytes, &full_bar[s]);
+                    bulk_load(st + 2 * A_BYTES + bbytes, static_cast<const uint8_t*>(p.b_lo) + bo, bbytes, &full_bar[s]);
                 } else {
                     tma_load(st, mPh, &full_bar[s], kb * TK, ya);
                     if (p.products == 3) tma_load(st + A_BYTES, mPl, &full_bar[s], kb * TK, ya);
+                    tma_load(st + 2 * A_BYTES, mIh, &full_bar[s], kb * TK, yb);
+                    if (p.products >= 2) tma_load(st + 2 * A_BYTES + bbytes, mIl, &full_bar[s], kb * TK, yb);
                 }
-                tma_load(st + 2 * A_BYTES, mIh, &full_bar[s], kb * TK, yb);
-                if (p.products >= 2) tma_load(st + 2 * A_BYTES + bbytes, mIl, &full_bar[s], kb * TK, yb);
                 issued[s] = 1;
                 last_par[s] = ph;
             }
@@ -560,7 +570,7 @@ __global__ void k_split_proj(const float2* __restrict__ proj, int rows, int P, c
 __global__ void __launch_bounds__(128) k_split_img(const float2* __restrict__ cvec, const float2* __restrict__ ab,
                                                    int ncols, int nrows, int T, int P, const int* __restrict__ kpix,
                                                    int nk, int kdim, __nv_bfloat16* __restrict__ hi,
-                                                   __nv_bfloat16* __restrict__ lo, const int* gate)
+                                                   __nv_bfloat16* __restrict__ lo, const int* gate, int swz)
 {
     if (gate && *gate != 0) return;
     const int nv = kdim / 8;  // groups of 4 complex values
@@ -569,8 +579,9 @@ __global__ void __launch_bounds__(128) k_split_img(const float2* __restrict__ cv
         const int b = ok ? col / T : 0, t = ok ? col - b * T : 0;
         const float2* cb = cvec ? cvec + (size_t)b * P : nullptr;
         const float2* at = ab + (size_t)t * P;
-        uint4* dh = reinterpret_cast<uint4*>(hi + (size_t)col * kdim);
-        uint4* dl = reinterpret_cast<uint4*>(lo + (size_t)col * kdim);
+        // row-major rows, or (swz) the pre-swizzled K-blocked layout of swz_offset
+        uint4* dh = reinterpret_cast<uint4*>(hi);
+        uint4* dl = reinterpret_cast<uint4*>(lo);
         for (int g = threadIdx.x; g < nv; g += blockDim.x) {
             __nv_bfloat162 h[4], l[4];
 #pragma unroll
@@ -593,8 +604,9 @@ __global__ void __launch_bounds__(128) k_split_img(const float2* __restrict__ cv
                 h[e] = __halves2bfloat162(h0, h1);
                 l[e] = __halves2bfloat162(l0, l1);
             }
-            dh[g] = *reinterpret_cast<const uint4*>(h);
-            dl[g] = *reinterpret_cast<const uint4*>(l);
+            const size_t o = swz ? swz_offset(col, 8 * g, nrows) / 8 : (size_t)col * (kdim / 8) + g;
+            dh[o] = *reinterpret_cast<const uint4*>(h);
+            dl[o] = *reinterpret_cast<const uint4*>(l);
         }
     }
 }
@@ -660,22 +672,6 @@ CUtensorMap make_map(void* ptr, int rows, int kdim, int box_rows)
     return m;
 }
 
-// K-blocked operand: element (row, k) at ((k / 64) * rows + row) * 64 + k % 64, so a
-// 64-wide box of consecutive rows is one contiguous block of memory
-CUtensorMap make_map_blocked(void* ptr, int rows, int kdim, int box_rows)
-{
-    CUtensorMap m;
-    const cuuint64_t dims[3] = {(cuuint64_t)TK, (cuuint64_t)rows, (cuuint64_t)(kdim / TK)};
-    const cuuint64_t strides[2] = {(cuuint64_t)TK * 2, (cuuint64_t)rows * TK * 2};
-    const cuuint32_t box[3] = {(cuuint32_t)TK, (cuuint32_t)box_rows, 1};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, ptr, dims, strides, box, estr,
-                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) throw Error{T2B_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
-    return m;
-}
-
 int sms()
 {
     int dev = 0, n = 0;
@@ -693,7 +689,7 @@ size_t tc_kn(int nk) { return (size_t)((nk + TK - 1) / TK) * TK; }
 
 // descriptor slots in op.maps (TC_MAP_SLOTS of 128 bytes)
 enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL,
-       MAP_PGH, MAP_PGL, MAP_IAH, MAP_IAL, MAP_ABH, MAP_ABL, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL,
+       MAP_IAH, MAP_IAL, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL,
        MAP_IH128, MAP_IL128, MAP_WAH, MAP_WAL, MAP_COUNT };
 static_assert(MAP_COUNT <= TC_MAP_SLOTS, "tensor-map slots");
 static_assert(sizeof(CUtensorMap) == 128, "tensor-map size");
@@ -784,15 +780,16 @@ void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     T2B_REQUIRE(n_pad <= op.n_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
     k_split_img<<<std::min(n_pad, 16 * sms()), 128, 0, st>>>(w.cvec, tb.ab_c, ncols, n_pad, tb.T, tb.P, tb.kpix, tb.nk,
                                                             op.kdim, (__nv_bfloat16*)op.ah, (__nv_bfloat16*)op.al,
-                                                            gate);
+                                                            gate, 0);
     T2B_CUDA(cudaGetLastError());
 }
 
 void tc_split_phases(const Tables& tb, const TcOperands& op, int rows, void* hi, void* lo, cudaStream_t st)
 {
     T2B_REQUIRE(rows >= tb.T, T2B_ERR_ARG, "phase operand rows");
+    T2B_REQUIRE(rows % 8 == 0, T2B_ERR_ARG, "phase operand rows");
     k_split_img<<<std::min(rows, 16 * sms()), 128, 0, st>>>(nullptr, tb.ab_c, tb.T, rows, tb.T, tb.P, tb.kpix, tb.nk,
-                                                           op.kdim, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, nullptr);
+                                                           op.kdim, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, nullptr, 1);
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -826,28 +823,19 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
 
 void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_side)
 {
-    T2B_REQUIRE(slot >= MAP_PGH && slot < MAP_COUNT && op.maps, T2B_ERR_STATE, "bad tensor-map slot");
+    T2B_REQUIRE(slot >= MAP_IAH && slot < MAP_COUNT && op.maps, T2B_ERR_STATE, "bad tensor-map slot");
     unsigned char blob[128];
     tc_encode(ptr, rows, kdim, a_side, blob);
     T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * slot, blob, 128, cudaMemcpyHostToDevice));
 }
 
-int tc_slot_proposals() { return MAP_PGH; }
 int tc_slot_audit() { return MAP_IAH; }
 int tc_slot_rescore() { return MAP_RAH; }
-int tc_slot_phases() { return MAP_ABH; }
 int tc_slot_audit_w2() { return MAP_WAH; }
-
-void tc_set_map_blocked(TcOperands& op, int slot, void* ptr, int rows, int kdim)
-{
-    T2B_REQUIRE(slot >= MAP_PGH && slot < MAP_COUNT && op.maps && kdim % TK == 0, T2B_ERR_STATE, "bad tensor-map slot");
-    const CUtensorMap m = make_map_blocked(ptr, rows, kdim, TM);
-    T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * slot, &m, 128, cudaMemcpyHostToDevice));
-}
 
 void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows)
 {
-    T2B_REQUIRE(slot >= MAP_PGH && slot < MAP_COUNT && op.maps, T2B_ERR_STATE, "bad tensor-map slot");
+    T2B_REQUIRE(slot >= MAP_IAH && slot < MAP_COUNT && op.maps, T2B_ERR_STATE, "bad tensor-map slot");
     const CUtensorMap m = make_map(ptr, rows, kdim, box_rows);
     T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * slot, &m, 128, cudaMemcpyHostToDevice));
 }
@@ -887,18 +875,25 @@ void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float
 // Restricted coarse pass: every particle against its own proposals only.
 // Cross term C[b, j][t] = Re sum_p P_oc(j)[p] conj(cvec_b[p] ab_t[p])
 //                       = Re sum_p (P_oc(j)[p] conj(cvec_b[p])) conj(ab_t[p]),
-// so the A rows (slots MAP_PGH/PGL, row b*kslot + j) hold the proposal times the
-// conjugate particle image (k_prop_gather) and B is the T phase rows ab_t (slots
-// MAP_ABH/ABL, a tn-row box), shared by every tile and resident in L2.  Tiles of
-// 128 / kslot particles.  Runs while *w.gate != 0.
+// so the A rows (a_hi/a_lo, a_rows rows, row b*kslot + j) hold the proposal times the
+// conjugate particle image (k_prop_gather) and B is the T phase rows ab_t padded to tn
+// rows (b_hi/b_lo), shared by every tile and resident in L2; both are stored
+// pre-swizzled and K-blocked (swz_offset) and fetched by one bulk copy per tile and
+// k-block.  Tiles of 128 / kslot particles.  Runs while *w.gate != 0.
 void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, int tn, const float* nprop,
+                    const void* a_hi, const void* a_lo, int a_rows, const void* b_hi, const void* b_lo,
                     float* part, int* fix, int part_tiles, cudaStream_t st)
 {
     T2B_REQUIRE((kslot == 64 || kslot == TM) && w.kprop <= kslot && tb.T <= tn && tn % 32 == 0 && tn <= TN,
                 T2B_ERR_STATE, "proposal tile shape");
     TcParams p{};
     p.mode = 1;
-    p.a3d = 1;
+    p.a_hi = a_hi;
+    p.a_lo = a_lo;
+    p.b_hi = b_hi;
+    p.b_lo = b_lo;
+    p.a_rows = a_rows;
+    p.b_rows = tn;
     p.ppt = TM / kslot;
     p.kslot = kslot;
     p.m_tiles = (w.n + p.ppt - 1) / p.ppt;
@@ -926,7 +921,8 @@ void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, 
     p.gate = w.gate;
     p.gate_run = 1;
     p.tn = tn;
-    launch_gemm(op, MAP_PGH, MAP_ABH, p, st);
+    T2B_REQUIRE(a_rows % 8 == 0 && (w.n + p.ppt - 1) / p.ppt * TM <= a_rows, T2B_ERR_STATE, "proposal operand rows");
+    launch_gemm(op, MAP_PH, MAP_IH, p, st);   // (the maps are not read: bulk copies)
 }
 
 // Norms of the audited particles N[a][oc] = sum_k w2_a[k] |P_oc|^2_k: the full

@@ -464,17 +464,14 @@ __global__ void __launch_bounds__(1024) k_rescore_select(const int* __restrict__
 // A rows of the proposal contraction: for every (particle b, proposal j) the
 // projection of orientation oc = prop[b][j] times the conjugate particle image,
 // P_oc[p] conj(cvec_b[p]) over the in-radius pixels (P_oc = hi + lo of the
-// configuration's split-BF16 coarse operand), split again into hi + lo; and the
-// norm N = sum_k w2_k |P|^2_k from the same split-BF16 operands the full pass's
-// norm contraction reads (|P|^2 hi + lo per orientation, w2 hi + lo per particle).
-// Row of (b, j): b * kslot + j, stored K-blocked (64-element k-blocks of all `rows`
-// rows one after the other: one contiguous tensor-core tile per k-block).
+// configuration's split-BF16 coarse operand), split again into hi + lo; and, from the
+// same values, the norm N = sum_p w2_p |P_oc[p]|^2.
+// Row of (b, j): b * kslot + j, stored pre-swizzled and K-blocked (swz_offset: a
+// tensor-core tile of 128 rows and one k-block is one contiguous 16 KB block).
 // Runs while *gate != 0.
 __global__ void __launch_bounds__(128) k_prop_gather(Work w, int P, const int* __restrict__ kpix, int nk, int kslot,
-                                                     int rows, int kdim, int kn,
+                                                     int rows, int kdim,
                                                      const bf16* __restrict__ bh, const bf16* __restrict__ bl,
-                                                     const bf16* __restrict__ nh, const bf16* __restrict__ nl,
-                                                     const bf16* __restrict__ wh, const bf16* __restrict__ wl,
                                                      bf16* __restrict__ ph, bf16* __restrict__ pl, float* __restrict__ nprop)
 {
     __shared__ float red[32];
@@ -483,15 +480,15 @@ __global__ void __launch_bounds__(128) k_prop_gather(Work w, int P, const int* _
     if (b >= w.n || j >= w.kprop) return;
     const size_t oc = (size_t)w.prop[(size_t)b * w.kprop + j];
     const size_t row = (size_t)b * kslot + j;
+    float acc = 0.f;
     {
         const uint4* sh = reinterpret_cast<const uint4*>(bh + oc * kdim);
         const uint4* sl = reinterpret_cast<const uint4*>(bl + oc * kdim);
         const int4* kp4 = reinterpret_cast<const int4*>(kpix);
         const float2* cb = w.cvec + (size_t)b * P;
-        // 16-byte group v of the row: k-block v / 8, group v % 8 of its 64 elements
-        uint4* dh = reinterpret_cast<uint4*>(ph) + row * 8;
-        uint4* dl = reinterpret_cast<uint4*>(pl) + row * 8;
-        const size_t kstride = (size_t)rows * 8;
+        const float* w2b = w.w2 + (size_t)b * P;
+        uint4* dh = reinterpret_cast<uint4*>(ph);
+        uint4* dl = reinterpret_cast<uint4*>(pl);
         for (int v = threadIdx.x; v < kdim / 8; v += blockDim.x) {
             const uint4 hv = sh[v], lv = sl[v];
             const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&hv);
@@ -514,33 +511,16 @@ __global__ void __launch_bounds__(128) k_prop_gather(Work w, int P, const int* _
                     const float2 pv = make_float2(hf.x + lf.x, hf.y + lf.y);
                     const float2 c = cb[kk[e]];
                     a = make_float2(pv.x * c.x + pv.y * c.y, pv.y * c.x - pv.x * c.y);
+                    acc += w2b[kk[e]] * (pv.x * pv.x + pv.y * pv.y);
                 }
                 const bf16 hx = __float2bfloat16_rn(a.x), hy = __float2bfloat16_rn(a.y);
                 h[e] = __halves2bfloat162(hx, hy);
                 l[e] = __halves2bfloat162(__float2bfloat16_rn(a.x - __bfloat162float(hx)),
                                           __float2bfloat16_rn(a.y - __bfloat162float(hy)));
             }
-            const size_t o = (size_t)(v >> 3) * kstride + (v & 7);
+            const size_t o = swz_offset(row, 8 * v, rows) / 8;   // 16-byte group v of the row
             dh[o] = *reinterpret_cast<const uint4*>(h);
             dl[o] = *reinterpret_cast<const uint4*>(l);
-        }
-    }
-    const uint4* nhv = reinterpret_cast<const uint4*>(nh + oc * kn);
-    const uint4* nlv = reinterpret_cast<const uint4*>(nl + oc * kn);
-    const uint4* whv = reinterpret_cast<const uint4*>(wh + (size_t)b * kn);
-    const uint4* wlv = reinterpret_cast<const uint4*>(wl + (size_t)b * kn);
-    float acc = 0.f;
-    for (int v = threadIdx.x; v < kn / 8; v += blockDim.x) {
-        const uint4 a0 = nhv[v], a1 = nlv[v], c0 = whv[v], c1 = wlv[v];
-        const __nv_bfloat162* x0 = reinterpret_cast<const __nv_bfloat162*>(&a0);
-        const __nv_bfloat162* x1 = reinterpret_cast<const __nv_bfloat162*>(&a1);
-        const __nv_bfloat162* y0 = reinterpret_cast<const __nv_bfloat162*>(&c0);
-        const __nv_bfloat162* y1 = reinterpret_cast<const __nv_bfloat162*>(&c1);
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const float2 p0 = __bfloat1622float2(x0[e]), p1 = __bfloat1622float2(x1[e]);
-            const float2 q0 = __bfloat1622float2(y0[e]), q1 = __bfloat1622float2(y1[e]);
-            acc += (q0.x + q1.x) * (p0.x + p1.x) + (q0.y + q1.y) * (p0.y + p1.y);
         }
     }
     acc = bsum(acc, red);
@@ -1430,16 +1410,12 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.pg_h, 0, pg_rows * op.kdim * sizeof(bf16)));
     T2B_CUDA(cudaMemset(N.pg_l, 0, pg_rows * op.kdim * sizeof(bf16)));
     N.nprop = (float*)net_dalloc(W, (size_t)B * 128 * sizeof(float));
-    N.pg_rows = (int)pg_rows;
-    tc_set_map_blocked(c->tc, tc_slot_proposals(), N.pg_h, (int)pg_rows, op.kdim);
-    tc_set_map_blocked(c->tc, tc_slot_proposals() + 1, N.pg_l, (int)pg_rows, op.kdim);
+    N.pg_rows = (int)pg_rows;   // pre-swizzled K-blocked (swz_offset), read by bulk copies
     // the B operand of the proposal tiles: the phase rows, zero beyond T
     const int ab_rows = (tb.T + 31) / 32 * 32;
     N.ab_h = net_dalloc(W, (size_t)ab_rows * op.kdim * sizeof(bf16));
     N.ab_l = net_dalloc(W, (size_t)ab_rows * op.kdim * sizeof(bf16));
-    tc_split_phases(tb, op, ab_rows, N.ab_h, N.ab_l, 0);
-    tc_set_map_box(c->tc, tc_slot_phases(), N.ab_h, ab_rows, op.kdim, ab_rows);
-    tc_set_map_box(c->tc, tc_slot_phases() + 1, N.ab_l, ab_rows, op.kdim, ab_rows);
+    tc_split_phases(tb, op, ab_rows, N.ab_h, N.ab_l, 0);   // pre-swizzled K-blocked, read by bulk copies
     // split-K exchange buffers of the proposal tiles: up to half the SMs' worth of m-tiles
     int nsm = 0;
     T2B_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
@@ -1649,15 +1625,13 @@ void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev
     ProposalNet& N = *c->net;
     const Tables& tb = c->tb;
     const TcOperands& op = c->tc;
-    k_prop_gather<<<dim3(N.kprop, w.n), 128, 0, st>>>(w, tb.P, tb.kpix, tb.nk, N.kslot, N.pg_rows, op.kdim, op.kn,
-                                                      (const bf16*)op.bh,
-                                                      (const bf16*)op.bl, (const bf16*)op.nh, (const bf16*)op.nl,
-                                                      (const bf16*)op.wh, (const bf16*)op.wl, (bf16*)N.pg_h,
+    k_prop_gather<<<dim3(N.kprop, w.n), 128, 0, st>>>(w, tb.P, tb.kpix, tb.nk, N.kslot, N.pg_rows, op.kdim,
+                                                      (const bf16*)op.bh, (const bf16*)op.bl, (bf16*)N.pg_h,
                                                       (bf16*)N.pg_l, N.nprop);
-    (void)tb;
     T2B_CUDA(cudaGetLastError());
     if (ev) cudaEventRecord(ev[0], st);
-    tc_launch_prop(tb, w, c->tc, N.kslot, N.tn, N.nprop, N.part, N.fix, N.part_tiles, st);
+    tc_launch_prop(tb, w, c->tc, N.kslot, N.tn, N.nprop, N.pg_h, N.pg_l, N.pg_rows, N.ab_h, N.ab_l, N.part, N.fix,
+                   N.part_tiles, st);
     if (ev) cudaEventRecord(ev[1], st);
 }
 

@@ -224,18 +224,24 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
 bool tc_supported();
 void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128, int box_rows = 0);
 void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_side);
-int tc_slot_proposals();
 int tc_slot_audit();
 int tc_slot_rescore();
 void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows);
-void tc_set_map_blocked(TcOperands& op, int slot, void* ptr, int rows, int kdim);
 void tc_launch_rescore(int n, int k1, int T, int kr, TcOperands& op, const float* norms, const unsigned char* skip,
                        const int* cand, const double* pdf_t, const double* pdf_oc, float* score, int* err,
                        cudaStream_t st);
+// Pre-swizzled K-blocked operand layout (proposal tiles): bf16 element (row, k) of a
+// `rows`-row operand at this element offset; the rows [y, y + n) of k-block k / 64 (y a
+// multiple of 8) are n * 128 contiguous bytes in the 128-byte-swizzled K-major layout of
+// the tensor cores' shared-memory operand.
+__host__ __device__ inline size_t swz_offset(size_t row, int k, size_t rows)
+{
+    return ((size_t)(k >> 6) * rows + row) * 64 + (size_t)((((k & 63) >> 3) ^ (int)(row & 7)) << 3) + (k & 7);
+}
 void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, int tn, const float* nprop,
+                    const void* a_hi, const void* a_lo, int a_rows, const void* b_hi, const void* b_lo,
                     float* part, int* fix, int part_tiles, cudaStream_t st);
 void tc_split_phases(const Tables& tb, const TcOperands& op, int rows, void* hi, void* lo, cudaStream_t st);
-int tc_slot_phases();
 int tc_slot_audit_w2();
 void tc_launch_audit_norms(const Tables& tb, TcOperands& op, int na_max, float* norma, int* err, cudaStream_t st);
 void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
