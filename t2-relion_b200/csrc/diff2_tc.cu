@@ -32,7 +32,7 @@ namespace {
 
 constexpr int TM = 128, TN = 256, TK = 64;
 constexpr int STAGES = 2;       // pipeline stages of 128 x 256 tiles (96 KB each)
-constexpr int MAXSTAGES = 3;    // 128 x 96 tiles: 56 KB stages, three fit in the same space
+constexpr int MAXSTAGES = 8;    // narrower tiles and fewer products: more, smaller stages in the same space
 constexpr uint32_t A_BYTES = TM * TK * 2;              // 16 KB
 constexpr uint32_t B_BYTES = TN * TK * 2;              // 32 KB
 constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
@@ -237,8 +237,11 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
     // stage geometry of this launch: B box of tn rows; narrow tiles get a third stage
     const int tn_l = p.tn ? p.tn : TN;
     const uint32_t bbytes = (uint32_t)tn_l * TK * 2;                 // multiple of 1024
-    const uint32_t sbytes = 2 * A_BYTES + 2 * bbytes;
-    const int nst = (2 * A_BYTES + 2 * bbytes) * MAXSTAGES <= STAGES * STAGE_BYTES ? MAXSTAGES : STAGES;
+    // stage layout [A hi | A lo (3 products) | B hi | B lo (2+ products)]; as many stages as
+    // fit in the stage area, so narrow or single-product tiles keep more copies in flight
+    const uint32_t a_st = A_BYTES * (p.products == 3 ? 2u : 1u);
+    const uint32_t sbytes = a_st + bbytes * (p.products >= 2 ? 2u : 1u);
+    const int nst = min(MAXSTAGES, (int)((uint32_t)(STAGES * STAGE_BYTES) / sbytes));
     const uint32_t base = (su32(smem_raw) + 1023u) & ~1023u;
     uint8_t* gbase = smem_raw + (base - su32(smem_raw));
     float* epi = reinterpret_cast<float*>(gbase + STAGES * STAGE_BYTES);          // 4 x 32 x 33
@@ -275,8 +278,8 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             asm volatile("prefetch.tensormap [%0];" ::"l"(ms[j]) : "memory");
         }
         int it = 0;
-        int issued[MAXSTAGES] = {0, 0, 0};
-        uint32_t last_par[MAXSTAGES] = {0, 0, 0};
+        int issued[MAXSTAGES] = {};
+        uint32_t last_par[MAXSTAGES] = {};
         const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + bbytes * (p.products >= 2 ? 2u : 1u);
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
             int ya, yb;
@@ -303,13 +306,13 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                     const size_t ao = ((size_t)kb * p.a_rows + ya) * (TK * 2), bo = ((size_t)kb * p.b_rows + yb) * (TK * 2);
                     bulk_load(st, static_cast<const uint8_t*>(p.a_hi) + ao, A_BYTES, &full_bar[s]);
                     bulk_load(st + A_BYTES, static_cast<const uint8_t*>(p.a_lo) + ao, A_BYTES, &full_bar[s]);
-                    bulk_load(st + 2 * A_BYTES, static_cast<const uint8_t*>(p.b_hi) + bo, bbytes, &full_bar[s]);
-                    bulk_load(st + 2 * A_BYTES + bbytes, static_cast<const uint8_t*>(p.b_lo) + bo, bbytes, &full_bar[s]);
+                    bulk_load(st + a_st, static_cast<const uint8_t*>(p.b_hi) + bo, bbytes, &full_bar[s]);
+                    bulk_load(st + a_st + bbytes, static_cast<const uint8_t*>(p.b_lo) + bo, bbytes, &full_bar[s]);
                 } else {
                     tma_load(st, mPh, &full_bar[s], kb * TK, ya);
                     if (p.products == 3) tma_load(st + A_BYTES, mPl, &full_bar[s], kb * TK, ya);
-                    tma_load(st + 2 * A_BYTES, mIh, &full_bar[s], kb * TK, yb);
-                    if (p.products >= 2) tma_load(st + 2 * A_BYTES + bbytes, mIl, &full_bar[s], kb * TK, yb);
+                    tma_load(st + a_st, mIh, &full_bar[s], kb * TK, yb);
+                    if (p.products >= 2) tma_load(st + a_st + bbytes, mIl, &full_bar[s], kb * TK, yb);
                 }
                 issued[s] = 1;
                 last_par[s] = ph;
@@ -340,7 +343,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 tc_fence_after();
                 const uint32_t sa = base + s * sbytes;
                 const uint64_t dPh = sdesc(sa), dPl = sdesc(sa + A_BYTES);
-                const uint64_t dIh = sdesc(sa + 2 * A_BYTES), dIl = sdesc(sa + 2 * A_BYTES + bbytes);
+                const uint64_t dIh = sdesc(sa + a_st), dIl = sdesc(sa + a_st + bbytes);
 #pragma unroll
                 for (int k = 0; k < TK / 16; k++) {
                     const uint64_t ko = (uint64_t)(k * 32) >> 4;  // 32 bytes per K=16 step
