@@ -773,7 +773,12 @@ def main():
         t_audit, t_prop = float(stages[7]), float(stages[8])
         f_audit = 8.0 * K * O * T * P * na
         f_prop = 8.0 * PROP["topk"] * T * P * B
-        ntile_audit = ((K * O + 127) // 128) * ((int(np.ceil(B / PROP["audit_every"])) * T + 255) // 256)
+        # audit launch: 128-row tiles over every orientation; na_max slots of T columns in
+        # 256-column tiles, or one narrower tile of (na_max - 1) slots when fewer were audited
+        na_max = int(np.ceil(B / PROP["audit_every"]))
+        tn_n = ((na_max - 1) * T + 31) // 32 * 32 if na_max > 1 else 0
+        narrow = 0 < na < na_max and 0 < tn_n <= 256 and tn_n < (na_max * T + 255) // 256 * 256
+        ntile_audit = ((K * O + 127) // 128) * (tn_n / 256.0 if narrow else (na_max * T + 255) // 256)
         tile_flops = 128 * 256 * kdim * 2 * 3.0
         # proposal tiles: 128 rows of 128 / kslot particles x T phase rows padded to 32 columns
         ppt = 2 if PROP["topk"] <= 64 else 1

@@ -201,6 +201,8 @@ struct TcParams {
     const int* prop;          // mode 1: global orientation of every (particle, proposal)
     const int* gate;          // run only when (*gate != 0) == gate_run (null: always)
     int gate_run;
+    const int* cnt;           // run only when cnt_lo <= *cnt <= cnt_hi (null: always)
+    int cnt_lo, cnt_hi;
     int tn;                   // N of the tile (multiple of 32, <= 256; 0 = 256); B maps with a tn-row box
     int mtp;                  // mode 2: consecutive tiles per particle (0 = 1); A rows of tile i are
                               // rows [i*128, i*128+128), candidate j = (i % mtp)*128 + row
@@ -224,6 +226,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
 {
     if (p.gate && ((*p.gate != 0) != (p.gate_run != 0))) return;  // uniform: the whole CTA leaves
+    if (p.cnt && (*p.cnt < p.cnt_lo || *p.cnt > p.cnt_hi)) return;
     const CUtensorMap* mPh = maps + ia;
     const CUtensorMap* mPl = maps + ia + 1;
     const CUtensorMap* mIh = maps + ib;
@@ -693,7 +696,7 @@ size_t tc_kn(int nk) { return (size_t)((nk + TK - 1) / TK) * TK; }
 // descriptor slots in op.maps (TC_MAP_SLOTS of 128 bytes)
 enum { MAP_PH = 0, MAP_PL, MAP_IH, MAP_IL, MAP_NH, MAP_NL, MAP_WH, MAP_WL,
        MAP_IAH, MAP_IAL, MAP_RAH, MAP_RAL, MAP_RBH, MAP_RBL,
-       MAP_IH128, MAP_IL128, MAP_WAH, MAP_WAL, MAP_COUNT };
+       MAP_IH128, MAP_IL128, MAP_WAH, MAP_WAL, MAP_IAH_N, MAP_IAL_N, MAP_COUNT };
 static_assert(MAP_COUNT <= TC_MAP_SLOTS, "tensor-map slots");
 static_assert(sizeof(CUtensorMap) == 128, "tensor-map size");
 
@@ -835,6 +838,7 @@ void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_
 int tc_slot_audit() { return MAP_IAH; }
 int tc_slot_rescore() { return MAP_RAH; }
 int tc_slot_audit_w2() { return MAP_WAH; }
+int tc_slot_audit_narrow() { return MAP_IAH_N; }
 
 void tc_set_map_box(TcOperands& op, int slot, void* ptr, int rows, int kdim, int box_rows)
 {
@@ -953,8 +957,19 @@ void tc_launch_audit_norms(const Tables& tb, TcOperands& op, int na_max, float* 
 
 // Full coarse pass of the audited particles: dense tiles over every
 // orientation against the audit image operand (MAP_IAH/IAL, na_max*T rows).
-void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
-                     unsigned* minkeya, int* err, cudaStream_t st)
+// The audited count na of a batch is known on the device only: with na_max slots, a
+// batch of fewer audited particles runs the narrower variant (tn_narrow columns for
+// na_max - 1 slots, MAP_IAH_N/IAL_N), a batch of na_max the full one; each launch returns
+// at once unless the count is its own.
+int tc_audit_narrow_tn(int na_max, int T)
+{
+    if (na_max < 2) return 0;
+    const int tn = ((na_max - 1) * T + 31) / 32 * 32;
+    return (tn <= TN && tn < (na_max * T + TN - 1) / TN * TN) ? tn : 0;
+}
+
+void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const int* na, const float* c0a,
+                     const float* norma, float* d2a, unsigned* minkeya, int* err, cudaStream_t st)
 {
     TcParams p{};
     p.m_tiles = op.m_pad / TM;
@@ -971,6 +986,20 @@ void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* 
     p.err = err;
     p.products = 3;
     p.group = op.group_m;
+    const int tn_n = tc_audit_narrow_tn(na_max, tb.T);
+    if (tn_n > 0 && na) {
+        TcParams q = p;
+        q.n_tiles = 1;
+        q.ncols = (na_max - 1) * tb.T;
+        q.tn = tn_n;
+        q.cnt = na;
+        q.cnt_lo = 1;
+        q.cnt_hi = na_max - 1;
+        launch_gemm(op, MAP_PH, MAP_IAH_N, q, st);
+        p.cnt = na;
+        p.cnt_lo = na_max;
+        p.cnt_hi = na_max;
+    }
     launch_gemm(op, MAP_PH, MAP_IAH, p, st);
 }
 

@@ -1434,6 +1434,10 @@ void net_setup(t2b_ctx* c, int na_max)
     T2B_CUDA(cudaMemset(N.ia_l, 0, (size_t)ia_rows * op.kdim * sizeof(bf16)));
     tc_set_map(c->tc, tc_slot_audit(), N.ia_h, ia_rows, op.kdim, false);
     tc_set_map(c->tc, tc_slot_audit() + 1, N.ia_l, ia_rows, op.kdim, false);
+    if (const int tn_n = tc_audit_narrow_tn(N.na_max, tb.T)) {
+        tc_set_map_box(c->tc, tc_slot_audit_narrow(), N.ia_h, ia_rows, op.kdim, tn_n);
+        tc_set_map_box(c->tc, tc_slot_audit_narrow() + 1, N.ia_l, ia_rows, op.kdim, tn_n);
+    }
     const int wa_rows = (N.na_max + 31) / 32 * 32;
     N.wa_h = net_dalloc(W, (size_t)wa_rows * op.kn * sizeof(bf16));
     N.wa_l = net_dalloc(W, (size_t)wa_rows * op.kn * sizeof(bf16));
@@ -1612,7 +1616,7 @@ void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev)
     tc_launch_audit_norms(tb, op, N.na_max, N.norma, w.err, st);
     T2B_CUDA(cudaGetLastError());
     if (ev) cudaEventRecord(ev[0], st);
-    tc_launch_audit(tb, op, N.na_max, N.c0a, N.norma, N.d2a, N.minkeya, w.err, st);
+    tc_launch_audit(tb, op, N.na_max, &N.ps->na, N.c0a, N.norma, N.d2a, N.minkeya, w.err, st);
     if (ev) cudaEventRecord(ev[1], st);
     k_audit_mass<<<dim3(2 * 148, N.na_max), 256, ((KO + 31) / 32) * sizeof(unsigned), st>>>(tb, w, N.ps, N.audit_b, N.d2a,
                                                                                      N.minkeya, N.asum);

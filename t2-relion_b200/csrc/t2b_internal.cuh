@@ -244,8 +244,10 @@ void tc_launch_prop(const Tables& tb, const Work& w, TcOperands& op, int kslot, 
 void tc_split_phases(const Tables& tb, const TcOperands& op, int rows, void* hi, void* lo, cudaStream_t st);
 int tc_slot_audit_w2();
 void tc_launch_audit_norms(const Tables& tb, TcOperands& op, int na_max, float* norma, int* err, cudaStream_t st);
-void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const float* c0a, const float* norma, float* d2a,
-                     unsigned* minkeya, int* err, cudaStream_t st);
+int tc_audit_narrow_tn(int na_max, int T);
+int tc_slot_audit_narrow();
+void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const int* na, const float* c0a,
+                     const float* norma, float* d2a, unsigned* minkeya, int* err, cudaStream_t st);
 int tc_gemm_raw(const void* maps, int ia, int ib, int M, int N, int K, float* out, int products, int* err,
                 cudaStream_t st, int ksplit = 1, int tn = 256);
 
