@@ -536,7 +536,9 @@ def run_recon(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    # 25 steps of 128 particles are one period of the audit pattern (every 50th particle:
+    # 64 audited in 3,200), so the timed steps hold the average mix of 2- and 3-particle audits
+    ap.add_argument("--steps", type=int, default=25)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="learned", choices=["learned", "splitbf16", "plain"],

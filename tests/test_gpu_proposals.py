@@ -202,3 +202,30 @@ def test_proposal_diff2_matches_full_pass(trained):
         worst = max(worst, np.max(np.abs(d2[live] - full[live])) / scale)
     print("proposal diff2 vs full pass, max relative deviation:", worst)
     assert worst <= 1e-5
+
+
+def test_audit_with_fewer_than_max_slots_graph_and_eager(trained):
+    """Batches whose audited count is below the slot maximum run the narrower audit
+    variant (each of the two launches gated on the device-side count): a stream of three
+    32-particle batches audited every 20th particle (2, 2 and 1 audited) gives the same
+    audit masses and poses replayed as graphs and launched one by one."""
+    es, P = trained["es"], trained["parts"]
+    n = 32
+    runs = []
+    for eager in (False, True):
+        es.stage_timing(eager)
+        es.enable_proposals(topk=64, rescore=512, audit_every=20, audit_mass=0.999)
+        out = []
+        for first in (0, 16, 0):
+            sl = slice(first, first + n)
+            out.append(es.expectation(P["fimg"][sl], P["ctf"][sl], P["minv"][sl], P["scalars"][sl]))
+        runs.append(out)
+    es.stage_timing(False)
+    es.disable_proposals()
+    counts = [int((r["audit_mass"] >= 0).sum()) for r in runs[0]]
+    assert counts == [2, 2, 1], counts
+    for a, b in zip(*runs):
+        assert np.array_equal(a["learned"], b["learned"])
+        assert np.array_equal(a["pose"], b["pose"])
+        assert np.allclose(a["audit_mass"], b["audit_mass"], rtol=1e-9)
+        assert np.all(a["audit_mass"][a["audit_mass"] >= 0] > 0.5)
