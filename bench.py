@@ -724,13 +724,16 @@ def main():
     e2e_s = timed(pipelined_loop)
     # per-stage device times (CUDA events around each stage) of separately synchronised
     # host-path steps; not part of `value`
-    stages = []
+    # (one period of the audit pattern when learned: each step's audited count is kept)
+    stage_steps, audited = [], []
     es.stage_timing(True)
-    for _ in range(min(3, args.steps)):
+    for _ in range(min(25, args.steps)):
         e2e_step()
-        stages.append(es.stage_ms())
+        stage_steps.append(es.stage_ms())
+        audited.append(int((hres["audit_mass"].numpy() >= 0).sum()))
     es.stage_timing(False)
-    stages = np.mean(np.array(stages), axis=0)
+    stage_steps = np.array(stage_steps)
+    stages = np.mean(stage_steps, axis=0)
     h2d = sum(v.numel() * v.element_size() for v in pin.values())
     d2h = sum(v.numel() * v.element_size() for v in hres.values())
     e2e = {"value": B * n_e2e * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
@@ -771,27 +774,33 @@ def main():
         # learned: the audit's full coarse contraction (audited particles x every orientation)
         # and the contraction on the proposals (every particle x its top-k), each one launch of
         # k_diff2_tc per step, timed by the library's CUDA events around exactly those launches
-        na = float((hres["audit_mass"].numpy() >= 0).sum())          # audited particles of the last step
+        # over the stage-timed steps, each with its own audited count
         t_audit, t_prop = float(stages[7]), float(stages[8])
-        f_audit = 8.0 * K * O * T * P * na
+        t_sum = float(np.sum(stage_steps[:, 7] + stage_steps[:, 8])) / 1000.0
         f_prop = 8.0 * PROP["topk"] * T * P * B
+        f_sum = sum(8.0 * K * O * T * P * na + f_prop for na in audited)
         # audit launch: 128-row tiles over every orientation; na_max slots of T columns in
         # 256-column tiles, or one narrower tile of (na_max - 1) slots when fewer were audited
         na_max = int(np.ceil(B / PROP["audit_every"]))
         tn_n = ((na_max - 1) * T + 31) // 32 * 32 if na_max > 1 else 0
-        narrow = 0 < na < na_max and 0 < tn_n <= 256 and tn_n < (na_max * T + 255) // 256 * 256
-        ntile_audit = ((K * O + 127) // 128) * (tn_n / 256.0 if narrow else (na_max * T + 255) // 256)
         tile_flops = 128 * 256 * kdim * 2 * 3.0
+
+        def audit_tiles(na):
+            if na == 0:
+                return 0.0
+            narrow = na < na_max and 0 < tn_n <= 256 and tn_n < (na_max * T + 255) // 256 * 256
+            return ((K * O + 127) // 128) * (tn_n / 256.0 if narrow else (na_max * T + 255) // 256)
         # proposal tiles: 128 rows of 128 / kslot particles x T phase rows padded to 32 columns
         ppt = 2 if PROP["topk"] <= 64 else 1
         prop_exec = ((B + ppt - 1) // ppt) * 128 * ((T + 31) // 32 * 32) * kdim * 2 * 3.0
-        executed = (ntile_audit * tile_flops + prop_exec) / ((t_audit + t_prop) / 1000.0) / 1e12
+        executed = sum(audit_tiles(na) * tile_flops + prop_exec for na in audited) / t_sum / 1e12
         peak = peaks.get("bf16_tflops_sustained", 1400.0)
-        achieved = (f_audit + f_prop) / ((t_audit + t_prop) / 1000.0) / 1e12
+        achieved = f_sum / t_sum / 1e12
+        na = float(np.mean(audited))
         roof = {"bound": "tensor", "kernel": "k_diff2_tc (audit + proposal launches)", "achieved": achieved,
                 "executed_tflops": executed, "contraction_pixels": nk, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "peak_source": src, "traffic": LEARNED_TRAFFIC,
-                "flops_per_launch": (f_audit + f_prop) / 2.0, "audit_ms": t_audit, "proposal_ms": t_prop,
+                "flops_per_launch": f_sum / (2.0 * len(audited)), "audit_ms": t_audit, "proposal_ms": t_prop,
                 "audited_particles": na}
     line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
