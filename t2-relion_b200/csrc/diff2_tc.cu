@@ -468,7 +468,25 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                                                            : m - my_norm + __logf(sacc) + (float)log(p.pdf_oc[p.prop[pj]]);
                 }
             }
-            for (int c = 0; c < (p.mode == 2 || !emit ? 0 : nchunk); c++) {
+            // raw products with one column per batch entry (norms, network layers: out[col][row]):
+            // the TMEM lane is the row, which is the contiguous axis of the output, so each of
+            // the 32 columns of a load is one coalesced 128-byte store, no transpose
+            const bool raw_rows = p.mode == 0 && p.raw && p.T == 1;
+            if (raw_rows) {
+                const int oc = mt * TM + q * 32 + lane;
+                for (int c = 0; c < nchunk; c++) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
+                    if (oc < p.KO) {
+#pragma unroll
+                        for (int e = 0; e < 32; e++) {
+                            const int col = n0 + c * 32 + e;
+                            if (col < p.ncols) outp[(size_t)col * p.KO + oc] = __uint_as_float(v[e]);
+                        }
+                    }
+                }
+            }
+            for (int c = 0; c < (p.mode == 2 || !emit || raw_rows ? 0 : nchunk); c++) {
                 uint32_t v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * TN + c * 32), v);
                 if (other) {
