@@ -623,15 +623,30 @@ __global__ void __launch_bounds__(256) k_audit_mass(Tables tb, Work w, const Pro
     // are below 1e-18 of the sum
     const double cut = fmin(700., 60. + (w.lbound[2 * b + 1] - w.lbound[2 * b]));
     double sa = 0., sp = 0.;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const float v = d[i];
-        if (v < 0.f) continue;
-        const double dd = (double)v - mn;
-        if (dd > cut) continue;
-        const int oc = (int)(i / T), t = (int)(i - (long long)oc * T);
-        const double wt = tb.pdf_oc[oc] * w.pdf_t[(size_t)b * T + t] * exp(-dd);
-        sa += wt;
-        if (inprop[oc >> 5] & (1u << (oc & 31))) sp += wt;
+    // 8 consecutive values per thread and pass (two 16-byte loads in flight; a slot's
+    // n = K*O*T values start 16-byte aligned when n is a multiple of 4, else scalar loads)
+    const bool vec = (n & 3) == 0;
+    const long long step = (long long)gridDim.x * blockDim.x * 8;
+    for (long long i0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 8; i0 < n; i0 += step) {
+        float v[8];
+        if (vec && i0 + 8 <= n) {
+            const float4 a = *reinterpret_cast<const float4*>(d + i0), c = *reinterpret_cast<const float4*>(d + i0 + 4);
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = c.x; v[5] = c.y; v[6] = c.z; v[7] = c.w;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; e++) v[e] = i0 + e < n ? d[i0 + e] : -1.f;
+        }
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            if (v[e] < 0.f) continue;
+            const double dd = (double)v[e] - mn;
+            if (dd > cut) continue;
+            const long long i = i0 + e;
+            const int oc = (int)(i / T), t = (int)(i - (long long)oc * T);
+            const double wt = tb.pdf_oc[oc] * w.pdf_t[(size_t)b * T + t] * exp(-dd);
+            sa += wt;
+            if (inprop[oc >> 5] & (1u << (oc & 31))) sp += wt;
+        }
     }
     sa = bsum(sa, red);
     sp = bsum(sp, red);
