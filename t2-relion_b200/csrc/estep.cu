@@ -449,7 +449,7 @@ __global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
     double* hs = reinterpret_cast<double*>(smem_raw + HIST_BINS * sizeof(unsigned));
     __shared__ double sh[32];
     const int b = blockIdx.y;
-    if (fine && w.status[b] != T2B_OK) return;
+    if (fine && (w.status[b] != T2B_OK || w.sel_f[b].fast == 2)) return;   // (fast 2: k_select_small)
     for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
     __syncthreads();
     const Seg sg = seg_of(tb, w, fine, b);
@@ -516,6 +516,7 @@ __global__ void k_sel_init(Work w, int fine, double frac)
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= w.n) return;
     SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    if (sel->fast == 2) return;   // selected by k_select_small
     const double S = fine ? w.sum_f[b] : w.sum_c[b];
     if (w.status[b] != T2B_OK) { sel->phase = 3; return; }
     if (!(S > 0.) || S != S) {
@@ -903,6 +904,108 @@ __global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass
     }
     if (threadIdx.x == 0) {
         sel->fast = 1;
+        sel->phase = 2;
+    }
+}
+
+// Fine-pass selection of a particle whose fine hypotheses fit in shared memory
+// (<= SMALL_CAP), in one CTA: FP64 weights (stored in wf, as k_weights), their sum and
+// maximum, a sort by weight (descending, then index), and the threshold where the
+// cumulative sum of the sorted weights first exceeds adaptive_fraction * sum
+// (src/ml_optimiser.cpp:7905-7935), found by a block-wide prefix sum in a fixed
+// order.  It leaves the particle marked (fast = 2) so the multi-kernel selection skips it.
+constexpr int SMALL_CAP = 8192;
+__global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, double frac)
+{
+    extern __shared__ unsigned char smem_raw[];
+    double* sw = reinterpret_cast<double*>(smem_raw);
+    long long* si = reinterpret_cast<long long*>(smem_raw + SMALL_CAP * sizeof(double));
+    __shared__ double shd[32];
+    __shared__ unsigned long long shu[32];
+    __shared__ long long kmin;
+    const int b = blockIdx.x;
+    SelState* sel = &w.sel_f[b];
+    const long long rv = (long long)tb.R * tb.V;
+    const long long beg = w.pair_off[b] * rv, n = w.pair_off[b + 1] * rv - beg;
+    if (n > SMALL_CAP) return;                      // the multi-kernel selection takes it
+    if (w.status[b] != T2B_OK) {
+        if (threadIdx.x == 0) { sel->fast = 2; sel->phase = 3; }
+        return;
+    }
+    const double mn = (double)key2f(w.minkey_f[b]);
+    int n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    double lsum = 0.;
+    unsigned long long lmax = 0;
+    for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+        double wt = -1.;                             // padding: sorts last
+        if (i < n) {
+            const float d = w.d2f[beg + i];
+            wt = 0.;
+            if (d >= 0.f) {
+                const double dd = (double)d - mn;
+                if (dd <= 700.) wt = fine_prior(tb, w, b, beg + i) * exp(-dd);
+            }
+            w.wf[beg + i] = wt;
+            lsum += wt;
+            lmax = max(lmax, (unsigned long long)__double_as_longlong(wt));
+        }
+        sw[i] = wt;
+        si[i] = beg + i;
+    }
+    const double S = block_sum(lsum, shd);
+    for (int o = 16; o > 0; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if ((threadIdx.x & 31) == 0) shu[threadIdx.x >> 5] = lmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) m = max(m, shu[i]);
+        w.sum_f[b] = S;
+        sel->maxbits = m;
+        sel->fast = 2;
+        sel->nr_sign = 0;
+        if (!(S > 0.) || S != S) {
+            sel->phase = 3;
+            w.status[b] = T2B_ERR_NOSIGNIF;
+        }
+        kmin = 0x7fffffffffffffffLL;
+    }
+    if (!(S > 0.) || S != S) return;
+    const double target = frac * S;
+    bitonic_pairs(sw, si, n2, true);
+    // inclusive prefix sums of the sorted weights: runs of `per` per thread, then the runs'
+    // exclusive offsets by a block scan
+    const int per = (n2 + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int i0 = threadIdx.x * per, i1 = min((long long)(i0 + per), n);
+    double run = 0.;
+    for (int i = i0; i < i1; i++) run += sw[i];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double incl = run;
+    for (int o = 1; o < 32; o <<= 1) {
+        const double x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    if (lane == 31) shd[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        double t = lane < (int)(blockDim.x >> 5) ? shd[lane] : 0.;
+        for (int o = 1; o < 32; o <<= 1) {
+            const double x = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += x;
+        }
+        shd[lane] = t;   // inclusive over warps
+    }
+    __syncthreads();
+    double cum = (wid > 0 ? shd[wid - 1] : 0.) + incl - run;
+    for (int i = i0; i < i1; i++) {
+        cum += sw[i];
+        if (cum > target) { atomicMin(&kmin, (long long)i); break; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const long long k = kmin < n ? kmin : n - 1;
+        sel->thr = sw[k];
+        sel->argmax = si[0];
         sel->phase = 2;
     }
 }
@@ -1550,6 +1653,7 @@ int grid_x_for(int nb)
 
 const size_t HIST_SMEM = HIST_BINS * (sizeof(unsigned) + sizeof(double));
 const size_t FAST_SMEM = FAST_CAP * (sizeof(double) + sizeof(long long));
+const size_t SMALL_SMEM = SMALL_CAP * (sizeof(double) + sizeof(long long));
 
 // a stream per device to capture conditional-node bodies on
 cudaStream_t body_stream()
@@ -1649,6 +1753,7 @@ void estep_init_attributes()
     T2B_CUDA(cudaFuncSetAttribute(k_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HIST_SMEM));
     T2B_CUDA(cudaFuncSetAttribute(k_hist_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HIST_SMEM));
     T2B_CUDA(cudaFuncSetAttribute(k_final_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FAST_SMEM));
+    T2B_CUDA(cudaFuncSetAttribute(k_select_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_SMEM));
     (void)sm_count();
 }
 
@@ -1680,6 +1785,7 @@ void launch_weights_fine(const Tables& tb, const Work& w, cudaStream_t st)
 {
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
+    k_select_small<<<w.n, 1024, SMALL_SMEM, st>>>(tb, w, tb.adaptive_fraction);
     k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 1);
     run_selection(tb, w, 1, 1, st);
     k_argmax_fine<<<grid, 256, 0, st>>>(tb, w);
