@@ -449,7 +449,8 @@ __global__ void __launch_bounds__(256) k_weights(Tables tb, Work w, int fine)
     double* hs = reinterpret_cast<double*>(smem_raw + HIST_BINS * sizeof(unsigned));
     __shared__ double sh[32];
     const int b = blockIdx.y;
-    if (fine && (w.status[b] != T2B_OK || w.sel_f[b].fast == 2)) return;   // (fast 2: k_select_small)
+    if ((fine ? w.sel_f[b] : w.sel_c[b]).fast == 2) return;   // selected by k_select_small
+    if (fine && w.status[b] != T2B_OK) return;
     for (int i = threadIdx.x; i < HIST_BINS; i += blockDim.x) { hc[i] = 0; hs[i] = 0.; }
     __syncthreads();
     const Seg sg = seg_of(tb, w, fine, b);
@@ -908,14 +909,20 @@ __global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass
     }
 }
 
-// Fine-pass selection of a particle whose fine hypotheses fit in shared memory
-// (<= SMALL_CAP), in one CTA: FP64 weights (stored in wf, as k_weights), their sum and
-// maximum, a sort by weight (descending, then index), and the threshold where the
-// cumulative sum of the sorted weights first exceeds adaptive_fraction * sum
-// (src/ml_optimiser.cpp:7905-7935), found by a block-wide prefix sum in a fixed
-// order.  It leaves the particle marked (fast = 2) so the multi-kernel selection skips it.
+// Selection of a particle whose hypotheses fit in shared memory (<= SMALL_CAP: the
+// fine pass, and the coarse pass on the proposals), in one CTA: FP64 weights (the fine
+// ones stored in wf, as k_weights), their sum and maximum, and the threshold where the
+// cumulative sum of the weights sorted by weight (descending, then index) first exceeds
+// adaptive_fraction * sum (src/ml_optimiser.cpp:7905-7935; the coarse pass also stops
+// at the maxsig-th weight, :7945-7966).  Only the weights >= (1 - f) S / n can be
+// reached before the crossing (all the others together hold less than (1 - f) S), so
+// only they are sorted; the prefix sum over them is a block scan in a fixed order.  The
+// coarse pass also emits the significant list in index order (as k_final_fast).  The
+// particle is left marked (fast = 2) so the multi-kernel selection skips it; a coarse
+// list longer than FAST_CAP is left to that path.
 constexpr int SMALL_CAP = 8192;
-__global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, double frac)
+constexpr int SMALL_PER = SMALL_CAP / 1024;   // hypotheses per thread
+__global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, int fine, int maxsig, double frac)
 {
     extern __shared__ unsigned char smem_raw[];
     double* sw = reinterpret_cast<double*>(smem_raw);
@@ -923,60 +930,88 @@ __global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, double
     __shared__ double shd[32];
     __shared__ unsigned long long shu[32];
     __shared__ long long kmin;
+    __shared__ int ncand;
     const int b = blockIdx.x;
-    SelState* sel = &w.sel_f[b];
-    const long long rv = (long long)tb.R * tb.V;
-    const long long beg = w.pair_off[b] * rv, n = w.pair_off[b + 1] * rv - beg;
+    SelState* sel = fine ? &w.sel_f[b] : &w.sel_c[b];
+    const bool pm = !fine && prop_mode(w);
+    const Seg sg = seg_of(tb, w, fine, b);
+    const long long n = sg.end - sg.beg;
     if (n > SMALL_CAP) return;                      // the multi-kernel selection takes it
     if (w.status[b] != T2B_OK) {
-        if (threadIdx.x == 0) { sel->fast = 2; sel->phase = 3; }
+        if (threadIdx.x == 0) {
+            sel->fast = 2;
+            sel->phase = 3;
+            if (!fine) w.r_ncsig[b] = 0;
+        }
         return;
     }
-    const double mn = (double)key2f(w.minkey_f[b]);
-    int n2 = 1;
-    while (n2 < n) n2 <<= 1;
+    const float* dsrc = fine ? w.d2f + sg.beg : w.d2c + (size_t)b * (size_t)n;
+    const double mn = (double)key2f(fine ? w.minkey_f[b] : w.minkey_c[b]);
+    // this thread's hypotheses i = threadIdx.x + j * blockDim.x, weights in registers
+    double wr[SMALL_PER];
     double lsum = 0.;
     unsigned long long lmax = 0;
-    for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-        double wt = -1.;                             // padding: sorts last
+#pragma unroll
+    for (int j = 0; j < SMALL_PER; j++) {
+        const long long i = threadIdx.x + (long long)j * blockDim.x;
+        double wt = 0.;
         if (i < n) {
-            const float d = w.d2f[beg + i];
-            wt = 0.;
-            if (d >= 0.f) {
-                const double dd = (double)d - mn;
-                if (dd <= 700.) wt = fine_prior(tb, w, b, beg + i) * exp(-dd);
+            const float d = dsrc[i];
+            if (fine) {
+                if (d >= 0.f) {
+                    const double dd = (double)d - mn;
+                    if (dd <= 700.) wt = fine_prior(tb, w, b, sg.beg + i) * exp(-dd);
+                }
+                w.wf[sg.beg + i] = wt;
+            } else {
+                wt = coarse_weight_ot(tb, w, b, glob_oc(w, b, i / tb.T, pm), (int)(i % tb.T), d, mn);
             }
-            w.wf[beg + i] = wt;
             lsum += wt;
             lmax = max(lmax, (unsigned long long)__double_as_longlong(wt));
         }
-        sw[i] = wt;
-        si[i] = beg + i;
+        wr[j] = wt;
     }
     const double S = block_sum(lsum, shd);
     for (int o = 16; o > 0; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
     if ((threadIdx.x & 31) == 0) shu[threadIdx.x >> 5] = lmax;
+    if (threadIdx.x == 0) { kmin = 0x7fffffffffffffffLL; ncand = 0; }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long m = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); i++) m = max(m, shu[i]);
-        w.sum_f[b] = S;
-        sel->maxbits = m;
-        sel->fast = 2;
-        sel->nr_sign = 0;
-        if (!(S > 0.) || S != S) {
+    unsigned long long maxbits = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) maxbits = max(maxbits, shu[i]);
+    if (!(S > 0.) || S != S) {
+        if (threadIdx.x == 0) {
+            if (fine) w.sum_f[b] = S;
+            else { w.sum_c[b] = S; w.r_ncsig[b] = 0; }
+            sel->maxbits = maxbits;
+            sel->fast = 2;
             sel->phase = 3;
             w.status[b] = T2B_ERR_NOSIGNIF;
         }
-        kmin = 0x7fffffffffffffffLL;
+        return;
     }
-    if (!(S > 0.) || S != S) return;
     const double target = frac * S;
+    const double floor_w = frac < 1. ? (1. - frac) * S / (double)n : 0.;
+    // the candidates (weight >= floor_w, > 0) into the front of sw / si, in any order
+#pragma unroll
+    for (int j = 0; j < SMALL_PER; j++) {
+        const long long i = threadIdx.x + (long long)j * blockDim.x;
+        if (i < n && wr[j] > 0. && wr[j] >= floor_w) {
+            const int pos = atomicAdd(&ncand, 1);
+            sw[pos] = wr[j];
+            si[pos] = sg.beg + i;
+        }
+    }
+    __syncthreads();
+    const int nc = ncand;
+    int n2 = 1;
+    while (n2 < nc) n2 <<= 1;
+    for (int i = nc + threadIdx.x; i < n2; i += blockDim.x) { sw[i] = -1.; si[i] = 0x7fffffffffffffffLL; }
+    __syncthreads();
     bitonic_pairs(sw, si, n2, true);
-    // inclusive prefix sums of the sorted weights: runs of `per` per thread, then the runs'
-    // exclusive offsets by a block scan
+    // inclusive prefix sums of the sorted candidates: runs of `per` per thread, then the
+    // runs' exclusive offsets by a block scan
     const int per = (n2 + (int)blockDim.x - 1) / (int)blockDim.x;
-    const int i0 = threadIdx.x * per, i1 = min((long long)(i0 + per), n);
+    const int i0 = threadIdx.x * per, i1 = min(i0 + per, nc);
     double run = 0.;
     for (int i = i0; i < i1; i++) run += sw[i];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -999,13 +1034,37 @@ __global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, double
     double cum = (wid > 0 ? shd[wid - 1] : 0.) + incl - run;
     for (int i = i0; i < i1; i++) {
         cum += sw[i];
-        if (cum > target) { atomicMin(&kmin, (long long)i); break; }
+        if (cum > target || (!fine && maxsig > 0 && i + 1 >= maxsig)) { atomicMin(&kmin, (long long)i); break; }
     }
     __syncthreads();
+    const long long k = kmin < nc ? kmin : nc - 1;
+    const double thr = sw[k];
+    const long long amax = si[0];
+    if (!fine) {
+        // the significant list: every weight >= thr (ties included), in index order
+        int cnt = 0;
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) cnt += sw[i] >= thr;
+        cnt = block_sum(cnt, reinterpret_cast<int*>(shu));
+        if (cnt > FAST_CAP) return;                  // too long for the list: left to the multi-kernel path
+        int m2 = 1;
+        while (m2 < cnt) m2 <<= 1;
+        for (int i = cnt + threadIdx.x; i < m2; i += blockDim.x) { sw[i] = 0.; si[i] = 0x7fffffffffffffffLL; }
+        __syncthreads();
+        bitonic_pairs(sw, si, m2, false);
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+            w.flist_w[(size_t)b * FAST_CAP + i] = sw[i];
+            w.flist_i[(size_t)b * FAST_CAP + i] = si[i];
+        }
+        if (threadIdx.x == 0) w.r_ncsig[b] = cnt;
+    }
     if (threadIdx.x == 0) {
-        const long long k = kmin < n ? kmin : n - 1;
-        sel->thr = sw[k];
-        sel->argmax = si[0];
+        if (fine) w.sum_f[b] = S;
+        else w.sum_c[b] = S;
+        sel->maxbits = maxbits;
+        sel->thr = thr;
+        sel->nr_sign = fine ? 0 : k + 1;
+        sel->argmax = amax;
+        sel->fast = 2;
         sel->phase = 2;
     }
 }
@@ -1762,6 +1821,7 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
     (void)maxsig;   // tb.maxsig
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
+    k_select_small<<<w.n, 1024, SMALL_SMEM, st>>>(tb, w, 0, tb.maxsig, tb.adaptive_fraction);
     k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 0);
     run_selection(tb, w, 0, 0, st);
     const long long n = (long long)tb.K * tb.O * tb.T;
@@ -1785,7 +1845,7 @@ void launch_weights_fine(const Tables& tb, const Work& w, cudaStream_t st)
 {
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
-    k_select_small<<<w.n, 1024, SMALL_SMEM, st>>>(tb, w, tb.adaptive_fraction);
+    k_select_small<<<w.n, 1024, SMALL_SMEM, st>>>(tb, w, 1, 0, tb.adaptive_fraction);
     k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 1);
     run_selection(tb, w, 1, 1, st);
     k_argmax_fine<<<grid, 256, 0, st>>>(tb, w);
