@@ -229,3 +229,27 @@ def test_audit_with_fewer_than_max_slots_graph_and_eager(trained):
         assert np.array_equal(a["pose"], b["pose"])
         assert np.allclose(a["audit_mass"], b["audit_mass"], rtol=1e-9)
         assert np.all(a["audit_mass"][a["audit_mass"] >= 0] > 0.5)
+
+
+def test_learned_coarse_selection_matches_oracle(trained):
+    """The coarse significance of a learned batch (one CTA per particle over its
+    proposals' hypotheses: weights, sum, candidates above the mass floor, threshold)
+    against the FP64 oracle's weights and threshold on the same diff2 values."""
+    es, P = trained["es"], trained["parts"]
+    n = 16
+    es.enable_proposals(topk=64, rescore=512, audit_every=1000, audit_mass=1e-6)
+    res = es.expectation(P["fimg"][:n], P["ctf"][:n], P["minv"][:n], P["scalars"][:n])
+    props = [es.proposals(b) for b in range(6)]
+    es.disable_proposals()
+    assert np.all(res["learned"] == 1)
+    T = trained["samp"]["n_trans"]
+    for b, (prop, d2) in enumerate(props):
+        d2 = d2.astype(np.float64).ravel()
+        ih = (prop[:, None].astype(np.int64) * T + np.arange(T)[None, :]).ravel()
+        mn = d2[d2 >= 0].min()
+        rc, wts, sw, sig, ns = trained["prob"].weights(trained["oparts"], b, 0, d2, ih, mn)
+        assert rc == 0
+        assert res["nr_sign"][b] == ns
+        assert res["coarse_sig_weight"][b] == pytest.approx(sig, rel=1e-12)
+        assert res["coarse_sum_weight"][b] == pytest.approx(sw, rel=1e-12)
+        assert res["n_coarse_sig"][b] == int(np.sum(wts >= sig))
