@@ -281,9 +281,11 @@ typedef struct t2b_tune_report {
 int t2b_autotune(t2b_ctx* ctx, const t2b_batch* batch, t2b_tune_report* report);
 int t2b_tune_set(t2b_ctx* ctx, const t2b_tune_report* shapes);
 
-/* Kernel launches of the last batch (the kernel nodes of its CUDA graph);
- * -1 when the last batch did not run as a graph.  With use_graph set, both
- * entry points replay a graph captured once per batch shape. */
+/* Kernel launches of the last batch: the kernel nodes of its CUDA graph that run
+ * every time (the bodies of its conditional nodes, the multi-kernel selection that
+ * runs only for particles with more hypotheses than one CTA selects, are not
+ * counted); -1 when the last batch did not run as a graph.  With use_graph set,
+ * both entry points replay a graph captured once per batch shape. */
 int t2b_last_launch_count(t2b_ctx* ctx, int* kernels);
 /* on != 0: host batches run uncaptured and record the per-stage events of
  * t2b_last_stage_ms (measurement support); 0 (default): graph replay. */

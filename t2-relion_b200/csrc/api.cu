@@ -562,8 +562,8 @@ static int replay_graph(t2b_ctx* c, Work& w, cudaStream_t st, const std::vector<
         T2B_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
         int kn = 0;
         for (auto nd : nodes) {
-            // this runtime reports conditional nodes (the selection's multi-level search) as an
-            // error: they are not kernel nodes either way
+            // this runtime reports conditional nodes (the selection's multi-kernel path) as an
+            // error: they are not kernel nodes either way, and their bodies run only when needed
             cudaGraphNodeType ty;
             if (cudaGraphNodeGetType(nd, &ty) != cudaSuccess) {
                 cudaGetLastError();

@@ -922,7 +922,8 @@ __global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass
 // list longer than FAST_CAP is left to that path.
 constexpr int SMALL_CAP = 8192;
 constexpr int SMALL_PER = SMALL_CAP / 1024;   // hypotheses per thread
-__global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, int fine, int maxsig, double frac)
+__global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, int fine, int maxsig, double frac,
+                                                       cudaGraphConditionalHandle cond)
 {
     extern __shared__ unsigned char smem_raw[];
     double* sw = reinterpret_cast<double*>(smem_raw);
@@ -936,7 +937,10 @@ __global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, int fi
     const bool pm = !fine && prop_mode(w);
     const Seg sg = seg_of(tb, w, fine, b);
     const long long n = sg.end - sg.beg;
-    if (n > SMALL_CAP) return;                      // the multi-kernel selection takes it
+    if (n > SMALL_CAP) {                            // the multi-kernel selection takes it
+        if (cond && threadIdx.x == 0) cudaGraphSetConditional(cond, 1);
+        return;
+    }
     if (w.status[b] != T2B_OK) {
         if (threadIdx.x == 0) {
             sel->fast = 2;
@@ -1045,7 +1049,10 @@ __global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, int fi
         int cnt = 0;
         for (int i = threadIdx.x; i < nc; i += blockDim.x) cnt += sw[i] >= thr;
         cnt = block_sum(cnt, reinterpret_cast<int*>(shu));
-        if (cnt > FAST_CAP) return;                  // too long for the list: left to the multi-kernel path
+        if (cnt > FAST_CAP) {                        // too long for the list: left to the multi-kernel path
+            if (cond && threadIdx.x == 0) cudaGraphSetConditional(cond, 1);
+            return;
+        }
         int m2 = 1;
         while (m2 < cnt) m2 <<= 1;
         for (int i = cnt + threadIdx.x; i < m2; i += blockDim.x) { sw[i] = 0.; si[i] = 0x7fffffffffffffffLL; }
@@ -1714,20 +1721,69 @@ const size_t HIST_SMEM = HIST_BINS * (sizeof(unsigned) + sizeof(double));
 const size_t FAST_SMEM = FAST_CAP * (sizeof(double) + sizeof(long long));
 const size_t SMALL_SMEM = SMALL_CAP * (sizeof(double) + sizeof(long long));
 
-// a stream per device to capture conditional-node bodies on
-cudaStream_t body_stream()
+// a stream per device and nesting depth to capture conditional-node bodies on
+cudaStream_t body_stream(int depth)
 {
     static std::mutex mu;
-    static std::map<int, cudaStream_t> streams;
+    static std::map<std::pair<int, int>, cudaStream_t> streams;
     int dev = 0;
     T2B_CUDA(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(mu);
-    cudaStream_t& bs = streams[dev];
+    cudaStream_t& bs = streams[{dev, depth}];
     if (!bs) T2B_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
     return bs;
 }
 
-void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStream_t st)
+// A condition for an IF node of the graph `st` is being captured into (reset to 0 at
+// every launch of the graph); 0 when `st` is not capturing.
+cudaGraphConditionalHandle cond_handle(cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    T2B_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
+    cudaGraphConditionalHandle h = 0;
+    if (cs == cudaStreamCaptureStatusActive && g != nullptr)
+        T2B_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    return h;
+}
+
+// Enqueue body(stream): under capture (h != 0) as the body of an IF node on h, whose
+// launches run only when a kernel before it set the condition; else directly on st.
+template <class F>
+void if_node(cudaStream_t st, cudaGraphConditionalHandle h, int depth, F body)
+{
+    if (!h) {
+        body(st);
+        return;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    T2B_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    T2B_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t bodyg = np.conditional.phGraph_out[0];
+    T2B_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t bs = body_stream(depth);
+    T2B_CUDA(cudaStreamBeginCaptureToGraph(bs, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+        body(bs);
+    } catch (...) {
+        cudaGraph_t dummy = nullptr;
+        cudaStreamEndCapture(bs, &dummy);
+        throw;
+    }
+    cudaGraph_t done = nullptr;
+    T2B_CUDA(cudaStreamEndCapture(bs, &done));
+}
+
+void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStream_t st, int depth)
 {
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
@@ -1735,12 +1791,7 @@ void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStr
     // under graph capture the multi-level search (levels 1-5, the candidate gather and sort)
     // is the body of an IF node whose condition the level-0 select sets when a particle needs
     // it, so the usual batch (every particle on the fast path) launches none of it
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    cudaGraph_t g = nullptr;
-    T2B_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
-    const bool cond = cs == cudaStreamCaptureStatusActive && g != nullptr;
-    cudaGraphConditionalHandle h = 0;
-    if (cond) T2B_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    const cudaGraphConditionalHandle h = cond_handle(st);
     k_sel_init<<<(w.n + 127) / 128, 128, 0, st>>>(w, fine, tb.adaptive_fraction);
     k_select<<<w.n, 1024, 0, st>>>(w, fine, maxsig, h);
     auto multilevel = [&](cudaStream_t s2) {
@@ -1751,33 +1802,7 @@ void run_selection(const Tables& tb, const Work& w, int fine, int ipass, cudaStr
         k_gather<<<grid, 256, 0, s2>>>(tb, w, fine);
         k_final<<<w.n, 1024, 0, s2>>>(w, fine, ipass, maxsig);
     };
-    if (cond) {
-        const cudaGraphNode_t* deps = nullptr;
-        size_t nd = 0;
-        T2B_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
-        cudaGraphNodeParams np{};
-        np.type = cudaGraphNodeTypeConditional;
-        np.conditional.handle = h;
-        np.conditional.type = cudaGraphCondTypeIf;
-        np.conditional.size = 1;
-        cudaGraphNode_t node = nullptr;
-        T2B_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
-        cudaGraph_t body = np.conditional.phGraph_out[0];
-        T2B_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
-        cudaStream_t bs = body_stream();
-        T2B_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        try {
-            multilevel(bs);
-        } catch (...) {
-            cudaGraph_t dummy = nullptr;
-            cudaStreamEndCapture(bs, &dummy);
-            throw;
-        }
-        cudaGraph_t done = nullptr;
-        T2B_CUDA(cudaStreamEndCapture(bs, &done));
-    } else {
-        multilevel(st);
-    }
+    if_node(st, h, depth, multilevel);
     k_gather_fast<<<grid, 256, 0, st>>>(tb, w, fine);
     k_final_fast<<<w.n, 1024, FAST_SMEM, st>>>(w, fine, ipass, maxsig);
 }
@@ -1821,16 +1846,21 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
     (void)maxsig;   // tb.maxsig
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
-    k_select_small<<<w.n, 1024, SMALL_SMEM, st>>>(tb, w, 0, tb.maxsig, tb.adaptive_fraction);
-    k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 0);
-    run_selection(tb, w, 0, 0, st);
     const long long n = (long long)tb.K * tb.O * tb.T;
     const int nch = (int)((n + CHUNK - 1) / CHUNK);
     dim3 gc(std::min(nch, gx), w.n);
-    k_count_sig<<<gc, 256, 0, st>>>(tb, w);
-    k_scan_chunks<<<w.n, 1024, 0, st>>>(tb, w);
+    // under capture, the multi-kernel selection and compaction are IF-node bodies that run
+    // only when the one-CTA selection left a particle to them
+    const cudaGraphConditionalHandle h = cond_handle(st);
+    k_select_small<<<w.n, 1024, SMALL_SMEM, st>>>(tb, w, 0, tb.maxsig, tb.adaptive_fraction, h);
+    if_node(st, h, 0, [&](cudaStream_t s) {
+        k_weights<<<grid, 256, HIST_SMEM, s>>>(tb, w, 0);
+        run_selection(tb, w, 0, 0, s, 1);
+        k_count_sig<<<gc, 256, 0, s>>>(tb, w);
+        k_scan_chunks<<<w.n, 1024, 0, s>>>(tb, w);
+    });
     k_pair_offsets<<<1, 1024, 0, st>>>(w);
-    k_compact<<<gc, 256, 0, st>>>(tb, w, tb.ovs ? 0 : 1);
+    k_compact<<<gc, 256, 0, st>>>(tb, w, tb.ovs ? 0 : 1);   // (a handle serves one IF node; this returns at once when unused)
     k_write_fast<<<w.n, 256, 0, st>>>(tb, w, tb.ovs ? 0 : 1);
     T2B_CUDA(cudaGetLastError());
 }
@@ -1845,10 +1875,13 @@ void launch_weights_fine(const Tables& tb, const Work& w, cudaStream_t st)
 {
     const int gx = grid_x_for(w.n);
     dim3 grid(gx, w.n);
-    k_select_small<<<w.n, 1024, SMALL_SMEM, st>>>(tb, w, 1, 0, tb.adaptive_fraction);
-    k_weights<<<grid, 256, HIST_SMEM, st>>>(tb, w, 1);
-    run_selection(tb, w, 1, 1, st);
-    k_argmax_fine<<<grid, 256, 0, st>>>(tb, w);
+    const cudaGraphConditionalHandle h = cond_handle(st);
+    k_select_small<<<w.n, 1024, SMALL_SMEM, st>>>(tb, w, 1, 0, tb.adaptive_fraction, h);
+    if_node(st, h, 0, [&](cudaStream_t s) {
+        k_weights<<<grid, 256, HIST_SMEM, s>>>(tb, w, 1);
+        run_selection(tb, w, 1, 1, s, 1);
+        k_argmax_fine<<<grid, 256, 0, s>>>(tb, w);
+    });
     T2B_CUDA(cudaGetLastError());
 }
 

@@ -41,7 +41,8 @@ def test_graph_replay_matches_host_path(mode):
             assert np.allclose(got[k], ref[k], rtol=1e-9, atol=0), k
         # FP32 per-pixel terms accumulated by atomics in arbitrary order
         assert np.allclose(got["wsum_norm"], ref["wsum_norm"], rtol=1e-5, atol=0)
-    assert es.launch_count() > 20
+    # kernel nodes outside the conditional bodies (the selection's multi-kernel path)
+    assert es.launch_count() >= 10
     es.close()
 
 
