@@ -153,7 +153,10 @@ typedef struct t2b_result {
  * the grids of t2b_backprojector_init.  The host variant copies the batch in,
  * runs, and copies the results out before returning.  The device variant only
  * enqueues on `stream` (cudaStream_t, NULL = the context's stream); result
- * pointers are device memory and valid after the stream completes. */
+ * pointers are device memory and valid after the stream completes.  Batches of
+ * one context run in the order they were enqueued, on whichever entry point and
+ * stream (the caller's stream waits for the context's earlier batches, and the
+ * context's later batches for it). */
 int t2b_estep_batch_host(t2b_ctx* ctx, const t2b_batch* batch, const t2b_result* out);
 int t2b_estep_batch_device(t2b_ctx* ctx, const t2b_batch* batch, const t2b_result* out, void* stream);
 

@@ -89,6 +89,7 @@ int t2b_create(int device, t2b_ctx** out)
             T2B_CUDA(e);
         }
         for (auto& ev : c->ev) cudaEventCreate(&ev);
+        for (auto& ev : c->handoff) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         *out = c;
     });
 }
@@ -109,6 +110,7 @@ void t2b_destroy(t2b_ctx* c)
         for (auto p : c->gdata) cudaFree(p);
         for (auto p : c->gweight) cudaFree(p);
         for (auto& ev : c->ev) cudaEventDestroy(ev);
+        for (auto& ev : c->handoff) cudaEventDestroy(ev);
         for (auto& s : c->in)
             for (cudaEvent_t ev : {s.copied, s.consumed, s.done}) cudaEventDestroy(ev);
         cudaStreamDestroy(c->copy_stream);
@@ -709,6 +711,13 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard g(c->device);
         cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+        // the batch shares the context's workspace with host batches still in flight on the
+        // context's stream: the caller's stream waits for them, and they for it
+        const bool other = st != c->stream;
+        if (other) {
+            T2B_CUDA(cudaEventRecord(c->handoff[0], c->stream));
+            T2B_CUDA(cudaStreamWaitEvent(st, c->handoff[0], 0));
+        }
         Work w = c->wk;
         w.n = b->n;
         w.fimg = (const float2*)b->fimg;
@@ -737,6 +746,10 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
         } else {
             enqueue_estep(c, w, st, true, true);
             c->last_kernels = -1;
+        }
+        if (other) {
+            T2B_CUDA(cudaEventRecord(c->handoff[1], st));
+            T2B_CUDA(cudaStreamWaitEvent(c->stream, c->handoff[1], 0));
         }
         c->last_n = b->n;
     });

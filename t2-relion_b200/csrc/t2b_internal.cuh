@@ -314,6 +314,7 @@ struct t2b_ctx {
     }
     int last_kernels = -1;
     cudaEvent_t ev[12]{};                     // 8 stage boundaries + 2 pairs around the proposal-path GEMMs
+    cudaEvent_t handoff[2]{};                 // orders a caller's stream after the context's and back
     float stage_ms[9]{};
     bool prop_events = false;                 // the last timed batch recorded ev[8..11]
     t2b::ProposalNet* net = nullptr;          // learned orientation proposals (proposal.cu)

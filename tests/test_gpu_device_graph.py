@@ -80,3 +80,45 @@ def test_pipelined_host_batches_match_synchronous_ones(t2b):
     with pytest.raises(t2b.T2BError):
         es.wait(tickets[-1][0] + 1)
     es.close()
+
+
+def test_host_submissions_and_device_batch_are_ordered():
+    """A device batch on the caller's stream, enqueued while pipelined host batches are in
+    flight on the context's stream, waits for them (shared workspace), and a host batch
+    submitted after it waits for the device batch: every result equals the batch run alone."""
+    import torch
+    pb = problems.build("refine_o1_ovs", n_particles=12, seed=14, diff2_mode=1)
+    P = pb["parts"]
+    es = pb["product"]()
+    halves = [(0, 6), (6, 12)]
+
+    def part(a, b):
+        return P["fimg"][a:b], P["ctf"][a:b], P["minv"][a:b], P["scalars"][a:b]
+
+    ref = [es.expectation(*part(a, b)) for a, b in halves]
+    dev = torch.device("cuda")
+    a, b = halves[1]
+    n = b - a
+    fimg = torch.from_numpy(np.ascontiguousarray(P["fimg"][a:b]).view(np.float32)).to(dev)
+    ctf = torch.from_numpy(np.ascontiguousarray(P["ctf"][a:b])).to(dev)
+    minv = torch.from_numpy(np.ascontiguousarray(P["minv"][a:b])).to(dev)
+    scal = torch.from_numpy(np.ascontiguousarray(P["scalars"][a:b])).to(dev)
+    host = es._result_arrays(n)
+    tmap = {np.dtype("float64"): torch.float64, np.dtype("int64"): torch.int64, np.dtype("int32"): torch.int32}
+    res = {k: torch.zeros(v.shape, dtype=tmap[v.dtype], device=dev) for k, v in host.items()}
+    ptrs = {k: ctypes.c_void_p(v.data_ptr()) for k, v in res.items()}
+    stream = torch.cuda.Stream()
+    t0, got0 = es.expectation_submit(*part(*halves[0]))
+    es.expectation_device(n, ctypes.c_void_p(fimg.data_ptr()), ctypes.c_void_p(ctf.data_ptr()),
+                          ctypes.c_void_p(minv.data_ptr()), ctypes.c_void_p(scal.data_ptr()), ptrs,
+                          stream=stream.cuda_stream)
+    t2, got2 = es.expectation_submit(*part(*halves[0]))
+    es.wait()
+    stream.synchronize()
+    got1 = {k: v.cpu().numpy() for k, v in res.items()}
+    for got, r in ((got0, ref[0]), (got1, ref[1]), (got2, ref[0])):
+        assert np.all(got["status"] == 0)
+        assert np.array_equal(got["pose"], r["pose"])
+        assert np.array_equal(got["nr_sign"], r["nr_sign"])
+        assert np.allclose(got["sum_weight"], r["sum_weight"], rtol=1e-9, atol=0)
+    es.close()
