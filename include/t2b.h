@@ -164,8 +164,8 @@ int t2b_estep_batch_device(t2b_ctx* ctx, const t2b_batch* batch, const t2b_resul
  * its own CUDA stream, src/acc/cuda/cuda_ml_optimiser.cu:511-561): submit
  * enqueues what t2b_estep_batch_host does and returns at once with a ticket
  * (0, 1, 2, ... per context).  A batch's inputs are copied in on a copy stream while
- * the previous batch computes; batches run and write their results in submission
- * order.  The batch's host inputs and result arrays must stay valid and untouched
+ * the previous batch computes, and its results are read back on a third stream while
+ * the next one computes; batches run and write their results in submission order.  The batch's host inputs and result arrays must stay valid and untouched
  * until t2b_estep_wait(ctx, ticket) (or a later ticket, or -1 = every batch) returns.
  * t2b_estep_batch_host is submit followed by wait. */
 int t2b_estep_submit_host(t2b_ctx* ctx, const t2b_batch* batch, const t2b_result* out, long long* ticket);

@@ -76,6 +76,7 @@ int t2b_create(int device, t2b_ctx** out)
         c->device = device;
         cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking);
         for (auto& s : c->in)
             for (cudaEvent_t* ev : {&s.copied, &s.consumed, &s.done})
                 if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
@@ -83,6 +84,7 @@ int t2b_create(int device, t2b_ctx** out)
             for (auto& s : c->in)
                 for (cudaEvent_t ev : {s.copied, s.consumed, s.done})
                     if (ev) cudaEventDestroy(ev);
+            if (c->d2h_stream) cudaStreamDestroy(c->d2h_stream);
             if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
             if (c->stream) cudaStreamDestroy(c->stream);
             delete c;
@@ -103,6 +105,7 @@ void t2b_destroy(t2b_ctx* c)
         cudaSetDevice(c->device);
         cudaStreamSynchronize(c->copy_stream);
         cudaStreamSynchronize(c->stream);
+        cudaStreamSynchronize(c->d2h_stream);
         free_allocs(c);
         proposal_release(c);
         imageprep_release(c);
@@ -113,6 +116,7 @@ void t2b_destroy(t2b_ctx* c)
         for (auto& ev : c->handoff) cudaEventDestroy(ev);
         for (auto& s : c->in)
             for (cudaEvent_t ev : {s.copied, s.consumed, s.done}) cudaEventDestroy(ev);
+        cudaStreamDestroy(c->d2h_stream);
         cudaStreamDestroy(c->copy_stream);
         cudaStreamDestroy(c->stream);
         if (prev >= 0) cudaSetDevice(prev);
@@ -259,8 +263,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         }
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard g(c->device);
-        T2B_CUDA(cudaStreamSynchronize(c->copy_stream));
-        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        c->quiesce();
         free_allocs(c);
         proposal_invalidate(c);
         estep_init_attributes();
@@ -429,6 +432,29 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         w.r_sigma2 = dalloc<double>(c, (size_t)B * (f.ori_size / 2 + 1));
         w.r_pdf_class = dalloc<double>(c, (size_t)B * K);
         w.r_pdf_dir = dalloc<double>(c, (size_t)B * K * f.n_dir);
+        // results of the two host slots: slot 0 the workspace's, slot 1 a second set
+        for (int i = 0; i < 2; i++) {
+            t2b_ctx::InSlot& s = c->in[i];
+            const bool own = i == 0;
+            s.r_min = own ? w.r_min : dalloc<double>(c, B);
+            s.r_sum = own ? w.r_sum : dalloc<double>(c, B);
+            s.r_sig = own ? w.r_sig : dalloc<double>(c, B);
+            s.r_csum = own ? w.r_csum : dalloc<double>(c, B);
+            s.r_csig = own ? w.r_csig : dalloc<double>(c, B);
+            s.r_pmax = own ? w.r_pmax : dalloc<double>(c, B);
+            s.r_nsign = own ? w.r_nsign : dalloc<long long>(c, B);
+            s.r_ncsig = own ? w.r_ncsig : dalloc<long long>(c, B);
+            s.r_pose = own ? w.r_pose : dalloc<int>(c, (size_t)B * 5);
+            s.r_norm = own ? w.r_norm : dalloc<double>(c, B);
+            s.r_sumw = own ? w.r_sumw : dalloc<double>(c, B);
+            s.r_sig_off = own ? w.r_sig_off : dalloc<double>(c, B);
+            s.r_sigma2 = own ? w.r_sigma2 : dalloc<double>(c, (size_t)B * (f.ori_size / 2 + 1));
+            s.r_pdf_class = own ? w.r_pdf_class : dalloc<double>(c, (size_t)B * K);
+            s.r_pdf_dir = own ? w.r_pdf_dir : dalloc<double>(c, (size_t)B * K * f.n_dir);
+            s.status = own ? w.status : dalloc<int>(c, B);
+            s.r_learned = own ? w.r_learned : dalloc<int>(c, B);
+            s.r_audit = own ? w.r_audit : dalloc<double>(c, B);
+        }
         // grid pointer tables
         float2** gd = dalloc<float2*>(c, K);
         float** gw = dalloc<float*>(c, K);
@@ -584,11 +610,12 @@ static int replay_graph(t2b_ctx* c, Work& w, cudaStream_t st, const std::vector<
 }
 
 // Enqueue one host batch: inputs into staging slot (ticket & 1) on the copy stream once
-// that slot's previous batch has read its own, the batch on the context's stream once
-// they are in, the results back to host memory after it.  Returns the ticket.
+// that slot's previous batch has read its own, the batch on the context's stream once they
+// are in and that batch's results have left the slot, and the results back to host memory
+// on the read-back stream after it.  Returns the ticket.
 static long long submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r)
 {
-    cudaStream_t st = c->stream, cs = c->copy_stream;
+    cudaStream_t st = c->stream, cs = c->copy_stream, ds = c->d2h_stream;
     const long long ticket = c->submitted;
     t2b_ctx::InSlot& in = c->in[ticket & 1];
     Work w = c->wk;
@@ -599,6 +626,11 @@ static long long submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r
     w.ctf = in.ctf;
     w.minv = in.minv;
     w.scal = in.scal;
+    w.r_min = in.r_min; w.r_sum = in.r_sum; w.r_sig = in.r_sig; w.r_csum = in.r_csum; w.r_csig = in.r_csig;
+    w.r_pmax = in.r_pmax; w.r_nsign = in.r_nsign; w.r_ncsig = in.r_ncsig; w.r_pose = in.r_pose;
+    w.r_norm = in.r_norm; w.r_sumw = in.r_sumw; w.r_sig_off = in.r_sig_off; w.r_sigma2 = in.r_sigma2;
+    w.r_pdf_class = in.r_pdf_class; w.r_pdf_dir = in.r_pdf_dir; w.status = in.status;
+    w.r_learned = in.r_learned; w.r_audit = in.r_audit;
     T2B_CUDA(cudaStreamWaitEvent(cs, in.consumed, 0));
     T2B_CUDA(cudaMemcpyAsync(in.fimg, b->fimg, (size_t)n * P * sizeof(float2), cudaMemcpyHostToDevice, cs));
     if (b->fimg_nomask)
@@ -608,6 +640,7 @@ static long long submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r
     T2B_CUDA(cudaMemcpyAsync(in.scal, b->scalars, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, cs));
     T2B_CUDA(cudaEventRecord(in.copied, cs));
     T2B_CUDA(cudaStreamWaitEvent(st, in.copied, 0));
+    T2B_CUDA(cudaStreamWaitEvent(st, in.done, 0));
     // the batch computation itself: a replayed graph unless stage timing is on
     const bool graph = c->cfg.use_graph && !c->stage_timing;
     if (graph) {
@@ -619,9 +652,10 @@ static long long submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r
         c->last_kernels = -1;
     }
     T2B_CUDA(cudaEventRecord(in.consumed, st));
+    T2B_CUDA(cudaStreamWaitEvent(ds, in.consumed, 0));
     const int K = c->tb.K, half = c->cfg.ori_size / 2 + 1;
     auto d2h = [&](void* dst, const void* src, size_t bytes) {
-        if (dst) T2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        if (dst) T2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ds));
     };
     d2h(r->min_diff2, w.r_min, n * sizeof(double));
     d2h(r->sum_weight, w.r_sum, n * sizeof(double));
@@ -641,7 +675,7 @@ static long long submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r
     d2h(r->status, w.status, n * sizeof(int));
     d2h(r->learned, w.r_learned, n * sizeof(int));
     d2h(r->audit_mass, w.r_audit, n * sizeof(double));
-    T2B_CUDA(cudaEventRecord(in.done, st));
+    T2B_CUDA(cudaEventRecord(in.done, ds));
     c->last_n = n;
     return c->submitted++;
 }
@@ -658,7 +692,10 @@ static void wait_host(t2b_ctx* c, long long ticket)
     DeviceGuard g(c->device);
     // a slot's event recorded again by a later batch completes after this one: stream order
     if (ev) T2B_CUDA(cudaEventSynchronize(ev));
-    else T2B_CUDA(cudaStreamSynchronize(c->stream));
+    else {
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        T2B_CUDA(cudaStreamSynchronize(c->d2h_stream));
+    }
 }
 
 }  // namespace t2b
@@ -764,6 +801,7 @@ int t2b_autotune(t2b_ctx* c, const t2b_batch* b, t2b_tune_report* rep)
         T2B_REQUIRE(b->fimg && b->ctf && b->minvsigma2 && b->scalars, T2B_ERR_ARG, "missing batch inputs");
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard g(c->device);
+        c->quiesce();   // the tuning batches use slot 0's buffers
         cudaStream_t st = c->stream;
         Work w = c->wk;
         const int n = b->n, P = c->tb.P, K = c->tb.K;

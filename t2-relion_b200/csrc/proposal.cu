@@ -1724,6 +1724,7 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
                     T2B_ERR_ARG, "bad proposal training configuration");
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard dg(c->device);
+        c->quiesce();   // training reallocates buffers that host batches in flight still use
         cudaStream_t st = c->stream;
         drop_graph(c);
         const Tables& tb = c->tb;

@@ -287,21 +287,34 @@ struct t2b_ctx {
         int kernels = -1;                     // its kernel nodes
     };
     GraphSlot g_dev;                          // device entry point
-    // Host entry points: two staging slots for the batch inputs.  A batch's inputs are
-    // copied into its slot on copy_stream while the previous batch computes on `stream`;
-    // slot 0 is the workspace's own input buffers, slot 1 a second set.
+    // Host entry points: two staging slots, each with the batch inputs and results.  A
+    // batch's inputs are copied into its slot on copy_stream while the previous batch
+    // computes on `stream`, and its results leave the slot on d2h_stream while the next one
+    // computes; slot 0 is the workspace's own buffers, slot 1 a second set.
     struct InSlot {
         float2* fimg = nullptr;
         float2* fimg_nm = nullptr;
         float* ctf = nullptr;
         float* minv = nullptr;
         double* scal = nullptr;
+        double *r_min = nullptr, *r_sum = nullptr, *r_sig = nullptr, *r_csum = nullptr, *r_csig = nullptr,
+               *r_pmax = nullptr, *r_norm = nullptr, *r_sumw = nullptr, *r_sig_off = nullptr, *r_sigma2 = nullptr,
+               *r_pdf_class = nullptr, *r_pdf_dir = nullptr, *r_audit = nullptr;
+        long long *r_nsign = nullptr, *r_ncsig = nullptr;
+        int *r_pose = nullptr, *status = nullptr, *r_learned = nullptr;
         cudaEvent_t copied = nullptr;         // inputs in the slot (copy_stream)
-        cudaEvent_t consumed = nullptr;       // the slot's batch has read them (stream)
-        cudaEvent_t done = nullptr;           // the slot's results are in host memory (stream)
-        GraphSlot g;                          // the captured batch reading this slot
+        cudaEvent_t consumed = nullptr;       // the slot's batch has run (stream)
+        cudaEvent_t done = nullptr;           // the slot's results are in host memory (d2h_stream)
+        GraphSlot g;                          // the captured batch of this slot
     } in[2];
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t d2h_stream = nullptr;
+    // Wait for every host batch in flight: its input copies, computation and result reads.
+    void quiesce()
+    {
+        for (cudaStream_t s : {copy_stream, stream, d2h_stream})
+            if (s) T2B_CUDA(cudaStreamSynchronize(s));
+    }
     long long submitted = 0;                  // host batches submitted: the next ticket
     bool stage_timing = false;                // host batches run uncaptured with stage events
     void drop_graphs()
