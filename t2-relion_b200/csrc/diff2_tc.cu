@@ -32,7 +32,11 @@ namespace {
 
 constexpr int TM = 128, TN = 256, TK = 64;
 constexpr int STAGES = 2;       // pipeline stages of 128 x 256 tiles (96 KB each)
-constexpr int MAXSTAGES = 8;    // narrower tiles and fewer products: more, smaller stages in the same space
+constexpr int MAXSTAGES = 8;
+#ifndef T2B_L2_AHEAD
+#define T2B_L2_AHEAD 4
+#endif
+constexpr int L2_AHEAD = T2B_L2_AHEAD;  // k-blocks between an A tile's L2 prefetch and its load    // narrower tiles and fewer products: more, smaller stages in the same space
 constexpr uint32_t A_BYTES = TM * TK * 2;              // 16 KB
 constexpr uint32_t B_BYTES = TN * TK * 2;              // 32 KB
 constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
@@ -98,6 +102,13 @@ __device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, uint
             su32(dst)),
         "l"(map), "r"(su32(bar)), "r"(x), "r"(y)
         : "memory");
+}
+
+// Bring one box of a tensor map into L2 ahead of its load (no shared memory, no barrier).
+__device__ __forceinline__ void tma_prefetch_l2(const CUtensorMap* map, int x, int y)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(map), "r"(x), "r"(y)
+                 : "memory");
 }
 
 // One contiguous block global -> shared (untiled bulk copy): the operand is stored
@@ -284,6 +295,14 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         int issued[MAXSTAGES] = {};
         uint32_t last_par[MAXSTAGES] = {};
         const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + bbytes * (p.products >= 2 ? 2u : 1u);
+        // A tiles read by one column tile only (the audit contractions) come from DRAM once and
+        // wide stages leave room for two in shared memory: fetch them into L2 L2_AHEAD k-blocks
+        // before their loads, so the loads find them there
+        const bool pf = L2_AHEAD > 0 && p.mode == 0 && p.n_tiles == 1;
+        auto prefetch_a = [&](int kb, int ya) {
+            tma_prefetch_l2(mPh, kb * TK, ya);
+            if (p.products == 3) tma_prefetch_l2(mPl, kb * TK, ya);
+        };
         for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
             int ya, yb;
             const int kb0 = (tile % ksp) * kper, kb1 = min(p.kblocks, kb0 + kper);
@@ -299,9 +318,12 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                 ya = tile * TM;
                 yb = (tile / (p.mtp ? p.mtp : 1)) * p.T;
             }
+            if (pf)
+                for (int kb = kb0 + 1; kb < min(kb1, kb0 + L2_AHEAD); kb++) prefetch_a(kb, ya);
             for (int kb = kb0; kb < kb1; kb++, it++) {
                 const int s = it % nst;
                 const uint32_t ph = (uint32_t)(it / nst) & 1u;
+                if (pf && kb + L2_AHEAD < kb1) prefetch_a(kb + L2_AHEAD, ya);
                 if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
                 uint8_t* st = gbase + s * sbytes;
                 mbar_expect_tx(&full_bar[s], tx_bytes);

@@ -122,3 +122,33 @@ def test_host_submissions_and_device_batch_are_ordered():
         assert np.array_equal(got["nr_sign"], r["nr_sign"])
         assert np.allclose(got["sum_weight"], r["sum_weight"], rtol=1e-9, atol=0)
     es.close()
+
+
+def test_autotune_waits_for_host_batches_in_flight():
+    """Two pipelined host batches (one per staging slot, their results read back on a
+    separate stream) are still in flight when t2b_autotune runs tuning batches on slot 0's
+    buffers: the tuner waits for them, both keep their own results, and a batch submitted
+    after the tuner (slot 0 again) gives the results of the same batch run alone."""
+    pb = problems.build("refine_o1_ovs", n_particles=12, seed=15, diff2_mode=1)
+    P = pb["parts"]
+    es = pb["product"]()
+    halves = [(0, 6), (6, 12)]
+
+    def part(a, b):
+        return P["fimg"][a:b], P["ctf"][a:b], P["minv"][a:b], P["scalars"][a:b]
+
+    ref = [es.expectation(*part(a, b)) for a, b in halves]
+    t0, got0 = es.expectation_submit(*part(*halves[0]))
+    t1, got1 = es.expectation_submit(*part(*halves[1]))
+    es.autotune(*part(0, 12))
+    es.wait(t1)
+    t2, got2 = es.expectation_submit(*part(*halves[0]))
+    es.wait()
+    for got, r in ((got0, ref[0]), (got1, ref[1]), (got2, ref[0])):
+        assert np.all(got["status"] == 0)
+        assert np.array_equal(got["pose"], r["pose"])
+        assert np.array_equal(got["nr_sign"], r["nr_sign"])
+        # the tuned tile shapes change no FP64 sum beyond rounding
+        assert np.allclose(got["sum_weight"], r["sum_weight"], rtol=1e-7, atol=0)
+        assert np.allclose(got["min_diff2"], r["min_diff2"], rtol=1e-7, atol=0)
+    es.close()
