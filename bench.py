@@ -60,9 +60,9 @@ PROP = dict(topk=64, rescore=1024, audit_every=50, audit_mass=0.999)
 E2E_STEPS = 30
 # DRAM bytes (read + write) of the audit + proposal k_diff2_tc launches of one learned step
 # at 128 particles, from one ncu capture
-# (audit 766.12 MB read + 18.88 MB written, proposal pass 169.96 MB + 0.11 MB;
+# (audit 766.60 MB read + 18.67 MB written, proposal pass 169.96 MB + 0.14 MB;
 # profiles/k_diff2_tc_box128_learned_b128_dram.md)
-LEARNED_TRAFFIC = 766.12e6 + 18.88e6 + 169.96e6 + 0.11e6
+LEARNED_TRAFFIC = 766.60e6 + 18.67e6 + 169.96e6 + 0.14e6
 
 
 def build_problem(t2b, sy, n_particles, seed):
