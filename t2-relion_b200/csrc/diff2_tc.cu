@@ -295,10 +295,11 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
         int issued[MAXSTAGES] = {};
         uint32_t last_par[MAXSTAGES] = {};
         const uint32_t tx_bytes = A_BYTES * (p.products == 3 ? 2u : 1u) + bbytes * (p.products >= 2 ? 2u : 1u);
-        // A tiles read by one column tile only (the audit contractions) come from DRAM once and
+        // A tiles read by one column tile only (the audit contractions) come from DRAM once, and
         // wide stages leave room for two in shared memory: fetch them into L2 L2_AHEAD k-blocks
-        // before their loads, so the loads find them there
-        const bool pf = L2_AHEAD > 0 && p.mode == 0 && p.n_tiles == 1;
+        // before their loads, so the loads find them there (with more stages the loads in
+        // flight already cover the latency, and the prefetches only add requests)
+        const bool pf = L2_AHEAD > 0 && p.mode == 0 && p.n_tiles == 1 && nst <= 2;
         auto prefetch_a = [&](int kb, int ya) {
             tma_prefetch_l2(mPh, kb * TK, ya);
             if (p.products == 3) tma_prefetch_l2(mPl, kb * TK, ya);
