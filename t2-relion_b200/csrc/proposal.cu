@@ -1920,6 +1920,7 @@ int t2b_proposal_enable(t2b_ctx* c, int topk, int rescore, int audit_every, doub
         T2B_REQUIRE(c, T2B_ERR_ARG, "null context");
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard dg(c->device);
+        c->quiesce();   // buffers of the network and of slot 0 may be in use by host batches in flight
         drop_graph(c);
         if (topk == 0) {
             if (c->net) c->net->enabled = false;
@@ -1958,6 +1959,7 @@ int t2b_proposal_params(t2b_ctx* c, float* get, const float* set, long long* cou
         DeviceGuard dg(c->device);
         ProposalNet& N = net_params(c, c->tb.K * c->tb.O);
         *count = (long long)N.L.total;
+        if (get || set) c->quiesce();   // the copies run outside the context's streams
         if (get) T2B_CUDA(cudaMemcpy(get, N.th, N.L.total * sizeof(float), cudaMemcpyDeviceToHost));
         if (set) {
             drop_graph(c);
@@ -1979,6 +1981,7 @@ int t2b_proposal_features(t2b_ctx* c, const t2b_batch* b, float* imgs)
         T2B_REQUIRE(c->configured && b->n >= 1 && b->n <= c->cfg.max_batch, T2B_ERR_ARG, "batch size out of range");
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard dg(c->device);
+        c->quiesce();   // buffers of the network and of slot 0 may be in use by host batches in flight
         ProposalNet& N = net_params(c, c->tb.K * c->tb.O);
         net_setup(c, std::max(1, N.na_max));
         cudaStream_t st = c->stream;
@@ -2001,6 +2004,7 @@ int t2b_proposal_logits(t2b_ctx* c, const float* imgs, int n, float* logits)
         T2B_REQUIRE(c->configured && n >= 1 && n <= c->cfg.max_batch, T2B_ERR_ARG, "n out of range");
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard dg(c->device);
+        c->quiesce();   // buffers of the network and of slot 0 may be in use by host batches in flight
         ProposalNet& N = net_params(c, c->tb.K * c->tb.O);
         net_setup(c, std::max(1, N.na_max));
         cudaStream_t st = c->stream;
@@ -2023,6 +2027,7 @@ int t2b_proposal_grad(t2b_ctx* c, const float* imgs, const int* tgt_oc, const fl
         T2B_REQUIRE(c->configured && n >= 1 && n <= 1024, T2B_ERR_ARG, "n out of range");
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard dg(c->device);
+        c->quiesce();   // buffers of the network and of slot 0 may be in use by host batches in flight
         const int KO = c->tb.K * c->tb.O;
         ProposalNet& N = net_params(c, KO);
         for (int i = 0; i < n * NET_NTGT; i++)
