@@ -104,6 +104,11 @@ typedef struct t2b_config {
     double pixel_size;
     double adaptive_fraction;
     size_t fine_capacity;      /* fine hypotheses per batch (0: default)                */
+    const double* data_vs_prior;/* nr_classes x (ori_size/2+1): mymodel.data_vs_prior_class, or
+                                  NULL.  Non-NULL turns on the scale-correction sums
+                                  (do_scale_correction): a pixel of ring ires in class k adds to
+                                  them when data_vs_prior[k][ires] > 3 (src/ml_optimiser.cpp:
+                                  8477-8486)                                             */
 } t2b_config;
 
 /* Validate the configuration, build the projection tables of all coarse and
@@ -145,6 +150,12 @@ typedef struct t2b_result {
     double* audit_mass;         /* n: posterior mass of the full coarse pass held by the
                                    particle's proposals (audited particles), else -1     */
     int* learned;               /* n: 1 if the coarse pass ran on the proposals          */
+    /* scale correction (optional, may be NULL; computed when t2b_config.data_vs_prior is set,
+       else 0): exp_wsum_scale_correction_XA / _AA of src/ml_optimiser.cpp:8477-8486, 8859-8860
+       = sum over significant hypotheses and pixels of w' Re(A conj(X_shift)) and w' |A|^2,
+       A = scale CTF P, divided by scale_correction and its square                         */
+    double* wsum_scale_xa;      /* n: thr_wsum_signal_product_spectra contribution          */
+    double* wsum_scale_aa;      /* n: thr_wsum_reference_power_spectra contribution         */
 } t2b_result;
 
 /* E-step of one batch (MlOptimiserCuda::doThreadExpectationSomeParticles,
@@ -253,6 +264,16 @@ int t2b_project(t2b_ctx* ctx, int iclass, const double* eulers, int n, int curre
  * nover_rot*nover_trans).  *count receives the number of pairs. */
 int t2b_debug_coarse_diff2(t2b_ctx* ctx, int b, float* out);
 int t2b_debug_fine(t2b_ctx* ctx, int b, long long* pairs, float* diff2, long long cap, long long* count);
+/* Final-pass weights of particle b in the last batch (FP64, before the division
+ * by sum_weight), in the order of t2b_debug_fine's pairs: pairs x
+ * nover_rot*nover_trans values with adaptive oversampling, else one per pair
+ * (the significant coarse pairs).  *count receives the number of values. */
+int t2b_debug_weights(t2b_ctx* ctx, int b, double* weights, long long cap, long long* count);
+/* Which significance search decided particle b's coarse and fine pass in the last batch:
+ * 2 = one CTA per particle (<= 8192 hypotheses), 1 = the multi-kernel search whose
+ * crossing-bin candidates were gathered by the fast path, 0 = the multi-kernel radix
+ * search with its finer histogram levels.  fine_path is -1 without adaptive oversampling. */
+int t2b_debug_selection(t2b_ctx* ctx, int b, int* coarse_path, int* fine_path);
 /* Learned proposals of particle b in the last batch (valid where that batch's
  * `learned` result is 1): *kprop receives the proposals per particle; prop
  * (kprop ints, may be NULL) their orientation indices k*n_dir*n_psi + o, and

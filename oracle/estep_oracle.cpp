@@ -237,6 +237,8 @@ struct OrcSetup {
     double* bp_data;              // complex interleaved, nr_classes x grid
     double* bp_weight;            // nr_classes x grid
     int bxdim, bydim, bzdim, binity, binitz, br_max, bpad;
+    // do_scale_correction: nr_classes x (ori_size/2+1) data_vs_prior_class, or nullptr (off)
+    const double* data_vs_prior;
 };
 
 struct OrcParticle {
@@ -266,6 +268,8 @@ struct OrcResult {
     double wsum_norm;
     double sumw;
     double wsum_sigma2_offset;
+    double wsum_scale_xa;    // exp_wsum_scale_correction_XA / scale_correction
+    double wsum_scale_aa;    // exp_wsum_scale_correction_AA / scale_correction^2
 };
 
 double orc_ctf_value(const double* params, double X, double Y)
@@ -325,6 +329,70 @@ static double diff2_one(const OrcSetup* S, const OrcParticle* pt, const double* 
     return d;
 }
 
+// The same sum as diff2_one with its per-hypothesis factors hoisted: `rc` the
+// reference times CTF and scale (per orientation), `sx` the shifted image (per
+// translation), `nz` the pixels whose Minvsigma2 is non-zero (the others add an
+// exact 0).  Every term is the same double expression, in the same order, so
+// the result equals diff2_one's bit for bit.
+static double diff2_pre(const OrcParticle* pt, const double* rc, const double* sx, const std::vector<int>& nz)
+{
+    double d = pt->highres_xi2 / 2.;
+    for (const int n : nz) {
+        const double dr = rc[2 * n] - sx[2 * n], di = rc[2 * n + 1] - sx[2 * n + 1];
+        d += (dr * dr + di * di) * 0.5 * pt->minvsigma2[n];
+    }
+    return d;
+}
+
+static std::vector<int> nonzero_pixels(const OrcSetup* S, const OrcParticle* pt)
+{
+    const int P = S->s * (S->s / 2 + 1);
+    std::vector<int> nz;
+    for (int n = 0; n < P; n++)
+        if (pt->minvsigma2[n] != 0.f) nz.push_back(n);
+    return nz;
+}
+
+// Shifted images of `nt` shifts (src/ml_optimiser.cpp:7205-7245): nt x 2P.
+static void shifted_images(const OrcSetup* S, const OrcParticle* pt, const double* shifts, int nt,
+                           std::vector<double>& out)
+{
+    const int P = S->s * (S->s / 2 + 1);
+    std::vector<double> ab((size_t)2 * P);
+    out.resize((size_t)2 * P * nt);
+    for (int t = 0; t < nt; t++) {
+        shift_table(S->s, S->ori_size, shifts[2 * t], shifts[2 * t + 1], ab.data());
+        double* o = &out[(size_t)2 * P * t];
+        for (int n = 0; n < P; n++) {
+            const double xr = pt->fimg[2 * n], xi = pt->fimg[2 * n + 1];
+            o[2 * n] = ab[2 * n] * xr - ab[2 * n + 1] * xi;
+            o[2 * n + 1] = ab[2 * n] * xi + ab[2 * n + 1] * xr;
+        }
+    }
+}
+
+// Frefctf = Fref * CTF * scale (src/ml_optimiser.cpp:7113-7140).
+static void ref_ctf(const OrcSetup* S, const OrcParticle* pt, const double* fref, double* out)
+{
+    const int P = S->s * (S->s / 2 + 1);
+    for (int n = 0; n < P; n++) {
+        const double c = pt->ctf[n] * pt->scale;
+        out[2 * n] = fref[2 * n] * c;
+        out[2 * n + 1] = fref[2 * n + 1] * c;
+    }
+}
+
+// diff2 of one hypothesis in the reference's literal per-pixel form (the check of
+// diff2_pre's hoisting): class iclass, Euler matrix A, shift (sx, sy) in pixels.
+double orc_diff2_literal(const OrcSetup* S, const OrcParticle* pt, int iclass, const double* A, double sx, double sy)
+{
+    const int P = S->s * (S->s / 2 + 1);
+    std::vector<double> fref((size_t)2 * P), ab((size_t)2 * P);
+    project(S, iclass, A, fref.data());
+    shift_table(S->s, S->ori_size, sx, sy, ab.data());
+    return diff2_one(S, pt, fref.data(), ab.data());
+}
+
 // Coarse pass diff2 over every (class, orientation, translation):
 // out[(iclass*O + iorient)*T + itrans]; -999 where the orientation is skipped.
 // Returns the minimum (src/ml_optimiser.cpp:6922-7300, exp_ipass == 0).
@@ -332,9 +400,9 @@ double orc_coarse_diff2(const OrcSetup* S, const OrcParticle* pt, double* out)
 {
     const int P = S->s * (S->s / 2 + 1);
     const int O = S->n_dir * S->n_psi, T = S->n_trans;
-    std::vector<double> fref(2 * P), ab((size_t)2 * P * T);
-    for (int t = 0; t < T; t++)
-        shift_table(S->s, S->ori_size, S->trans_px[2 * t], S->trans_px[2 * t + 1], &ab[(size_t)2 * P * t]);
+    std::vector<double> fref(2 * P), rc(2 * P), sx;
+    shifted_images(S, pt, S->trans_px, T, sx);
+    const std::vector<int> nz = nonzero_pixels(S, pt);
     double mn = 1e300;
     for (int k = 0; k < S->nr_classes; k++) {
         for (int o = 0; o < O; o++) {
@@ -345,8 +413,9 @@ double orc_coarse_diff2(const OrcSetup* S, const OrcParticle* pt, double* out)
                 continue;
             }
             project(S, k, S->eul_coarse + 9 * o, fref.data());
+            ref_ctf(S, pt, fref.data(), rc.data());
             for (int t = 0; t < T; t++) {
-                dst[t] = diff2_one(S, pt, fref.data(), &ab[(size_t)2 * P * t]);
+                dst[t] = diff2_pre(pt, rc.data(), &sx[(size_t)2 * P * t], nz);
                 mn = std::min(mn, dst[t]);
             }
         }
@@ -462,9 +531,9 @@ long long orc_fine_diff2(const OrcSetup* S, const OrcParticle* pt, const unsigne
     const int P = S->s * (S->s / 2 + 1);
     const int O = S->n_dir * S->n_psi, T = S->n_trans;
     const int R = S->nover_rot, V = S->nover_trans;
-    std::vector<double> fref((size_t)2 * P * R), ab((size_t)2 * P * T * V);
-    for (int t = 0; t < T * V; t++)
-        shift_table(S->s, S->ori_size, S->trans_px_fine[2 * t], S->trans_px_fine[2 * t + 1], &ab[(size_t)2 * P * t]);
+    std::vector<double> fref((size_t)2 * P), rc((size_t)2 * P * R), sx;
+    shifted_images(S, pt, S->trans_px_fine, T * V, sx);
+    const std::vector<int> nz = nonzero_pixels(S, pt);
     long long np = 0;
     double mn = 1e300;
     for (int k = 0; k < S->nr_classes; k++)
@@ -473,14 +542,16 @@ long long orc_fine_diff2(const OrcSetup* S, const OrcParticle* pt, const unsigne
             bool any = false;
             for (int t = 0; t < T; t++) any |= mask[base + t] != 0;
             if (!any) continue;
-            for (int r = 0; r < R; r++)
-                project(S, k, S->eul_fine + 9 * ((size_t)o * R + r), &fref[(size_t)2 * P * r]);
+            for (int r = 0; r < R; r++) {
+                project(S, k, S->eul_fine + 9 * ((size_t)o * R + r), fref.data());
+                ref_ctf(S, pt, fref.data(), &rc[(size_t)2 * P * r]);
+            }
             for (int t = 0; t < T; t++) {
                 if (!mask[base + t]) continue;
                 pairs[np] = base + t;
                 for (int r = 0; r < R; r++)
                     for (int v = 0; v < V; v++) {
-                        const double d = diff2_one(S, pt, &fref[(size_t)2 * P * r], &ab[(size_t)2 * P * (t * V + v)]);
+                        const double d = diff2_pre(pt, &rc[(size_t)2 * P * r], &sx[(size_t)2 * P * (t * V + v)], nz);
                         out[np * R * V + r * V + v] = d;
                         mn = std::min(mn, d);
                     }
@@ -589,6 +660,99 @@ void orc_backproject(const OrcSetup* S, int iclass, const double* A, const doubl
     else backproject2d(S, iclass, A, fimg, fweight);
 }
 
+// Weighted sums and backprojection of one particle's final-pass hypotheses
+// (src/ml_optimiser.cpp:8153-8700, storeWeightedSums): `pairs` are the
+// significant coarse pairs (coarse hidden index, ascending), `wf` their
+// npairs x R x V final weights (R = V = 1 without adaptive oversampling),
+// `fsum` / `fsig` the final sum of weights and significance threshold.
+static void wsum_stage(const OrcSetup* S, const OrcParticle* pt, const long long* pairs, long long npairs,
+                       const double* wf, double fsum, double fsig, OrcResult* res, double* wsum_sigma2,
+                       double* wsum_pdf_class, double* wsum_pdf_dir)
+{
+    const int P = S->s * (S->s / 2 + 1);
+    const int O = S->n_dir * S->n_psi, T = S->n_trans;
+    const int R = S->adaptive_oversampling ? S->nover_rot : 1;
+    const int V = S->adaptive_oversampling ? S->nover_trans : 1;
+    // ---- weighted sums (src/ml_optimiser.cpp:8153-8700), pairs grouped by orientation
+    std::vector<double> fref((size_t)2 * P), fimg((size_t)2 * P), fw(P), ab((size_t)2 * P);
+    const int half = S->ori_size / 2 + 1;
+    res->pmax = -1.;
+    res->wsum_norm = 0.; res->sumw = 0.; res->wsum_sigma2_offset = 0.;
+    res->wsum_scale_xa = 0.; res->wsum_scale_aa = 0.;
+    long long a = 0;
+    while (a < npairs) {
+        const long long ioc = pairs[a] / T;
+        long long b = a;
+        while (b < npairs && pairs[b] / T == ioc) b++;
+        const int k = (int)(ioc / O), o = (int)(ioc % O);
+        const int idir = o / S->n_psi;
+        for (int r = 0; r < R; r++) {
+            const double* A = S->adaptive_oversampling ? S->eul_fine + 9 * ((size_t)o * R + r) : S->eul_coarse + 9 * (size_t)o;
+            project(S, k, A, fref.data());
+            std::fill(fimg.begin(), fimg.end(), 0.);
+            std::fill(fw.begin(), fw.end(), 0.);
+            bool any = false;
+            for (long long q = a; q < b; q++) {
+                const int t = (int)(pairs[q] % T);
+                for (int v = 0; v < V; v++) {
+                    double weight = wf[(size_t)q * R * V + r * V + v];
+                    if (!(weight >= fsig)) continue;
+                    weight /= fsum;
+                    any = true;
+                    const double* sh = S->adaptive_oversampling ? &S->trans_px_fine[2 * (t * V + v)] : &S->trans_px[2 * t];
+                    shift_table(S->s, S->ori_size, sh[0], sh[1], ab.data());
+                    for (int n = 0; n < P; n++) {
+                        const double c = pt->ctf[n] * pt->scale;
+                        const double rr = fref[2 * n] * c, ri = fref[2 * n + 1] * c;
+                        const double xr = pt->fimg[2 * n], xi = pt->fimg[2 * n + 1];
+                        const double sr = ab[2 * n] * xr - ab[2 * n + 1] * xi;
+                        const double si = ab[2 * n] * xi + ab[2 * n + 1] * xr;
+                        const int ires = pt->mresol[n];
+                        if (ires > -1) {
+                            const double dr = rr - sr, di = ri - si;
+                            const double wd = weight * (dr * dr + di * di);
+                            wsum_sigma2[ires] += wd;
+                            res->wsum_norm += wd;
+                            // scale correction (src/ml_optimiser.cpp:8477-8486)
+                            if (S->data_vs_prior && S->data_vs_prior[(size_t)k * half + ires] > 3.) {
+                                res->wsum_scale_xa += weight * (rr * sr + ri * si);
+                                res->wsum_scale_aa += weight * (rr * rr + ri * ri);
+                            }
+                        }
+                        const double ur = pt->fimg_nomask[2 * n], ui = pt->fimg_nomask[2 * n + 1];
+                        const double nr = ab[2 * n] * ur - ab[2 * n + 1] * ui;
+                        const double ni = ab[2 * n] * ui + ab[2 * n + 1] * ur;
+                        const double minv = (n == 0) ? pt->minvsigma2_dc : pt->minvsigma2[n];
+                        const double wx = weight * c * minv;
+                        fimg[2 * n] += nr * wx;
+                        fimg[2 * n + 1] += ni * wx;
+                        fw[n] += wx * c;
+                    }
+                    res->sumw += weight;
+                    wsum_pdf_class[k] += weight;
+                    const double dx = pt->prior[0] - pt->old_offset[0] - sh[0];
+                    const double dy = pt->prior[1] - pt->old_offset[1] - sh[1];
+                    res->wsum_sigma2_offset += weight * S->pixel_size * S->pixel_size * (dx * dx + dy * dy);
+                    wsum_pdf_dir[(size_t)k * S->n_dir + idir] += weight;
+                    if (weight > res->pmax) {
+                        res->pmax = weight;
+                        res->pose[0] = k; res->pose[1] = o; res->pose[2] = r; res->pose[3] = t; res->pose[4] = v;
+                    }
+                }
+            }
+            if (any) {
+                std::lock_guard<std::mutex> lock(g_bp_mutex);
+                orc_backproject(S, k, A, fimg.data(), fw.data());
+            }
+        }
+        a = b;
+    }
+    // divided by scale_correction and its square: the scale entered Frefctf through the CTF
+    // (src/ml_optimiser.cpp:8856-8861)
+    res->wsum_scale_xa /= pt->scale;
+    res->wsum_scale_aa /= pt->scale * pt->scale;
+}
+
 // Full E-step of one particle: coarse pass, weights, optional fine pass,
 // weights, weighted sums and backprojection (src/ml_optimiser.cpp:4418-4560
 // expectationOneParticle, single image, no bodies / helix / CC).
@@ -644,77 +808,18 @@ int orc_estep_particle(const OrcSetup* S, const OrcParticle* pt, OrcResult* res,
     res->sum_weight = fsum;
     res->sig_weight = fsig;
 
-    // ---- weighted sums (src/ml_optimiser.cpp:8153-8700), pairs grouped by orientation
-    std::vector<double> fref((size_t)2 * P), fimg((size_t)2 * P), fw(P), ab((size_t)2 * P);
-    const int half = S->ori_size / 2 + 1;
-    res->pmax = -1.;
-    res->wsum_norm = 0.; res->sumw = 0.; res->wsum_sigma2_offset = 0.;
-    long long a = 0;
-    const long long npairs = (long long)pairs.size();
-    while (a < npairs) {
-        const long long ioc = pairs[a] / T;
-        long long b = a;
-        while (b < npairs && pairs[b] / T == ioc) b++;
-        const int k = (int)(ioc / O), o = (int)(ioc % O);
-        const int idir = o / S->n_psi;
-        for (int r = 0; r < R; r++) {
-            const double* A = S->adaptive_oversampling ? S->eul_fine + 9 * ((size_t)o * R + r) : S->eul_coarse + 9 * (size_t)o;
-            project(S, k, A, fref.data());
-            std::fill(fimg.begin(), fimg.end(), 0.);
-            std::fill(fw.begin(), fw.end(), 0.);
-            bool any = false;
-            for (long long q = a; q < b; q++) {
-                const int t = (int)(pairs[q] % T);
-                for (int v = 0; v < V; v++) {
-                    double weight = wf[(size_t)q * R * V + r * V + v];
-                    if (!(weight >= fsig)) continue;
-                    weight /= fsum;
-                    any = true;
-                    const double* sh = S->adaptive_oversampling ? &S->trans_px_fine[2 * (t * V + v)] : &S->trans_px[2 * t];
-                    shift_table(S->s, S->ori_size, sh[0], sh[1], ab.data());
-                    for (int n = 0; n < P; n++) {
-                        const double c = pt->ctf[n] * pt->scale;
-                        const double rr = fref[2 * n] * c, ri = fref[2 * n + 1] * c;
-                        const double xr = pt->fimg[2 * n], xi = pt->fimg[2 * n + 1];
-                        const double sr = ab[2 * n] * xr - ab[2 * n + 1] * xi;
-                        const double si = ab[2 * n] * xi + ab[2 * n + 1] * xr;
-                        const int ires = pt->mresol[n];
-                        if (ires > -1) {
-                            const double dr = rr - sr, di = ri - si;
-                            const double wd = weight * (dr * dr + di * di);
-                            wsum_sigma2[ires] += wd;
-                            res->wsum_norm += wd;
-                        }
-                        const double ur = pt->fimg_nomask[2 * n], ui = pt->fimg_nomask[2 * n + 1];
-                        const double nr = ab[2 * n] * ur - ab[2 * n + 1] * ui;
-                        const double ni = ab[2 * n] * ui + ab[2 * n + 1] * ur;
-                        const double minv = (n == 0) ? pt->minvsigma2_dc : pt->minvsigma2[n];
-                        const double wx = weight * c * minv;
-                        fimg[2 * n] += nr * wx;
-                        fimg[2 * n + 1] += ni * wx;
-                        fw[n] += wx * c;
-                    }
-                    res->sumw += weight;
-                    wsum_pdf_class[k] += weight;
-                    const double dx = pt->prior[0] - pt->old_offset[0] - sh[0];
-                    const double dy = pt->prior[1] - pt->old_offset[1] - sh[1];
-                    res->wsum_sigma2_offset += weight * S->pixel_size * S->pixel_size * (dx * dx + dy * dy);
-                    wsum_pdf_dir[(size_t)k * S->n_dir + idir] += weight;
-                    if (weight > res->pmax) {
-                        res->pmax = weight;
-                        res->pose[0] = k; res->pose[1] = o; res->pose[2] = r; res->pose[3] = t; res->pose[4] = v;
-                    }
-                }
-            }
-            if (any) {
-                std::lock_guard<std::mutex> lock(g_bp_mutex);
-                orc_backproject(S, k, A, fimg.data(), fw.data());
-            }
-        }
-        a = b;
-    }
-    (void)half;
+    wsum_stage(S, pt, pairs.data(), (long long)pairs.size(), wf.data(), fsum, fsig, res, wsum_sigma2,
+               wsum_pdf_class, wsum_pdf_dir);
     return 0;
+}
+
+// The weighted-sums stage alone on caller-supplied final weights (same-input
+// checks of the device stage).  Grids accumulate into S->bp_data / bp_weight.
+void orc_wsum_bp(const OrcSetup* S, const OrcParticle* pt, const long long* pairs, long long npairs,
+                 const double* wf, double fsum, double fsig, OrcResult* res, double* wsum_sigma2,
+                 double* wsum_pdf_class, double* wsum_pdf_dir)
+{
+    wsum_stage(S, pt, pairs, npairs, wf, fsum, fsig, res, wsum_sigma2, wsum_pdf_class, wsum_pdf_dir);
 }
 
 // Batch driver: particles spread over `nthreads` host threads (dynamic

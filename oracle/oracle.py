@@ -42,7 +42,8 @@ class Setup(ctypes.Structure):
                           "pdf_direction", "pdf_class")] + [
         ("sigma2_offset", ctypes.c_double), ("pixel_size", ctypes.c_double),
         ("adaptive_fraction", ctypes.c_double), ("bp_data", _p), ("bp_weight", _p)] + [
-        (n, ctypes.c_int) for n in ("bxdim", "bydim", "bzdim", "binity", "binitz", "br_max", "bpad")]
+        (n, ctypes.c_int) for n in ("bxdim", "bydim", "bzdim", "binity", "binitz", "br_max", "bpad")] + [
+        ("data_vs_prior", _p)]
 
 
 class Particle(ctypes.Structure):
@@ -58,7 +59,8 @@ class Result(ctypes.Structure):
                 ("coarse_sum_weight", ctypes.c_double), ("coarse_sig_weight", ctypes.c_double),
                 ("nr_sign", ctypes.c_longlong), ("n_coarse_sig", ctypes.c_longlong),
                 ("pmax", ctypes.c_double), ("pose", ctypes.c_int * 5), ("wsum_norm", ctypes.c_double),
-                ("sumw", ctypes.c_double), ("wsum_sigma2_offset", ctypes.c_double)]
+                ("sumw", ctypes.c_double), ("wsum_sigma2_offset", ctypes.c_double),
+                ("wsum_scale_xa", ctypes.c_double), ("wsum_scale_aa", ctypes.c_double)]
 
 
 L.orc_ctf_value.restype = ctypes.c_double
@@ -73,6 +75,11 @@ L.orc_fine_diff2.restype = ctypes.c_longlong
 L.orc_fine_diff2.argtypes = [ctypes.POINTER(Setup), ctypes.POINTER(Particle), _p, _p, _p, _p]
 L.orc_estep.argtypes = [ctypes.POINTER(Setup), ctypes.POINTER(Particle), ctypes.c_int,
                         ctypes.POINTER(Result), _p, _p, _p, ctypes.c_int]
+L.orc_wsum_bp.argtypes = [ctypes.POINTER(Setup), ctypes.POINTER(Particle), _p, ctypes.c_longlong, _p,
+                          ctypes.c_double, ctypes.c_double, ctypes.POINTER(Result), _p, _p, _p]
+L.orc_diff2_literal.restype = ctypes.c_double
+L.orc_diff2_literal.argtypes = [ctypes.POINTER(Setup), ctypes.POINTER(Particle), ctypes.c_int, _p,
+                                ctypes.c_double, ctypes.c_double]
 L.orc_reconstruct_divide.argtypes = [_p, _p] + [ctypes.c_int] * 7 + [_p]
 L.orc_healpix_nest_pix2zphi.argtypes = [ctypes.c_int, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_double)]
@@ -104,7 +111,8 @@ class Problem:
     """Holds the numpy arrays an OrcSetup points to (keeps them alive)."""
 
     def __init__(self, *, ori_size, s, ref_dim, maps, r_max, pad, samp, pdf_direction, pdf_class,
-                 sigma2_offset, pixel_size, adaptive_fraction, ovs, bp_pad_size, bp_r_max, maximum_significants=-1):
+                 sigma2_offset, pixel_size, adaptive_fraction, ovs, bp_pad_size, bp_r_max, maximum_significants=-1,
+                 data_vs_prior=None):
         self.maps = np.ascontiguousarray(np.stack(maps), np.complex64)
         self.eul_coarse = np.ascontiguousarray(samp["eul_coarse"], np.float64)
         self.eul_fine = np.ascontiguousarray(samp["eul_fine"], np.float64)
@@ -145,6 +153,8 @@ class Problem:
         S.bxdim, S.bydim, S.bzdim = bp_pad_size // 2 + 1, bp_pad_size, bz
         S.binity, S.binitz = -(bp_pad_size // 2), (-(bp_pad_size // 2) if ref_dim == 3 else 0)
         S.br_max, S.bpad = bp_r_max, pad
+        self.data_vs_prior = None if data_vs_prior is None else np.ascontiguousarray(data_vs_prior, np.float64)
+        S.data_vs_prior = _ptr(self.data_vs_prior)
         self.S = S
         self.half = ori_size // 2 + 1
         self.K, self.n_dir = K, samp["n_dir"]
@@ -218,6 +228,31 @@ class Problem:
         out["pose"] = np.array([list(r.pose) for r in res])
         out.update(wsum_sigma2=sig, wsum_pdf_class=pc, wsum_pdf_dir=pd, fails=fails)
         return out
+
+    def wsum_bp(self, parts, b, pairs, wf, fsum, fsig):
+        """Weighted sums + backprojection of particle b on given final weights (the oracle's
+        stage on the same input as the device's); grids accumulate into this Problem's."""
+        pr = np.ascontiguousarray(pairs, np.int64)
+        w = np.ascontiguousarray(wf, np.float64)
+        res = Result()
+        sig = np.zeros(self.half)
+        pc = np.zeros(self.K)
+        pd = np.zeros(self.K * self.n_dir)
+        L.orc_wsum_bp(ctypes.byref(self.S), ctypes.byref(parts[b]), _ptr(pr), pr.size, _ptr(w), fsum, fsig,
+                      ctypes.byref(res), _ptr(sig), _ptr(pc), _ptr(pd))
+        out = {k: getattr(res, k) for k, _ in Result._fields_ if k != "pose"}
+        out["pose"] = np.array(list(res.pose))
+        out.update(wsum_sigma2=sig, wsum_pdf_class=pc, wsum_pdf_dir=pd)
+        return out
+
+    def diff2_literal(self, parts, b, iclass, A, shift):
+        a = np.ascontiguousarray(A, np.float64).reshape(9)
+        return L.orc_diff2_literal(ctypes.byref(self.S), ctypes.byref(parts[b]), iclass, _ptr(a),
+                                   float(shift[0]), float(shift[1]))
+
+    def clear_grids(self):
+        self.bp_data[...] = 0
+        self.bp_weight[...] = 0
 
     def grids(self):
         return self.bp_data[..., 0] + 1j * self.bp_data[..., 1], self.bp_weight

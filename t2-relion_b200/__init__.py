@@ -36,7 +36,8 @@ ABI_SYMBOLS = (
     "t2b_backprojector_get", "t2b_backprojector_device_ptrs", "t2b_configure",
     "t2b_estep_batch_host", "t2b_estep_batch_device", "t2b_estep_submit_host", "t2b_estep_wait",
     "t2b_reconstruct_divide",
-    "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_debug_proposals", "t2b_last_stage_ms",
+    "t2b_project", "t2b_debug_coarse_diff2", "t2b_debug_fine", "t2b_debug_weights", "t2b_debug_selection",
+    "t2b_debug_proposals", "t2b_last_stage_ms",
     "t2b_sampling", "t2b_reconstruct_divide_noalloc", "t2b_last_launch_count",
     "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
@@ -78,6 +79,7 @@ class Config(ctypes.Structure):
         ("trans_prior", _p), ("pdf_direction", _p), ("pdf_class", _p), ("mresol", _p),
         ("sigma2_offset", ctypes.c_double), ("pixel_size", ctypes.c_double),
         ("adaptive_fraction", ctypes.c_double), ("fine_capacity", ctypes.c_size_t),
+        ("data_vs_prior", _p),
     ]
 
 
@@ -90,7 +92,8 @@ class Result(ctypes.Structure):
     _fields_ = [(name, _p) for name in (
         "min_diff2", "sum_weight", "sig_weight", "coarse_sum_weight", "coarse_sig_weight",
         "nr_sign", "n_coarse_sig", "pmax", "pose", "wsum_norm", "sumw", "wsum_sigma2_offset",
-        "wsum_sigma2", "wsum_pdf_class", "wsum_pdf_dir", "status", "audit_mass", "learned")]
+        "wsum_sigma2", "wsum_pdf_class", "wsum_pdf_dir", "status", "audit_mass", "learned",
+        "wsum_scale_xa", "wsum_scale_aa")]
 
 
 class ProposalTrainConfig(ctypes.Structure):
@@ -179,6 +182,8 @@ def _setup_prototypes():
     lib.t2b_debug_coarse_diff2.argtypes = [v, i, v]
     lib.t2b_debug_fine.argtypes = [v, i, v, v, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.t2b_debug_proposals.argtypes = [v, i, v, v, ctypes.POINTER(ctypes.c_int)]
+    lib.t2b_debug_weights.argtypes = [v, i, v, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+    lib.t2b_debug_selection.argtypes = [v, i, ctypes.POINTER(i), ctypes.POINTER(i)]
     lib.t2b_last_stage_ms.argtypes = [v, v, i]
     lib.t2b_last_launch_count.argtypes = [v, ctypes.POINTER(i)]
     lib.t2b_stage_timing.argtypes = [v, i]
@@ -433,7 +438,7 @@ class EStep:
     def configure(self, *, ori_size, current_size, ref_dim, nr_classes, samp, pdf_direction,
                   pdf_class, sigma2_offset, pixel_size, adaptive_fraction=0.999,
                   adaptive_oversampling=0, diff2_mode=DIFF2_PLAIN_FP32, max_batch=64,
-                  fine_capacity=0, maximum_significants=-1, use_graph=1):
+                  fine_capacity=0, maximum_significants=-1, use_graph=1, data_vs_prior=None):
         arrays = dict(
             eul_coarse=np.ascontiguousarray(samp["eul_coarse"], np.float64),
             eul_fine=np.ascontiguousarray(samp["eul_fine"], np.float64),
@@ -443,6 +448,9 @@ class EStep:
             pdf_direction=np.ascontiguousarray(pdf_direction, np.float64),
             pdf_class=np.ascontiguousarray(pdf_class, np.float64),
             mresol=mresol_map(current_size))
+        if data_vs_prior is not None:
+            arrays["data_vs_prior"] = np.ascontiguousarray(data_vs_prior, np.float64).reshape(
+                nr_classes, ori_size // 2 + 1)
         c = Config()
         c.ori_size, c.current_size, c.ref_dim = ori_size, current_size, ref_dim
         c.nr_classes, c.n_dir, c.n_psi, c.n_trans = nr_classes, samp["n_dir"], samp["n_psi"], samp["n_trans"]
@@ -473,7 +481,8 @@ class EStep:
             pose=np.zeros((n, 5), np.int32), wsum_norm=np.zeros(n), sumw=np.zeros(n),
             wsum_sigma2_offset=np.zeros(n), wsum_sigma2=np.zeros((n, half)),
             wsum_pdf_class=np.zeros((n, K)), wsum_pdf_dir=np.zeros((n, K * nd)),
-            status=np.zeros(n, np.int32), audit_mass=np.zeros(n), learned=np.zeros(n, np.int32))
+            status=np.zeros(n, np.int32), audit_mass=np.zeros(n), learned=np.zeros(n, np.int32),
+            wsum_scale_xa=np.zeros(n), wsum_scale_aa=np.zeros(n))
 
     # MlOptimiserCuda::doThreadExpectationSomeParticles for one batch (host buffers)
     def expectation(self, fimg, ctf, minvsigma2, scalars, fimg_nomask=None):
@@ -708,6 +717,22 @@ class EStep:
         d2 = np.zeros((max(m, 1), cfg["R"] * cfg["V"]), np.float32)
         _check(lib.t2b_debug_fine(self._h, b, _ptr(pairs), _ptr(d2), m, ctypes.byref(cnt)))
         return pairs[:m], d2[:m]
+
+    def weights(self, b, cap=1 << 24):
+        """Final-pass FP64 weights of particle b in the last batch (pairs x R*V, or one per pair)."""
+        cnt = ctypes.c_longlong()
+        _check(lib.t2b_debug_weights(self._h, b, None, 0, ctypes.byref(cnt)))
+        m = min(cnt.value, cap)
+        out = np.zeros(max(m, 1))
+        _check(lib.t2b_debug_weights(self._h, b, _ptr(out), m, ctypes.byref(cnt)))
+        return out[:m]
+
+    def selection_path(self, b):
+        """(coarse, fine) significance search of particle b: 2 one-CTA, 1 multi-kernel with the
+        fast gather, 0 multi-kernel radix levels; fine is -1 without oversampling."""
+        c, f = ctypes.c_int(), ctypes.c_int()
+        _check(lib.t2b_debug_selection(self._h, b, ctypes.byref(c), ctypes.byref(f)))
+        return c.value, f.value
 
     def reconstruct_divide(self, iclass):
         zdim, ydim, xdim = self._grid_shape

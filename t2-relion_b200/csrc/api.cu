@@ -313,6 +313,14 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             tb.pdf_oc = (const double*)up(poc.data(), poc.size() * sizeof(double));
         }
         tb.skip = (const unsigned char*)up(skip.data(), skip.size());
+        if (f.data_vs_prior) {
+            // do_scale_correction: rings of each class whose data_vs_prior exceeds 3 enter the
+            // XA / AA sums (src/ml_optimiser.cpp:8477)
+            const int half = f.ori_size / 2 + 1;
+            std::vector<unsigned char> ring((size_t)K * half);
+            for (size_t i = 0; i < ring.size(); i++) ring[i] = f.data_vs_prior[i] > 3. ? 1 : 0;
+            tb.scl_ring = (const unsigned char*)up(ring.data(), ring.size());
+        }
         tb.mresol = (const int*)up(f.mresol, (size_t)P * sizeof(int));
         {
             // pixels inside the largest projection radius of all classes
@@ -432,6 +440,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         w.r_sigma2 = dalloc<double>(c, (size_t)B * (f.ori_size / 2 + 1));
         w.r_pdf_class = dalloc<double>(c, (size_t)B * K);
         w.r_pdf_dir = dalloc<double>(c, (size_t)B * K * f.n_dir);
+        w.r_xa = dalloc<double>(c, B); w.r_aa = dalloc<double>(c, B);
         // results of the two host slots: slot 0 the workspace's, slot 1 a second set
         for (int i = 0; i < 2; i++) {
             t2b_ctx::InSlot& s = c->in[i];
@@ -454,6 +463,8 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             s.status = own ? w.status : dalloc<int>(c, B);
             s.r_learned = own ? w.r_learned : dalloc<int>(c, B);
             s.r_audit = own ? w.r_audit : dalloc<double>(c, B);
+            s.r_xa = own ? w.r_xa : dalloc<double>(c, B);
+            s.r_aa = own ? w.r_aa : dalloc<double>(c, B);
         }
         // grid pointer tables
         float2** gd = dalloc<float2*>(c, K);
@@ -630,7 +641,7 @@ static long long submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r
     w.r_pmax = in.r_pmax; w.r_nsign = in.r_nsign; w.r_ncsig = in.r_ncsig; w.r_pose = in.r_pose;
     w.r_norm = in.r_norm; w.r_sumw = in.r_sumw; w.r_sig_off = in.r_sig_off; w.r_sigma2 = in.r_sigma2;
     w.r_pdf_class = in.r_pdf_class; w.r_pdf_dir = in.r_pdf_dir; w.status = in.status;
-    w.r_learned = in.r_learned; w.r_audit = in.r_audit;
+    w.r_learned = in.r_learned; w.r_audit = in.r_audit; w.r_xa = in.r_xa; w.r_aa = in.r_aa;
     T2B_CUDA(cudaStreamWaitEvent(cs, in.consumed, 0));
     T2B_CUDA(cudaMemcpyAsync(in.fimg, b->fimg, (size_t)n * P * sizeof(float2), cudaMemcpyHostToDevice, cs));
     if (b->fimg_nomask)
@@ -675,6 +686,8 @@ static long long submit_host(t2b_ctx* c, const t2b_batch* b, const t2b_result* r
     d2h(r->status, w.status, n * sizeof(int));
     d2h(r->learned, w.r_learned, n * sizeof(int));
     d2h(r->audit_mass, w.r_audit, n * sizeof(double));
+    d2h(r->wsum_scale_xa, w.r_xa, n * sizeof(double));
+    d2h(r->wsum_scale_aa, w.r_aa, n * sizeof(double));
     T2B_CUDA(cudaEventRecord(in.done, ds));
     c->last_n = n;
     return c->submitted++;
@@ -770,6 +783,8 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
         w.status = r->status;
         w.r_learned = r->learned;
         w.r_audit = r->audit_mass;
+        w.r_xa = r->wsum_scale_xa;
+        w.r_aa = r->wsum_scale_aa;
         if (c->cfg.use_graph) {
             const std::vector<const void*> key = {(const void*)(intptr_t)b->n, b->fimg, b->fimg_nomask, b->ctf,
                                                   b->minvsigma2, b->scalars, r->min_diff2, r->sum_weight, r->sig_weight,
@@ -777,7 +792,7 @@ int t2b_estep_batch_device(t2b_ctx* c, const t2b_batch* b, const t2b_result* r, 
                                                   r->n_coarse_sig, r->pmax, r->pose, r->wsum_norm, r->sumw,
                                                   r->wsum_sigma2_offset, r->wsum_sigma2, r->wsum_pdf_class,
                                                   r->wsum_pdf_dir, r->status, r->learned, r->audit_mass,
-                                                  (const void*)st,
+                                                  r->wsum_scale_xa, r->wsum_scale_aa, (const void*)st,
                                                   (const void*)(intptr_t)(c->net && c->net->enabled ? c->net->kprop : 0)};
             c->last_kernels = replay_graph(c, w, st, key, c->g_dev);
         } else {
@@ -1031,6 +1046,39 @@ int t2b_debug_fine(t2b_ctx* c, int b, long long* pairs, float* diff2, long long 
             T2B_CUDA(cudaMemcpy(pairs, c->wk.pairs + off[0], m * sizeof(long long), cudaMemcpyDeviceToHost));
         if (diff2 && m > 0 && c->tb.ovs)
             T2B_CUDA(cudaMemcpy(diff2, c->wk.d2f + off[0] * rv, (size_t)m * rv * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+int t2b_debug_weights(t2b_ctx* c, int b, double* weights, long long cap, long long* count)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && count && c->configured && b >= 0 && b < c->last_n, T2B_ERR_ARG, "bad particle index");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        long long off[2];
+        T2B_CUDA(cudaMemcpy(off, c->wk.pair_off + b, 2 * sizeof(long long), cudaMemcpyDeviceToHost));
+        const long long rv = c->tb.ovs ? (long long)c->tb.R * c->tb.V : 1;
+        const long long nv = (off[1] - off[0]) * rv;
+        *count = nv;
+        const long long m = std::min(nv, cap);
+        if (weights && m > 0)
+            T2B_CUDA(cudaMemcpy(weights, c->wk.wf + off[0] * rv, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int t2b_debug_selection(t2b_ctx* c, int b, int* coarse_path, int* fine_path)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c && c->configured && b >= 0 && b < c->last_n, T2B_ERR_ARG, "bad particle index");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
+        SelState sc, sf;
+        T2B_CUDA(cudaMemcpy(&sc, c->wk.sel_c + b, sizeof(SelState), cudaMemcpyDeviceToHost));
+        T2B_CUDA(cudaMemcpy(&sf, c->wk.sel_f + b, sizeof(SelState), cudaMemcpyDeviceToHost));
+        if (coarse_path) *coarse_path = sc.fast;
+        if (fine_path) *fine_path = c->tb.ovs ? sf.fast : -1;
     });
 }
 

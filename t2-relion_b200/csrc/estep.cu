@@ -86,6 +86,8 @@ __global__ void k_prep(Tables tb, Work w)
         w.sel_c[b] = z;
         w.sel_f[b] = z;
         w.r_norm[b] = 0.; w.r_sumw[b] = 0.; w.r_sig_off[b] = 0.;
+        if (w.r_xa) w.r_xa[b] = 0.;
+        if (w.r_aa) w.r_aa[b] = 0.;
     }
     const int half = tb.ori_size / 2 + 1;
     for (int i = threadIdx.x; i < half; i += blockDim.x) w.r_sigma2[(size_t)b * half + i] = 0.;
@@ -1422,6 +1424,8 @@ __global__ void k_group_starts(Tables tb, Work w)
     }
 }
 
+// SCL: with the scale-correction sums (a separate build: they cost the default path 16 registers)
+template <bool SCL>
 __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, GridPtrs gp)
 {
     __shared__ long long item;
@@ -1492,8 +1496,15 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                 __syncthreads();
                 const int ne = nent;
                 if (ne > 0) {
-                    double nacc = 0.;
+                    double nacc = 0., xacc = 0., aacc = 0.;
                     const float scale = (float)sc[6];
+                    // scale-correction sums (src/ml_optimiser.cpp:8477-8486; the GPU path's
+                    // per-pixel XA / AA of wavg.cuh:155-163): sum_e w'_e Re(A conj sX_e) and
+                    // |A|^2 sum_e w'_e over the rings of this class with data_vs_prior > 3
+                    const unsigned char* scl = SCL ? tb.scl_ring + (size_t)k * (tb.ori_size / 2 + 1) : nullptr;
+                    float wsum_e = 0.f;
+                    if (SCL)
+                        for (int e = 0; e < ne; e++) wsum_e += ent_w[e];
                     for (int n = threadIdx.x; n < P; n += blockDim.x) {
                         const float2 pv = proj[(size_t)tab * P + n];
                         const float c = w.ctf[(size_t)b * P + n] * scale;
@@ -1502,13 +1513,14 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                         const float2 Xn = w.fimg_nm[(size_t)b * P + n];
                         const float minv = n == 0 ? (float)sc[0] : w.minv[(size_t)b * P + n];
                         const int ires = tb.mresol[n];
-                        float fir = 0.f, fii = 0.f, fw = 0.f, wd = 0.f;
+                        float fir = 0.f, fii = 0.f, fw = 0.f, wd = 0.f, xa = 0.f;
                         for (int e = 0; e < ne; e++) {
                             const float wn = ent_w[e];
                             const float2 ab = abt[(size_t)ent_tv[e] * P + n];
                             const float sr = ab.x * X.x - ab.y * X.y, si = ab.x * X.y + ab.y * X.x;
                             const float dr = frr - sr, di = fri - si;
                             wd += wn * (dr * dr + di * di);
+                            if (SCL) xa += wn * (frr * sr + fri * si);
                             const float wx = wn * c * minv;
                             const float nr_ = ab.x * Xn.x - ab.y * Xn.y, ni = ab.x * Xn.y + ab.y * Xn.x;
                             fir += nr_ * wx;
@@ -1518,6 +1530,10 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                         if (ires > -1) {
                             atomicAdd(&ssig[ires], wd);
                             nacc += wd;
+                            if (SCL && scl[ires]) {
+                                xacc += xa;
+                                aacc += (frr * frr + fri * fri) * wsum_e;
+                            }
                         }
                         // backprojection of this pixel (src/backprojector.cpp:140-228)
                         if (fw > 0.f && !w.no_bp) {
@@ -1566,6 +1582,16 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                     }
                     nacc = block_sum(nacc, shr);
                     if (threadIdx.x == 0) atomicAdd(&w.r_norm[b], nacc);
+                    if (SCL) {
+                        // divided by scale_correction and its square (src/ml_optimiser.cpp:8859-8860):
+                        // the scale entered A through the CTF
+                        xacc = block_sum(xacc, shr);
+                        aacc = block_sum(aacc, shr);
+                        if (threadIdx.x == 0) {
+                            atomicAdd(&w.r_xa[b], xacc / sc[6]);
+                            atomicAdd(&w.r_aa[b], aacc / (sc[6] * sc[6]));
+                        }
+                    }
                 }
                 __syncthreads();
                 if (threadIdx.x == 0) nent = 0;
@@ -1890,7 +1916,11 @@ void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* co
 {
     GridPtrs gp{grid_data, grid_weight};
     k_group_starts<<<2 * sm_count(), 256, 0, st>>>(tb, w);
-    k_wsum_bp<<<(w.wsum_ctas > 0 ? w.wsum_ctas : 4) * sm_count(), 256, 0, st>>>(tb, w, g, gp);   // 64 registers: <= 4 CTAs per SM
+    const int ctas = (w.wsum_ctas > 0 ? w.wsum_ctas : 4) * sm_count();
+    if (tb.scl_ring && w.r_xa && w.r_aa)
+        k_wsum_bp<true><<<ctas, 256, 0, st>>>(tb, w, g, gp);    // 80 registers: <= 3 CTAs per SM
+    else
+        k_wsum_bp<false><<<ctas, 256, 0, st>>>(tb, w, g, gp);   // 64 registers: <= 4 CTAs per SM
     k_results<<<(w.n + 127) / 128, 128, 0, st>>>(tb, w);
     T2B_CUDA(cudaGetLastError());
 }

@@ -115,6 +115,8 @@ struct Tables {
     int nk;                   //     pixels whose projection, hence contraction term, can be non-zero)
     double sigma2_offset, pixel_size, adaptive_fraction;
     double lpo_min, lpo_max;  // extremes of log(pdf_o) over evaluated orientations
+    const unsigned char* scl_ring; // K x (ori_size/2+1): ring enters the scale-correction sums
+                                   // (data_vs_prior > 3), or nullptr: do_scale_correction off
 };
 
 // Device views of the batch workspace.
@@ -173,6 +175,7 @@ struct Work {
     long long *r_nsign, *r_ncsig;
     int* r_pose;
     double *r_norm, *r_sumw, *r_sig_off, *r_sigma2, *r_pdf_class, *r_pdf_dir;
+    double *r_xa, *r_aa;      // n (optional): scale-correction sums XA, AA
 };
 
 // ------------------------------------------------------------- kernels
@@ -299,7 +302,7 @@ struct t2b_ctx {
         double* scal = nullptr;
         double *r_min = nullptr, *r_sum = nullptr, *r_sig = nullptr, *r_csum = nullptr, *r_csig = nullptr,
                *r_pmax = nullptr, *r_norm = nullptr, *r_sumw = nullptr, *r_sig_off = nullptr, *r_sigma2 = nullptr,
-               *r_pdf_class = nullptr, *r_pdf_dir = nullptr, *r_audit = nullptr;
+               *r_pdf_class = nullptr, *r_pdf_dir = nullptr, *r_audit = nullptr, *r_xa = nullptr, *r_aa = nullptr;
         long long *r_nsign = nullptr, *r_ncsig = nullptr;
         int *r_pose = nullptr, *status = nullptr, *r_learned = nullptr;
         cudaEvent_t copied = nullptr;         // inputs in the slot (copy_stream)

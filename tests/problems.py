@@ -4,7 +4,10 @@ import numpy as np
 from conftest import load_package
 
 
-def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=None, ref_dim=3, maxsig=-1):
+def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=None, ref_dim=3, maxsig=-1,
+          scale_correction=False):
+    """scale_correction: per-particle scale_correction in U(0.8, 1.2) and a data_vs_prior per
+    class and ring spread around the threshold 3, so both kinds of ring occur."""
     t2b = load_package()
     import t2relion_b200.synthetic as sy
     import oracle as orc
@@ -31,6 +34,11 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
     parts = sy.make_particles(maps[0], n_particles, ori_size=N, s=s, r_max=r, angpix=p["angpix"],
                               snr=p["snr"], seed=seed, max_shift=p["rng"], ref_dim=ref_dim,
                               classes=cls, class_maps=maps)
+    dvp = None
+    if scale_correction:
+        srng = np.random.default_rng(seed + 977)
+        parts["scalars"][:, 6] = srng.uniform(0.8, 1.2, n_particles)
+        dvp = srng.uniform(0.0, 8.0, (nr_classes, N // 2 + 1))
     sigma2_offset = (p["rng"] * p["angpix"]) ** 2
     pdf_dir = np.ones((nr_classes, samp["n_dir"])) / (samp["n_dir"] * nr_classes)
     pdf_cls = np.ones(nr_classes) / nr_classes
@@ -38,7 +46,7 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
     prob = orc.Problem(ori_size=N, s=s, ref_dim=ref_dim, maps=maps, r_max=r, pad=2, samp=samp,
                        pdf_direction=pdf_dir, pdf_class=pdf_cls, sigma2_offset=sigma2_offset,
                        pixel_size=p["angpix"], adaptive_fraction=0.999, ovs=p["ovs"], bp_pad_size=ps,
-                       bp_r_max=r, maximum_significants=maxsig)
+                       bp_r_max=r, maximum_significants=maxsig, data_vs_prior=dvp)
     mres = sy.mresol(s)
     oparts = prob.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], mres)
 
@@ -50,11 +58,20 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
         es.configure(ori_size=N, current_size=s, ref_dim=ref_dim, nr_classes=nr_classes, samp=samp,
                      pdf_direction=pdf_dir, pdf_class=pdf_cls, sigma2_offset=sigma2_offset,
                      pixel_size=p["angpix"], adaptive_oversampling=p["ovs"], diff2_mode=diff2_mode,
-                     max_batch=max_batch or n_particles, maximum_significants=maxsig)
+                     max_batch=max_batch or n_particles, maximum_significants=maxsig, data_vs_prior=dvp)
         return es
 
+    def oracle_problem():
+        """A second oracle Problem of the same setup (own grids) for same-input stage checks;
+        `oparts` can be passed to it."""
+        return orc.Problem(ori_size=N, s=s, ref_dim=ref_dim, maps=maps, r_max=r, pad=2, samp=samp,
+                           pdf_direction=pdf_dir, pdf_class=pdf_cls, sigma2_offset=sigma2_offset,
+                           pixel_size=p["angpix"], adaptive_fraction=0.999, ovs=p["ovs"], bp_pad_size=ps,
+                           bp_r_max=r, maximum_significants=maxsig, data_vs_prior=dvp)
+
     return dict(t2b=t2b, sy=sy, maps=maps, samp=samp, parts=parts, prob=prob, oparts=oparts,
-                product=product, N=N, s=s, r=r, pad_size=ps, ovs=p["ovs"], K=nr_classes, ref_dim=ref_dim)
+                product=product, oracle_problem=oracle_problem, N=N, s=s, r=r, pad_size=ps, ovs=p["ovs"],
+                K=nr_classes, ref_dim=ref_dim, data_vs_prior=dvp)
 
 
 def fsc(a, b, shells, nshell):

@@ -134,3 +134,88 @@ def test_coarse_diff2_matches_reference_cpu_kernel(oracle, synth):
         assert np.max(rel) < 5e-6, np.max(rel)      # measured 5.7e-7
         assert np.median(rel) < 5e-7                 # measured 9.5e-8
         assert np.array_equal(np.argmin(out, axis=1), np.argmin(ref_o, axis=1))
+
+
+def _small_problem(t2b, synth, oracle, scale=1.0, dvp=None, n=2, seed=5):
+    N, r, s = 32, 8, 16
+    fmap = synth.fourier_map(synth.blob_volume(N, 12, seed=seed), r)
+    samp = t2b.sampling(3, 1, 15.0, 1, 2, 1, 2.0)
+    parts = synth.make_particles(fmap, n, ori_size=N, s=s, r_max=r, angpix=2.0, snr=0.5, seed=seed,
+                                 max_shift=2.0)
+    parts["scalars"][:, 6] = scale
+    pr = oracle.Problem(ori_size=N, s=s, ref_dim=3, maps=[fmap], r_max=r, pad=2, samp=samp,
+                        pdf_direction=np.ones((1, samp["n_dir"])), pdf_class=np.ones(1), sigma2_offset=16.,
+                        pixel_size=2.0, adaptive_fraction=0.999, ovs=1, bp_pad_size=synth.pad_size(r), bp_r_max=r,
+                        data_vs_prior=dvp)
+    return pr, parts, samp, synth.mresol(s)
+
+
+def test_hoisted_diff2_equals_literal_form(t2b, synth, oracle):
+    """The oracle's coarse and fine diff2 hoist the CTF-scaled reference and the shifted
+    image out of the per-hypothesis loop; every value equals the reference's literal
+    per-pixel form (src/ml_optimiser.cpp:7251-7272) bit for bit."""
+    pr, parts, samp, mres = _small_problem(t2b, synth, oracle, scale=1.1)
+    op = pr.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], mres)
+    d2, _ = pr.coarse_diff2(op, 1)
+    rng = np.random.default_rng(3)
+    for o, t in zip(rng.integers(0, pr.O, 40), rng.integers(0, pr.T, 40)):
+        assert d2[o * pr.T + t] == pr.diff2_literal(op, 1, 0, samp["eul_coarse"][o], samp["trans_px"][t])
+    mask = np.zeros(pr.O * pr.T, np.uint8)
+    mask[rng.integers(0, mask.size, 30)] = 1
+    pairs, fd, _ = pr.fine_diff2(op, 1, mask)
+    R, V = samp["nover_rot"], samp["nover_trans"]
+    for q in range(0, len(pairs), 7):
+        o, t = divmod(int(pairs[q]), pr.T)
+        for r in range(R):
+            for v in range(V):
+                lit = pr.diff2_literal(op, 1, 0, samp["eul_fine"][o * R + r], samp["trans_px_fine"][t * V + v])
+                assert fd[q, r * V + v] == lit
+
+
+def test_scale_correction_sums_follow_the_scale(t2b, synth, oracle):
+    """XA / AA are divided by scale_correction and its square (src/ml_optimiser.cpp:8859-8860):
+    a particle whose CTF is halved while its scale doubles has the same diff2, weights and
+    A = scale CTF P, so its XA halves and its AA quarters; rings with data_vs_prior <= 3 add
+    nothing, and without data_vs_prior both sums are 0."""
+    dvp = np.full((1, 17), 5.0)
+    dvp[0, 5:9] = 1.0
+    pa, parts, _, mres = _small_problem(t2b, synth, oracle, scale=1.0, dvp=dvp)
+    ra = pa.estep(pa.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], mres), nthreads=1)
+    pb, parts_b, _, _ = _small_problem(t2b, synth, oracle, scale=2.0, dvp=dvp)
+    ctf_b = (parts_b["ctf"].astype(np.float64) / 2).astype(np.float32)
+    assert np.array_equal(ctf_b.astype(np.float64) * 2, parts_b["ctf"].astype(np.float64))
+    rb = pb.estep(pb.particles(parts_b["fimg"], ctf_b, parts_b["minv"], parts_b["scalars"], mres), nthreads=1)
+    assert np.array_equal(ra["pose"], rb["pose"])
+    assert np.all(ra["wsum_scale_aa"] > 0)
+    assert np.allclose(rb["wsum_scale_xa"], ra["wsum_scale_xa"] / 2, rtol=1e-12)
+    assert np.allclose(rb["wsum_scale_aa"], ra["wsum_scale_aa"] / 4, rtol=1e-12)
+    pn, parts_n, _, _ = _small_problem(t2b, synth, oracle, scale=1.0, dvp=None)
+    rn = pn.estep(pn.particles(parts_n["fimg"], parts_n["ctf"], parts_n["minv"], parts_n["scalars"], mres),
+                  nthreads=1)
+    assert np.all(rn["wsum_scale_xa"] == 0) and np.all(rn["wsum_scale_aa"] == 0)
+    pz, parts_z, _, _ = _small_problem(t2b, synth, oracle, scale=1.0, dvp=np.zeros((1, 17)))
+    rz = pz.estep(pz.particles(parts_z["fimg"], parts_z["ctf"], parts_z["minv"], parts_z["scalars"], mres),
+                  nthreads=1)
+    assert np.all(rz["wsum_scale_xa"] == 0) and np.all(rz["wsum_scale_aa"] == 0)
+
+
+def test_wsum_stage_alone_reproduces_the_estep(t2b, synth, oracle):
+    """orc_wsum_bp (the stage the device's weighted sums are checked against on the same
+    weights) gives the E-step's own sums and grid when fed the E-step's final weights,
+    rebuilt here from the oracle's fine pass and weights."""
+    dvp = np.full((1, 17), 5.0)
+    pa, parts, samp, mres = _small_problem(t2b, synth, oracle, scale=1.05, dvp=dvp, n=1)
+    op = pa.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], mres)
+    ra = pa.estep(op, nthreads=1)
+    d2, mn = pa.coarse_diff2(op, 0)
+    rc, w, sw, sig, _ = pa.weights(op, 0, 0, d2, np.arange(d2.size), mn)
+    mask = (w >= sig).astype(np.uint8)
+    pairs, fd, fmn = pa.fine_diff2(op, 0, mask)
+    rc, wf, fsum, fsig, _ = pa.weights(op, 0, 1, fd.reshape(-1), np.repeat(pairs, pa.RV), fmn)
+    pb, _, _, _ = _small_problem(t2b, synth, oracle, scale=1.05, dvp=dvp, n=1)
+    o = pb.wsum_bp(op, 0, pairs, wf, fsum, fsig)
+    for k in ("wsum_norm", "sumw", "wsum_sigma2_offset", "pmax", "wsum_scale_xa", "wsum_scale_aa"):
+        assert o[k] == ra[k][0], k
+    assert np.array_equal(o["pose"], ra["pose"][0])
+    assert np.array_equal(o["wsum_sigma2"], ra["wsum_sigma2"][0])
+    assert np.array_equal(pb.bp_data, pa.bp_data) and np.array_equal(pb.bp_weight, pa.bp_weight)
