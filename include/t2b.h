@@ -211,6 +211,16 @@ typedef struct t2b_recon_config {
 } t2b_recon_config;
 int t2b_reconstruct(t2b_ctx* ctx, int iclass, const t2b_recon_config* cfg, double* vol);
 
+/* Hermitian symmetry of the x = 0 plane of a grid, in place on the device
+ * (BackProjector::enforceHermitianSymmetry, src/backprojector.cpp:2104-2121, which
+ * MlOptimiser::maximization applies to every class before reconstructing,
+ * src/ml_optimiser.cpp:4626): each Friedel pair (z, y, 0) <-> (-z, -y, 0) gets the sum
+ * data(z, y) + conj(data(-z, -y)) (conjugated on the partner) and the sum of the two
+ * weights.  Linear, so it may run before or after the reduction of the grids over GPUs, but
+ * once.  Point-group symmetry (applyPointGroupSymmetry) is C1 only: no other operator is
+ * applied. */
+int t2b_backprojector_enforce_hermitian(t2b_ctx* ctx, int iclass);
+
 /* Fourier shell correlation of two grids (two half-sets) after down-sampling to
  * the unpadded box (BackProjector::getDownsampledAverage +
  * calculateDownSampledFourierShellCorrelation, src/backprojector.cpp:933-1040);

@@ -71,6 +71,8 @@ public:
     }
     void initMdl() { check(t2b_backprojector_init(b_.ctx(), iclass_, z_ > 1 ? 3 : 2, x_, y_, z_, iy_, iz_, r_, pad_)); }
     void clear() { check(t2b_backprojector_clear(b_.ctx(), iclass_)); }
+    // BackProjector::enforceHermitianSymmetry on the device grid (before reconstructing)
+    void enforceHermitianSymmetry() { check(t2b_backprojector_enforce_hermitian(b_.ctx(), iclass_)); }
     void getMdlData(float* real, float* imag, float* weight)
     {
         check(t2b_backprojector_get(b_.ctx(), iclass_, real, imag, weight));

@@ -22,6 +22,10 @@ complex, weight real; z, y centred at -initz, -inity; x from 0; 3D grids of
                     ori_size / 2, cosine width 3, average background); and
                     Projector::griddingCorrect (src/projector.cpp:489-522:
                     divide by sinc^2 of r / (ori_size pad), trilinear)
+  enforce_hermitian_symmetry
+                    BackProjector::enforceHermitianSymmetry (src/backprojector.cpp:2104-2121),
+                    applied by MlOptimiser::maximization before reconstruct
+                    (src/ml_optimiser.cpp:4626)
   downsampled_fsc   getDownsampledAverage + calculateDownSampledFourierShellCorrelation
                     (src/backprojector.cpp:933-1040)
   update_ssnr       BackProjector::updateSSNRarrays (src/backprojector.cpp:1041-1205)
@@ -42,6 +46,31 @@ def _logical(shape, initz, inity):
     i = np.arange(yd)[None, :, None] + inity
     j = np.arange(xd)[None, None, :]
     return k, i, j
+
+
+def enforce_hermitian_symmetry(data, weight):
+    """The reference's loop over the x = 0 plane, element by element in its order: for z from
+    STARTINGZ to FINISHINGZ, y from (z < 0 ? 0 : 1) to FINISHINGY, the pair (z, y) / (-z, -y)
+    gets fsum = data(z, y) + conj(data(-z, -y)) and conj(fsum), and both weights their sum.
+    Returns new arrays (3D [z][y][x] or 2D [y][x] centred grids)."""
+    d = np.array(data, copy=True)
+    w = np.array(weight, copy=True)
+    two_d = w.ndim == 2
+    if two_d:
+        d, w = d[None], w[None]
+    zd, yd = w.shape[0], w.shape[1]
+    initz, inity = -(zd // 2), -(yd // 2)
+    for z in range(initz, initz + zd):
+        for y in range(0 if z < 0 else 1, inity + yd):
+            a = (z - initz, y - inity, 0)
+            b = (-z - initz, -y - inity, 0)
+            f = d[a] + np.conj(d[b])
+            d[a] = f
+            d[b] = np.conj(f)
+            ws = w[a] + w[b]
+            w[a] = ws
+            w[b] = ws
+    return (d[0], w[0]) if two_d else (d, w)
 
 
 def decenter_divide(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_map=0):

@@ -42,7 +42,7 @@ ABI_SYMBOLS = (
     "t2b_proposal_train", "t2b_proposal_enable", "t2b_proposal_params", "t2b_proposal_features",
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
     "t2b_prep_configure", "t2b_prep_batch_host", "t2b_prep_batch_device", "t2b_autotune", "t2b_tune_set",
-    "t2b_reconstruct", "t2b_fsc_halves", "t2b_update_ssnr",
+    "t2b_reconstruct", "t2b_fsc_halves", "t2b_update_ssnr", "t2b_backprojector_enforce_hermitian",
     "t2b_mrc_info", "t2b_mrc_read", "t2b_mrc_write", "t2b_star_open", "t2b_star_shape", "t2b_star_label",
     "t2b_star_column", "t2b_star_value", "t2b_star_close", "t2b_star_write",
 )
@@ -168,6 +168,7 @@ def _setup_prototypes():
     lib.t2b_projector_set.argtypes = [v, i, i, i, i, i, i, i, i, i, v]
     lib.t2b_backprojector_init.argtypes = [v, i, i, i, i, i, i, i, i, i]
     lib.t2b_backprojector_clear.argtypes = [v, i]
+    lib.t2b_backprojector_enforce_hermitian.argtypes = [v, i]
     lib.t2b_backprojector_get.argtypes = [v, i, v, v, v]
     lib.t2b_backprojector_device_ptrs.argtypes = [v, i, ctypes.POINTER(v), ctypes.POINTER(v)]
     lib.t2b_configure.argtypes = [v, ctypes.POINTER(Config)]
@@ -420,6 +421,10 @@ class EStep:
 
     def clear_backprojector(self, iclass):
         _check(lib.t2b_backprojector_clear(self._h, iclass))
+
+    # BackProjector::enforceHermitianSymmetry (before the reconstruction, once per iteration)
+    def enforce_hermitian_symmetry(self, iclass):
+        _check(lib.t2b_backprojector_enforce_hermitian(self._h, iclass))
 
     # AccBackprojector::getMdlData
     def get_backprojector(self, iclass):
@@ -781,6 +786,9 @@ class AccBackprojector:
     def initMdl(self):
         xdim, ydim, zdim, max_r, pad = self._dims
         self.estep.init_backprojector(self.iclass, 3 if zdim > 1 else 2, ydim, max_r, pad)
+
+    def enforceHermitianSymmetry(self):
+        self.estep.enforce_hermitian_symmetry(self.iclass)
 
     def getMdlData(self):
         data, w = self.estep.get_backprojector(self.iclass)

@@ -18,6 +18,7 @@
 //             prior sums, then trilinear backprojection with float2 atomics
 //             (src/ml_optimiser.cpp:8153-8700, src/backprojector.cpp:55-230)
 #include "t2b_internal.cuh"
+#include "project_pixel.cuh"
 #include <map>
 #include <algorithm>
 #include <cfloat>
@@ -1541,9 +1542,9 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                             const int y = (i < xh) ? i : i - s;
                             if (i >= xh && x == 0) continue;
                             if (x * x + y * y > g.r_max * g.r_max) continue;
-                            double xp = (A[0] * x + A[3] * y) * g.pad;
-                            double yp = (A[1] * x + A[4] * y) * g.pad;
-                            double zp = (A[2] * x + A[5] * y) * g.pad;
+                            double xp = rot_coord(A[0], A[3], g.pad, x, y);
+                            double yp = rot_coord(A[1], A[4], g.pad, x, y);
+                            double zp = rot_coord(A[2], A[5], g.pad, x, y);
                             float vr = fir, vi = fii;
                             if (xp < 0) { xp = -xp; yp = -yp; zp = -zp; vi = -vi; }
                             const int x0 = (int)floor(xp);

@@ -19,12 +19,24 @@ __device__ __forceinline__ void pp_lerp(double a, double lr, double li, double h
     i = li + (hi - li) * a;
 }
 
+// One coordinate of the padded, rotated window pixel (x, y): (a pad) x + (b pad) y with
+// a, b a column of A (A^-1 = A^T), the padding factor folded into the matrix first and
+// each product and the sum rounded on their own, as the reference CPU path evaluates it
+// (Ainv *= padding_factor; xp = Ainv(0,0) x + Ainv(0,1) y, src/backprojector.cpp:79-83,
+// 215; src/projector.cpp:566-590).  No fused multiply-add: on the x = 0 plane the sign
+// of xp is rounding noise, and it decides which Friedel partner a backprojected pixel
+// lands on, so the device takes the same decision as the CPU path.
+__device__ __forceinline__ double rot_coord(double a, double b, int pad, int x, int y)
+{
+    return __dadd_rn(__dmul_rn(a * (double)pad, (double)x), __dmul_rn(b * (double)pad, (double)y));
+}
+
 __device__ __forceinline__ float2 project_pixel(const float2* __restrict__ mdl, const Volume& v,
                                                 const double* A, int x, int y)
 {
-    double xp = (A[0] * x + A[3] * y) * v.pad;
-    double yp = (A[1] * x + A[4] * y) * v.pad;
-    double zp = v.ref_dim == 3 ? (A[2] * x + A[5] * y) * v.pad : 0.;
+    double xp = rot_coord(A[0], A[3], v.pad, x, y);
+    double yp = rot_coord(A[1], A[4], v.pad, x, y);
+    double zp = v.ref_dim == 3 ? rot_coord(A[2], A[5], v.pad, x, y) : 0.;
     const bool neg = xp < 0;
     if (neg) { xp = -xp; yp = -yp; zp = -zp; }
     const int x0 = (int)floor(xp);

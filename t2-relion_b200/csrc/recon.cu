@@ -305,6 +305,35 @@ __global__ void k_ssnr_prior(Volume g, int nb, const float* __restrict__ weight,
     shell_flush(sb, 3 * nb, acc);
 }
 
+// BackProjector::enforceHermitianSymmetry (src/backprojector.cpp:2104-2121) on the x = 0
+// plane: every Friedel pair (z, y) <-> (-z, -y) once (z < 0 with y >= 0, or z >= 0 with
+// y >= 1), both members set to the data sum (conjugated on the partner) and the weight sum.
+// The visited set and the partners' set are disjoint, so one thread per pair writes without
+// conflicts.  Grids are centred: (z, y) at ((z - initz) * ydim + (y - inity)) * xdim.
+__global__ void k_hermitian(Volume g, float2* __restrict__ data, float* __restrict__ weight)
+{
+    const int zlo = g.initz, zhi = g.initz + g.zdim - 1;
+    const int ylo = g.inity, yhi = g.inity + g.ydim - 1;
+    const int ny = yhi + 1;                       // y = 0 .. yhi
+    const long long total = (long long)g.zdim * ny;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int z = zlo + (int)(i / ny), y = (int)(i % ny);
+        if (z >= 0 && y == 0) continue;           // starty = (iz < 0) ? 0 : 1
+        const int mz = -z, my = -y;
+        if (mz < zlo || mz > zhi || my < ylo) continue;
+        const size_t a = ((size_t)(z - g.initz) * g.ydim + (y - g.inity)) * g.xdim;
+        const size_t b = ((size_t)(mz - g.initz) * g.ydim + (my - g.inity)) * g.xdim;
+        const float2 da = data[a], db = data[b];
+        const float2 f = make_float2(da.x + db.x, da.y - db.y);
+        data[a] = f;
+        data[b] = make_float2(f.x, -f.y);
+        const float w = weight[a] + weight[b];
+        weight[a] = w;
+        weight[b] = w;
+    }
+}
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
@@ -415,6 +444,22 @@ int t2b_reconstruct(t2b_ctx* c, int iclass, const t2b_recon_config* cf, double* 
         T2B_CUDA(cudaGetLastError());
         T2B_CUDA(cudaMemcpyAsync(vol_out, out.p, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
         T2B_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int t2b_backprojector_enforce_hermitian(t2b_ctx* c, int iclass)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c, T2B_ERR_ARG, "null argument");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard dg(c->device);
+        const Volume& v = grid_volume(c, iclass);
+        T2B_REQUIRE(v.ref_dim == 2 || -v.initz == v.zdim / 2, T2B_ERR_ARG, "grid is not centred in z");
+        T2B_REQUIRE(-v.inity == v.ydim / 2, T2B_ERR_ARG, "grid is not centred in y");
+        const long long pairs = (long long)v.zdim * (v.ydim / 2 + 1);
+        k_hermitian<<<grid_of(pairs), RC_THREADS, 0, c->stream>>>(v, c->gdata[iclass], c->gweight[iclass]);
+        T2B_CUDA(cudaGetLastError());
+        T2B_CUDA(cudaStreamSynchronize(c->stream));
     });
 }
 

@@ -81,7 +81,8 @@ def test_weights_match_oracle_on_same_diff2(run):
         mn = d2[ok].min()
         rc, w, sw, sig, ns = prob.weights(op, b, 0, d2, np.arange(d2.size), mn)
         assert rc == 0
-        assert res["coarse_sum_weight"][b] == pytest.approx(sw, rel=1e-12)
+        # the sum of up to K*O*T FP64 weights in another order: 1e-10; single weights 1e-12
+        assert res["coarse_sum_weight"][b] == pytest.approx(sw, rel=1e-10)
         assert res["coarse_sig_weight"][b] == pytest.approx(sig, rel=1e-12)
         assert res["nr_sign"][b] == ns
         assert res["n_coarse_sig"][b] == int(np.sum(w >= sig))
@@ -111,7 +112,7 @@ def test_fine_weights_match_oracle_on_same_diff2(run):
         ih = np.repeat(pairs, RV)
         rc, w, sw, sig, _ = prob.weights(op, b, 1, d2, ih, d2[d2 >= 0].min())
         assert rc == 0
-        assert res["sum_weight"][b] == pytest.approx(sw, rel=1e-12)
+        assert res["sum_weight"][b] == pytest.approx(sw, rel=1e-10)
         assert res["sig_weight"][b] == pytest.approx(sig, rel=1e-12)
         pw = es.weights(b)
         assert pw.size == w.size

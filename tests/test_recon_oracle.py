@@ -137,3 +137,27 @@ def test_reconstruction_of_a_known_image_2d(synth, ori, r_max):
     sinc = np.where(r > 0, np.sin(np.pi * rv) / (np.pi * np.where(r > 0, rv, 1)), 1.0)
     want = ro.soft_mask_bg(lp, ori / 2.0, 3.0) / (sinc * sinc)
     assert np.max(np.abs(got - want)) <= 1e-10 * np.max(np.abs(want))
+
+
+@pytest.mark.parametrize("shape", [(9, 9, 5), (9, 5)], ids=["3d", "2d"])
+def test_hermitian_symmetry_restatement(shape):
+    """enforceHermitianSymmetry (src/backprojector.cpp:2104-2121) on a grid whose Friedel
+    partners of the x = 0 plane differ: each pair holds old(z, y) + conj(old(-z, -y)) and
+    its conjugate, weights the pair's sum; the origin and every x > 0 element stay."""
+    rng = np.random.default_rng(4)
+    d = rng.normal(size=shape) + 1j * rng.normal(size=shape)
+    w = rng.uniform(0, 1, shape)
+    sd, sw = ro.enforce_hermitian_symmetry(d, w)
+    d3, w3, s3, t3 = (a[None] if len(shape) == 2 else a for a in (d, w, sd, sw))
+    zd, yd = w3.shape[0], w3.shape[1]
+    cz, cy = zd // 2, yd // 2
+    for z in range(-cz, cz + 1):
+        for y in range(-cy, cy + 1):
+            a, b = (z + cz, y + cy, 0), (-z + cz, -y + cy, 0)
+            if z == 0 and y == 0:
+                assert s3[a] == d3[a] and t3[a] == w3[a]
+                continue
+            assert s3[a] == np.conj(s3[b])
+            assert t3[a] == t3[b] == w3[a] + w3[b]
+            assert np.isclose(s3[a], d3[a] + np.conj(d3[b]), rtol=1e-15)
+    assert np.array_equal(s3[..., 1:], d3[..., 1:]) and np.array_equal(t3[..., 1:], w3[..., 1:])
