@@ -58,11 +58,24 @@ METRIC = "E-step particles/s box128: learned+split-BF16 vs plain FP32 GPU; roofl
 PROP = dict(topk=64, rescore=1024, audit_every=50, audit_mass=0.999)
 # end-to-end timing: at least this many steps per timed run
 E2E_STEPS = 30
-# DRAM bytes (read + write) of the audit + proposal k_diff2_tc launches of one learned step
-# at 128 particles, from one ncu capture
-# (audit 766.60 MB read + 18.67 MB written, proposal pass 169.96 MB + 0.14 MB;
-# profiles/k_diff2_tc_box128_learned_b128_dram.md)
-LEARNED_TRAFFIC = 766.60e6 + 18.67e6 + 169.96e6 + 0.14e6
+# DRAM bytes (read + write) per launch of k_diff2_tc from one ncu capture, stamped with the
+# SHA-256 (first 16 hex digits) of the kernel's source at capture time; a line whose kernel
+# source differs reports traffic null rather than a stale figure.
+#   learned: audit 766.60 MB read + 18.67 MB written, proposal pass 169.96 MB + 0.14 MB (one step)
+#   splitbf16: the full coarse pass, 8.16 GB read + 1.56 GB written per 128 particles
+TRAFFIC = {"kernel_sha": "28a6bb4cdd72dd50",
+           "learned": 766.60e6 + 18.67e6 + 169.96e6 + 0.14e6,
+           "splitbf16_per128": 8.16e9 + 1.56e9}
+# particles of the learned-vs-plain quality check (not the timed batch)
+QUALITY_PARTICLES = 2048
+# timed steps of the plain FP32 comparator (1,154 particles/s: about 0.11 s per 128-particle step)
+PLAIN_STEPS = 5
+
+
+def kernel_sha():
+    import hashlib
+    with open(os.path.join(ROOT, "t2-relion_b200", "csrc", "diff2_tc.cu"), "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()[:16]
 
 
 def build_problem(t2b, sy, n_particles, seed):
@@ -194,102 +207,136 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def _coarse_slice_timer(sy, fmap, samp, parts):
-    """A function (n_dir, n_particles) -> seconds that runs the coarse pass of one
-    particle per host thread over the first n_dir directions x all psi.
+def load_synthetic():
+    """The particle generator, t2-relion_b200/synthetic.py (numpy only), loaded by its path
+    without the package: the reference arm and the CPU baseline must not load the library."""
+    name = "t2b_synthetic_standalone"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "t2-relion_b200", "synthetic.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules[name] = mod
+    return sys.modules[name]
 
-    The reference's own CPU kernel (CpuKernels::diff2_coarse, compiled from the
-    reference sources into oracle/_ref/libacc_ref.so) when that library is
-    present, else the FP64 port in oracle/.  Returns (timer, kind).
-    """
+
+def workload_config():
+    """`config` of the JSON line: the workload alone, identical in both arms."""
     w = WORKLOAD
     s = 2 * w["r_max"]
-    lib_path = os.path.join(ROOT, "oracle", "_ref", "libacc_ref.so")
-    if os.path.exists(lib_path):
-        lib = ctypes.CDLL(lib_path)
-        lib.ref_coarse_diff2.restype = ctypes.c_int
-        fm = np.ascontiguousarray(fmap.view(np.float32))
-        mz, my, mx = fmap.shape
-        eul = samp["eul_coarse"].reshape(-1, 3, 3)
-        einv = np.ascontiguousarray(np.transpose(eul, (0, 2, 1)).reshape(-1, 9), np.float32)
-        N = w["ori_size"]
-        tx = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 0] / N, np.float32)
-        ty = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 1] / N, np.float32)
-        T = len(tx)
-        ops = []
-        for b in range(parts["fimg"].shape[0]):
-            ctf = parts["ctf"][b].astype(np.float64)
-            X = parts["fimg"][b].astype(np.complex128) / ctf
-            ops.append((np.ascontiguousarray(X.real, np.float32), np.ascontiguousarray(X.imag, np.float32),
-                        np.ascontiguousarray(parts["minv"][b] * ctf * ctf, np.float32),
-                        float(parts["scalars"][b, 1] / 2)))
+    return {"workload": w["name"], "box": w["ori_size"], "healpix_order": w["order"], "psi_step": w["psi_step"],
+            "orientations": 12 * 4 ** w["order"] * int(np.ceil(360 / w["psi_step"])),
+            "translations": 81 if w["offset_range"] == 5 else None, "pixels": s * (s // 2 + 1),
+            "adaptive_oversampling": 1, "fine_hypotheses_per_pair": 32, "snr": w["snr"],
+            "grid": [259, 259, 130]}
 
-        def run(nd, npart):
-            no = nd * samp["n_psi"]
-            outs = [np.empty((no, T), np.float32) for _ in range(npart)]
 
-            def one(b):
-                re, im, corr, xi2 = ops[b]
-                lib.ref_coarse_diff2(ctypes.c_void_p(fm.ctypes.data), mx, my, mz, -(my // 2), -(mz // 2),
-                                     w["r_max"], 2, ctypes.c_void_p(einv.ctypes.data), no,
-                                     ctypes.c_void_p(re.ctypes.data), ctypes.c_void_p(im.ctypes.data),
-                                     ctypes.c_void_p(corr.ctypes.data), s // 2 + 1, s,
-                                     ctypes.c_void_p(tx.ctypes.data), ctypes.c_void_p(ty.ctypes.data), T,
-                                     ctypes.c_float(xi2), ctypes.c_void_p(outs[b].ctypes.data))
-            t0 = time.perf_counter()
-            ths = [threading.Thread(target=one, args=(b,)) for b in range(npart)]
-            for th in ths:
-                th.start()
-            for th in ths:
-                th.join()
-            return time.perf_counter() - t0
-        return run, "reference"
+class CpuEStep:
+    """The reference's CPU E-step of the workload on the host cores, one particle per thread.
 
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
+    Coarse pass: the reference's own CPU kernel, CpuKernels::diff2_coarse
+    (src/acc/cpu/cpu_kernels/diff2.h:329-606, compiled from the reference sources into
+    oracle/_ref/libacc_ref.so), over every orientation and translation; where that library is
+    absent, the FP64 oracle's coarse pass.  The rest -- weights and significance, fine pass,
+    weights, weighted sums, backprojection -- by the FP64 oracle port (oracle/), which is
+    more than 95 % cheaper than the coarse pass at this workload.  Nothing of the library is
+    loaded: sampling from oracle/sampling_oracle.py, particles from synthetic.py by path.
+    """
 
-    def run(nd, npart):
-        sub = dict(samp)
-        sub["n_dir"] = nd
-        sub["eul_coarse"] = samp["eul_coarse"][: nd * samp["n_psi"]]
-        prob = orc.Problem(ori_size=w["ori_size"], s=s, ref_dim=3, maps=[fmap], r_max=w["r_max"], pad=2,
-                           samp=sub, pdf_direction=np.ones((1, nd)), pdf_class=np.ones(1),
-                           sigma2_offset=1.0, pixel_size=w["angpix"], adaptive_fraction=0.999, ovs=0,
-                           bp_pad_size=sy.pad_size(w["r_max"]), bp_r_max=w["r_max"])
-        op = prob.particles(parts["fimg"][:npart], parts["ctf"][:npart], parts["minv"][:npart],
-                            parts["scalars"][:npart], sy.mresol(s))
+    def __init__(self, n_particles, seed):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        import sampling_oracle as so
+        w = WORKLOAD
+        self.sy = sy = load_synthetic()
+        N, r = w["ori_size"], w["r_max"]
+        self.s = s = 2 * r
+        self.fmap = fmap = sy.fourier_map(sy.blob_volume(N, w["n_blobs"], seed=w["seed"]), r)
+        self.samp = samp = so.sampling(w["order"], w["psi_step"], 1, w["offset_range"], w["offset_step"], w["angpix"])
+        self.parts = parts = sy.make_particles(fmap, n_particles, ori_size=N, s=s, r_max=r, angpix=w["angpix"],
+                                               snr=w["snr"], seed=seed, max_shift=w["offset_range"])
+        self.prob = orc.Problem(ori_size=N, s=s, ref_dim=3, maps=[fmap], r_max=r, pad=2, samp=samp,
+                                pdf_direction=np.full((1, samp["n_dir"]), 1.0 / samp["n_dir"]), pdf_class=np.ones(1),
+                                sigma2_offset=(w["offset_range"] * w["angpix"]) ** 2, pixel_size=w["angpix"],
+                                adaptive_fraction=0.999, ovs=1, bp_pad_size=sy.pad_size(w["bp_r_max"]),
+                                bp_r_max=w["bp_r_max"])
+        self.op = self.prob.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], sy.mresol(s))
+        self.O, self.T = samp["n_dir"] * samp["n_psi"], samp["n_trans"]
+        lib_path = os.path.join(ROOT, "oracle", "_ref", "libacc_ref.so")
+        self.kind = "reference" if os.path.exists(lib_path) else "port"
+        if self.kind == "reference":
+            self.lib = ctypes.CDLL(lib_path)
+            self.lib.ref_coarse_diff2.restype = ctypes.c_int
+            self.fm = np.ascontiguousarray(fmap.view(np.float32))
+            eul = samp["eul_coarse"].reshape(-1, 3, 3)
+            self.einv = np.ascontiguousarray(np.transpose(eul, (0, 2, 1)).reshape(-1, 9), np.float32)
+            self.tx = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 0] / N, np.float32)
+            self.ty = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 1] / N, np.float32)
+            # the reference kernel's operands (refs_are_ctf_corrected): X / CTF and Minvsigma2 CTF^2
+            self.ops = []
+            for b in range(n_particles):
+                ctf = parts["ctf"][b].astype(np.float64)
+                X = parts["fimg"][b].astype(np.complex128) / ctf
+                self.ops.append((np.ascontiguousarray(X.real, np.float32), np.ascontiguousarray(X.imag, np.float32),
+                                 np.ascontiguousarray(parts["minv"][b] * ctf * ctf, np.float32),
+                                 float(parts["scalars"][b, 1] / 2)))
+
+    def coarse(self, b, n_orient=None):
+        no = self.O if n_orient is None else n_orient
+        if self.kind != "reference":
+            d2, _ = self.prob.coarse_diff2(self.op, b)
+            return d2
+        w, mz, my, mx = WORKLOAD, *self.fmap.shape
+        out = np.empty((no, self.T), np.float32)
+        re, im, corr, xi2 = self.ops[b]
+        rc = self.lib.ref_coarse_diff2(
+            ctypes.c_void_p(self.fm.ctypes.data), mx, my, mz, -(my // 2), -(mz // 2), w["r_max"], 2,
+            ctypes.c_void_p(self.einv.ctypes.data), no, ctypes.c_void_p(re.ctypes.data),
+            ctypes.c_void_p(im.ctypes.data), ctypes.c_void_p(corr.ctypes.data), self.s // 2 + 1, self.s,
+            ctypes.c_void_p(self.tx.ctypes.data), ctypes.c_void_p(self.ty.ctypes.data), self.T, ctypes.c_float(xi2),
+            ctypes.c_void_p(out.ctypes.data))
+        if rc != 0:
+            raise RuntimeError("reference coarse kernel refused the orientation count")
+        return out.reshape(-1)
+
+    def particle(self, b):
+        """The whole E-step of particle b (its backprojection into the oracle's grid)."""
+        prob, op = self.prob, self.op
+        d2 = self.coarse(b).astype(np.float64)
+        rc, w, sw, sig, _ = prob.weights(op, b, 0, d2, np.arange(d2.size), d2.min())
+        if rc != 0:
+            raise RuntimeError("no significant coarse sample")
+        pairs, fd, fmn = prob.fine_diff2(op, b, (w >= sig).astype(np.uint8))
+        rc, wf, fsum, fsig, _ = prob.weights(op, b, 1, fd.reshape(-1), np.repeat(pairs, prob.RV), fmn)
+        prob.wsum_bp(op, b, pairs, wf, fsum, fsig)
+
+    def run(self, particles, warm=False):
+        """Seconds for `particles`, one host thread each (warm: one direction's coarse pass only)."""
+        fn = (lambda b: self.coarse(b, self.samp["n_psi"])) if warm else self.particle
         t0 = time.perf_counter()
-        ths = [threading.Thread(target=prob.coarse_diff2, args=(op, i)) for i in range(npart)]
+        ths = [threading.Thread(target=fn, args=(b,)) for b in particles]
         for th in ths:
             th.start()
         for th in ths:
             th.join()
         return time.perf_counter() - t0
-    return run, "port"
+
+    def sample_text(self, n):
+        src = ("the reference's CpuKernels::diff2_coarse, compiled from its sources" if self.kind == "reference"
+               else "the FP64 oracle port")
+        return (f"{n} particles per step, one per host thread, each through the whole E-step: coarse pass over "
+                f"all {self.O} orientations x {self.T} translations by {src}; FP64 weights and significance, fine "
+                f"pass, weighted sums and backprojection by the FP64 oracle port")
 
 
-def cpu_baseline(sy, fmap, samp, parts, seconds=20.0, timer=None):
-    """The reference's CPU E-step on the host cores, bounded sample.
-
-    Sample: one particle per host thread through the coarse pass (the part of the
-    reference's E-step that is > 95 % of its time at this workload) over a slice
-    of the 36,864 orientations sized to take about `seconds`; particles/s is
-    extrapolated to the full orientation set.
-    """
-    run, kind = timer or _coarse_slice_timer(sy, fmap, samp, parts)
-    cores = os.cpu_count() or 1
-    O = samp["n_dir"] * samp["n_psi"]
-    t1 = run(1, 1)                      # one direction = 48 orientations, one thread
-    nd = int(max(1, min(samp["n_dir"], seconds / max(t1, 1e-6))))
-    npart = min(cores, parts["fimg"].shape[0])
-    t = run(nd, npart)
-    frac = nd * samp["n_psi"] / O
-    value = npart * frac / t
-    src = ("CpuKernels::diff2_coarse of the reference, compiled from its sources" if kind == "reference"
-           else "FP64 oracle port")
-    return {"value": value, "unit": "particles/s", "cores": npart, "kind": kind,
-            "sample": f"{npart} particles x {nd * samp['n_psi']} of {O} orientations (coarse pass, {src}), "
-                      f"{t:.1f} s, extrapolated to the full orientation set"}
+def cpu_baseline(cores=None):
+    """The reference's CPU E-step on the host cores, bounded sample: one step of CpuEStep
+    (a particle per host thread through the whole E-step, about 12-20 s)."""
+    n = cores or os.cpu_count() or 1
+    cpu = CpuEStep(n, WORKLOAD["seed"] + 1)
+    cpu.run(range(n), warm=True)
+    t = cpu.run(range(n))
+    return {"value": n / t, "unit": "particles/s", "cores": n, "kind": cpu.kind, "sample": cpu.sample_text(n) +
+            f"; {t:.1f} s"}
 
 
 def _fsc_min(a, b, r_max_pad):
@@ -308,23 +355,30 @@ def _fsc_min(a, b, r_max_pad):
     return float(fsc.min())
 
 
-def quality_vs_full(es, parts):
-    """Learned E-step against the full coarse pass on the same particles (host entry
-    point, outside the timed region): pose agreement and the FSC of the two
-    reconstructions (FP64 skip-gridding division of the backprojected grids)."""
-    n = parts["fimg"].shape[0]
-    args = (parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"])
+def quality_vs_plain(es, es_plain, sy, fmap, n_check, batch, seed):
+    """The learned E-step against the plain FP32 path on `n_check` particles that are not the
+    timed batch (host entry points, outside the timed region): pose agreement, and the FSC of
+    the two reconstructions (FP64 skip-gridding division of the backprojected grids) after
+    Hermitian symmetrisation, as the M-step sees them."""
+    w = WORKLOAD
+    parts = sy.make_particles(fmap, n_check, ori_size=w["ori_size"], s=2 * w["r_max"], r_max=w["r_max"],
+                              angpix=w["angpix"], snr=w["snr"], seed=seed, max_shift=w["offset_range"])
     es.clear_backprojector(0)
-    got = es.expectation(*args)
-    map_l = es.reconstruct_divide(0)
-    es.disable_proposals()
-    es.clear_backprojector(0)
-    full = es.expectation(*args)
-    map_f = es.reconstruct_divide(0)
-    same = float(np.all(got["pose"] == full["pose"], axis=1).mean())
-    rp = WORKLOAD["r_max"] * 2   # padded-grid radius reached by the r_max window (padding factor 2)
-    return {"pose_agreement_vs_full": same, "particles_compared": n, "map_fsc_min_vs_full": _fsc_min(map_l, map_f, rp),
-            "learned_in_check": float(got["learned"].mean())}
+    es_plain.clear_backprojector(0)
+    same, learned, audited = 0, 0, 0
+    for a in range(0, n_check, batch):
+        args = [parts[k][a:a + batch] for k in ("fimg", "ctf", "minv", "scalars")]
+        got = es.expectation(*args)
+        ref = es_plain.expectation(*args)
+        same += int(np.all(got["pose"] == ref["pose"], axis=1).sum())
+        learned += int(got["learned"].sum())
+        audited += int((got["audit_mass"] >= 0).sum())
+    for e in (es, es_plain):
+        e.enforce_hermitian_symmetry(0)
+    rp = w["r_max"] * 2   # padded-grid radius reached by the r_max window (padding factor 2)
+    fsc = _fsc_min(es.reconstruct_divide(0), es_plain.reconstruct_divide(0), rp)
+    return {"particles": n_check, "pose_agreement_vs_plain": same / n_check, "map_fsc_min_vs_plain": fsc,
+            "learned_fraction": learned / n_check, "audited_particles": audited}
 
 
 def dist_init():
@@ -351,28 +405,26 @@ def max_over_ranks(x, world):
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU E-step (CpuEStep) on the host cores: every step one particle per host
+    thread through the whole E-step; warm-up steps run one direction's coarse pass per thread.
+    Rank 0 alone runs and prints; other ranks exit without work."""
     if rank != 0:
         return
-    t2b = load_package()
-    import t2relion_b200.synthetic as sy
-    fmap, samp, parts = build_problem(t2b, sy, max(8, os.cpu_count() or 1), WORKLOAD["seed"] + 1)
-    timer = _coarse_slice_timer(sy, fmap, samp, parts)
-    # each step a bounded sample: the whole --warmup W --steps K run stays within a few minutes
-    per_step = min(args.ref_seconds, 150.0 / max(1, args.warmup + args.steps))
-    vals = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(sy, fmap, samp, parts, seconds=per_step, timer=timer)
-        if i >= args.warmup:
-            vals.append(cb["value"])
-    v = statistics.median(vals)
-    cb["value"] = v
+    n = os.cpu_count() or 1
+    cpu = CpuEStep(n, WORKLOAD["seed"] + 1)
+    for _ in range(args.warmup):
+        cpu.run(range(n), warm=True)
+    times = [cpu.run(range(n)) for _ in range(args.steps)]
+    total = float(np.sum(times))
+    v = n * args.steps / total
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v if v else None,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if cb["kind"] == "reference" else "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD["name"], "particles_per_step": cb["cores"]},
-            "cpu_baseline": cb, "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0,
-                                        "d2h_bytes_per_step": 0}}
+            "dtype": "f32 (coarse kernel) / f64 (rest)" if cpu.kind == "reference" else "f64",
+            "data": "synthetic", "config": workload_config(), "particles_per_step": n,
+            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": n, "kind": cpu.kind,
+                             "sample": cpu.sample_text(n)},
+            "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -550,6 +602,7 @@ def main():
     ap.add_argument("--train-epochs", type=int, default=8)
     ap.add_argument("--batch", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparator and quality check")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--profile-case", action="store_true",
                     help="HEALPix order 2 instead of 3 (for ncu captures; not a bench number)")
@@ -613,16 +666,148 @@ def main():
                    **PROP}
         es.enable_proposals(topk=PROP["topk"], rescore=PROP["rescore"], audit_every=PROP["audit_every"],
                             audit_mass=PROP["audit_mass"])
-    dev = torch.device("cuda", local)
+    timing = time_device(es, parts, B, args.steps, args.warmup, local, world, t2b)
+    e2e, pin, hres = time_e2e(es, parts, B, args.steps, world, t2b)
+    # per-stage device times (CUDA events around each stage) of separately synchronised
+    # host-path steps; not part of `value`
+    # (one period of the audit pattern when learned: each step's audited count is kept)
+    lib = t2b.lib
+    batch = t2b.Batch(B, 0, ctypes.c_void_p(pin["fimg"].data_ptr()), None, ctypes.c_void_p(pin["ctf"].data_ptr()),
+                      ctypes.c_void_p(pin["minv"].data_ptr()), ctypes.c_void_p(pin["scal"].data_ptr()))
+    result = t2b.Result(*[ctypes.c_void_p(hres[n].data_ptr()) if n in hres else None for n, _ in t2b.Result._fields_])
+    stage_steps, audited = [], []
+    es.stage_timing(True)
+    for _ in range(min(25, args.steps)):
+        t2b._check(lib.t2b_estep_batch_host(es._h, ctypes.byref(batch), ctypes.byref(result)))
+        stage_steps.append(es.stage_ms())
+        audited.append(int((hres["audit_mass"].numpy() >= 0).sum()))
+    es.stage_timing(False)
+    stage_steps = np.array(stage_steps)
+    stages = np.mean(stage_steps, axis=0)
+    clocks = timing["clocks"]
+    value = timing["value"]
+
+    # roofline of the dominant kernel (the tcgen05 contraction k_diff2_tc)
+    O, T = samp["n_dir"] * samp["n_psi"], samp["n_trans"]
     P = parts["fimg"].shape[1]
     s = 2 * WORKLOAD["r_max"]
-    fimg = torch.from_numpy(parts["fimg"].view(np.float32)).to(dev)
-    ctf = torch.from_numpy(parts["ctf"]).to(dev)
-    minv = torch.from_numpy(parts["minv"]).to(dev)
-    scal = torch.from_numpy(parts["scalars"]).to(dev)
+    K = 1
+    peaks, src = measured_peaks()
+    # the burst tensor peak when the timed region ran at the maximum SM clock (no power cap
+    # bit it), the sustained one otherwise
+    at_max = bool(clocks.get("sm_mhz") and clocks.get("sm_max_mhz")
+                  and clocks["sm_mhz"] >= 0.97 * clocks["sm_max_mhz"] and "sw_power_cap" not in clocks["reasons"])
+    tensor_peak = peaks.get("bf16_tflops", 1590.0) if at_max else peaks.get("bf16_tflops_sustained", 1400.0)
+    peak_kind = "burst (timed region at the maximum SM clock)" if at_max else "sustained"
+    traffic_ok = kernel_sha() == TRAFFIC["kernel_sha"] and not args.profile_case
+    # the contraction runs over the nk window pixels inside the projection radius only
+    # (projections are zero outside); "executed" counts what the tensor cores did
+    nk = int(sum(1 for n in range(P) if (lambda i, x: x * x + (i if i < s // 2 + 1 else i - s) ** 2)(n // (s // 2 + 1), n % (s // 2 + 1)) <= (s // 2) ** 2))
+    kdim = (2 * nk + 63) // 64 * 64
+    if learned is None:
+        flops = 8.0 * K * O * T * P * B
+        gemm = float(stages[2])
+        if mode == t2b.DIFF2_SPLIT_BF16:
+            peak = tensor_peak
+            bound = "tensor"
+        else:
+            peak = 148 * 128 * 2 * 1.965e-3  # FP32 SIMT nominal TFLOP/s (no measured figure)
+            bound = "fp32_simt"
+            src, peak_kind = "nominal", "FP32 FMA nominal"
+        achieved = flops / (gemm / 1000.0) / 1e12
+        executed = (12.0 if mode == t2b.DIFF2_SPLIT_BF16 else 4.0) * K * O * T * nk * B / (gemm / 1000.0) / 1e12
+        traffic = TRAFFIC["splitbf16_per128"] * B / 128.0 if (mode == t2b.DIFF2_SPLIT_BF16 and traffic_ok) else None
+        roof = {"bound": bound, "kernel": "k_diff2_tc" if mode else "k_diff2_simt", "achieved": achieved,
+                "executed_tflops": executed, "contraction_pixels": nk,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src, "peak_kind": peak_kind,
+                "traffic": traffic, "flops_per_launch": flops}
+    else:
+        # learned: the audit's full coarse contraction (audited particles x every orientation)
+        # and the contraction on the proposals (every particle x its top-k), each one launch of
+        # k_diff2_tc per step, timed by the library's CUDA events around exactly those launches
+        # over the stage-timed steps, each with its own audited count
+        t_audit, t_prop = float(stages[7]), float(stages[8])
+        t_sum = float(np.sum(stage_steps[:, 7] + stage_steps[:, 8])) / 1000.0
+        f_prop = 8.0 * PROP["topk"] * T * P * B
+        f_sum = sum(8.0 * K * O * T * P * na + f_prop for na in audited)
+        # audit launch: 128-row tiles over every orientation; na_max slots of T columns in
+        # 256-column tiles, or one narrower tile of (na_max - 1) slots when fewer were audited
+        na_max = int(np.ceil(B / PROP["audit_every"]))
+        tn_n = ((na_max - 1) * T + 31) // 32 * 32 if na_max > 1 else 0
+        tile_flops = 128 * 256 * kdim * 2 * 3.0
+
+        def audit_tiles(na):
+            if na == 0:
+                return 0.0
+            narrow = na < na_max and 0 < tn_n <= 256 and tn_n < (na_max * T + 255) // 256 * 256
+            return ((K * O + 127) // 128) * (tn_n / 256.0 if narrow else (na_max * T + 255) // 256)
+        # proposal tiles: 128 rows of 128 / kslot particles x T phase rows padded to 32 columns
+        ppt = 2 if PROP["topk"] <= 64 else 1
+        prop_exec = ((B + ppt - 1) // ppt) * 128 * ((T + 31) // 32 * 32) * kdim * 2 * 3.0
+        executed = sum(audit_tiles(na) * tile_flops + prop_exec for na in audited) / t_sum / 1e12
+        achieved = f_sum / t_sum / 1e12
+        na = float(np.mean(audited))
+        roof = {"bound": "tensor", "kernel": "k_diff2_tc (audit + proposal launches)", "achieved": achieved,
+                "executed_tflops": executed, "contraction_pixels": nk, "peak": tensor_peak, "unit": "TFLOP/s",
+                "frac": achieved / tensor_peak, "peak_source": src, "peak_kind": peak_kind,
+                "traffic": TRAFFIC["learned"] if traffic_ok else None,
+                "flops_per_launch": f_sum / (2.0 * len(audited)), "audit_ms": t_audit, "proposal_ms": t_prop,
+                "audited_particles": na}
+    roof["traffic_capture"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel source (sha256 "
+                               f"{TRAFFIC['kernel_sha']})" if roof["traffic"] is not None else
+                               "no capture of this kernel source")
+    line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": timing["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16x3/f64" if mode else "f32/f64",
+            "data": "synthetic (seeded blob map, CTF, white noise; stands in for the reference's datasets)",
+            "config": workload_config(), "particles_per_step": B,
+            "run": {"diff2": args.mode, "l2": "working set > L2 (bf16 hi/lo projection operands 0.97 GB per step)"},
+            "e2e": e2e, "gpu_launches": timing["gpu_launches"], "clocks": clocks, "roofline": roof,
+            "stage_ms": {n: float(v) for n, v in zip(
+                ["prep_network", "operands_audit_norms", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
+                 "wsum_bp", "audit_contraction", "proposal_contraction"], stages)},
+            "nr_sign_mean": float(timing["res"]["nr_sign"].double().mean())}
+    if tuned is not None:
+        line["run"]["tile_shapes"] = tuned
+    if learned is not None:
+        learned["learned_fraction"] = float(hres["learned"].double().mean())
+        line["run"]["learned"] = learned
+    if args.mode != "plain" and not args.no_plain:
+        # the metric's comparator, in the same run: the plain FP32 SIMT coarse pass on the same
+        # batch, timed the same way (device and end to end), then the learned path's quality
+        # against it on QUALITY_PARTICLES other particles
+        es_plain = setup_context(t2b, sy, fmap, samp, t2b.DIFF2_PLAIN_FP32, B, device=local)
+        if tuned is not None:
+            es_plain.tune_set(**{k: tuned[k] for k in ("diff2_tn", "diff2_group", "fine_ctas_per_sm",
+                                                        "wsum_ctas_per_sm", "project_pixels", "project_orients")})
+        pt = time_device(es_plain, parts, B, PLAIN_STEPS, 3, local, world, t2b)
+        pe, _, _ = time_e2e(es_plain, parts, B, PLAIN_STEPS, world, t2b, min_steps=PLAIN_STEPS)
+        line["plain"] = {"value": pt["value"], "ms_per_step": pt["ms_per_step"], "steps": PLAIN_STEPS,
+                         "e2e": {"value": pe["value"], "synchronous_value": pe["synchronous_value"]},
+                         "clocks": pt["clocks"]}
+        line["vs_baseline"] = value / pt["value"]
+        line["vs_baseline_definition"] = ("value / plain.value: the plain FP32 GPU path timed in this run "
+                                          "(no published number exists for this metric)")
+        line["vs_plain_e2e"] = e2e["value"] / pe["value"]
+        if rank == 0 and learned is not None:
+            line["quality_vs_plain"] = quality_vs_plain(es, es_plain, sy, fmap, QUALITY_PARTICLES, B,
+                                                        WORKLOAD["seed"] + 5000 + 1000 * rank)
+        es_plain.close()
+    if world > 1:
+        line["exchange"] = exchange_once(es, world, t2b)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    es.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def result_tensors(B, K, nd, dev):
+    import torch
     half = WORKLOAD["ori_size"] // 2 + 1
-    K, nd = 1, samp["n_dir"]
-    res = {k: torch.zeros(shape, dtype=dt, device=dev) for k, shape, dt in [
+    return {k: torch.zeros(shape, dtype=dt, device=dev) for k, shape, dt in [
         ("min_diff2", B, torch.float64), ("sum_weight", B, torch.float64), ("sig_weight", B, torch.float64),
         ("coarse_sum_weight", B, torch.float64), ("coarse_sig_weight", B, torch.float64),
         ("nr_sign", B, torch.int64), ("n_coarse_sig", B, torch.int64), ("pmax", B, torch.float64),
@@ -630,6 +815,18 @@ def main():
         ("wsum_sigma2_offset", B, torch.float64), ("wsum_sigma2", (B, half), torch.float64),
         ("wsum_pdf_class", (B, K), torch.float64), ("wsum_pdf_dir", (B, K * nd), torch.float64),
         ("status", B, torch.int32), ("audit_mass", B, torch.float64), ("learned", B, torch.int32)]}
+
+
+def time_device(es, parts, B, steps, warmup, local, world, t2b):
+    """`steps` E-steps of the batch through the device entry point (inputs resident in HBM),
+    CUDA events on the launching stream, barrier + synchronize on both sides, max over ranks."""
+    import torch
+    dev = torch.device("cuda", local)
+    fimg = torch.from_numpy(parts["fimg"].view(np.float32)).to(dev)
+    ctf = torch.from_numpy(parts["ctf"]).to(dev)
+    minv = torch.from_numpy(parts["minv"]).to(dev)
+    scal = torch.from_numpy(parts["scalars"]).to(dev)
+    res = result_tensors(B, es.cfg["nr_classes"], es.cfg["n_dir"], dev)
     rptr = {k: ctypes.c_void_p(v.data_ptr()) for k, v in res.items()}
     # an explicit stream: the library runs a NULL stream argument on its own stream
     stream = torch.cuda.Stream(dev)
@@ -640,13 +837,12 @@ def main():
                               ctypes.c_void_p(minv.data_ptr()), ctypes.c_void_p(scal.data_ptr()), rptr,
                               stream=stream.cuda_stream)
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         step()
     torch.cuda.synchronize()
     assert stream.cuda_stream != 0
     if int(res["status"].ne(0).sum()) != 0:
         raise RuntimeError(f"E-step status errors: {res['status'].cpu().numpy()}")
-    gemm_ms = []
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -654,34 +850,39 @@ def main():
     with ClockSampler(local) as clk:
         torch.cuda.nvtx.range_push("timed_steps")   # lets a profiler select the timed launches
         ev0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
     # kernel nodes of the captured step graph, times the timed steps
-    gpu_launches = es.launch_count() * args.steps if es.launch_count() > 0 else None
+    gpu_launches = es.launch_count() * steps if es.launch_count() > 0 else None
     total_ms = ev0.elapsed_time(ev1)
     if world > 1:
         torch.distributed.barrier()
     total_ms = max_over_ranks(total_ms, world)
-    ms_per_step = total_ms / args.steps
-    value = B * args.steps * world / (total_ms / 1000.0)
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    return {"value": B * steps * world / (total_ms / 1000.0), "ms_per_step": total_ms / steps,
+            "gpu_launches": gpu_launches, "clocks": clk.summary(), "res": res}
 
-    # end to end through the host entry point (pinned host buffers)
+
+def time_e2e(es, parts, B, steps, world, t2b, min_steps=E2E_STEPS):
+    """The same metric end to end through the host entry points with pinned host buffers:
+    H2D of each step's batch and D2H of its results inside the timed region, host wall clock,
+    median of 3 runs.  Returns (e2e dict, pinned inputs, pinned results)."""
+    import torch
     pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
            [("fimg", parts["fimg"].view(np.float32)), ("ctf", parts["ctf"]), ("minv", parts["minv"]),
             ("scal", parts["scalars"])]}
-    hres = {k: torch.zeros(v.shape, dtype=v.dtype).pin_memory() for k, v in res.items()}
+    hres = {k: v.pin_memory() for k, v in result_tensors(B, es.cfg["nr_classes"], es.cfg["n_dir"], "cpu").items()}
     lib = t2b.lib
     batch = t2b.Batch(B, 0, ctypes.c_void_p(pin["fimg"].data_ptr()), None, ctypes.c_void_p(pin["ctf"].data_ptr()),
                       ctypes.c_void_p(pin["minv"].data_ptr()), ctypes.c_void_p(pin["scal"].data_ptr()))
-    result = t2b.Result(*[ctypes.c_void_p(hres[n].data_ptr()) for n, _ in t2b.Result._fields_])
+    result = t2b.Result(*[ctypes.c_void_p(hres[n].data_ptr()) if n in hres else None for n, _ in t2b.Result._fields_])
+    ticket = ctypes.c_longlong(-1)
 
     def e2e_step():
         t2b._check(lib.t2b_estep_batch_host(es._h, ctypes.byref(batch), ctypes.byref(result)))
-
-    ticket = ctypes.c_longlong(-1)
 
     def e2e_submit():
         t2b._check(lib.t2b_estep_submit_host(es._h, ctypes.byref(batch), ctypes.byref(result), ctypes.byref(ticket)))
@@ -690,9 +891,7 @@ def main():
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
-    # host wall clock over E2E_STEPS steps, the median of three runs (a run of a few
-    # milliseconds is at the mercy of one host scheduling hiccup)
-    n_e2e = max(args.steps, E2E_STEPS)
+    n_e2e = max(steps, min_steps)
 
     def timed(loop):
         runs = []
@@ -722,111 +921,29 @@ def main():
 
     sync_s = timed(sync_loop)
     e2e_s = timed(pipelined_loop)
-    # per-stage device times (CUDA events around each stage) of separately synchronised
-    # host-path steps; not part of `value`
-    # (one period of the audit pattern when learned: each step's audited count is kept)
-    stage_steps, audited = [], []
-    es.stage_timing(True)
-    for _ in range(min(25, args.steps)):
-        e2e_step()
-        stage_steps.append(es.stage_ms())
-        audited.append(int((hres["audit_mass"].numpy() >= 0).sum()))
-    es.stage_timing(False)
-    stage_steps = np.array(stage_steps)
-    stages = np.mean(stage_steps, axis=0)
     h2d = sum(v.numel() * v.element_size() for v in pin.values())
     d2h = sum(v.numel() * v.element_size() for v in hres.values())
-    e2e = {"value": B * n_e2e * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h, "api": "t2b_estep_submit_host + t2b_estep_wait (one step in flight)",
-           "steps": n_e2e, "timing": "host wall clock, median of 3 runs",
-           "synchronous_value": B * n_e2e * world / sync_s}
+    return ({"value": B * n_e2e * world / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
+             "d2h_bytes_per_step": d2h, "api": "t2b_estep_submit_host + t2b_estep_wait (one step in flight)",
+             "steps": n_e2e, "timing": "host wall clock, median of 3 runs",
+             "synchronous_value": B * n_e2e * world / sync_s}, pin, hres)
 
-    # roofline of the dominant kernel (the tcgen05 contraction k_diff2_tc)
-    O, T = samp["n_dir"] * samp["n_psi"], samp["n_trans"]
-    peaks, src = measured_peaks()
-    # the contraction runs over the nk window pixels inside the projection radius only
-    # (projections are zero outside); "executed" counts what the tensor cores did
-    nk = int(sum(1 for n in range(P) if (lambda i, x: x * x + (i if i < s // 2 + 1 else i - s) ** 2)(n // (s // 2 + 1), n % (s // 2 + 1)) <= (s // 2) ** 2))
-    kdim = (2 * nk + 63) // 64 * 64
-    if learned is None:
-        flops = 8.0 * K * O * T * P * B
-        gemm = float(stages[2])
-        if mode == t2b.DIFF2_SPLIT_BF16:
-            peak = peaks.get("bf16_tflops_sustained", 1400.0)
-            bound = "tensor"
-        else:
-            peak = 148 * 128 * 2 * 1.965e-3  # FP32 SIMT nominal TFLOP/s (no measured figure)
-            bound = "fp32_simt"
-            src = "nominal"
-        achieved = flops / (gemm / 1000.0) / 1e12
-        executed = (12.0 if mode == t2b.DIFF2_SPLIT_BF16 else 4.0) * K * O * T * nk * B / (gemm / 1000.0) / 1e12
-        # DRAM bytes (read + write) of one diff2 launch of this exact workload from one ncu capture
-        # (dram__bytes_read.sum 8.16 GB + dram__bytes_write.sum 1.56 GB at 128 particles;
-        # profiles/k_diff2_tc_box128_order3_b128_dram.md), scaled by the batch size
-        traffic = None
-        if mode == t2b.DIFF2_SPLIT_BF16 and not args.profile_case:
-            traffic = (8.16e9 + 1.56e9) * B / 128.0
-        roof = {"bound": bound, "kernel": "k_diff2_tc" if mode else "k_diff2_simt", "achieved": achieved,
-                "executed_tflops": executed, "contraction_pixels": nk,
-                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src,
-                "traffic": traffic, "flops_per_launch": flops}
-    else:
-        # learned: the audit's full coarse contraction (audited particles x every orientation)
-        # and the contraction on the proposals (every particle x its top-k), each one launch of
-        # k_diff2_tc per step, timed by the library's CUDA events around exactly those launches
-        # over the stage-timed steps, each with its own audited count
-        t_audit, t_prop = float(stages[7]), float(stages[8])
-        t_sum = float(np.sum(stage_steps[:, 7] + stage_steps[:, 8])) / 1000.0
-        f_prop = 8.0 * PROP["topk"] * T * P * B
-        f_sum = sum(8.0 * K * O * T * P * na + f_prop for na in audited)
-        # audit launch: 128-row tiles over every orientation; na_max slots of T columns in
-        # 256-column tiles, or one narrower tile of (na_max - 1) slots when fewer were audited
-        na_max = int(np.ceil(B / PROP["audit_every"]))
-        tn_n = ((na_max - 1) * T + 31) // 32 * 32 if na_max > 1 else 0
-        tile_flops = 128 * 256 * kdim * 2 * 3.0
 
-        def audit_tiles(na):
-            if na == 0:
-                return 0.0
-            narrow = na < na_max and 0 < tn_n <= 256 and tn_n < (na_max * T + 255) // 256 * 256
-            return ((K * O + 127) // 128) * (tn_n / 256.0 if narrow else (na_max * T + 255) // 256)
-        # proposal tiles: 128 rows of 128 / kslot particles x T phase rows padded to 32 columns
-        ppt = 2 if PROP["topk"] <= 64 else 1
-        prop_exec = ((B + ppt - 1) // ppt) * 128 * ((T + 31) // 32 * 32) * kdim * 2 * 3.0
-        executed = sum(audit_tiles(na) * tile_flops + prop_exec for na in audited) / t_sum / 1e12
-        peak = peaks.get("bf16_tflops_sustained", 1400.0)
-        achieved = f_sum / t_sum / 1e12
-        na = float(np.mean(audited))
-        roof = {"bound": "tensor", "kernel": "k_diff2_tc (audit + proposal launches)", "achieved": achieved,
-                "executed_tflops": executed, "contraction_pixels": nk, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "peak_source": src, "traffic": LEARNED_TRAFFIC,
-                "flops_per_launch": f_sum / (2.0 * len(audited)), "audit_ms": t_audit, "proposal_ms": t_prop,
-                "audited_particles": na}
-    line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+bf16x3/f64" if mode else "f32/f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD["name"], "particles_per_step": B, "diff2": args.mode,
-                       "orientations": O, "translations": T, "pixels": P,
-                       "l2": "working set > L2 (bf16 hi/lo projection operands 0.97 GB per step)"},
-            "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk.summary(), "roofline": roof,
-            "stage_ms": {n: float(v) for n, v in zip(
-                ["prep_network", "operands_audit_norms", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
-                 "wsum_bp", "audit_contraction", "proposal_contraction"], stages)},
-            "nr_sign_mean": float(res["nr_sign"].double().mean())}
-    if tuned is not None:
-        line["config"]["tile_shapes"] = tuned
-    if learned is not None:
-        learned["learned_fraction"] = float(hres["learned"].double().mean())
-        learned.update(quality_vs_full(es, parts))
-        line["config"]["learned"] = learned
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sy, fmap, samp, parts)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    es.close()
-    if world > 1:
-        torch.distributed.destroy_process_group()
-
+def exchange_once(es, world, t2b):
+    """The iteration's one exchange, after the timed region: the backprojection grids summed
+    over each gold-standard half in place (NCCL all-reduce on the library's device grids)."""
+    import torch
+    import t2relion_b200.parallel as par
+    halves = par.gold_standard_groups(world)
+    torch.cuda.synchronize()
+    torch.distributed.barrier()
+    t0 = time.perf_counter()
+    par.allreduce_grids_(es, es.cfg["nr_classes"], group=halves.mine)
+    torch.cuda.synchronize()
+    dt = max_over_ranks(time.perf_counter() - t0, world)
+    nvox = int(np.prod(es._grid_shape))
+    return {"what": "in-place all-reduce of the grids (data + weight) within each gold-standard half",
+            "bytes_per_rank": 12 * nvox * es.cfg["nr_classes"], "ms": dt * 1e3, "halves": halves.sizes}
 
 if __name__ == "__main__":
     main()

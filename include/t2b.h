@@ -178,7 +178,9 @@ int t2b_estep_batch_device(t2b_ctx* ctx, const t2b_batch* batch, const t2b_resul
  * the previous batch computes, and its results are read back on a third stream while
  * the next one computes; batches run and write their results in submission order.  The batch's host inputs and result arrays must stay valid and untouched
  * until t2b_estep_wait(ctx, ticket) (or a later ticket, or -1 = every batch) returns.
- * t2b_estep_batch_host is submit followed by wait. */
+ * t2b_estep_batch_host is submit followed by wait.  The batch's input and result
+ * arrays must be pinned host memory (cudaHostAlloc / cudaHostRegister) for batches to
+ * overlap: copies from or into pageable memory make the call wait for them. */
 int t2b_estep_submit_host(t2b_ctx* ctx, const t2b_batch* batch, const t2b_result* out, long long* ticket);
 int t2b_estep_wait(t2b_ctx* ctx, long long ticket);
 
@@ -251,14 +253,21 @@ int t2b_update_ssnr(t2b_ctx* ctx, int iclass, const t2b_ssnr_config* cfg, double
  * memory, and cudaMalloc/cudaFree would synchronise the whole device under
  * work running on other streams.  Everything is caller-owned device memory:
  * `data` (complex interleaved) and `weight` are a centred 3D grid as returned
- * by t2b_backprojector_device_ptrs; `fconv` receives [pad][pad][pad/2+1]
- * complex doubles.  Enqueued on `stream` (cudaStream_t, NULL = legacy default
+ * by t2b_backprojector_device_ptrs (3D only: zdim == ydim, xdim == ydim/2+1);
+ * `fconv` receives [ydim][ydim][ydim/2+1] complex doubles in FFTW order, ydim
+ * being the padded grid size (pad_size, e.g. 259), not the padding factor.  Enqueued on `stream` (cudaStream_t, NULL = legacy default
  * stream); no cudaMalloc, cudaFree or allocating library call.  Scratch (the
  * radial weight averages) is a fixed device array of 2 * T2B_NOALLOC_MAX_RMAX
  * doubles per device, shared by all calls and cleared by each: calls on one
  * device must not overlap on the GPU.  r_max > T2B_NOALLOC_MAX_RMAX returns
- * T2B_ERR_ARG.  The first call on a device resolves the scratch address; make
- * it before any stream capture. */
+ * T2B_ERR_ARG.  Once per device the scratch address is resolved and the
+ * division's kernels are loaded (lazy module loading: device memory for the code
+ * and the array, possibly a context synchronisation): t2b_create does this for
+ * its device; without a context, the first call on a device does it, so make that
+ * call at set-up, before any stream capture and before an arena allocator
+ * reserves the device's memory.  The grid must be complete: a context's grid is
+ * written by batches on the context's own streams, so wait for them
+ * (t2b_estep_wait(ctx, -1), or order `stream` after the context's work) first. */
 int t2b_reconstruct_divide_noalloc(const float* data, const float* weight, int xdim, int ydim, int zdim,
                                    int inity, int initz, int r_max, int padding_factor, double* fconv,
                                    void* stream);

@@ -92,6 +92,13 @@ int t2b_create(int device, t2b_ctx** out)
         }
         for (auto& ev : c->ev) cudaEventCreate(&ev);
         for (auto& ev : c->handoff) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        // the allocation-free division's once-per-device set-up, here where allocating is fine
+        try {
+            noalloc_prepare_current_device();
+        } catch (...) {
+            t2b_destroy(c);
+            throw;
+        }
         *out = c;
     });
 }

@@ -15,9 +15,14 @@
 // device whose kernels overlap on the GPU race on it: serialise them (one
 // stream, or events).  r_max is limited to T2B_NOALLOC_MAX_RMAX.
 //
-// The first call on a device looks up the device address of the array
-// (cudaGetSymbolAddress, with that device current) and caches it; make that
-// first call before any stream capture.
+// The set-up of a device -- the device address of the array (cudaGetSymbolAddress,
+// with that device current), cached, and the loading of the division's four kernels
+// (with CUDA's lazy module loading, the first launch of a kernel loads its module,
+// which takes device memory for the code and the array and can synchronise the
+// context) -- runs once per device: in t2b_create for the context's device, else in
+// the entry point's first call on that device.  A caller without a context makes that
+// first call at its own set-up: before any stream capture, and before an arena
+// allocator reserves the device's free memory.
 #include "t2b_internal.cuh"
 #include <mutex>
 
@@ -31,22 +36,6 @@ static __device__ __align__(256) double g_noalloc_scratch[2 * MAX_RMAX];
 constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
 double* g_addr[MAX_DEVICES] = {};
-
-double* scratch_for_current_device()
-{
-    int dev = 0;
-    T2B_CUDA(cudaGetDevice(&dev));
-    T2B_REQUIRE(dev >= 0 && dev < MAX_DEVICES, T2B_ERR_UNSUPPORTED, "device index beyond the scratch table");
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            throw Error{T2B_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
-        g_addr[dev] = static_cast<double*>(p);
-    }
-    return g_addr[dev];
-}
 
 struct Geo {
     int xdim, ydim, zdim, inity, initz, r_max, pad;
@@ -115,7 +104,36 @@ __global__ void k_na_divide(Geo g, const float2* __restrict__ data, const float*
     out[n] = v;
 }
 
+// Set-up of the current device (once): the scratch array's device address, and every
+// kernel of the division loaded (cudaFuncGetAttributes loads a kernel's module).
+double* scratch_for_current_device()
+{
+    int dev = 0;
+    T2B_CUDA(cudaGetDevice(&dev));
+    T2B_REQUIRE(dev >= 0 && dev < MAX_DEVICES, T2B_ERR_UNSUPPORTED, "device index beyond the scratch table");
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            throw Error{T2B_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
+        cudaFuncAttributes fa;
+        for (const void* k : {(const void*)k_na_clear, (const void*)k_na_radial, (const void*)k_na_radnorm,
+                              (const void*)k_na_divide})
+            T2B_CUDA(cudaFuncGetAttributes(&fa, k));
+        g_addr[dev] = static_cast<double*>(p);
+    }
+    return g_addr[dev];
+}
+
 }  // namespace
+
+// t2b_create's part of the set-up: the context's device is current.
+void noalloc_prepare_current_device()
+{
+    (void)scratch_for_current_device();
+}
+
 }  // namespace t2b
 
 using namespace t2b;

@@ -264,6 +264,7 @@ void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool
 
 namespace t2b {
 void imageprep_release(t2b_ctx* c);   // context destruction (imageprep.cu)
+void noalloc_prepare_current_device(); // set-up of t2b_reconstruct_divide_noalloc (noalloc.cu)
 }
 
 struct t2b_ctx {

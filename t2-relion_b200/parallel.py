@@ -55,15 +55,16 @@ def _release(ptr):
 
 
 def device_view(ptr, n_floats, device):
-    """A float32 torch tensor aliasing `n_floats` floats of CUDA memory at `ptr`.
+    """A float32 torch tensor aliasing `n_floats` floats at `ptr`: CUDA memory of device
+    `device` (an int), or host memory when `device` is "cpu".
 
-    The memory stays owned by the library; the view must not outlive it.
+    The memory stays owned by whoever allocated it; the view must not outlive it.
     """
     import torch
     shape = (ctypes.c_int64 * 1)(n_floats)
     mt = _DLManagedTensor()
     mt.dl_tensor.data = ptr
-    mt.dl_tensor.device = _DLDevice(2, device)  # kDLCUDA
+    mt.dl_tensor.device = _DLDevice(1, 0) if device == "cpu" else _DLDevice(2, device)  # kDLCPU / kDLCUDA
     mt.dl_tensor.ndim = 1
     mt.dl_tensor.dtype = _DLDataType(2, 32, 1)  # kDLFloat, 32 bits
     mt.dl_tensor.shape = shape
@@ -79,16 +80,71 @@ def device_view(ptr, n_floats, device):
     return torch.utils.dlpack.from_dlpack(cap)
 
 
-def allreduce_grids_(estep, nr_classes, group=None):
-    """Sum the device BP grids of every class over the ranks of `group`, in place."""
+def allreduce_grids_(grids, nr_classes, group=None):
+    """Sum the BP grids of every class over the ranks of `group`, in place (FP32, as the
+    device grids hold them).
+
+    `grids`: a t2relion_b200.EStep (the library's device grids, t2b_backprojector_device_ptrs;
+    NCCL over NVLink) or any object with the same backprojector_device_ptrs(k) and _grid_shape
+    whose `device` attribute is "cpu" (host grids; gloo).  The views alias the memory: no
+    copy, the reduction writes the grids themselves.
+    """
     import torch
     import torch.distributed as dist
-    dev = torch.cuda.current_device()
+    dev = getattr(grids, "device", None)
+    if dev != "cpu":
+        dev = torch.cuda.current_device()
+    nvox = int(np.prod(grids._grid_shape))
     for k in range(nr_classes):
-        data_ptr, w_ptr = estep.backprojector_device_ptrs(k)
-        nvox = int(np.prod(estep._grid_shape))
+        data_ptr, w_ptr = grids.backprojector_device_ptrs(k)
         for ptr, n in ((data_ptr, 2 * nvox), (w_ptr, nvox)):
             dist.all_reduce(device_view(ptr, n, dev), op=dist.ReduceOp.SUM, group=group)
+
+
+class Halves:
+    """The two gold-standard halves of one job as process groups."""
+
+    def __init__(self, groups, ranks, rank):
+        self.groups, self.ranks = groups, ranks
+        self.index = 0 if rank in ranks[0] else 1     # 0: random subset 1, 1: random subset 2
+        self.mine = groups[self.index]
+        self.sizes = [len(r) for r in ranks]
+
+
+def half_of(rank):
+    """Random subset (1 or 2) of torch rank `rank`.  Rank r plays the reference's follower r + 1;
+    followers of odd MPI rank form subset 1, even ones subset 2 (MpiNode::myRandomSubset,
+    src/mpi.cpp:90-96), and each subset's weighted sums and grids are summed over its own
+    followers only (combineAllWeightedSums, src/ml_optimiser_mpi.cpp:1732-1830)."""
+    return 1 if rank % 2 == 0 else 2
+
+
+def gold_standard_groups(world, rank=None):
+    """Process groups of the two halves (every rank creates both: dist.new_group is collective).
+    A world of one rank has one group holding both halves' data (no exchange is needed)."""
+    import torch.distributed as dist
+    rank = dist.get_rank() if rank is None else rank
+    ranks = [[r for r in range(world) if half_of(r) == h] for h in (1, 2)]
+    groups = [dist.new_group(r) if r else None for r in ranks]
+    return Halves(groups, ranks, rank)
+
+
+class HostGrids:
+    """Backprojection grids in host memory with the EStep grid interface (float32 data
+    interleaved re/im and weight, [K] x grid), for the exchange on CPU ranks (gloo)."""
+    device = "cpu"
+
+    def __init__(self, data, weight):
+        w = np.asarray(weight)
+        self._grid_shape = w.shape[1:]
+        self.data = np.ascontiguousarray(np.stack([np.asarray(data).real, np.asarray(data).imag], -1), np.float32)
+        self.weight = np.ascontiguousarray(w, np.float32)
+
+    def backprojector_device_ptrs(self, k):
+        return self.data[k].ctypes.data, self.weight[k].ctypes.data
+
+    def grids(self):
+        return self.data[..., 0] + 1j * self.data[..., 1], self.weight
 
 
 # per-particle fields of a result dict that are summed into the model

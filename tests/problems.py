@@ -97,3 +97,54 @@ def shells_of(shape):
         kx = np.arange(x)[None, :]
         r = np.sqrt(ky * ky + kx * kx)
     return np.rint(r).astype(int).reshape(-1)
+
+
+# The benchmarked workload: box 128, 1.3 A/px, 40-blob map (seed 11), HEALPix order 3 x psi
+# 7.5 deg, adaptive oversampling 1, translations range 5 step 1, Fourier radius 40, 2x padded
+# backprojection grid of r_max 64, white noise at SNR 0.03.
+BOX128 = dict(ori_size=128, angpix=1.3, n_blobs=40, map_seed=11, order=3, psi_step=7.5, offset_range=5,
+              offset_step=1, r_max=40, bp_r_max=64, snr=0.03)
+
+
+def box128(n_particles, seed, data_vs_prior=None):
+    """Inputs, sampling and an oracle Problem of the box-128 workload (n particles, seed)."""
+    t2b = load_package()
+    import t2relion_b200.synthetic as sy
+    import oracle as orc
+    w = BOX128
+    N, r = w["ori_size"], w["r_max"]
+    s = 2 * r
+    fmap = sy.fourier_map(sy.blob_volume(N, w["n_blobs"], seed=w["map_seed"]), r)
+    samp = t2b.sampling(3, w["order"], w["psi_step"], 1, w["offset_range"], w["offset_step"], w["angpix"])
+    parts = sy.make_particles(fmap, n_particles, ori_size=N, s=s, r_max=r, angpix=w["angpix"], snr=w["snr"],
+                              seed=seed, max_shift=w["offset_range"])
+    pdf_dir = np.full((1, samp["n_dir"]), 1.0 / samp["n_dir"])
+    sigma2_offset = (w["offset_range"] * w["angpix"]) ** 2
+    ps = sy.pad_size(w["bp_r_max"])
+    prob = orc.Problem(ori_size=N, s=s, ref_dim=3, maps=[fmap], r_max=r, pad=2, samp=samp, pdf_direction=pdf_dir,
+                       pdf_class=np.ones(1), sigma2_offset=sigma2_offset, pixel_size=w["angpix"],
+                       adaptive_fraction=0.999, ovs=1, bp_pad_size=ps, bp_r_max=w["bp_r_max"],
+                       data_vs_prior=data_vs_prior)
+    oparts = prob.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], sy.mresol(s))
+
+    def product(diff2_mode, max_batch=None, use_graph=1):
+        es = t2b.EStep(0)
+        es.set_projector(0, fmap, 3, r, 2)
+        es.init_backprojector(0, 3, ps, w["bp_r_max"], 2)
+        es.configure(ori_size=N, current_size=s, ref_dim=3, nr_classes=1, samp=samp, pdf_direction=pdf_dir,
+                     pdf_class=np.ones(1), sigma2_offset=sigma2_offset, pixel_size=w["angpix"],
+                     adaptive_oversampling=1, diff2_mode=diff2_mode, max_batch=max_batch or n_particles,
+                     use_graph=use_graph, data_vs_prior=data_vs_prior)
+        return es
+
+    return dict(t2b=t2b, sy=sy, fmap=fmap, samp=samp, parts=parts, prob=prob, oparts=oparts, product=product,
+                pad_size=ps)
+
+
+def input_digest(parts):
+    """SHA-256 of the E-step inputs (detects a change of the generator)."""
+    import hashlib
+    h = hashlib.sha256()
+    for k in ("fimg", "ctf", "minv", "scalars"):
+        h.update(np.ascontiguousarray(parts[k]).tobytes())
+    return h.hexdigest()

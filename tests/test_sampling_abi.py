@@ -91,3 +91,18 @@ def test_cpp_adapter_compiles_and_links(tmp_path):
                         "-Wl,--unresolved-symbols=ignore-in-shared-libs", "-o", str(out)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("order,psi,rng,angpix", [(1, 15.0, 3, 2.0), (3, 7.5, 5, 1.3)])
+def test_sampling_matches_oracle_restatement(t2b, order, psi, rng, angpix):
+    """The library's sampler against the oracle's numpy restatement of HealpixSampling (the lists
+    the reference arm of the benchmark uses): identical translations, matrices within 1e-15."""
+    import sampling_oracle as so
+    a = t2b.sampling(3, order, psi, 1, rng, 1, angpix)
+    b = so.sampling(order, psi, 1, rng, 1, angpix)
+    for k in ("n_dir", "n_psi", "n_trans", "nover_rot", "nover_trans"):
+        assert a[k] == b[k], k
+    for k in ("trans_px", "trans_px_fine", "trans_prior"):
+        assert np.array_equal(a[k], b[k]), k
+    for k in ("eul_coarse", "eul_fine"):
+        assert np.max(np.abs(a[k] - b[k])) <= 1e-15, k

@@ -41,6 +41,46 @@ def test_noalloc_division_matches_allocating_entry_point():
     es.close()
 
 
+def _noalloc(t2b, data_ptr, w_ptr, ps, r, stream):
+    import torch
+    out = torch.full((ps, ps, ps // 2 + 1, 2), float("nan"), dtype=torch.float64, device="cuda")
+    rc = t2b.lib.t2b_reconstruct_divide_noalloc(
+        ctypes.c_void_p(data_ptr), ctypes.c_void_p(w_ptr), ps // 2 + 1, ps, ps, -(ps // 2), -(ps // 2), r, 2,
+        ctypes.c_void_p(out.data_ptr()), None if stream is None else ctypes.c_void_p(stream.cuda_stream))
+    assert rc == t2b.T2B_OK, t2b.lib.t2b_last_error()
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    return got[..., 0] + 1j * got[..., 1]
+
+
+def test_noalloc_larger_then_smaller_grid():
+    """A grid of larger r_max, then the smaller one again on the legacy default stream
+    (stream NULL): each call clears what the previous one left in the shared array."""
+    import torch
+    pb = problems.build("refine_o1_ovs", n_particles=8, seed=6)
+    t2b, P, samp = pb["t2b"], pb["parts"], pb["samp"]
+    small = pb["product"]()
+    small.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    ref_small = small.reconstruct_divide(0)
+    big_r = pb["N"] // 2 - 4
+    big = t2b.EStep(0)
+    big.set_projector(0, pb["maps"][0], 3, pb["r"], 2)
+    ps_big = 2 * (2 * big_r + 1) + 1
+    big.init_backprojector(0, 3, ps_big, big_r, 2)
+    big.configure(ori_size=pb["N"], current_size=pb["s"], ref_dim=3, nr_classes=1, samp=samp,
+                  pdf_direction=np.ones((1, samp["n_dir"])) / samp["n_dir"], pdf_class=np.ones(1),
+                  sigma2_offset=36.0, pixel_size=2.0, adaptive_oversampling=1, diff2_mode=0, max_batch=8)
+    big.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    ref_big = big.reconstruct_divide(0)
+    stream = torch.cuda.Stream()
+    got = _noalloc(t2b, *big.backprojector_device_ptrs(0), ps_big, big_r, stream)
+    assert np.max(np.abs(got - ref_big)) <= 1e-12 * max(1.0, np.max(np.abs(ref_big)))
+    got = _noalloc(t2b, *small.backprojector_device_ptrs(0), pb["pad_size"], pb["r"], None)
+    assert np.max(np.abs(got - ref_small)) <= 1e-12 * max(1.0, np.max(np.abs(ref_small)))
+    big.close()
+    small.close()
+
+
 def test_noalloc_rejects_r_max_beyond_limit():
     pb = problems.build("refine_o1_ovs", n_particles=2, seed=5)
     t2b = pb["t2b"]
