@@ -219,3 +219,168 @@ def test_wsum_stage_alone_reproduces_the_estep(t2b, synth, oracle):
     assert np.array_equal(o["pose"], ra["pose"][0])
     assert np.array_equal(o["wsum_sigma2"], ra["wsum_sigma2"][0])
     assert np.array_equal(pb.bp_data, pa.bp_data) and np.array_equal(pb.bp_weight, pa.bp_weight)
+
+
+def _ref_stage_setup(b=0, seed=29):
+    """refine_o1_ovs problem, the oracle's own final-pass hypotheses of particle b, and the
+    reference kernels' shared operands (model, fine orientations, fine shift phases)."""
+    import problems
+    lib = _ref_acc()
+    f, i, p, ll = ctypes.c_float, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong
+    lib.ref_fine_diff2.argtypes = [p, i, i, i, i, i, i, i, p, i, p, p, p, i, i, p, p, i, f, i, p, p, p, p, ll, p]
+    lib.ref_wavg.argtypes = [p, i, i, i, i, i, i, i, p, i, p, p, p, i, i, p, p, i, p, f, f, p, p, p]
+    lib.ref_backproject.argtypes = [p, p, i, i, p, p, i, p, p, p, f, f, p, i, p, p, p, i, i, i, i, i, i, i]
+    for fn in (lib.ref_fine_diff2, lib.ref_wavg, lib.ref_backproject):
+        fn.restype = i
+    dvp = np.full((1, 33), 6.0)
+    dvp[0, 14:] = 1.0           # rings from 14 on out of the scale-correction sums
+    pb = problems.build("refine_o1_ovs", n_particles=2, seed=seed)
+    prob, op, samp, P = pb["prob"], pb["oparts"], pb["samp"], pb["parts"]
+    d2, mn = prob.coarse_diff2(op, b)
+    rc, w, sw, sig, _ = prob.weights(op, b, 0, d2, np.arange(d2.size), mn)
+    pairs, fd, fmn = prob.fine_diff2(op, b, (w >= sig).astype(np.uint8))
+    rc, wf, fsum, fsig, _ = prob.weights(op, b, 1, fd.reshape(-1), np.repeat(pairs, prob.RV), fmn)
+    fmap = pb["maps"][0]
+    N, s = pb["N"], pb["s"]
+    tpf = samp["trans_px_fine"]
+    op_ = dict(lib=lib, pb=pb, b=b, pairs=pairs, fd=fd, wf=wf, fsum=fsum, fsig=fsig, dvp=dvp,
+               mdl=np.ascontiguousarray(fmap.view(np.float32)), mshape=fmap.shape,
+               tx=np.ascontiguousarray(-2 * np.pi * tpf[:, 0] / N, np.float32),
+               ty=np.ascontiguousarray(-2 * np.pi * tpf[:, 1] / N, np.float32), xh=s // 2 + 1, s=s)
+    return op_
+
+
+def _dense_weights(st):
+    """The final weights as the reference's kernels take them: one row of every fine
+    translation per fine orientation holding a significant hypothesis (0 elsewhere)."""
+    pb, prob = st["pb"], st["pb"]["prob"]
+    R, V, T = prob.S.nover_rot, prob.S.nover_trans, prob.T
+    w = st["wf"].reshape(len(st["pairs"]), R, V)
+    rows = {}
+    for q, ih in enumerate(st["pairs"]):
+        o, t = divmod(int(ih), T)
+        for r in range(R):
+            for v in range(V):
+                if w[q, r, v] >= st["fsig"]:
+                    rows.setdefault(o * R + r, np.zeros(T * V))[t * V + v] = w[q, r, v]
+    rot = np.array(sorted(rows))
+    return rot, np.ascontiguousarray(np.stack([rows[k] for k in rot]), np.float32)
+
+
+def test_fine_diff2_matches_reference_cpu_kernel(oracle):
+    """The oracle's fine pass against CpuKernels::diff2_fine_2D<REF3D> (FP32) over the same
+    significant pairs, 8 rotations x 4 shifts each (the reference's FinePassWeights jobs)."""
+    st = _ref_stage_setup()
+    lib, pb, b = st["lib"], st["pb"], st["b"]
+    prob, samp, P = pb["prob"], pb["samp"], pb["parts"]
+    R, V, T = prob.S.nover_rot, prob.S.nover_trans, prob.T
+    pairs = st["pairs"]
+    eul = samp["eul_fine"].reshape(-1, 3, 3)
+    einv = np.ascontiguousarray(np.transpose(eul, (0, 2, 1)).reshape(-1, 9), np.float32)
+    nj = len(pairs) * R
+    rot_idx, trans_idx = np.zeros(nj * V, np.uint64), np.zeros(nj * V, np.uint64)
+    job_idx, job_num = np.zeros(nj, np.uint64), np.full(nj, V, np.uint64)
+    for q, ih in enumerate(pairs):
+        o, t = divmod(int(ih), T)
+        for r in range(R):
+            e0 = (q * R + r) * V
+            job_idx[q * R + r] = e0
+            rot_idx[e0:e0 + V] = o * R + r
+            trans_idx[e0:e0 + V] = t * V + np.arange(V)
+    ctf = P["ctf"][b].astype(np.float64)
+    X = P["fimg"][b].astype(np.complex128) / ctf
+    re, im = (np.ascontiguousarray(a, np.float32) for a in (X.real, X.imag))
+    corr = np.ascontiguousarray(P["minv"][b] * ctf * ctf, np.float32)
+    out = np.zeros(nj * V, np.float32)
+    mz, my, mx = st["mshape"]
+    rc = lib.ref_fine_diff2(st["mdl"].ctypes.data, mx, my, mz, -(my // 2), -(mz // 2), pb["r"], 2, einv.ctypes.data,
+                            einv.shape[0], re.ctypes.data, im.ctypes.data, corr.ctypes.data, st["xh"], st["s"],
+                            st["tx"].ctypes.data, st["ty"].ctypes.data, T * V, float(P["scalars"][b, 1] / 2), nj,
+                            rot_idx.ctypes.data, trans_idx.ctypes.data, job_idx.ctypes.data, job_num.ctypes.data,
+                            nj * V, out.ctypes.data)
+    assert rc == 0
+    ref = st["fd"].reshape(-1)
+    rel = np.abs(out.astype(np.float64) - ref) / np.abs(ref)
+    assert np.max(rel) < 5e-6, np.max(rel)
+    assert np.array_equal(np.argmin(out.reshape(-1, R * V), 1), np.argmin(st["fd"], 1))
+
+
+def test_weighted_sums_match_reference_cpu_kernel(oracle):
+    """The oracle's sigma2 ring sums and scale-correction XA / AA against CpuKernels::wavg_ref3D
+    (FP32, REFCTF) on the same final weights.  Rings 0-14: ring 16 holds the pixels on the
+    projection circle, where the reference tests the rotated radius in floating point and the
+    oracle the integer radius of the pixel (a documented convention of both paths)."""
+    st = _ref_stage_setup()
+    lib, pb, b = st["lib"], st["pb"], st["b"]
+    prob, samp, P = pb["prob"], pb["samp"], pb["parts"]
+    T, V = prob.T, prob.S.nover_trans
+    rot, wd = _dense_weights(st)
+    eul = samp["eul_fine"].reshape(-1, 3, 3)[rot]
+    einv = np.ascontiguousarray(np.transpose(eul, (0, 2, 1)).reshape(-1, 9), np.float32)
+    re, im = (np.ascontiguousarray(a, np.float32) for a in (P["fimg"][b].real, P["fimg"][b].imag))
+    ctf = np.ascontiguousarray(P["ctf"][b] * P["scalars"][b, 6], np.float32)
+    Pn = re.size
+    parts, xa, aa = np.zeros(Pn, np.float32), np.zeros(Pn, np.float32), np.zeros(Pn, np.float32)
+    mz, my, mx = st["mshape"]
+    rc = lib.ref_wavg(st["mdl"].ctypes.data, mx, my, mz, -(my // 2), -(mz // 2), pb["r"], 2, einv.ctypes.data,
+                      len(rot), re.ctypes.data, im.ctypes.data, ctf.ctypes.data, st["xh"], st["s"],
+                      st["tx"].ctypes.data, st["ty"].ctypes.data, T * V, wd.ctypes.data, float(st["fsum"]), 1e-38,
+                      parts.ctypes.data, xa.ctypes.data, aa.ctypes.data)
+    assert rc == 0
+    prob2 = oracle.Problem(ori_size=pb["N"], s=st["s"], ref_dim=3, maps=pb["maps"], r_max=pb["r"], pad=2,
+                           samp=samp, pdf_direction=np.ones((1, samp["n_dir"])), pdf_class=np.ones(1),
+                           sigma2_offset=36., pixel_size=2.0, adaptive_fraction=0.999, ovs=1,
+                           bp_pad_size=pb["pad_size"], bp_r_max=pb["r"], data_vs_prior=st["dvp"])
+    o = prob2.wsum_bp(pb["oparts"], b, st["pairs"], st["wf"], st["fsum"], st["fsig"])
+    mres = pb["sy"].mresol(st["s"])
+    ring = np.bincount(mres[mres >= 0], parts[mres >= 0].astype(np.float64), 33)
+    rel = np.abs(ring[:15] - o["wsum_sigma2"][:15]) / o["wsum_sigma2"][:15]
+    assert np.max(rel) < 1e-5, rel
+    sel = (mres >= 0) & (st["dvp"][0][np.maximum(mres, 0)] > 3.)
+    for k, arr in (("wsum_scale_xa", xa), ("wsum_scale_aa", aa)):
+        v = float(np.sum(arr[sel].astype(np.float64)))
+        assert abs(v - o[k]) <= 1e-5 * abs(o[k]), (k, v, o[k])
+
+
+def test_backprojection_matches_reference_cpu_kernel(oracle, synth):
+    """The oracle's backprojection (backproject2Dto3D) against CpuKernels::backprojectRef3D
+    (FP32) on the same final weights, compared after enforceHermitianSymmetry (the x = 0 plane's
+    Friedel choice is rounding noise in both).  Pixels the two paths treat differently by
+    construction carry zero Minvsigma2 here: the duplicated x = 0 column of negative y (the
+    CPU path skips it, src/backprojector.cpp:136-141; the accelerated kernels backproject
+    it) and the rim the accelerated kernel's x < floor(sqrt(r^2 - y^2)) leaves out."""
+    import recon_oracle as ro
+    st = _ref_stage_setup()
+    lib, pb, b = st["lib"], st["pb"], st["b"]
+    prob, samp, P = pb["prob"], pb["samp"], pb["parts"]
+    T, V = prob.T, prob.S.nover_trans
+    s, xh, r = st["s"], st["xh"], pb["r"]
+    ky, kx = synth.window_coords(s)
+    minv = P["minv"][b].astype(np.float32).copy()
+    rim = kx >= np.floor(np.sqrt(np.maximum(r * r - ky * ky, 0))).astype(int)
+    minv[((kx == 0) & (ky < 0)) | rim] = 0.
+    minv[0] = P["scalars"][b, 0]       # the DC term carries minvsigma2_dc in both
+    rot, wd = _dense_weights(st)
+    # inverted matrices, as the reference's weighted-sum setup builds them for the backprojection
+    # (generateEulerMatrices(..., inverse = true), src/acc/acc_store_weight_sum.h:1041-1046)
+    eul = samp["eul_fine"].reshape(-1, 3, 3)[rot]
+    eul = np.ascontiguousarray(np.transpose(eul, (0, 2, 1)).reshape(-1, 9), np.float32)
+    re, im = (np.ascontiguousarray(a, np.float32) for a in (P["fimg"][b].real, P["fimg"][b].imag))
+    ctf = np.ascontiguousarray(P["ctf"][b], np.float32)
+    ps = pb["pad_size"]
+    gshape = (ps, ps, ps // 2 + 1)
+    gr, gi, gw = (np.zeros(gshape, np.float32) for _ in range(3))
+    rc = lib.ref_backproject(re.ctypes.data, im.ctypes.data, xh, s, st["tx"].ctypes.data, st["ty"].ctypes.data,
+                             T * V, wd.ctypes.data, minv.ctypes.data, ctf.ctypes.data, 1e-38, float(st["fsum"]),
+                             eul.ctypes.data, len(rot), gr.ctypes.data, gi.ctypes.data, gw.ctypes.data, r, 2,
+                             ps // 2 + 1, ps, ps, -(ps // 2), -(ps // 2))
+    assert rc == 0
+    prob2 = pb["oracle_problem"]()
+    sc = P["scalars"][b:b + 1].copy()
+    op2 = prob2.particles(P["fimg"][b:b + 1], P["ctf"][b:b + 1], minv[None], sc, synth.mresol(s))
+    prob2.wsum_bp(op2, 0, st["pairs"], st["wf"], st["fsum"], st["fsig"])
+    od, ow = prob2.grids()
+    od, ow = ro.enforce_hermitian_symmetry(od[0], ow[0])
+    rd, rw = ro.enforce_hermitian_symmetry(gr.astype(np.float64) + 1j * gi, gw.astype(np.float64))
+    assert np.max(np.abs(rd - od)) <= 1e-5 * np.max(np.abs(od)), np.max(np.abs(rd - od)) / np.max(np.abs(od))
+    assert np.max(np.abs(rw - ow)) <= 1e-5 * np.max(ow), np.max(np.abs(rw - ow)) / np.max(ow)
