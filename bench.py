@@ -585,6 +585,254 @@ def run_recon(args):
     es.close()
 
 
+# 2D classification: K = 50 seeded blob references of 100 x 100 at 2 A/px, 20,000 particles drawn
+# from them (in-plane rotation, shifts U(-5, 5) px, SNR 0.05); psi step 6 deg, translations range
+# 5 step 1, adaptive oversampling 1 (2 psi x 4 shifts per significant pair), window to Nyquist
+CLASS2D = dict(name="class2d_k50_box100_psi6_ovs1", ori_size=100, angpix=2.0, n_blobs=12, n_classes=50,
+               map_seed=31, psi_step=6.0, offset_range=5, offset_step=1, r_max=50, snr=0.05, seed=57,
+               n_particles=20000, batch=500)
+METRIC_CLASS2D = "E-step particles/s 2D classification K=50 box100: split-BF16 vs plain FP32 GPU; roofline %"
+
+
+def class2d_inputs(sy, samp_fn, n, seed, chunk=2000):
+    """References, sampling and n particles of the 2D-classification workload (numpy; particles
+    generated in chunks with one noise variance)."""
+    w = CLASS2D
+    N, r, K = w["ori_size"], w["r_max"], w["n_classes"]
+    maps = [sy.fourier_map(sy.blob_volume(N, w["n_blobs"], seed=w["map_seed"] + 101 * k, ndim=2), r)
+            for k in range(K)]
+    samp = samp_fn()
+    cls = np.random.default_rng(seed + 7).integers(0, K, n)
+    out, sigma2 = [], None
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        p = sy.make_particles(maps[0], b - a, ori_size=N, s=2 * r, r_max=r, angpix=w["angpix"], snr=w["snr"],
+                              seed=seed + a, max_shift=w["offset_range"], ref_dim=2, classes=cls[a:b],
+                              class_maps=maps, sigma2=sigma2)
+        sigma2 = p["sigma2"]
+        out.append(p)
+    parts = {k: np.concatenate([p[k] for p in out]) for k in ("fimg", "ctf", "minv", "scalars")}
+    return maps, samp, parts, cls
+
+
+def class2d_config():
+    w = CLASS2D
+    s = 2 * w["r_max"]
+    return {"workload": w["name"], "box": w["ori_size"], "classes": w["n_classes"], "psi_step": w["psi_step"],
+            "orientations_per_class": int(np.ceil(360 / w["psi_step"])), "translations": 81,
+            "pixels": s * (s // 2 + 1), "adaptive_oversampling": 1, "fine_hypotheses_per_pair": 8,
+            "snr": w["snr"], "particles": w["n_particles"]}
+
+
+def class2d_cpu(maps, samp, parts, n, sy):
+    """The FP64 oracle port's whole E-step on n particles, one per host thread: (seconds, text)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    w = CLASS2D
+    K, r, s = w["n_classes"], w["r_max"], 2 * w["r_max"]
+    prob = orc.Problem(ori_size=w["ori_size"], s=s, ref_dim=2, maps=maps, r_max=r, pad=2, samp=samp,
+                       pdf_direction=np.ones((K, 1)), pdf_class=np.full(K, 1.0 / K),
+                       sigma2_offset=(w["offset_range"] * w["angpix"]) ** 2, pixel_size=w["angpix"],
+                       adaptive_fraction=0.999, ovs=1, bp_pad_size=sy.pad_size(r), bp_r_max=r)
+    op = prob.particles(parts["fimg"][:n], parts["ctf"][:n], parts["minv"][:n], parts["scalars"][:n], sy.mresol(s))
+    t0 = time.perf_counter()
+    prob.estep(op, nthreads=n)
+    t = time.perf_counter() - t0
+    return t, (f"{n} particles, one per host thread, through the whole E-step of the FP64 oracle port (2D "
+               f"references: the reference's CPU kernels are compiled here for 3D references only)")
+
+
+def run_class2d(args, world, rank):
+    w = CLASS2D
+    K, N, r = w["n_classes"], w["ori_size"], w["r_max"]
+    s = 2 * r
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import sampling_oracle as so
+        sy = load_synthetic()
+        n = os.cpu_count() or 1
+        maps, samp, parts, _ = class2d_inputs(
+            sy, lambda: so.sampling2d(w["psi_step"], 1, w["offset_range"], w["offset_step"], w["angpix"]), n,
+            w["seed"] + 1)
+        class2d_cpu(maps, samp, parts, 1, sy)
+        times = [class2d_cpu(maps, samp, parts, n, sy)[0] for _ in range(args.steps)]
+        v = n * args.steps / float(np.sum(times))
+        text = class2d_cpu(maps, samp, parts, 1, sy)[1].replace("1 particles", f"{n} particles")
+        print(json.dumps({"impl": "reference", "metric": METRIC_CLASS2D, "value": v, "unit": "particles/s",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1000.0 * float(np.mean(times)), "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": class2d_config(), "particles_per_step": n,
+                          "cpu_baseline": {"value": v, "unit": "particles/s", "cores": n, "kind": "port",
+                                           "sample": text},
+                          "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    t2b = load_package()
+    import t2relion_b200.synthetic as sy
+    torch.cuda.set_device(local_rank())
+    dev = torch.device("cuda", local_rank())
+    B = w["batch"]
+    n_all = w["n_particles"]
+    maps, samp, parts, cls = class2d_inputs(
+        sy, lambda: t2b.sampling(2, 0, w["psi_step"], 1, w["offset_range"], w["offset_step"], w["angpix"]), n_all,
+        w["seed"] + 1000 * rank)
+    ps = sy.pad_size(r)
+
+    def context(mode):
+        es = t2b.EStep(local_rank())
+        for k in range(K):
+            es.set_projector(k, maps[k], 2, r, 2)
+            es.init_backprojector(k, 2, ps, r, 2)
+        es.configure(ori_size=N, current_size=s, ref_dim=2, nr_classes=K, samp=samp, pdf_direction=np.ones((K, 1)),
+                     pdf_class=np.full(K, 1.0 / K), sigma2_offset=(w["offset_range"] * w["angpix"]) ** 2,
+                     pixel_size=w["angpix"], adaptive_oversampling=1, diff2_mode=mode, max_batch=B)
+        return es
+
+    es = context(t2b.DIFF2_SPLIT_BF16)
+    first = {k: v[:B] for k, v in parts.items()}
+    t0 = time.perf_counter()
+    rep = es.autotune(first["fimg"], first["ctf"], first["minv"], first["scalars"])
+    tuned = {k: rep[k] for k in ("diff2_tn", "diff2_group", "fine_ctas_per_sm", "wsum_ctas_per_sm",
+                                 "project_pixels", "project_orients")}
+    tune_s = time.perf_counter() - t0
+    # the whole dataset resident in HBM; each step copies its batch into the entry point's
+    # fixed input buffers (device to device) and runs the E-step on them
+    alld = {"fimg": torch.from_numpy(parts["fimg"].view(np.float32)).to(dev),
+            "ctf": torch.from_numpy(parts["ctf"]).to(dev), "minv": torch.from_numpy(parts["minv"]).to(dev),
+            "scal": torch.from_numpy(parts["scalars"]).to(dev)}
+    stage = {k: v[:B].clone() for k, v in alld.items()}
+    half = N // 2 + 1
+
+    def device_pass(e, steps):
+        res = result_tensors(B, K, 1, dev, half)
+        rptr = {k: ctypes.c_void_p(v.data_ptr()) for k, v in res.items()}
+        stream = torch.cuda.Stream(dev)
+        poses = []
+
+        def step(i):
+            a = (i * B) % n_all
+            with torch.cuda.stream(stream):
+                for k in stage:
+                    stage[k].copy_(alld[k][a:a + B], non_blocking=True)
+            e.expectation_device(B, ctypes.c_void_p(stage["fimg"].data_ptr()), ctypes.c_void_p(stage["ctf"].data_ptr()),
+                                 ctypes.c_void_p(stage["minv"].data_ptr()), ctypes.c_void_p(stage["scal"].data_ptr()),
+                                 rptr, stream=stream.cuda_stream)
+        for i in range(3):
+            step(i)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local_rank()) as clk:
+            ev0.record(stream)
+            for i in range(steps):
+                step(i)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        if int(res["status"].ne(0).sum()) != 0:
+            raise RuntimeError("E-step status errors")
+        ms = ev0.elapsed_time(ev1)
+        return B * steps / (ms / 1000.0), ms / steps, clk.summary(), e.launch_count()
+
+    steps = n_all // B
+    value, ms_step, clocks, launches = device_pass(es, steps)
+    # per-stage device times of host-path steps (coarse contraction = stage 2)
+    es.stage_timing(True)
+    st = []
+    for i in range(3):
+        a = i * B
+        es.expectation(*[parts[k][a:a + B] for k in ("fimg", "ctf", "minv", "scalars")])
+        st.append(es.stage_ms())
+    es.stage_timing(False)
+    stages = np.mean(np.array(st), axis=0)
+    # end to end: host entry points over the dataset's batches (pinned)
+    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
+           [("fimg", parts["fimg"].view(np.float32)), ("ctf", parts["ctf"]), ("minv", parts["minv"]),
+            ("scal", parts["scalars"])]}
+    hres = [{k: v.pin_memory() for k, v in result_tensors(B, K, 1, "cpu", half).items()} for _ in range(2)]
+    P = s * (s // 2 + 1)
+
+    def host_batch(i):
+        a = (i * B) % n_all
+        b = t2b.Batch(B, 0, ctypes.c_void_p(pin["fimg"][a:a + B].data_ptr()), None,
+                      ctypes.c_void_p(pin["ctf"][a:a + B].data_ptr()), ctypes.c_void_p(pin["minv"][a:a + B].data_ptr()),
+                      ctypes.c_void_p(pin["scal"][a:a + B].data_ptr()))
+        h = hres[i & 1]
+        res = t2b.Result(*[ctypes.c_void_p(h[n].data_ptr()) if n in h else None for n, _ in t2b.Result._fields_])
+        return b, res
+    ticket = ctypes.c_longlong(-1)
+    keep = []
+    t0 = time.perf_counter()
+    prev = None
+    for i in range(steps):
+        b, res = host_batch(i)
+        keep.append((b, res))
+        t2b._check(t2b.lib.t2b_estep_submit_host(es._h, ctypes.byref(b), ctypes.byref(res), ctypes.byref(ticket)))
+        if prev is not None:
+            t2b._check(t2b.lib.t2b_estep_wait(es._h, prev))
+        prev = ticket.value
+    t2b._check(t2b.lib.t2b_estep_wait(es._h, prev))
+    e2e_s = time.perf_counter() - t0
+    h2d = B * (P * 8 + P * 4 + P * 4 + 8 * 8)
+    d2h = sum(v.numel() * v.element_size() for v in hres[0].values())
+    # the plain FP32 comparator on the first PLAIN_STEPS batches, and the poses of both passes there
+    es_p = context(t2b.DIFF2_PLAIN_FP32)
+    es_p.tune_set(**tuned)
+    pv, pms, pclk, _ = device_pass(es_p, PLAIN_STEPS)
+    same, n_cmp = 0, 0
+    for i in range(PLAIN_STEPS):
+        a = i * B
+        args_ = [parts[k][a:a + B] for k in ("fimg", "ctf", "minv", "scalars")]
+        ra, rb = es.expectation(*args_), es_p.expectation(*args_)
+        same += int(np.all(ra["pose"] == rb["pose"], axis=1).sum())
+        n_cmp += B
+        if i == 0:
+            nsig = ra["nr_sign"]
+            cls_ok = float(np.mean(ra["pose"][:, 0] == cls[a:a + B]))
+    es_p.close()
+    peaks, src = measured_peaks()
+    at_max = bool(clocks.get("sm_mhz") and clocks.get("sm_max_mhz") and clocks["sm_mhz"] >= 0.97 * clocks["sm_max_mhz"]
+                  and "sw_power_cap" not in clocks["reasons"])
+    peak = peaks.get("bf16_tflops", 1590.0) if at_max else peaks.get("bf16_tflops_sustained", 1400.0)
+    O, T = samp["n_psi"], samp["n_trans"]
+    flops = 8.0 * K * O * T * P * B
+    achieved = flops / (float(stages[2]) / 1000.0) / 1e12
+    line = {"metric": METRIC_CLASS2D, "value": value, "unit": "particles/s", "n_gpus": world,
+            "steps": steps, "warmup": 3, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / pv,
+            "vs_baseline_definition": "value / plain.value: the plain FP32 GPU path timed in this run",
+            "dtype": "f32+bf16x3/f64", "data": "synthetic (seeded blob references, CTF, white noise)",
+            "config": class2d_config(), "particles_per_step": B,
+            "run": {"diff2": "splitbf16", "tile_shapes": dict(tuned, tune_s=tune_s),
+                    "l2": "inputs: 20,000 distinct particles (1.6 GB) resident, one pass"},
+            "e2e": {"value": B * steps / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "api": "t2b_estep_submit_host + t2b_estep_wait over the dataset"},
+            "gpu_launches": launches * steps if launches > 0 else None, "clocks": clocks,
+            "plain": {"value": pv, "ms_per_step": pms, "steps": PLAIN_STEPS, "clocks": pclk},
+            "quality_vs_plain": {"particles": n_cmp, "pose_agreement": same / n_cmp,
+                                 "true_class_fraction": cls_ok},
+            "nr_sign": {"min": int(nsig.min()), "median": float(np.median(nsig)), "max": int(nsig.max())},
+            "roofline": {"bound": "tensor", "kernel": "k_diff2_tc", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src, "traffic": None,
+                         "flops_per_launch": flops},
+            "stage_ms": {n: float(v) for n, v in zip(
+                ["prep_network", "operands_audit_norms", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
+                 "wsum_bp", "audit_contraction", "proposal_contraction"], stages)}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n = os.cpu_count() or 1
+        t, text = class2d_cpu(maps, samp, parts, n, sy)
+        line["cpu_baseline"] = {"value": n / t, "unit": "particles/s", "cores": n, "kind": "port", "sample": text}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    es.close()
+
+
+def local_rank():
+    return int(os.environ.get("LOCAL_RANK", "0"))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -614,7 +862,17 @@ def main():
     ap.add_argument("--no-graph", action="store_true",
                     help="launch each step's kernels one by one instead of replaying its CUDA graph (ncu cannot "
                          "profile the kernel nodes of a graph with conditional nodes; not a bench number)")
+    ap.add_argument("--workload", default="box128", choices=["box128", "class2d"],
+                    help="box128: the 3D refinement headline; class2d: 2D classification, K = 50 references of "
+                         "100 x 100, 20,000 particles (its own JSON line)")
     args = ap.parse_args()
+    if args.workload == "class2d":
+        world, rank, _ = dist_init()
+        run_class2d(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.stage == "prep":
         run_prep(args)
         return
@@ -804,9 +1062,9 @@ def main():
         torch.distributed.destroy_process_group()
 
 
-def result_tensors(B, K, nd, dev):
+def result_tensors(B, K, nd, dev, half=None):
     import torch
-    half = WORKLOAD["ori_size"] // 2 + 1
+    half = half or WORKLOAD["ori_size"] // 2 + 1
     return {k: torch.zeros(shape, dtype=dt, device=dev) for k, shape, dt in [
         ("min_diff2", B, torch.float64), ("sum_weight", B, torch.float64), ("sig_weight", B, torch.float64),
         ("coarse_sum_weight", B, torch.float64), ("coarse_sig_weight", B, torch.float64),
@@ -826,7 +1084,7 @@ def time_device(es, parts, B, steps, warmup, local, world, t2b):
     ctf = torch.from_numpy(parts["ctf"]).to(dev)
     minv = torch.from_numpy(parts["minv"]).to(dev)
     scal = torch.from_numpy(parts["scalars"]).to(dev)
-    res = result_tensors(B, es.cfg["nr_classes"], es.cfg["n_dir"], dev)
+    res = result_tensors(B, es.cfg["nr_classes"], es.cfg["n_dir"], dev, es.cfg["ori_size"] // 2 + 1)
     rptr = {k: ctypes.c_void_p(v.data_ptr()) for k, v in res.items()}
     # an explicit stream: the library runs a NULL stream argument on its own stream
     stream = torch.cuda.Stream(dev)
@@ -874,7 +1132,8 @@ def time_e2e(es, parts, B, steps, world, t2b, min_steps=E2E_STEPS):
     pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
            [("fimg", parts["fimg"].view(np.float32)), ("ctf", parts["ctf"]), ("minv", parts["minv"]),
             ("scal", parts["scalars"])]}
-    hres = {k: v.pin_memory() for k, v in result_tensors(B, es.cfg["nr_classes"], es.cfg["n_dir"], "cpu").items()}
+    hres = {k: v.pin_memory() for k, v in result_tensors(B, es.cfg["nr_classes"], es.cfg["n_dir"], "cpu",
+                                                          es.cfg["ori_size"] // 2 + 1).items()}
     lib = t2b.lib
     batch = t2b.Batch(B, 0, ctypes.c_void_p(pin["fimg"].data_ptr()), None, ctypes.c_void_p(pin["ctf"].data_ptr()),
                       ctypes.c_void_p(pin["minv"].data_ptr()), ctypes.c_void_p(pin["scal"].data_ptr()))

@@ -92,3 +92,21 @@ def sampling(order, psi_step, ovs, range_px, step_px, pixel_size):
     return dict(n_dir=npix, n_psi=npsi, n_trans=len(tr), nover_rot=8 if ovs else 1, nover_trans=4 if ovs else 1,
                 eul_coarse=np.array(coarse), eul_fine=np.array(fine).reshape(-1, 9),
                 trans_px=tr / pixel_size, trans_px_fine=tf / pixel_size, trans_prior=tr)
+
+
+def sampling2d(psi_step, ovs, range_px, step_px, pixel_size):
+    """2D classification (one direction, in-plane psi): the library's layout; fine psi are the
+    2 halves of each psi step, wrapped above 180 deg (src/healpix_sampling.cpp:1914-2040)."""
+    npsi = math.ceil(360. / psi_step)
+    step_psi = 360. / npsi
+    coarse, fine = [], []
+    for p in range(npsi):
+        coarse.append(euler(0., 0., p * step_psi))
+        if ovs:
+            for po in range(2):
+                over = p * step_psi - 0.5 * step_psi + (0.5 + po) * step_psi / 2
+                fine.append(euler(0., 0., over - 360. if over > 180. else over))
+    s3 = sampling(0, 360., ovs, range_px, step_px, pixel_size)   # translations only
+    return dict(n_dir=1, n_psi=npsi, n_trans=s3["n_trans"], nover_rot=2 if ovs else 1, nover_trans=s3["nover_trans"],
+                eul_coarse=np.array(coarse), eul_fine=np.array(fine).reshape(-1, 9), trans_px=s3["trans_px"],
+                trans_px_fine=s3["trans_px_fine"], trans_prior=s3["trans_prior"])

@@ -52,13 +52,16 @@ def fourier_map(vol, r_max, padding_factor=2):
     rp2 = (r_max * padding_factor) ** 2
     k = np.arange(-c, c + 1)
     x = np.arange(xdim)
+    # a grid of r_max at Nyquist reaches one column past the transform's last (m/2): such
+    # elements lie outside r_max * padding_factor and are zeroed, so their index is clipped
+    xc = min(xdim, F.shape[-1]) - 1
     if ndim == 3:
         kz, ky, kx = np.meshgrid(k, k, x, indexing="ij")
-        out = F[kz % m, ky % m, kx]
+        out = F[kz % m, ky % m, np.minimum(kx, xc)]
         out[kz * kz + ky * ky + kx * kx > rp2] = 0
     else:
         ky, kx = np.meshgrid(k, x, indexing="ij")
-        out = F[ky % m, kx]
+        out = F[ky % m, np.minimum(kx, xc)]
         out[ky * ky + kx * kx > rp2] = 0
     return np.ascontiguousarray(out.astype(np.complex64))
 

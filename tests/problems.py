@@ -19,6 +19,9 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
         # box 64, order 2 + adaptive oversampling, high SNR: a sharp posterior, the regime in
         # which the learned proposals hold the posterior (the box-128 benchmark's regime)
         "learn_o2": dict(N=64, angpix=2.0, order=2, psi=7.5, rng=3, r=16, snr=0.5, ovs=1),
+        # the same at SNR 0.03 (the box-128 benchmark's noise level): broad posteriors at box 64,
+        # where 64 proposals miss posterior mass and the audit must send batches to the full pass
+        "learn_o2_lowsnr": dict(N=64, angpix=2.0, order=2, psi=7.5, rng=3, r=16, snr=0.03, ovs=1),
         # 2D classification: 2D references, psi 6 deg, oversampling 1
         "class2d": dict(N=48, angpix=2.0, order=0, psi=6.0, rng=3, r=12, snr=0.2, ovs=1),
     }
@@ -148,3 +151,50 @@ def input_digest(parts):
     for k in ("fimg", "ctf", "minv", "scalars"):
         h.update(np.ascontiguousarray(parts[k]).tobytes())
     return h.hexdigest()
+
+
+# 2D classification at its stated size: K = 50 references of 100 x 100 (seeded blob images),
+# particles from those classes with random in-plane rotation and shifts U(-5, 5) px, SNR
+# 0.05; psi step 6 deg (60), translations range 5 step 1 (81), adaptive oversampling 1 (2 psi
+# x 4 shifts per significant pair), the window to Nyquist (r 50: 100 x 51 pixels).
+CLASS2D = dict(ori_size=100, angpix=2.0, n_blobs=12, n_classes=50, map_seed=31, psi_step=6.0, offset_range=5,
+               offset_step=1, r_max=50, snr=0.05)
+
+
+def class2d_k50(n_particles, seed, n_classes=None):
+    """Inputs, sampling and an oracle Problem of the 2D-classification workload."""
+    t2b = load_package()
+    import t2relion_b200.synthetic as sy
+    import oracle as orc
+    w = CLASS2D
+    K = n_classes or w["n_classes"]
+    N, r = w["ori_size"], w["r_max"]
+    s = 2 * r
+    maps = [sy.fourier_map(sy.blob_volume(N, w["n_blobs"], seed=w["map_seed"] + 101 * k, ndim=2), r)
+            for k in range(K)]
+    samp = t2b.sampling(2, 0, w["psi_step"], 1, w["offset_range"], w["offset_step"], w["angpix"])
+    cls = np.random.default_rng(seed + 7).integers(0, K, n_particles)
+    parts = sy.make_particles(maps[0], n_particles, ori_size=N, s=s, r_max=r, angpix=w["angpix"], snr=w["snr"],
+                              seed=seed, max_shift=w["offset_range"], ref_dim=2, classes=cls, class_maps=maps)
+    pdf_dir = np.ones((K, 1))
+    pdf_cls = np.full(K, 1.0 / K)
+    sigma2_offset = (w["offset_range"] * w["angpix"]) ** 2
+    ps = sy.pad_size(r)
+    prob = orc.Problem(ori_size=N, s=s, ref_dim=2, maps=maps, r_max=r, pad=2, samp=samp, pdf_direction=pdf_dir,
+                       pdf_class=pdf_cls, sigma2_offset=sigma2_offset, pixel_size=w["angpix"],
+                       adaptive_fraction=0.999, ovs=1, bp_pad_size=ps, bp_r_max=r)
+    oparts = prob.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], sy.mresol(s))
+
+    def product(diff2_mode, max_batch=None, use_graph=1):
+        es = t2b.EStep(0)
+        for k in range(K):
+            es.set_projector(k, maps[k], 2, r, 2)
+            es.init_backprojector(k, 2, ps, r, 2)
+        es.configure(ori_size=N, current_size=s, ref_dim=2, nr_classes=K, samp=samp, pdf_direction=pdf_dir,
+                     pdf_class=pdf_cls, sigma2_offset=sigma2_offset, pixel_size=w["angpix"],
+                     adaptive_oversampling=1, diff2_mode=diff2_mode, max_batch=max_batch or n_particles,
+                     use_graph=use_graph)
+        return es
+
+    return dict(t2b=t2b, sy=sy, maps=maps, samp=samp, parts=parts, prob=prob, oparts=oparts, product=product,
+                pad_size=ps, K=K, classes=cls)

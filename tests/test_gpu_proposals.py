@@ -253,3 +253,42 @@ def test_learned_coarse_selection_matches_oracle(trained):
         assert res["coarse_sig_weight"][b] == pytest.approx(sig, rel=1e-12)
         assert res["coarse_sum_weight"][b] == pytest.approx(sw, rel=1e-12)
         assert res["n_coarse_sig"][b] == int(np.sum(wts >= sig))
+
+
+def test_low_snr_audit_falls_back_where_proposals_miss():
+    """SNR 0.03 at box 64 (the noise level of the box-128 benchmark, where the posterior is
+    broad): a network trained as above, 8-particle batches with one audited particle each.
+    A batch whose audited particle keeps >= 0.999 of its posterior mass in its proposals stays
+    on them; a batch where it does not runs the full coarse pass, and its results are then
+    exactly the full E-step's.  At this noise level the fallback must fire in some batch, and
+    the poses of the learned batches agree with the full E-step."""
+    pb = problems.build("learn_o2_lowsnr", n_particles=64, seed=37, diff2_mode=1, max_batch=8)
+    es, P = pb["product"](), pb["parts"]
+    es.train_proposals(P["minv"][0], n_train=40000, n_posterior=4096, n_val=512, epochs=4, batch=256, lr=3e-4,
+                       topk=64, rescore=512, seed=3, max_shift=3.0)
+    fell, stayed, same, n = 0, 0, 0, 0
+    for a in range(0, 64, 8):
+        args = [P[k][a:a + 8] for k in ("fimg", "ctf", "minv", "scalars")]
+        es.disable_proposals()
+        full = es.expectation(*args)
+        es.enable_proposals(topk=64, rescore=512, audit_every=8, audit_mass=0.999)
+        got = es.expectation(*args)
+        es.disable_proposals()
+        assert np.all(got["status"] == 0)
+        mass = got["audit_mass"][got["audit_mass"] >= 0]
+        assert mass.size == 1
+        if mass[0] < 0.999:
+            fell += 1
+            assert np.all(got["learned"] == 0)
+            assert np.array_equal(got["pose"], full["pose"])
+            assert np.array_equal(got["nr_sign"], full["nr_sign"])
+            assert np.allclose(got["sum_weight"], full["sum_weight"], rtol=1e-9)
+        else:
+            stayed += 1
+            assert np.all(got["learned"] == 1)
+            same += int(np.all(got["pose"] == full["pose"], axis=1).sum())
+            n += 8
+    es.close()
+    print(f"low-SNR audit: {fell} batches fell back, {stayed} stayed on the proposals")
+    assert fell >= 1
+    assert n == 0 or same / n >= 0.9

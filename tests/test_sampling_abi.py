@@ -106,3 +106,15 @@ def test_sampling_matches_oracle_restatement(t2b, order, psi, rng, angpix):
         assert np.array_equal(a[k], b[k]), k
     for k in ("eul_coarse", "eul_fine"):
         assert np.max(np.abs(a[k] - b[k])) <= 1e-15, k
+
+
+def test_sampling_2d_matches_oracle_restatement(t2b):
+    import sampling_oracle as so
+    a = t2b.sampling(2, 0, 6.0, 1, 5, 1, 2.0)
+    b = so.sampling2d(6.0, 1, 5, 1, 2.0)
+    for k in ("n_dir", "n_psi", "n_trans", "nover_rot", "nover_trans"):
+        assert a[k] == b[k], k
+    for k in ("trans_px", "trans_px_fine", "trans_prior"):
+        assert np.array_equal(a[k], b[k]), k
+    for k in ("eul_coarse", "eul_fine"):
+        assert np.max(np.abs(a[k] - b[k])) <= 1e-15, k
