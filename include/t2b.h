@@ -109,6 +109,18 @@ typedef struct t2b_config {
                                   (do_scale_correction): a pixel of ring ires in class k adds to
                                   them when data_vs_prior[k][ires] > 3 (src/ml_optimiser.cpp:
                                   8477-8486)                                             */
+    int orientation_chunk;     /* coarse orientations projected and contracted per chunk inside
+                                  each batch.  0: automatic -- every projection table resident
+                                  (built once here) when the coarse and fine tables and their
+                                  split-BF16 operands fit in 60 % of the free device memory,
+                                  else chunks of 16384; > 0: chunks of this many rows (at most
+                                  nr_classes * n_dir * n_psi).  Chunked: split-BF16 contraction
+                                  only, the fine pass and the weighted sums interpolate their
+                                  projections from the models on the fly (the same FP64
+                                  interpolation, so the same values), no learned proposals.
+                                  The reference re-projects every orientation for every
+                                  particle (orientation_matrix_handler.cuh:99-126)         */
+    int _pad2;
 } t2b_config;
 
 /* Validate the configuration, build the projection tables of all coarse and

@@ -79,7 +79,7 @@ class Config(ctypes.Structure):
         ("trans_prior", _p), ("pdf_direction", _p), ("pdf_class", _p), ("mresol", _p),
         ("sigma2_offset", ctypes.c_double), ("pixel_size", ctypes.c_double),
         ("adaptive_fraction", ctypes.c_double), ("fine_capacity", ctypes.c_size_t),
-        ("data_vs_prior", _p),
+        ("data_vs_prior", _p), ("orientation_chunk", ctypes.c_int), ("_pad2", ctypes.c_int),
     ]
 
 
@@ -443,7 +443,8 @@ class EStep:
     def configure(self, *, ori_size, current_size, ref_dim, nr_classes, samp, pdf_direction,
                   pdf_class, sigma2_offset, pixel_size, adaptive_fraction=0.999,
                   adaptive_oversampling=0, diff2_mode=DIFF2_PLAIN_FP32, max_batch=64,
-                  fine_capacity=0, maximum_significants=-1, use_graph=1, data_vs_prior=None):
+                  fine_capacity=0, maximum_significants=-1, use_graph=1, data_vs_prior=None,
+                  orientation_chunk=0):
         arrays = dict(
             eul_coarse=np.ascontiguousarray(samp["eul_coarse"], np.float64),
             eul_fine=np.ascontiguousarray(samp["eul_fine"], np.float64),
@@ -468,6 +469,7 @@ class EStep:
             setattr(c, k, _ptr(a))
         c.sigma2_offset, c.pixel_size, c.adaptive_fraction = sigma2_offset, pixel_size, adaptive_fraction
         c.fine_capacity = fine_capacity
+        c.orientation_chunk = orientation_chunk
         _check(lib.t2b_configure(self._h, ctypes.byref(c)))
         self.cfg = dict(ori_size=ori_size, current_size=current_size, nr_classes=nr_classes,
                         n_dir=samp["n_dir"], n_psi=samp["n_psi"], n_trans=samp["n_trans"],

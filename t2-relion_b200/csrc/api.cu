@@ -341,6 +341,24 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             tb.nk = (int)kp.size();
             tb.kpix = (const int*)up(kp.data(), kp.size() * sizeof(int));
         }
+        // resident projection tables, or one chunk of the coarse orientations per batch step
+        int chunk = 0;
+        {
+            const double kd = (double)tc_kdim(tb.nk), kn = (double)tc_kn(tb.nk);
+            const double resident = (double)KO * P * 8. * (1 + (tb.ovs ? R : 0)) +
+                                    (f.diff2_mode == T2B_DIFF2_SPLIT_BF16 ? (double)KO * (kd + kn) * 4. : 0.);
+            size_t fr = 0, tot = 0;
+            T2B_CUDA(cudaMemGetInfo(&fr, &tot));
+            T2B_REQUIRE(f.orientation_chunk >= 0, T2B_ERR_ARG, "orientation_chunk must be >= 0");
+            if (f.orientation_chunk > 0) chunk = f.orientation_chunk;
+            else if (resident > 0.6 * (double)fr) chunk = 16384;
+            if (chunk >= KO) chunk = 0;
+            chunk = std::min(chunk, O);   // chunks never straddle two classes
+        }
+        T2B_REQUIRE(chunk == 0 || f.diff2_mode == T2B_DIFF2_SPLIT_BF16, T2B_ERR_UNSUPPORTED,
+                    "projection tables do not fit (or orientation_chunk was set): the chunked coarse pass "
+                    "runs on the split-BF16 contraction only");
+        tb.chunk = chunk;
         tb.eul_c = (const double*)up(f.eul_coarse, (size_t)O * 9 * sizeof(double));
         tb.trans_c = (const double*)up(f.trans_px, (size_t)T * 2 * sizeof(double));
         tb.trans_prior = (const double*)up(f.trans_prior, (size_t)T * 2 * sizeof(double));
@@ -351,23 +369,33 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             tb.eul_f = tb.eul_c;
             tb.trans_f = tb.trans_c;
         }
-        // projection tables (per class, resident)
-        float2* pc = dalloc<float2>(c, (size_t)KO * P);
-        for (int k = 0; k < K; k++) {
-            const Volume& v = c->mvol[k];
-            T2B_REQUIRE(v.r_max * v.pad + 1 < v.xdim, T2B_ERR_ARG, "projector too small");
-            launch_project_table(v, c->mdl[k], tb.eul_c, O, s, pc + (size_t)k * O * P, st, c->tune.proj_px,
-                                 c->tune.proj_orients);
-        }
-        tb.proj_c = pc;
-        if (tb.ovs) {
-            float2* pf = dalloc<float2>(c, (size_t)KO * R * P);
-            for (int k = 0; k < K; k++)
-                launch_project_table(c->mvol[k], c->mdl[k], tb.eul_f, O * R, s, pf + (size_t)k * O * R * P, st,
-                                     c->tune.proj_px, c->tune.proj_orients);
-            tb.proj_f = pf;
+        for (int k = 0; k < K; k++)
+            T2B_REQUIRE(c->mvol[k].r_max * c->mvol[k].pad + 1 < c->mvol[k].xdim, T2B_ERR_ARG, "projector too small");
+        if (chunk) {
+            // one chunk of coarse projections, filled inside each batch; the fine pass and the
+            // weighted sums interpolate from the models
+            tb.proj_c = dalloc<float2>(c, (size_t)chunk * P);
+            tb.proj_f = nullptr;
+            std::vector<const float2*> mp(c->mdl.begin(), c->mdl.begin() + K);
+            std::vector<Volume> mv(c->mvol.begin(), c->mvol.begin() + K);
+            tb.mdl = (const float2* const*)up(mp.data(), K * sizeof(float2*));
+            tb.mvol = (const Volume*)up(mv.data(), K * sizeof(Volume));
         } else {
-            tb.proj_f = pc;
+            // projection tables (per class, resident)
+            float2* pc = dalloc<float2>(c, (size_t)KO * P);
+            for (int k = 0; k < K; k++)
+                launch_project_table(c->mvol[k], c->mdl[k], tb.eul_c, O, s, pc + (size_t)k * O * P, st,
+                                     c->tune.proj_px, c->tune.proj_orients);
+            tb.proj_c = pc;
+            if (tb.ovs) {
+                float2* pf = dalloc<float2>(c, (size_t)KO * R * P);
+                for (int k = 0; k < K; k++)
+                    launch_project_table(c->mvol[k], c->mdl[k], tb.eul_f, O * R, s, pf + (size_t)k * O * R * P, st,
+                                         c->tune.proj_px, c->tune.proj_orients);
+                tb.proj_f = pf;
+            } else {
+                tb.proj_f = pc;
+            }
         }
         float2* abc = dalloc<float2>(c, (size_t)T * P);
         launch_phase_table(tb.trans_c, T, s, f.ori_size, abc, st);
@@ -486,7 +514,8 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         if (f.diff2_mode == T2B_DIFF2_SPLIT_BF16) {
             TcOperands& op = c->tc;
             op.kdim = (int)tc_kdim(tb.nk);
-            op.m_pad = (int)((KO + 127) / 128 * 128);
+            op.chunk = chunk;
+            op.m_pad = (int)(((chunk ? chunk : KO) + 127) / 128 * 128);
             op.n_pad = (B * T + 255) / 256 * 256;
             op.bh = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kdim);
             op.bl = dalloc<uint16_t>(c, (size_t)op.m_pad * op.kdim);
@@ -537,12 +566,33 @@ void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool
     if (stage_events) cudaEventRecord(c->ev[1], st);
     if (pm) proposal_audit(c, w, st, stage_events ? c->ev + 8 : nullptr);
     if (tc) tc_split_images(tb, w, c->tc, st, w.gate);   // the full pass's operand: skipped while proposals hold
-    if (tc) tc_launch_norms(tb, w, c->tc, st, w.gate, 0);
-    else launch_norms(tb, w, st);
-    if (stage_events) cudaEventRecord(c->ev[2], st);
-    if (pm) proposal_coarse(c, w, st, stage_events ? c->ev + 10 : nullptr);
-    if (tc) tc_launch_diff2(tb, w, c->tc, st, w.gate, 0);
-    else launch_diff2_simt(tb, w, st);
+    if (tb.chunk) {
+        // chunked coarse pass: per chunk of one class's orientations, its projections, their
+        // split-BF16 operands, the norms and the contraction into the batch's diff2 rows
+        if (stage_events) cudaEventRecord(c->ev[2], st);
+        bool first = true;
+        float2* table = const_cast<float2*>(tb.proj_c);
+        for (int k = 0; k < tb.K; k++)
+            for (int o0 = 0; o0 < tb.O; o0 += tb.chunk) {
+                const int n = std::min(tb.chunk, tb.O - o0);
+                launch_project_table(c->mvol[k], c->mdl[k], tb.eul_c + 9 * (size_t)o0, n, tb.s, table, st,
+                                     c->tune.proj_px, c->tune.proj_orients);
+                tc_split_chunk(tb, c->tc, n, st);
+                RowChunk ch;
+                ch.row0 = k * tb.O + o0;
+                ch.rows = n;
+                tc_launch_norms(tb, w, c->tc, st, nullptr, 0, ch, first);
+                tc_launch_diff2(tb, w, c->tc, st, nullptr, 0, ch);
+                first = false;
+            }
+    } else {
+        if (tc) tc_launch_norms(tb, w, c->tc, st, w.gate, 0);
+        else launch_norms(tb, w, st);
+        if (stage_events) cudaEventRecord(c->ev[2], st);
+        if (pm) proposal_coarse(c, w, st, stage_events ? c->ev + 10 : nullptr);
+        if (tc) tc_launch_diff2(tb, w, c->tc, st, w.gate, 0);
+        else launch_diff2_simt(tb, w, st);
+    }
     if (stage_events) cudaEventRecord(c->ev[3], st);
     launch_weights_coarse(tb, w, c->cfg.maximum_significants, st);
     if (stage_events) cudaEventRecord(c->ev[4], st);
@@ -918,9 +968,12 @@ int t2b_autotune(t2b_ctx* c, const t2b_batch* b, t2b_tune_report* rep)
         // 4. projection tile: pixels x orientations per CTA, on the first (up to 16384) rows of
         // the fine (else coarse) table of class 0, rewritten with identical values
         {
-            const int rows = std::min(16384, c->tb.ovs ? c->tb.O * c->tb.R : c->tb.O);
-            float2* out = const_cast<float2*>(c->tb.ovs ? c->tb.proj_f : c->tb.proj_c);
-            const double* eul = c->tb.ovs ? c->tb.eul_f : c->tb.eul_c;
+            // (chunked configurations: the chunk table and the coarse orientations)
+            const bool fine = c->tb.ovs && !c->tb.chunk;
+            const int rows = std::min(c->tb.chunk ? std::min(c->tb.chunk, c->tb.O) : 16384,
+                                      fine ? c->tb.O * c->tb.R : c->tb.O);
+            float2* out = const_cast<float2*>(fine ? c->tb.proj_f : c->tb.proj_c);
+            const double* eul = fine ? c->tb.eul_f : c->tb.eul_c;
             const int pxs[3] = {128, 256, 512}, ors[3] = {1, 2, 4};
             cudaEvent_t e0, e1;
             T2B_CUDA(cudaEventCreate(&e0));

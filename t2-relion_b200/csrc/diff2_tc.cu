@@ -228,6 +228,10 @@ struct TcParams {
     // fix[m-tile * 4 + warp] (zero before the launch) adds the other slice's and emits
     float* part;
     int* fix;
+    // dense and raw-row tiles over one chunk of the orientations (mode 0): the tile's row oc
+    // (< KO, the chunk's rows) is global orientation row0 + oc of a batch layout whose rows
+    // are ko_stride long (0: KO); skip, norms and the output are indexed globally
+    int row0, ko_stride;
 };
 
 // maps: device array of tensor-map descriptors (encoded once per configuration);
@@ -495,6 +499,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
             // the TMEM lane is the row, which is the contiguous axis of the output, so each of
             // the 32 columns of a load is one coalesced 128-byte store, no transpose
             const bool raw_rows = p.mode == 0 && p.raw && p.T == 1;
+            const size_t ks = p.ko_stride ? (size_t)p.ko_stride : (size_t)p.KO;
             if (raw_rows) {
                 const int oc = mt * TM + q * 32 + lane;
                 for (int c = 0; c < nchunk; c++) {
@@ -504,7 +509,7 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
 #pragma unroll
                         for (int e = 0; e < 32; e++) {
                             const int col = n0 + c * 32 + e;
-                            if (col < p.ncols) outp[(size_t)col * p.KO + oc] = __uint_as_float(v[e]);
+                            if (col < p.ncols) outp[(size_t)col * ks + p.row0 + oc] = __uint_as_float(v[e]);
                         }
                     }
                 }
@@ -532,16 +537,17 @@ k_diff2_tc(const CUtensorMap* __restrict__ maps, int ia, int ib, TcParams p)
                     for (int r = 0; r < 32; r++) {
                         const int oc = mt * TM + q * 32 + r;
                         if (!cok || oc >= p.KO) continue;
+                        const size_t og = (size_t)p.row0 + oc;
                         float d;
                         if (p.raw) {
                             d = sbuf[r * EPI_LD + lane];
-                        } else if (p.skip[oc]) {
+                        } else if (p.skip[og]) {
                             d = -999.f;
                         } else {
-                            d = c0 + p.norms[(size_t)b * p.KO + oc] - sbuf[r * EPI_LD + lane];
+                            d = c0 + p.norms[(size_t)b * ks + og] - sbuf[r * EPI_LD + lane];
                             lmin = min(lmin, f2key(d));
                         }
-                        outp[((size_t)b * p.KO + oc) * p.T + t] = d;
+                        outp[((size_t)b * ks + og) * p.T + t] = d;
                     }
                 } else {
                     // proposal tile: column = translation; the warp's 32 rows are proposals of
@@ -765,18 +771,24 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
     CUtensorMap h128[2] = {make_map(op.ah, op.n_pad, op.kdim, 128), make_map(op.al, op.n_pad, op.kdim, 128)};
     T2B_CUDA(cudaMemcpy(static_cast<unsigned char*>(op.maps) + 128 * MAP_IH128, h128, sizeof(h128),
                         cudaMemcpyHostToDevice));
-    const int rows = tb.K * tb.O;
+    const int rows = op.chunk > 0 ? op.chunk : tb.K * tb.O;
     // sizes were fixed when the operand buffers were allocated
     T2B_REQUIRE(op.m_pad == (rows + TM - 1) / TM * TM && op.kdim == (int)tc_kdim(tb.nk), T2B_ERR_STATE,
                 "tensor-core operand sizes do not match their allocation");
-    const size_t n = (size_t)op.m_pad * op.kdim;
-    T2B_REQUIRE(op.bh && op.bl, T2B_ERR_STATE, "tensor-core operands not allocated");
-    const long long total = (long long)n / 2;
+    if (op.chunk == 0) tc_split_chunk(tb, op, rows, st);   // chunked: split per chunk in each batch
+}
+
+// Rows [0, rows) of tb.proj_c into the split-BF16 projection and |projection|^2 operands; the
+// rows up to the operands' next multiple of 128 are zeroed.
+void tc_split_chunk(const Tables& tb, TcOperands& op, int rows, cudaStream_t st)
+{
+    T2B_REQUIRE(op.bh && op.bl && rows >= 1 && rows <= op.m_pad, T2B_ERR_STATE, "tensor-core operands not allocated");
+    const long long rpad = (rows + TM - 1) / TM * TM;
     k_split_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, tb.kpix, tb.nk, op.kdim, (__nv_bfloat16*)op.bh,
-                                            (__nv_bfloat16*)op.bl, total);
+                                            (__nv_bfloat16*)op.bl, rpad * op.kdim / 2);
     T2B_REQUIRE(op.nh && op.nl && op.kn == (int)tc_kn(tb.nk), T2B_ERR_STATE, "norm operands not allocated");
     k_split_norm_proj<<<4 * sms(), 256, 0, st>>>(tb.proj_c, rows, tb.P, tb.kpix, tb.nk, op.kn, (__nv_bfloat16*)op.nh,
-                                                 (__nv_bfloat16*)op.nl, (long long)op.m_pad * op.kn);
+                                                 (__nv_bfloat16*)op.nl, rpad * op.kn);
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -795,19 +807,24 @@ static void launch_gemm(const TcOperands& op, int ia, int ib, TcParams& p, cudaS
 }
 
 // N[b][oc] = sum_p w2[b][p] |P_oc[p]|^2 with the same split-BF16 tensor-core kernel
-void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate, int gate_run)
+void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate, int gate_run,
+                     RowChunk ch, bool split_w2)
 {
     const int b_pad = (w.n + TN - 1) / TN * TN;
     T2B_REQUIRE(b_pad <= op.b_pad, T2B_ERR_ARG, "batch larger than the tensor-core workspace");
-    k_split_w2<<<4 * sms(), 256, 0, st>>>(w.w2, w.n, tb.P, tb.kpix, tb.nk, op.kn, (__nv_bfloat16*)op.wh, (__nv_bfloat16*)op.wl,
-                                          (long long)b_pad * op.kn);
-    T2B_CUDA(cudaGetLastError());
+    if (split_w2) {
+        k_split_w2<<<4 * sms(), 256, 0, st>>>(w.w2, w.n, tb.P, tb.kpix, tb.nk, op.kn, (__nv_bfloat16*)op.wh,
+                                              (__nv_bfloat16*)op.wl, (long long)b_pad * op.kn);
+        T2B_CUDA(cudaGetLastError());
+    }
     TcParams p{};
-    p.m_tiles = op.m_pad / TM;
+    p.m_tiles = ch.rows ? (ch.rows + TM - 1) / TM : op.m_pad / TM;
     p.n_tiles = b_pad / TN;
     p.kblocks = op.kn / TK;
     p.raw = 1;
-    p.KO = tb.K * tb.O;
+    p.KO = ch.rows ? ch.rows : tb.K * tb.O;
+    p.row0 = ch.row0;
+    p.ko_stride = ch.rows ? tb.K * tb.O : 0;
     p.T = 1;
     p.ncols = w.n;
     p.skip = tb.skip;
@@ -840,7 +857,8 @@ void tc_split_phases(const Tables& tb, const TcOperands& op, int rows, void* hi,
     T2B_CUDA(cudaGetLastError());
 }
 
-void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate, int gate_run)
+void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate, int gate_run,
+                     RowChunk ch)
 {
     const int ncols = w.n * tb.T;
     const int n_pad = (ncols + TN - 1) / TN * TN;
@@ -848,12 +866,14 @@ void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream
     T2B_REQUIRE(op.dense_tn == 256 || op.dense_tn == 128, T2B_ERR_ARG, "dense tile width");
     TcParams p{};
     p.raw = 0;
-    p.m_tiles = op.m_pad / TM;
+    p.m_tiles = ch.rows ? (ch.rows + TM - 1) / TM : op.m_pad / TM;
     p.n_tiles = (ncols + op.dense_tn - 1) / op.dense_tn;
     p.tn = op.dense_tn == TN ? 0 : op.dense_tn;
     p.group = op.group_m;
     p.kblocks = op.kdim / TK;
-    p.KO = tb.K * tb.O;
+    p.KO = ch.rows ? ch.rows : tb.K * tb.O;
+    p.row0 = ch.row0;
+    p.ko_stride = ch.rows ? tb.K * tb.O : 0;
     p.T = tb.T;
     p.ncols = ncols;
     p.c0 = w.c0;

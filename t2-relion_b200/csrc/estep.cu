@@ -1298,6 +1298,8 @@ __global__ void __launch_bounds__(256) k_compact(Tables tb, Work w, int gather_f
 // (src/ml_optimiser.cpp:7090-7272 with exp_ipass == 1).
 constexpr int MAXR = 8, MAXV = 4;
 
+// ONFLY: the chunked configurations' build, which interpolates the fine projections itself
+template <bool ONFLY>
 __global__ void __launch_bounds__(256, 4) k_fine(Tables tb, Work w)
 {
     __shared__ long long item;
@@ -1339,7 +1341,11 @@ __global__ void __launch_bounds__(256, 4) k_fine(Tables tb, Work w)
 #pragma unroll
             for (int r = 0; r < MAXR; r++) {
                 if (r < R) {
-                    const float2 pv = tb.proj_f[((size_t)oc * R + r) * P + p];
+                    // chunked configurations hold no fine table: the same interpolation, here
+                    const float2 pv = !ONFLY ? tb.proj_f[((size_t)oc * R + r) * P + p]
+                                             : project_window_pixel(tb.mdl[oc / tb.O], tb.mvol[oc / tb.O],
+                                                                       tb.eul_f + 9 * ((size_t)(oc % tb.O) * R + r), p,
+                                                                       tb.s);
                     nr[r] += wv * (pv.x * pv.x + pv.y * pv.y);
 #pragma unroll
                     for (int v = 0; v < MAXV; v++) cr[r][v] += pv.x * a[v].x + pv.y * a[v].y;
@@ -1425,8 +1431,9 @@ __global__ void k_group_starts(Tables tb, Work w)
     }
 }
 
-// SCL: with the scale-correction sums (a separate build: they cost the default path 16 registers)
-template <bool SCL>
+// SCL: with the scale-correction sums (a separate build: they cost the default path 16 registers);
+// ONFLY: projections interpolated from the models (chunked configurations hold no table)
+template <bool SCL, bool ONFLY>
 __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, GridPtrs gp)
 {
     __shared__ long long item;
@@ -1507,7 +1514,8 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                     if (SCL)
                         for (int e = 0; e < ne; e++) wsum_e += ent_w[e];
                     for (int n = threadIdx.x; n < P; n += blockDim.x) {
-                        const float2 pv = proj[(size_t)tab * P + n];
+                        const float2 pv = ONFLY ? project_window_pixel(tb.mdl[k], tb.mvol[k], A, n, s)
+                                                : proj[(size_t)tab * P + n];
                         const float c = w.ctf[(size_t)b * P + n] * scale;
                         const float frr = pv.x * c, fri = pv.y * c;
                         const float2 X = w.fimg[(size_t)b * P + n];
@@ -1894,7 +1902,9 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
 
 void launch_fine(const Tables& tb, const Work& w, cudaStream_t st)
 {
-    k_fine<<<(w.fine_ctas > 0 ? w.fine_ctas : 4) * sm_count(), 256, 0, st>>>(tb, w);   // <= 64 registers: <= 4 CTAs per SM
+    const int ctas = (w.fine_ctas > 0 ? w.fine_ctas : 4) * sm_count();
+    if (tb.chunk) k_fine<true><<<ctas, 256, 0, st>>>(tb, w);
+    else k_fine<false><<<ctas, 256, 0, st>>>(tb, w);   // <= 64 registers: <= 4 CTAs per SM
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -1918,10 +1928,15 @@ void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* co
     GridPtrs gp{grid_data, grid_weight};
     k_group_starts<<<2 * sm_count(), 256, 0, st>>>(tb, w);
     const int ctas = (w.wsum_ctas > 0 ? w.wsum_ctas : 4) * sm_count();
-    if (tb.scl_ring && w.r_xa && w.r_aa)
-        k_wsum_bp<true><<<ctas, 256, 0, st>>>(tb, w, g, gp);    // 80 registers: <= 3 CTAs per SM
-    else
-        k_wsum_bp<false><<<ctas, 256, 0, st>>>(tb, w, g, gp);   // 64 registers: <= 4 CTAs per SM
+    const bool scl = tb.scl_ring && w.r_xa && w.r_aa;
+    if (tb.chunk) {
+        if (scl) k_wsum_bp<true, true><<<ctas, 256, 0, st>>>(tb, w, g, gp);
+        else k_wsum_bp<false, true><<<ctas, 256, 0, st>>>(tb, w, g, gp);
+    } else if (scl) {
+        k_wsum_bp<true, false><<<ctas, 256, 0, st>>>(tb, w, g, gp);    // 80 registers: <= 3 CTAs per SM
+    } else {
+        k_wsum_bp<false, false><<<ctas, 256, 0, st>>>(tb, w, g, gp);   // 64 registers: <= 4 CTAs per SM
+    }
     k_results<<<(w.n + 127) / 128, 128, 0, st>>>(tb, w);
     T2B_CUDA(cudaGetLastError());
 }

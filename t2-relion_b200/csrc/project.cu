@@ -27,13 +27,8 @@ __global__ void k_project(const float2* __restrict__ mdl, Volume v, const double
     const int xh = s / 2 + 1, P = s * xh;
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     if (px >= P) return;
-    const int i = px / xh, x = px - i * xh;
-    const int y = (i < xh) ? i : i - s;
-    const int rmo = s / 2;
-    const bool inside = x * x + y * y <= rmo * rmo && x * x + y * y <= v.r_max * v.r_max;
     const int o0 = blockIdx.y * orients, o1 = min(n, o0 + orients);
-    for (int o = o0; o < o1; ++o)
-        out[(size_t)o * P + px] = inside ? project_pixel(mdl, v, eul + 9 * (size_t)o, x, y) : make_float2(0.f, 0.f);
+    for (int o = o0; o < o1; ++o) out[(size_t)o * P + px] = project_window_pixel(mdl, v, eul + 9 * (size_t)o, px, s);
 }
 
 // e^{-2 pi i (kx sx + ky sy)/N} for every pixel of the window

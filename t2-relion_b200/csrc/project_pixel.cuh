@@ -79,4 +79,19 @@ __device__ __forceinline__ float2 project_pixel(const float2* __restrict__ mdl, 
     return make_float2((float)rr, (float)(neg ? -ri : ri));
 }
 
+// Window pixel px (FFTW layout of the s-window) of the projection for Euler matrix A: zero
+// outside the window's circle and the model's r_max (the exact integer radius test), else
+// project_pixel.  The resident tables (k_project) and the on-the-fly projections of the
+// chunked mode both call this, so they hold the same values.
+__device__ __forceinline__ float2 project_window_pixel(const float2* __restrict__ mdl, const Volume& v,
+                                                       const double* A, int px, int s)
+{
+    const int xh = s / 2 + 1;
+    const int i = px / xh, x = px - i * xh;
+    const int y = (i < xh) ? i : i - s;
+    const int rmo = s / 2;
+    const bool inside = x * x + y * y <= rmo * rmo && x * x + y * y <= v.r_max * v.r_max;
+    return inside ? project_pixel(mdl, v, A, x, y) : make_float2(0.f, 0.f);
+}
+
 }  // namespace t2b

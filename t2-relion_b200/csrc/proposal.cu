@@ -1717,6 +1717,8 @@ int t2b_proposal_train(t2b_ctx* c, const t2b_proposal_train_config* cfg, t2b_pro
     return guarded([&] {
         T2B_REQUIRE(c && cfg && rep, T2B_ERR_ARG, "null argument");
         T2B_REQUIRE(c->configured, T2B_ERR_STATE, "t2b_configure must be called before t2b_proposal_train");
+        T2B_REQUIRE(!c->tb.chunk, T2B_ERR_UNSUPPORTED,
+                    "learned proposals need the resident projection tables (this configuration is chunked)");
         const t2b_proposal_train_config& f = *cfg;
         T2B_REQUIRE(f.batch >= 8 && f.batch <= 1024 && f.n_train >= f.batch && f.epochs >= 0 && f.n_val >= 0 &&
                         f.n_posterior >= 0 && f.topk >= 1 && f.topk <= 128 && f.minvsigma2 && f.lr >= 0.f &&
@@ -1927,6 +1929,8 @@ int t2b_proposal_enable(t2b_ctx* c, int topk, int rescore, int audit_every, doub
             return;
         }
         T2B_REQUIRE(c->configured, T2B_ERR_STATE, "t2b_configure must be called before t2b_proposal_enable");
+        T2B_REQUIRE(!c->tb.chunk || topk <= 0, T2B_ERR_UNSUPPORTED,
+                    "learned proposals need the resident projection tables (this configuration is chunked)");
         const int KO = c->tb.K * c->tb.O;
         T2B_REQUIRE(c->net && c->net->trained && c->net->KO == KO, T2B_ERR_STATE,
                     "no trained proposal network for this orientation sampling");

@@ -117,6 +117,10 @@ struct Tables {
     double lpo_min, lpo_max;  // extremes of log(pdf_o) over evaluated orientations
     const unsigned char* scl_ring; // K x (ori_size/2+1): ring enters the scale-correction sums
                                    // (data_vs_prior > 3), or nullptr: do_scale_correction off
+    int chunk;                // > 0: coarse orientations in chunks of this many rows (proj_c holds one
+                              // chunk, proj_f is null: fine and weighted-sum projections on the fly)
+    const float2* const* mdl; // K: device models (on-the-fly projection)
+    const Volume* mvol;       // K: their geometry
 };
 
 // Device views of the batch workspace.
@@ -214,16 +218,23 @@ struct TcOperands {
     void* maps;               // TC_MAP_SLOTS CUtensorMap descriptors (128 B each) in device memory
     int dense_tn = 256;       // N columns of a dense coarse-pass tile (256 or 128; t2b_autotune)
     int group_m = 16;         // orientation tiles per raster group of the dense and audit tiles
+    int chunk = 0;            // > 0: the projection operands hold one chunk of this many rows
+};
+// One chunk of the coarse orientations: rows [row0, row0 + rows) of the K*O layout.
+struct RowChunk {
+    int row0 = 0, rows = 0;   // rows == 0: every row (the resident operands)
 };
 constexpr int TC_MAP_SLOTS = 24;
 size_t tc_kdim(int nk);
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
+// chunked: split rows [0, rows) of the chunk table tb.proj_c into the projection operands
+void tc_split_chunk(const Tables& tb, TcOperands& op, int rows, cudaStream_t st);
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate);
 void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate = nullptr,
-                     int gate_run = 0);
+                     int gate_run = 0, RowChunk ch = RowChunk{}, bool split_w2 = true);
 size_t tc_kn(int nk);
 void tc_launch_diff2(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate = nullptr,
-                     int gate_run = 0);
+                     int gate_run = 0, RowChunk ch = RowChunk{});
 bool tc_supported();
 void tc_encode(void* ptr, int rows, int kdim, bool a_side, void* out128, int box_rows = 0);
 void tc_set_map(TcOperands& op, int slot, void* ptr, int rows, int kdim, bool a_side);

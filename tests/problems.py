@@ -53,7 +53,7 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
     mres = sy.mresol(s)
     oparts = prob.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], mres)
 
-    def product(use_graph=1):
+    def product(use_graph=1, orientation_chunk=0):
         es = t2b.EStep(0)
         for k in range(nr_classes):
             es.set_projector(k, maps[k], ref_dim, r, 2)
@@ -62,7 +62,7 @@ def build(name, n_particles=16, seed=7, nr_classes=1, diff2_mode=0, max_batch=No
                      pdf_direction=pdf_dir, pdf_class=pdf_cls, sigma2_offset=sigma2_offset,
                      pixel_size=p["angpix"], adaptive_oversampling=p["ovs"], diff2_mode=diff2_mode,
                      max_batch=max_batch or n_particles, maximum_significants=maxsig, data_vs_prior=dvp,
-                     use_graph=use_graph)
+                     use_graph=use_graph, orientation_chunk=orientation_chunk)
         return es
 
     def oracle_problem():
