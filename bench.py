@@ -829,6 +829,228 @@ def run_class2d(args, world, rank):
     es.close()
 
 
+# Large 3D classification: K = 4 maps of 256^3 at 0.85 A/px differing by 10 % of their blobs,
+# particles 256 x 256 at SNR 0.02, defocus U(0.8, 2.5) um; HEALPix order 4 x psi 3.75 deg,
+# adaptive oversampling 1, translations range 4 step 1, Fourier radius 100, 515^3 grids.
+LARGE3D = dict(name="class3d_k4_box256_order4_ovs1", ori_size=256, angpix=0.85, n_blobs=40, n_classes=4,
+               map_seed=5, order=4, psi_step=3.75, offset_range=4, offset_step=1, r_max=100, bp_r_max=128,
+               snr=0.02, defocus=(8000., 25000.), seed=73, batch=32)
+METRIC_LARGE3D = "E-step particles/s 3D classification K=4 box256 order4 (chunked split-BF16); roofline %"
+
+
+def large3d_inputs(sy, samp_fn, n, seed):
+    w = LARGE3D
+    K, N, r = w["n_classes"], w["ori_size"], w["r_max"]
+    maps = [sy.fourier_map(v, r) for v in sy.blob_class_volumes(N, K, w["n_blobs"], seed=w["map_seed"])]
+    samp = samp_fn()
+    cls = np.arange(n) % K
+    parts = sy.make_particles(maps[0], n, ori_size=N, s=2 * r, r_max=r, angpix=w["angpix"], snr=w["snr"], seed=seed,
+                              max_shift=w["offset_range"], defocus=w["defocus"], classes=cls, class_maps=maps)
+    return maps, samp, parts, cls
+
+
+def large3d_config():
+    w = LARGE3D
+    s = 2 * w["r_max"]
+    return {"workload": w["name"], "box": w["ori_size"], "classes": w["n_classes"], "healpix_order": w["order"],
+            "psi_step": w["psi_step"], "orientations": w["n_classes"] * 12 * 4 ** w["order"] * int(360 / w["psi_step"]),
+            "translations": 49, "pixels": s * (s // 2 + 1), "adaptive_oversampling": 1, "fine_hypotheses_per_pair": 32,
+            "snr": w["snr"], "grid": [515, 515, 258]}
+
+
+def large3d_cpu(maps, samp, parts, n, n_dir_slice=16):
+    """The reference's CPU coarse kernel (CpuKernels::diff2_coarse, oracle/_ref) on a bounded
+    sample: one particle per host thread over the first n_dir_slice directions x all psi of
+    class 0, extrapolated to every class and orientation (the coarse pass is > 95 % of the
+    CPU E-step).  Returns (particles/s, text) or None without the library."""
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libacc_ref.so")
+    if not os.path.exists(lib_path):
+        return None
+    w = LARGE3D
+    lib = ctypes.CDLL(lib_path)
+    lib.ref_coarse_diff2.restype = ctypes.c_int
+    N, r, s, K = w["ori_size"], w["r_max"], 2 * w["r_max"], w["n_classes"]
+    fm = np.ascontiguousarray(maps[0].view(np.float32))
+    mz, my, mx = maps[0].shape
+    no = n_dir_slice * samp["n_psi"]
+    eul = samp["eul_coarse"][:no].reshape(-1, 3, 3)
+    einv = np.ascontiguousarray(np.transpose(eul, (0, 2, 1)).reshape(-1, 9), np.float32)
+    tx = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 0] / N, np.float32)
+    ty = np.ascontiguousarray(-2 * np.pi * samp["trans_px"][:, 1] / N, np.float32)
+    T = len(tx)
+
+    def one(b):
+        ctf = parts["ctf"][b].astype(np.float64)
+        X = parts["fimg"][b].astype(np.complex128) / ctf
+        re, im = np.ascontiguousarray(X.real, np.float32), np.ascontiguousarray(X.imag, np.float32)
+        corr = np.ascontiguousarray(parts["minv"][b] * ctf * ctf, np.float32)
+        out = np.empty((no, T), np.float32)
+        lib.ref_coarse_diff2(ctypes.c_void_p(fm.ctypes.data), mx, my, mz, -(my // 2), -(mz // 2), r, 2,
+                             ctypes.c_void_p(einv.ctypes.data), no, ctypes.c_void_p(re.ctypes.data),
+                             ctypes.c_void_p(im.ctypes.data), ctypes.c_void_p(corr.ctypes.data), s // 2 + 1, s,
+                             ctypes.c_void_p(tx.ctypes.data), ctypes.c_void_p(ty.ctypes.data), T,
+                             ctypes.c_float(parts["scalars"][b, 1] / 2), ctypes.c_void_p(out.ctypes.data))
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=one, args=(b,)) for b in range(n)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    t = time.perf_counter() - t0
+    total = K * samp["n_dir"] * samp["n_psi"]
+    return n * (no / total) / t, (f"{n} particles, one per host thread, through the reference's "
+                                  f"CpuKernels::diff2_coarse over {no} of {total} class-orientations x {T} "
+                                  f"translations ({t:.1f} s), extrapolated to all of them")
+
+
+def run_large3d(args, world, rank):
+    w = LARGE3D
+    K = w["n_classes"]
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import sampling_oracle as so
+        sy = load_synthetic()
+        n = os.cpu_count() or 1
+        maps, samp, parts, _ = large3d_inputs(
+            sy, lambda: so.sampling(w["order"], w["psi_step"], 0, w["offset_range"], w["offset_step"], w["angpix"]),
+            n, w["seed"] + 1)
+        vals = [large3d_cpu(maps, samp, parts, n) for _ in range(args.steps)]
+        v = float(np.median([x[0] for x in vals]))
+        print(json.dumps({"impl": "reference", "metric": METRIC_LARGE3D, "value": v, "unit": "particles/s",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1000.0 * n / v, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": large3d_config(),
+                          "particles_per_step": n,
+                          "cpu_baseline": {"value": v, "unit": "particles/s", "cores": n, "kind": "reference",
+                                           "sample": vals[-1][1]},
+                          "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    t2b = load_package()
+    import t2relion_b200.synthetic as sy
+    torch.cuda.set_device(local_rank())
+    dev = torch.device("cuda", local_rank())
+    B = w["batch"]
+    steps = args.steps if args.steps_given else 4
+    n_all = B * steps
+    t0 = time.perf_counter()
+    maps, samp, parts, cls = large3d_inputs(
+        sy, lambda: t2b.sampling(3, w["order"], w["psi_step"], 1, w["offset_range"], w["offset_step"], w["angpix"]),
+        n_all, w["seed"] + 1000 * rank)
+    gen_s = time.perf_counter() - t0
+    N, r, s = w["ori_size"], w["r_max"], 2 * w["r_max"]
+    ps = sy.pad_size(w["bp_r_max"])
+    es = t2b.EStep(local_rank())
+    for k in range(K):
+        es.set_projector(k, maps[k], 3, r, 2)
+        es.init_backprojector(k, 3, ps, w["bp_r_max"], 2)
+    t0 = time.perf_counter()
+    es.configure(ori_size=N, current_size=s, ref_dim=3, nr_classes=K, samp=samp,
+                 pdf_direction=np.full((K, samp["n_dir"]), 1.0 / samp["n_dir"]), pdf_class=np.full(K, 1.0 / K),
+                 sigma2_offset=(w["offset_range"] * w["angpix"]) ** 2, pixel_size=w["angpix"],
+                 adaptive_oversampling=1, diff2_mode=t2b.DIFF2_SPLIT_BF16, max_batch=B)
+    conf_s = time.perf_counter() - t0
+    alld = {"fimg": torch.from_numpy(parts["fimg"].view(np.float32)).to(dev),
+            "ctf": torch.from_numpy(parts["ctf"]).to(dev), "minv": torch.from_numpy(parts["minv"]).to(dev),
+            "scal": torch.from_numpy(parts["scalars"]).to(dev)}
+    stage = {k: v[:B].clone() for k, v in alld.items()}
+    res = result_tensors(B, K, samp["n_dir"], dev, N // 2 + 1)
+    rptr = {k: ctypes.c_void_p(v.data_ptr()) for k, v in res.items()}
+    stream = torch.cuda.Stream(dev)
+    poses = []
+
+    def step(i):
+        a = (i % steps) * B
+        with torch.cuda.stream(stream):
+            for k in stage:
+                stage[k].copy_(alld[k][a:a + B], non_blocking=True)
+        es.expectation_device(B, ctypes.c_void_p(stage["fimg"].data_ptr()), ctypes.c_void_p(stage["ctf"].data_ptr()),
+                              ctypes.c_void_p(stage["minv"].data_ptr()), ctypes.c_void_p(stage["scal"].data_ptr()),
+                              rptr, stream=stream.cuda_stream)
+    for i in range(max(args.warmup, 3)):
+        step(i)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank()) as clk:
+        ev0.record(stream)
+        for i in range(steps):
+            step(i)
+            if i == steps - 1:
+                pass
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if int(res["status"].ne(0).sum()) != 0:
+        raise RuntimeError("E-step status errors")
+    value = B * steps / (ms / 1000.0)
+    # poses of every particle against the simulated truth (host entry point, outside the timed region)
+    R = samp["nover_rot"]
+    O = samp["n_dir"] * samp["n_psi"]
+    good_cls, errs = 0, []
+    es.stage_timing(True)
+    st = []
+    for i in range(steps):
+        a = i * B
+        got = es.expectation(*[parts[k][a:a + B] for k in ("fimg", "ctf", "minv", "scalars")])
+        st.append(es.stage_ms())
+        for j in range(B):
+            k, o, rr = got["pose"][j][:3]
+            good_cls += int(k == cls[a + j])
+            Af = samp["eul_fine"][o * R + rr].reshape(3, 3)
+            c = (np.trace(Af @ parts["A"][a + j].T) - 1) / 2
+            errs.append(float(np.degrees(np.arccos(np.clip(c, -1, 1)))))
+    es.stage_timing(False)
+    stages = np.mean(np.array(st), axis=0)
+    peaks, src = measured_peaks()
+    at_max = bool(clk.summary().get("sm_mhz") and clk.summary()["sm_mhz"] >= 0.97 * (clk.summary()["sm_max_mhz"] or 1e9)
+                  and "sw_power_cap" not in clk.summary()["reasons"])
+    peak = peaks.get("bf16_tflops", 1590.0) if at_max else peaks.get("bf16_tflops_sustained", 1400.0)
+    P = s * (s // 2 + 1)
+    T = samp["n_trans"]
+    flops = 8.0 * K * O * T * P * B
+    achieved = flops / (float(stages[2]) / 1000.0) / 1e12
+    line = {"metric": METRIC_LARGE3D, "value": value, "unit": "particles/s", "n_gpus": world, "steps": steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+bf16x3/f64",
+            "data": "synthetic (seeded blob maps, CTF, white noise; stands in for the reference's datasets)",
+            "config": large3d_config(), "particles_per_step": B,
+            "run": {"diff2": "splitbf16, chunked coarse pass (projection tables would need 190 GB coarse + "
+                             "1.5 TB fine)", "input_gen_s": gen_s, "configure_s": conf_s,
+                    "l2": "inputs and model larger than L2; %d distinct particles" % n_all},
+            "gpu_launches": es.launch_count() * steps if es.launch_count() > 0 else None,
+            "clocks": clk.summary(),
+            "quality_vs_truth": {"particles": len(errs), "class_fraction": good_cls / len(errs),
+                                 "orientation_error_deg_median": float(np.median(errs)),
+                                 "within_5deg_fraction": float(np.mean(np.array(errs) < 5.0))},
+            "roofline": {"bound": "tensor", "kernel": "k_diff2_tc (chunked, with the per-chunk projection)",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": src, "traffic": None, "flops_per_launch": flops},
+            "stage_ms": {n: float(v) for n, v in zip(
+                ["prep_network", "operands_audit_norms", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
+                 "wsum_bp", "audit_contraction", "proposal_contraction"], stages)}}
+    # end to end through the host entry point, the same steps
+    t0 = time.perf_counter()
+    for i in range(steps):
+        a = i * B
+        es.expectation(*[parts[k][a:a + B] for k in ("fimg", "ctf", "minv", "scalars")])
+    e2e_s = time.perf_counter() - t0
+    P8 = P * 16 + 64
+    line["e2e"] = {"value": B * steps / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": B * P8,
+                   "d2h_bytes_per_step": sum(v.numel() * v.element_size() for v in res.values()),
+                   "api": "t2b_estep_batch_host (blocking), host arrays"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = large3d_cpu(maps, samp, parts, min(os.cpu_count() or 1, n_all))
+        if cb:
+            line["cpu_baseline"] = {"value": cb[0], "unit": "particles/s", "cores": min(os.cpu_count() or 1, n_all),
+                                    "kind": "reference", "sample": cb[1]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    es.close()
+
+
 def local_rank():
     return int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -862,10 +1084,18 @@ def main():
     ap.add_argument("--no-graph", action="store_true",
                     help="launch each step's kernels one by one instead of replaying its CUDA graph (ncu cannot "
                          "profile the kernel nodes of a graph with conditional nodes; not a bench number)")
-    ap.add_argument("--workload", default="box128", choices=["box128", "class2d"],
+    ap.add_argument("--workload", default="box128", choices=["box128", "class2d", "class3d_large"],
                     help="box128: the 3D refinement headline; class2d: 2D classification, K = 50 references of "
                          "100 x 100, 20,000 particles (its own JSON line)")
     args = ap.parse_args()
+    args.steps_given = any(a == "--steps" or a.startswith("--steps=") for a in sys.argv[1:])
+    if args.workload == "class3d_large":
+        world, rank, _ = dist_init()
+        run_large3d(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload == "class2d":
         world, rank, _ = dist_init()
         run_class2d(args, world, rank)

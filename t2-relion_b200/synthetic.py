@@ -28,6 +28,33 @@ def blob_volume(n, n_blobs=40, sigma=(2.0, 5.0), seed=0, ndim=3):
     return vol
 
 
+def blob_class_volumes(n, n_classes, n_blobs=40, swap_frac=0.1, sigma=(2.0, 5.0), seed=0):
+    """n^3 maps of `n_classes` classes that differ by a subset of their blobs: a seeded set of
+    n_blobs Gaussian blobs, of which each class replaces its own swap_frac share (class k drops
+    blobs [k m, k m + m), m = round(swap_frac n_blobs), and adds m blobs of its own).  Each blob
+    is evaluated inside its own box of +-4 sigma (the rest is below 4e-4 of its peak)."""
+    rng = np.random.default_rng(seed)
+    m = int(round(swap_frac * n_blobs))
+
+    def draw(k):
+        return [(rng.uniform(-0.3 * n, 0.3 * n, 3), rng.uniform(*sigma), rng.uniform(0.5, 1.5)) for _ in range(k)]
+    base = draw(n_blobs)
+    extra = [draw(m) for _ in range(n_classes)]
+    vols = []
+    for k in range(n_classes):
+        blobs = [b for i, b in enumerate(base) if not (k * m <= i < (k + 1) * m)] + extra[k]
+        vol = np.zeros((n, n, n))
+        for c, sg, a in blobs:
+            ctr = c + n // 2
+            lo = np.maximum(np.floor(ctr - 4 * sg).astype(int), 0)
+            hi = np.minimum(np.ceil(ctr + 4 * sg).astype(int) + 1, n)
+            ax = [np.arange(lo[d], hi[d]) - ctr[d] for d in range(3)]
+            r2 = ax[0][:, None, None] ** 2 + ax[1][None, :, None] ** 2 + ax[2][None, None, :] ** 2
+            vol[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] += a * np.exp(-r2 / (2 * sg * sg))
+        vols.append(vol)
+    return vols
+
+
 def pad_size(r_max, padding_factor=2):
     """Projector::initialiseData (src/projector.cpp:56-84)."""
     return 2 * (int(np.floor(padding_factor * r_max + 0.5)) + 1) + 1

@@ -198,3 +198,58 @@ def class2d_k50(n_particles, seed, n_classes=None):
 
     return dict(t2b=t2b, sy=sy, maps=maps, samp=samp, parts=parts, prob=prob, oparts=oparts, product=product,
                 pad_size=ps, K=K, classes=cls)
+
+
+# Large 3D classification: K = 4 maps of 256^3 at 0.85 A/px that differ by 10 % of their blobs,
+# particles 256 x 256 at SNR 0.02, defocus U(0.8, 2.5) um; HEALPix order 4 x psi 3.75 deg
+# (294,912 orientations per class), adaptive oversampling 1, translations range 4 step 1 (49),
+# Fourier radius 100 (200 x 101 pixels), 2x padded grids of r_max 128 (515 x 515 x 258).
+LARGE3D = dict(ori_size=256, angpix=0.85, n_blobs=40, n_classes=4, map_seed=5, order=4, psi_step=3.75,
+               offset_range=4, offset_step=1, r_max=100, bp_r_max=128, snr=0.02, defocus=(8000., 25000.))
+
+
+def large3d(n_particles, seed, with_grids=True):
+    """Inputs and sampling of the large 3D classification, and an oracle Problem for literal
+    per-hypothesis diff2 checks (its own grids are tiny: the full pass is out of the oracle's
+    reach at this size)."""
+    t2b = load_package()
+    import t2relion_b200.synthetic as sy
+    import oracle as orc
+    w = LARGE3D
+    K, N, r = w["n_classes"], w["ori_size"], w["r_max"]
+    s = 2 * r
+    maps = [sy.fourier_map(v, r) for v in sy.blob_class_volumes(N, K, w["n_blobs"], seed=w["map_seed"])]
+    samp = t2b.sampling(3, w["order"], w["psi_step"], 1, w["offset_range"], w["offset_step"], w["angpix"])
+    cls = np.arange(n_particles) % K
+    parts = sy.make_particles(maps[0], n_particles, ori_size=N, s=s, r_max=r, angpix=w["angpix"], snr=w["snr"],
+                              seed=seed, max_shift=w["offset_range"], defocus=w["defocus"], classes=cls,
+                              class_maps=maps)
+    pdf_dir = np.full((K, samp["n_dir"]), 1.0 / samp["n_dir"])
+    pdf_cls = np.full(K, 1.0 / K)
+    sigma2_offset = (w["offset_range"] * w["angpix"]) ** 2
+    ps = sy.pad_size(w["bp_r_max"])
+    prob = orc.Problem(ori_size=N, s=s, ref_dim=3, maps=maps, r_max=r, pad=2, samp=samp, pdf_direction=pdf_dir,
+                       pdf_class=pdf_cls, sigma2_offset=sigma2_offset, pixel_size=w["angpix"],
+                       adaptive_fraction=0.999, ovs=1, bp_pad_size=sy.pad_size(1), bp_r_max=1)
+    oparts = prob.particles(parts["fimg"], parts["ctf"], parts["minv"], parts["scalars"], sy.mresol(s))
+
+    def product(max_batch=None, use_graph=1, orientation_chunk=0):
+        es = t2b.EStep(0)
+        for k in range(K):
+            es.set_projector(k, maps[k], 3, r, 2)
+            if with_grids:
+                es.init_backprojector(k, 3, ps, w["bp_r_max"], 2)
+        es.configure(ori_size=N, current_size=s, ref_dim=3, nr_classes=K, samp=samp, pdf_direction=pdf_dir,
+                     pdf_class=pdf_cls, sigma2_offset=sigma2_offset, pixel_size=w["angpix"],
+                     adaptive_oversampling=1, diff2_mode=1, max_batch=max_batch or n_particles,
+                     use_graph=use_graph, orientation_chunk=orientation_chunk)
+        return es
+
+    return dict(t2b=t2b, sy=sy, maps=maps, samp=samp, parts=parts, prob=prob, oparts=oparts, product=product,
+                pad_size=ps, K=K, classes=cls)
+
+
+def angle_between(A, B):
+    """Rotation angle (degrees) between rotation matrices A and B (3 x 3)."""
+    c = (np.trace(np.asarray(A).reshape(3, 3) @ np.asarray(B).reshape(3, 3).T) - 1) / 2
+    return float(np.degrees(np.arccos(np.clip(c, -1.0, 1.0))))
