@@ -42,9 +42,11 @@ def test_chunked_equals_resident(name, chunk):
     # FP64 sums taken by atomics, whose order is not fixed: equal to the last bits
     for k in ("sum_weight", "coarse_sum_weight", "pmax"):
         assert np.allclose(r0[k], r1[k], rtol=1e-12, atol=0), k
-    for k in ("sumw", "wsum_pdf_class", "wsum_pdf_dir", "wsum_sigma2_offset", "wsum_norm", "wsum_sigma2",
-              "wsum_scale_xa", "wsum_scale_aa"):
+    for k in ("sumw", "wsum_pdf_class", "wsum_pdf_dir", "wsum_sigma2_offset"):
         assert np.allclose(r0[k], r1[k], rtol=1e-10, atol=0), k
+    # per-item sums over pixels taken by FP32 atomics in shared memory: their order is not fixed
+    for k in ("wsum_norm", "wsum_sigma2", "wsum_scale_xa", "wsum_scale_aa"):
+        assert np.allclose(r0[k], r1[k], rtol=1e-6, atol=1e-12 * np.abs(r0[k]).max()), k
     for (da, wa), (db, wb) in zip(g0, g1):
         assert np.max(np.abs(da - db)) <= 1e-5 * np.max(np.abs(da))
         assert np.max(np.abs(wa - wb)) <= 1e-5 * np.max(wa)
