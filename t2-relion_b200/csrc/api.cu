@@ -353,7 +353,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             if (f.orientation_chunk > 0) chunk = f.orientation_chunk;
             else if (resident > 0.6 * (double)fr) chunk = 16384;
             if (chunk >= KO) chunk = 0;
-            chunk = std::min(chunk, O);   // chunks never straddle two classes
+            chunk = std::min({chunk, O, 32768});   // chunks never straddle two classes; one launch row each
         }
         T2B_REQUIRE(chunk == 0 || f.diff2_mode == T2B_DIFF2_SPLIT_BF16, T2B_ERR_UNSUPPORTED,
                     "projection tables do not fit (or orientation_chunk was set): the chunked coarse pass "
@@ -374,7 +374,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
         if (chunk) {
             // one chunk of coarse projections, filled inside each batch; the fine pass and the
             // weighted sums interpolate from the models
-            tb.proj_c = dalloc<float2>(c, (size_t)chunk * P);
+            tb.proj_c = nullptr;   // projections go straight into the chunk's operands
             tb.proj_f = nullptr;
             std::vector<const float2*> mp(c->mdl.begin(), c->mdl.begin() + K);
             std::vector<Volume> mv(c->mvol.begin(), c->mvol.begin() + K);
@@ -571,13 +571,10 @@ void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool
         // split-BF16 operands, the norms and the contraction into the batch's diff2 rows
         if (stage_events) cudaEventRecord(c->ev[2], st);
         bool first = true;
-        float2* table = const_cast<float2*>(tb.proj_c);
         for (int k = 0; k < tb.K; k++)
             for (int o0 = 0; o0 < tb.O; o0 += tb.chunk) {
                 const int n = std::min(tb.chunk, tb.O - o0);
-                launch_project_table(c->mvol[k], c->mdl[k], tb.eul_c + 9 * (size_t)o0, n, tb.s, table, st,
-                                     c->tune.proj_px, c->tune.proj_orients);
-                tc_split_chunk(tb, c->tc, n, st);
+                tc_project_split(tb, c->tc, c->mdl[k], c->mvol[k], tb.eul_c + 9 * (size_t)o0, n, st);
                 RowChunk ch;
                 ch.row0 = k * tb.O + o0;
                 ch.rows = n;
@@ -966,12 +963,13 @@ int t2b_autotune(t2b_ctx* c, const t2b_batch* b, t2b_tune_report* rep)
         }
         c->tune.wsum_ctas = c->wk.wsum_ctas = bw;
         // 4. projection tile: pixels x orientations per CTA, on the first (up to 16384) rows of
-        // the fine (else coarse) table of class 0, rewritten with identical values
-        {
-            // (chunked configurations: the chunk table and the coarse orientations)
-            const bool fine = c->tb.ovs && !c->tb.chunk;
-            const int rows = std::min(c->tb.chunk ? std::min(c->tb.chunk, c->tb.O) : 16384,
-                                      fine ? c->tb.O * c->tb.R : c->tb.O);
+        // the fine (else coarse) table of class 0, rewritten with identical values (chunked
+        // configurations have no table: their projections go straight into the operands)
+        if (c->tb.chunk) {
+            for (int i = 0; i < 9; i++) rep->project_ms[i] = -1.f;
+        } else {
+            const bool fine = c->tb.ovs;
+            const int rows = std::min(16384, fine ? c->tb.O * c->tb.R : c->tb.O);
             float2* out = const_cast<float2*>(fine ? c->tb.proj_f : c->tb.proj_c);
             const double* eul = fine ? c->tb.eul_f : c->tb.eul_c;
             const int pxs[3] = {128, 256, 512}, ors[3] = {1, 2, 4};

@@ -22,6 +22,7 @@
 // T2B_ERR_TIMEOUT in a device flag, waits (bounded) for its own copies and
 // MMAs, frees TMEM and returns.
 #include "t2b_internal.cuh"
+#include "project_pixel.cuh"
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <algorithm>
@@ -599,6 +600,32 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
     lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
+// Chunked coarse pass: the projections of `rows` orientations (Euler matrices eul) interpolated
+// straight into the split-BF16 operands, element (row, kk) = window pixel kpix[kk]: Ph/Pl
+// (re, im pairs, kdim / 2 per row) and the |projection|^2 operand Nh/Nl (kn per row), rows up
+// to rpad and elements beyond nk zero.  The same values as k_project followed by k_split_proj
+// and k_split_norm_proj (one project_window_pixel each), without the FP32 table in between.
+__global__ void __launch_bounds__(256) k_project_split(const float2* __restrict__ mdl, Volume v,
+                                                       const double* __restrict__ eul, int rows, int rpad, int s,
+                                                       const int* __restrict__ kpix, int nk, int kh, int kn,
+                                                       __nv_bfloat162* __restrict__ ph, __nv_bfloat162* __restrict__ pl,
+                                                       __nv_bfloat16* __restrict__ nh, __nv_bfloat16* __restrict__ nl)
+{
+    const int r = blockIdx.y;
+    const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rpad || kk >= kn) return;
+    float2 z = make_float2(0.f, 0.f);
+    if (r < rows && kk < nk) z = project_window_pixel(mdl, v, eul + 9 * (size_t)r, kpix[kk], s);
+    if (kk < kh) {
+        __nv_bfloat16 h0, l0, h1, l1;
+        split_bf16(z.x, h0, l0);
+        split_bf16(z.y, h1, l1);
+        ph[(size_t)r * kh + kk] = __halves2bfloat162(h0, h1);
+        pl[(size_t)r * kh + kk] = __halves2bfloat162(l0, l1);
+    }
+    split_bf16(z.x * z.x + z.y * z.y, nh[(size_t)r * kn + kk], nl[(size_t)r * kn + kk]);
+}
+
 // projections (K*O x P complex) -> Ph/Pl (m_pad x kdim bf16), zero padded
 __global__ void k_split_proj(const float2* __restrict__ proj, int rows, int P, const int* __restrict__ kpix, int nk,
                              int kdim, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long total)
@@ -778,7 +805,20 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
     if (op.chunk == 0) tc_split_chunk(tb, op, rows, st);   // chunked: split per chunk in each batch
 }
 
-// Rows [0, rows) of tb.proj_c into the split-BF16 projection and |projection|^2 operands; the
+void tc_project_split(const Tables& tb, TcOperands& op, const float2* mdl, const Volume& v, const double* eul,
+                      int rows, cudaStream_t st)
+{
+    T2B_REQUIRE(op.bh && op.nh && rows >= 1 && rows <= op.m_pad && op.kn >= op.kdim / 2, T2B_ERR_STATE,
+                "tensor-core operands not allocated");
+    const int rpad = (rows + TM - 1) / TM * TM;
+    dim3 grid((op.kn + 255) / 256, rpad);
+    k_project_split<<<grid, 256, 0, st>>>(mdl, v, eul, rows, rpad, tb.s, tb.kpix, tb.nk, op.kdim / 2, op.kn,
+                                          (__nv_bfloat162*)op.bh, (__nv_bfloat162*)op.bl, (__nv_bfloat16*)op.nh,
+                                          (__nv_bfloat16*)op.nl);
+    T2B_CUDA(cudaGetLastError());
+}
+
+// Rows [0, rows) of the resident table tb.proj_c into the split-BF16 projection and |projection|^2 operands; the
 // rows up to the operands' next multiple of 128 are zeroed.
 void tc_split_chunk(const Tables& tb, TcOperands& op, int rows, cudaStream_t st)
 {

@@ -227,8 +227,11 @@ struct RowChunk {
 constexpr int TC_MAP_SLOTS = 24;
 size_t tc_kdim(int nk);
 void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
-// chunked: split rows [0, rows) of the chunk table tb.proj_c into the projection operands
+// resident tables: split rows [0, rows) of tb.proj_c into the projection operands
 void tc_split_chunk(const Tables& tb, TcOperands& op, int rows, cudaStream_t st);
+// chunked: the projections of `rows` orientations (eul) of one model straight into the operands
+void tc_project_split(const Tables& tb, TcOperands& op, const float2* mdl, const Volume& v, const double* eul,
+                      int rows, cudaStream_t st);
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate);
 void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate = nullptr,
                      int gate_run = 0, RowChunk ch = RowChunk{}, bool split_w2 = true);
