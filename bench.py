@@ -933,7 +933,7 @@ def run_large3d(args, world, rank):
     import t2relion_b200.synthetic as sy
     torch.cuda.set_device(local_rank())
     dev = torch.device("cuda", local_rank())
-    B = w["batch"]
+    B = args.batch if args.batch_given else w["batch"]
     steps = args.steps if args.steps_given else 4
     n_all = B * steps
     t0 = time.perf_counter()
@@ -1089,6 +1089,7 @@ def main():
                          "100 x 100, 20,000 particles (its own JSON line)")
     args = ap.parse_args()
     args.steps_given = any(a == "--steps" or a.startswith("--steps=") for a in sys.argv[1:])
+    args.batch_given = any(a == "--batch" or a.startswith("--batch=") for a in sys.argv[1:])
     if args.workload == "class3d_large":
         world, rank, _ = dist_init()
         run_large3d(args, world, rank)
