@@ -263,7 +263,7 @@ def make_particles(fmap, n, *, ori_size, s, r_max, angpix, snr, seed, max_shift=
                 rot=rot, tilt=tilt, psi=psi, shifts=shifts, A=A, classes=cls, defU=defU, defV=defV, dang=dang)
 
 
-# Named workloads.  Sizes only; seeds are per call.
+# Named workloads: the 3D refinements at box 64 and box 128.  Sizes only; seeds are per call.
 CONFIGS = {
     # 3D refine, CPU-runnable: 64^3, 2 A/px, order 2, psi 7.5, range 3 step 1, r 16
     "refine3d_box64": dict(ori_size=64, angpix=2.0, n_blobs=40, healpix_order=2, psi_step=7.5,
