@@ -834,7 +834,7 @@ def run_class2d(args, world, rank):
 # adaptive oversampling 1, translations range 4 step 1, Fourier radius 100, 515^3 grids.
 LARGE3D = dict(name="class3d_k4_box256_order4_ovs1", ori_size=256, angpix=0.85, n_blobs=40, n_classes=4,
                map_seed=5, order=4, psi_step=3.75, offset_range=4, offset_step=1, r_max=100, bp_r_max=128,
-               snr=0.02, defocus=(8000., 25000.), seed=73, batch=32)
+               snr=0.02, defocus=(8000., 25000.), seed=73, batch=128)
 METRIC_LARGE3D = "E-step particles/s 3D classification K=4 box256 order4 (chunked split-BF16); roofline %"
 
 
@@ -1058,8 +1058,8 @@ def local_rank():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    # 25 steps of 128 particles are one period of the audit pattern (every 50th particle:
-    # 64 audited in 3,200), so the timed steps hold the average mix of 2- and 3-particle audits
+    # 25 steps of 512 particles are whole periods of the audit pattern (every 50th particle:
+    # 256 audited in 12,800), so the timed steps hold the average mix of 10- and 11-particle audits
     ap.add_argument("--steps", type=int, default=25)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -1070,7 +1070,12 @@ def main():
     ap.add_argument("--rescore", type=int, default=PROP["rescore"], help="learned: network candidates rescored")
     ap.add_argument("--train-particles", type=int, default=200000)
     ap.add_argument("--train-epochs", type=int, default=8)
-    ap.add_argument("--batch", type=int, default=128)
+    # particles per step: the audit streams the whole projection operand once per step, so a
+    # larger batch spreads it over more audited particles (128: 110.6k, 256: 93.6k with one
+    # fallback step, 512: 150.6k, 768: 158.0k, 1024: 108.4k with one fallback step, particles/s
+    # on one box); 512 keeps a fallback step -- the whole batch re-run on the full coarse
+    # pass when an audited particle's proposals miss posterior mass -- affordable
+    ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparator and quality check")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
