@@ -956,7 +956,8 @@ def run_large3d(args, world, rank):
     es.configure(ori_size=N, current_size=s, ref_dim=3, nr_classes=K, samp=samp,
                  pdf_direction=np.full((K, samp["n_dir"]), 1.0 / samp["n_dir"]), pdf_class=np.full(K, 1.0 / K),
                  sigma2_offset=(w["offset_range"] * w["angpix"]) ** 2, pixel_size=w["angpix"],
-                 adaptive_oversampling=1, diff2_mode=t2b.DIFF2_SPLIT_BF16, max_batch=B)
+                 adaptive_oversampling=1, diff2_mode=t2b.DIFF2_SPLIT_BF16, max_batch=B,
+                 use_graph=0 if args.no_graph else 1)
     conf_s = time.perf_counter() - t0
     alld = {"fimg": torch.from_numpy(parts["fimg"].view(np.float32)).to(dev),
             "ctf": torch.from_numpy(parts["ctf"]).to(dev), "minv": torch.from_numpy(parts["minv"]).to(dev),
