@@ -58,14 +58,14 @@ METRIC = "E-step particles/s box128: learned+split-BF16 vs plain FP32 GPU; roofl
 PROP = dict(topk=64, rescore=1024, audit_every=50, audit_mass=0.999)
 # end-to-end timing: at least this many steps per timed run
 E2E_STEPS = 30
-# DRAM bytes (read + write) per launch of k_diff2_tc from one ncu capture, stamped with the
+# DRAM bytes (read + write) of k_diff2_tc per step from one ncu capture, stamped with the
 # SHA-256 (first 16 hex digits) of the kernel's source at capture time; a line whose kernel
 # source differs reports traffic null rather than a stale figure.
-#   learned: audit 766.60 MB read + 18.67 MB written, proposal pass 169.96 MB + 0.14 MB (one step)
-#   splitbf16: the full coarse pass, 8.16 GB read + 1.56 GB written per 128 particles
-TRAFFIC = {"kernel_sha": "28a6bb4cdd72dd50",
-           "learned": 766.60e6 + 18.67e6 + 169.96e6 + 0.14e6,
-           "splitbf16_per128": 8.16e9 + 1.56e9}
+#   learned, 512 particles: the audit + proposal launches; captured on the reduced case (HEALPix
+#   order 2), the audit's operand and output scaled x 4 to the 36,864 orientations (audit 273.1 MB
+#   read + 17.4 MB written, proposal pass 675.5 + 6.7 MB, which does not depend on them)
+TRAFFIC = {"kernel_sha": "21c6f5b71dfe045c", "learned_batch": 512,
+           "learned": 4 * (273.1e6 + 17.4e6) + 675.5e6 + 6.7e6}
 # particles of the learned-vs-plain quality check (not the timed batch)
 QUALITY_PARTICLES = 2048
 # timed steps of the plain FP32 comparator (1,154 particles/s: about 0.11 s per 128-particle step)
@@ -1216,7 +1216,7 @@ def main():
             src, peak_kind = "nominal", "FP32 FMA nominal"
         achieved = flops / (gemm / 1000.0) / 1e12
         executed = (12.0 if mode == t2b.DIFF2_SPLIT_BF16 else 4.0) * K * O * T * nk * B / (gemm / 1000.0) / 1e12
-        traffic = TRAFFIC["splitbf16_per128"] * B / 128.0 if (mode == t2b.DIFF2_SPLIT_BF16 and traffic_ok) else None
+        traffic = None   # no capture of the dense pass of this kernel source
         roof = {"bound": bound, "kernel": "k_diff2_tc" if mode else "k_diff2_simt", "achieved": achieved,
                 "executed_tflops": executed, "contraction_pixels": nk,
                 "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src, "peak_kind": peak_kind,
@@ -1250,7 +1250,7 @@ def main():
         roof = {"bound": "tensor", "kernel": "k_diff2_tc (audit + proposal launches)", "achieved": achieved,
                 "executed_tflops": executed, "contraction_pixels": nk, "peak": tensor_peak, "unit": "TFLOP/s",
                 "frac": achieved / tensor_peak, "peak_source": src, "peak_kind": peak_kind,
-                "traffic": TRAFFIC["learned"] if traffic_ok else None,
+                "traffic": TRAFFIC["learned"] if (traffic_ok and B == TRAFFIC["learned_batch"]) else None,
                 "flops_per_launch": f_sum / (2.0 * len(audited)), "audit_ms": t_audit, "proposal_ms": t_prop,
                 "audited_particles": na}
     roof["traffic_capture"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel source (sha256 "
