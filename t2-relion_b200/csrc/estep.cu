@@ -1343,7 +1343,8 @@ __global__ void __launch_bounds__(256, 4) k_fine(Tables tb, Work w)
                 if (r < R) {
                     // chunked configurations hold no fine table: the same interpolation, here
                     const float2 pv = !ONFLY ? tb.proj_f[((size_t)oc * R + r) * P + p]
-                                             : project_window_pixel(tb.mdl[oc / tb.O], tb.mvol[oc / tb.O],
+                                             : project_window_pixel(static_cast<const Quad*>(tb.mdlq[oc / tb.O]),
+                                                                    tb.mvol[oc / tb.O],
                                                                        tb.eul_f + 9 * ((size_t)(oc % tb.O) * R + r), p,
                                                                        tb.s);
                     nr[r] += wv * (pv.x * pv.x + pv.y * pv.y);
@@ -1514,7 +1515,8 @@ __global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, Gr
                     if (SCL)
                         for (int e = 0; e < ne; e++) wsum_e += ent_w[e];
                     for (int n = threadIdx.x; n < P; n += blockDim.x) {
-                        const float2 pv = ONFLY ? project_window_pixel(tb.mdl[k], tb.mvol[k], A, n, s)
+                        const float2 pv = ONFLY ? project_window_pixel(static_cast<const Quad*>(tb.mdlq[k]),
+                                                                       tb.mvol[k], A, n, s)
                                                 : proj[(size_t)tab * P + n];
                         const float c = w.ctf[(size_t)b * P + n] * scale;
                         const float frr = pv.x * c, fri = pv.y * c;

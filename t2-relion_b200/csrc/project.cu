@@ -49,7 +49,29 @@ __global__ void k_phase(const double* __restrict__ shifts, int s, int ori, float
     out[(size_t)t * P + n] = make_float2((float)cs, (float)sn);
 }
 
+// neighbourhood copy of a model: record (z, y, x) = the voxel with its x + 1, y + 1 and
+// (x + 1, y + 1) neighbours (zero past the grid's last column or row)
+__global__ void k_expand_quads(const float2* __restrict__ mdl, Volume v, Quad* __restrict__ out)
+{
+    const size_t n = (size_t)v.xdim * v.ydim * v.zdim;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % v.xdim), y = (int)((i / v.xdim) % v.ydim);
+        const float2 z = make_float2(0.f, 0.f);
+        const float2 a = mdl[i], b = x + 1 < v.xdim ? mdl[i + 1] : z;
+        const float2 c = y + 1 < v.ydim ? mdl[i + v.xdim] : z;
+        const float2 d = (x + 1 < v.xdim && y + 1 < v.ydim) ? mdl[i + v.xdim + 1] : z;
+        out[i].lo = make_float4(a.x, a.y, b.x, b.y);
+        out[i].hi = make_float4(c.x, c.y, d.x, d.y);
+    }
+}
+
 }  // namespace
+
+void launch_expand_quads(const Volume& v, const float2* mdl, void* out, cudaStream_t st)
+{
+    k_expand_quads<<<148 * 8, 256, 0, st>>>(mdl, v, static_cast<Quad*>(out));
+    T2B_CUDA(cudaGetLastError());
+}
 
 void launch_project_table(const Volume& v, const float2* mdl, const double* eul9, int n, int s,
                           float2* out, cudaStream_t st, int px, int orients)

@@ -31,8 +31,40 @@ __device__ __forceinline__ double rot_coord(double a, double b, int pad, int x, 
     return __dadd_rn(__dmul_rn(a * (double)pad, (double)x), __dmul_rn(b * (double)pad, (double)y));
 }
 
-__device__ __forceinline__ float2 project_pixel(const float2* __restrict__ mdl, const Volume& v,
-                                                const double* A, int x, int y)
+// A model as the interpolation reads it: the centred half-complex grid (8 corner loads per
+// trilinear sample), or its neighbourhood copy (Quad: every voxel with its x + 1, y + 1 and
+// (x + 1, y + 1) neighbours in one 32-byte, sector-aligned record; 2 loads per sample).  The
+// values are the same, so is every projection.
+struct Quad {
+    float4 lo, hi;   // (v[z][y][x], v[z][y][x+1]), (v[z][y+1][x], v[z][y+1][x+1])
+};
+
+struct GridFetch {
+    const float2* __restrict__ mdl;
+    // the 2 x 2 corners (z, y..y+1, x..x+1): d[0] = (y, x), d[1] = (y, x+1), d[2] = (y+1, x), d[3] = (y+1, x+1)
+    __device__ __forceinline__ void operator()(const Volume& v, size_t b, float2* d) const
+    {
+        d[0] = mdl[b];
+        d[1] = mdl[b + 1];
+        d[2] = mdl[b + v.xdim];
+        d[3] = mdl[b + v.xdim + 1];
+    }
+};
+
+struct QuadFetch {
+    const Quad* __restrict__ q;
+    __device__ __forceinline__ void operator()(const Volume&, size_t b, float2* d) const
+    {
+        const float4 a = q[b].lo, c = q[b].hi;
+        d[0] = make_float2(a.x, a.y);
+        d[1] = make_float2(a.z, a.w);
+        d[2] = make_float2(c.x, c.y);
+        d[3] = make_float2(c.z, c.w);
+    }
+};
+
+template <typename Fetch>
+__device__ __forceinline__ float2 project_pixel_t(const Fetch& fetch, const Volume& v, const double* A, int x, int y)
 {
     double xp = rot_coord(A[0], A[3], v.pad, x, y);
     double yp = rot_coord(A[1], A[4], v.pad, x, y);
@@ -52,46 +84,62 @@ __device__ __forceinline__ float2 project_pixel(const float2* __restrict__ mdl, 
         if (x0 < 0 || x0 + 1 >= v.xdim || y0 < 0 || y0 + 1 >= v.ydim || z0 < 0 || z0 + 1 >= v.zdim)
             return make_float2(0.f, 0.f);
         const size_t b00 = ((size_t)z0 * v.ydim + y0) * v.xdim + x0;
-        const size_t b01 = b00 + v.xdim;                            // y0+1
-        const size_t b10 = b00 + (size_t)v.ydim * v.xdim;           // z0+1
-        const size_t b11 = b10 + v.xdim;
-        const float2 d000 = mdl[b00], d001 = mdl[b00 + 1];
-        const float2 d010 = mdl[b01], d011 = mdl[b01 + 1];
-        const float2 d100 = mdl[b10], d101 = mdl[b10 + 1];
-        const float2 d110 = mdl[b11], d111 = mdl[b11 + 1];
+        float2 d0[4], d1[4];
+        fetch(v, b00, d0);                                   // z0: (y0, x0) (y0, x0+1) (y0+1, x0) (y0+1, x0+1)
+        fetch(v, b00 + (size_t)v.ydim * v.xdim, d1);         // z0 + 1
         double x00r, x00i, x01r, x01i, x10r, x10i, x11r, x11i, y0r, y0i, y1r, y1i;
-        pp_lerp(fx, d000.x, d000.y, d001.x, d001.y, x00r, x00i);
-        pp_lerp(fx, d100.x, d100.y, d101.x, d101.y, x01r, x01i);
-        pp_lerp(fx, d010.x, d010.y, d011.x, d011.y, x10r, x10i);
-        pp_lerp(fx, d110.x, d110.y, d111.x, d111.y, x11r, x11i);
+        pp_lerp(fx, d0[0].x, d0[0].y, d0[1].x, d0[1].y, x00r, x00i);
+        pp_lerp(fx, d1[0].x, d1[0].y, d1[1].x, d1[1].y, x01r, x01i);
+        pp_lerp(fx, d0[2].x, d0[2].y, d0[3].x, d0[3].y, x10r, x10i);
+        pp_lerp(fx, d1[2].x, d1[2].y, d1[3].x, d1[3].y, x11r, x11i);
         pp_lerp(fy, x00r, x00i, x10r, x10i, y0r, y0i);
         pp_lerp(fy, x01r, x01i, x11r, x11i, y1r, y1i);
         pp_lerp(fz, y0r, y0i, y1r, y1i, rr, ri);
     } else {
         if (x0 < 0 || x0 + 1 >= v.xdim || y0 < 0 || y0 + 1 >= v.ydim) return make_float2(0.f, 0.f);
-        const size_t b0 = (size_t)y0 * v.xdim + x0, b1 = b0 + v.xdim;
-        const float2 d00 = mdl[b0], d01 = mdl[b0 + 1], d10 = mdl[b1], d11 = mdl[b1 + 1];
+        float2 d[4];
+        fetch(v, (size_t)y0 * v.xdim + x0, d);
         double a0r, a0i, a1r, a1i;
-        pp_lerp(fx, d00.x, d00.y, d01.x, d01.y, a0r, a0i);
-        pp_lerp(fx, d10.x, d10.y, d11.x, d11.y, a1r, a1i);
+        pp_lerp(fx, d[0].x, d[0].y, d[1].x, d[1].y, a0r, a0i);
+        pp_lerp(fx, d[2].x, d[2].y, d[3].x, d[3].y, a1r, a1i);
         pp_lerp(fy, a0r, a0i, a1r, a1i, rr, ri);
     }
     return make_float2((float)rr, (float)(neg ? -ri : ri));
+}
+
+__device__ __forceinline__ float2 project_pixel(const float2* __restrict__ mdl, const Volume& v,
+                                                const double* A, int x, int y)
+{
+    return project_pixel_t(GridFetch{mdl}, v, A, x, y);
 }
 
 // Window pixel px (FFTW layout of the s-window) of the projection for Euler matrix A: zero
 // outside the window's circle and the model's r_max (the exact integer radius test), else
 // project_pixel.  The resident tables (k_project) and the on-the-fly projections of the
 // chunked mode both call this, so they hold the same values.
-__device__ __forceinline__ float2 project_window_pixel(const float2* __restrict__ mdl, const Volume& v,
-                                                       const double* A, int px, int s)
+template <typename Fetch>
+__device__ __forceinline__ float2 project_window_pixel_t(const Fetch& fetch, const Volume& v, const double* A, int px,
+                                                         int s)
 {
     const int xh = s / 2 + 1;
     const int i = px / xh, x = px - i * xh;
     const int y = (i < xh) ? i : i - s;
     const int rmo = s / 2;
     const bool inside = x * x + y * y <= rmo * rmo && x * x + y * y <= v.r_max * v.r_max;
-    return inside ? project_pixel(mdl, v, A, x, y) : make_float2(0.f, 0.f);
+    return inside ? project_pixel_t(fetch, v, A, x, y) : make_float2(0.f, 0.f);
+}
+
+__device__ __forceinline__ float2 project_window_pixel(const float2* __restrict__ mdl, const Volume& v,
+                                                       const double* A, int px, int s)
+{
+    return project_window_pixel_t(GridFetch{mdl}, v, A, px, s);
+}
+
+// the same from a model's neighbourhood copy (chunked configurations)
+__device__ __forceinline__ float2 project_window_pixel(const Quad* __restrict__ q, const Volume& v,
+                                                       const double* A, int px, int s)
+{
+    return project_window_pixel_t(QuadFetch{q}, v, A, px, s);
 }
 
 }  // namespace t2b
