@@ -1230,17 +1230,23 @@ def main():
         t_sum = float(np.sum(stage_steps[:, 7] + stage_steps[:, 8])) / 1000.0
         f_prop = 8.0 * PROP["topk"] * T * P * B
         f_sum = sum(8.0 * K * O * T * P * na + f_prop for na in audited)
-        # audit launch: 128-row tiles over every orientation; na_max slots of T columns in
-        # 256-column tiles, or one narrower tile of (na_max - 1) slots when fewer were audited
+        # audit launch: 128-row tiles over every orientation; na_max slots of T columns in the
+        # fewest 256-wide column tiles, each narrowed to a multiple of 32, or the (na_max - 1)-slot
+        # variant when fewer were audited and its tiles cover fewer columns
         na_max = int(np.ceil(B / PROP["audit_every"]))
-        tn_n = ((na_max - 1) * T + 31) // 32 * 32 if na_max > 1 else 0
-        tile_flops = 128 * 256 * kdim * 2 * 3.0
+
+        def audit_shape(cols):
+            nt = (cols + 255) // 256
+            return nt, ((cols + nt - 1) // nt + 31) // 32 * 32
+        full = audit_shape(na_max * T)
+        narrow = audit_shape((na_max - 1) * T) if na_max > 1 else full
+        tile_flops = 128 * kdim * 2 * 3.0
 
         def audit_tiles(na):
             if na == 0:
                 return 0.0
-            narrow = na < na_max and 0 < tn_n <= 256 and tn_n < (na_max * T + 255) // 256 * 256
-            return ((K * O + 127) // 128) * (tn_n / 256.0 if narrow else (na_max * T + 255) // 256)
+            nt, tn = narrow if (na < na_max and narrow[0] * narrow[1] < full[0] * full[1]) else full
+            return ((K * O + 127) // 128) * nt * tn
         # proposal tiles: 128 rows of 128 / kslot particles x T phase rows padded to 32 columns
         ppt = 2 if PROP["topk"] <= 64 else 1
         prop_exec = ((B + ppt - 1) // ppt) * 128 * ((T + 31) // 32 * 32) * kdim * 2 * 3.0

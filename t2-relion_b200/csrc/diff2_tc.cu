@@ -1059,23 +1059,42 @@ void tc_launch_audit_norms(const Tables& tb, TcOperands& op, int na_max, float* 
 
 // Full coarse pass of the audited particles: dense tiles over every
 // orientation against the audit image operand (MAP_IAH/IAL, na_max*T rows).
+// Column tiles: the fewest 256-wide ones for the audited columns, each narrowed to a
+// multiple of 32 (11 audited particles x 81 shifts: 4 x 224 columns, not 4 x 256).
 // The audited count na of a batch is known on the device only: with na_max slots, a
-// batch of fewer audited particles runs the narrower variant (tn_narrow columns for
-// na_max - 1 slots, MAP_IAH_N/IAL_N), a batch of na_max the full one; each launch returns
-// at once unless the count is its own.
+// batch of fewer audited particles runs the narrower variant (na_max - 1 slots,
+// MAP_IAH_N/IAL_N) when its tiles cover fewer columns, a batch of na_max the full one;
+// each launch returns at once unless the count is its own.
+static void audit_shape(int cols, int& n_tiles, int& tn)
+{
+    n_tiles = (cols + TN - 1) / TN;
+    tn = ((cols + n_tiles - 1) / n_tiles + 31) / 32 * 32;
+}
+
+int tc_audit_tn(int na, int T)
+{
+    int nt, tn;
+    audit_shape(na * T, nt, tn);
+    return tn;
+}
+
 int tc_audit_narrow_tn(int na_max, int T)
 {
     if (na_max < 2) return 0;
-    const int tn = ((na_max - 1) * T + 31) / 32 * 32;
-    return (tn <= TN && tn < (na_max * T + TN - 1) / TN * TN) ? tn : 0;
+    int nf, tf, nn, tnn;
+    audit_shape(na_max * T, nf, tf);
+    audit_shape((na_max - 1) * T, nn, tnn);
+    return nn * tnn < nf * tf ? tnn : 0;
 }
 
 void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const int* na, const float* c0a,
                      const float* norma, float* d2a, unsigned* minkeya, int* err, cudaStream_t st)
 {
     TcParams p{};
+    int tf = TN;
     p.m_tiles = op.m_pad / TM;
-    p.n_tiles = (na_max * tb.T + TN - 1) / TN;
+    audit_shape(na_max * tb.T, p.n_tiles, tf);
+    p.tn = tf == TN ? 0 : tf;
     p.kblocks = op.kdim / TK;
     p.KO = tb.K * tb.O;
     p.T = tb.T;
@@ -1091,9 +1110,10 @@ void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const int* na
     const int tn_n = tc_audit_narrow_tn(na_max, tb.T);
     if (tn_n > 0 && na) {
         TcParams q = p;
-        q.n_tiles = 1;
+        int tq = TN;
+        audit_shape((na_max - 1) * tb.T, q.n_tiles, tq);
         q.ncols = (na_max - 1) * tb.T;
-        q.tn = tn_n;
+        q.tn = tq == TN ? 0 : tq;
         q.cnt = na;
         q.cnt_lo = 1;
         q.cnt_hi = na_max - 1;

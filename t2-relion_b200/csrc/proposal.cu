@@ -1447,8 +1447,9 @@ void net_setup(t2b_ctx* c, int na_max)
     N.ia_l = net_dalloc(W, (size_t)ia_rows * op.kdim * sizeof(bf16));
     T2B_CUDA(cudaMemset(N.ia_h, 0, (size_t)ia_rows * op.kdim * sizeof(bf16)));
     T2B_CUDA(cudaMemset(N.ia_l, 0, (size_t)ia_rows * op.kdim * sizeof(bf16)));
-    tc_set_map(c->tc, tc_slot_audit(), N.ia_h, ia_rows, op.kdim, false);
-    tc_set_map(c->tc, tc_slot_audit() + 1, N.ia_l, ia_rows, op.kdim, false);
+    const int tn_f = tc_audit_tn(N.na_max, tb.T);
+    tc_set_map_box(c->tc, tc_slot_audit(), N.ia_h, ia_rows, op.kdim, tn_f);
+    tc_set_map_box(c->tc, tc_slot_audit() + 1, N.ia_l, ia_rows, op.kdim, tn_f);
     if (const int tn_n = tc_audit_narrow_tn(N.na_max, tb.T)) {
         tc_set_map_box(c->tc, tc_slot_audit_narrow(), N.ia_h, ia_rows, op.kdim, tn_n);
         tc_set_map_box(c->tc, tc_slot_audit_narrow() + 1, N.ia_l, ia_rows, op.kdim, tn_n);

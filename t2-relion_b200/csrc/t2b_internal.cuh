@@ -265,6 +265,7 @@ void tc_split_phases(const Tables& tb, const TcOperands& op, int rows, void* hi,
 int tc_slot_audit_w2();
 void tc_launch_audit_norms(const Tables& tb, TcOperands& op, int na_max, float* norma, int* err, cudaStream_t st);
 int tc_audit_narrow_tn(int na_max, int T);
+int tc_audit_tn(int na, int T);   // column-tile width of the audit's full variant
 int tc_slot_audit_narrow();
 void tc_launch_audit(const Tables& tb, TcOperands& op, int na_max, const int* na, const float* c0a,
                      const float* norma, float* d2a, unsigned* minkeya, int* err, cudaStream_t st);
