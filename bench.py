@@ -1272,7 +1272,8 @@ def main():
             "stage_ms": {n: float(v) for n, v in zip(
                 ["prep_network", "operands_audit_norms", "coarse_diff2", "coarse_weights", "fine", "fine_weights",
                  "wsum_bp", "audit_contraction", "proposal_contraction"], stages)},
-            "nr_sign_mean": float(timing["res"]["nr_sign"].double().mean())}
+            "nr_sign_mean": float(timing["res"]["nr_sign"].double().mean()),
+            "n_coarse_sig_mean": float(timing["res"]["n_coarse_sig"].double().mean())}
     if tuned is not None:
         line["run"]["tile_shapes"] = tuned
     if learned is not None:
