@@ -1149,6 +1149,8 @@ def main():
                                      "project_pixels", "project_orients")}
         tuned["tune_s"] = time.perf_counter() - t0
         tuned["coarse_diff2_ms"] = rep["diff2_ms"]
+        tuned["fine_ms"] = rep["fine_ms"]     # per CTAs-per-SM build, 1..4
+        tuned["wsum_ms"] = rep["wsum_ms"]
     learned = None
     if args.mode == "learned":
         # once per iteration, before the E-step: train the proposal network on particles

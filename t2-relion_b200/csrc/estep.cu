@@ -22,6 +22,7 @@
 #include <map>
 #include <algorithm>
 #include <cfloat>
+#include <type_traits>
 
 namespace t2b {
 namespace {
@@ -1298,9 +1299,12 @@ __global__ void __launch_bounds__(256) k_compact(Tables tb, Work w, int gather_f
 // (src/ml_optimiser.cpp:7090-7272 with exp_ipass == 1).
 constexpr int MAXR = 8, MAXV = 4;
 
-// ONFLY: the chunked configurations' build, which interpolates the fine projections itself
-template <bool ONFLY>
-__global__ void __launch_bounds__(256, 4) k_fine(Tables tb, Work w)
+// ONFLY: the chunked configurations' build, which interpolates the fine projections itself.
+// MINB: CTAs per SM the build is register-limited to (256 threads: 64 registers at 4, 85 at 3,
+// 128 at 2).  With more registers all loads of a pixel are in flight at once; with fewer the 40
+// accumulators leave room for only a few.  The tile autotuner picks the build.
+template <bool ONFLY, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_fine(Tables tb, Work w)
 {
     __shared__ long long item;
     __shared__ float red[8][MAXR * MAXV + MAXR];
@@ -1326,30 +1330,35 @@ __global__ void __launch_bounds__(256, 4) k_fine(Tables tb, Work w)
         // cross and norm terms, are zero outside
         for (int k = threadIdx.x; k < tb.nk; k += blockDim.x) {
             const int p = tb.kpix[k];
+            // every load of this pixel first, then the arithmetic
             const float2 c = w.cvec[(size_t)b * P + p];
             const float wv = w.w2[(size_t)b * P + p];
-            float2 a[MAXV];
+            float2 ab[MAXV], pv[MAXR];
 #pragma unroll
-            for (int v = 0; v < MAXV; v++) {
-                if (v < V) {
-                    const float2 ab = tb.ab_f[(size_t)(t * V + v) * P + p];
-                    a[v] = make_float2(c.x * ab.x - c.y * ab.y, c.x * ab.y + c.y * ab.x);
-                } else {
-                    a[v] = make_float2(0.f, 0.f);
-                }
-            }
+            for (int v = 0; v < MAXV; v++)
+                ab[v] = v < V ? tb.ab_f[(size_t)(t * V + v) * P + p] : make_float2(0.f, 0.f);
 #pragma unroll
             for (int r = 0; r < MAXR; r++) {
                 if (r < R) {
                     // chunked configurations hold no fine table: the same interpolation, here
-                    const float2 pv = !ONFLY ? tb.proj_f[((size_t)oc * R + r) * P + p]
-                                             : project_window_pixel(static_cast<const Quad*>(tb.mdlq[oc / tb.O]),
-                                                                    tb.mvol[oc / tb.O],
-                                                                       tb.eul_f + 9 * ((size_t)(oc % tb.O) * R + r), p,
-                                                                       tb.s);
-                    nr[r] += wv * (pv.x * pv.x + pv.y * pv.y);
+                    pv[r] = !ONFLY ? tb.proj_f[((size_t)oc * R + r) * P + p]
+                                   : project_window_pixel(static_cast<const Quad*>(tb.mdlq[oc / tb.O]),
+                                                          tb.mvol[oc / tb.O],
+                                                          tb.eul_f + 9 * ((size_t)(oc % tb.O) * R + r), p, tb.s);
+                } else {
+                    pv[r] = make_float2(0.f, 0.f);
+                }
+            }
+            float2 a[MAXV];
 #pragma unroll
-                    for (int v = 0; v < MAXV; v++) cr[r][v] += pv.x * a[v].x + pv.y * a[v].y;
+            for (int v = 0; v < MAXV; v++)
+                a[v] = make_float2(c.x * ab[v].x - c.y * ab[v].y, c.x * ab[v].y + c.y * ab[v].x);
+#pragma unroll
+            for (int r = 0; r < MAXR; r++) {
+                if (r < R) {
+                    nr[r] += wv * (pv[r].x * pv[r].x + pv[r].y * pv[r].y);
+#pragma unroll
+                    for (int v = 0; v < MAXV; v++) cr[r][v] += pv[r].x * a[v].x + pv[r].y * a[v].y;
                 }
             }
         }
@@ -1434,8 +1443,9 @@ __global__ void k_group_starts(Tables tb, Work w)
 
 // SCL: with the scale-correction sums (a separate build: they cost the default path 16 registers);
 // ONFLY: projections interpolated from the models (chunked configurations hold no table)
-template <bool SCL, bool ONFLY>
-__global__ void __launch_bounds__(256) k_wsum_bp(Tables tb, Work w, Volume g, GridPtrs gp)
+// MINB: CTAs per SM the build is register-limited to (as k_fine; the tile autotuner picks it)
+template <bool SCL, bool ONFLY, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_wsum_bp(Tables tb, Work w, Volume g, GridPtrs gp)
 {
     __shared__ long long item;
     __shared__ int nent;
@@ -1904,9 +1914,19 @@ void launch_weights_coarse(const Tables& tb, const Work& w, int maxsig, cudaStre
 
 void launch_fine(const Tables& tb, const Work& w, cudaStream_t st)
 {
-    const int ctas = (w.fine_ctas > 0 ? w.fine_ctas : 4) * sm_count();
-    if (tb.chunk) k_fine<true><<<ctas, 256, 0, st>>>(tb, w);
-    else k_fine<false><<<ctas, 256, 0, st>>>(tb, w);   // <= 64 registers: <= 4 CTAs per SM
+    const int per_sm = w.fine_ctas > 0 ? std::min(w.fine_ctas, 4) : 4;
+    const int ctas = per_sm * sm_count();
+    const auto run = [&](auto onfly) {
+        constexpr bool F = decltype(onfly)::value;
+        switch (per_sm) {
+        case 1: k_fine<F, 1><<<ctas, 256, 0, st>>>(tb, w); break;
+        case 2: k_fine<F, 2><<<ctas, 256, 0, st>>>(tb, w); break;
+        case 3: k_fine<F, 3><<<ctas, 256, 0, st>>>(tb, w); break;
+        default: k_fine<F, 4><<<ctas, 256, 0, st>>>(tb, w); break;
+        }
+    };
+    if (tb.chunk) run(std::true_type{});
+    else run(std::false_type{});
     T2B_CUDA(cudaGetLastError());
 }
 
@@ -1929,15 +1949,25 @@ void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* co
 {
     GridPtrs gp{grid_data, grid_weight};
     k_group_starts<<<2 * sm_count(), 256, 0, st>>>(tb, w);
-    const int ctas = (w.wsum_ctas > 0 ? w.wsum_ctas : 4) * sm_count();
+    const int per_sm = w.wsum_ctas > 0 ? std::min(w.wsum_ctas, 4) : 4;
+    const int ctas = per_sm * sm_count();
     const bool scl = tb.scl_ring && w.r_xa && w.r_aa;
+    const auto run = [&](auto sclv, auto onfly) {
+        constexpr bool S = decltype(sclv)::value, F = decltype(onfly)::value;
+        switch (per_sm) {
+        case 1: k_wsum_bp<S, F, 1><<<ctas, 256, 0, st>>>(tb, w, g, gp); break;
+        case 2: k_wsum_bp<S, F, 2><<<ctas, 256, 0, st>>>(tb, w, g, gp); break;
+        case 3: k_wsum_bp<S, F, 3><<<ctas, 256, 0, st>>>(tb, w, g, gp); break;
+        default: k_wsum_bp<S, F, 4><<<ctas, 256, 0, st>>>(tb, w, g, gp); break;
+        }
+    };
     if (tb.chunk) {
-        if (scl) k_wsum_bp<true, true><<<ctas, 256, 0, st>>>(tb, w, g, gp);
-        else k_wsum_bp<false, true><<<ctas, 256, 0, st>>>(tb, w, g, gp);
+        if (scl) run(std::true_type{}, std::true_type{});
+        else run(std::false_type{}, std::true_type{});
     } else if (scl) {
-        k_wsum_bp<true, false><<<ctas, 256, 0, st>>>(tb, w, g, gp);    // 80 registers: <= 3 CTAs per SM
+        run(std::true_type{}, std::false_type{});
     } else {
-        k_wsum_bp<false, false><<<ctas, 256, 0, st>>>(tb, w, g, gp);   // 64 registers: <= 4 CTAs per SM
+        run(std::false_type{}, std::false_type{});
     }
     k_results<<<(w.n + 127) / 128, 128, 0, st>>>(tb, w);
     T2B_CUDA(cudaGetLastError());
