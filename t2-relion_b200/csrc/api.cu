@@ -77,6 +77,9 @@ int t2b_create(int device, t2b_ctx** out)
         cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking);
+        for (cudaEvent_t* ev : {&c->fork[0], &c->fork[1]})
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
         for (auto& s : c->in)
             for (cudaEvent_t* ev : {&s.copied, &s.consumed, &s.done})
                 if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
@@ -84,6 +87,9 @@ int t2b_create(int device, t2b_ctx** out)
             for (auto& s : c->in)
                 for (cudaEvent_t ev : {s.copied, s.consumed, s.done})
                     if (ev) cudaEventDestroy(ev);
+            for (cudaEvent_t ev : c->fork)
+                if (ev) cudaEventDestroy(ev);
+            if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
             if (c->d2h_stream) cudaStreamDestroy(c->d2h_stream);
             if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
             if (c->stream) cudaStreamDestroy(c->stream);
@@ -112,6 +118,7 @@ void t2b_destroy(t2b_ctx* c)
         cudaSetDevice(c->device);
         cudaStreamSynchronize(c->copy_stream);
         cudaStreamSynchronize(c->stream);
+        cudaStreamSynchronize(c->aux_stream);
         cudaStreamSynchronize(c->d2h_stream);
         free_allocs(c);
         proposal_release(c);
@@ -123,6 +130,8 @@ void t2b_destroy(t2b_ctx* c)
         for (auto& ev : c->handoff) cudaEventDestroy(ev);
         for (auto& s : c->in)
             for (cudaEvent_t ev : {s.copied, s.consumed, s.done}) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : c->fork) cudaEventDestroy(ev);
+        cudaStreamDestroy(c->aux_stream);
         cudaStreamDestroy(c->d2h_stream);
         cudaStreamDestroy(c->copy_stream);
         cudaStreamDestroy(c->stream);
@@ -572,9 +581,22 @@ void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool
     T2B_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     if (stage_events) cudaEventRecord(c->ev[0], st);
     launch_prep(tb, w, st);
-    if (pm) proposal_infer(c, w, st);
-    if (stage_events) cudaEventRecord(c->ev[1], st);
-    if (pm) proposal_audit(c, w, st, stage_events ? c->ev + 8 : nullptr);
+    if (pm && !stage_events) {
+        // the audit's contraction (tensor cores) needs the prepared images only: a second
+        // branch beside the proposal inference (mostly latency-bound), joined before the
+        // audit mass reads the proposals.  Timed stages keep the two in sequence.
+        T2B_CUDA(cudaEventRecord(c->fork[0], st));
+        T2B_CUDA(cudaStreamWaitEvent(c->aux_stream, c->fork[0], 0));
+        proposal_audit_contract(c, w, c->aux_stream);
+        proposal_infer(c, w, st);
+        T2B_CUDA(cudaEventRecord(c->fork[1], c->aux_stream));
+        T2B_CUDA(cudaStreamWaitEvent(st, c->fork[1], 0));
+        proposal_audit_mass(c, w, st);
+    } else {
+        if (pm) proposal_infer(c, w, st);
+        if (stage_events) cudaEventRecord(c->ev[1], st);
+        if (pm) proposal_audit(c, w, st, stage_events ? c->ev + 8 : nullptr);
+    }
     if (tc) tc_split_images(tb, w, c->tc, st, w.gate);   // the full pass's operand: skipped while proposals hold
     if (tb.chunk) {
         // chunked coarse pass: per chunk of one class's orientations, its projections, their

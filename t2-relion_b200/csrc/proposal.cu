@@ -1621,10 +1621,15 @@ void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st)
 
 void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev)
 {
+    proposal_audit_contract(c, w, st, ev);
+    proposal_audit_mass(c, w, st);
+}
+
+void proposal_audit_contract(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev)
+{
     ProposalNet& N = *c->net;
     const Tables& tb = c->tb;
     TcOperands& op = c->tc;
-    const int KO = tb.K * tb.O;
     k_audit_begin<<<1, 256, 0, st>>>(N.ps, N.audit_b, w.n, N.every, N.na_max, N.minkeya, N.asum, w.r_audit);
     k_audit_operands<<<dim3(tb.T + 1, N.na_max), 256, 0, st>>>(N.ps, N.audit_b, w, tb.T, tb.P, tb.kpix, tb.nk, op.kn,
                                                                op.kdim, tb.ab_c, (bf16*)N.ia_h,
@@ -1634,6 +1639,14 @@ void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev)
     if (ev) cudaEventRecord(ev[0], st);
     tc_launch_audit(tb, op, N.na_max, &N.ps->na, N.c0a, N.norma, N.d2a, N.minkeya, w.err, st);
     if (ev) cudaEventRecord(ev[1], st);
+    T2B_CUDA(cudaGetLastError());
+}
+
+void proposal_audit_mass(t2b_ctx* c, const Work& w, cudaStream_t st)
+{
+    ProposalNet& N = *c->net;
+    const Tables& tb = c->tb;
+    const int KO = tb.K * tb.O;
     k_audit_mass<<<dim3(2 * 148, N.na_max), 256, ((KO + 31) / 32) * sizeof(unsigned), st>>>(tb, w, N.ps, N.audit_b, N.d2a,
                                                                                      N.minkeya, N.asum);
     k_audit_final<<<1, 1024, 0, st>>>(N.ps, N.audit_b, N.asum, N.thr, w.r_audit);

@@ -84,8 +84,13 @@ struct ProposalNet {
 
 // inference, audit and restricted coarse pass of one batch (proposal.cu)
 void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st);
-// ev (optional): two events recorded around the audit / proposal contraction
+// ev (optional): two events recorded around the audit / proposal contraction.
+// proposal_audit = proposal_audit_contract (audited particles, their operands, norms and full
+// contraction: needs the prepared images only) then proposal_audit_mass (the posterior mass
+// inside the proposals, the gate: needs proposal_infer's proposals).
 void proposal_audit(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev = nullptr);
+void proposal_audit_contract(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev = nullptr);
+void proposal_audit_mass(t2b_ctx* c, const Work& w, cudaStream_t st);
 void proposal_coarse(t2b_ctx* c, const Work& w, cudaStream_t st, cudaEvent_t* ev = nullptr);
 void proposal_release(t2b_ctx* c);    // context destruction
 void proposal_invalidate(t2b_ctx* c); // configuration changed

@@ -332,10 +332,14 @@ struct t2b_ctx {
     } in[2];
     cudaStream_t copy_stream = nullptr;
     cudaStream_t d2h_stream = nullptr;
+    // second branch of a learned step: the audit's contraction beside the proposal inference
+    // (fork: recorded after the image preparation; join: after the audit contraction)
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t fork[2]{};
     // Wait for every host batch in flight: its input copies, computation and result reads.
     void quiesce()
     {
-        for (cudaStream_t s : {copy_stream, stream, d2h_stream})
+        for (cudaStream_t s : {copy_stream, stream, aux_stream, d2h_stream})
             if (s) T2B_CUDA(cudaStreamSynchronize(s));
     }
     long long submitted = 0;                  // host batches submitted: the next ticket
