@@ -834,7 +834,7 @@ def run_class2d(args, world, rank):
 # adaptive oversampling 1, translations range 4 step 1, Fourier radius 100, 515^3 grids.
 LARGE3D = dict(name="class3d_k4_box256_order4_ovs1", ori_size=256, angpix=0.85, n_blobs=40, n_classes=4,
                map_seed=5, order=4, psi_step=3.75, offset_range=4, offset_step=1, r_max=100, bp_r_max=128,
-               snr=0.02, defocus=(8000., 25000.), seed=73, batch=128)
+               snr=0.02, defocus=(8000., 25000.), seed=73, batch=256)
 METRIC_LARGE3D = "E-step particles/s 3D classification K=4 box256 order4 (chunked split-BF16); roofline %"
 
 

@@ -1416,6 +1416,26 @@ __device__ __forceinline__ void red_add2(float2* p, float x, float y)
     asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(x), "f"(y) : "memory");
 }
 
+// The two x-neighbours (idx, idx + 1) of one row of a trilinear footprint, weights d0 and d1:
+// from an even idx (the grids are separate cudaMalloc allocations, so 16-byte aligned at every
+// even voxel for the complex values and 8-byte for the weights) one 16-byte reduction of the two
+// complex values and one 8-byte of the two weights; from an odd idx two of each.  The same sums.
+__device__ __forceinline__ void red_xpair(float2* gd, float* gw, size_t idx, float d0, float d1, float vr, float vi,
+                                          float fw)
+{
+    if ((idx & 1) == 0) {
+        asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(gd + idx), "f"(d0 * vr), "f"(d0 * vi),
+                     "f"(d1 * vr), "f"(d1 * vi)
+                     : "memory");
+        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(gw + idx), "f"(d0 * fw), "f"(d1 * fw) : "memory");
+    } else {
+        red_add2(gd + idx, d0 * vr, d0 * vi);
+        red_add(gw + idx, d0 * fw);
+        red_add2(gd + idx + 1, d1 * vr, d1 * vi);
+        red_add(gw + idx + 1, d1 * fw);
+    }
+}
+
 struct GridPtrs {
     float2* const* data;
     float* const* weight;
@@ -1583,20 +1603,18 @@ __global__ void __launch_bounds__(256, MINB) k_wsum_bp(Tables tb, Work w, Volume
                                 const float dd[8] = {mfz * mfy * mfx, mfz * mfy * fx, mfz * fy * mfx, mfz * fy * fx,
                                                      fz * mfy * mfx,  fz * mfy * fx,  fz * fy * mfx,  fz * fy * fx};
 #pragma unroll
-                                for (int cc = 0; cc < 8; cc++) {
-                                    const size_t idx = ((size_t)(z0 + (cc >> 2)) * g.ydim + y0 + ((cc >> 1) & 1)) * g.xdim + x0 + (cc & 1);
-                                    red_add2(&gd[idx], dd[cc] * vr, dd[cc] * vi);
-                                    red_add(&gw[idx], dd[cc] * fw);
+                                for (int cc = 0; cc < 8; cc += 2) {
+                                    const size_t idx = ((size_t)(z0 + (cc >> 2)) * g.ydim + y0 + ((cc >> 1) & 1)) * g.xdim + x0;
+                                    red_xpair(gd, gw, idx, dd[cc], dd[cc + 1], vr, vi, fw);
                                 }
                             } else {
                                 if (x0 < 0 || x0 + 1 >= g.xdim || y0 < 0 || y0 + 1 >= g.ydim) continue;
                                 const float mfx = 1.f - fx, mfy = 1.f - fy;
                                 const float dd[4] = {mfy * mfx, mfy * fx, fy * mfx, fy * fx};
 #pragma unroll
-                                for (int cc = 0; cc < 4; cc++) {
-                                    const size_t idx = (size_t)(y0 + (cc >> 1)) * g.xdim + x0 + (cc & 1);
-                                    red_add2(&gd[idx], dd[cc] * vr, dd[cc] * vi);
-                                    red_add(&gw[idx], dd[cc] * fw);
+                                for (int cc = 0; cc < 4; cc += 2) {
+                                    const size_t idx = (size_t)(y0 + (cc >> 1)) * g.xdim + x0;
+                                    red_xpair(gd, gw, idx, dd[cc], dd[cc + 1], vr, vi, fw);
                                 }
                             }
                         }
