@@ -38,6 +38,10 @@ static void free_allocs(t2b_ctx* c)
     c->drop_graphs();
     for (void* p : c->allocs) cudaFree(p);
     c->allocs.clear();
+    for (cudaTextureObject_t t : c->mtex) cudaDestroyTextureObject(t);
+    for (cudaArray_t a : c->marr) cudaFreeArray(a);
+    c->mtex.clear();
+    c->marr.clear();
     c->configured = false;
 }
 
@@ -368,7 +372,6 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
                     "projection tables do not fit (or orientation_chunk was set): the chunked coarse pass "
                     "runs on the split-BF16 contraction only");
         tb.chunk = chunk;
-        c->mdlq.clear();
         tb.eul_c = (const double*)up(f.eul_coarse, (size_t)O * 9 * sizeof(double));
         tb.trans_c = (const double*)up(f.trans_px, (size_t)T * 2 * sizeof(double));
         tb.trans_prior = (const double*)up(f.trans_prior, (size_t)T * 2 * sizeof(double));
@@ -390,15 +393,17 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             std::vector<Volume> mv(c->mvol.begin(), c->mvol.begin() + K);
             tb.mdl = (const float2* const*)up(mp.data(), K * sizeof(float2*));
             tb.mvol = (const Volume*)up(mv.data(), K * sizeof(Volume));
-            // neighbourhood copies of the models: two 32-byte loads per trilinear sample
-            std::vector<const void*> mq(K);
+            // the models as 3D arrays, read through the texture path (point sampling)
+            std::vector<unsigned long long> mt(K);
             for (int k = 0; k < K; k++) {
-                void* q = dalloc<unsigned char>(c, c->mvol[k].nvox() * 32);
-                launch_expand_quads(c->mvol[k], c->mdl[k], q, st);
-                mq[k] = q;
+                cudaArray_t a = nullptr;
+                cudaTextureObject_t t = 0;
+                make_model_texture(c->mvol[k], c->mdl[k], &a, &t, st);
+                c->marr.push_back(a);
+                c->mtex.push_back(t);
+                mt[k] = (unsigned long long)t;
             }
-            c->mdlq = mq;
-            tb.mdlq = (const void* const*)up(mq.data(), K * sizeof(void*));
+            tb.mtex = (const unsigned long long*)up(mt.data(), K * sizeof(unsigned long long));
         } else {
             // projection tables (per class, resident)
             float2* pc = dalloc<float2>(c, (size_t)KO * P);
@@ -606,7 +611,7 @@ void enqueue_estep(t2b_ctx* c, Work& w, cudaStream_t st, bool stage_events, bool
         for (int k = 0; k < tb.K; k++)
             for (int o0 = 0; o0 < tb.O; o0 += tb.chunk) {
                 const int n = std::min(tb.chunk, tb.O - o0);
-                tc_project_split(tb, c->tc, c->mdlq[k], c->mvol[k], tb.eul_c + 9 * (size_t)o0, n, st);
+                tc_project_split(tb, c->tc, c->mtex[k], c->mvol[k], tb.eul_c + 9 * (size_t)o0, n, st);
                 RowChunk ch;
                 ch.row0 = k * tb.O + o0;
                 ch.rows = n;

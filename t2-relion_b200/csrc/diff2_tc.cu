@@ -605,7 +605,7 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
 // (re, im pairs, kdim / 2 per row) and the |projection|^2 operand Nh/Nl (kn per row), rows up
 // to rpad and elements beyond nk zero.  The same values as k_project followed by k_split_proj
 // and k_split_norm_proj (one project_window_pixel each), without the FP32 table in between.
-__global__ void __launch_bounds__(256) k_project_split(const Quad* __restrict__ mdl, Volume v,
+__global__ void __launch_bounds__(256) k_project_split(cudaTextureObject_t mdl, Volume v,
                                                        const double* __restrict__ eul, int rows, int rpad, int s,
                                                        const int* __restrict__ kpix, int nk, int kh, int kn,
                                                        __nv_bfloat162* __restrict__ ph, __nv_bfloat162* __restrict__ pl,
@@ -805,14 +805,14 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st)
     if (op.chunk == 0) tc_split_chunk(tb, op, rows, st);   // chunked: split per chunk in each batch
 }
 
-void tc_project_split(const Tables& tb, TcOperands& op, const void* mdlq, const Volume& v, const double* eul,
+void tc_project_split(const Tables& tb, TcOperands& op, cudaTextureObject_t mtex, const Volume& v, const double* eul,
                       int rows, cudaStream_t st)
 {
     T2B_REQUIRE(op.bh && op.nh && rows >= 1 && rows <= op.m_pad && op.kn >= op.kdim / 2, T2B_ERR_STATE,
                 "tensor-core operands not allocated");
     const int rpad = (rows + TM - 1) / TM * TM;
     dim3 grid((op.kn + 255) / 256, rpad);
-    k_project_split<<<grid, 256, 0, st>>>(static_cast<const Quad*>(mdlq), v, eul, rows, rpad, tb.s, tb.kpix, tb.nk,
+    k_project_split<<<grid, 256, 0, st>>>(mtex, v, eul, rows, rpad, tb.s, tb.kpix, tb.nk,
                                           op.kdim / 2, op.kn,
                                           (__nv_bfloat162*)op.bh, (__nv_bfloat162*)op.bl, (__nv_bfloat16*)op.nh,
                                           (__nv_bfloat16*)op.nl);

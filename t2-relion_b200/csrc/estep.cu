@@ -1342,7 +1342,7 @@ __global__ void __launch_bounds__(256, MINB) k_fine(Tables tb, Work w)
                 if (r < R) {
                     // chunked configurations hold no fine table: the same interpolation, here
                     pv[r] = !ONFLY ? tb.proj_f[((size_t)oc * R + r) * P + p]
-                                   : project_window_pixel(static_cast<const Quad*>(tb.mdlq[oc / tb.O]),
+                                   : project_window_pixel((cudaTextureObject_t)tb.mtex[oc / tb.O],
                                                           tb.mvol[oc / tb.O],
                                                           tb.eul_f + 9 * ((size_t)(oc % tb.O) * R + r), p, tb.s);
                 } else {
@@ -1545,7 +1545,7 @@ __global__ void __launch_bounds__(256, MINB) k_wsum_bp(Tables tb, Work w, Volume
                     if (SCL)
                         for (int e = 0; e < ne; e++) wsum_e += ent_w[e];
                     for (int n = threadIdx.x; n < P; n += blockDim.x) {
-                        const float2 pv = ONFLY ? project_window_pixel(static_cast<const Quad*>(tb.mdlq[k]),
+                        const float2 pv = ONFLY ? project_window_pixel((cudaTextureObject_t)tb.mtex[k],
                                                                        tb.mvol[k], A, n, s)
                                                 : proj[(size_t)tab * P + n];
                         const float c = w.ctf[(size_t)b * P + n] * scale;

@@ -49,28 +49,44 @@ __global__ void k_phase(const double* __restrict__ shifts, int s, int ori, float
     out[(size_t)t * P + n] = make_float2((float)cs, (float)sn);
 }
 
-// neighbourhood copy of a model: record (z, y, x) = the voxel with its x + 1, y + 1 and
-// (x + 1, y + 1) neighbours (zero past the grid's last column or row)
-__global__ void k_expand_quads(const float2* __restrict__ mdl, Volume v, Quad* __restrict__ out)
-{
-    const size_t n = (size_t)v.xdim * v.ydim * v.zdim;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % v.xdim), y = (int)((i / v.xdim) % v.ydim);
-        const float2 z = make_float2(0.f, 0.f);
-        const float2 a = mdl[i], b = x + 1 < v.xdim ? mdl[i + 1] : z;
-        const float2 c = y + 1 < v.ydim ? mdl[i + v.xdim] : z;
-        const float2 d = (x + 1 < v.xdim && y + 1 < v.ydim) ? mdl[i + v.xdim + 1] : z;
-        out[i].lo = make_float4(a.x, a.y, b.x, b.y);
-        out[i].hi = make_float4(c.x, c.y, d.x, d.y);
-    }
-}
-
 }  // namespace
 
-void launch_expand_quads(const Volume& v, const float2* mdl, void* out, cudaStream_t st)
+void make_model_texture(const Volume& v, const float2* mdl, cudaArray_t* arr, cudaTextureObject_t* tex,
+                        cudaStream_t st)
 {
-    k_expand_quads<<<148 * 8, 256, 0, st>>>(mdl, v, static_cast<Quad*>(out));
-    T2B_CUDA(cudaGetLastError());
+    int dev = 0, m3 = 0;
+    T2B_CUDA(cudaGetDevice(&dev));
+    T2B_CUDA(cudaDeviceGetAttribute(&m3, cudaDevAttrMaxTexture3DWidth, dev));
+    T2B_REQUIRE(v.xdim <= m3 && v.ydim <= m3 && v.zdim <= m3, T2B_ERR_UNSUPPORTED, "model larger than a 3D texture");
+    const cudaChannelFormatDesc cd = cudaCreateChannelDesc<float2>();
+    const cudaExtent ext = make_cudaExtent(v.xdim, v.ydim, v.zdim);
+    cudaArray_t a = nullptr;
+    if (cudaMalloc3DArray(&a, &cd, ext) != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{T2B_ERR_NOMEM, "3D array allocation failed"};
+    }
+    cudaMemcpy3DParms cp = {};
+    cp.srcPtr = make_cudaPitchedPtr(const_cast<float2*>(mdl), (size_t)v.xdim * sizeof(float2), v.xdim, v.ydim);
+    cp.dstArray = a;
+    cp.extent = ext;
+    cp.kind = cudaMemcpyDeviceToDevice;
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = a;
+    cudaTextureDesc td = {};
+    for (int i = 0; i < 3; i++) td.addressMode[i] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t t = 0;
+    cudaError_t e = cudaMemcpy3DAsync(&cp, st);
+    if (e == cudaSuccess) e = cudaCreateTextureObject(&t, &rd, &td, nullptr);
+    if (e != cudaSuccess) {
+        cudaFreeArray(a);
+        T2B_CUDA(e);
+    }
+    *arr = a;
+    *tex = t;
 }
 
 void launch_project_table(const Volume& v, const float2* mdl, const double* eul9, int n, int s,

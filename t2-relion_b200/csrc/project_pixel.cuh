@@ -31,19 +31,18 @@ __device__ __forceinline__ double rot_coord(double a, double b, int pad, int x, 
     return __dadd_rn(__dmul_rn(a * (double)pad, (double)x), __dmul_rn(b * (double)pad, (double)y));
 }
 
-// A model as the interpolation reads it: the centred half-complex grid (8 corner loads per
-// trilinear sample), or its neighbourhood copy (Quad: every voxel with its x + 1, y + 1 and
-// (x + 1, y + 1) neighbours in one 32-byte, sector-aligned record; 2 loads per sample).  The
-// values are the same, so is every projection.
-struct Quad {
-    float4 lo, hi;   // (v[z][y][x], v[z][y][x+1]), (v[z][y+1][x], v[z][y+1][x+1])
-};
-
+// A model as the interpolation reads it: the centred half-complex grid in linear memory (the
+// resident tables' projection), or the same values in a 3D CUDA array read through the texture
+// path with point sampling (the chunked configurations, which interpolate every class-orientation
+// of every batch: the array's block-linear layout keeps a slice's corners in fewer cache lines,
+// and the loads leave the LSU's queue).  Each fetch returns the 2 x 2 corners (z, y..y+1,
+// x..x+1) of grid index (x, y, z) (0-based): d[0] = (y, x), d[1] = (y, x+1), d[2] = (y+1, x),
+// d[3] = (y+1, x+1).  The values are the same, so is every projection.
 struct GridFetch {
     const float2* __restrict__ mdl;
-    // the 2 x 2 corners (z, y..y+1, x..x+1): d[0] = (y, x), d[1] = (y, x+1), d[2] = (y+1, x), d[3] = (y+1, x+1)
-    __device__ __forceinline__ void operator()(const Volume& v, size_t b, float2* d) const
+    __device__ __forceinline__ void operator()(const Volume& v, int x, int y, int z, float2* d) const
     {
+        const size_t b = ((size_t)z * v.ydim + y) * v.xdim + x;
         d[0] = mdl[b];
         d[1] = mdl[b + 1];
         d[2] = mdl[b + v.xdim];
@@ -51,15 +50,16 @@ struct GridFetch {
     }
 };
 
-struct QuadFetch {
-    const Quad* __restrict__ q;
-    __device__ __forceinline__ void operator()(const Volume&, size_t b, float2* d) const
+struct TexFetch {
+    cudaTextureObject_t t;   // float2 texels, point sampling, unnormalised coordinates
+    __device__ __forceinline__ void operator()(const Volume&, int x, int y, int z, float2* d) const
     {
-        const float4 a = q[b].lo, c = q[b].hi;
-        d[0] = make_float2(a.x, a.y);
-        d[1] = make_float2(a.z, a.w);
-        d[2] = make_float2(c.x, c.y);
-        d[3] = make_float2(c.z, c.w);
+        // texel centres: a point-sampled fetch at i + 0.5 returns texel i exactly
+        const float fx = (float)x + 0.5f, fy = (float)y + 0.5f, fz = (float)z + 0.5f;
+        d[0] = tex3D<float2>(t, fx, fy, fz);
+        d[1] = tex3D<float2>(t, fx + 1.f, fy, fz);
+        d[2] = tex3D<float2>(t, fx, fy + 1.f, fz);
+        d[3] = tex3D<float2>(t, fx + 1.f, fy + 1.f, fz);
     }
 };
 
@@ -83,10 +83,9 @@ __device__ __forceinline__ float2 project_pixel_t(const Fetch& fetch, const Volu
         z0 -= v.initz;
         if (x0 < 0 || x0 + 1 >= v.xdim || y0 < 0 || y0 + 1 >= v.ydim || z0 < 0 || z0 + 1 >= v.zdim)
             return make_float2(0.f, 0.f);
-        const size_t b00 = ((size_t)z0 * v.ydim + y0) * v.xdim + x0;
         float2 d0[4], d1[4];
-        fetch(v, b00, d0);                                   // z0: (y0, x0) (y0, x0+1) (y0+1, x0) (y0+1, x0+1)
-        fetch(v, b00 + (size_t)v.ydim * v.xdim, d1);         // z0 + 1
+        fetch(v, x0, y0, z0, d0);                            // z0: (y0, x0) (y0, x0+1) (y0+1, x0) (y0+1, x0+1)
+        fetch(v, x0, y0, z0 + 1, d1);                        // z0 + 1
         double x00r, x00i, x01r, x01i, x10r, x10i, x11r, x11i, y0r, y0i, y1r, y1i;
         pp_lerp(fx, d0[0].x, d0[0].y, d0[1].x, d0[1].y, x00r, x00i);
         pp_lerp(fx, d1[0].x, d1[0].y, d1[1].x, d1[1].y, x01r, x01i);
@@ -98,7 +97,7 @@ __device__ __forceinline__ float2 project_pixel_t(const Fetch& fetch, const Volu
     } else {
         if (x0 < 0 || x0 + 1 >= v.xdim || y0 < 0 || y0 + 1 >= v.ydim) return make_float2(0.f, 0.f);
         float2 d[4];
-        fetch(v, (size_t)y0 * v.xdim + x0, d);
+        fetch(v, x0, y0, 0, d);
         double a0r, a0i, a1r, a1i;
         pp_lerp(fx, d[0].x, d[0].y, d[1].x, d[1].y, a0r, a0i);
         pp_lerp(fx, d[2].x, d[2].y, d[3].x, d[3].y, a1r, a1i);
@@ -135,11 +134,11 @@ __device__ __forceinline__ float2 project_window_pixel(const float2* __restrict_
     return project_window_pixel_t(GridFetch{mdl}, v, A, px, s);
 }
 
-// the same from a model's neighbourhood copy (chunked configurations)
-__device__ __forceinline__ float2 project_window_pixel(const Quad* __restrict__ q, const Volume& v,
-                                                       const double* A, int px, int s)
+// the same from a model's 3D array (chunked configurations)
+__device__ __forceinline__ float2 project_window_pixel(cudaTextureObject_t t, const Volume& v, const double* A, int px,
+                                                       int s)
 {
-    return project_window_pixel_t(QuadFetch{q}, v, A, px, s);
+    return project_window_pixel_t(TexFetch{t}, v, A, px, s);
 }
 
 }  // namespace t2b

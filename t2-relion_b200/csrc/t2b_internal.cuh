@@ -120,7 +120,7 @@ struct Tables {
     int chunk;                // > 0: coarse orientations in chunks of this many rows (proj_c holds one
                               // chunk, proj_f is null: fine and weighted-sum projections on the fly)
     const float2* const* mdl; // K: device models (on-the-fly projection)
-    const void* const* mdlq;  // K: their neighbourhood copies (Quad records, project_pixel.cuh)
+    const unsigned long long* mtex; // K: texture objects over their 3D arrays (project_pixel.cuh)
     const Volume* mvol;       // K: their geometry
 };
 
@@ -189,7 +189,9 @@ void launch_project_table(const Volume& v, const float2* mdl, const double* eul9
                           float2* out, cudaStream_t st, int px = 256, int orients = 1);
 void launch_phase_table(const double* shifts, int n, int s, int ori_size, float2* out, cudaStream_t st);
 // neighbourhood copy of a model (32 bytes per voxel) for the on-the-fly projections
-void launch_expand_quads(const Volume& v, const float2* mdl, void* out, cudaStream_t st);
+// a model as a 3D array of float2 texels and a point-sampled texture object over it
+void make_model_texture(const Volume& v, const float2* mdl, cudaArray_t* arr, cudaTextureObject_t* tex,
+                        cudaStream_t st);
 
 // E-step stages (estep.cu)
 void estep_init_attributes();
@@ -233,7 +235,7 @@ void tc_prepare_projections(const Tables& tb, TcOperands& op, cudaStream_t st);
 // resident tables: split rows [0, rows) of tb.proj_c into the projection operands
 void tc_split_chunk(const Tables& tb, TcOperands& op, int rows, cudaStream_t st);
 // chunked: the projections of `rows` orientations (eul) of one model straight into the operands
-void tc_project_split(const Tables& tb, TcOperands& op, const void* mdlq, const Volume& v, const double* eul,
+void tc_project_split(const Tables& tb, TcOperands& op, cudaTextureObject_t mtex, const Volume& v, const double* eul,
                       int rows, cudaStream_t st);
 void tc_split_images(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate);
 void tc_launch_norms(const Tables& tb, const Work& w, TcOperands& op, cudaStream_t st, const int* gate = nullptr,
@@ -291,7 +293,9 @@ struct t2b_ctx {
     std::mutex mu;
     std::vector<t2b::Volume> mvol;            // per class projector geometry
     std::vector<float2*> mdl;                 // per class device model
-    std::vector<const void*> mdlq;            // chunked configurations: their neighbourhood copies
+    // chunked configurations: the models as 3D arrays, read through the texture path
+    std::vector<cudaArray_t> marr;
+    std::vector<cudaTextureObject_t> mtex;
     std::vector<t2b::Volume> gvol;            // per class BP grid geometry
     std::vector<float2*> gdata;               // per class grid data
     std::vector<float*> gweight;              // per class grid weight
