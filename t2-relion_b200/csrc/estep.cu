@@ -830,6 +830,33 @@ __global__ void __launch_bounds__(256) k_gather_fast(Tables tb, Work w, int fine
 
 // bitonic sort of n2 (power of two) (key, index) pairs in shared memory;
 // by_weight: weight descending then index ascending; else index ascending
+// The first n (<= blockDim.x) pairs sorted in place in bitonic_pairs' order -- by weight
+// descending, ties by index ascending (by_weight), else by index ascending; the indices are
+// distinct, so the order is total -- each thread placing its own pair at its rank (the
+// number of pairs before it): one pass over the pairs, no sorting network.
+__device__ void rank_pairs(double* kw, long long* ki, int n, bool by_weight)
+{
+    double mw = 0.;
+    long long mi = 0;
+    int rank = 0;
+    const bool mine = (int)threadIdx.x < n;
+    if (mine) {
+        mw = kw[threadIdx.x];
+        mi = ki[threadIdx.x];
+        for (int j = 0; j < n; j++) {
+            const double wj = kw[j];
+            const long long ij = ki[j];
+            rank += by_weight ? (wj > mw || (wj == mw && ij < mi)) : (ij < mi);
+        }
+    }
+    __syncthreads();
+    if (mine) {
+        kw[rank] = mw;
+        ki[rank] = mi;
+    }
+    __syncthreads();
+}
+
 __device__ void bitonic_pairs(double* kw, long long* ki, int n2, bool by_weight)
 {
     for (int k = 2; k <= n2; k <<= 1)
@@ -920,18 +947,20 @@ __global__ void __launch_bounds__(1024) k_final_fast(Work w, int fine, int ipass
 // adaptive_fraction * sum (src/ml_optimiser.cpp:7905-7935; the coarse pass also stops
 // at the maxsig-th weight, :7945-7966).  Only the weights >= (1 - f) S / n can be
 // reached before the crossing (all the others together hold less than (1 - f) S), so
-// only they are sorted; the prefix sum over them is a block scan in a fixed order.  The
-// coarse pass also emits the significant list in index order (as k_final_fast).  The
+// only they are sorted (up to 1,024 by rank counting, up to SMALL_SORT bitonically; more are
+// left to the multi-kernel path); the prefix sum over them is a block scan in a fixed order.
+// The coarse pass also emits the significant list in index order (as k_final_fast).  The
 // particle is left marked (fast = 2) so the multi-kernel selection skips it; a coarse
 // list longer than FAST_CAP is left to that path.
 constexpr int SMALL_CAP = 8192;
 constexpr int SMALL_PER = SMALL_CAP / 1024;   // hypotheses per thread
-__global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, int fine, int maxsig, double frac,
+constexpr int SMALL_SORT = 4096;               // candidates the one-CTA selection sorts (shared memory)
+__global__ void __launch_bounds__(1024, 2) k_select_small(Tables tb, Work w, int fine, int maxsig, double frac,
                                                        cudaGraphConditionalHandle cond)
 {
     extern __shared__ unsigned char smem_raw[];
     double* sw = reinterpret_cast<double*>(smem_raw);
-    long long* si = reinterpret_cast<long long*>(smem_raw + SMALL_CAP * sizeof(double));
+    long long* si = reinterpret_cast<long long*>(smem_raw + SMALL_SORT * sizeof(double));
     __shared__ double shd[32];
     __shared__ unsigned long long shu[32];
     __shared__ long long kmin;
@@ -1005,17 +1034,27 @@ __global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, int fi
         const long long i = threadIdx.x + (long long)j * blockDim.x;
         if (i < n && wr[j] > 0. && wr[j] >= floor_w) {
             const int pos = atomicAdd(&ncand, 1);
-            sw[pos] = wr[j];
-            si[pos] = sg.beg + i;
+            if (pos < SMALL_SORT) {
+                sw[pos] = wr[j];
+                si[pos] = sg.beg + i;
+            }
         }
     }
     __syncthreads();
     const int nc = ncand;
+    if (nc > SMALL_SORT) {                          // too many to sort here: the multi-kernel selection
+        if (cond && threadIdx.x == 0) cudaGraphSetConditional(cond, 1);
+        return;
+    }
     int n2 = 1;
     while (n2 < nc) n2 <<= 1;
-    for (int i = nc + threadIdx.x; i < n2; i += blockDim.x) { sw[i] = -1.; si[i] = 0x7fffffffffffffffLL; }
-    __syncthreads();
-    bitonic_pairs(sw, si, n2, true);
+    if (nc <= (int)blockDim.x) {
+        rank_pairs(sw, si, nc, true);
+    } else {
+        for (int i = nc + threadIdx.x; i < n2; i += blockDim.x) { sw[i] = -1.; si[i] = 0x7fffffffffffffffLL; }
+        __syncthreads();
+        bitonic_pairs(sw, si, n2, true);
+    }
     // inclusive prefix sums of the sorted candidates: runs of `per` per thread, then the
     // runs' exclusive offsets by a block scan
     const int per = (n2 + (int)blockDim.x - 1) / (int)blockDim.x;
@@ -1057,11 +1096,15 @@ __global__ void __launch_bounds__(1024) k_select_small(Tables tb, Work w, int fi
             if (cond && threadIdx.x == 0) cudaGraphSetConditional(cond, 1);
             return;
         }
-        int m2 = 1;
-        while (m2 < cnt) m2 <<= 1;
-        for (int i = cnt + threadIdx.x; i < m2; i += blockDim.x) { sw[i] = 0.; si[i] = 0x7fffffffffffffffLL; }
-        __syncthreads();
-        bitonic_pairs(sw, si, m2, false);
+        if (cnt <= (int)blockDim.x) {
+            rank_pairs(sw, si, cnt, false);
+        } else {
+            int m2 = 1;
+            while (m2 < cnt) m2 <<= 1;
+            for (int i = cnt + threadIdx.x; i < m2; i += blockDim.x) { sw[i] = 0.; si[i] = 0x7fffffffffffffffLL; }
+            __syncthreads();
+            bitonic_pairs(sw, si, m2, false);
+        }
         for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
             w.flist_w[(size_t)b * FAST_CAP + i] = sw[i];
             w.flist_i[(size_t)b * FAST_CAP + i] = si[i];
@@ -1784,7 +1827,7 @@ int grid_x_for(int nb)
 
 const size_t HIST_SMEM = HIST_BINS * (sizeof(unsigned) + sizeof(double));
 const size_t FAST_SMEM = FAST_CAP * (sizeof(double) + sizeof(long long));
-const size_t SMALL_SMEM = SMALL_CAP * (sizeof(double) + sizeof(long long));
+const size_t SMALL_SMEM = SMALL_SORT * (sizeof(double) + sizeof(long long));
 
 // a stream per device and nesting depth to capture conditional-node bodies on
 cudaStream_t body_stream(int depth)
