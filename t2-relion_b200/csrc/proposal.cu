@@ -278,24 +278,31 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
     if (!ranked) {
         // the set only, in index order: keys above the k-th, then the first ties at it;
         // thread t owns the contiguous index range [t*per, (t+1)*per)
-        __shared__ unsigned sc_hi[1024], sc_eq[1024];
+        __shared__ unsigned wsum_hi[32], wsum_eq[32];
         const int per = (KO + blockDim.x - 1) / blockDim.x;
         const int i0 = threadIdx.x * per, i1 = min(KO, i0 + per);
         unsigned nhi = 0, neq = 0;
         for (int i = i0; i < i1; i++) { nhi += keys[i] > kth; neq += keys[i] == kth; }
-        sc_hi[threadIdx.x] = nhi;
-        sc_eq[threadIdx.x] = neq;
-        __syncthreads();
-        for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-            const unsigned a = threadIdx.x >= off ? sc_hi[threadIdx.x - off] : 0u;
-            const unsigned e = threadIdx.x >= off ? sc_eq[threadIdx.x - off] : 0u;
-            __syncthreads();
-            sc_hi[threadIdx.x] += a;
-            sc_eq[threadIdx.x] += e;
-            __syncthreads();
+        // prefix sums over the threads in order: within the warp by shuffles, then over the warps
+        unsigned hi = nhi, eq = neq;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned a = __shfl_up_sync(0xffffffffu, hi, o), e = __shfl_up_sync(0xffffffffu, eq, o);
+            if (lane >= o) { hi += a; eq += e; }
         }
-        const unsigned total_hi = sc_hi[blockDim.x - 1];
-        unsigned ph = sc_hi[threadIdx.x] - nhi, pe = sc_eq[threadIdx.x] - neq;
+        if (lane == 31) { wsum_hi[wid] = hi; wsum_eq[wid] = eq; }
+        __syncthreads();
+        const int nw = blockDim.x >> 5;
+        if (wid == 0) {
+            unsigned th = lane < nw ? wsum_hi[lane] : 0u, te = lane < nw ? wsum_eq[lane] : 0u;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned a = __shfl_up_sync(0xffffffffu, th, o), e = __shfl_up_sync(0xffffffffu, te, o);
+                if (lane >= o) { th += a; te += e; }
+            }
+            if (lane < nw) { wsum_hi[lane] = th; wsum_eq[lane] = te; }   // inclusive over the warps
+        }
+        __syncthreads();
+        const unsigned total_hi = wsum_hi[nw - 1];
+        unsigned ph = (wid > 0 ? wsum_hi[wid - 1] : 0u) + hi - nhi, pe = (wid > 0 ? wsum_eq[wid - 1] : 0u) + eq - neq;
         for (int i = i0; i < i1; i++) {
             if (keys[i] > kth) {
                 prop[(size_t)b * k + ph++] = i;
@@ -430,30 +437,60 @@ __global__ void __launch_bounds__(256) k_rescore_gather(int n, int k1, int nring
     if (lane == 0) rnorm[gw] = acc;
 }
 
-// the k best-scored candidates of each particle, ranked (ties by rank in the network's list)
+// the k best-scored candidates of each particle, ranked (ties by rank in the network's list):
+// a bitonic sort of the keys (score, then the candidate's position), descending.  Up to 1,024
+// candidates (the usual K1) one key per thread: the exchanges with a partner in the same warp
+// (distance < 32) are shuffles, only the wider ones go through shared memory and a barrier
+// (15 barriers instead of 55 for 1,024 keys); the same network, the same order.
 __global__ void __launch_bounds__(1024) k_rescore_select(const int* __restrict__ cand, const float* __restrict__ score,
                                                          int k1, int k, int* __restrict__ prop)
 {
     __shared__ unsigned long long key[NET_TOPK_CAND];
     const int b = blockIdx.x;
+    const auto key_of = [&](int i) -> unsigned long long {
+        // keys are > 0 (the low word holds ~i): padding with 0 sorts last
+        return i < k1 ? ((unsigned long long)f2key(score[(size_t)b * k1 + i]) << 32) | (unsigned)(0xffffffffu - (unsigned)i)
+                      : 0ull;
+    };
     int n2 = 1;
     while (n2 < k1) n2 <<= 1;
-    for (int i = threadIdx.x; i < n2; i += blockDim.x)
-        key[i] = i < k1 ? ((unsigned long long)f2key(score[(size_t)b * k1 + i]) << 32) | (unsigned)(0xffffffffu - (unsigned)i)
-                        : 0ull;
-    __syncthreads();
-    for (int kk = 2; kk <= n2; kk <<= 1)
-        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
-            for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-                const int l = i ^ jj;
-                if (l > i) {
-                    const bool desc = (i & kk) == 0;
-                    const unsigned long long a = key[i], c = key[l];
-                    if (desc ? (a < c) : (a > c)) { key[i] = c; key[l] = a; }
+    if (n2 <= (int)blockDim.x) {
+        const int i = threadIdx.x;
+        const int nb = blockDim.x;   // sorted as nb keys (the padding at the end)
+        unsigned long long v = key_of(i);
+        for (int kk = 2; kk <= nb; kk <<= 1)
+            for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+                unsigned long long o;
+                if (jj >= 32) {
+                    key[i] = v;
+                    __syncthreads();
+                    o = key[i ^ jj];
+                    __syncthreads();
+                } else {
+                    o = __shfl_xor_sync(0xffffffffu, v, jj);
                 }
+                // the pair (i, i ^ jj): in a descending block the lower index keeps the larger
+                const bool keep_max = ((i & kk) == 0) == ((i & jj) == 0);
+                v = keep_max ? (v > o ? v : o) : (v < o ? v : o);
             }
-            __syncthreads();
-        }
+        key[i] = v;
+        __syncthreads();
+    } else {
+        for (int i = threadIdx.x; i < n2; i += blockDim.x) key[i] = key_of(i);
+        __syncthreads();
+        for (int kk = 2; kk <= n2; kk <<= 1)
+            for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+                for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+                    const int l = i ^ jj;
+                    if (l > i) {
+                        const bool desc = (i & kk) == 0;
+                        const unsigned long long a = key[i], c = key[l];
+                        if (desc ? (a < c) : (a > c)) { key[i] = c; key[l] = a; }
+                    }
+                }
+                __syncthreads();
+            }
+    }
     for (int j = threadIdx.x; j < k; j += blockDim.x) {
         const int r = (int)(0xffffffffu - (unsigned)(key[j] & 0xffffffffull));
         prop[(size_t)b * k + j] = cand[(size_t)b * k1 + r];
