@@ -389,9 +389,7 @@ int t2b_configure(t2b_ctx* c, const t2b_config* cfg)
             // weighted sums interpolate from the models
             tb.proj_c = nullptr;   // projections go straight into the chunk's operands
             tb.proj_f = nullptr;
-            std::vector<const float2*> mp(c->mdl.begin(), c->mdl.begin() + K);
             std::vector<Volume> mv(c->mvol.begin(), c->mvol.begin() + K);
-            tb.mdl = (const float2* const*)up(mp.data(), K * sizeof(float2*));
             tb.mvol = (const Volume*)up(mv.data(), K * sizeof(Volume));
             // the models as 3D arrays, read through the texture path (point sampling)
             std::vector<unsigned long long> mt(K);

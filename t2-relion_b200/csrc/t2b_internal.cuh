@@ -119,8 +119,8 @@ struct Tables {
                                    // (data_vs_prior > 3), or nullptr: do_scale_correction off
     int chunk;                // > 0: coarse orientations in chunks of this many rows (proj_c holds one
                               // chunk, proj_f is null: fine and weighted-sum projections on the fly)
-    const float2* const* mdl; // K: device models (on-the-fly projection)
-    const unsigned long long* mtex; // K: texture objects over their 3D arrays (project_pixel.cuh)
+    const unsigned long long* mtex; // K: texture objects over the models' 3D arrays (on-the-fly
+                                    // projection, project_pixel.cuh)
     const Volume* mvol;       // K: their geometry
 };
 
