@@ -7,7 +7,8 @@ the weighted sums interpolate their projections from the models.  Every diff2 is
 product over the same contraction blocks and every projection the same FP64 interpolation, so
 coarse and fine diff2, weights, poses and sums equal the resident pass's bit for bit; the
 grids and the FP64 sums of weights differ only by the order of their atomic additions.  Chunks of 1,000 and 700 rows
-over 2 classes: partial chunks, and chunks that end at a class boundary.
+over 2 classes: partial chunks, and chunks that end at a class boundary; and 2D references (60
+psi per class in chunks of 40), whose models are read as one-voxel-deep 3D textures.
 """
 import numpy as np
 import pytest
@@ -17,7 +18,7 @@ import problems
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name,chunk", [("refine_o2", 1000), ("refine_o1_ovs", 700)])
+@pytest.mark.parametrize("name,chunk", [("refine_o2", 1000), ("refine_o1_ovs", 700), ("class2d", 40)])
 def test_chunked_equals_resident(name, chunk):
     pb = problems.build(name, n_particles=12, seed=43, nr_classes=2, diff2_mode=1, scale_correction=True)
     P = pb["parts"]
