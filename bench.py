@@ -62,10 +62,10 @@ E2E_STEPS = 30
 # SHA-256 (first 16 hex digits) of the kernel's source at capture time; a line whose kernel
 # source differs reports traffic null rather than a stale figure.
 #   learned, 512 particles: the audit + proposal launches; captured on the reduced case (HEALPix
-#   order 2), the audit's operand and output scaled x 4 to the 36,864 orientations (audit 267.8 MB
-#   read + 16.9 MB written, proposal pass 675.5 + 6.3 MB, which does not depend on them)
-TRAFFIC = {"kernel_sha": "d3baa023a20ba317", "learned_batch": 512,
-           "learned": 4 * (267.8e6 + 16.9e6) + 675.5e6 + 6.3e6}
+#   order 2), the audit's operand and output scaled x 4 to the 36,864 orientations (audit 267.5 MB
+#   read + 16.8 MB written, proposal pass 675.5 + 6.3 MB, which does not depend on them)
+TRAFFIC = {"kernel_sha": "84303c0f85bebd48", "learned_batch": 512,
+           "learned": 4 * (267.5e6 + 16.8e6) + 675.5e6 + 6.3e6}
 # particles of the learned-vs-plain quality check (not the timed batch)
 QUALITY_PARTICLES = 2048
 # timed steps of the plain FP32 comparator (1,154 particles/s: about 0.11 s per 128-particle step)
