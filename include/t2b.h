@@ -213,15 +213,27 @@ int t2b_reconstruct_divide(t2b_ctx* ctx, int iclass, double* fconv);
  * width 3, average background), sinc^2 gridding correction.  vol: host,
  * ori_size^3 doubles [z][y][x] (a 2D grid of 2D classification: ori_size^2,
  * normalisation pad^2), centre at ori_size/2.  pad * ori_size must be
- * a product of 2, 3, 5 and <= 512.  The gridding iterations
- * (--dont_skip_gridding) are not implemented. */
+ * a product of 2, 3, 5 and <= 512.  With gridding_iter > 0 (--dont_skip_gridding,
+ * src/backprojector.cpp:1532-1655) the division is replaced by the iterative
+ * gridding weights of Pipe & Menon: data and weight divided by normalise, weights
+ * w = 1 inside ROUND(r_max pad)^2, each iteration convolving w * weight with the
+ * blob (radius 3.8, alpha 15) through inverse and forward FFTs of the pad_size box
+ * (FP32, shared-memory FFTs of any size) and dividing w by max(1e-6, |result|);
+ * Fconv = data * w.  Expects the Hermitian-symmetrised grid
+ * (t2b_backprojector_enforce_hermitian), as MlOptimiser::maximization provides it. */
 typedef struct t2b_recon_config {
     int ori_size;               /* model box                                       */
     int do_map;                 /* add the inverse tau2 spectrum to the weights    */
     int minres_map;             /* first shell that gets the MAP term              */
-    int _pad;
+    int gridding_iter;          /* 0: skip gridding (the default); > 0: that many
+                                   iterations of the gridding weights
+                                   (--dont_skip_gridding, gridding_nr_iter, 10 in
+                                   the reference; src/backprojector.cpp:1532-1655) */
     double tau2_fudge;
     const double* tau2;         /* ori_size/2+1 (host); required with do_map       */
+    double normalise;           /* gridding only: data and weight are divided by it
+                                   first (the class's sum of weights, pdf_class;
+                                   src/ml_optimiser.cpp:4861-4867)                 */
 } t2b_recon_config;
 int t2b_reconstruct(t2b_ctx* ctx, int iclass, const t2b_recon_config* cfg, double* vol);
 

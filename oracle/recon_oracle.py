@@ -22,6 +22,18 @@ complex, weight real; z, y centred at -initz, -inity; x from 0; 3D grids of
                     ori_size / 2, cosine width 3, average background); and
                     Projector::griddingCorrect (src/projector.cpp:489-522:
                     divide by sinc^2 of r / (ori_size pad), trilinear)
+                    With gridding_iter > 0 (--dont_skip_gridding, :1532-1655), the
+                    division is replaced by the iterative weights of Pipe & Menon
+                    (1999): data and weight divided by `normalise`; weights w_n = 1
+                    inside r^2 < max_r2; each iteration convolves w_n * weight with the
+                    blob (inverse FFT, multiply by the blob's tabulated Fourier
+                    transform over its value at 0, forward FFT:
+                    BackProjector::convoluteBlobRealSpace, :2439-2480) and divides w_n
+                    by max(1e-6, |result|) inside max_r2; then Fconv = data * w_n.
+  ftblob_table      TabFtBlob (src/tabfuncs.cpp:95-121): the Fourier transform of the
+                    order-0 Kaiser-Bessel blob of radius 3.8 and alpha 15 in 3D
+                    (Lewitt 1990), 10,000 samples over [0, 0.5), looked up at
+                    floor(|r| / 5e-5), 0 beyond
   enforce_hermitian_symmetry
                     BackProjector::enforceHermitianSymmetry (src/backprojector.cpp:2104-2121),
                     applied by MlOptimiser::maximization before reconstruct
@@ -73,9 +85,62 @@ def enforce_hermitian_symmetry(data, weight):
     return (d[0], w[0]) if two_d else (d, w)
 
 
-def decenter_divide(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_map=0):
-    """Fconv of the pad_size box (FFTW layout [ps][ps][ps/2+1], 2D: [ps][ps/2+1]) after the MAP
-    term and the skip-gridding division, FP64."""
+def ftblob_table(radius=3.8, alpha=15.0, nr=10000):
+    """The blob's Fourier transform sampled at w = i * 0.5 / nr (TabFtBlob::fillTable): for the
+    order-0 Kaiser-Bessel blob in 3D, (2 pi)^(3/2) a^3 I_{3/2}(s) / (I_0(alpha) s^(3/2)) with
+    s = sqrt(alpha^2 - (2 pi a w)^2), and J_{3/2} of sqrt((2 pi a w)^2 - alpha^2) where
+    2 pi a w > alpha; the half-integer Bessel functions in closed form."""
+    w = np.arange(nr) * (0.5 / nr)
+    u = 2.0 * PI * radius * w
+    s = np.sqrt(np.abs(alpha * alpha - u * u))
+    i32 = np.sqrt(2.0 / (PI * s)) * (np.cosh(s) - np.sinh(s) / s)
+    j32 = np.sqrt(2.0 / (PI * s)) * (np.sin(s) / s - np.cos(s))
+    bes = np.where(u > alpha, j32, i32)
+    return (2.0 * PI) ** 1.5 * radius ** 3 * bes / (np.i0(alpha) * s ** 1.5)
+
+
+def _fftw_coords(ps, two_d):
+    fx = ps // 2 + 1
+    k = np.arange(ps)
+    kp = np.where(k < fx, k, k - ps)
+    kz = np.zeros(1, np.int64) if two_d else kp
+    return np.meshgrid(kz, kp, np.arange(fx), indexing="ij")
+
+
+def gridding_weights(W, ps, ori_size, pad, max_r2, niter, two_d=False):
+    """The iterative weights (FFTW layout of W, FP64) of BackProjector::reconstruct's gridding
+    branch, W already divided by `normalise`."""
+    KP, IP, JP = _fftw_coords(ps, two_d)
+    inside = (KP * KP + IP * IP + JP * JP) < max_r2
+    FN = inside.astype(float)
+    tab = ftblob_table()
+    ph = ps // 2
+    k = np.arange(ps)
+    kc = np.where(k < ph, k, k - ps)
+    if two_d:
+        r2 = kc[:, None] ** 2 + kc[None, :] ** 2
+    else:
+        r2 = kc[:, None, None] ** 2 + kc[None, :, None] ** 2 + kc[None, None, :] ** 2
+    rval = np.sqrt(r2.astype(float)) / (ori_size * pad)
+    idx = (np.abs(rval) / (0.5 / 10000)).astype(np.int64)
+    B = np.where(idx < tab.size, tab[np.minimum(idx, tab.size - 1)], 0.0) / tab[0]
+    axes = (0, 1) if two_d else (0, 1, 2)
+    shape = (ps, ps) if two_d else (ps, ps, ps)
+    for _ in range(niter):
+        G = FN * W
+        G = G[0] if two_d else G
+        real = np.fft.irfftn(G, s=shape, axes=axes)
+        conv = np.fft.rfftn(real * B, axes=axes)
+        conv = conv[None] if two_d else conv
+        w = np.maximum(1e-6, np.abs(conv))
+        FN = np.where(inside, FN / w, FN)
+    return FN
+
+
+def decenter(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_map=0):
+    """Projector::decenter of data and weight to the FFTW layout of the pad_size box
+    (r^2 <= ROUND(r_max pad)^2), the MAP term added to the weight; FP64, 3D layout (a 2D
+    grid as one plane).  Returns F, W, r2, max_r2."""
     two_d = weight.ndim == 2
     if two_d:
         data, weight = data[None], weight[None]
@@ -105,6 +170,20 @@ def decenter_divide(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_
         invtau2 = np.where(t > 0, 1.0 / (oc * tau2_fudge * np.where(t > 0, t, 1.0)),
                            np.where(invw > 1e-20, 1.0 / (0.001 * np.where(invw > 1e-20, invw, 1.0)), 0.0))
         W[m] = np.where(ires >= minres_map, invw + invtau2, invw)
+    return F, W, r2, max_r2
+
+
+def decenter_divide(data, weight, r_max, pad, tau2=None, tau2_fudge=1.0, minres_map=0, gridding_iter=0,
+                    normalise=1.0, ori_size=None):
+    """Fconv of the pad_size box (FFTW layout [ps][ps][ps/2+1], 2D: [ps][ps/2+1]) after the MAP
+    term and the skip-gridding division (gridding_iter 0), or the gridding iterations, FP64."""
+    two_d = weight.ndim == 2
+    F, W, r2, max_r2 = decenter(data, weight, r_max, pad, tau2, tau2_fudge, minres_map)
+    if gridding_iter > 0:
+        ps = W.shape[1]
+        FN = gridding_weights(W / normalise, ps, ori_size, pad, max_r2, gridding_iter, two_d)
+        out = F / normalise * FN
+        return out[0] if two_d else out
     # radial averages below ROUND((r_max pad)^2)
     rr2 = int(relion_round(r_max * pad * r_max * pad))
     m = r2 < rr2
@@ -139,11 +218,12 @@ def soft_mask_bg(vol, radius, width):
     return res
 
 
-def reconstruct_map(data, weight, r_max, pad, ori_size, tau2=None, tau2_fudge=1.0, minres_map=0):
-    """Real-space map (ori_size^3, or ori_size^2 for a 2D grid; FP64) of the skip-gridding
-    reconstruction (2D particles)."""
+def reconstruct_map(data, weight, r_max, pad, ori_size, tau2=None, tau2_fudge=1.0, minres_map=0, gridding_iter=0,
+                    normalise=1.0):
+    """Real-space map (ori_size^3, or ori_size^2 for a 2D grid; FP64) of the reconstruction (2D
+    particles): skip-gridding, or gridding_iter iterations of the gridding weights."""
     nd = weight.ndim
-    F = decenter_divide(data, weight, r_max, pad, tau2, tau2_fudge, minres_map)
+    F = decenter_divide(data, weight, r_max, pad, tau2, tau2_fudge, minres_map, gridding_iter, normalise, ori_size)
     if nd == 2:
         F = F[None]
     ps = F.shape[1]

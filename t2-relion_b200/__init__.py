@@ -135,7 +135,8 @@ class PrepOut(ctypes.Structure):
 
 class ReconConfig(ctypes.Structure):
     _fields_ = [("ori_size", ctypes.c_int), ("do_map", ctypes.c_int), ("minres_map", ctypes.c_int),
-                ("_pad", ctypes.c_int), ("tau2_fudge", ctypes.c_double), ("tau2", _p)]
+                ("gridding_iter", ctypes.c_int), ("tau2_fudge", ctypes.c_double), ("tau2", _p),
+                ("normalise", ctypes.c_double)]
 
 
 class SsnrConfig(ctypes.Structure):
@@ -534,10 +535,12 @@ class EStep:
                                           ctypes.c_void_p(stream)))
 
     # ---------------------------------------------- M-step reconstruction
-    def reconstruct(self, iclass, ori_size, tau2=None, tau2_fudge=1.0, minres_map=0):
-        """t2b_reconstruct: the real-space map (ori_size^3, or ori_size^2 of a 2D class; FP64) of grid `iclass`."""
+    def reconstruct(self, iclass, ori_size, tau2=None, tau2_fudge=1.0, minres_map=0, gridding_iter=0, normalise=1.0):
+        """t2b_reconstruct: the real-space map (ori_size^3, or ori_size^2 of a 2D class; FP64) of grid `iclass`;
+        gridding_iter > 0: the gridding iterations (--dont_skip_gridding) with the class's sum of weights
+        `normalise`."""
         t = None if tau2 is None else np.ascontiguousarray(tau2, np.float64)
-        cfg = ReconConfig(ori_size, 0 if t is None else 1, minres_map, 0, tau2_fudge, _ptr(t))
+        cfg = ReconConfig(ori_size, 0 if t is None else 1, minres_map, gridding_iter, tau2_fudge, _ptr(t), normalise)
         vol = np.zeros((ori_size,) * getattr(self, "_grid_dims", {}).get(iclass, 3))
         _check(lib.t2b_reconstruct(self._h, iclass, ctypes.byref(cfg), _ptr(vol)))
         return vol

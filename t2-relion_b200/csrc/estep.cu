@@ -2049,4 +2049,16 @@ void launch_reconstruct(const Volume& g, const float2* data, const float* weight
     T2B_CUDA(cudaGetLastError());
 }
 
+void launch_decenter(const Volume& g, const float2* data, const float* weight, double2* fconv, double* fw,
+                     double* rad, double* cnt, cudaStream_t st, const double* tau2, double tscale, int minres_map)
+{
+    const int ps = g.ydim, fx = ps / 2 + 1, nz = g.ref_dim == 3 ? ps : 1;
+    const long long total = (long long)nz * ps * fx;
+    T2B_CUDA(cudaMemsetAsync(rad, 0, sizeof(double) * g.r_max, st));
+    T2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(double) * g.r_max, st));
+    k_decenter<<<(int)((total + 255) / 256), 256, 0, st>>>(g, data, weight, fconv, fw, rad, cnt, tau2, tscale,
+                                                          minres_map);
+    T2B_CUDA(cudaGetLastError());
+}
+
 }  // namespace t2b

@@ -1,6 +1,8 @@
 // Batched 1D FFTs in shared memory (libt2b): mixed-radix Stockham autosort
-// over nfft sequences of length N (any N = 2^a 3^b 5^c), ping-ponging between
-// two shared buffers; radix-4, 2, 3, 5 stages with a runtime plan, or, for a
+// over nfft sequences of length N, ping-ponging between two shared buffers;
+// radix-4, 2, 3, 5 stages with a runtime plan, any other prime factor p by a
+// direct length-p DFT per output (N p work for that stage: the odd padded boxes
+// of the reconstruction's gridding iterations, e.g. 259 = 7 x 37), or, for a
 // size known at compile time, radix-16 and radix-8 register butterflies first
 // and constant index arithmetic.  Twiddles tw[t] = e^{-2 pi i t / N} (a table
 // the caller stages in shared memory); the inverse transform uses their
@@ -19,8 +21,9 @@ struct FftPlan {
     int rad[FFT_MAX_STAGES] = {};
 };
 
-// runtime plan: radices 4, then 2, 3, 5
-inline FftPlan fft_plan(int N)
+// runtime plan: radices 4, then 2, 3, 5; with any_prime, then every remaining prime factor
+// (generic stages)
+inline FftPlan fft_plan(int N, bool any_prime = false)
 {
     FftPlan pl;
     pl.n = N;
@@ -35,7 +38,10 @@ inline FftPlan fft_plan(int N)
     take(2);
     take(3);
     take(5);
-    T2B_REQUIRE(n == 1, T2B_ERR_UNSUPPORTED, "transform sizes must be products of 2, 3 and 5");
+    if (any_prime)
+        for (int p = 7; p <= n; p += 2) take(p);
+    T2B_REQUIRE(n == 1, T2B_ERR_UNSUPPORTED,
+                any_prime ? "transform size has too many prime factors" : "transform sizes must be products of 2, 3 and 5");
     return pl;
 }
 
@@ -140,6 +146,32 @@ __device__ __forceinline__ void fft_stage(const float2* a, float2* b, int nfft, 
     }
 }
 
+// The same stage for a radix R known only at run time (a prime >= 7): one thread per output,
+// X[m Ns R + q Ns + k] = sum_r in[m Ns + k + r N/R] e^{-+2 pi i (k r N/(Ns R) + (q r mod R) N/R) / N},
+// the Stockham twiddle and the length-R DFT's root folded into one table entry.
+template <bool INV>
+__device__ __forceinline__ void fft_stage_gen(const float2* a, float2* b, int nfft, int N, int Ns, int R,
+                                              const float2* tw)
+{
+    const int NR = N / R;
+    const int tstride = N / (Ns * R);
+    for (int e = threadIdx.x; e < nfft * N; e += blockDim.x) {
+        const int f = e / N, o = e - f * N;
+        const int k = o % Ns, q = (o / Ns) % R, m = o / (Ns * R);
+        const float2* in = a + f * N + m * Ns + k;
+        float2 acc = make_float2(0.f, 0.f);
+        int qr = 0;   // (q r) mod R
+        for (int r = 0; r < R; ++r) {
+            int t = k * r * tstride + qr * NR;
+            if (t >= N) t -= N;
+            acc = cadd(acc, cmul(in[r * NR], twid<INV>(tw, t)));
+            qr += q;
+            if (qr >= R) qr -= R;
+        }
+        b[f * N + o] = acc;
+    }
+}
+
 // All stages; returns the buffer holding the transform (natural order).
 template <bool INV>
 __device__ float2* fft_smem(float2* a, float2* b, int nfft, const FftPlan& pl, const float2* tw)
@@ -151,7 +183,8 @@ __device__ float2* fft_smem(float2* a, float2* b, int nfft, const FftPlan& pl, c
         case 4: fft_stage<4, INV>(a, b, nfft, pl.n, Ns, tw); break;
         case 2: fft_stage<2, INV>(a, b, nfft, pl.n, Ns, tw); break;
         case 3: fft_stage<3, INV>(a, b, nfft, pl.n, Ns, tw); break;
-        default: fft_stage<5, INV>(a, b, nfft, pl.n, Ns, tw); break;
+        case 5: fft_stage<5, INV>(a, b, nfft, pl.n, Ns, tw); break;
+        default: fft_stage_gen<INV>(a, b, nfft, pl.n, Ns, R, tw); break;
         }
         __syncthreads();
         float2* t = a;

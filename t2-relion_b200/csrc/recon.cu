@@ -334,6 +334,148 @@ __global__ void k_hermitian(Volume g, float2* __restrict__ data, float* __restri
     }
 }
 
+// ---- gridding iterations (BackProjector::reconstruct with max_iter_preweight > 0,
+// src/backprojector.cpp:1532-1655): weights w_n (FP64, FFTW layout of the pad_size box)
+// start at 1 inside r^2 < max_r2; each iteration convolves w_n * weight with the blob
+// through the Fourier transform of the full box (BackProjector::convoluteBlobRealSpace,
+// :2439-2480) and divides w_n by max(1e-6, |result|) inside max_r2.  The half-complex grids
+// are expanded to the full complex box by Hermitian symmetry (the box is odd: no Nyquist
+// plane), transformed by the shared-memory FFTs along x, y and z, multiplied in real space
+// by the blob's tabulated Fourier transform over its value at 0, and transformed back.
+constexpr int GD_CX = 8;   // lines per CTA of the full-box transforms
+
+// data and weight divided by `normalise`; w_n = 1 inside r^2 < max_r2, else 0
+__global__ void k_gd_init(double2* __restrict__ fc, double* __restrict__ fw, double* __restrict__ fn, int ps, int nz,
+                          int max_r2, double inv_norm)
+{
+    const int fx = ps / 2 + 1;
+    const long long total = (long long)nz * ps * fx;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % fx), i = (int)((n / fx) % ps), k = (int)(n / ((long long)fx * ps));
+        const int kp = k < fx ? k : k - ps, ip = i < fx ? i : i - ps;
+        const double2 d = fc[n];
+        fc[n] = make_double2(d.x * inv_norm, d.y * inv_norm);
+        fw[n] *= inv_norm;
+        fn[n] = kp * kp + ip * ip + j * j < max_r2 ? 1. : 0.;
+    }
+}
+
+// the full box V[z][y][x] (2D: one plane) of w_n * weight (real), from the half by Hermitian
+// symmetry: x > ps/2 reads (-z, -y, ps - x)
+__global__ void k_gd_expand(const double* __restrict__ fn, const double* __restrict__ fw, int ps, int nz,
+                            float2* __restrict__ V)
+{
+    const int fx = ps / 2 + 1;
+    const long long total = (long long)nz * ps * ps;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(n % ps), y = (int)((n / ps) % ps), z = (int)(n / ((long long)ps * ps));
+        size_t h;
+        if (x < fx) h = ((size_t)z * ps + y) * fx + x;
+        else h = ((size_t)(nz == 1 ? 0 : (ps - z) % ps) * ps + (ps - y) % ps) * fx + (ps - x);
+        V[n] = make_float2((float)(fn[h] * fw[h]), 0.f);
+    }
+}
+
+// FFT of GD_CX lines of the full box along one axis: axis 0 = x (rows blockIdx.x * GD_CX + c),
+// axis 1 = y (plane z = blockIdx.x), axis 2 = z (row y = blockIdx.x); x tile blockIdx.y
+template <bool INV>
+__global__ void __launch_bounds__(RC_THREADS) k_gd_fft(float2* __restrict__ V, int N, int nz, int axis,
+                                                       const float2* __restrict__ tw, FftPlan plan)
+{
+    extern __shared__ float2 sm[];
+    float2* s_tw = sm;
+    float2* A = sm + N;
+    float2* B = A + GD_CX * N;
+    for (int t = threadIdx.x; t < N; t += blockDim.x) s_tw[t] = tw[t];
+    const long long nrows = (long long)nz * N;
+    const size_t o = blockIdx.x;
+    const int x0 = blockIdx.y * GD_CX;
+    auto ok = [&](int c) -> bool { return axis == 0 ? (long long)o * GD_CX + c < nrows : x0 + c < N; };
+    auto idx = [&](int q, int c) -> size_t {
+        if (axis == 0) return ((size_t)o * GD_CX + c) * N + q;
+        if (axis == 1) return (o * N + q) * N + x0 + c;
+        return ((size_t)q * N + o) * N + x0 + c;
+    };
+    for (int e = threadIdx.x; e < GD_CX * N; e += blockDim.x) {
+        // rows: consecutive threads along the row; columns: along x
+        const int c = axis == 0 ? e / N : e % GD_CX, q = axis == 0 ? e % N : e / GD_CX;
+        A[c * N + q] = ok(c) ? V[idx(q, c)] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2* r = fft_smem<INV>(A, B, GD_CX, plan, s_tw);
+    for (int e = threadIdx.x; e < GD_CX * N; e += blockDim.x) {
+        const int c = axis == 0 ? e / N : e % GD_CX, q = axis == 0 ? e % N : e / GD_CX;
+        if (ok(c)) V[idx(q, c)] = r[c * N + q];
+    }
+}
+
+// real space: multiply by the blob's tabulated Fourier transform at
+// r = |(k, i, j)| / (ori_size pad) (coordinates k < ps/2 ? k : k - ps), entry floor(r / 5e-5),
+// 0 beyond the table (TabFtBlob::operator(), src/tabfuncs.cpp:114-121); the imaginary part
+// (rounding of a Hermitian transform) dropped
+__global__ void k_gd_blob(float2* __restrict__ V, int N, int nz, const double* __restrict__ ratio, int ntab,
+                          double ori_pad)
+{
+    const int ph = N / 2;
+    const long long total = (long long)nz * N * N;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(n % N), y = (int)((n / N) % N), z = (int)(n / ((long long)N * N));
+        const int kz = nz == 1 ? 0 : (z < ph ? z : z - N), ky = y < ph ? y : y - N, kx = x < ph ? x : x - N;
+        const double rval = sqrt((double)(kz * kz + ky * ky + kx * kx)) / ori_pad;
+        const int id = (int)(rval / (0.5 / (double)ntab));
+        const double m = id < ntab ? ratio[id] : 0.;
+        V[n] = make_float2((float)((double)V[n].x * m), 0.f);
+    }
+}
+
+// w_n /= max(1e-6, |V| / N^d) inside r^2 < max_r2 (the forward transform's 1 / N^d here)
+__global__ void k_gd_update(double* __restrict__ fn, const float2* __restrict__ V, int ps, int nz, int max_r2,
+                            double inv_n)
+{
+    const int fx = ps / 2 + 1;
+    const long long total = (long long)nz * ps * fx;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % fx), i = (int)((n / fx) % ps), k = (int)(n / ((long long)fx * ps));
+        const int kp = k < fx ? k : k - ps, ip = i < fx ? i : i - ps;
+        if (kp * kp + ip * ip + j * j >= max_r2) continue;
+        const float2 v = V[((size_t)k * ps + i) * ps + j];
+        const double a = sqrt((double)v.x * v.x + (double)v.y * v.y) * inv_n;
+        fn[n] /= (a > 1e-6 ? a : 1e-6);
+    }
+}
+
+// Fconv = data * w_n
+__global__ void k_gd_apply(double2* __restrict__ fc, const double* __restrict__ fn, long long total)
+{
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const double2 d = fc[n];
+        fc[n] = make_double2(d.x * fn[n], d.y * fn[n]);
+    }
+}
+
+// The blob's Fourier transform over its value at 0, 10,000 samples of [0, 0.5)
+// (TabFtBlob::initialise(2 * 1.9, 15, 0, 10000), src/backprojector.h:111, src/tabfuncs.cpp:95-112):
+// for the order-0 Kaiser-Bessel blob of radius a and taper alpha in 3D (Lewitt 1990),
+// FT(w) = (2 pi)^(3/2) a^3 I_{3/2}(s) / (I_0(alpha) s^(3/2)), s = sqrt(alpha^2 - (2 pi a w)^2)
+// (J_{3/2} of sqrt((2 pi a w)^2 - alpha^2) beyond 2 pi a w = alpha), with the half-integer
+// Bessel functions in closed form.
+std::vector<double> ftblob_ratio(int ntab)
+{
+    const double a = 3.8, alpha = 15.0;
+    std::vector<double> t(ntab);
+    for (int i = 0; i < ntab; ++i) {
+        const double w = (double)i * (0.5 / (double)ntab);
+        const double u = 2.0 * PI_R * a * w;
+        const double sg = std::sqrt(std::fabs(alpha * alpha - u * u));
+        const double pre = std::sqrt(2.0 / (PI_R * sg));
+        const double bes = u > alpha ? pre * (std::sin(sg) / sg - std::cos(sg)) : pre * (std::cosh(sg) - std::sinh(sg) / sg);
+        t[i] = bes / std::pow(sg, 1.5);   // the factor (2 pi)^(3/2) a^3 / I_0(alpha) cancels in the ratio
+    }
+    const double t0 = t[0];
+    for (double& x : t) x /= t0;
+    return t;
+}
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
@@ -363,6 +505,50 @@ void recon_kernels(int N, ColKernel& col, RowKernel& row)
 int grid_of(long long total)
 {
     return (int)std::min<long long>((total + RC_THREADS - 1) / RC_THREADS, 148LL * 16);
+}
+
+// the gridding iterations on (fc, fw) of the pad_size box, in place: fc becomes data * w_n
+void gridding_weights(const Volume& v, int ori, int pad, int niter, double normalise, double2* fc, double* fw,
+                      cudaStream_t st)
+{
+    const int ps = v.ydim, nz = v.ref_dim == 3 ? ps : 1, fx = ps / 2 + 1;
+    const int rp = v.r_max * pad;
+    const int max_r2 = rp * rp;
+    const long long nh = (long long)nz * ps * fx, nf = (long long)nz * ps * ps;
+    const size_t smem = sizeof(float2) * ((size_t)ps + 2 * (size_t)GD_CX * ps);
+    T2B_REQUIRE(smem <= 227 * 1024, T2B_ERR_UNSUPPORTED, "pad_size box too large for the gridding transforms");
+    const FftPlan plan = fft_plan(ps, true);
+    constexpr int ntab = 10000;
+    DevBuf<double> fn(nh), ratio(ntab);
+    DevBuf<float2> V(nf), tw(ps);
+    std::vector<float2> htw(ps);
+    for (int t = 0; t < ps; ++t) {
+        const double a = -2.0 * PI_R * (double)t / (double)ps;
+        htw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    const std::vector<double> hr = ftblob_ratio(ntab);
+    T2B_CUDA(cudaMemcpyAsync(tw.p, htw.data(), ps * sizeof(float2), cudaMemcpyHostToDevice, st));
+    T2B_CUDA(cudaMemcpyAsync(ratio.p, hr.data(), ntab * sizeof(double), cudaMemcpyHostToDevice, st));
+    T2B_CUDA(cudaFuncSetAttribute((const void*)k_gd_fft<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    T2B_CUDA(cudaFuncSetAttribute((const void*)k_gd_fft<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int xt = (ps + GD_CX - 1) / GD_CX;
+    const auto fft3 = [&](auto kern) {
+        kern<<<(int)((nz * (long long)ps + GD_CX - 1) / GD_CX), RC_THREADS, smem, st>>>(V.p, ps, nz, 0, tw.p, plan);
+        kern<<<dim3(nz, xt), RC_THREADS, smem, st>>>(V.p, ps, nz, 1, tw.p, plan);
+        if (nz > 1) kern<<<dim3(ps, xt), RC_THREADS, smem, st>>>(V.p, ps, nz, 2, tw.p, plan);
+    };
+    const double inv_n = 1.0 / ((double)ps * ps * (nz > 1 ? ps : 1));
+    k_gd_init<<<grid_of(nh), RC_THREADS, 0, st>>>(fc, fw, fn.p, ps, nz, max_r2, 1.0 / normalise);
+    for (int it = 0; it < niter; ++it) {
+        k_gd_expand<<<grid_of(nf), RC_THREADS, 0, st>>>(fn.p, fw, ps, nz, V.p);
+        fft3(k_gd_fft<true>);
+        k_gd_blob<<<grid_of(nf), RC_THREADS, 0, st>>>(V.p, ps, nz, ratio.p, ntab, (double)ori * pad);
+        fft3(k_gd_fft<false>);
+        k_gd_update<<<grid_of(nh), RC_THREADS, 0, st>>>(fn.p, V.p, ps, nz, max_r2, inv_n);
+    }
+    k_gd_apply<<<grid_of(nh), RC_THREADS, 0, st>>>(fc, fn.p, nh);
+    T2B_CUDA(cudaGetLastError());
+    T2B_CUDA(cudaStreamSynchronize(st));   // the buffers above are freed on return
 }
 
 const Volume& grid_volume(t2b_ctx* c, int ig)
@@ -404,8 +590,17 @@ int t2b_reconstruct(t2b_ctx* c, int iclass, const t2b_recon_config* cf, double* 
         if (cf->do_map)
             T2B_CUDA(cudaMemcpyAsync(t2.p, cf->tau2, (ori / 2 + 1) * sizeof(double), cudaMemcpyHostToDevice, st));
         const double tscale = (dim == 3 ? (double)pad * pad * pad : (double)pad * pad) * cf->tau2_fudge;
-        launch_reconstruct(v, c->gdata[iclass], c->gweight[iclass], fc.p, fw.p, rad.p, rad.p + v.r_max, st,
-                           cf->do_map ? t2.p : nullptr, tscale, cf->minres_map);
+        if (cf->gridding_iter > 0) {
+            // --dont_skip_gridding: the iterative weights in place of the division
+            T2B_REQUIRE(cf->normalise > 0., T2B_ERR_ARG,
+                        "gridding iterations need normalise > 0 (the class's sum of weights)");
+            launch_decenter(v, c->gdata[iclass], c->gweight[iclass], fc.p, fw.p, rad.p, rad.p + v.r_max, st,
+                            cf->do_map ? t2.p : nullptr, tscale, cf->minres_map);
+            gridding_weights(v, ori, pad, cf->gridding_iter, cf->normalise, fc.p, fw.p, st);
+        } else {
+            launch_reconstruct(v, c->gdata[iclass], c->gweight[iclass], fc.p, fw.p, rad.p, rad.p + v.r_max, st,
+                               cf->do_map ? t2.p : nullptr, tscale, cf->minres_map);
+        }
         // window + centre by sign, inverse 3D FFT, real-space window
         DevBuf<float2> G((size_t)(dim == 3 ? N : 1) * N * h), tw(N);
         std::vector<float2> htw(N);

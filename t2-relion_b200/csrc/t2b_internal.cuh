@@ -207,6 +207,10 @@ void launch_wsum_bp(const Tables& tb, const Work& w, const Volume& g, float2* co
 void launch_reconstruct(const Volume& g, const float2* data, const float* weight, double2* fconv,
                         double* fw, double* rad, double* cnt, cudaStream_t st, const double* tau2 = nullptr,
                         double tscale = 1., int minres_map = 0);
+// Projector::decenter of a grid with the MAP term (the first step of launch_reconstruct,
+// without its division): the gridding iterations' input
+void launch_decenter(const Volume& g, const float2* data, const float* weight, double2* fconv, double* fw,
+                     double* rad, double* cnt, cudaStream_t st, const double* tau2, double tscale, int minres_map);
 
 // tcgen05 split-BF16 coarse diff2 (diff2_tc.cu)
 struct TcOperands {

@@ -159,3 +159,39 @@ def test_2d_fsc_and_ssnr_match_oracle(classes_2d):
     rr = ro.update_ssnr(w1.astype(np.float64), r, 2, N, 1.5, tau2, got)
     for a, b in zip(g, rr):
         assert np.allclose(a, b, rtol=1e-9, atol=1e-14)
+
+
+@pytest.fixture(scope="module", params=["refine_o2", "class2d"])
+def symmetric_grid(request):
+    """A grid the E-step filled, Hermitian-symmetrised on the device (as the M-step receives
+    it): 3D box 64 (pad_size 67, a prime) and 2D classes of box 48 (pad_size 51 = 3 x 17)."""
+    pb = problems.build(request.param, n_particles=16, seed=31)
+    P = pb["parts"]
+    es = pb["product"]()
+    res = es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    es.enforce_hermitian_symmetry(0)
+    pb["es"] = es
+    pb["grid"] = es.get_backprojector(0)
+    pb["sumw"] = float(np.sum(res["sumw"]))
+    yield pb
+    es.close()
+
+
+@pytest.mark.parametrize("with_map", [False, True], ids=["plain", "map_tau2"])
+def test_gridding_reconstruction_matches_oracle(symmetric_grid, with_map):
+    """--dont_skip_gridding: 10 iterations of the gridding weights (pad_size transforms of
+    prime or composite odd length) before the windowed inverse transform, against the FP64
+    oracle; the same tolerance as the skip-gridding path."""
+    pb, es = symmetric_grid, symmetric_grid["es"]
+    N, r = pb["N"], pb["r"]
+    data, w = pb["grid"]
+    tau2 = None
+    if with_map:
+        tau2 = np.random.default_rng(5).uniform(0.5, 2.0, N // 2 + 1) * np.mean(w)
+    got = es.reconstruct(0, N, tau2=tau2, tau2_fudge=1.1, minres_map=1, gridding_iter=10, normalise=pb["sumw"])
+    ref = ro.reconstruct_map(data.astype(np.complex128), w.astype(np.float64), r, 2, N, tau2=tau2, tau2_fudge=1.1,
+                             minres_map=1, gridding_iter=10, normalise=pb["sumw"])
+    _map_close(got, ref)
+    # and it is not the skip-gridding map
+    skip = es.reconstruct(0, N, tau2=tau2, tau2_fudge=1.1, minres_map=1)
+    assert np.max(np.abs(skip - got)) > 1e-3 * np.max(np.abs(got))

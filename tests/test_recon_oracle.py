@@ -161,3 +161,52 @@ def test_hermitian_symmetry_restatement(shape):
             assert t3[a] == t3[b] == w3[a] + w3[b]
             assert np.isclose(s3[a], d3[a] + np.conj(d3[b]), rtol=1e-15)
     assert np.array_equal(s3[..., 1:], d3[..., 1:]) and np.array_equal(t3[..., 1:], w3[..., 1:])
+
+
+def test_blob_fourier_table_against_a_direct_transform():
+    """TabFtBlob's values (the order-0 Kaiser-Bessel blob, radius 3.8, alpha 15, in 3D): the
+    closed form of the oracle against the radial Fourier integral of the blob profile
+    I_0(alpha sqrt(1 - (r/a)^2)) / I_0(alpha), 4 pi int r^2 b(r) sinc(2 w r) dr."""
+    from scipy import integrate, special
+    a, al = 3.8, 15.0
+    tab = ro.ftblob_table()
+
+    def direct(w):
+        f = lambda r: special.i0(al * np.sqrt(max(0.0, 1 - (r / a) ** 2))) / special.i0(al) * r * r * np.sinc(2 * w * r)
+        return 4 * np.pi * integrate.quad(f, 0, a, limit=400, epsabs=1e-14, epsrel=1e-13)[0]
+
+    for i in (0, 1000, 3000, 5000, 8000, 9999):
+        assert abs(tab[i] - direct(i * 0.5 / 10000)) <= 1e-12 * tab[0], i
+
+
+@pytest.mark.parametrize("two_d", [False, True], ids=["3d", "2d"])
+def test_gridding_weights_on_uniform_sampling(synth, two_d):
+    """With weight 1 everywhere the gridding iterations keep the weights near 1 (the blob
+    kernel sums to 1), so the map is the skip-gridding map up to the edge of the sphere."""
+    ori, r_max = 32, 16
+    m = 2 * ori
+    if two_d:
+        img = synth.blob_volume(ori, 6, sigma=(2.5, 4.0), seed=5, ndim=2)
+        big0 = np.zeros((m, m))
+        big0[ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori] = img
+        F0 = np.fft.rfft2(np.fft.ifftshift(big0)) / float(ori) ** 2
+        ps = 2 * (2 * r_max + 1) + 1
+        kk = np.arange(ps) - ps // 2
+        KY, KX = np.meshgrid(kk, np.arange(ps // 2 + 1), indexing="ij")
+        keep = KY * KY + KX * KX <= (2 * r_max) ** 2
+        fmap = np.where(keep, F0[KY % m, np.minimum(KX, m // 2)], 0)
+    else:
+        vol = synth.blob_volume(ori, 8, sigma=(2.5, 4.0), seed=3)
+        big0 = np.zeros((m,) * 3)
+        big0[ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori, ori // 2:ori // 2 + ori] = vol
+        F0 = np.fft.rfftn(np.fft.ifftshift(big0)) / float(ori) ** 3
+        ps = 2 * (2 * r_max + 1) + 1
+        kk = np.arange(ps) - ps // 2
+        KZ, KY, KX = np.meshgrid(kk, kk, np.arange(ps // 2 + 1), indexing="ij")
+        keep = KZ * KZ + KY * KY + KX * KX <= (2 * r_max) ** 2
+        fmap = np.where(keep, F0[KZ % m, KY % m, np.minimum(KX, m // 2)], 0)
+    w = np.ones(fmap.shape)
+    skip = ro.reconstruct_map(fmap, w, r_max, 2, ori)
+    grid = ro.reconstruct_map(fmap, w, r_max, 2, ori, gridding_iter=10, normalise=3.7)
+    assert np.corrcoef(skip.ravel(), grid.ravel())[0, 1] >= 0.9999
+    assert np.max(np.abs(skip - grid)) <= 1e-2 * np.max(np.abs(skip))
