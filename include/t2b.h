@@ -243,9 +243,31 @@ int t2b_reconstruct(t2b_ctx* ctx, int iclass, const t2b_recon_config* cfg, doubl
  * src/ml_optimiser.cpp:4626): each Friedel pair (z, y, 0) <-> (-z, -y, 0) gets the sum
  * data(z, y) + conj(data(-z, -y)) (conjugated on the partner) and the sum of the two
  * weights.  Linear, so it may run before or after the reduction of the grids over GPUs, but
- * once.  Point-group symmetry (applyPointGroupSymmetry) is C1 only: no other operator is
- * applied. */
+ * once.  Point-group symmetry follows it (t2b_backprojector_apply_symmetry). */
 int t2b_backprojector_enforce_hermitian(t2b_ctx* ctx, int iclass);
+
+/* The operators of a point group other than the identity, 3 x 3 row-major into
+ * mats (capacity cap matrices; fewer are written when cap is smaller), their number
+ * in *count: the rotations k 360 / n about the group's generating axes, transposed, closed
+ * under products, entries below 1e-6 zeroed, matrices equal within 1e-6 taken as one
+ * (SymList::read_sym_file + compute_subgroup, src/symmetries.cpp:133-191, 273-325;
+ * generating axes of SymList::fill_symmetry_class, src/symmetries.cpp:606-725).  Groups:
+ * C1, Cn, Dn (n of one or two digits), T, O, I (= I2), I1, I3, I4, case-insensitive.
+ * Groups with mirror planes or an inversion (Ci, Cs, Cnv, Cnh, Sn, Dnv, Dnh, Td, Th, Oh,
+ * Ih ...) return T2B_ERR_UNSUPPORTED.  Orders: Cn n - 1, Dn 2n - 1, T 11, O 23, I 59. */
+int t2b_point_group(const char* group, double* mats, int cap, int* count);
+
+/* Point-group symmetrisation of a 3D grid, in place on the device
+ * (BackProjector::applyPointGroupSymmetry, src/backprojector.cpp:2279-2435, applied by
+ * MlOptimiser::maximization after enforceHermitianSymmetry, src/ml_optimiser.cpp:4643):
+ * each voxel with x^2 + y^2 + z^2 <= ROUND(r_max pad)^2 gains, for every operator R of the
+ * group other than the identity, the grid read at R (x, y, z) by trilinear interpolation
+ * (the complex conjugate of the Friedel partner where the rotated x < 0), data and weight
+ * alike; not averaged.  Coordinates and sums in FP64, the grid in FP32; all reads come
+ * from the grid as it was before the call.  C1 and 2D grids are left unchanged.  Expects
+ * the Hermitian-symmetrised grid.  Linear, so it may run before or after the reduction of
+ * the grids over GPUs, but once. */
+int t2b_backprojector_apply_symmetry(t2b_ctx* ctx, int iclass, const char* group);
 
 /* Fourier shell correlation of two grids (two half-sets) after down-sampling to
  * the unpadded box (BackProjector::getDownsampledAverage +

@@ -73,6 +73,11 @@ public:
     void clear() { check(t2b_backprojector_clear(b_.ctx(), iclass_)); }
     // BackProjector::enforceHermitianSymmetry on the device grid (before reconstructing)
     void enforceHermitianSymmetry() { check(t2b_backprojector_enforce_hermitian(b_.ctx(), iclass_)); }
+    // BackProjector::applyPointGroupSymmetry (after enforceHermitianSymmetry); group as --sym
+    void applyPointGroupSymmetry(const char* group)
+    {
+        check(t2b_backprojector_apply_symmetry(b_.ctx(), iclass_, group));
+    }
     void getMdlData(float* real, float* imag, float* weight)
     {
         check(t2b_backprojector_get(b_.ctx(), iclass_, real, imag, weight));

@@ -38,6 +38,15 @@ complex, weight real; z, y centred at -initz, -inity; x from 0; 3D grids of
                     BackProjector::enforceHermitianSymmetry (src/backprojector.cpp:2104-2121),
                     applied by MlOptimiser::maximization before reconstruct
                     (src/ml_optimiser.cpp:4626)
+  point_group       SymList::read_sym_file + compute_subgroup (src/symmetries.cpp:133-191,
+                    273-325) for the proper groups, with the generating axes of
+                    SymList::fill_symmetry_class (:606-725): rotations k 360 / n about
+                    each axis, transposed, entries below 1e-6 zeroed, closed under
+                    products, equality within 1e-6, the identity left out
+  apply_point_group_symmetry
+                    BackProjector::applyPointGroupSymmetry (src/backprojector.cpp:2279-2435):
+                    the sum over the operators of the trilinear read at R (x, y, z)
+                    (conjugated where the rotated x < 0), inside ROUND(r_max pad)^2
   downsampled_fsc   getDownsampledAverage + calculateDownSampledFourierShellCorrelation
                     (src/backprojector.cpp:933-1040)
   update_ssnr       BackProjector::updateSSNRarrays (src/backprojector.cpp:1041-1205)
@@ -83,6 +92,106 @@ def enforce_hermitian_symmetry(data, weight):
             w[a] = ws
             w[b] = ws
     return (d[0], w[0]) if two_d else (d, w)
+
+
+# generating axes (fold, axis) of the proper point groups (src/symmetries.cpp:606-725)
+_PG_AXES = {
+    "T": [(3, (0., 0., 1.)), (2, (0., 0.816496, 0.577350))],
+    "O": [(3, (.5773502, .5773502, .5773502)), (4, (0., 0., 1.))],
+    "I": [(2, (0., 0., 1.)), (5, (0.525731114, 0., 0.850650807)), (3, (0., 0.356822076, 0.934172364))],
+    "I1": [(2, (1., 0., 0.)), (5, (0.85065080702670, 0., -0.5257311142635)), (3, (0.9341723640, 0.3568220765, 0.))],
+    "I3": [(2, (-0.5257311143, 0., 0.8506508070)), (5, (0., 0., 1.)),
+           (3, (-0.4911234778630044, 0.3568220764705179, 0.7946544753759428))],
+    "I4": [(2, (0.5257311143, 0., 0.8506508070)), (5, (0.8944271932547096, 0., 0.4472135909903704)),
+           (3, (0.4911234778630044, 0.3568220764705179, 0.7946544753759428))],
+}
+_PG_AXES["I2"] = _PG_AXES["I"]
+
+
+def _pg_generators(name):
+    g = name.upper()
+    if g in _PG_AXES:
+        return _PG_AXES[g]
+    if len(g) in (2, 3) and g[0] in "CD" and g[1:].isdigit():
+        n = int(g[1:])
+        if g[0] == "C":
+            return [(n, (0., 0., 1.))]
+        return ([(n, (0., 0., 1.))] if n > 1 else []) + [(2, (1., 0., 0.))]
+    raise ValueError(f"point group {name!r}: only the proper groups Cn, Dn, T, O, I, I1-I4")
+
+
+def point_group(name):
+    """The group's operators other than the identity, (n, 3, 3).  Each generator contributes
+    the transposes of its rotations by k 360 / fold (axis-angle matrix cos I + sin [a]x +
+    (1 - cos) a a^T); the list is then closed under products R_i R_j, taken in the order of
+    found_not_tried (src/symmetries.cpp:243-270: for n = 0, 1, ..., the pairs (0..n, n), then
+    (n, n-1..0)), appending each product that is neither the identity nor present (every
+    entry within 1e-6), zeroed below 1e-6."""
+    zero = lambda m: np.where(np.abs(m) < 1e-6, 0.0, m)
+    eq = lambda a, b: bool(np.all(np.abs(a - b) <= 1e-6))
+    ops = []
+    for fold, ax in _pg_generators(name):
+        a = np.asarray(ax, float) / np.linalg.norm(ax)
+        cross = np.array([[0., -a[2], a[1]], [a[2], 0., -a[0]], [-a[1], a[0], 0.]])
+        for k in range(1, fold):
+            t = k * 2.0 * PI / fold
+            rot = np.cos(t) * np.eye(3) + np.sin(t) * cross + (1.0 - np.cos(t)) * np.outer(a, a)
+            ops.append(zero(rot.T))
+    n = 0
+    while n < len(ops):
+        for i, j in [(i, n) for i in range(n + 1)] + [(n, j) for j in range(n - 1, -1, -1)]:
+            p = ops[i] @ ops[j]
+            if not (eq(p, np.eye(3)) or any(eq(p, o) for o in ops)):
+                ops.append(zero(p))
+        n += 1
+    return np.array(ops).reshape(-1, 3, 3)
+
+
+def apply_point_group_symmetry(data, weight, mats, r_max, pad):
+    """Sum over the operators R of the grid read at R (x, y, z), added to the grid itself, for
+    r^2 <= ROUND(r_max pad)^2 (FP64 coordinates and sums; the reads come from the input
+    grid).  3D centred half-complex grids; returns new complex128 / float64 arrays."""
+    d = np.asarray(data, np.complex128)
+    w = np.asarray(weight, np.float64)
+    zd, yd, xd = w.shape
+    initz, inity = -(zd // 2), -(yd // 2)
+    k, i, j = _logical(w.shape, initz, inity)
+    x, y, z = [np.broadcast_to(a, w.shape).astype(np.float64).ravel() for a in (j, i, k)]
+    rp = int(relion_round(r_max * pad))
+    inside = x * x + y * y + z * z <= rp * rp
+    x, y, z = x[inside], y[inside], z[inside]
+    sd = d.ravel().copy()
+    sw = w.ravel().copy()
+    acc_d = np.zeros(x.size, np.complex128)
+    acc_w = np.zeros(x.size)
+    for m in mats:
+        xp = x * m[0, 0] + y * m[0, 1] + z * m[0, 2]
+        yp = x * m[1, 0] + y * m[1, 1] + z * m[1, 2]
+        zp = x * m[2, 0] + y * m[2, 1] + z * m[2, 2]
+        neg = xp < 0
+        xp, yp, zp = np.where(neg, -xp, xp), np.where(neg, -yp, yp), np.where(neg, -zp, zp)
+        x0, y0, z0 = np.floor(xp).astype(np.int64), np.floor(yp).astype(np.int64), np.floor(zp).astype(np.int64)
+        fx, fy, fz = xp - x0, yp - y0, zp - z0
+        y0, z0 = y0 - inity, z0 - initz
+        ok = (x0 >= 0) & (x0 + 1 < xd) & (y0 >= 0) & (y0 + 1 < yd) & (z0 >= 0) & (z0 + 1 < zd)
+        x0, y0, z0 = np.where(ok, x0, 0), np.where(ok, y0, 0), np.where(ok, z0, 0)
+
+        def tri(a):
+            c = lambda dz, dy, dx: a[z0 + dz, y0 + dy, x0 + dx]
+            x00 = c(0, 0, 0) + (c(0, 0, 1) - c(0, 0, 0)) * fx
+            x01 = c(1, 0, 0) + (c(1, 0, 1) - c(1, 0, 0)) * fx
+            x10 = c(0, 1, 0) + (c(0, 1, 1) - c(0, 1, 0)) * fx
+            x11 = c(1, 1, 0) + (c(1, 1, 1) - c(1, 1, 0)) * fx
+            y0v = x00 + (x10 - x00) * fy
+            y1v = x01 + (x11 - x01) * fy
+            return y0v + (y1v - y0v) * fz
+
+        vd = tri(d)
+        acc_d += np.where(ok, np.where(neg, np.conj(vd), vd), 0)
+        acc_w += np.where(ok, tri(w), 0.0)
+    sd[inside] += acc_d
+    sw[inside] += acc_w
+    return sd.reshape(d.shape), sw.reshape(w.shape)
 
 
 def ftblob_table(radius=3.8, alpha=15.0, nr=10000):

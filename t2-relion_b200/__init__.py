@@ -43,6 +43,7 @@ ABI_SYMBOLS = (
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
     "t2b_prep_configure", "t2b_prep_batch_host", "t2b_prep_batch_device", "t2b_autotune", "t2b_tune_set",
     "t2b_reconstruct", "t2b_fsc_halves", "t2b_update_ssnr", "t2b_backprojector_enforce_hermitian",
+    "t2b_point_group", "t2b_backprojector_apply_symmetry",
     "t2b_mrc_info", "t2b_mrc_read", "t2b_mrc_write", "t2b_star_open", "t2b_star_shape", "t2b_star_label",
     "t2b_star_column", "t2b_star_value", "t2b_star_close", "t2b_star_write",
 )
@@ -170,6 +171,8 @@ def _setup_prototypes():
     lib.t2b_backprojector_init.argtypes = [v, i, i, i, i, i, i, i, i, i]
     lib.t2b_backprojector_clear.argtypes = [v, i]
     lib.t2b_backprojector_enforce_hermitian.argtypes = [v, i]
+    lib.t2b_point_group.argtypes = [ctypes.c_char_p, v, i, ctypes.POINTER(i)]
+    lib.t2b_backprojector_apply_symmetry.argtypes = [v, i, ctypes.c_char_p]
     lib.t2b_backprojector_get.argtypes = [v, i, v, v, v]
     lib.t2b_backprojector_device_ptrs.argtypes = [v, i, ctypes.POINTER(v), ctypes.POINTER(v)]
     lib.t2b_configure.argtypes = [v, ctypes.POINTER(Config)]
@@ -233,6 +236,16 @@ def _ptr(a):
 
 def version():
     return lib.t2b_version().decode()
+
+
+def point_group(group):
+    """t2b_point_group: the operators of a proper point group other than the identity, an
+    (n, 3, 3) array (SymList after read_sym_file, src/symmetries.cpp:51-191)."""
+    n = ctypes.c_int(0)
+    _check(lib.t2b_point_group(group.encode(), None, 0, ctypes.byref(n)))
+    m = np.zeros((max(n.value, 1), 3, 3))
+    _check(lib.t2b_point_group(group.encode(), _ptr(m), n.value, ctypes.byref(n)))
+    return m[:n.value]
 
 
 # ------------------------------------------------------------------ on-disk formats
@@ -426,6 +439,12 @@ class EStep:
     # BackProjector::enforceHermitianSymmetry (before the reconstruction, once per iteration)
     def enforce_hermitian_symmetry(self, iclass):
         _check(lib.t2b_backprojector_enforce_hermitian(self._h, iclass))
+
+    # BackProjector::applyPointGroupSymmetry
+    def apply_point_group_symmetry(self, iclass, group):
+        """t2b_backprojector_apply_symmetry: sum of the grid over the operators of a proper
+        point group ("C1", "Cn", "Dn", "T", "O", "I", "I1"-"I4"), in place."""
+        _check(lib.t2b_backprojector_apply_symmetry(self._h, iclass, group.encode()))
 
     # AccBackprojector::getMdlData
     def get_backprojector(self, iclass):
@@ -794,6 +813,9 @@ class AccBackprojector:
 
     def enforceHermitianSymmetry(self):
         self.estep.enforce_hermitian_symmetry(self.iclass)
+
+    def applyPointGroupSymmetry(self, group):
+        self.estep.apply_point_group_symmetry(self.iclass, group)
 
     def getMdlData(self):
         data, w = self.estep.get_backprojector(self.iclass)

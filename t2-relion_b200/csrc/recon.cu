@@ -26,7 +26,11 @@
 #include "t2b_internal.cuh"
 #include "fft_smem.cuh"
 
+#include <array>
+#include <cctype>
 #include <cmath>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 namespace t2b {
@@ -476,6 +480,62 @@ std::vector<double> ftblob_ratio(int ntab)
     return t;
 }
 
+// ---- point-group symmetry (BackProjector::applyPointGroupSymmetry,
+// src/backprojector.cpp:2279-2435): every voxel (x, y, z) of the grid inside r^2 <= ROUND(r_max pad)^2
+// gets the sum, over the group's operators R other than the identity, of the grid read at
+// R (x, y, z) by trilinear interpolation (the conjugate Friedel partner where the rotated x < 0),
+// added to its own value; data and weight alike.  FP64 coordinates and sums, FP32 grids.
+__global__ void k_symmetrise(Volume g, const float2* __restrict__ data, const float* __restrict__ weight,
+                             float2* __restrict__ sdata, float* __restrict__ sweight, const double* __restrict__ R,
+                             int nsym, int rmax2)
+{
+    const long long total = (long long)g.zdim * g.ydim * g.xdim;
+    const size_t plane = (size_t)g.ydim * g.xdim;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < total; n += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % g.xdim), i = (int)((n / g.xdim) % g.ydim), k = (int)(n / (long long)plane);
+        const int x = j, y = i + g.inity, z = k + g.initz;
+        double sr = data[n].x, si = data[n].y, sw = weight[n];
+        if (x * x + y * y + z * z <= rmax2) {
+            for (int s = 0; s < nsym; ++s) {
+                const double* m = R + 9 * s;
+                // rounded products and sums in the reference's order (no contraction), so
+                // that floor() and the sign test see the reference's coordinates
+                double xp = __dadd_rn(__dadd_rn(__dmul_rn(x, m[0]), __dmul_rn(y, m[1])), __dmul_rn(z, m[2]));
+                double yp = __dadd_rn(__dadd_rn(__dmul_rn(x, m[3]), __dmul_rn(y, m[4])), __dmul_rn(z, m[5]));
+                double zp = __dadd_rn(__dadd_rn(__dmul_rn(x, m[6]), __dmul_rn(y, m[7])), __dmul_rn(z, m[8]));
+                const bool neg = xp < 0;
+                if (neg) { xp = -xp; yp = -yp; zp = -zp; }
+                const int x0 = (int)floor(xp), y0f = (int)floor(yp), z0f = (int)floor(zp);
+                const double fx = xp - x0, fy = yp - y0f, fz = zp - z0f;
+                const int y0 = y0f - g.inity, z0 = z0f - g.initz;
+                if (x0 < 0 || x0 + 1 >= g.xdim || y0 < 0 || y0 + 1 >= g.ydim || z0 < 0 || z0 + 1 >= g.zdim) continue;
+                const size_t b = ((size_t)z0 * g.ydim + y0) * g.xdim + x0;
+                const size_t c[8] = {b, b + 1, b + g.xdim, b + g.xdim + 1,
+                                     b + plane, b + plane + 1, b + plane + g.xdim, b + plane + g.xdim + 1};
+                // (z, y, x) corners: 000 001 010 011 100 101 110 111
+                double dr[8], di[8], dw[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    dr[q] = data[c[q]].x;
+                    di[q] = data[c[q]].y;
+                    dw[q] = weight[c[q]];
+                }
+                const auto tri = [&](const double* d) {
+                    const double x00 = d[0] + (d[1] - d[0]) * fx, x01 = d[4] + (d[5] - d[4]) * fx;
+                    const double x10 = d[2] + (d[3] - d[2]) * fx, x11 = d[6] + (d[7] - d[6]) * fx;
+                    const double y0v = x00 + (x10 - x00) * fy, y1v = x01 + (x11 - x01) * fy;
+                    return y0v + (y1v - y0v) * fz;
+                };
+                sr += tri(dr);
+                si += neg ? -tri(di) : tri(di);
+                sw += tri(dw);
+            }
+        }
+        sdata[n] = make_float2((float)sr, (float)si);
+        sweight[n] = (float)sw;
+    }
+}
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
@@ -557,6 +617,108 @@ const Volume& grid_volume(t2b_ctx* c, int ig)
     const Volume& v = c->gvol[ig];
     T2B_REQUIRE(v.ref_dim == 3 || v.ref_dim == 2, T2B_ERR_UNSUPPORTED, "grids are 2D or 3D");
     return v;
+}
+
+// The operators of a proper point group, 3 x 3 row-major, the identity excluded: the rotations
+// k * 360 / n about each generating axis, transposed, then every product until the set is
+// closed (SymList::read_sym_file + compute_subgroup, src/symmetries.cpp:133-191, 273-325),
+// entries below 1e-6 set to 0 and matrices equal within 1e-6 taken as one.  The generating
+// axes are the reference's (SymList::fill_symmetry_class, src/symmetries.cpp:606-725; names as
+// SymList::isSymmetryGroup: case-insensitive, orders of one or two digits): Cn the
+// z axis; Dn that and a 2-fold about x; T, O and I (= I2) and I1, I3, I4 their tabulated axes.
+// Groups with mirrors or an inversion (Cs, Ci, Cnv, Cnh, Sn, Dnv, Dnh, Td, Th, Oh, Ih ...) are
+// refused: the maps of chiral molecules use none.
+std::vector<std::array<double, 9>> point_group(const char* name)
+{
+    using M = std::array<double, 9>;
+    std::string g;
+    for (const char* p = name; p && *p; ++p)
+        if (*p != ' ') g += (char)std::toupper((unsigned char)*p);
+    struct Gen { int fold; double ax, ay, az; };
+    std::vector<Gen> gens;
+    auto order = [&](size_t from) -> int {
+        if (g.size() <= from || g.size() > from + 2) return -1;
+        for (size_t i = from; i < g.size(); ++i)
+            if (!std::isdigit((unsigned char)g[i])) return -1;
+        return std::atoi(g.c_str() + from);
+    };
+    if (g.empty() || g == "C1") {
+        return {};
+    } else if (g[0] == 'C' && order(1) >= 1) {
+        if (order(1) > 1) gens.push_back({order(1), 0, 0, 1});
+    } else if (g[0] == 'D' && order(1) >= 1) {
+        if (order(1) > 1) gens.push_back({order(1), 0, 0, 1});
+        gens.push_back({2, 1, 0, 0});
+    } else if (g == "T") {
+        gens = {{3, 0., 0., 1.}, {2, 0., 0.816496, 0.577350}};
+    } else if (g == "O") {
+        gens = {{3, .5773502, .5773502, .5773502}, {4, 0, 0, 1}};
+    } else if (g == "I" || g == "I2") {
+        gens = {{2, 0, 0, 1}, {5, 0.525731114, 0, 0.850650807}, {3, 0, 0.356822076, 0.934172364}};
+    } else if (g == "I1") {
+        gens = {{2, 1, 0, 0}, {5, 0.85065080702670, 0, -0.5257311142635}, {3, 0.9341723640, 0.3568220765, 0}};
+    } else if (g == "I3") {
+        gens = {{2, -0.5257311143, 0, 0.8506508070}, {5, 0., 0., 1.},
+                {3, -0.4911234778630044, 0.3568220764705179, 0.7946544753759428}};
+    } else if (g == "I4") {
+        gens = {{2, 0.5257311143, 0, 0.8506508070}, {5, 0.8944271932547096, 0, 0.4472135909903704},
+                {3, 0.4911234778630044, 0.3568220764705179, 0.7946544753759428}};
+    } else {
+        throw Error{T2B_ERR_UNSUPPORTED, std::string("point group '") + (name ? name : "") +
+                                             "' not supported: C1, Cn, Dn, T, O, I, I1-I4 (rotations only)"};
+    }
+    const auto clean = [](M& a) {
+        for (double& v : a)
+            if (std::fabs(v) < 1e-6) v = 0.;
+    };
+    const auto same = [](const M& a, const M& b) {
+        for (int i = 0; i < 9; ++i)
+            if (std::fabs(a[i] - b[i]) > 1e-6) return false;
+        return true;
+    };
+    const auto mul = [](const M& a, const M& b) {
+        M r{};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) r[3 * i + j] += a[3 * i + k] * b[3 * k + j];
+        return r;
+    };
+    const M ident = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    std::vector<M> ops;
+    for (const Gen& ge : gens) {
+        const double nrm = std::sqrt(ge.ax * ge.ax + ge.ay * ge.ay + ge.az * ge.az);
+        const double a[3] = {ge.ax / nrm, ge.ay / nrm, ge.az / nrm};
+        for (int kk = 1; kk < ge.fold; ++kk) {
+            const double ang = kk * (2.0 * PI_R / ge.fold), cs = std::cos(ang), sn = std::sin(ang);
+            // rotation by ang about a (Rodrigues), transposed
+            M r;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    const double cross = (i == j) ? 0. : ((3 + j - i) % 3 == 1 ? -1. : 1.) * a[3 - i - j];
+                    r[3 * j + i] = (i == j ? cs : 0.) + sn * cross + (1. - cs) * a[i] * a[j];
+                }
+            clean(r);
+            ops.push_back(r);
+        }
+    }
+    // Products in the reference's order (found_not_tried, src/symmetries.cpp:243-270): shell
+    // n = 0, 1, ... holds the pairs (i, n) for i = 0..n, then (n, j) for j = n-1..0; an operator
+    // appended while shell n runs opens a later shell.  The order fixes which chain of
+    // products each operator comes from, and so its last digits (the generating axes carry
+    // six to ten).
+    const auto visit = [&](size_t i, size_t j) {
+        M p = mul(ops[i], ops[j]);
+        if (same(p, ident)) return;
+        for (const M& o : ops)
+            if (same(o, p)) return;
+        clean(p);
+        ops.push_back(p);
+    };
+    for (size_t n = 0; n < ops.size(); ++n) {
+        for (size_t i = 0; i <= n; ++i) visit(i, n);
+        for (size_t j = n; j-- > 0;) visit(n, j);
+    }
+    return ops;
 }
 
 }  // namespace
@@ -655,6 +817,45 @@ int t2b_backprojector_enforce_hermitian(t2b_ctx* c, int iclass)
         k_hermitian<<<grid_of(pairs), RC_THREADS, 0, c->stream>>>(v, c->gdata[iclass], c->gweight[iclass]);
         T2B_CUDA(cudaGetLastError());
         T2B_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int t2b_point_group(const char* group, double* mats, int cap, int* count)
+{
+    return guarded([&] {
+        T2B_REQUIRE(count && (cap <= 0 || mats), T2B_ERR_ARG, "null argument");
+        const auto ops = point_group(group);
+        *count = (int)ops.size();
+        for (int i = 0; i < (int)ops.size() && i < cap; ++i)
+            for (int e = 0; e < 9; ++e) mats[9 * i + e] = ops[i][e];
+    });
+}
+
+int t2b_backprojector_apply_symmetry(t2b_ctx* c, int iclass, const char* group)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c, T2B_ERR_ARG, "null argument");
+        const auto ops = point_group(group);
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard dg(c->device);
+        const Volume& v = grid_volume(c, iclass);
+        if (ops.empty() || v.ref_dim != 3) return;   // C1, and 2D grids: nothing to do (as the reference)
+        const int rp = v.r_max * v.pad;
+        const size_t nv = v.nvox();
+        cudaStream_t st = c->stream;
+        DevBuf<float2> sd(nv);
+        DevBuf<float> sw(nv);
+        DevBuf<double> R(9 * ops.size());
+        std::vector<double> hr(9 * ops.size());
+        for (size_t i = 0; i < ops.size(); ++i)
+            for (int e = 0; e < 9; ++e) hr[9 * i + e] = ops[i][e];
+        T2B_CUDA(cudaMemcpyAsync(R.p, hr.data(), hr.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        k_symmetrise<<<grid_of((long long)nv), RC_THREADS, 0, st>>>(v, c->gdata[iclass], c->gweight[iclass], sd.p, sw.p,
+                                                                   R.p, (int)ops.size(), rp * rp);
+        T2B_CUDA(cudaGetLastError());
+        T2B_CUDA(cudaMemcpyAsync(c->gdata[iclass], sd.p, nv * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+        T2B_CUDA(cudaMemcpyAsync(c->gweight[iclass], sw.p, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        T2B_CUDA(cudaStreamSynchronize(st));
     });
 }
 

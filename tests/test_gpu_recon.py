@@ -1,5 +1,5 @@
 """M-step reconstruction on the GPU (t2b_reconstruct, t2b_fsc_halves,
-t2b_update_ssnr) against the FP64 oracle (oracle/recon_oracle.py), on the
+t2b_update_ssnr, t2b_backprojector_enforce_hermitian, t2b_backprojector_apply_symmetry) against the FP64 oracle (oracle/recon_oracle.py), on the
 backprojection grids the E-step filled.
 
 Tolerances: the map within 2e-5 of its largest value (the inverse 3D FFT is
@@ -89,6 +89,51 @@ def test_hermitian_symmetry_matches_oracle(name):
     ref = ro.reconstruct_map(rd.astype(np.complex128), rw.astype(np.float64), pb["r"], 2, pb["N"])
     es.close()
     _map_close(got, ref)
+
+
+@pytest.mark.parametrize("group", ["C3", "D2", "T", "I3"])
+def test_point_group_symmetry_matches_oracle(group):
+    """t2b_backprojector_apply_symmetry on the Hermitian-symmetrised grid of an E-step against
+    the oracle's restatement of applyPointGroupSymmetry on the same FP32 grid: the coordinates
+    are rounded as the reference rounds them, the reads and sums are FP64, so the device's
+    FP32 result is the oracle's FP64 sum rounded once (rtol 1e-6); the symmetrised grid then
+    reconstructs to the oracle's map."""
+    pb = problems.build("refine_o2", n_particles=16, seed=37)
+    P = pb["parts"]
+    es = pb["product"]()
+    es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    es.enforce_hermitian_symmetry(0)
+    data, w = es.get_backprojector(0)
+    es.apply_point_group_symmetry(0, group)
+    gd, gw = es.get_backprojector(0)
+    rd, rw = ro.apply_point_group_symmetry(data, w, ro.point_group(group), pb["r"], 2)
+    for g, r in ((gd, rd), (gw, rw)):
+        assert np.max(np.abs(g - r) / (np.abs(r) + 1e-9 * np.max(np.abs(r)))) <= 1e-6
+    assert np.max(np.abs(gw - w)) > 0.1 * np.max(np.abs(w))
+    got = es.reconstruct(0, pb["N"])
+    es.close()
+    ref = ro.reconstruct_map(gd.astype(np.complex128), gw.astype(np.float64), pb["r"], 2, pb["N"])
+    _map_close(got, ref)
+
+
+def test_point_group_symmetry_identity_cases():
+    """C1 leaves a 3D grid as it is, any group a 2D grid (the reference symmetrises 3D only);
+    a group with mirror planes is refused and the grid is left as it was."""
+    t2b = problems.load_package()
+    for name, group in (("refine_o2", "C1"), ("class2d", "O"), ("refine_o2", "D2h")):
+        pb = problems.build(name, n_particles=8, seed=41)
+        P = pb["parts"]
+        es = pb["product"]()
+        es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+        data, w = es.get_backprojector(0)
+        if group == "D2h":
+            with pytest.raises(t2b.T2BError):
+                es.apply_point_group_symmetry(0, group)
+        else:
+            es.apply_point_group_symmetry(0, group)
+        gd, gw = es.get_backprojector(0)
+        es.close()
+        assert np.array_equal(gd, data) and np.array_equal(gw, w)
 
 
 def test_fsc_matches_oracle(two_classes):
