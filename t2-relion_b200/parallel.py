@@ -2,7 +2,9 @@
 
 Particles of an iteration are independent (the reference farms them out to MPI
 followers, src/ml_optimiser_mpi.cpp:1155-1444), so every rank runs the E-step on
-its own shard with no communication on the data path.  The one exchange is at
+its own particles with no communication on the data path: a fixed shard
+(`shard_range`) or jobs drawn from a shared counter (`JobFarm`, the leader's
+job loop without a leader).  The one exchange is at
 the end of the iteration: summing the backprojection grids and the weighted
 sums over the ranks of one gold-standard half, which the reference does by a
 device-to-host copy, a host double sum and MPI Send/Recv
@@ -145,6 +147,115 @@ class HostGrids:
 
     def grids(self):
         return self.data[..., 0] + 1j * self.data[..., 1], self.weight
+
+
+# --- particle jobs: the leader's job loop without a leader --------------------
+def farm_jobs(first, last, followers, nr_pool, guided):
+    """The particle jobs [(first, last), ...] the reference's leader hands out, in the order it
+    grants them, for the particles first..last (inclusive) of one random subset
+    (MlOptimiserMpi::expectation, src/ml_optimiser_mpi.cpp:1187-1227).  With `guided` (split
+    random halves) and more than one follower per half, each job is the particles still to do
+    over 2 x followers, rounded up, at least nr_pool; with one follower the whole subset is one
+    job.  Otherwise (no split halves) jobs are nr_pool particles.  The k-th grant's range depends
+    on k alone, so any rank that draws ticket k can compute it."""
+    todo = last - first + 1
+    if todo <= 0:
+        return []
+    if nr_pool < 1 or followers < 1:
+        raise ValueError("nr_pool and followers must be >= 1")
+    jobs, done = [], 0
+    while done < todo:
+        if not guided:
+            n = nr_pool
+        elif followers == 1:
+            n = todo
+        else:
+            n = max(nr_pool, (todo - done + 2 * followers - 1) // (2 * followers))
+        n = min(n, todo - done)
+        jobs.append((first + done, first + done + n - 1))
+        done += n
+    return jobs
+
+
+class JobFarm:
+    """Dynamic distribution of an iteration's particles over the ranks, in place of the
+    leader/follower exchange of the reference (src/ml_optimiser_mpi.cpp:1155-1444: followers
+    send a job request, the leader replies with the next particle range and the images, the
+    follower runs expectationSomeParticles on it and sends the metadata back).
+
+    Here there is no leader rank: every rank reads its particles itself (the reference's
+    parallel disc I/O) and draws the next job of its random subset with one atomic add on the
+    torch.distributed key-value store (a ticket; the k-th ticket is the k-th job of
+    `farm_jobs`).  A rank that finishes early draws again, so slow and fast GPUs balance as they
+    do under the leader.  With split random halves (gold-standard refinement) rank r plays
+    follower r + 1: even ranks take the particles of subset 1 (0 .. n_half1 - 1), odd ranks those
+    of subset 2, and each subset counts world // 2 followers ((size - 1) / 2 in the reference);
+    a single rank takes both subsets in turn.  Keys are scoped by `tag` (e.g. the iteration), so
+    each iteration starts from ticket 0 without resetting the store."""
+
+    def __init__(self, store, n_particles, nr_pool, rank, world, split_halves=True, n_half1=None, tag=0):
+        if world < 1 or not 0 <= rank < world:
+            raise ValueError("bad rank / world")
+        self.store, self.rank, self.world, self.tag = store, rank, world, tag
+        if split_halves:
+            n1 = (n_particles + 1) // 2 if n_half1 is None else n_half1
+            if not 0 <= n1 <= n_particles:
+                raise ValueError("n_half1 out of range")
+            per_half = max(1, world // 2)
+            subsets = {1: farm_jobs(0, n1 - 1, per_half, nr_pool, True),
+                       2: farm_jobs(n1, n_particles - 1, per_half, nr_pool, True)}
+            self.order = [1, 2] if world == 1 else [half_of(rank)]
+        else:
+            subsets = {0: farm_jobs(0, n_particles - 1, world, nr_pool, False)}
+            self.order = [0]
+        self.subsets = subsets
+
+    def _key(self, subset):
+        return f"t2b_jobfarm/{self.tag}/{subset}"
+
+    def next_job(self):
+        """(subset, first, last) of the next job for this rank, or None when its subsets are done."""
+        while self.order:
+            subset = self.order[0]
+            ticket = int(self.store.add(self._key(subset), 1)) - 1
+            jobs = self.subsets[subset]
+            if ticket < len(jobs):
+                return (subset,) + jobs[ticket]
+            self.order.pop(0)
+        return None
+
+    def __iter__(self):
+        while True:
+            job = self.next_job()
+            if job is None:
+                return
+            yield job
+
+
+def gather_jobs(local, n_particles, group=None):
+    """Collect every rank's per-job results into particle order, as the leader's
+    setMetaDataSubset does with the metadata the followers send back
+    (src/ml_optimiser_mpi.cpp:1166-1180).  `local`: list of (first, last, rows) with rows an
+    array of last - first + 1 rows.  Returns the (n_particles, ...) array on every rank; raises
+    if the jobs do not cover each particle exactly once."""
+    import torch.distributed as dist
+    parts = [local]
+    if dist.is_initialized() and dist.get_world_size(group) > 1:
+        parts = [None] * dist.get_world_size(group)
+        dist.all_gather_object(parts, local, group=group)
+    seen = np.zeros(n_particles, np.int64)
+    out = None
+    for first, last, rows in (j for p in parts for j in p):
+        rows = np.asarray(rows)
+        if rows.shape[0] != last - first + 1 or first < 0 or last >= n_particles:
+            raise ValueError(f"job {first}..{last}: {rows.shape[0]} rows")
+        if out is None:
+            out = np.zeros((n_particles,) + rows.shape[1:], rows.dtype)
+        out[first:last + 1] = rows
+        seen[first:last + 1] += 1
+    if n_particles and not np.all(seen == 1):
+        raise ValueError(f"particles not covered exactly once: {np.flatnonzero(seen != 1)[:8]}")
+    return out
 
 
 # per-particle fields of a result dict that are summed into the model
