@@ -248,13 +248,16 @@ int t2b_backprojector_enforce_hermitian(t2b_ctx* ctx, int iclass);
 
 /* The operators of a point group other than the identity, 3 x 3 row-major into
  * mats (capacity cap matrices; fewer are written when cap is smaller), their number
- * in *count: the rotations k 360 / n about the group's generating axes, transposed, closed
- * under products, entries below 1e-6 zeroed, matrices equal within 1e-6 taken as one
- * (SymList::read_sym_file + compute_subgroup, src/symmetries.cpp:133-191, 273-325;
- * generating axes of SymList::fill_symmetry_class, src/symmetries.cpp:606-725).  Groups:
- * C1, Cn, Dn (n of one or two digits), T, O, I (= I2), I1, I3, I4, case-insensitive.
- * Groups with mirror planes or an inversion (Ci, Cs, Cnv, Cnh, Sn, Dnv, Dnh, Td, Th, Oh,
- * Ih ...) return T2B_ERR_UNSUPPORTED.  Orders: Cn n - 1, Dn 2n - 1, T 11, O 23, I 59. */
+ * in *count, as SymList builds them (read_sym_file + compute_subgroup,
+ * src/symmetries.cpp:133-191, 243-325, generators of fill_symmetry_class, :606-725): the
+ * rotations k 360 / n about each generating axis, transposed; the reflections I - 2 u u^T of
+ * mirror planes of normal u; the inversion -I; closed under products in the reference's
+ * order, entries below 1e-6 zeroed, matrices equal within 1e-6 taken as one.  Groups, named
+ * as the reference reads them (case-insensitive, n of one or two digits): C1, Cn, Ci, Cs, Cnv,
+ * Cnh, Sn (n even; C(n/2) x Ci), Dn, Dnv, Dnh, T, Td, Th, O, Oh, I (= I2), I1, I3, I4, Ih
+ * (= I2h), I1h, I3h, I4h.  Others (I5, I5h, which the reference does not implement either)
+ * return T2B_ERR_UNSUPPORTED, an odd Sn T2B_ERR_ARG.  Orders: Cn n - 1, Dn 2n - 1, Cnv and
+ * Cnh 2n - 1, Dnv and Dnh 4n - 1, T 11, Td, Th and O 23, Oh 47, I 59, Ih 119. */
 int t2b_point_group(const char* group, double* mats, int cap, int* count);
 
 /* Point-group symmetrisation of a 3D grid, in place on the device

@@ -39,10 +39,11 @@ complex, weight real; z, y centred at -initz, -inity; x from 0; 3D grids of
                     applied by MlOptimiser::maximization before reconstruct
                     (src/ml_optimiser.cpp:4626)
   point_group       SymList::read_sym_file + compute_subgroup (src/symmetries.cpp:133-191,
-                    273-325) for the proper groups, with the generating axes of
-                    SymList::fill_symmetry_class (:606-725): rotations k 360 / n about
-                    each axis, transposed, entries below 1e-6 zeroed, closed under
-                    products, equality within 1e-6, the identity left out
+                    243-325), with the generators of SymList::fill_symmetry_class
+                    (:606-725): rotations k 360 / n about each axis, transposed, entries
+                    below 1e-6 zeroed; mirror planes I - 2 u u^T; the inversion -I; closed
+                    under products in the reference's order, equality within 1e-6, the
+                    identity left out
   apply_point_group_symmetry
                     BackProjector::applyPointGroupSymmetry (src/backprojector.cpp:2279-2435):
                     the sum over the operators of the trilinear read at R (x, y, z)
@@ -94,57 +95,98 @@ def enforce_hermitian_symmetry(data, weight):
     return (d[0], w[0]) if two_d else (d, w)
 
 
-# generating axes (fold, axis) of the proper point groups (src/symmetries.cpp:606-725)
-_PG_AXES = {
-    "T": [(3, (0., 0., 1.)), (2, (0., 0.816496, 0.577350))],
-    "O": [(3, (.5773502, .5773502, .5773502)), (4, (0., 0., 1.))],
-    "I": [(2, (0., 0., 1.)), (5, (0.525731114, 0., 0.850650807)), (3, (0., 0.356822076, 0.934172364))],
-    "I1": [(2, (1., 0., 0.)), (5, (0.85065080702670, 0., -0.5257311142635)), (3, (0.9341723640, 0.3568220765, 0.))],
-    "I3": [(2, (-0.5257311143, 0., 0.8506508070)), (5, (0., 0., 1.)),
-           (3, (-0.4911234778630044, 0.3568220764705179, 0.7946544753759428))],
-    "I4": [(2, (0.5257311143, 0., 0.8506508070)), (5, (0.8944271932547096, 0., 0.4472135909903704)),
-           (3, (0.4911234778630044, 0.3568220764705179, 0.7946544753759428))],
+# generators of the point groups (src/symmetries.cpp:606-725): ("rot", fold, axis),
+# ("mirror", normal) or ("inv",)
+_T = [("rot", 3, (0., 0., 1.)), ("rot", 2, (0., 0.816496, 0.577350))]
+_O = [("rot", 3, (.5773502, .5773502, .5773502)), ("rot", 4, (0., 0., 1.))]
+_I2 = [("rot", 2, (0., 0., 1.)), ("rot", 5, (0.525731114, 0., 0.850650807)),
+       ("rot", 3, (0., 0.356822076, 0.934172364))]
+_I1 = [("rot", 2, (1., 0., 0.)), ("rot", 5, (0.85065080702670, 0., -0.5257311142635)),
+       ("rot", 3, (0.9341723640, 0.3568220765, 0.))]
+_I3 = [("rot", 2, (-0.5257311143, 0., 0.8506508070)), ("rot", 5, (0., 0., 1.)),
+       ("rot", 3, (-0.4911234778630044, 0.3568220764705179, 0.7946544753759428))]
+_I4 = [("rot", 2, (0.5257311143, 0., 0.8506508070)), ("rot", 5, (0.8944271932547096, 0., 0.4472135909903704)),
+       ("rot", 3, (0.4911234778630044, 0.3568220764705179, 0.7946544753759428))]
+_PG_FIXED = {
+    "CI": [("inv",)], "CS": [("mirror", (0., 0., 1.))],
+    "T": _T, "TD": _T + [("mirror", (1.4142136, 2.4494897, 0.0000000))],
+    "TH": [("rot", 3, (0., 0., 1.)), ("rot", 2, (0., -0.816496, -0.577350)), ("inv",)],
+    "O": _O, "OH": _O + [("mirror", (0., 1., 1.))],
+    "I": _I2, "I2": _I2, "I1": _I1, "I3": _I3, "I4": _I4,
+    "IH": _I2 + [("mirror", (1., 0., 0.))], "I2H": _I2 + [("mirror", (1., 0., 0.))],
+    "I1H": _I1 + [("mirror", (0., 0., -1.))], "I3H": _I3 + [("mirror", (0.850650807, 0., 0.525731114))],
+    "I4H": _I4 + [("mirror", (0.850650807, 0., -0.525731114))],
 }
-_PG_AXES["I2"] = _PG_AXES["I"]
 
 
 def _pg_generators(name):
-    g = name.upper()
-    if g in _PG_AXES:
-        return _PG_AXES[g]
-    if len(g) in (2, 3) and g[0] in "CD" and g[1:].isdigit():
-        n = int(g[1:])
+    """Generators of a group named as SymList::isSymmetryGroup reads it (src/symmetries.cpp:331-600)."""
+    g = name.upper().replace(" ", "")
+    if g in ("", "C1"):
+        return []
+    if g in _PG_FIXED:
+        return _PG_FIXED[g]
+    suffix = g[-1] if g[-1:] in ("V", "H") else ""
+    digits = g[1:len(g) - len(suffix)]
+    if g[:1] in ("C", "D", "S") and 1 <= len(digits) <= 2 and digits.isdigit() and int(digits) >= 1:
+        n = int(digits)
+        z = ("rot", n, (0., 0., 1.))
+        if g[0] == "S" and not suffix:
+            if n % 2:
+                raise ValueError("the order of an Sn group must be even")
+            return [("rot", n // 2, (0., 0., 1.)), ("inv",)]
         if g[0] == "C":
-            return [(n, (0., 0., 1.))]
-        return ([(n, (0., 0., 1.))] if n > 1 else []) + [(2, (1., 0., 0.))]
-    raise ValueError(f"point group {name!r}: only the proper groups Cn, Dn, T, O, I, I1-I4")
+            return {"": [z], "V": [z, ("mirror", (0., 1., 0.))], "H": [z, ("mirror", (0., 0., 1.))]}[suffix]
+        if g[0] == "D":
+            dn = ([z] if n > 1 else []) + [("rot", 2, (1., 0., 0.))]
+            return {"": dn, "V": dn + [("mirror", (1., 0., 0.))], "H": dn + [("mirror", (0., 0., 1.))]}[suffix]
+    raise ValueError(f"point group {name!r} is not one of C1, Cn, Ci, Cs, Cnv, Cnh, Sn, Dn, Dnv, Dnh, "
+                     "T, Td, Th, O, Oh, I, I1-I4, Ih, I1h-I4h")
 
 
 def point_group(name):
-    """The group's operators other than the identity, (n, 3, 3).  Each generator contributes
-    the transposes of its rotations by k 360 / fold (axis-angle matrix cos I + sin [a]x +
-    (1 - cos) a a^T); the list is then closed under products R_i R_j, taken in the order of
-    found_not_tried (src/symmetries.cpp:243-270: for n = 0, 1, ..., the pairs (0..n, n), then
-    (n, n-1..0)), appending each product that is neither the identity nor present (every
-    entry within 1e-6), zeroed below 1e-6."""
+    """The group's operators other than the identity, (n, 3, 3), built as SymList builds them.
+    A rotation axis contributes the transposes of its rotations by k 360 / fold (axis-angle matrix
+    cos I + sin [a]x + (1 - cos) a a^T, zeroed below 1e-6); a mirror plane of unit normal u the
+    reflection I - 2 u u^T; an inversion -I.  Each operator carries the reference's second matrix
+    L = diag(1, 1, lz): lz = -1 for the inversion, 1 otherwise.  The list is then closed under
+    products (R_i R_j, lz_i lz_j) in the order of found_not_tried (src/symmetries.cpp:243-270:
+    for n = 0, 1, ..., the pairs (0..n, n), then (n, n-1..0)), appending each product that is
+    neither the identity nor present (lz equal and every entry within 1e-6), zeroed below 1e-6."""
     zero = lambda m: np.where(np.abs(m) < 1e-6, 0.0, m)
-    eq = lambda a, b: bool(np.all(np.abs(a - b) <= 1e-6))
     ops = []
-    for fold, ax in _pg_generators(name):
-        a = np.asarray(ax, float) / np.linalg.norm(ax)
+    for gen in _pg_generators(name):
+        if gen[0] == "inv":
+            ops.append((-np.eye(3), -1))
+            continue
+        a = np.asarray(gen[-1], float) / np.linalg.norm(gen[-1])
+        if gen[0] == "mirror":
+            ops.append((np.eye(3) - 2.0 * np.outer(a, a), 1))
+            continue
+        fold = gen[1]
         cross = np.array([[0., -a[2], a[1]], [a[2], 0., -a[0]], [-a[1], a[0], 0.]])
         for k in range(1, fold):
             t = k * 2.0 * PI / fold
             rot = np.cos(t) * np.eye(3) + np.sin(t) * cross + (1.0 - np.cos(t)) * np.outer(a, a)
-            ops.append(zero(rot.T))
-    n = 0
-    while n < len(ops):
-        for i, j in [(i, n) for i in range(n + 1)] + [(n, j) for j in range(n - 1, -1, -1)]:
-            p = ops[i] @ ops[j]
-            if not (eq(p, np.eye(3)) or any(eq(p, o) for o in ops)):
-                ops.append(zero(p))
+            ops.append((zero(rot.T), 1))
+    R = np.zeros((1001, 3, 3))
+    L = np.zeros(1001, np.int64)
+    R[0], L[0] = np.eye(3), 1            # slot 0: the identity, never part of the result
+    for m, (r, lz) in enumerate(ops, 1):
+        R[m], L[m] = r, lz
+    m = len(ops) + 1
+    n = 1
+    while n < m:
+        for i, j in [(i, n) for i in range(1, n + 1)] + [(n, j) for j in range(n - 1, 0, -1)]:
+            p, plz = R[i] @ R[j], L[i] * L[j]
+            if np.any(np.all(np.abs(R[:m] - p) <= 1e-6, axis=(1, 2)) & (L[:m] == plz)):
+                continue
+            if m == 1001:
+                raise ValueError("point group does not close")
+            R[m], L[m] = zero(p), plz
+            m += 1
         n += 1
-    return np.array(ops).reshape(-1, 3, 3)
+    return R[1:m].copy()
 
 
 def apply_point_group_symmetry(data, weight, mats, r_max, pad):

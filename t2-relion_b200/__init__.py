@@ -239,7 +239,7 @@ def version():
 
 
 def point_group(group):
-    """t2b_point_group: the operators of a proper point group other than the identity, an
+    """t2b_point_group: the operators of a point group other than the identity, an
     (n, 3, 3) array (SymList after read_sym_file, src/symmetries.cpp:51-191)."""
     n = ctypes.c_int(0)
     _check(lib.t2b_point_group(group.encode(), None, 0, ctypes.byref(n)))
@@ -442,8 +442,8 @@ class EStep:
 
     # BackProjector::applyPointGroupSymmetry
     def apply_point_group_symmetry(self, iclass, group):
-        """t2b_backprojector_apply_symmetry: sum of the grid over the operators of a proper
-        point group ("C1", "Cn", "Dn", "T", "O", "I", "I1"-"I4"), in place."""
+        """t2b_backprojector_apply_symmetry: sum of the grid over the operators of a point
+        group named as the reference's --sym ("C1", "C4", "D7", "D2h", "O", "I", "I3h" ...), in place."""
         _check(lib.t2b_backprojector_apply_symmetry(self._h, iclass, group.encode()))
 
     # AccBackprojector::getMdlData

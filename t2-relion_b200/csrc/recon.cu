@@ -30,6 +30,7 @@
 #include <cctype>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -619,61 +620,102 @@ const Volume& grid_volume(t2b_ctx* c, int ig)
     return v;
 }
 
-// The operators of a proper point group, 3 x 3 row-major, the identity excluded: the rotations
-// k * 360 / n about each generating axis, transposed, then every product until the set is
-// closed (SymList::read_sym_file + compute_subgroup, src/symmetries.cpp:133-191, 273-325),
-// entries below 1e-6 set to 0 and matrices equal within 1e-6 taken as one.  The generating
-// axes are the reference's (SymList::fill_symmetry_class, src/symmetries.cpp:606-725; names as
-// SymList::isSymmetryGroup: case-insensitive, orders of one or two digits): Cn the
-// z axis; Dn that and a 2-fold about x; T, O and I (= I2) and I1, I3, I4 their tabulated axes.
-// Groups with mirrors or an inversion (Cs, Ci, Cnv, Cnh, Sn, Dnv, Dnh, Td, Th, Oh, Ih ...) are
-// refused: the maps of chiral molecules use none.
+// The operators of a point group, 3 x 3 row-major, the identity excluded, as SymList builds
+// them (SymList::read_sym_file + compute_subgroup, src/symmetries.cpp:133-191, 243-325):
+//  - a rotation axis of order n gives the rotations k * 360 / n about it, transposed, entries
+//    below 1e-6 set to 0;
+//  - a mirror plane with unit normal u gives I - 2 u u^T (the reference's A^T diag(1, 1, -1) A,
+//    A turning u onto z), an inversion -I; the reference pairs every operator with a second
+//    matrix L, diag(1, 1, -1) for the inversion and the identity otherwise, and so do we (lz);
+//  - then every product in the reference's order: shells n = 0, 1, ..., the pairs (i, n) for
+//    i = 0..n, then (n, j) for j = n-1..0 (found_not_tried), appended unless it is the identity
+//    or equals a listed operator (L and R within 1e-6), zeroed below 1e-6.  The order fixes
+//    which chain of products each operator comes from, and so its last digits (the generating
+//    axes carry six to ten).
+// The generators are the reference's (SymList::fill_symmetry_class, src/symmetries.cpp:606-725),
+// the names as SymList::isSymmetryGroup reads them (:331-600: case-insensitive, orders of one or
+// two digits): C1, Cn, Ci, Cs, Cnv, Cnh, Sn (n even), Dn, Dnv, Dnh, T, Td, Th, O, Oh, I, I1-I4,
+// Ih, I1h-I4h.  I5 and I5h, which the reference does not implement either, are refused.
 std::vector<std::array<double, 9>> point_group(const char* name)
 {
     using M = std::array<double, 9>;
+    struct Op { M r; int lz; };
+    enum Kind { ROT, MIRROR, INVERSION };
+    struct Gen { Kind kind; int fold; double ax, ay, az; };
     std::string g;
     for (const char* p = name; p && *p; ++p)
         if (*p != ' ') g += (char)std::toupper((unsigned char)*p);
-    struct Gen { int fold; double ax, ay, az; };
-    std::vector<Gen> gens;
-    auto order = [&](size_t from) -> int {
-        if (g.size() <= from || g.size() > from + 2) return -1;
-        for (size_t i = from; i < g.size(); ++i)
+    // order n of a name "<letter><n><suffix>", n of one or two digits; -1 if it does not match
+    const auto order = [&](char lead, const char* suffix) -> int {
+        const size_t ls = std::strlen(suffix);
+        if (g.size() < 2 + ls || g.size() > 3 + ls || g[0] != lead) return -1;
+        if (g.compare(g.size() - ls, ls, suffix) != 0) return -1;
+        for (size_t i = 1; i < g.size() - ls; ++i)
             if (!std::isdigit((unsigned char)g[i])) return -1;
-        return std::atoi(g.c_str() + from);
+        return std::atoi(g.substr(1, g.size() - 1 - ls).c_str());
     };
-    if (g.empty() || g == "C1") {
-        return {};
-    } else if (g[0] == 'C' && order(1) >= 1) {
-        if (order(1) > 1) gens.push_back({order(1), 0, 0, 1});
-    } else if (g[0] == 'D' && order(1) >= 1) {
-        if (order(1) > 1) gens.push_back({order(1), 0, 0, 1});
-        gens.push_back({2, 1, 0, 0});
-    } else if (g == "T") {
-        gens = {{3, 0., 0., 1.}, {2, 0., 0.816496, 0.577350}};
-    } else if (g == "O") {
-        gens = {{3, .5773502, .5773502, .5773502}, {4, 0, 0, 1}};
-    } else if (g == "I" || g == "I2") {
-        gens = {{2, 0, 0, 1}, {5, 0.525731114, 0, 0.850650807}, {3, 0, 0.356822076, 0.934172364}};
-    } else if (g == "I1") {
-        gens = {{2, 1, 0, 0}, {5, 0.85065080702670, 0, -0.5257311142635}, {3, 0.9341723640, 0.3568220765, 0}};
-    } else if (g == "I3") {
-        gens = {{2, -0.5257311143, 0, 0.8506508070}, {5, 0., 0., 1.},
-                {3, -0.4911234778630044, 0.3568220764705179, 0.7946544753759428}};
-    } else if (g == "I4") {
-        gens = {{2, 0.5257311143, 0, 0.8506508070}, {5, 0.8944271932547096, 0, 0.4472135909903704},
-                {3, 0.4911234778630044, 0.3568220764705179, 0.7946544753759428}};
-    } else {
+    const std::vector<Gen> T_ = {{ROT, 3, 0., 0., 1.}, {ROT, 2, 0., 0.816496, 0.577350}};
+    const std::vector<Gen> O_ = {{ROT, 3, .5773502, .5773502, .5773502}, {ROT, 4, 0, 0, 1}};
+    const std::vector<Gen> I2_ = {{ROT, 2, 0, 0, 1}, {ROT, 5, 0.525731114, 0, 0.850650807},
+                                  {ROT, 3, 0, 0.356822076, 0.934172364}};
+    const std::vector<Gen> I1_ = {{ROT, 2, 1, 0, 0}, {ROT, 5, 0.85065080702670, 0, -0.5257311142635},
+                                  {ROT, 3, 0.9341723640, 0.3568220765, 0}};
+    const std::vector<Gen> I3_ = {{ROT, 2, -0.5257311143, 0, 0.8506508070}, {ROT, 5, 0., 0., 1.},
+                                  {ROT, 3, -0.4911234778630044, 0.3568220764705179, 0.7946544753759428}};
+    const std::vector<Gen> I4_ = {{ROT, 2, 0.5257311143, 0, 0.8506508070},
+                                  {ROT, 5, 0.8944271932547096, 0, 0.4472135909903704},
+                                  {ROT, 3, 0.4911234778630044, 0.3568220764705179, 0.7946544753759428}};
+    const auto plus = [](std::vector<Gen> a, const Gen& b) {
+        a.push_back(b);
+        return a;
+    };
+    const auto dihedral = [&](int n) {
+        std::vector<Gen> v;
+        if (n > 1) v.push_back({ROT, n, 0, 0, 1});
+        v.push_back({ROT, 2, 1, 0, 0});
+        return v;
+    };
+    std::vector<Gen> gens;
+    bool known = true;
+    int n;
+    if (g.empty() || g == "C1") return {};
+    if ((n = order('C', "")) >= 1) gens = {{ROT, n, 0, 0, 1}};
+    else if (g == "CI") gens = {{INVERSION, 0, 0, 0, 0}};
+    else if (g == "CS") gens = {{MIRROR, 0, 0, 0, 1}};
+    else if ((n = order('C', "V")) >= 1) gens = {{ROT, n, 0, 0, 1}, {MIRROR, 0, 0, 1, 0}};
+    else if ((n = order('C', "H")) >= 1) gens = {{ROT, n, 0, 0, 1}, {MIRROR, 0, 0, 0, 1}};
+    else if ((n = order('S', "")) >= 1) {
+        if (n % 2) throw Error{T2B_ERR_ARG, "the order of an Sn group must be even"};
+        gens = {{ROT, n / 2, 0, 0, 1}, {INVERSION, 0, 0, 0, 0}};
+    } else if ((n = order('D', "")) >= 1) gens = dihedral(n);
+    else if ((n = order('D', "V")) >= 1) gens = plus(dihedral(n), {MIRROR, 0, 1, 0, 0});
+    else if ((n = order('D', "H")) >= 1) gens = plus(dihedral(n), {MIRROR, 0, 0, 0, 1});
+    else if (g == "T") gens = T_;
+    else if (g == "TD") gens = plus(T_, {MIRROR, 0, 1.4142136, 2.4494897, 0.0000000});
+    else if (g == "TH") gens = {{ROT, 3, 0., 0., 1.}, {ROT, 2, 0., -0.816496, -0.577350}, {INVERSION, 0, 0, 0, 0}};
+    else if (g == "O") gens = O_;
+    else if (g == "OH") gens = plus(O_, {MIRROR, 0, 0, 1, 1});
+    else if (g == "I" || g == "I2") gens = I2_;
+    else if (g == "I1") gens = I1_;
+    else if (g == "I3") gens = I3_;
+    else if (g == "I4") gens = I4_;
+    else if (g == "IH" || g == "I2H") gens = plus(I2_, {MIRROR, 0, 1, 0, 0});
+    else if (g == "I1H") gens = plus(I1_, {MIRROR, 0, 0, 0, -1});
+    else if (g == "I3H") gens = plus(I3_, {MIRROR, 0, 0.850650807, 0, 0.525731114});
+    else if (g == "I4H") gens = plus(I4_, {MIRROR, 0, 0.850650807, 0, -0.525731114});
+    else known = false;
+    if (!known)
         throw Error{T2B_ERR_UNSUPPORTED, std::string("point group '") + (name ? name : "") +
-                                             "' not supported: C1, Cn, Dn, T, O, I, I1-I4 (rotations only)"};
-    }
+                                             "' not supported: C1, Cn, Ci, Cs, Cnv, Cnh, Sn, Dn, Dnv, Dnh, T, Td, Th, "
+                                             "O, Oh, I, I1-I4, Ih, I1h-I4h"};
     const auto clean = [](M& a) {
         for (double& v : a)
             if (std::fabs(v) < 1e-6) v = 0.;
     };
-    const auto same = [](const M& a, const M& b) {
+    const auto same = [](const Op& a, const Op& b) {
+        if (a.lz != b.lz) return false;
         for (int i = 0; i < 9; ++i)
-            if (std::fabs(a[i] - b[i]) > 1e-6) return false;
+            if (std::fabs(a.r[i] - b.r[i]) > 1e-6) return false;
         return true;
     };
     const auto mul = [](const M& a, const M& b) {
@@ -683,42 +725,49 @@ std::vector<std::array<double, 9>> point_group(const char* name)
                 for (int k = 0; k < 3; ++k) r[3 * i + j] += a[3 * i + k] * b[3 * k + j];
         return r;
     };
-    const M ident = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-    std::vector<M> ops;
+    const Op ident = {{1, 0, 0, 0, 1, 0, 0, 0, 1}, 1};
+    std::vector<Op> ops;
     for (const Gen& ge : gens) {
         const double nrm = std::sqrt(ge.ax * ge.ax + ge.ay * ge.ay + ge.az * ge.az);
         const double a[3] = {ge.ax / nrm, ge.ay / nrm, ge.az / nrm};
-        for (int kk = 1; kk < ge.fold; ++kk) {
-            const double ang = kk * (2.0 * PI_R / ge.fold), cs = std::cos(ang), sn = std::sin(ang);
-            // rotation by ang about a (Rodrigues), transposed
+        if (ge.kind == INVERSION) {
+            ops.push_back({{-1, 0, 0, 0, -1, 0, 0, 0, -1}, -1});
+        } else if (ge.kind == MIRROR) {
             M r;
             for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    const double cross = (i == j) ? 0. : ((3 + j - i) % 3 == 1 ? -1. : 1.) * a[3 - i - j];
-                    r[3 * j + i] = (i == j ? cs : 0.) + sn * cross + (1. - cs) * a[i] * a[j];
-                }
-            clean(r);
-            ops.push_back(r);
+                for (int j = 0; j < 3; ++j) r[3 * i + j] = (i == j ? 1. : 0.) - 2. * a[i] * a[j];
+            ops.push_back({r, 1});
+        } else {
+            for (int kk = 1; kk < ge.fold; ++kk) {
+                const double ang = kk * (2.0 * PI_R / ge.fold), cs = std::cos(ang), sn = std::sin(ang);
+                // rotation by ang about a (Rodrigues), transposed
+                M r;
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        const double cross = (i == j) ? 0. : ((3 + j - i) % 3 == 1 ? -1. : 1.) * a[3 - i - j];
+                        r[3 * j + i] = (i == j ? cs : 0.) + sn * cross + (1. - cs) * a[i] * a[j];
+                    }
+                clean(r);
+                ops.push_back({r, 1});
+            }
         }
     }
-    // Products in the reference's order (found_not_tried, src/symmetries.cpp:243-270): shell
-    // n = 0, 1, ... holds the pairs (i, n) for i = 0..n, then (n, j) for j = n-1..0; an operator
-    // appended while shell n runs opens a later shell.  The order fixes which chain of
-    // products each operator comes from, and so its last digits (the generating axes carry
-    // six to ten).
     const auto visit = [&](size_t i, size_t j) {
-        M p = mul(ops[i], ops[j]);
+        Op p = {mul(ops[i].r, ops[j].r), ops[i].lz * ops[j].lz};
         if (same(p, ident)) return;
-        for (const M& o : ops)
+        for (const Op& o : ops)
             if (same(o, p)) return;
-        clean(p);
+        clean(p.r);
         ops.push_back(p);
+        T2B_REQUIRE(ops.size() < 1000, T2B_ERR_ARG, "point group does not close");
     };
-    for (size_t n = 0; n < ops.size(); ++n) {
-        for (size_t i = 0; i <= n; ++i) visit(i, n);
-        for (size_t j = n; j-- > 0;) visit(n, j);
+    for (size_t q = 0; q < ops.size(); ++q) {
+        for (size_t i = 0; i <= q; ++i) visit(i, q);
+        for (size_t j = q; j-- > 0;) visit(q, j);
     }
-    return ops;
+    std::vector<M> out;
+    for (const Op& o : ops) out.push_back(o.r);
+    return out;
 }
 
 }  // namespace

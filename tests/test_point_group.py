@@ -1,6 +1,7 @@
 """Point-group symmetry on the host: the library's group generator (t2b_point_group) against
 the oracle's restatement of SymList (oracle/recon_oracle.py), both pinned by facts of the
-groups themselves (orders, angle classes, the exact matrices of C4, D2 and O), and the
+groups themselves (orders, improper counts, angle classes, the exact matrices of C4, D2, O,
+Oh, Cs, C2v and S4, the inversion groups as rotations x Ci), and the
 oracle's symmetrisation of a grid against a direct loop for the 4-fold group, whose rotated
 coordinates are integers.  No GPU."""
 import itertools
@@ -11,7 +12,12 @@ import pytest
 import recon_oracle as ro
 
 ORDERS = {"C1": 0, "c2": 1, "C4": 3, "C12": 11, "D1": 1, "D2": 3, "d7": 13, "T": 11, "O": 23,
-          "I": 59, "I1": 59, "I2": 59, "I3": 59, "I4": 59}
+          "I": 59, "I1": 59, "I2": 59, "I3": 59, "I4": 59,
+          # with mirror planes or an inversion (Sn is C(n/2) x Ci in the reference)
+          "Ci": 1, "Cs": 1, "C3v": 5, "c4h": 7, "S4": 3, "S10": 9, "D1h": 3, "D3v": 11, "D2h": 7, "D12h": 47,
+          "Td": 23, "Th": 23, "Oh": 47, "Ih": 119, "I1h": 119, "I2h": 119, "I3h": 119, "I4h": 119}
+IMPROPER = {"Ci": 1, "Cs": 1, "C3v": 3, "c4h": 4, "S4": 2, "S10": 5, "D1h": 2, "D3v": 6, "D2h": 4, "D12h": 24,
+            "Td": 12, "Th": 12, "Oh": 24, "Ih": 60, "I1h": 60, "I2h": 60, "I3h": 60, "I4h": 60}
 
 
 @pytest.mark.parametrize("group", list(ORDERS))
@@ -23,17 +29,21 @@ def test_library_group_equals_oracle(t2b, group):
         assert np.max(np.abs(got - ref)) <= 1e-12
 
 
-@pytest.mark.parametrize("group", ["C12", "D7", "T", "O", "I", "I1", "I3", "I4"])
-def test_group_is_closed_rotations(group):
+@pytest.mark.parametrize("group", ["C12", "D7", "T", "O", "I", "I1", "I3", "I4", "C3v", "S10", "D12h", "Td", "Th",
+                                   "Oh", "Ih", "I3h"])
+def test_group_is_closed_and_orthogonal(group):
     ops = ro.point_group(group)
     eye = np.eye(3)
+    dets = []
     for m in ops:
         assert np.max(np.abs(m @ m.T - eye)) <= 1e-6
-        assert abs(np.linalg.det(m) - 1.0) <= 1e-6
-    members = list(ops) + [eye]
-    for a, b in itertools.product(members, members):
-        p = a @ b
-        assert min(np.max(np.abs(p - m)) for m in members) <= 1e-5
+        dets.append(np.linalg.det(m))
+        assert abs(abs(dets[-1]) - 1.0) <= 1e-6
+    assert int(np.sum(np.array(dets) < 0)) == IMPROPER.get(group, 0)
+    members = np.concatenate([ops, eye[None]])
+    prods = np.einsum("aij,bjk->abik", members, members).reshape(-1, 1, 3, 3)
+    dist = np.max(np.abs(prods - members[None]), axis=(2, 3)).min(axis=1)
+    assert np.all(dist <= 1e-5)
 
 
 def _angles(ops):
@@ -61,6 +71,44 @@ def test_octahedral_group_is_the_signed_permutations():
         assert min(np.max(np.abs(w - m)) for m in ops) <= 1e-12
 
 
+def test_octahedral_with_mirrors_is_every_signed_permutation():
+    ops = ro.point_group("Oh")
+    want = []
+    for perm in itertools.permutations(range(3)):
+        for signs in itertools.product((1, -1), repeat=3):
+            m = np.zeros((3, 3))
+            m[range(3), perm] = signs
+            if not np.array_equal(m, np.eye(3)):
+                want.append(m)
+    assert len(want) == len(ops) == 47
+    for w in want:
+        assert min(np.max(np.abs(w - m)) for m in ops) <= 1e-12
+
+
+@pytest.mark.parametrize("proper,full", [("I", "Ih"), ("I1", "I1h"), ("I3", "I3h"), ("I4", "I4h"), ("T", "Th"),
+                                         ("D6", "D6h"), ("C4", "C4h")])
+def test_groups_with_a_centre_of_inversion(proper, full):
+    """Each of these holds the inversion, so its improper operators are minus its rotations: the
+    rotations of the proper group (Th is generated about the negated 2-fold axis, the same group)."""
+    rot = list(ro.point_group(proper)) + [np.eye(3)]
+    ops = ro.point_group(full)
+    assert len(ops) == 2 * len(rot) - 1
+    for m in ops:
+        cand = m if np.linalg.det(m) > 0 else -m
+        assert min(np.max(np.abs(cand - r)) for r in rot) <= 1e-6
+
+
+def test_mirror_generators():
+    """Cs: the mirror z -> -z; C2v: the two vertical mirrors (normals x and y) and the 2-fold;
+    S4 (the reference's C2 x Ci): the 2-fold about z, the inversion and the mirror z -> -z."""
+    assert np.array_equal(ro.point_group("Cs")[0], np.diag([1., 1., -1.]))
+    for ops, want in ((ro.point_group("C2v"), [np.diag([-1., -1., 1.]), np.diag([1., -1., 1.]), np.diag([-1., 1., 1.])]),
+                      (ro.point_group("S4"), [np.diag([-1., -1., 1.]), -np.eye(3), np.diag([1., 1., -1.])])):
+        assert len(ops) == 3
+        for w in want:
+            assert min(np.max(np.abs(w - m)) for m in ops) <= 1e-12
+
+
 def test_dihedral_and_cyclic_matrices():
     d2 = ro.point_group("D2")
     for diag in ((1, -1, -1), (-1, 1, -1), (-1, -1, 1)):
@@ -75,11 +123,12 @@ def test_dihedral_and_cyclic_matrices():
         assert min(np.max(np.abs(two - m)) for m in ro.point_group(g)) <= 1e-9
 
 
-@pytest.mark.parametrize("bad", ["C2v", "D2h", "Ci", "Cs", "S4", "Td", "Oh", "Ih", "I5", "C123", "X"])
-def test_groups_with_mirrors_or_unknown_are_refused(t2b, bad):
+@pytest.mark.parametrize("bad", ["I5", "I5h", "C0", "C123", "D2x", "Tv", "X", "S3"])
+def test_unknown_groups_are_refused(t2b, bad):
+    """I5 / I5h are not implemented by the reference either; an Sn group needs an even n."""
     with pytest.raises(t2b.T2BError) as e:
         t2b.point_group(bad)
-    assert e.value.code == t2b.T2B_ERR_UNSUPPORTED
+    assert e.value.code == (t2b.T2B_ERR_ARG if bad == "S3" else t2b.T2B_ERR_UNSUPPORTED)
     with pytest.raises(ValueError):
         ro.point_group(bad)
 
