@@ -272,6 +272,18 @@ int t2b_point_group(const char* group, double* mats, int cap, int* count);
  * the grids over GPUs, but once. */
 int t2b_backprojector_apply_symmetry(t2b_ctx* ctx, int iclass, const char* group);
 
+/* Helical symmetrisation of a 3D grid, in place on the device
+ * (BackProjector::applyHelicalSymmetry, src/backprojector.cpp:2122-2277, applied by
+ * MlOptimiser::maximization between enforceHermitianSymmetry and applyPointGroupSymmetry,
+ * src/ml_optimiser.cpp:4630): for the asymmetric units hh = -n/2 .. n/2 - 1 (.. n/2 for odd
+ * n = nr_asu) other than 0, each voxel inside ROUND(r_max pad)^2 gains the grid read at
+ * Rz(-hh twist) (x, y, z) (twist in degrees; entries of the rotation below 1e-6 zeroed) by
+ * trilinear interpolation (the conjugate where the rotated x < 0); the data term, when rise
+ * (pixels: the reference passes helical_rise / pixel_size) is not 0, times
+ * e^{2 pi i z hh rise / (-ori_size pad)}.  FP64 coordinates, phases and sums, FP32 grid; reads
+ * from the grid as it was before the call.  nr_asu < 2 and 2D grids: unchanged. */
+int t2b_backprojector_apply_helical(t2b_ctx* ctx, int iclass, int nr_asu, double twist, double rise, int ori_size);
+
 /* Fourier shell correlation of two grids (two half-sets) after down-sampling to
  * the unpadded box (BackProjector::getDownsampledAverage +
  * calculateDownSampledFourierShellCorrelation, src/backprojector.cpp:933-1040);

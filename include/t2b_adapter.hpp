@@ -78,6 +78,11 @@ public:
     {
         check(t2b_backprojector_apply_symmetry(b_.ctx(), iclass_, group));
     }
+    // BackProjector::applyHelicalSymmetry (rise in pixels; ori_size: the BackProjector's)
+    void applyHelicalSymmetry(int nr_helical_asu, double helical_twist, double helical_rise, int ori_size)
+    {
+        check(t2b_backprojector_apply_helical(b_.ctx(), iclass_, nr_helical_asu, helical_twist, helical_rise, ori_size));
+    }
     void getMdlData(float* real, float* imag, float* weight)
     {
         check(t2b_backprojector_get(b_.ctx(), iclass_, real, imag, weight));

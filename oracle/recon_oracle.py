@@ -48,6 +48,9 @@ complex, weight real; z, y centred at -initz, -inity; x from 0; 3D grids of
                     BackProjector::applyPointGroupSymmetry (src/backprojector.cpp:2279-2435):
                     the sum over the operators of the trilinear read at R (x, y, z)
                     (conjugated where the rotated x < 0), inside ROUND(r_max pad)^2
+  helical_operators BackProjector::applyHelicalSymmetry (:2122-2277): the rotations about z
+                    and the z phase shifts of the helical units, summed by
+                    apply_point_group_symmetry(..., zshift)
   downsampled_fsc   getDownsampledAverage + calculateDownSampledFourierShellCorrelation
                     (src/backprojector.cpp:933-1040)
   update_ssnr       BackProjector::updateSSNRarrays (src/backprojector.cpp:1041-1205)
@@ -189,10 +192,31 @@ def point_group(name):
     return R[1:m].copy()
 
 
-def apply_point_group_symmetry(data, weight, mats, r_max, pad):
+def helical_operators(nr_asu, twist, rise, ori_size, pad):
+    """The operators and z shifts of BackProjector::applyHelicalSymmetry (src/backprojector.cpp:
+    2122-2277): for hh = -n/2 .. n/2 - 1 (+1 for odd n) other than 0, rotation3DMatrix(-hh twist,
+    'Z') = [[c, -s, 0], [s, c, 0], [0, 0, 1]] zeroed below 1e-6, and zshift = hh rise /
+    (-ori_size pad) (0 when rise is 0)."""
+    mats, zsh = [], []
+    if nr_asu < 2:
+        return np.zeros((0, 3, 3)), np.zeros(0)
+    h_min = -(nr_asu // 2)
+    for hh in range(h_min, -h_min + nr_asu % 2):
+        if hh == 0:
+            continue
+        ang = (hh * -twist) * PI / 180.0
+        r = np.array([[np.cos(ang), -np.sin(ang), 0.], [np.sin(ang), np.cos(ang), 0.], [0., 0., 1.]])
+        mats.append(np.where(np.abs(r) < 1e-6, 0.0, r))
+        zsh.append((hh * rise) / (-ori_size * float(pad)) if abs(rise) > 0 else 0.0)
+    return np.array(mats), np.array(zsh)
+
+
+def apply_point_group_symmetry(data, weight, mats, r_max, pad, zshift=None):
     """Sum over the operators R of the grid read at R (x, y, z), added to the grid itself, for
     r^2 <= ROUND(r_max pad)^2 (FP64 coordinates and sums; the reads come from the input
-    grid).  3D centred half-complex grids; returns new complex128 / float64 arrays."""
+    grid).  With zshift (helical symmetry), operator s's data read is also multiplied by
+    e^{2 pi i z zshift[s]}, z the voxel's own, formed as (ac - bd, (a + b)(c + d) - ac - bd).
+    3D centred half-complex grids; returns new complex128 / float64 arrays."""
     d = np.asarray(data, np.complex128)
     w = np.asarray(weight, np.float64)
     zd, yd, xd = w.shape
@@ -206,7 +230,7 @@ def apply_point_group_symmetry(data, weight, mats, r_max, pad):
     sw = w.ravel().copy()
     acc_d = np.zeros(x.size, np.complex128)
     acc_w = np.zeros(x.size)
-    for m in mats:
+    for s_, m in enumerate(mats):
         xp = x * m[0, 0] + y * m[0, 1] + z * m[0, 2]
         yp = x * m[1, 0] + y * m[1, 1] + z * m[1, 2]
         zp = x * m[2, 0] + y * m[2, 1] + z * m[2, 2]
@@ -229,7 +253,14 @@ def apply_point_group_symmetry(data, weight, mats, r_max, pad):
             return y0v + (y1v - y0v) * fz
 
         vd = tri(d)
-        acc_d += np.where(ok, np.where(neg, np.conj(vd), vd), 0)
+        vd = np.where(neg, np.conj(vd), vd)
+        if zshift is not None and zshift[s_] != 0:
+            dotp = 2 * PI * (z * zshift[s_])
+            a, b = np.cos(dotp), np.sin(dotp)
+            c, dd = vd.real, vd.imag
+            ac, bd = a * c, b * dd
+            vd = (ac - bd) + 1j * ((a + b) * (c + dd) - ac - bd)
+        acc_d += np.where(ok, vd, 0)
         acc_w += np.where(ok, tri(w), 0.0)
     sd[inside] += acc_d
     sw[inside] += acc_w

@@ -43,7 +43,7 @@ ABI_SYMBOLS = (
     "t2b_proposal_logits", "t2b_proposal_grad", "t2b_stage_timing",
     "t2b_prep_configure", "t2b_prep_batch_host", "t2b_prep_batch_device", "t2b_autotune", "t2b_tune_set",
     "t2b_reconstruct", "t2b_fsc_halves", "t2b_update_ssnr", "t2b_backprojector_enforce_hermitian",
-    "t2b_point_group", "t2b_backprojector_apply_symmetry",
+    "t2b_point_group", "t2b_backprojector_apply_symmetry", "t2b_backprojector_apply_helical",
     "t2b_mrc_info", "t2b_mrc_read", "t2b_mrc_write", "t2b_star_open", "t2b_star_shape", "t2b_star_label",
     "t2b_star_column", "t2b_star_value", "t2b_star_close", "t2b_star_write",
 )
@@ -173,6 +173,7 @@ def _setup_prototypes():
     lib.t2b_backprojector_enforce_hermitian.argtypes = [v, i]
     lib.t2b_point_group.argtypes = [ctypes.c_char_p, v, i, ctypes.POINTER(i)]
     lib.t2b_backprojector_apply_symmetry.argtypes = [v, i, ctypes.c_char_p]
+    lib.t2b_backprojector_apply_helical.argtypes = [v, i, i, ctypes.c_double, ctypes.c_double, i]
     lib.t2b_backprojector_get.argtypes = [v, i, v, v, v]
     lib.t2b_backprojector_device_ptrs.argtypes = [v, i, ctypes.POINTER(v), ctypes.POINTER(v)]
     lib.t2b_configure.argtypes = [v, ctypes.POINTER(Config)]
@@ -445,6 +446,12 @@ class EStep:
         """t2b_backprojector_apply_symmetry: sum of the grid over the operators of a point
         group named as the reference's --sym ("C1", "C4", "D7", "D2h", "O", "I", "I3h" ...), in place."""
         _check(lib.t2b_backprojector_apply_symmetry(self._h, iclass, group.encode()))
+
+    # BackProjector::applyHelicalSymmetry
+    def apply_helical_symmetry(self, iclass, nr_asu, twist, rise, ori_size):
+        """t2b_backprojector_apply_helical: sum of the grid over nr_asu helical units (twist in
+        degrees, rise in pixels), in place."""
+        _check(lib.t2b_backprojector_apply_helical(self._h, iclass, nr_asu, twist, rise, ori_size))
 
     # AccBackprojector::getMdlData
     def get_backprojector(self, iclass):
@@ -816,6 +823,9 @@ class AccBackprojector:
 
     def applyPointGroupSymmetry(self, group):
         self.estep.apply_point_group_symmetry(self.iclass, group)
+
+    def applyHelicalSymmetry(self, nr_helical_asu, helical_twist, helical_rise, ori_size):
+        self.estep.apply_helical_symmetry(self.iclass, nr_helical_asu, helical_twist, helical_rise, ori_size)
 
     def getMdlData(self):
         data, w = self.estep.get_backprojector(self.iclass)

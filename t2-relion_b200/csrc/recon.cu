@@ -486,9 +486,13 @@ std::vector<double> ftblob_ratio(int ntab)
 // gets the sum, over the group's operators R other than the identity, of the grid read at
 // R (x, y, z) by trilinear interpolation (the conjugate Friedel partner where the rotated x < 0),
 // added to its own value; data and weight alike.  FP64 coordinates and sums, FP32 grids.
+// With zsh (helical symmetry, BackProjector::applyHelicalSymmetry, src/backprojector.cpp:2122-2277),
+// the data read for operator s is also multiplied by e^{2 pi i z zsh[s]} (z the voxel's own z;
+// zsh[s] = hh rise / (-ori_size pad)), formed as the reference forms it: (ac - bd,
+// (a + b)(c + d) - ac - bd).
 __global__ void k_symmetrise(Volume g, const float2* __restrict__ data, const float* __restrict__ weight,
                              float2* __restrict__ sdata, float* __restrict__ sweight, const double* __restrict__ R,
-                             int nsym, int rmax2)
+                             const double* __restrict__ zsh, int nsym, int rmax2)
 {
     const long long total = (long long)g.zdim * g.ydim * g.xdim;
     const size_t plane = (size_t)g.ydim * g.xdim;
@@ -527,8 +531,16 @@ __global__ void k_symmetrise(Volume g, const float2* __restrict__ data, const fl
                     const double y0v = x00 + (x10 - x00) * fy, y1v = x01 + (x11 - x01) * fy;
                     return y0v + (y1v - y0v) * fz;
                 };
-                sr += tri(dr);
-                si += neg ? -tri(di) : tri(di);
+                double cr = tri(dr), ci = neg ? -tri(di) : tri(di);
+                if (zsh && zsh[s] != 0.) {
+                    double sn, cs;
+                    sincos(2. * PI_R * (z * zsh[s]), &sn, &cs);
+                    const double ac = cs * cr, bd = sn * ci, abcd = (cs + sn) * (cr + ci);
+                    cr = ac - bd;
+                    ci = abcd - ac - bd;
+                }
+                sr += cr;
+                si += ci;
                 sw += tri(dw);
             }
         }
@@ -775,6 +787,38 @@ std::vector<std::array<double, 9>> point_group(const char* name)
 
 using namespace t2b;
 
+namespace t2b {
+namespace {
+// the grid of a class summed over operators (and, for helical symmetry, z phase shifts) in place:
+// the sums go to scratch arrays, copied back once the kernel has read the whole grid.  C1 (no
+// operator) and 2D grids are left as they are, as the reference leaves them.
+void symmetrise_grid(t2b_ctx* c, int iclass, const std::vector<std::array<double, 9>>& ops,
+                     const std::vector<double>& zsh)
+{
+    const Volume& v = grid_volume(c, iclass);
+    if (ops.empty() || v.ref_dim != 3) return;
+    const int rp = v.r_max * v.pad;
+    const size_t nv = v.nvox();
+    cudaStream_t st = c->stream;
+    DevBuf<float2> sd(nv);
+    DevBuf<float> sw(nv);
+    DevBuf<double> R(9 * ops.size() + zsh.size());
+    std::vector<double> hr(9 * ops.size());
+    for (size_t i = 0; i < ops.size(); ++i)
+        for (int e = 0; e < 9; ++e) hr[9 * i + e] = ops[i][e];
+    hr.insert(hr.end(), zsh.begin(), zsh.end());
+    T2B_CUDA(cudaMemcpyAsync(R.p, hr.data(), hr.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_symmetrise<<<grid_of((long long)nv), RC_THREADS, 0, st>>>(v, c->gdata[iclass], c->gweight[iclass], sd.p, sw.p, R.p,
+                                                               zsh.empty() ? nullptr : R.p + 9 * ops.size(),
+                                                               (int)ops.size(), rp * rp);
+    T2B_CUDA(cudaGetLastError());
+    T2B_CUDA(cudaMemcpyAsync(c->gdata[iclass], sd.p, nv * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+    T2B_CUDA(cudaMemcpyAsync(c->gweight[iclass], sw.p, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    T2B_CUDA(cudaStreamSynchronize(st));
+}
+}  // namespace
+}  // namespace t2b
+
 extern "C" {
 
 int t2b_reconstruct(t2b_ctx* c, int iclass, const t2b_recon_config* cf, double* vol_out)
@@ -887,24 +931,34 @@ int t2b_backprojector_apply_symmetry(t2b_ctx* c, int iclass, const char* group)
         const auto ops = point_group(group);
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceGuard dg(c->device);
+        symmetrise_grid(c, iclass, ops, {});
+    });
+}
+
+int t2b_backprojector_apply_helical(t2b_ctx* c, int iclass, int nr_asu, double twist, double rise, int ori_size)
+{
+    return guarded([&] {
+        T2B_REQUIRE(c, T2B_ERR_ARG, "null argument");
+        T2B_REQUIRE(nr_asu < 2 || ori_size > 0, T2B_ERR_ARG, "ori_size must be positive");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard dg(c->device);
         const Volume& v = grid_volume(c, iclass);
-        if (ops.empty() || v.ref_dim != 3) return;   // C1, and 2D grids: nothing to do (as the reference)
-        const int rp = v.r_max * v.pad;
-        const size_t nv = v.nvox();
-        cudaStream_t st = c->stream;
-        DevBuf<float2> sd(nv);
-        DevBuf<float> sw(nv);
-        DevBuf<double> R(9 * ops.size());
-        std::vector<double> hr(9 * ops.size());
-        for (size_t i = 0; i < ops.size(); ++i)
-            for (int e = 0; e < 9; ++e) hr[9 * i + e] = ops[i][e];
-        T2B_CUDA(cudaMemcpyAsync(R.p, hr.data(), hr.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-        k_symmetrise<<<grid_of((long long)nv), RC_THREADS, 0, st>>>(v, c->gdata[iclass], c->gweight[iclass], sd.p, sw.p,
-                                                                   R.p, (int)ops.size(), rp * rp);
-        T2B_CUDA(cudaGetLastError());
-        T2B_CUDA(cudaMemcpyAsync(c->gdata[iclass], sd.p, nv * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-        T2B_CUDA(cudaMemcpyAsync(c->gweight[iclass], sw.p, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
-        T2B_CUDA(cudaStreamSynchronize(st));
+        std::vector<std::array<double, 9>> ops;
+        std::vector<double> zsh;
+        // the asymmetric units hh = -n/2 .. n/2 - 1 (+1 for odd n) other than 0: a rotation by
+        // -hh twist degrees about z (rotation3DMatrix(ang, 'Z'), entries below 1e-6 zeroed) and
+        // a shift of hh rise pixels along z
+        const int h_min = -nr_asu / 2, h_max = -h_min + nr_asu % 2;
+        for (int hh = h_min; nr_asu >= 2 && hh < h_max; ++hh) {
+            if (hh == 0) continue;
+            const double ang = (hh * -twist) * PI_R / 180.;
+            std::array<double, 9> r = {std::cos(ang), -std::sin(ang), 0., std::sin(ang), std::cos(ang), 0., 0., 0., 1.};
+            for (double& e : r)
+                if (std::fabs(e) < 1e-6) e = 0.;
+            ops.push_back(r);
+            zsh.push_back(std::fabs(rise) > 0. ? (hh * rise) / (-ori_size * (double)v.pad) : 0.);
+        }
+        symmetrise_grid(c, iclass, ops, zsh);
     });
 }
 

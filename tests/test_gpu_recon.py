@@ -1,5 +1,6 @@
 """M-step reconstruction on the GPU (t2b_reconstruct, t2b_fsc_halves,
-t2b_update_ssnr, t2b_backprojector_enforce_hermitian, t2b_backprojector_apply_symmetry) against the FP64 oracle (oracle/recon_oracle.py), on the
+t2b_update_ssnr, t2b_backprojector_enforce_hermitian, t2b_backprojector_apply_symmetry,
+t2b_backprojector_apply_helical) against the FP64 oracle (oracle/recon_oracle.py), on the
 backprojection grids the E-step filled.
 
 Tolerances: the map within 2e-5 of its largest value (the inverse 3D FFT is
@@ -116,12 +117,38 @@ def test_point_group_symmetry_matches_oracle(group):
     _map_close(got, ref)
 
 
+@pytest.mark.parametrize("nr_asu,twist,rise,group", [(5, -35.3, 4.7, "C1"), (2, 12.0, 0.0, "C1"), (3, 61.2, 2.9, "C3")])
+def test_helical_symmetry_matches_oracle(nr_asu, twist, rise, group):
+    """t2b_backprojector_apply_helical, then the point group, as MlOptimiser::maximization runs
+    them on the Hermitian-symmetrised grid, against the oracle: 1e-6 relative per element (FP64
+    coordinates, phases and sums, one FP32 rounding per step)."""
+    pb = problems.build("refine_o2", n_particles=16, seed=43)
+    P = pb["parts"]
+    es = pb["product"]()
+    es.expectation(P["fimg"], P["ctf"], P["minv"], P["scalars"])
+    es.enforce_hermitian_symmetry(0)
+    data, w = es.get_backprojector(0)
+    es.apply_helical_symmetry(0, nr_asu, twist, rise, pb["N"])
+    hd, hw = es.get_backprojector(0)
+    mats, zsh = ro.helical_operators(nr_asu, twist, rise, pb["N"], 2)
+    rd, rw = ro.apply_point_group_symmetry(data, w, mats, pb["r"], 2, zshift=zsh)
+    for g, r in ((hd, rd), (hw, rw)):
+        assert np.max(np.abs(g - r) / (np.abs(r) + 1e-9 * np.max(np.abs(r)))) <= 1e-6
+    es.apply_point_group_symmetry(0, group)
+    gd, gw = es.get_backprojector(0)
+    es.close()
+    rd2, rw2 = ro.apply_point_group_symmetry(hd, hw, ro.point_group(group), pb["r"], 2)
+    for g, r in ((gd, rd2), (gw, rw2)):
+        assert np.max(np.abs(g - r) / (np.abs(r) + 1e-9 * np.max(np.abs(r)))) <= 1e-6
+
+
 def test_point_group_symmetry_identity_cases():
     """C1 leaves a 3D grid as it is, any group a 2D grid (the reference symmetrises 3D only);
     an unknown group (I5, not implemented by the reference either) is refused and the grid is
-    left as it was."""
+    left as it was; helical symmetry with one unit, or on a 2D grid, changes nothing."""
     t2b = problems.load_package()
-    for name, group in (("refine_o2", "C1"), ("class2d", "O"), ("refine_o2", "I5")):
+    for name, group in (("refine_o2", "C1"), ("class2d", "O"), ("refine_o2", "I5"), ("refine_o2", "helix1"),
+                        ("class2d", "helix5")):
         pb = problems.build(name, n_particles=8, seed=41)
         P = pb["parts"]
         es = pb["product"]()
@@ -130,6 +157,8 @@ def test_point_group_symmetry_identity_cases():
         if group == "I5":
             with pytest.raises(t2b.T2BError):
                 es.apply_point_group_symmetry(0, group)
+        elif group.startswith("helix"):   # one unit, or a 2D grid: unchanged
+            es.apply_helical_symmetry(0, int(group[5:]), 20.0, 3.0, pb["N"])
         else:
             es.apply_point_group_symmetry(0, group)
         gd, gw = es.get_backprojector(0)

@@ -176,3 +176,57 @@ def test_symmetrisation_of_an_invariant_weight():
     inside = r2 <= rp * rp
     assert np.allclose(sw[inside], 24 * w[inside], rtol=1e-9)
     assert np.array_equal(sw[~inside], w[~inside])
+
+
+def test_helical_operators_follow_the_unit_range():
+    """n units hh = -n/2 .. n/2 - 1 (+1 for odd n), hh = 0 left out; rotations by -hh twist."""
+    for n, hs in ((2, [-1]), (3, [-1, 1]), (4, [-2, -1, 1]), (5, [-2, -1, 1, 2])):
+        mats, zsh = ro.helical_operators(n, 30.0, 2.5, 64, 2)
+        assert len(mats) == len(hs)
+        for m, z, hh in zip(mats, zsh, hs):
+            t = np.radians(-hh * 30.0)
+            assert np.allclose(m, [[np.cos(t), -np.sin(t), 0], [np.sin(t), np.cos(t), 0], [0, 0, 1]], atol=1e-6)
+            assert z == hh * 2.5 / (-64 * 2.0)
+    assert len(ro.helical_operators(1, 30.0, 2.5, 64, 2)[0]) == 0
+    assert np.all(ro.helical_operators(3, 30.0, 0.0, 64, 2)[1] == 0)
+
+
+def test_helical_rise_alone_is_a_phase_sum():
+    """Twist 0: every unit reads the voxel itself, so the data become data x sum_hh
+    e^{2 pi i z hh rise / (-ori pad)} (hh = 0 included) and the weights n x weight."""
+    rp, n, rise, ori, pad = 5, 4, 3.7, 10, 1
+    d, w = _grid(rp, 5)
+    mats, zsh = ro.helical_operators(n, 0.0, rise, ori, pad)
+    sd, sw = ro.apply_point_group_symmetry(d, w, mats, rp, pad, zshift=zsh)
+    c = rp + 1
+    z, y, x = np.meshgrid(np.arange(-c, c + 1), np.arange(-c, c + 1), np.arange(0, c + 1), indexing="ij")
+    inside = x * x + y * y + z * z <= rp * rp
+    hh = np.array([-2, -1, 0, 1])
+    phase = np.exp(2j * np.pi * z[..., None] * hh * rise / (-ori * pad)).sum(-1)
+    assert np.allclose(sd[inside], d[inside] * phase[inside], rtol=1e-12, atol=1e-12)
+    assert np.allclose(sw[inside], n * w[inside], rtol=1e-12)
+    assert np.array_equal(sd[~inside], d[~inside])
+
+
+def test_helical_quarter_twist_matches_a_direct_loop():
+    """Twist 90 degrees, three units: integer rotations about z, so the reads are grid values."""
+    rp, rise, ori, pad = 5, 1.5, 12, 1
+    d, w = _grid(rp, 7)
+    mats, zsh = ro.helical_operators(3, 90.0, rise, ori, pad)
+    sd, sw = ro.apply_point_group_symmetry(d, w, mats, rp, pad, zshift=zsh)
+    c = rp + 1
+    for z, y, x in itertools.product(range(-c, c + 1), range(-c, c + 1), range(0, c + 1)):
+        ed, ew = d[z + c, y + c, x], w[z + c, y + c, x]
+        if x * x + y * y + z * z <= rp * rp:
+            for hh in (-1, 1):
+                t = np.radians(-hh * 90.0)
+                p = np.rint(np.array([[np.cos(t), -np.sin(t), 0], [np.sin(t), np.cos(t), 0], [0, 0, 1]])
+                            @ np.array([x, y, z], float)).astype(int)
+                neg = p[0] < 0
+                if neg:
+                    p = -p
+                v = d[p[2] + c, p[1] + c, p[0]]
+                v = np.conj(v) if neg else v
+                ed += v * np.exp(2j * np.pi * z * hh * rise / (-ori * pad))
+                ew += w[p[2] + c, p[1] + c, p[0]]
+        assert abs(sd[z + c, y + c, x] - ed) <= 1e-12 and abs(sw[z + c, y + c, x] - ew) <= 1e-12
