@@ -130,6 +130,7 @@ void t2b_destroy(t2b_ctx* c)
         for (auto p : c->mdl) cudaFree(p);
         for (auto p : c->gdata) cudaFree(p);
         for (auto p : c->gweight) cudaFree(p);
+        cudaFree(c->sym_scratch);
         for (auto& ev : c->ev) cudaEventDestroy(ev);
         for (auto& ev : c->handoff) cudaEventDestroy(ev);
         for (auto& s : c->in)

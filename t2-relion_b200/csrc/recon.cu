@@ -790,8 +790,9 @@ using namespace t2b;
 namespace t2b {
 namespace {
 // the grid of a class summed over operators (and, for helical symmetry, z phase shifts) in place:
-// the sums go to scratch arrays, copied back once the kernel has read the whole grid.  C1 (no
-// operator) and 2D grids are left as they are, as the reference leaves them.
+// the sums go to the context's scratch (kept between calls: an M-step symmetrises every class of
+// every iteration), copied back once the kernel has read the whole grid.  C1 (no operator) and
+// 2D grids are left as they are, as the reference leaves them.
 void symmetrise_grid(t2b_ctx* c, int iclass, const std::vector<std::array<double, 9>>& ops,
                      const std::vector<double>& zsh)
 {
@@ -800,21 +801,37 @@ void symmetrise_grid(t2b_ctx* c, int iclass, const std::vector<std::array<double
     const int rp = v.r_max * v.pad;
     const size_t nv = v.nvox();
     cudaStream_t st = c->stream;
-    DevBuf<float2> sd(nv);
-    DevBuf<float> sw(nv);
-    DevBuf<double> R(9 * ops.size() + zsh.size());
     std::vector<double> hr(9 * ops.size());
     for (size_t i = 0; i < ops.size(); ++i)
         for (int e = 0; e < 9; ++e) hr[9 * i + e] = ops[i][e];
     hr.insert(hr.end(), zsh.begin(), zsh.end());
-    T2B_CUDA(cudaMemcpyAsync(R.p, hr.data(), hr.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    k_symmetrise<<<grid_of((long long)nv), RC_THREADS, 0, st>>>(v, c->gdata[iclass], c->gweight[iclass], sd.p, sw.p, R.p,
-                                                               zsh.empty() ? nullptr : R.p + 9 * ops.size(),
+    // [operators | sums of the data (float2) | sums of the weights], each part 256-byte aligned
+    const size_t r_bytes = (hr.size() * sizeof(double) + 255) & ~size_t(255);
+    const size_t d_bytes = (nv * sizeof(float2) + 255) & ~size_t(255);
+    const size_t need = r_bytes + d_bytes + nv * sizeof(float);
+    if (c->sym_bytes < need) {
+        T2B_CUDA(cudaStreamSynchronize(st));
+        cudaFree(c->sym_scratch);
+        c->sym_scratch = nullptr;
+        c->sym_bytes = 0;
+        if (cudaMalloc(&c->sym_scratch, need) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{T2B_ERR_NOMEM, "symmetrisation scratch of " + std::to_string(need) + " bytes"};
+        }
+        c->sym_bytes = need;
+    }
+    char* base = static_cast<char*>(c->sym_scratch);
+    double* R = reinterpret_cast<double*>(base);
+    float2* sd = reinterpret_cast<float2*>(base + r_bytes);
+    float* sw = reinterpret_cast<float*>(base + r_bytes + d_bytes);
+    T2B_CUDA(cudaMemcpyAsync(R, hr.data(), hr.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_symmetrise<<<grid_of((long long)nv), RC_THREADS, 0, st>>>(v, c->gdata[iclass], c->gweight[iclass], sd, sw, R,
+                                                               zsh.empty() ? nullptr : R + 9 * ops.size(),
                                                                (int)ops.size(), rp * rp);
     T2B_CUDA(cudaGetLastError());
-    T2B_CUDA(cudaMemcpyAsync(c->gdata[iclass], sd.p, nv * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-    T2B_CUDA(cudaMemcpyAsync(c->gweight[iclass], sw.p, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    T2B_CUDA(cudaStreamSynchronize(st));
+    T2B_CUDA(cudaMemcpyAsync(c->gdata[iclass], sd, nv * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+    T2B_CUDA(cudaMemcpyAsync(c->gweight[iclass], sw, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    T2B_CUDA(cudaStreamSynchronize(st));   // the host table hr is read by the copy above
 }
 }  // namespace
 }  // namespace t2b

@@ -303,6 +303,8 @@ struct t2b_ctx {
     std::vector<t2b::Volume> gvol;            // per class BP grid geometry
     std::vector<float2*> gdata;               // per class grid data
     std::vector<float*> gweight;              // per class grid weight
+    void* sym_scratch = nullptr;              // symmetrisation sums of one grid (grown on demand)
+    size_t sym_bytes = 0;
     bool configured = false;
     t2b_config cfg{};
     t2b::Tables tb{};
