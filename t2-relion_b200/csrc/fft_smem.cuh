@@ -1,8 +1,9 @@
 // Batched 1D FFTs in shared memory (libt2b): mixed-radix Stockham autosort
 // over nfft sequences of length N, ping-ponging between two shared buffers;
-// radix-4, 2, 3, 5 stages with a runtime plan, any other prime factor p by a
-// direct length-p DFT per output (N p work for that stage: the odd padded boxes
-// of the reconstruction's gridding iterations, e.g. 259 = 7 x 37), or, for a
+// radix-4, 2, 3, 5, 7 stages with a runtime plan, any other prime factor p by a
+// direct length-p DFT (the odd padded boxes of the reconstruction's gridding
+// iterations, e.g. 259 = 7 x 37): as the first stage in conjugate output pairs,
+// later ones one output per thread (N p work for that stage), or, for a
 // size known at compile time, radix-16 and radix-8 register butterflies first
 // and constant index arithmetic.  Twiddles tw[t] = e^{-2 pi i t / N} (a table
 // the caller stages in shared memory); the inverse transform uses their
@@ -21,8 +22,9 @@ struct FftPlan {
     int rad[FFT_MAX_STAGES] = {};
 };
 
-// runtime plan: radices 4, then 2, 3, 5; with any_prime, then every remaining prime factor
-// (generic stages)
+// runtime plan: radices 4, then 2, 3, 5; with any_prime, the prime factors >= 7 come first,
+// largest first, so that the largest one runs as the first stage (no input twiddles there:
+// fft_stage_prime_first), the others by the radix-7 or the generic stage
 inline FftPlan fft_plan(int N, bool any_prime = false)
 {
     FftPlan pl;
@@ -34,12 +36,21 @@ inline FftPlan fft_plan(int N, bool any_prime = false)
             n /= r;
         }
     };
+    if (any_prime) {
+        int m = N, primes[FFT_MAX_STAGES], np = 0;
+        for (int p : {2, 3, 5})
+            while (m % p == 0) m /= p;
+        for (int p = 7; m > 1 && np < FFT_MAX_STAGES; p += 2)
+            while (m % p == 0 && np < FFT_MAX_STAGES) {
+                primes[np++] = p;
+                m /= p;
+            }
+        for (int i = np - 1; i >= 0; --i) take(primes[i]);
+    }
     take(4);
     take(2);
     take(3);
     take(5);
-    if (any_prime)
-        for (int p = 7; p <= n; p += 2) take(p);
     T2B_REQUIRE(n == 1, T2B_ERR_UNSUPPORTED,
                 any_prime ? "transform size has too many prime factors" : "transform sizes must be products of 2, 3 and 5");
     return pl;
@@ -172,8 +183,50 @@ __device__ __forceinline__ void fft_stage_gen(const float2* a, float2* b, int nf
     }
 }
 
-// All stages; returns the buffer holding the transform (natural order).
+// The first stage (Ns = 1: no input twiddles) for an odd prime radix R >= 7: one thread per
+// (sequence, group m, pair u), X[u] and X[R - u] from the same sums over r = 1 .. (R - 1) / 2 of
+// S_r = x_r + x_{R-r} and D_r = x_r - x_{R-r}: X[u] = x_0 + A -+ i B, X[R - u] = x_0 + A +- i B
+// with A = sum_r cos(2 pi u r / R) S_r, B = sum_r sin(2 pi u r / R) D_r (upper signs forward);
+// u = 0 gives X[0] = x_0 + sum_r S_r.  About a quarter of the generic stage's loads and products.
 template <bool INV>
+__device__ __forceinline__ void fft_stage_prime_first(const float2* a, float2* b, int nfft, int N, int R,
+                                                      const float2* tw)
+{
+    const int NR = N / R, h = (R - 1) / 2, per = NR * (h + 1);
+    for (int e = threadIdx.x; e < nfft * per; e += blockDim.x) {
+        const int f = e / per, rem = e - f * per;
+        const int m = rem / (h + 1), u = rem - m * (h + 1);
+        const float2* in = a + f * N + m;
+        float2* out = b + f * N + m * R;
+        const float2 x0 = in[0];
+        float2 A = make_float2(0.f, 0.f), Bs = make_float2(0.f, 0.f);
+        int ur = 0;   // (u r) mod R
+        for (int r = 1; r <= h; ++r) {
+            ur += u;
+            if (ur >= R) ur -= R;
+            const float2 xr = in[r * NR], xm = in[(R - r) * NR];
+            const float2 S = cadd(xr, xm), D = csub(xr, xm);
+            const float2 w = tw[ur * NR];   // (cos, -sin) of 2 pi u r / R
+            A.x = fmaf(w.x, S.x, A.x);
+            A.y = fmaf(w.x, S.y, A.y);
+            Bs.x = fmaf(-w.y, D.x, Bs.x);
+            Bs.y = fmaf(-w.y, D.y, Bs.y);
+        }
+        const float2 c0 = cadd(x0, A);
+        if (u == 0) {
+            out[0] = c0;
+        } else {
+            const float2 mib = make_float2(Bs.y, -Bs.x);   // -i B
+            out[u] = INV ? csub(c0, mib) : cadd(c0, mib);
+            out[R - u] = INV ? cadd(c0, mib) : csub(c0, mib);
+        }
+    }
+}
+
+// All stages; returns the buffer holding the transform (natural order).  PRIMES (the plans of
+// fft_plan(N, true)): the radix-7 register stage and the first-stage pairs for larger primes,
+// compiled only into the kernels that take such plans (they cost the others registers).
+template <bool INV, bool PRIMES = false>
 __device__ float2* fft_smem(float2* a, float2* b, int nfft, const FftPlan& pl, const float2* tw)
 {
     int Ns = 1;
@@ -184,7 +237,15 @@ __device__ float2* fft_smem(float2* a, float2* b, int nfft, const FftPlan& pl, c
         case 2: fft_stage<2, INV>(a, b, nfft, pl.n, Ns, tw); break;
         case 3: fft_stage<3, INV>(a, b, nfft, pl.n, Ns, tw); break;
         case 5: fft_stage<5, INV>(a, b, nfft, pl.n, Ns, tw); break;
-        default: fft_stage_gen<INV>(a, b, nfft, pl.n, Ns, R, tw); break;
+        default:
+            if constexpr (PRIMES) {
+                if (R == 7) fft_stage<7, INV>(a, b, nfft, pl.n, Ns, tw);
+                else if (Ns == 1) fft_stage_prime_first<INV>(a, b, nfft, pl.n, R, tw);
+                else fft_stage_gen<INV>(a, b, nfft, pl.n, Ns, R, tw);
+            } else {
+                fft_stage_gen<INV>(a, b, nfft, pl.n, Ns, R, tw);
+            }
+            break;
         }
         __syncthreads();
         float2* t = a;

@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(RC_THREADS) k_gd_fft(float2* __restrict__ V, i
         A[c * N + q] = ok(c) ? V[idx(q, c)] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    const float2* r = fft_smem<INV>(A, B, GD_CX, plan, s_tw);
+    const float2* r = fft_smem<INV, true>(A, B, GD_CX, plan, s_tw);
     for (int e = threadIdx.x; e < GD_CX * N; e += blockDim.x) {
         const int c = axis == 0 ? e / N : e % GD_CX, q = axis == 0 ? e % N : e / GD_CX;
         if (ok(c)) V[idx(q, c)] = r[c * N + q];
