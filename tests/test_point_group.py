@@ -230,3 +230,21 @@ def test_helical_quarter_twist_matches_a_direct_loop():
                 ed += v * np.exp(2j * np.pi * z * hh * rise / (-ori * pad))
                 ew += w[p[2] + c, p[1] + c, p[0]]
         assert abs(sd[z + c, y + c, x] - ed) <= 1e-12 and abs(sw[z + c, y + c, x] - ew) <= 1e-12
+
+
+def test_point_group_abi_contract(t2b):
+    """t2b_point_group fills at most cap matrices and always reports the count; a null count is
+    refused.  The grid entry points refuse a null context before touching a device."""
+    import ctypes
+    lib = t2b.lib
+    n = ctypes.c_int(-1)
+    assert lib.t2b_point_group(b"O", None, 0, ctypes.byref(n)) == t2b.T2B_OK and n.value == 23
+    buf = np.full((30, 3, 3), 7.0)
+    assert lib.t2b_point_group(b"O", buf.ctypes.data_as(ctypes.c_void_p), 5, ctypes.byref(n)) == t2b.T2B_OK
+    assert n.value == 23
+    assert np.array_equal(buf[:5], t2b.point_group("O")[:5]) and np.all(buf[5:] == 7.0)
+    assert lib.t2b_point_group(b"O", None, 0, None) == t2b.T2B_ERR_ARG
+    assert lib.t2b_point_group(b"O", None, 4, ctypes.byref(n)) == t2b.T2B_ERR_ARG
+    assert lib.t2b_point_group(None, None, 0, ctypes.byref(n)) == t2b.T2B_OK and n.value == 0   # C1
+    assert lib.t2b_backprojector_apply_symmetry(None, 0, b"C2") == t2b.T2B_ERR_ARG
+    assert lib.t2b_backprojector_apply_helical(None, 0, 3, 10.0, 2.0, 64) == t2b.T2B_ERR_ARG
