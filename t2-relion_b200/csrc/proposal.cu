@@ -147,18 +147,23 @@ __global__ void __launch_bounds__(256) k_conv_fwd(const float* __restrict__ img,
                                                   int n, float* __restrict__ a1_out, float* __restrict__ x0,
                                                   bf16* __restrict__ x0b)
 {
+    static_assert(NET_C2 == 32 && NET_H0 == NET_C2 * 64, "conv2 thread layout: 4 groups of 8 channels x 8 x 8");
     __shared__ float im[18][18];
     __shared__ float a1[NET_C1][18][18];
     __shared__ float w1[NET_C1 * 9 + NET_C1];
-    __shared__ float w2[NET_C2 * NET_C1 * 9 + NET_C2];
+    __shared__ __align__(16) float w2t[NET_C1 * 9][NET_C2];   // conv2 weights as [tap][output channel]
+    __shared__ float b2[NET_C2];
     const int b = blockIdx.x;
     if (b >= n) return;
     for (int i = threadIdx.x; i < 18 * 18; i += blockDim.x) (&im[0][0])[i] = 0.f;
     for (int i = threadIdx.x; i < NET_C1 * 18 * 18; i += blockDim.x) (&a1[0][0][0])[i] = 0.f;
     for (int i = threadIdx.x; i < NET_C1 * 9; i += blockDim.x) w1[i] = ldw(th, L.wc1 + i);
     for (int i = threadIdx.x; i < NET_C1; i += blockDim.x) w1[NET_C1 * 9 + i] = ldw(th, L.bc1 + i);
-    for (int i = threadIdx.x; i < NET_C2 * NET_C1 * 9; i += blockDim.x) w2[i] = ldw(th, L.wc2 + i);
-    for (int i = threadIdx.x; i < NET_C2; i += blockDim.x) w2[NET_C2 * NET_C1 * 9 + i] = ldw(th, L.bc2 + i);
+    for (int i = threadIdx.x; i < NET_C2 * NET_C1 * 9; i += blockDim.x) {
+        const int c2 = i / (NET_C1 * 9), tap = i - c2 * (NET_C1 * 9);   // global layout [c2][c1][dy][dx]
+        w2t[tap][c2] = ldw(th, L.wc2 + i);
+    }
+    for (int i = threadIdx.x; i < NET_C2; i += blockDim.x) b2[i] = ldw(th, L.bc2 + i);
     __syncthreads();
     {
         const int y = threadIdx.x >> 4, x = threadIdx.x & 15;
@@ -179,18 +184,38 @@ __global__ void __launch_bounds__(256) k_conv_fwd(const float* __restrict__ img,
         }
     }
     __syncthreads();
-    for (int o = threadIdx.x; o < NET_H0; o += blockDim.x) {
-        const int c2 = o >> 6, Y = (o >> 3) & 7, X = o & 7;
-        float acc = w2[NET_C2 * NET_C1 * 9 + c2];
-        const float* wc = w2 + c2 * NET_C1 * 9;
+    // conv2: each thread one output position (Y, X) and eight output channels g*8 .. g*8+7, so
+    // one read of a1 serves eight products and the weights of a tap come as two broadcast
+    // 16-byte reads; every output sums its bias and taps in the order (c1, dy, dx) as before
+    for (int e = threadIdx.x; e < NET_H0 / 8; e += blockDim.x) {
+        const int pos = e & 63, g = e >> 6, Y = pos >> 3, X = pos & 7;
+        float acc[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[j] = b2[g * 8 + j];
         for (int c1 = 0; c1 < NET_C1; c1++)
 #pragma unroll
             for (int dy = 0; dy < 3; dy++)
 #pragma unroll
-                for (int dx = 0; dx < 3; dx++) acc += wc[c1 * 9 + dy * 3 + dx] * a1[c1][2 * Y + dy][2 * X + dx];
-        acc = fmaxf(acc, 0.f);
-        if (x0) x0[(size_t)b * NET_H0 + o] = acc;
-        if (x0b) x0b[(size_t)b * NET_H0 + o] = __float2bfloat16_rn(acc);
+                for (int dx = 0; dx < 3; dx++) {
+                    const float a = a1[c1][2 * Y + dy][2 * X + dx];
+                    const float4 wa = *reinterpret_cast<const float4*>(&w2t[c1 * 9 + dy * 3 + dx][g * 8]);
+                    const float4 wb = *reinterpret_cast<const float4*>(&w2t[c1 * 9 + dy * 3 + dx][g * 8 + 4]);
+                    acc[0] += wa.x * a;
+                    acc[1] += wa.y * a;
+                    acc[2] += wa.z * a;
+                    acc[3] += wa.w * a;
+                    acc[4] += wb.x * a;
+                    acc[5] += wb.y * a;
+                    acc[6] += wb.z * a;
+                    acc[7] += wb.w * a;
+                }
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int o = (g * 8 + j) * 64 + pos;   // output layout [c2][Y][X]
+            const float v = fmaxf(acc[j], 0.f);
+            if (x0) x0[(size_t)b * NET_H0 + o] = v;
+            if (x0b) x0b[(size_t)b * NET_H0 + o] = __float2bfloat16_rn(v);
+        }
     }
 }
 
