@@ -249,8 +249,25 @@ __global__ void __launch_bounds__(1024) k_topk(const float* __restrict__ logits,
     __shared__ unsigned s_prefix, s_want, s_n;
     __shared__ unsigned long long cand[NET_TOPK_CAND];
     const int b = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < KO; i += blockDim.x)
-        keys[i] = skip[i] ? 0u : f2key(logits[(size_t)b * KO + i] + __bfloat162float(bias[i]));
+    {
+        // eight elements per thread in flight: all their loads issued before any key is formed
+        const float* lg = logits + (size_t)b * KO;
+        const int bd = blockDim.x;
+        int i = threadIdx.x;
+        for (; i + 7 * bd < KO; i += 8 * bd) {
+            float v[8], bb[8];
+            unsigned char sk[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                v[u] = lg[i + u * bd];
+                bb[u] = __bfloat162float(bias[i + u * bd]);
+                sk[u] = skip[i + u * bd];
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) keys[i + u * bd] = sk[u] ? 0u : f2key(v[u] + bb[u]);
+        }
+        for (; i < KO; i += bd) keys[i] = skip[i] ? 0u : f2key(lg[i] + __bfloat162float(bias[i]));
+    }
     if (threadIdx.x == 0) { s_prefix = 0; s_want = (unsigned)k; s_n = 0; }
     __syncthreads();
     unsigned mask = 0;
