@@ -226,8 +226,18 @@ __global__ void k_bias_act(const float* __restrict__ y, const bf16* __restrict__
 {
     const size_t total = (size_t)rows * cols;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        // the slices' loads four at a time in flight, summed in slice order
         float acc = y[i];
-        for (int s = 1; s < slices; ++s) acc += y[(size_t)s * total + i];
+        int s = 1;
+        for (; s + 3 < slices; s += 4) {
+            const float a0 = y[(size_t)s * total + i], a1 = y[(size_t)(s + 1) * total + i];
+            const float a2 = y[(size_t)(s + 2) * total + i], a3 = y[(size_t)(s + 3) * total + i];
+            acc += a0;
+            acc += a1;
+            acc += a2;
+            acc += a3;
+        }
+        for (; s < slices; ++s) acc += y[(size_t)s * total + i];
         float v = acc + __bfloat162float(bias[i % cols]);
         if (relu) v = fmaxf(v, 0.f);
         if (outf) outf[i] = v;
@@ -419,26 +429,48 @@ __global__ void k_ring_table(const float2* __restrict__ proj, int P, const int* 
 
 // per batch: the shifted ring images cvec_b ab_t as split-BF16 rows b*T + t (the
 // contraction's B operand), and w2 at the ring pixels
-__global__ void __launch_bounds__(128) k_ring_images(Tables tb, Work w, const int* __restrict__ ring, int nring, int kr,
+// One CTA per particle: its ring pixels' indices and image values staged once in shared memory,
+// then every (shift t, ring pixel q) of its T rows, four of them per thread in flight.
+constexpr int RING_MAX = 512;   // kr / 2 (ring pixels + padding) at most
+__global__ void __launch_bounds__(256) k_ring_images(Tables tb, Work w, const int* __restrict__ ring, int nring, int kr,
                                                      bf16* __restrict__ sh, bf16* __restrict__ sl, float* __restrict__ w2r)
 {
-    const int row = blockIdx.x, P = tb.P;
-    const int b = row / tb.T, t = row - b * tb.T;
-    if (b >= w.n) return;
-    for (int q = threadIdx.x; q < kr / 2; q += blockDim.x) {
-        float2 v = make_float2(0.f, 0.f);
-        if (q < nring) {
-            const int n = ring[q];
-            const float2 c = w.cvec[(size_t)b * P + n];
-            const float2 a = tb.ab_c[(size_t)t * P + n];
-            v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
-            if (t == 0) w2r[(size_t)b * nring + q] = w.w2[(size_t)b * P + n];
-        }
-        const bf16 hx = __float2bfloat16_rn(v.x), hy = __float2bfloat16_rn(v.y);
-        reinterpret_cast<__nv_bfloat162*>(sh + (size_t)row * kr)[q] = __halves2bfloat162(hx, hy);
-        reinterpret_cast<__nv_bfloat162*>(sl + (size_t)row * kr)[q] =
-            __halves2bfloat162(__float2bfloat16_rn(v.x - __bfloat162float(hx)), __float2bfloat16_rn(v.y - __bfloat162float(hy)));
+    __shared__ int s_n[RING_MAX];
+    __shared__ float2 s_c[RING_MAX];
+    const int b = blockIdx.x, P = tb.P, T = tb.T, kh = kr / 2;
+    if (b >= w.n || kh > RING_MAX) return;
+    for (int q = threadIdx.x; q < kh; q += blockDim.x) {
+        const int n = q < nring ? ring[q] : -1;
+        s_n[q] = n;
+        s_c[q] = n >= 0 ? w.cvec[(size_t)b * P + n] : make_float2(0.f, 0.f);
+        if (n >= 0) w2r[(size_t)b * nring + q] = w.w2[(size_t)b * P + n];
     }
+    __syncthreads();
+    const int total = T * kh;
+    const auto emit = [&](int e, float2 a) {
+        const int t = e / kh, q = e - t * kh;
+        const float2 c = s_c[q];
+        const float2 v = make_float2(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+        const size_t row = (size_t)b * T + t;
+        const bf16 hx = __float2bfloat16_rn(v.x), hy = __float2bfloat16_rn(v.y);
+        reinterpret_cast<__nv_bfloat162*>(sh + row * kr)[q] = __halves2bfloat162(hx, hy);
+        reinterpret_cast<__nv_bfloat162*>(sl + row * kr)[q] =
+            __halves2bfloat162(__float2bfloat16_rn(v.x - __bfloat162float(hx)), __float2bfloat16_rn(v.y - __bfloat162float(hy)));
+    };
+    const auto phase = [&](int e) -> float2 {   // ab_t at ring pixel q (zero for the padding)
+        const int t = e / kh, n = s_n[e - t * kh];
+        return n >= 0 ? tb.ab_c[(size_t)t * P + n] : make_float2(0.f, 0.f);
+    };
+    const int bd = blockDim.x;
+    int e = threadIdx.x;
+    for (; e + 3 * bd < total; e += 4 * bd) {
+        const float2 a0 = phase(e), a1 = phase(e + bd), a2 = phase(e + 2 * bd), a3 = phase(e + 3 * bd);
+        emit(e, a0);
+        emit(e + bd, a1);
+        emit(e + 2 * bd, a2);
+        emit(e + 3 * bd, a3);
+    }
+    for (; e < total; e += bd) emit(e, phase(e));
 }
 
 // candidate rows (b*K1 + j) of the A operand and their ring norms; one warp per candidate
@@ -1463,6 +1495,7 @@ void net_setup(t2b_ctx* c, int na_max)
     N.score1 = (float*)net_dalloc(W, (size_t)B * NET_TOPK_CAND * sizeof(float));
     // low-resolution rescoring operands (K = 2 x ring pixels, padded to a multiple of 64)
     N.kr = (2 * N.nring + 63) / 64 * 64;
+    T2B_REQUIRE(N.kr / 2 <= RING_MAX, T2B_ERR_UNSUPPORTED, "too many low-resolution ring pixels");
     N.projR = (float2*)net_dalloc(W, (size_t)KO * N.nring * sizeof(float2));
     N.rth = net_dalloc(W, (size_t)KO * N.kr * sizeof(bf16));
     N.rtl = net_dalloc(W, (size_t)KO * N.kr * sizeof(bf16));
@@ -1683,7 +1716,7 @@ void proposal_infer(t2b_ctx* c, const Work& w, cudaStream_t st)
         k_topk<<<w.n, 1024, N.KO * sizeof(unsigned), st>>>(N.logits, (const bf16*)N.thb + N.L.b3, tb.skip, N.KO, N.k1,
                                                            N.cand1, 0);
         const long long nc = (long long)w.n * N.k1;
-        k_ring_images<<<w.n * tb.T, 128, 0, st>>>(tb, w, N.ring, N.nring, N.kr, (bf16*)N.rbh, (bf16*)N.rbl, N.w2r);
+        k_ring_images<<<w.n, 256, 0, st>>>(tb, w, N.ring, N.nring, N.kr, (bf16*)N.rbh, (bf16*)N.rbl, N.w2r);
         k_rescore_gather<<<(int)((nc * 32 + 255) / 256), 256, 0, st>>>(w.n, N.k1, N.nring, N.kr, N.cand1, N.projR,
                                                                        (const bf16*)N.rth, (const bf16*)N.rtl, N.w2r,
                                                                        (bf16*)N.rah, (bf16*)N.ral, N.rnorm);
