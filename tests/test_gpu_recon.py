@@ -270,3 +270,35 @@ def test_gridding_reconstruction_matches_oracle(symmetric_grid, with_map):
     # and it is not the skip-gridding map
     skip = es.reconstruct(0, N, tau2=tau2, tau2_fudge=1.1, minres_map=1)
     assert np.max(np.abs(skip - got)) > 1e-3 * np.max(np.abs(got))
+
+
+@pytest.mark.parametrize("r_max", [32, 64], ids=["pad131_prime", "pad259_7x37"])
+def test_gridding_on_odd_boxes_from_a_written_grid(t2b, r_max):
+    """The gridding iterations' transforms at pad sizes 131 (a prime: first-stage conjugate pairs)
+    and 259 = 7 x 37 (37 in pairs, then the radix-7 register stage), on a seeded grid written into
+    the library's device grid through its DLPack view (no E-step), against the oracle."""
+    import torch
+    import t2relion_b200.parallel as par
+    ps = 2 * (2 * r_max + 1) + 1
+    ori = 2 * r_max
+    rng = np.random.default_rng(r_max)
+    shape = (ps, ps, ps // 2 + 1)
+    data = (rng.normal(size=shape) + 1j * rng.normal(size=shape)).astype(np.complex64)
+    w = rng.uniform(0.5, 2.0, size=shape).astype(np.float32)
+    es = t2b.EStep(0)
+    es.init_backprojector(0, 3, ps, r_max, 2)
+    nvox = int(np.prod(shape))
+    d_ptr, w_ptr = es.backprojector_device_ptrs(0)
+    dv = par.device_view(d_ptr, 2 * nvox, 0)
+    wv = par.device_view(w_ptr, nvox, 0)
+    dv.copy_(torch.from_numpy(np.ascontiguousarray(data).view(np.float32).reshape(-1)))
+    wv.copy_(torch.from_numpy(w.reshape(-1)))
+    torch.cuda.synchronize()
+    del dv, wv
+    gd, gw = es.get_backprojector(0)
+    assert np.array_equal(gd, data) and np.array_equal(gw, w)
+    got = es.reconstruct(0, ori, gridding_iter=2, normalise=3.0)
+    es.close()
+    ref = ro.reconstruct_map(data.astype(np.complex128), w.astype(np.float64), r_max, 2, ori, gridding_iter=2,
+                             normalise=3.0)
+    _map_close(got, ref)
